@@ -1,0 +1,84 @@
+"""Loader of libhodlr_b200.so and ctypes signatures of include/hodlr_b200.h."""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libhodlr_b200.so")
+
+OK = 0
+ERR_ARG = 1
+ERR_CUDA = 2
+ERR_ALLOC = 3
+ERR_UNSUPPORTED = 4
+ERR_SINGULAR = 5
+ERR_STATE = 6
+ERR_NONFINITE = 7
+ERR_TIMEOUT = 8
+
+_STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "device memory exhausted",
+           4: "unsupported on the GPU path", 5: "exact-zero pivot", 6: "call out of order",
+           7: "non-finite value", 8: "device wait timed out"}
+
+
+def status_string(s):
+    return _STATUS.get(s, "unknown status")
+
+
+class KernelDesc(ctypes.Structure):
+    _fields_ = [("type", ctypes.c_int), ("length_scale", ctypes.c_double),
+                ("diag_shift", ctypes.c_double), ("diag_replace", ctypes.c_int),
+                ("diag_value", ctypes.c_double)]
+
+
+_H = ctypes.c_void_p
+_I = ctypes.c_int
+_D = ctypes.c_double
+_PD = ctypes.POINTER(ctypes.c_double)
+_PI = ctypes.POINTER(ctypes.c_int)
+_V = ctypes.c_void_p
+
+SIGNATURES = {
+    "hodlr_create_kernel": (_I, [ctypes.POINTER(_H), _I, _I, _PD, ctypes.POINTER(KernelDesc), _I]),
+    "hodlr_create_dense": (_I, [ctypes.POINTER(_H), _I, _PD, _I, _I]),
+    "hodlr_create_fnptr": (_I, [ctypes.POINTER(_H), _I, _I, _V, _V, _I]),
+    "hodlr_destroy": (None, [_H]),
+    "hodlr_set_lr_tolerance": (_I, [_H, _D]),
+    "hodlr_set_min_pivot": (_I, [_H, _D]),
+    "hodlr_set_lr_method": (_I, [_H, ctypes.c_char_p]),
+    "hodlr_compress": (_I, [_H]),
+    "hodlr_factorize": (_I, [_H]),
+    "hodlr_solve": (_I, [_H, _I, _PD, _I, _PD, _I]),
+    "hodlr_solve_device": (_I, [_H, _I, _V, _I, _V, _I]),
+    "hodlr_kernel_matvec_device": (_I, [_H, _I, _V, _I, _V, _I]),
+    "hodlr_residual": (_I, [_H, _I, _PD, _I, _PD, _I, _PD]),
+    "hodlr_get_times": (_I, [_H, _PD, _PD, _PD, _PD]),
+    "hodlr_get_num_levels": (_I, [_H, _PI]),
+    "hodlr_get_num_blocks": (_I, [_H, _PI]),
+    "hodlr_get_block_info": (_I, [_H, _I, _PI, _PI, _PI, _PI, _PI, _PI, _PI]),
+    "hodlr_get_ranks": (_I, [_H, _PI]),
+    "hodlr_get_pivots": (_I, [_H, _I, _PI, _PI, _PI]),
+    "hodlr_get_lowrank": (_I, [_H, _I, _PD, _PD]),
+    "hodlr_get_block_margin": (_I, [_H, _I, _PD, _PI]),
+    "hodlr_get_aca_stats": (_I, [_H, _PI, _PD, _PD]),
+    "hodlr_status_string": (ctypes.c_char_p, [_I]),
+    "hodlr_last_error": (ctypes.c_char_p, [_H]),
+}
+
+_LIB = None
+
+
+def lib():
+    """Load the CUDA library; raise if it has not been built."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                "libhodlr_b200.so is missing: build it with `python -m dense_hodlr_b200.build` "
+                "(the solver has no CPU fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _LIB = L
+    return _LIB

@@ -1,0 +1,169 @@
+// Grouped batched FP64 GEMMs for the Woodbury level updates.
+//
+// Replaces the per-node Eigen products of recLU_Factorize / recLU_Solve:
+//   V^T * (K^-1 U) and V^T * X   (src/HODLR_Matrix.cpp:672-673, 679-680, 743-744)
+//   X - (K^-1 U) * y             (src/HODLR_Matrix.cpp:686-687, 749-750)
+// All nodes of one tree level are one launch.  A tile list maps every CTA to
+// (problem, tile row, tile column, K split); TN products with a long
+// reduction dimension (the top levels) are split along K into a workspace
+// and summed in a fixed order by gemm_splitk_reduce, so results do not
+// depend on scheduling.
+#include "common.cuh"
+#include "gemm.h"
+
+namespace {
+
+constexpr int BM = 64, BN = 64, BK = 16, NT = 256;
+
+// mode: 0 store C = A^T B (or split partial), 1 C -= A B
+template <bool TRANS_A, int MODE>
+__global__ void __launch_bounds__(NT) gemm_kernel(const GemmProblem* __restrict__ probs,
+                                                  const int4* __restrict__ tiles,
+                                                  double* __restrict__ ws) {
+  __shared__ double As[BK][BM + 2];
+  __shared__ double Bs[BK][BN + 2];
+  const int4 t = tiles[blockIdx.x];
+  const GemmProblem P = probs[t.x];
+  const int m0 = t.y * BM, n0 = t.z * BN;
+  const int ks = t.w;
+  const int kchunk = P.kchunk > 0 ? P.kchunk : P.K;
+  const int kb = ks * kchunk, ke = min(P.K, kb + kchunk);
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  double acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+
+  for (int k0 = kb; k0 < ke; k0 += BK) {
+    // A tile -> As[kk][mm]
+#pragma unroll
+    for (int r = 0; r < (BK * BM) / NT; ++r) {
+      int e = threadIdx.x + r * NT;
+      int kk, mm;
+      double v = 0.0;
+      if (TRANS_A) {  // A is K x M (column-major): contiguous along k
+        kk = e % BK;
+        mm = e / BK;
+        int gk = k0 + kk, gm = m0 + mm;
+        if (gk < ke && gm < P.M) v = __ldg(P.A + (int64_t)gm * P.lda + gk);
+      } else {  // A is M x K: contiguous along m
+        mm = e % BM;
+        kk = e / BM;
+        int gk = k0 + kk, gm = m0 + mm;
+        if (gk < ke && gm < P.M) v = __ldg(P.A + (int64_t)gk * P.lda + gm);
+      }
+      As[kk][mm] = v;
+    }
+    // B tile (K x N, column-major) -> Bs[kk][nn]
+#pragma unroll
+    for (int r = 0; r < (BK * BN) / NT; ++r) {
+      int e = threadIdx.x + r * NT;
+      int kk = e % BK, nn = e / BK;
+      int gk = k0 + kk, gn = n0 + nn;
+      double v = 0.0;
+      if (gk < ke && gn < P.N) v = __ldg(P.B + (int64_t)gn * P.ldb + gk);
+      Bs[kk][nn] = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < BK; ++kk) {
+      double a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = As[kk][ty * 4 + i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx * 4 + j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+    }
+    __syncthreads();
+  }
+  // epilogue
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    int gm = m0 + ty * 4 + i;
+    if (gm >= P.M) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      int gn = n0 + tx * 4 + j;
+      if (gn >= P.N) continue;
+      if (MODE == 1) {
+        double* c = P.C + (int64_t)gn * P.ldc + gm;
+        *c = *c - acc[i][j];
+      } else if (P.splits > 1) {
+        ws[P.ws_off + ((int64_t)ks * P.N + gn) * P.M + gm] = acc[i][j];
+      } else {
+        P.C[(int64_t)gn * P.ldc + gm] = acc[i][j];
+      }
+    }
+  }
+}
+
+__global__ void splitk_reduce_kernel(const GemmProblem* __restrict__ probs, int nprob,
+                                     const double* __restrict__ ws) {
+  const GemmProblem P = probs[blockIdx.y];
+  if (P.splits <= 1) return;
+  const int64_t total = (int64_t)P.M * P.N;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int q = 0; q < P.splits; ++q) s += ws[P.ws_off + q * total + e];
+    int gm = (int)(e % P.M), gn = (int)(e / P.M);
+    P.C[(int64_t)gn * P.ldc + gm] = s;
+  }
+}
+
+}  // namespace
+
+int gemm_tn_launch(const GemmProblem* d_probs, const int4* d_tiles, int ntiles, int nprob,
+                   double* d_ws, bool any_split, cudaStream_t s) {
+  if (ntiles == 0) return 0;
+  gemm_kernel<true, 0><<<ntiles, NT, 0, s>>>(d_probs, d_tiles, d_ws);
+  if (any_split) splitk_reduce_kernel<<<dim3(64, nprob), 256, 0, s>>>(d_probs, nprob, d_ws);
+  return (int)cudaGetLastError();
+}
+
+int gemm_nn_sub_launch(const GemmProblem* d_probs, const int4* d_tiles, int ntiles,
+                       cudaStream_t s) {
+  if (ntiles == 0) return 0;
+  gemm_kernel<false, 1><<<ntiles, NT, 0, s>>>(d_probs, d_tiles, nullptr);
+  return (int)cudaGetLastError();
+}
+
+// Host-side planning: tile list and split-K workspace layout.
+void gemm_plan(std::vector<GemmProblem>& probs, std::vector<int4>& tiles, int64_t& ws_elems,
+               bool allow_split, int target_ctas) {
+  tiles.clear();
+  ws_elems = 0;
+  int64_t mn_tiles = 0;
+  for (auto& p : probs) mn_tiles += (int64_t)((p.M + BM - 1) / BM) * ((p.N + BN - 1) / BN);
+  for (size_t q = 0; q < probs.size(); ++q) {
+    GemmProblem& p = probs[q];
+    if (p.M <= 0 || p.N <= 0 || p.K <= 0) {
+      p.splits = 1;
+      p.kchunk = 0;
+      continue;
+    }
+    int tm = (p.M + BM - 1) / BM, tn = (p.N + BN - 1) / BN;
+    int splits = 1;
+    if (allow_split && mn_tiles < target_ctas) {
+      int want = (int)((target_ctas + mn_tiles - 1) / mn_tiles);
+      int maxs = std::max(1, p.K / 512);
+      splits = std::max(1, std::min(want, maxs));
+    }
+    int kchunk = (p.K + splits - 1) / splits;
+    kchunk = ((kchunk + BK - 1) / BK) * BK;
+    splits = (p.K + kchunk - 1) / kchunk;
+    p.splits = splits;
+    p.kchunk = splits > 1 ? kchunk : 0;
+    if (splits > 1) {
+      p.ws_off = ws_elems;
+      ws_elems += (int64_t)splits * p.M * p.N;
+    }
+    for (int ks = 0; ks < splits; ++ks)
+      for (int j = 0; j < tn; ++j)
+        for (int i = 0; i < tm; ++i) tiles.push_back(make_int4((int)q, i, j, ks));
+  }
+}

@@ -1,0 +1,27 @@
+// Grouped batched FP64 GEMM interface (gemm.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <algorithm>
+#include <vector>
+
+// One product of a group.  TN: C (M x N) = A^T B with A K x M, B K x N.
+// NN-sub: C (M x N) -= A B with A M x K, B K x N.  All column-major.
+struct GemmProblem {
+  const double* A;
+  const double* B;
+  double* C;
+  int M, N, K;
+  int lda, ldb, ldc;
+  int splits;      // K splits (TN only), set by gemm_plan
+  int kchunk;      // K per split
+  int64_t ws_off;  // workspace offset of split partials
+};
+
+void gemm_plan(std::vector<GemmProblem>& probs, std::vector<int4>& tiles, int64_t& ws_elems,
+               bool allow_split, int target_ctas);
+int gemm_tn_launch(const GemmProblem* d_probs, const int4* d_tiles, int ntiles, int nprob,
+                   double* d_ws, bool any_split, cudaStream_t s);
+int gemm_nn_sub_launch(const GemmProblem* d_probs, const int4* d_tiles, int ntiles,
+                       cudaStream_t s);

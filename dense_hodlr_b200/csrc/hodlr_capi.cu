@@ -1,0 +1,1272 @@
+// Host orchestration and C ABI of the B200 HODLR solver (include/hodlr_b200.h).
+//
+// Replaces, for the recLU path, HODLR_Matrix (include/HODLR_Matrix.hpp:38-413,
+// src/HODLR_Matrix.cpp) and HODLR_Tree::createDefaultTree
+// (src/HODLR_Tree.cpp:33-132).  The pointer tree of the reference becomes
+// level arrays; the recursions of recLU_Factorize / recLU_Solve
+// (src/HODLR_Matrix.cpp:612-755) become bottom-up sweeps over levels in which
+// every node of a level is processed by one batched launch.
+//
+// HBM layout (N = matrix size, column-major, leading dimension N):
+//   pts        dim x N coordinates (SoA)            or A  N x N dense input
+//   W_l, V_l   N x kcap_l per inner level l: the blocks of a level tile the
+//              rows (W) and the columns (V) of the matrix exactly once
+//   Y          N x C, C = sum_l kmax_l: level l occupies columns
+//              [coff_l, coff_l + kmax_l); after the factorization it holds
+//              K^-1 U for every node (topDiagSoln_LR / bottDiagSoln_LR)
+//   leaf LU    sum over leaves of s^2, plus a row permutation (N ints)
+//   S_l        per node (k_b + k_t)^2 capacitance LU + pivots
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/hodlr_b200.h"
+#include "common.cuh"
+#include "gemm.h"
+#include "kmatvec.h"
+#include "lu.h"
+
+int aca_launch(const AcaLaunch& L, int nt, int kcap_max, bool cooperative, cudaStream_t s);
+int aca_max_coresident(int nt, int kcap_max, int* per_sm);
+
+namespace {
+
+struct DevPlan {  // a grouped GEMM uploaded to the device
+  GemmProblem* probs = nullptr;
+  int4* tiles = nullptr;
+  int nprob = 0, ntiles = 0;
+  int64_t ws_elems = 0;
+  bool any_split = false;
+};
+
+struct Level {
+  std::vector<int> nmin, nsplit, nmax;  // inner nodes of this level
+  int nblocks() const { return 2 * (int)nmin.size(); }
+  int ub_max = 0;  // largest min(m, n) of the level's blocks
+  int kcap = 0;
+  double* W = nullptr;
+  double* V = nullptr;
+  unsigned char* cR = nullptr;
+  unsigned char* cC = nullptr;
+  int* prow = nullptr;
+  int* pcol = nullptr;
+  AcaState* d_st = nullptr;
+  std::vector<AcaState> st;
+  int G = 1;
+  int kmax = 0, coff = 0;
+  // factorization
+  double* S = nullptr;
+  int* piv = nullptr;
+  SchurNode* d_nodes = nullptr;
+  std::vector<SchurNode> nodes;
+  int max_sd = 0;
+  DevPlan tn, nn;          // factor GEMMs
+  int solve_nrhs = -1;     // nrhs the solve plans were built for
+  DevPlan stn, snn;        // solve GEMMs
+  SchurNode* d_snodes = nullptr;  // solve: r_off into the solve buffer
+  int64_t zs_elems = 0;
+};
+
+void block_geom(const Level& L, int q, int& r0, int& c0, int& m, int& n) {
+  int p = q >> 1;
+  if ((q & 1) == 0) {  // top off-diagonal: rows [min, split], cols [split+1, max]
+    r0 = L.nmin[p];
+    c0 = L.nsplit[p] + 1;
+    m = L.nsplit[p] - L.nmin[p] + 1;
+    n = L.nmax[p] - L.nsplit[p];
+  } else {  // bottom off-diagonal: rows [split+1, max], cols [min, split]
+    r0 = L.nsplit[p] + 1;
+    c0 = L.nmin[p];
+    m = L.nmax[p] - L.nsplit[p];
+    n = L.nsplit[p] - L.nmin[p] + 1;
+  }
+}
+
+}  // namespace
+
+struct hodlr_handle_s {
+  int n = 0, leaf = 30, dim = 0;
+  bool dense = false;
+  hx_kparams kp{};
+  double* d_pts = nullptr;
+  double* d_A = nullptr;
+  double tol = 1e-6;
+  int minPivot = 0;
+  std::vector<Level> lv;
+  std::vector<int> leaf_min, leaf_size;
+  int* d_leaf_min = nullptr;
+  int* d_leaf_size = nullptr;
+  int64_t* d_lu_off = nullptr;
+  double* d_lu = nullptr;
+  int* d_perm = nullptr;
+  int smax = 0;
+  double* Y = nullptr;
+  int64_t C = 0;
+  double* ws = nullptr;  // GEMM split-K / kmatvec workspace
+  int64_t ws_cap = 0;
+  double* Z = nullptr;  // per-level Schur right-hand sides (factor)
+  int64_t z_cap = 0;
+  double* X = nullptr;  // solve panel N x nrhs
+  int x_cols = 0;
+  double* zs = nullptr;  // solve Schur right-hand sides
+  int64_t zs_cap = 0;
+  double* part = nullptr;
+  int64_t part_cap = 0;
+  unsigned* bar = nullptr;
+  int bar_cap = 0;
+  AcaBlock* d_blocks = nullptr;
+  int blocks_cap = 0;
+  unsigned* d_err = nullptr;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  int num_sms = 0;
+  bool compressed = false, factored = false;
+  double t_lr = 0, t_fact = 0, t_solve = 0, t_total = 0;
+  int aca_launches = 0;
+  double aca_seconds = 0, aca_bytes = 0;
+  std::string err;
+};
+
+namespace {
+
+int fail(hodlr_t h, int code, const std::string& msg) {
+  if (h) h->err = msg;
+  return code;
+}
+
+int cuda_fail(hodlr_t h, cudaError_t e, const char* where) {
+  return fail(h, e == cudaErrorMemoryAllocation ? HODLR_ERR_ALLOC : HODLR_ERR_CUDA,
+              std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call)                                               \
+  do {                                                         \
+    cudaError_t e__ = (call);                                  \
+    if (e__ != cudaSuccess) return cuda_fail(h, e__, #call);   \
+  } while (0)
+
+template <class T>
+cudaError_t dalloc(T** p, size_t count) {
+  *p = nullptr;
+  if (count == 0) return cudaSuccess;
+  return cudaMalloc((void**)p, sizeof(T) * count);
+}
+
+template <class T>
+void dfree(T*& p) {
+  if (p) cudaFree((void*)p);
+  p = nullptr;
+}
+
+void free_plan(DevPlan& p) {
+  dfree(p.probs);
+  dfree(p.tiles);
+  p = DevPlan();
+}
+
+void free_factor(hodlr_t h) {
+  for (auto& L : h->lv) {
+    dfree(L.S);
+    dfree(L.piv);
+    dfree(L.d_nodes);
+    dfree(L.d_snodes);
+    free_plan(L.tn);
+    free_plan(L.nn);
+    free_plan(L.stn);
+    free_plan(L.snn);
+    L.solve_nrhs = -1;
+    L.nodes.clear();
+  }
+  dfree(h->d_lu);
+  dfree(h->d_lu_off);
+  dfree(h->d_perm);
+  dfree(h->Y);
+  h->factored = false;
+}
+
+void free_compress(hodlr_t h) {
+  free_factor(h);
+  for (auto& L : h->lv) {
+    dfree(L.W);
+    dfree(L.V);
+    dfree(L.cR);
+    dfree(L.cC);
+    dfree(L.prow);
+    dfree(L.pcol);
+    dfree(L.d_st);
+    L.st.clear();
+    L.kcap = 0;
+  }
+  h->compressed = false;
+}
+
+// createDefaultTree (src/HODLR_Tree.cpp:33-132): root is a leaf iff N < leaf;
+// a child splits iff its size > leaf; a left-type child splits at
+// min + floor(s/2) - 1, a right-type child at max - floor(s/2).  Nodes of a
+// level are listed left to right (pre-order pushes), leaves in index order.
+void build_tree(hodlr_t h) {
+  h->lv.clear();
+  h->leaf_min.clear();
+  h->leaf_size.clear();
+  const int N = h->n, leaf = h->leaf;
+  if (N < leaf || N < 2) {
+    h->leaf_min.push_back(0);
+    h->leaf_size.push_back(N);
+    return;
+  }
+  struct Fr {
+    int level, mn, split, mx;
+  };
+  std::vector<Fr> stack;
+  stack.push_back({0, 0, N / 2 - 1, N - 1});
+  auto push_inner = [&](const Fr& f) {
+    if ((int)h->lv.size() <= f.level) h->lv.resize(f.level + 1);
+    Level& L = h->lv[f.level];
+    L.nmin.push_back(f.mn);
+    L.nsplit.push_back(f.split);
+    L.nmax.push_back(f.mx);
+  };
+  // explicit pre-order, left before right
+  while (!stack.empty()) {
+    Fr f = stack.back();
+    stack.pop_back();
+    push_inner(f);
+    int top = f.split - f.mn + 1, bott = f.mx - f.split;
+    Fr right{f.level + 1, f.mn + top, -1, f.mx};
+    Fr left{f.level + 1, f.mn, -1, f.mn + top - 1};
+    bool rsplit = bott > leaf, lsplit = top > leaf;
+    if (rsplit) right.split = f.mx - bott / 2;
+    if (lsplit) left.split = f.mn + top / 2 - 1;
+    if (rsplit) stack.push_back(right);
+    if (lsplit) stack.push_back(left);
+  }
+  // Walk the tree again to list the leaves in index order.
+  std::vector<Fr> st2;
+  st2.push_back({0, 0, N / 2 - 1, N - 1});
+  while (!st2.empty()) {
+    Fr f = st2.back();
+    st2.pop_back();
+    if (f.split < 0) {
+      h->leaf_min.push_back(f.mn);
+      h->leaf_size.push_back(f.mx - f.mn + 1);
+      continue;
+    }
+    int top = f.split - f.mn + 1, bott = f.mx - f.split;
+    Fr right{f.level + 1, f.mn + top, -1, f.mx};
+    Fr left{f.level + 1, f.mn, -1, f.mn + top - 1};
+    if (bott > leaf) right.split = f.mx - bott / 2;
+    if (top > leaf) left.split = f.mn + top / 2 - 1;
+    st2.push_back(right);
+    st2.push_back(left);
+  }
+  for (auto& L : h->lv) {
+    L.ub_max = 0;
+    for (int q = 0; q < L.nblocks(); ++q) {
+      int r0, c0, m, n;
+      block_geom(L, q, r0, c0, m, n);
+      L.ub_max = std::max(L.ub_max, std::min(m, n));
+    }
+  }
+  h->smax = 0;
+  for (int s : h->leaf_size) h->smax = std::max(h->smax, s);
+}
+
+int ensure_ws(hodlr_t h, int64_t elems) {
+  if (elems <= h->ws_cap) return HODLR_OK;
+  dfree(h->ws);
+  CK(dalloc(&h->ws, (size_t)elems));
+  h->ws_cap = elems;
+  return HODLR_OK;
+}
+
+int check_dev_err(hodlr_t h, const char* where) {
+  unsigned e = 0;
+  CK(cudaMemcpy(&e, h->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost));
+  if (e == 0) return HODLR_OK;
+  CK(cudaMemset(h->d_err, 0, sizeof(unsigned)));
+  if (e & DEV_ERR_TIMEOUT) return fail(h, HODLR_ERR_TIMEOUT, std::string(where) + ": device wait timed out");
+  if (e & DEV_ERR_NONFINITE) return fail(h, HODLR_ERR_NONFINITE, std::string(where) + ": non-finite value");
+  if (e & DEV_ERR_SINGULAR) return fail(h, HODLR_ERR_SINGULAR, std::string(where) + ": exact-zero pivot");
+  return fail(h, HODLR_ERR_CUDA, where);
+}
+
+EntrySrc make_src(hodlr_t h) {
+  EntrySrc s;
+  s.pts = h->d_pts;
+  s.A = h->d_A;
+  s.ld = h->n;
+  s.kp = h->kp;
+  s.dense = h->dense ? 1 : 0;
+  return s;
+}
+
+// Grow level L to `cap` columns, keeping the first `keep` columns.
+int grow_level(hodlr_t h, Level& L, int cap) {
+  const int64_t N = h->n;
+  double *W2 = nullptr, *V2 = nullptr;
+  CK(dalloc(&W2, (size_t)(N * cap)));
+  cudaError_t e = dalloc(&V2, (size_t)(N * cap));
+  if (e != cudaSuccess) {
+    dfree(W2);
+    return cuda_fail(h, e, "grow_level");
+  }
+  if (L.W && L.kcap > 0) {
+    CK(cudaMemcpyAsync(W2, L.W, sizeof(double) * N * L.kcap, cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(V2, L.V, sizeof(double) * N * L.kcap, cudaMemcpyDeviceToDevice, h->stream));
+  }
+  CK(cudaStreamSynchronize(h->stream));
+  dfree(L.W);
+  dfree(L.V);
+  L.W = W2;
+  L.V = V2;
+  L.kcap = cap;
+  return HODLR_OK;
+}
+
+void fill_block(hodlr_t h, Level& L, int q, AcaBlock& B) {
+  int r0, c0, m, n;
+  block_geom(L, q, r0, c0, m, n);
+  (void)h;
+  B.st = L.d_st + q;
+  B.W = L.W + r0;
+  B.V = L.V + c0;
+  B.cR = L.cR + r0;
+  B.cC = L.cC + c0;
+  B.prow = L.prow + r0;
+  B.pcol = L.pcol + c0;
+  B.r0 = r0;
+  B.c0 = c0;
+  B.m = m;
+  B.n = n;
+  B.kcap = L.kcap;
+  B.level = 0;
+}
+
+bool level_done(const Level& L) {
+  for (auto& s : L.st)
+    if (s.status != ACA_DONE) return false;
+  return true;
+}
+
+// Run one ACA launch over `blocks` with group size G.
+int run_aca(hodlr_t h, std::vector<AcaBlock>& blocks, int G, int nt, int kcap_max) {
+  const int nb = (int)blocks.size();
+  if (nb == 0) return HODLR_OK;
+  if (nb > h->blocks_cap) {
+    dfree(h->d_blocks);
+    CK(dalloc(&h->d_blocks, (size_t)nb));
+    h->blocks_cap = nb;
+  }
+  CK(cudaMemcpyAsync(h->d_blocks, blocks.data(), sizeof(AcaBlock) * nb, cudaMemcpyHostToDevice,
+                     h->stream));
+  int64_t stride = 16 + 2 * (int64_t)kcap_max;
+  int64_t need = stride * nb * G;
+  if (need > h->part_cap) {
+    dfree(h->part);
+    CK(dalloc(&h->part, (size_t)need));
+    h->part_cap = need;
+  }
+  if (nb > h->bar_cap) {
+    dfree(h->bar);
+    CK(dalloc(&h->bar, (size_t)nb));
+    h->bar_cap = nb;
+  }
+  CK(cudaMemsetAsync(h->bar, 0, sizeof(unsigned) * nb, h->stream));
+  AcaLaunch L;
+  L.blocks = h->d_blocks;
+  L.nblocks = nb;
+  L.G = G;
+  L.ld = h->n;
+  L.tol = h->tol;
+  L.minPivot = (double)h->minPivot;
+  L.part = h->part;
+  L.part_stride = stride;
+  L.bar = h->bar;
+  L.err = h->d_err;
+  L.src = make_src(h);
+  CK(cudaEventRecord(h->ev0, h->stream));
+  int rc = aca_launch(L, nt, kcap_max, G > 1, h->stream);
+  if (rc) return cuda_fail(h, (cudaError_t)rc, "aca_launch");
+  CK(cudaEventRecord(h->ev1, h->stream));
+  CK(cudaEventSynchronize(h->ev1));
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+  h->aca_seconds += ms * 1e-3;
+  h->aca_launches += 1;
+  return check_dev_err(h, "ACA");
+}
+
+int do_compress(hodlr_t h) {
+  if (h->compressed) return HODLR_OK;
+  free_compress(h);
+  const int64_t N = h->n;
+  h->aca_launches = 0;
+  h->aca_seconds = 0;
+  h->aca_bytes = 0;
+  const int init_cap = 64;
+  for (auto& L : h->lv) {
+    int cap = std::max(1, std::min(L.ub_max, init_cap));
+    int rc = grow_level(h, L, cap);
+    if (rc) return rc;
+    CK(dalloc(&L.cR, (size_t)N));
+    CK(dalloc(&L.cC, (size_t)N));
+    CK(dalloc(&L.prow, (size_t)N));
+    CK(dalloc(&L.pcol, (size_t)N));
+    CK(cudaMemsetAsync(L.cR, 0, N, h->stream));
+    CK(cudaMemsetAsync(L.cC, 0, N, h->stream));
+    const int nb = L.nblocks();
+    CK(dalloc(&L.d_st, (size_t)nb));
+    L.st.assign(nb, AcaState());
+    for (auto& s : L.st) {
+      s.frob2 = 0;
+      s.eps = 1;
+      s.margin = HUGE_VAL;
+      s.k = 0;
+      s.cur = 0;
+      s.status = ACA_RUNNING;
+      s.iters = 0;
+      s.rank = 0;
+      s.near = 0;
+    }
+    CK(cudaMemcpyAsync(L.d_st, L.st.data(), sizeof(AcaState) * nb, cudaMemcpyHostToDevice,
+                       h->stream));
+  }
+  for (int round = 0; round < 64; ++round) {
+    int kcap_max = 1;
+    for (auto& L : h->lv) kcap_max = std::max(kcap_max, L.kcap);
+    int per_sm256 = 0, per_sm128 = 0;
+    if (aca_max_coresident(256, kcap_max, &per_sm256) ||
+        aca_max_coresident(128, kcap_max, &per_sm128))
+      return fail(h, HODLR_ERR_CUDA, "occupancy query failed");
+    const int P = std::max(1, per_sm256) * h->num_sms;
+    std::vector<AcaBlock> pooled;
+    std::vector<std::pair<int64_t, AcaBlock>> pooled_sorted;
+    for (auto& L : h->lv) {
+      if (level_done(L)) continue;
+      const int nb = L.nblocks();
+      int G = P / nb;
+      if (G >= 2) {
+        L.G = G;
+        std::vector<AcaBlock> bl(nb);
+        for (int q = 0; q < nb; ++q) fill_block(h, L, q, bl[q]);
+        int rc = run_aca(h, bl, G, 256, kcap_max);
+        if (rc) return rc;
+      } else {
+        L.G = 1;
+        for (int q = 0; q < nb; ++q) {
+          if (L.st[q].status == ACA_DONE) continue;
+          AcaBlock B;
+          fill_block(h, L, q, B);
+          pooled_sorted.push_back({(int64_t)B.m * B.n, B});
+        }
+      }
+    }
+    std::stable_sort(pooled_sorted.begin(), pooled_sorted.end(),
+                     [](const std::pair<int64_t, AcaBlock>& a,
+                        const std::pair<int64_t, AcaBlock>& b) { return a.first > b.first; });
+    for (auto& pb : pooled_sorted) pooled.push_back(pb.second);
+    if (!pooled.empty()) {
+      int rc = run_aca(h, pooled, 1, 128, kcap_max);
+      if (rc) return rc;
+    }
+    // read back states, grow where needed
+    bool all_done = true;
+    for (auto& L : h->lv) {
+      const int nb = L.nblocks();
+      CK(cudaMemcpy(L.st.data(), L.d_st, sizeof(AcaState) * nb, cudaMemcpyDeviceToHost));
+      int need = 0;
+      for (int q = 0; q < nb; ++q) {
+        auto& s = L.st[q];
+        if (s.status == ACA_ERROR) return fail(h, HODLR_ERR_TIMEOUT, "ACA group failed");
+        if (s.status == ACA_NEED_CAP) need = std::max(need, L.kcap * 2);
+        if (s.status == ACA_NEED_CAP_POST) need = std::max(need, s.rank);
+        if (s.status != ACA_DONE) all_done = false;
+      }
+      if (need > 0) {
+        int cap = std::min(std::max(need, L.kcap + 1), std::max(L.ub_max, L.kcap + 1));
+        int rc = grow_level(h, L, cap);
+        if (rc) return rc;
+        for (auto& s : L.st) {
+          if (s.status == ACA_NEED_CAP) s.status = ACA_RUNNING;
+          if (s.status == ACA_NEED_CAP_POST) s.status = ACA_POST;
+        }
+        CK(cudaMemcpy(L.d_st, L.st.data(), sizeof(AcaState) * nb, cudaMemcpyHostToDevice));
+      }
+    }
+    if (all_done) break;
+  }
+  for (auto& L : h->lv)
+    if (!level_done(L)) return fail(h, HODLR_ERR_STATE, "ACA did not converge in 64 rounds");
+  // ranks, level widths, column offsets, algorithmic bytes
+  int64_t coff = 0;
+  double bytes = 0;
+  for (auto& L : h->lv) {
+    L.kmax = 0;
+    for (int q = 0; q < L.nblocks(); ++q) {
+      L.kmax = std::max(L.kmax, L.st[q].rank);
+      int r0, c0, m, n;
+      block_geom(L, q, r0, c0, m, n);
+      double K = L.st[q].iters;
+      bytes += 8.0 * (m + n) * (K * (K - 1) + K * (1 + h->dim));
+    }
+    L.coff = (int)coff;
+    coff += L.kmax;
+  }
+  h->C = coff;
+  h->aca_bytes = bytes;
+  h->compressed = true;
+  return HODLR_OK;
+}
+
+int upload_plan(hodlr_t h, std::vector<GemmProblem>& probs, bool split, DevPlan& out) {
+  std::vector<int4> tiles;
+  int64_t ws = 0;
+  gemm_plan(probs, tiles, ws, split, 2 * h->num_sms * 4);
+  free_plan(out);
+  out.nprob = (int)probs.size();
+  out.ntiles = (int)tiles.size();
+  out.ws_elems = ws;
+  out.any_split = false;
+  for (auto& p : probs) out.any_split |= p.splits > 1;
+  if (out.nprob) {
+    CK(dalloc(&out.probs, (size_t)out.nprob));
+    CK(cudaMemcpy(out.probs, probs.data(), sizeof(GemmProblem) * out.nprob,
+                  cudaMemcpyHostToDevice));
+  }
+  if (out.ntiles) {
+    CK(dalloc(&out.tiles, (size_t)out.ntiles));
+    CK(cudaMemcpy(out.tiles, tiles.data(), sizeof(int4) * out.ntiles, cudaMemcpyHostToDevice));
+  }
+  return ensure_ws(h, ws);
+}
+
+int level_rank(const Level& L, int q) { return L.st[q].rank; }
+
+__global__ void y_init_kernel(double* Y, int64_t ldy, int coff, const double* W, int64_t ldw,
+                              const int* r0s, const int* ms, const int* ranks, int nb) {
+  int q = blockIdx.y;
+  if (q >= nb) return;
+  const int r0 = r0s[q], m = ms[q], rank = ranks[q];
+  for (int c = blockIdx.z; c < rank; c += gridDim.z)
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x)
+      Y[(int64_t)(coff + c) * ldy + r0 + i] = W[(int64_t)c * ldw + r0 + i];
+}
+
+int do_factorize(hodlr_t h) {
+  if (h->factored) return HODLR_OK;
+  int rc = do_compress(h);
+  if (rc) return rc;
+  free_factor(h);
+  const int64_t N = h->n;
+  CK(cudaEventRecord(h->ev0, h->stream));
+  // leaves: assemble + LU
+  const int nl = (int)h->leaf_min.size();
+  std::vector<int64_t> lu_off(nl);
+  int64_t tot = 0;
+  for (int p = 0; p < nl; ++p) {
+    lu_off[p] = tot;
+    tot += (int64_t)h->leaf_size[p] * h->leaf_size[p];
+  }
+  CK(dalloc(&h->d_lu, (size_t)tot));
+  CK(dalloc(&h->d_lu_off, (size_t)nl));
+  CK(dalloc(&h->d_perm, (size_t)N));
+  CK(cudaMemcpyAsync(h->d_lu_off, lu_off.data(), sizeof(int64_t) * nl, cudaMemcpyHostToDevice,
+                     h->stream));
+  {
+    LeafLULaunch L;
+    L.leaf_min = h->d_leaf_min;
+    L.leaf_size = h->d_leaf_size;
+    L.lu_off = h->d_lu_off;
+    L.lu = h->d_lu;
+    L.perm = h->d_perm;
+    L.src = make_src(h);
+    L.err = h->d_err;
+    int e = leaf_lu_launch(L, nl, h->smax, h->stream);
+    if (e) return cuda_fail(h, (cudaError_t)e, "leaf_lu_launch");
+  }
+  // Y = [U panels of every level], zero padded
+  if (h->C > 0) {
+    CK(dalloc(&h->Y, (size_t)(N * h->C)));
+    CK(cudaMemsetAsync(h->Y, 0, sizeof(double) * N * h->C, h->stream));
+    for (auto& L : h->lv) {
+      const int nb = L.nblocks();
+      std::vector<int> r0s(nb), ms(nb), rk(nb);
+      for (int q = 0; q < nb; ++q) {
+        int r0, c0, m, n;
+        block_geom(L, q, r0, c0, m, n);
+        r0s[q] = r0;
+        ms[q] = m;
+        rk[q] = level_rank(L, q);
+      }
+      int *d_r0 = nullptr, *d_m = nullptr, *d_rk = nullptr;
+      CK(dalloc(&d_r0, nb));
+      CK(dalloc(&d_m, nb));
+      CK(dalloc(&d_rk, nb));
+      CK(cudaMemcpyAsync(d_r0, r0s.data(), 4 * nb, cudaMemcpyHostToDevice, h->stream));
+      CK(cudaMemcpyAsync(d_m, ms.data(), 4 * nb, cudaMemcpyHostToDevice, h->stream));
+      CK(cudaMemcpyAsync(d_rk, rk.data(), 4 * nb, cudaMemcpyHostToDevice, h->stream));
+      int maxm = 0;
+      for (int m : ms) maxm = std::max(maxm, m);
+      dim3 grid(std::min(64, (maxm + 255) / 256), nb, std::min(L.kmax, 64));
+      y_init_kernel<<<grid, 256, 0, h->stream>>>(h->Y, N, L.coff, L.W, N, d_r0, d_m, d_rk, nb);
+      CK(cudaGetLastError());
+      CK(cudaStreamSynchronize(h->stream));
+      dfree(d_r0);
+      dfree(d_m);
+      dfree(d_rk);
+    }
+    // leaf solves on every column: Y <- blockdiag(leaf LU)^-1 Y
+    LeafSolveLaunch S;
+    S.leaf_min = h->d_leaf_min;
+    S.leaf_size = h->d_leaf_size;
+    S.lu_off = h->d_lu_off;
+    S.lu = h->d_lu;
+    S.perm = h->d_perm;
+    S.X = h->Y;
+    S.ldx = N;
+    S.ncols = (int)h->C;
+    int e = leaf_solve_launch(S, nl, h->smax, h->stream);
+    if (e) return cuda_fail(h, (cudaError_t)e, "leaf_solve_launch");
+  }
+  // levels bottom-up
+  for (int l = (int)h->lv.size() - 1; l >= 0; --l) {
+    Level& L = h->lv[l];
+    const int nn = (int)L.nmin.size();
+    L.nodes.resize(nn);
+    int64_t s_tot = 0, z_tot = 0, p_tot = 0;
+    L.max_sd = 0;
+    for (int p = 0; p < nn; ++p) {
+      SchurNode& sn = L.nodes[p];
+      sn.kt = level_rank(L, 2 * p);
+      sn.kb = level_rank(L, 2 * p + 1);
+      sn.coff = L.coff;
+      sn.pad = 0;
+      const int sd = sn.kb + sn.kt;
+      L.max_sd = std::max(L.max_sd, sd);
+      sn.s_off = s_tot;
+      s_tot += (int64_t)sd * sd;
+      sn.z_off = z_tot;
+      sn.r_off = z_tot;
+      z_tot += (int64_t)sd * (L.coff + std::max(sn.kb, sn.kt));
+      sn.p_off = p_tot;
+      p_tot += sd;
+    }
+    CK(dalloc(&L.S, (size_t)s_tot));
+    CK(dalloc(&L.piv, (size_t)p_tot));
+    CK(dalloc(&L.d_nodes, (size_t)nn));
+    CK(cudaMemcpyAsync(L.d_nodes, L.nodes.data(), sizeof(SchurNode) * nn,
+                       cudaMemcpyHostToDevice, h->stream));
+    if (z_tot > h->z_cap) {
+      dfree(h->Z);
+      CK(dalloc(&h->Z, (size_t)z_tot));
+      h->z_cap = z_tot;
+    }
+    // Z_h = V_h^T Y[rows_h, 0 : coff + rank(U_h)]
+    std::vector<GemmProblem> tn;
+    for (int p = 0; p < nn; ++p) {
+      const SchurNode& sn = L.nodes[p];
+      const int sd = sn.kb + sn.kt;
+      const int mn = L.nmin[p], sp = L.nsplit[p], mx = L.nmax[p];
+      GemmProblem a{};
+      a.A = L.V + mn;  // V of the bottom block lives on the top rows
+      a.M = sn.kb;
+      a.K = sp - mn + 1;
+      a.lda = (int)N;
+      a.B = h->Y + mn;
+      a.N = L.coff + sn.kt;
+      a.ldb = (int)N;
+      a.C = h->Z + sn.z_off;
+      a.ldc = sd;
+      tn.push_back(a);
+      GemmProblem b{};
+      b.A = L.V + sp + 1;  // V of the top block lives on the bottom rows
+      b.M = sn.kt;
+      b.K = mx - sp;
+      b.lda = (int)N;
+      b.B = h->Y + sp + 1;
+      b.N = L.coff + sn.kb;
+      b.ldb = (int)N;
+      b.C = h->Z + sn.z_off + sn.kb;
+      b.ldc = sd;
+      tn.push_back(b);
+    }
+    int rc2 = upload_plan(h, tn, true, L.tn);
+    if (rc2) return rc2;
+    int e = gemm_tn_launch(L.tn.probs, L.tn.tiles, L.tn.ntiles, L.tn.nprob, h->ws,
+                           L.tn.any_split, h->stream);
+    if (e) return cuda_fail(h, (cudaError_t)e, "gemm_tn");
+    SchurLaunch S;
+    S.nodes = L.d_nodes;
+    S.S = L.S;
+    S.Z = h->Z;
+    S.R = h->Z;
+    S.piv = L.piv;
+    S.err = h->d_err;
+    e = schur_factor_launch(S, nn, h->stream);
+    if (e) return cuda_fail(h, (cudaError_t)e, "schur_factor");
+    if (L.coff > 0) {
+      e = schur_solve_launch(S, nn, -1, L.coff, h->stream);
+      if (e) return cuda_fail(h, (cudaError_t)e, "schur_solve");
+      // Y[rows_h, 0:coff] -= Y[rows_h, coff : coff + rank(U_h)] * y_h
+      std::vector<GemmProblem> up;
+      for (int p = 0; p < nn; ++p) {
+        const SchurNode& sn = L.nodes[p];
+        const int sd = sn.kb + sn.kt;
+        const int mn = L.nmin[p], sp = L.nsplit[p], mx = L.nmax[p];
+        GemmProblem a{};
+        a.C = h->Y + mn;
+        a.ldc = (int)N;
+        a.A = h->Y + mn + (int64_t)L.coff * N;
+        a.lda = (int)N;
+        a.M = sp - mn + 1;
+        a.K = sn.kt;
+        a.B = h->Z + sn.z_off + sn.kb;
+        a.ldb = sd;
+        a.N = L.coff;
+        up.push_back(a);
+        GemmProblem b{};
+        b.C = h->Y + sp + 1;
+        b.ldc = (int)N;
+        b.A = h->Y + sp + 1 + (int64_t)L.coff * N;
+        b.lda = (int)N;
+        b.M = mx - sp;
+        b.K = sn.kb;
+        b.B = h->Z + sn.z_off;
+        b.ldb = sd;
+        b.N = L.coff;
+        up.push_back(b);
+      }
+      rc2 = upload_plan(h, up, false, L.nn);
+      if (rc2) return rc2;
+      e = gemm_nn_sub_launch(L.nn.probs, L.nn.tiles, L.nn.ntiles, h->stream);
+      if (e) return cuda_fail(h, (cudaError_t)e, "gemm_nn_sub");
+    }
+  }
+  CK(cudaEventRecord(h->ev1, h->stream));
+  CK(cudaEventSynchronize(h->ev1));
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+  h->t_fact = ms * 1e-3;
+  rc = check_dev_err(h, "factorize");
+  if (rc) return rc;
+  h->factored = true;
+  return HODLR_OK;
+}
+
+int build_solve_plans(hodlr_t h, int nrhs) {
+  const int64_t N = h->n;
+  int64_t zs_tot = 0;
+  for (auto& L : h->lv) {
+    int64_t t = 0;
+    for (auto& sn : L.nodes) t += (int64_t)(sn.kb + sn.kt) * nrhs;
+    zs_tot = std::max(zs_tot, t);
+  }
+  if (zs_tot > h->zs_cap) {
+    dfree(h->zs);
+    CK(dalloc(&h->zs, (size_t)zs_tot));
+    h->zs_cap = zs_tot;
+  }
+  if (nrhs > h->x_cols) {
+    dfree(h->X);
+    CK(dalloc(&h->X, (size_t)(N * nrhs)));
+    h->x_cols = nrhs;
+  }
+  for (auto& L : h->lv) {
+    if (L.solve_nrhs == nrhs) continue;
+    const int nn = (int)L.nmin.size();
+    std::vector<SchurNode> sn = L.nodes;
+    int64_t off = 0;
+    for (auto& s : sn) {
+      s.r_off = off;
+      off += (int64_t)(s.kb + s.kt) * nrhs;
+    }
+    dfree(L.d_snodes);
+    CK(dalloc(&L.d_snodes, (size_t)nn));
+    CK(cudaMemcpy(L.d_snodes, sn.data(), sizeof(SchurNode) * nn, cudaMemcpyHostToDevice));
+    std::vector<GemmProblem> tn, up;
+    for (int p = 0; p < nn; ++p) {
+      const int sd = sn[p].kb + sn[p].kt;
+      const int mn = L.nmin[p], sp = L.nsplit[p], mx = L.nmax[p];
+      GemmProblem a{};
+      a.A = L.V + mn;
+      a.M = sn[p].kb;
+      a.K = sp - mn + 1;
+      a.lda = (int)N;
+      a.B = h->X + mn;
+      a.N = nrhs;
+      a.ldb = (int)N;
+      a.C = h->zs + sn[p].r_off;
+      a.ldc = sd;
+      tn.push_back(a);
+      GemmProblem b{};
+      b.A = L.V + sp + 1;
+      b.M = sn[p].kt;
+      b.K = mx - sp;
+      b.lda = (int)N;
+      b.B = h->X + sp + 1;
+      b.N = nrhs;
+      b.ldb = (int)N;
+      b.C = h->zs + sn[p].r_off + sn[p].kb;
+      b.ldc = sd;
+      tn.push_back(b);
+      GemmProblem c{};
+      c.C = h->X + mn;
+      c.ldc = (int)N;
+      c.A = h->Y + mn + (int64_t)L.coff * N;
+      c.lda = (int)N;
+      c.M = sp - mn + 1;
+      c.K = sn[p].kt;
+      c.B = h->zs + sn[p].r_off + sn[p].kb;
+      c.ldb = sd;
+      c.N = nrhs;
+      up.push_back(c);
+      GemmProblem d{};
+      d.C = h->X + sp + 1;
+      d.ldc = (int)N;
+      d.A = h->Y + sp + 1 + (int64_t)L.coff * N;
+      d.lda = (int)N;
+      d.M = mx - sp;
+      d.K = sn[p].kb;
+      d.B = h->zs + sn[p].r_off;
+      d.ldb = sd;
+      d.N = nrhs;
+      up.push_back(d);
+    }
+    int rc = upload_plan(h, tn, true, L.stn);
+    if (rc) return rc;
+    rc = upload_plan(h, up, false, L.snn);
+    if (rc) return rc;
+    L.solve_nrhs = nrhs;
+  }
+  return HODLR_OK;
+}
+
+// x <- K_HODLR^-1 b, with b already in h->X (N x nrhs, ld N).
+int solve_in_place(hodlr_t h, int nrhs) {
+  const int64_t N = h->n;
+  LeafSolveLaunch S;
+  S.leaf_min = h->d_leaf_min;
+  S.leaf_size = h->d_leaf_size;
+  S.lu_off = h->d_lu_off;
+  S.lu = h->d_lu;
+  S.perm = h->d_perm;
+  S.X = h->X;
+  S.ldx = N;
+  S.ncols = nrhs;
+  int e = leaf_solve_launch(S, (int)h->leaf_min.size(), h->smax, h->stream);
+  if (e) return cuda_fail(h, (cudaError_t)e, "leaf_solve");
+  for (int l = (int)h->lv.size() - 1; l >= 0; --l) {
+    Level& L = h->lv[l];
+    const int nn = (int)L.nmin.size();
+    e = gemm_tn_launch(L.stn.probs, L.stn.tiles, L.stn.ntiles, L.stn.nprob, h->ws,
+                       L.stn.any_split, h->stream);
+    if (e) return cuda_fail(h, (cudaError_t)e, "solve gemm_tn");
+    SchurLaunch SL;
+    SL.nodes = L.d_snodes;
+    SL.S = L.S;
+    SL.Z = nullptr;
+    SL.R = h->zs;
+    SL.piv = L.piv;
+    SL.err = h->d_err;
+    e = schur_solve_launch(SL, nn, nrhs, nrhs, h->stream);
+    if (e) return cuda_fail(h, (cudaError_t)e, "solve schur");
+    e = gemm_nn_sub_launch(L.snn.probs, L.snn.tiles, L.snn.ntiles, h->stream);
+    if (e) return cuda_fail(h, (cudaError_t)e, "solve gemm_nn");
+  }
+  return HODLR_OK;
+}
+
+int do_solve_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double* d_x, int ldx,
+                    bool host_io) {
+  int rc = do_factorize(h);
+  if (rc) return rc;
+  rc = build_solve_plans(h, nrhs);
+  if (rc) return rc;
+  const int64_t N = h->n;
+  cudaMemcpyKind kin = host_io ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+  cudaMemcpyKind kout = host_io ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+  CK(cudaEventRecord(h->ev0, h->stream));
+  CK(cudaMemcpy2DAsync(h->X, sizeof(double) * N, d_b, sizeof(double) * ldb, sizeof(double) * N,
+                       nrhs, kin, h->stream));
+  rc = solve_in_place(h, nrhs);
+  if (rc) return rc;
+  CK(cudaMemcpy2DAsync(d_x, sizeof(double) * ldx, h->X, sizeof(double) * N, sizeof(double) * N,
+                       nrhs, kout, h->stream));
+  CK(cudaEventRecord(h->ev1, h->stream));
+  CK(cudaEventSynchronize(h->ev1));
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+  h->t_solve = ms * 1e-3;
+  h->t_total = h->t_lr + h->t_fact + h->t_solve;
+  return check_dev_err(h, "solve");
+}
+
+int init_common(hodlr_t h) {
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, dev));
+  int coop = 0;
+  CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+  if (!coop) return fail(h, HODLR_ERR_UNSUPPORTED, "device lacks cooperative launch");
+  CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  CK(cudaEventCreate(&h->ev0));
+  CK(cudaEventCreate(&h->ev1));
+  CK(dalloc(&h->d_err, 1));
+  CK(cudaMemset(h->d_err, 0, sizeof(unsigned)));
+  build_tree(h);
+  const int nl = (int)h->leaf_min.size();
+  if (h->smax > 160) return fail(h, HODLR_ERR_UNSUPPORTED, "leaf size above 160");
+  CK(dalloc(&h->d_leaf_min, (size_t)nl));
+  CK(dalloc(&h->d_leaf_size, (size_t)nl));
+  CK(cudaMemcpy(h->d_leaf_min, h->leaf_min.data(), 4 * nl, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h->d_leaf_size, h->leaf_size.data(), 4 * nl, cudaMemcpyHostToDevice));
+  return HODLR_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- C ABI
+extern "C" {
+
+int hodlr_create_kernel(hodlr_t* out, int n, int dim, const double* pts,
+                        const hodlr_kernel_desc* k, int leaf_size) {
+  if (!out || n <= 0 || dim < 1 || dim > 3 || !pts || !k || leaf_size < 1)
+    return HODLR_ERR_ARG;
+  if (k->type < 0 || k->type > 4 || !(k->length_scale > 0)) return HODLR_ERR_ARG;
+  *out = nullptr;
+  hodlr_t h = new hodlr_handle_s();
+  h->n = n;
+  h->dim = dim;
+  h->leaf = leaf_size;
+  h->kp = hx_make_kparams(k->type, dim, k->length_scale, k->diag_shift, k->diag_replace,
+                          k->diag_value);
+  int rc = init_common(h);
+  if (!rc) {
+    cudaError_t e = dalloc(&h->d_pts, (size_t)n * dim);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(h->d_pts, pts, sizeof(double) * (size_t)n * dim, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) rc = cuda_fail(h, e, "points upload");
+  }
+  if (rc) {
+    hodlr_destroy(h);
+    return rc;
+  }
+  *out = h;
+  return HODLR_OK;
+}
+
+int hodlr_create_dense(hodlr_t* out, int n, const double* A, int lda, int leaf_size) {
+  if (!out || n <= 0 || !A || lda < n || leaf_size < 1) return HODLR_ERR_ARG;
+  *out = nullptr;
+  hodlr_t h = new hodlr_handle_s();
+  h->n = n;
+  h->dim = 0;
+  h->leaf = leaf_size;
+  h->dense = true;
+  int rc = init_common(h);
+  if (!rc) {
+    cudaError_t e = dalloc(&h->d_A, (size_t)n * n);
+    if (e == cudaSuccess)
+      e = cudaMemcpy2D(h->d_A, sizeof(double) * n, A, sizeof(double) * lda, sizeof(double) * n,
+                       n, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) rc = cuda_fail(h, e, "matrix upload");
+  }
+  if (rc) {
+    hodlr_destroy(h);
+    return rc;
+  }
+  *out = h;
+  return HODLR_OK;
+}
+
+int hodlr_create_fnptr(hodlr_t* out, int rows, int cols, double (*kernel)(int, int, void*),
+                       void* data, int leaf_size) {
+  (void)rows;
+  (void)cols;
+  (void)kernel;
+  (void)data;
+  (void)leaf_size;
+  if (out) *out = nullptr;
+  return HODLR_ERR_UNSUPPORTED;
+}
+
+void hodlr_destroy(hodlr_t h) {
+  if (!h) return;
+  free_compress(h);
+  dfree(h->d_pts);
+  dfree(h->d_A);
+  dfree(h->d_leaf_min);
+  dfree(h->d_leaf_size);
+  dfree(h->ws);
+  dfree(h->Z);
+  dfree(h->X);
+  dfree(h->zs);
+  dfree(h->part);
+  dfree(h->bar);
+  dfree(h->d_blocks);
+  dfree(h->d_err);
+  if (h->ev0) cudaEventDestroy(h->ev0);
+  if (h->ev1) cudaEventDestroy(h->ev1);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+}
+
+int hodlr_set_lr_tolerance(hodlr_t h, double tol) {
+  if (!h || !(tol > 0)) return HODLR_ERR_ARG;
+  if (tol != h->tol) {
+    h->tol = tol;
+    free_compress(h);
+  }
+  return HODLR_OK;
+}
+
+int hodlr_set_min_pivot(hodlr_t h, double mp) {
+  if (!h || mp < 0) return HODLR_ERR_ARG;
+  int v = (int)mp;
+  if (v != h->minPivot) {
+    h->minPivot = v;
+    free_compress(h);
+  }
+  return HODLR_OK;
+}
+
+int hodlr_set_lr_method(hodlr_t h, const char* method) {
+  if (!h || !method) return HODLR_ERR_ARG;
+  if (std::strcmp(method, "partialPiv_ACA") != 0)
+    return fail(h, HODLR_ERR_UNSUPPORTED, std::string("low-rank method not on the GPU path: ") + method);
+  return HODLR_OK;
+}
+
+int hodlr_compress(hodlr_t h) {
+  if (!h) return HODLR_ERR_ARG;
+  if (h->compressed) return HODLR_OK;
+  cudaEvent_t a, b;
+  CK(cudaEventCreate(&a));
+  CK(cudaEventCreate(&b));
+  CK(cudaEventRecord(a, h->stream));
+  int rc = do_compress(h);
+  CK(cudaEventRecord(b, h->stream));
+  CK(cudaEventSynchronize(b));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (!rc) h->t_lr = ms * 1e-3;
+  return rc;
+}
+
+int hodlr_factorize(hodlr_t h) {
+  if (!h) return HODLR_ERR_ARG;
+  int rc = hodlr_compress(h);
+  if (rc) return rc;
+  return do_factorize(h);
+}
+
+int hodlr_solve(hodlr_t h, int nrhs, const double* b, int ldb, double* x, int ldx) {
+  if (!h || nrhs < 1 || !b || !x || ldb < h->n || ldx < h->n) return HODLR_ERR_ARG;
+  int rc = hodlr_factorize(h);
+  if (rc) return rc;
+  return do_solve_device(h, nrhs, b, ldb, x, ldx, true);
+}
+
+int hodlr_solve_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double* d_x, int ldx) {
+  if (!h || nrhs < 1 || !d_b || !d_x || ldb < h->n || ldx < h->n) return HODLR_ERR_ARG;
+  int rc = hodlr_factorize(h);
+  if (rc) return rc;
+  return do_solve_device(h, nrhs, d_b, ldb, d_x, ldx, false);
+}
+
+int hodlr_kernel_matvec_device(hodlr_t h, int nrhs, const double* d_x, int ldx, double* d_y,
+                               int ldy) {
+  if (!h || nrhs < 1 || nrhs > 16 || !d_x || !d_y || ldx < h->n || ldy < h->n)
+    return HODLR_ERR_ARG;
+  int sp = kmatvec_splits(h->n, h->num_sms);
+  if (sp > 1) {
+    int rc = ensure_ws(h, (int64_t)sp * nrhs * h->n);
+    if (rc) return rc;
+  }
+  KmatvecLaunch L;
+  L.src = make_src(h);
+  L.X = d_x;
+  L.ldx = ldx;
+  L.Y = d_y;
+  L.ldy = ldy;
+  L.ws = h->ws;
+  L.n = h->n;
+  L.nrhs = nrhs;
+  int e = kmatvec_launch(L, sp, h->stream);
+  if (e) return cuda_fail(h, (cudaError_t)e, "kmatvec");
+  CK(cudaStreamSynchronize(h->stream));
+  return HODLR_OK;
+}
+
+int hodlr_residual(hodlr_t h, int nrhs, const double* b, int ldb, const double* x, int ldx,
+                   double* relres) {
+  if (!h || nrhs < 1 || !b || !x || !relres || ldb < h->n || ldx < h->n) return HODLR_ERR_ARG;
+  const int64_t N = h->n;
+  double *dx = nullptr, *dy = nullptr;
+  CK(dalloc(&dx, (size_t)(N * nrhs)));
+  cudaError_t e = dalloc(&dy, (size_t)(N * nrhs));
+  if (e != cudaSuccess) {
+    dfree(dx);
+    return cuda_fail(h, e, "residual alloc");
+  }
+  int rc = HODLR_OK;
+  std::vector<double> y((size_t)(N * nrhs));
+  e = cudaMemcpy2D(dx, sizeof(double) * N, x, sizeof(double) * ldx, sizeof(double) * N, nrhs,
+                   cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    for (int c0 = 0; c0 < nrhs && !rc; c0 += 16) {
+      int nc = std::min(16, nrhs - c0);
+      rc = hodlr_kernel_matvec_device(h, nc, dx + c0 * N, (int)N, dy + c0 * N, (int)N);
+    }
+    if (!rc) e = cudaMemcpy(y.data(), dy, sizeof(double) * N * nrhs, cudaMemcpyDeviceToHost);
+  }
+  dfree(dx);
+  dfree(dy);
+  if (e != cudaSuccess) return cuda_fail(h, e, "residual");
+  if (rc) return rc;
+  for (int c = 0; c < nrhs; ++c) {
+    long double num = 0, den = 0;
+    for (int64_t i = 0; i < N; ++i) {
+      long double bi = b[c * (int64_t)ldb + i];
+      long double r = (long double)y[c * N + i] - bi;
+      num += r * r;
+      den += bi * bi;
+    }
+    relres[c] = den > 0 ? (double)std::sqrt(num / den) : (double)std::sqrt(num);
+  }
+  return HODLR_OK;
+}
+
+int hodlr_get_times(hodlr_t h, double* lr, double* factor, double* solve, double* total) {
+  if (!h) return HODLR_ERR_ARG;
+  if (lr) *lr = h->t_lr;
+  if (factor) *factor = h->t_fact;
+  if (solve) *solve = h->t_solve;
+  if (total) *total = h->t_lr + h->t_fact + h->t_solve;
+  return HODLR_OK;
+}
+
+int hodlr_get_num_levels(hodlr_t h, int* levels) {
+  if (!h || !levels) return HODLR_ERR_ARG;
+  *levels = (int)h->lv.size();
+  return HODLR_OK;
+}
+
+int hodlr_get_num_blocks(hodlr_t h, int* blocks) {
+  if (!h || !blocks) return HODLR_ERR_ARG;
+  int t = 0;
+  for (auto& L : h->lv) t += L.nblocks();
+  *blocks = t;
+  return HODLR_OK;
+}
+
+static bool locate(hodlr_t h, int block, int& l, int& q) {
+  if (block < 0) return false;
+  int base = 0;
+  for (l = 0; l < (int)h->lv.size(); ++l) {
+    int nb = h->lv[l].nblocks();
+    if (block < base + nb) {
+      q = block - base;
+      return true;
+    }
+    base += nb;
+  }
+  return false;
+}
+
+int hodlr_get_block_info(hodlr_t h, int block, int* level, int* row0, int* col0, int* m, int* n,
+                         int* rank, int* iters) {
+  int l, q;
+  if (!h || !locate(h, block, l, q)) return HODLR_ERR_ARG;
+  int r0, c0, mm, nn;
+  block_geom(h->lv[l], q, r0, c0, mm, nn);
+  if (level) *level = l;
+  if (row0) *row0 = r0;
+  if (col0) *col0 = c0;
+  if (m) *m = mm;
+  if (n) *n = nn;
+  bool have = h->compressed;
+  if (rank) *rank = have ? h->lv[l].st[q].rank : -1;
+  if (iters) *iters = have ? h->lv[l].st[q].iters : -1;
+  return HODLR_OK;
+}
+
+int hodlr_get_ranks(hodlr_t h, int* ranks) {
+  if (!h || !ranks) return HODLR_ERR_ARG;
+  if (!h->compressed) return fail(h, HODLR_ERR_STATE, "not compressed");
+  int t = 0;
+  for (auto& L : h->lv)
+    for (auto& s : L.st) ranks[t++] = s.rank;
+  return HODLR_OK;
+}
+
+int hodlr_get_pivots(hodlr_t h, int block, int* rows, int* cols, int* count) {
+  int l, q;
+  if (!h || !locate(h, block, l, q) || !count) return HODLR_ERR_ARG;
+  if (!h->compressed) return fail(h, HODLR_ERR_STATE, "not compressed");
+  Level& L = h->lv[l];
+  int r0, c0, m, n;
+  block_geom(L, q, r0, c0, m, n);
+  const int k = L.st[q].k;
+  *count = k;
+  if (k > 0) {
+    if (rows) CK(cudaMemcpy(rows, L.prow + r0, 4 * (size_t)k, cudaMemcpyDeviceToHost));
+    if (cols) CK(cudaMemcpy(cols, L.pcol + c0, 4 * (size_t)k, cudaMemcpyDeviceToHost));
+  }
+  return HODLR_OK;
+}
+
+int hodlr_get_lowrank(hodlr_t h, int block, double* W, double* V) {
+  int l, q;
+  if (!h || !locate(h, block, l, q)) return HODLR_ERR_ARG;
+  if (!h->compressed) return fail(h, HODLR_ERR_STATE, "not compressed");
+  Level& L = h->lv[l];
+  int r0, c0, m, n;
+  block_geom(L, q, r0, c0, m, n);
+  const int r = L.st[q].rank;
+  const int64_t N = h->n;
+  if (W) CK(cudaMemcpy2D(W, sizeof(double) * m, L.W + r0, sizeof(double) * N, sizeof(double) * m, r, cudaMemcpyDeviceToHost));
+  if (V) CK(cudaMemcpy2D(V, sizeof(double) * n, L.V + c0, sizeof(double) * N, sizeof(double) * n, r, cudaMemcpyDeviceToHost));
+  return HODLR_OK;
+}
+
+int hodlr_get_block_margin(hodlr_t h, int block, double* margin, int* near) {
+  int l, q;
+  if (!h || !locate(h, block, l, q)) return HODLR_ERR_ARG;
+  if (!h->compressed) return fail(h, HODLR_ERR_STATE, "not compressed");
+  if (margin) *margin = h->lv[l].st[q].margin;
+  if (near) *near = h->lv[l].st[q].near;
+  return HODLR_OK;
+}
+
+int hodlr_get_aca_stats(hodlr_t h, int* launches, double* seconds, double* bytes) {
+  if (!h) return HODLR_ERR_ARG;
+  if (launches) *launches = h->aca_launches;
+  if (seconds) *seconds = h->aca_seconds;
+  if (bytes) *bytes = h->aca_bytes;
+  return HODLR_OK;
+}
+
+const char* hodlr_status_string(int s) {
+  switch (s) {
+    case HODLR_OK: return "ok";
+    case HODLR_ERR_ARG: return "invalid argument";
+    case HODLR_ERR_CUDA: return "CUDA error";
+    case HODLR_ERR_ALLOC: return "device memory exhausted";
+    case HODLR_ERR_UNSUPPORTED: return "unsupported on the GPU path";
+    case HODLR_ERR_SINGULAR: return "exact-zero pivot";
+    case HODLR_ERR_STATE: return "call out of order";
+    case HODLR_ERR_NONFINITE: return "non-finite value";
+    case HODLR_ERR_TIMEOUT: return "device wait timed out";
+    default: return "unknown status";
+  }
+}
+
+const char* hodlr_last_error(hodlr_t h) { return h ? h->err.c_str() : "null handle"; }
+
+}  // extern "C"

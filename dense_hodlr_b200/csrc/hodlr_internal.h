@@ -1,0 +1,64 @@
+// Internal structures shared by the kernels and the host orchestration.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "kfun.h"
+
+// Where a matrix entry comes from: a kernel of point coordinates, or a
+// dense column-major matrix resident in HBM.
+struct EntrySrc {
+  const double* pts;  // SoA coordinates, pts[d * ld + i]
+  const double* A;    // dense input, A[i + j * ld]
+  int64_t ld;         // = n
+  hx_kparams kp;
+  int dense;
+};
+
+// ----------------------------------------------------------------- ACA
+enum {
+  ACA_RUNNING = 0,   // loop in progress (or not started)
+  ACA_POST = 1,      // loop finished, post-processing pending
+  ACA_DONE = 2,      // W, V and rank final
+  ACA_NEED_CAP = 3,  // loop paused: more columns of W/V are needed
+  ACA_ERROR = 4,
+  ACA_NEED_CAP_POST = 5,  // loop done; the full-rank form needs more columns
+};
+
+// One off-diagonal block.  W and V point at the block's first row inside the
+// level arenas (leading dimension = N), so W(i,l) = W[i + l*N] for the block's
+// local row i, and V(j,l) = V[j + l*N] for its local column j.
+struct AcaState;
+
+struct AcaBlock {
+  AcaState* st;       // loop state of this block
+  double* W;
+  double* V;
+  unsigned char* cR;  // chosen rows, local index
+  unsigned char* cC;  // chosen columns, local index
+  int* prow;          // pivot row of step t, local index
+  int* pcol;          // pivot column of step t
+  int r0, c0, m, n;
+  int kcap;           // columns available in W and V
+  int level;
+};
+
+// Loop state of one block; lets a paused block resume where it stopped.
+struct AcaState {
+  double frob2, eps, margin;
+  int k, cur, status, iters, rank, near;
+};
+
+struct AcaLaunch {
+  const AcaBlock* blocks;
+  int nblocks;
+  int G;                 // CTAs per block
+  int64_t ld;            // N
+  double tol, minPivot;
+  double* part;          // per-CTA partials, part_stride doubles each
+  int64_t part_stride;
+  unsigned* bar;         // per-block barrier counters (zeroed before launch)
+  unsigned* err;         // device error word
+  EntrySrc src;
+};

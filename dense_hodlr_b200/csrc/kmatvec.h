@@ -1,0 +1,20 @@
+// Full-kernel FP64 product interface (kmatvec.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "hodlr_internal.h"
+
+struct KmatvecLaunch {
+  EntrySrc src;
+  const double* X;
+  int64_t ldx;
+  double* Y;
+  int64_t ldy;
+  double* ws;  // nsplit x nrhs x n partials (nsplit > 1)
+  int n, nrhs;
+};
+
+int kmatvec_splits(int n, int num_sms);
+int kmatvec_launch(const KmatvecLaunch& L, int nsplit, cudaStream_t s);

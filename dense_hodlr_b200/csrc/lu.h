@@ -1,0 +1,53 @@
+// Batched LU interfaces (lu.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "hodlr_internal.h"
+
+struct LeafLULaunch {
+  const int* leaf_min;
+  const int* leaf_size;
+  const int64_t* lu_off;  // offset of each leaf's s x s LU in `lu`
+  double* lu;
+  int* perm;              // length N: row permutation of each leaf, local indices
+  EntrySrc src;
+  unsigned* err;
+};
+
+struct LeafSolveLaunch {
+  const int* leaf_min;
+  const int* leaf_size;
+  const int64_t* lu_off;
+  const double* lu;
+  const int* perm;
+  double* X;     // N x ncols panel, column-major
+  int64_t ldx;
+  int ncols;
+};
+
+struct SchurNode {
+  int kb, kt;       // ranks of the bottom / top off-diagonal blocks
+  int coff;         // number of ancestor columns (Schur right-hand sides)
+  int pad;
+  int64_t s_off;    // S (sd x sd) offset
+  int64_t z_off;    // Z (sd x zcols) offset
+  int64_t r_off;    // right-hand sides (sd x cols) offset for the solve
+  int64_t p_off;    // pivots offset
+};
+
+struct SchurLaunch {
+  const SchurNode* nodes;
+  double* S;
+  const double* Z;
+  double* R;
+  int* piv;
+  unsigned* err;
+};
+
+int leaf_lu_launch(const LeafLULaunch& L, int nleaves, int smax, cudaStream_t s);
+int leaf_solve_launch(const LeafSolveLaunch& L, int nleaves, int smax, cudaStream_t s);
+int schur_factor_launch(const SchurLaunch& L, int nnodes, cudaStream_t s);
+int schur_solve_launch(const SchurLaunch& L, int nnodes, int ncols, int max_cols,
+                       cudaStream_t s);

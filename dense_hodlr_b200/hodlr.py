@@ -1,0 +1,283 @@
+"""Python mirror of the reference's HODLR_Matrix interface for the recLU path.
+
+Same names, argument meaning and error behaviour as include/HODLR_Matrix.hpp
+(constructors :76 and :162, recLU_Solve :214, recLU_Compute :217,
+set_LRTolerance / set_minPivot / set_LRMethod :222-225, timing getters
+:234-241, printResultInfo :45).  Every call goes through the C ABI of
+libhodlr_b200.so (include/hodlr_b200.h); there is no CPU fallback, and a
+missing library or GPU raises HODLRError.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from . import _lib as _L
+
+GAUSSIAN = 0
+MATERN32 = 1
+INV_MULTIQUADRIC = 2
+QUADRATIC = 3
+EXPONENTIAL = 4
+
+_KERNEL_NAMES = {"gaussian": GAUSSIAN, "matern32": MATERN32,
+                 "inv_multiquadric": INV_MULTIQUADRIC, "quadratic": QUADRATIC,
+                 "exponential": EXPONENTIAL}
+
+
+class HODLRError(RuntimeError):
+    def __init__(self, status, msg=""):
+        self.status = status
+        super().__init__(f"{_L.status_string(status)} ({status}): {msg}")
+
+
+class KernelSpec:
+    """Closed-form kernel K_ij = f(r_ij), diagonal shifted or replaced."""
+
+    def __init__(self, kind, length_scale=1.0, diag_shift=0.0, diag_replace=False,
+                 diag_value=0.0):
+        self.type = _KERNEL_NAMES[kind] if isinstance(kind, str) else int(kind)
+        self.length_scale = float(length_scale)
+        self.diag_shift = float(diag_shift)
+        self.diag_replace = bool(diag_replace)
+        self.diag_value = float(diag_value)
+
+    def desc(self):
+        return _L.KernelDesc(self.type, self.length_scale, self.diag_shift,
+                             int(self.diag_replace), self.diag_value)
+
+
+class kernelMatrix:
+    """Stand-in for the reference kernelMatrix (include/kernel.hpp:6-33).
+
+    The reference wraps `double (*)(int i, int j, void* data)`; on the GPU the
+    entry must be a closed form of point coordinates, so `kernel` is a
+    KernelSpec and `data` the points (dim x n).  A Python callable is
+    rejected with HODLR_ERR_UNSUPPORTED, like hodlr_create_fnptr.
+    """
+
+    def __init__(self, numRows, numCols, kernel, data):
+        if numRows != numCols:
+            raise HODLRError(_L.ERR_ARG, "only square kernel matrices form a HODLR tree")
+        self.numRows, self.numCols = int(numRows), int(numCols)
+        self.kernel = kernel
+        self.data = data
+
+    def rows(self):
+        return self.numRows
+
+    def cols(self):
+        return self.numCols
+
+
+def _check(h, rc):
+    if rc != 0:
+        msg = _L.lib().hodlr_last_error(h).decode() if h else ""
+        raise HODLRError(rc, msg)
+
+
+def _as_f64_fortran(a):
+    a = np.asarray(a, dtype=np.float64)
+    if a.ndim == 1:
+        a = a.reshape(-1, 1)
+    return np.asfortranarray(a)
+
+
+class HODLR_Matrix:
+    """HODLR_Matrix for the recLU path on one B200.
+
+    HODLR_Matrix(A, leaf=30, LR_Method="partialPiv_ACA")           dense input
+    HODLR_Matrix(numRows, numCols, kernel, data, leaf=30)           kernel input
+    HODLR_Matrix(kernelMatrix(...), leaf=30)
+    """
+
+    def __init__(self, *args, leaf=None, LR_Method="partialPiv_ACA", **kw):
+        self.printResultInfo = False
+        self._h = None
+        lib = _L.lib()
+        h = ctypes.c_void_p()
+        if len(args) >= 1 and isinstance(args[0], np.ndarray) and args[0].ndim == 2:
+            A = np.asfortranarray(args[0], dtype=np.float64)
+            if A.shape[0] != A.shape[1]:
+                raise HODLRError(_L.ERR_ARG, "matrix must be square")
+            leaf = int(args[1]) if len(args) > 1 else (leaf or 30)
+            if len(args) > 2:
+                LR_Method = args[2]
+            self.n = A.shape[0]
+            rc = lib.hodlr_create_dense(ctypes.byref(h), self.n,
+                                        A.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                        self.n, int(leaf))
+            _check(None, rc)
+        else:
+            if len(args) >= 1 and isinstance(args[0], kernelMatrix):
+                km = args[0]
+                leaf = int(args[1]) if len(args) > 1 else (leaf or 30)
+                n, kernel, data = km.numRows, km.kernel, km.data
+            else:
+                if len(args) < 4:
+                    raise HODLRError(_L.ERR_ARG, "expected (numRows, numCols, kernel, data[, leaf])")
+                n, ncols, kernel, data = args[:4]
+                if n != ncols:
+                    raise HODLRError(_L.ERR_ARG, "only square kernel matrices form a HODLR tree")
+                leaf = int(args[4]) if len(args) > 4 else (leaf or 30)
+            if callable(kernel) and not isinstance(kernel, KernelSpec):
+                rc = lib.hodlr_create_fnptr(ctypes.byref(h), int(n), int(n), None, None, int(leaf))
+                _check(None, rc)
+            pts = np.ascontiguousarray(np.atleast_2d(np.asarray(data, dtype=np.float64)))
+            dim = pts.shape[0]
+            if pts.shape[1] != n:
+                raise HODLRError(_L.ERR_ARG, "data must be dim x n point coordinates")
+            d = kernel.desc()
+            self.n = int(n)
+            rc = lib.hodlr_create_kernel(ctypes.byref(h), self.n, dim,
+                                         pts.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                         ctypes.byref(d), int(leaf))
+            _check(None, rc)
+        self._h = h
+        self.leaf = leaf
+        if LR_Method != "partialPiv_ACA":
+            self.set_LRMethod(LR_Method)
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            _L.lib().hodlr_destroy(self._h)
+            self._h = None
+
+    # ------------------------------------------------------------ setters
+    def set_LRTolerance(self, tolerance):
+        _check(self._h, _L.lib().hodlr_set_lr_tolerance(self._h, float(tolerance)))
+
+    def set_minPivot(self, minPivot):
+        _check(self._h, _L.lib().hodlr_set_min_pivot(self._h, float(minPivot)))
+
+    def set_LRMethod(self, method):
+        _check(self._h, _L.lib().hodlr_set_lr_method(self._h, method.encode()))
+
+    # ------------------------------------------------------------- solver
+    def storeLRinTree(self):
+        _check(self._h, _L.lib().hodlr_compress(self._h))
+
+    def recLU_Compute(self):
+        _check(self._h, _L.lib().hodlr_factorize(self._h))
+
+    def recLU_Solve(self, input_RHS):
+        b = _as_f64_fortran(input_RHS)
+        if b.shape[0] != self.n:
+            raise HODLRError(_L.ERR_ARG, "right-hand side has the wrong number of rows")
+        x = np.zeros_like(b, order="F")
+        dp = ctypes.POINTER(ctypes.c_double)
+        _check(self._h, _L.lib().hodlr_solve(self._h, b.shape[1], b.ctypes.data_as(dp), self.n,
+                                             x.ctypes.data_as(dp), self.n))
+        if self.printResultInfo:
+            rel = self.residual(x, b)
+            print("**************************************************")
+            print("Solver Type                      = recLU")
+            print(f"Low-Rank Computation Time        = {self.get_LR_ComputationTime()} seconds")
+            print(f"Factorization Time               = {self.get_recLU_FactorizationTime()} seconds")
+            print(f"Solve Time                       = {self.get_recLU_SolveTime()} seconds")
+            print(f"Total Solve Time                 = {self.get_recLU_TotalTime()} seconds")
+            print(f"Residual l2 Relative Error       = {rel.max()}")
+        return x
+
+    def solve_device(self, b_ptr, x_ptr, nrhs, ldb=None, ldx=None):
+        """recLU_Solve on device buffers (raw CUDA pointers)."""
+        _check(self._h, _L.lib().hodlr_solve_device(self._h, int(nrhs), ctypes.c_void_p(b_ptr),
+                                                    int(ldb or self.n), ctypes.c_void_p(x_ptr),
+                                                    int(ldx or self.n)))
+
+    def kernel_matvec_device(self, x_ptr, y_ptr, nrhs):
+        _check(self._h, _L.lib().hodlr_kernel_matvec_device(self._h, int(nrhs),
+                                                            ctypes.c_void_p(x_ptr), self.n,
+                                                            ctypes.c_void_p(y_ptr), self.n))
+
+    def residual(self, x, b):
+        """Per-column ||K x - b|| / ||b|| with the full FP64 kernel."""
+        x = _as_f64_fortran(x)
+        b = _as_f64_fortran(b)
+        out = np.zeros(b.shape[1])
+        dp = ctypes.POINTER(ctypes.c_double)
+        _check(self._h, _L.lib().hodlr_residual(self._h, b.shape[1], b.ctypes.data_as(dp), self.n,
+                                                x.ctypes.data_as(dp), self.n,
+                                                out.ctypes.data_as(dp)))
+        return out
+
+    # ------------------------------------------------------------ getters
+    def _times(self):
+        t = [ctypes.c_double() for _ in range(4)]
+        _check(self._h, _L.lib().hodlr_get_times(self._h, *[ctypes.byref(x) for x in t]))
+        return [x.value for x in t]
+
+    def get_LR_ComputationTime(self):
+        return self._times()[0]
+
+    def get_recLU_FactorizationTime(self):
+        return self._times()[1]
+
+    def get_recLU_SolveTime(self):
+        return self._times()[2]
+
+    def get_recLU_TotalTime(self):
+        return self._times()[3]
+
+    def get_MatrixSize(self):
+        return self.n
+
+    def rows(self):
+        return self.n
+
+    def cols(self):
+        return self.n
+
+    # -------------------------------------------------------- diagnostics
+    def num_levels(self):
+        v = ctypes.c_int()
+        _check(self._h, _L.lib().hodlr_get_num_levels(self._h, ctypes.byref(v)))
+        return v.value
+
+    def num_blocks(self):
+        v = ctypes.c_int()
+        _check(self._h, _L.lib().hodlr_get_num_blocks(self._h, ctypes.byref(v)))
+        return v.value
+
+    def block_info(self, b):
+        v = [ctypes.c_int() for _ in range(7)]
+        _check(self._h, _L.lib().hodlr_get_block_info(self._h, int(b), *[ctypes.byref(x) for x in v]))
+        return dict(zip(("level", "row0", "col0", "m", "n", "rank", "iters"), [x.value for x in v]))
+
+    def ranks(self):
+        out = np.zeros(self.num_blocks(), dtype=np.int32)
+        _check(self._h, _L.lib().hodlr_get_ranks(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int))))
+        return out
+
+    def pivots(self, b):
+        info = self.block_info(b)
+        cap = max(1, min(info["m"], info["n"]))
+        rows = np.zeros(cap, dtype=np.int32)
+        cols = np.zeros(cap, dtype=np.int32)
+        cnt = ctypes.c_int()
+        ip = ctypes.POINTER(ctypes.c_int)
+        _check(self._h, _L.lib().hodlr_get_pivots(self._h, int(b), rows.ctypes.data_as(ip),
+                                                  cols.ctypes.data_as(ip), ctypes.byref(cnt)))
+        return rows[:cnt.value].copy(), cols[:cnt.value].copy()
+
+    def lowrank(self, b):
+        info = self.block_info(b)
+        W = np.zeros((info["m"], info["rank"]), order="F")
+        V = np.zeros((info["n"], info["rank"]), order="F")
+        dp = ctypes.POINTER(ctypes.c_double)
+        _check(self._h, _L.lib().hodlr_get_lowrank(self._h, int(b), W.ctypes.data_as(dp),
+                                                   V.ctypes.data_as(dp)))
+        return W, V
+
+    def margin(self, b):
+        m = ctypes.c_double()
+        n = ctypes.c_int()
+        _check(self._h, _L.lib().hodlr_get_block_margin(self._h, int(b), ctypes.byref(m),
+                                                        ctypes.byref(n)))
+        return m.value, n.value
+
+    def aca_stats(self):
+        a, s, b = ctypes.c_int(), ctypes.c_double(), ctypes.c_double()
+        _check(self._h, _L.lib().hodlr_get_aca_stats(self._h, ctypes.byref(a), ctypes.byref(s),
+                                                     ctypes.byref(b)))
+        return {"launches": a.value, "seconds": s.value, "bytes": b.value}

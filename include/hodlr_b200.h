@@ -1,0 +1,137 @@
+/*
+ * hodlr_b200.h -- C ABI of the B200 HODLR direct solver.
+ *
+ * Drop-in boundary for the recLU hot path of amiraa127/Dense_HODLR: kernel
+ * matrix assembly, partial-pivot ACA compression of every off-diagonal
+ * block, recursive LU / Sherman-Morrison-Woodbury factorization and solve.
+ * Every entry point names the reference interface it replaces
+ * (include/HODLR_Matrix.hpp unless stated).  Plain pointers and sizes only;
+ * matrices are column-major FP64.  Every call returns an int status
+ * (HODLR_OK == 0).  A handle is used by one host thread at a time; all its
+ * GPU work runs on one CUDA stream.  There is no CPU fallback: without a
+ * usable GPU, hodlr_create_* returns HODLR_ERR_CUDA.
+ */
+#ifndef HODLR_B200_H
+#define HODLR_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct hodlr_handle_s* hodlr_t;
+
+/* status codes */
+#define HODLR_OK 0
+#define HODLR_ERR_ARG 1         /* invalid argument */
+#define HODLR_ERR_CUDA 2        /* CUDA runtime error / no device */
+#define HODLR_ERR_ALLOC 3       /* device memory exhausted */
+#define HODLR_ERR_UNSUPPORTED 4 /* feature not available on the GPU path */
+#define HODLR_ERR_SINGULAR 5    /* exact-zero pivot in a leaf or capacitance LU */
+#define HODLR_ERR_STATE 6       /* call out of order */
+#define HODLR_ERR_NONFINITE 7   /* a NaN/Inf matrix entry or residual */
+#define HODLR_ERR_TIMEOUT 8     /* a bounded device wait gave up */
+
+/* kernel families: K_ij = f(r_ij) (+ shift on the diagonal) */
+#define HODLR_KERNEL_GAUSSIAN 0          /* exp(-r^2/l^2) */
+#define HODLR_KERNEL_MATERN32 1          /* (1+sqrt(3)r/l) exp(-sqrt(3)r/l) */
+#define HODLR_KERNEL_INV_MULTIQUADRIC 2  /* 1/sqrt(1+r^2/l^2) */
+#define HODLR_KERNEL_QUADRATIC 3         /* 1 + r^2/l^2 */
+#define HODLR_KERNEL_EXPONENTIAL 4       /* exp(-r/l) */
+
+typedef struct {
+  int type;            /* HODLR_KERNEL_* */
+  double length_scale; /* l */
+  double diag_shift;   /* K_ii = f(0) + diag_shift   (diag_replace == 0) */
+  int diag_replace;    /* 1: K_ii = diag_value instead */
+  double diag_value;
+} hodlr_kernel_desc;
+
+/* Low-rank methods (set_LRMethod strings of the reference). */
+#define HODLR_LR_PARTIAL_PIV_ACA 0 /* "partialPiv_ACA", the only GPU method */
+
+/* HODLR_Matrix(int numRows, int numCols, double (*kernel)(int,int,void*),
+ *              void* data, int leaf = 30)                         (:162)
+ * The entry functor becomes a closed-form kernel of points: pts holds dim
+ * rows of n coordinates (SoA, pts[d*n + i]), host memory, copied.  dim <= 3. */
+int hodlr_create_kernel(hodlr_t* out, int n, int dim, const double* pts,
+                        const hodlr_kernel_desc* kernel, int leaf_size);
+
+/* HODLR_Matrix(Eigen::MatrixXd& A, int leaf = 30,
+ *              std::string LR_Method = "partialPiv_ACA")           (:76)
+ * A is n x n column-major host memory with leading dimension lda, copied. */
+int hodlr_create_dense(hodlr_t* out, int n, const double* A, int lda, int leaf_size);
+
+/* HODLR_Matrix(int, int, double (*)(int,int,void*), void*, int)     (:162)
+ * with an arbitrary host function: returns HODLR_ERR_UNSUPPORTED, because a
+ * host function pointer cannot be evaluated by GPU kernels.  Use
+ * hodlr_create_kernel (closed-form kernels) or hodlr_create_dense. */
+int hodlr_create_fnptr(hodlr_t* out, int rows, int cols,
+                       double (*kernel)(int, int, void*), void* data, int leaf_size);
+
+void hodlr_destroy(hodlr_t h);
+
+/* set_LRTolerance(double) (:222); default 1e-6.  A changed value discards the
+ * compression and the factorization (reset_attributes,
+ * src/HODLR_Matrix.cpp:1232-1257). */
+int hodlr_set_lr_tolerance(hodlr_t h, double tol);
+/* set_minPivot(double) (:223); truncated to int as the reference does when it
+ * passes it to ACA (include/lowRank.hpp:25). */
+int hodlr_set_min_pivot(hodlr_t h, double min_pivot);
+/* set_LRMethod(std::string) (:225): "partialPiv_ACA" only, else
+ * HODLR_ERR_UNSUPPORTED. */
+int hodlr_set_lr_method(hodlr_t h, const char* method);
+
+/* storeLRinTree() (:211): ACA of every off-diagonal block. */
+int hodlr_compress(hodlr_t h);
+/* recLU_Compute() (:217): compression (if needed) + recLU_Factorize. */
+int hodlr_factorize(hodlr_t h);
+/* recLU_Solve(const Eigen::MatrixXd&) (:214): compresses and factors on
+ * first use, then solves.  b and x are host memory, n x nrhs. */
+int hodlr_solve(hodlr_t h, int nrhs, const double* b, int ldb, double* x, int ldx);
+/* Same with device pointers (no host copies). */
+int hodlr_solve_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double* d_x,
+                       int ldx);
+
+/* kernelMatrix::operator* (src/kernel.cpp:27-35): d_y = K d_x, FP64, entries
+ * generated on the fly (device pointers). */
+int hodlr_kernel_matvec_device(hodlr_t h, int nrhs, const double* d_x, int ldx,
+                               double* d_y, int ldy);
+/* The printResultInfo residual (src/HODLR_Matrix.cpp:785-787) per column:
+ * relres[c] = ||K x_c - b_c||_2 / ||b_c||_2, full kernel in FP64.  Host
+ * buffers. */
+int hodlr_residual(hodlr_t h, int nrhs, const double* b, int ldb, const double* x,
+                   int ldx, double* relres);
+
+/* get_LR_ComputationTime / get_recLU_FactorizationTime / get_recLU_SolveTime /
+ * get_recLU_TotalTime (:234-241), seconds of device time (CUDA events). */
+int hodlr_get_times(hodlr_t h, double* lr, double* factor, double* solve, double* total);
+
+/* Tree and block introspection.  Blocks are numbered 2p (top off-diagonal)
+ * and 2p+1 (bottom off-diagonal) for inner node p in level order, the order
+ * of HODLR_Tree::nodeLevelVec (include/HODLR_Tree.hpp:86). */
+int hodlr_get_num_levels(hodlr_t h, int* levels); /* inner levels */
+int hodlr_get_num_blocks(hodlr_t h, int* blocks);
+int hodlr_get_block_info(hodlr_t h, int block, int* level, int* row0, int* col0, int* m,
+                         int* n, int* rank, int* iters);
+int hodlr_get_ranks(hodlr_t h, int* ranks);
+/* ACA pivot (row, column) of each stored step, block-local indices. */
+int hodlr_get_pivots(hodlr_t h, int block, int* rows, int* cols, int* count);
+/* Low-rank factors of a block: W (m x rank) and V (n x rank), host memory. */
+int hodlr_get_lowrank(hodlr_t h, int block, double* W, double* V);
+/* Smallest |eps - tol| / tol met by the block's stopping tests, and how many
+ * of them were within 1e-10 (ranks can differ from a CPU run only there). */
+int hodlr_get_block_margin(hodlr_t h, int block, double* margin, int* near);
+
+/* ACA kernel statistics of the last compression: launches, summed device
+ * time (seconds) and algorithmic bytes (one read of the W and V panels for
+ * the residual and one for the norm update per step, plus the new columns). */
+int hodlr_get_aca_stats(hodlr_t h, int* launches, double* seconds, double* bytes);
+
+const char* hodlr_status_string(int status);
+const char* hodlr_last_error(hodlr_t h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HODLR_B200_H */

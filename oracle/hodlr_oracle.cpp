@@ -1,0 +1,687 @@
+// CPU restatement of the reference HODLR hot path.  TEST INFRASTRUCTURE ONLY:
+// this library is the parity checker for the CUDA path.  Only tests/,
+// __graft_entry__.smoke() and the cpu_baseline leg of bench.py may load it;
+// the product never links or calls it.
+//
+// It follows the reference (amiraa127/Dense_HODLR) step by step:
+//   tree        src/HODLR_Tree.cpp:33-132        (createDefaultTree)
+//   compression src/HODLR_Matrix.cpp:274-338     (storeLRinTree, kernel + dense)
+//   ACA         src/lowRank.cpp:117-279,291-298  (partialPivACA_LowRankApprox,
+//                                                 chooseNextRowCol)
+//   factorize   src/HODLR_Matrix.cpp:505-518,612-692 (recLU_Factorize)
+//   solve       src/HODLR_Matrix.cpp:694-755     (recLU_Solve)
+//   entries     src/kernel.cpp:19-39             (kernelMatrix block / () / *)
+// Eigen's PartialPivLU, GEMM and norms (third party, not in the reference
+// tree) are restated from their mathematical definitions: row partial
+// pivoting on the first maximum |a| of the column, unit-lower L; plain
+// triple-loop products; norms as sqrt of the sequential sum of squares.
+// Built with -ffp-contract=off so every product and sum is rounded on its
+// own, as in the reference's SSE2 build (CMakeLists.txt:8, no -march).
+//
+// Parity status: the reference cannot be compiled in this environment (it
+// needs Eigen and CppUnit, neither present).  This restatement is pinned to
+// the reference's own test assertions (test/test.cpp:57-69 random exact-rank
+// HODLR, rel. error < 1e-8; test/test.cpp:112-129 1D inverse multiquadric,
+// rel. error < 1e-6) and to a dense LU of the same matrices; ACA pivot/rank
+// reduction orders inside Eigen are not pinned by any reference test.
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+#include "../dense_hodlr_b200/csrc/kfun.h"
+
+namespace {
+
+struct Mat {  // column-major dense matrix
+  int r = 0, c = 0;
+  std::vector<double> a;
+  Mat() {}
+  Mat(int r_, int c_) : r(r_), c(c_), a((size_t)r_ * c_, 0.0) {}
+  double& operator()(int i, int j) { return a[(size_t)j * r + i]; }
+  double operator()(int i, int j) const { return a[(size_t)j * r + i]; }
+};
+
+// Partial-pivot LU (Eigen PartialPivLU semantics, restated).
+struct LU {
+  Mat lu;
+  std::vector<int> piv;  // row swapped with row p at step p
+  int nzero = 0;         // exact-zero pivots met
+  void factor(const Mat& A) {
+    lu = A;
+    int n = lu.r;
+    piv.assign(n, 0);
+    for (int p = 0; p < n; ++p) {
+      int best = p;
+      double bv = std::fabs(lu(p, p));
+      for (int i = p + 1; i < n; ++i)
+        if (std::fabs(lu(i, p)) > bv) { bv = std::fabs(lu(i, p)); best = i; }
+      piv[p] = best;
+      if (best != p)
+        for (int j = 0; j < n; ++j) std::swap(lu(p, j), lu(best, j));
+      double d = lu(p, p);
+      if (d == 0.0) { ++nzero; continue; }
+      for (int i = p + 1; i < n; ++i) lu(i, p) = lu(i, p) / d;
+      for (int j = p + 1; j < n; ++j) {
+        double u = lu(p, j);
+        for (int i = p + 1; i < n; ++i) lu(i, j) = lu(i, j) - lu(i, p) * u;
+      }
+    }
+  }
+  Mat solve(const Mat& B) const {
+    Mat X = B;
+    int n = lu.r;
+    for (int p = 0; p < n; ++p)
+      if (piv[p] != p)
+        for (int j = 0; j < X.c; ++j) std::swap(X(p, j), X(piv[p], j));
+    for (int j = 0; j < X.c; ++j) {
+      for (int p = 0; p < n; ++p) {
+        double v = X(p, j);
+        for (int i = p + 1; i < n; ++i) X(i, j) = X(i, j) - lu(i, p) * v;
+      }
+      for (int p = n - 1; p >= 0; --p) {
+        X(p, j) = X(p, j) / lu(p, p);
+        double v = X(p, j);
+        for (int i = 0; i < p; ++i) X(i, j) = X(i, j) - lu(i, p) * v;
+      }
+    }
+    return X;
+  }
+};
+
+// C = A^T B
+Mat matTmul(const Mat& A, const Mat& B) {
+  Mat C(A.c, B.c);
+  for (int j = 0; j < B.c; ++j)
+    for (int i = 0; i < A.c; ++i) {
+      double s = 0.0;
+      for (int k = 0; k < A.r; ++k) s = s + A(k, i) * B(k, j);
+      C(i, j) = s;
+    }
+  return C;
+}
+// C = A B
+Mat matmul(const Mat& A, const Mat& B) {
+  Mat C(A.r, B.c);
+  for (int j = 0; j < B.c; ++j)
+    for (int k = 0; k < A.c; ++k) {
+      double b = B(k, j);
+      for (int i = 0; i < A.r; ++i) C(i, j) = C(i, j) + A(i, k) * b;
+    }
+  return C;
+}
+
+struct Node {
+  int level, min, split, max;  // split == last row of the top half
+  int left = -1, right = -1;   // child indices: >= 0 inner node, < 0 leaf (-1-id)
+  bool leaf;
+};
+
+struct Block {  // one off-diagonal block and its ACA result
+  int r0 = 0, c0 = 0, m = 0, n = 0;
+  int rank = 0, iters = 0;
+  Mat W, V;
+  std::vector<int> prow, pcol;
+  double eps = 1.0;
+  double margin = HUGE_VAL;  // min |eps - tol| / tol over the loop tests
+};
+
+struct Oracle {
+  int n = 0, leaf = 30, dim = 1;
+  bool dense = false;
+  std::vector<double> pts;  // SoA, dim-major
+  std::vector<double> A;    // dense input, column-major n x n
+  hx_kparams kp{};
+  double tol = 1e-6;
+  int minPivot = 0;
+  // tree: inner nodes in level order (nodeLevelVec order), leaves in index order
+  std::vector<Node> nodes;       // all nodes (pointer-tree restatement)
+  std::vector<int> inner;        // node ids of inner nodes, level order
+  std::vector<int> leaves;       // node ids of leaves, index order
+  std::vector<int> inner_pos;    // node id -> position in `inner` (-1 if leaf)
+  int numLevels = 0;
+  std::vector<Block> blocks;     // 2 per inner node: [2p] top, [2p+1] bottom
+  std::vector<Mat> leafMat;      // per leaf
+  // factor
+  std::vector<LU> leafLU;
+  std::vector<LU> schurLU;        // per inner node
+  std::vector<Mat> topSolnLR, bottSolnLR;
+  std::vector<int> leaf_pos;     // node id -> leaf position
+  bool compressed = false, factored = false;
+  int status = 0;
+
+  double entry(int i, int j) const {
+    if (dense) return A[(size_t)j * n + i];
+    return hx_entry(kp, pts.data(), n, i, j);
+  }
+};
+
+// ---------------------------------------------------------------- tree
+// createDefaultTree (src/HODLR_Tree.cpp:33-132): the root is a leaf iff
+// N < leaf; a child splits iff its size > leaf; a left-type child splits at
+// min + floor(s/2) - 1, a right-type child at max - floor(s/2).
+void build_tree(Oracle& o) {
+  o.nodes.clear();
+  std::vector<std::vector<int>> levelVec;
+  Node root;
+  root.level = 0;
+  root.min = 0;
+  root.max = o.n - 1;
+  root.split = o.n / 2 - 1;
+  root.leaf = o.n < o.leaf;
+  o.nodes.push_back(root);
+  o.numLevels = 1;
+  std::vector<int> leafOrder;
+  if (root.leaf) {
+    leafOrder.push_back(0);
+  } else {
+    levelVec.resize(1);
+    levelVec[0].push_back(0);
+  }
+  // Pre-order recursion, left child before right child.
+  struct R {
+    static void go(Oracle& o, int id, std::vector<std::vector<int>>& lv,
+                   std::vector<int>& lo) {
+      Node nd = o.nodes[id];
+      int topSize = nd.split - nd.min + 1;
+      int bottSize = nd.max - nd.split;
+      if (nd.level > o.numLevels - 1) o.numLevels = nd.level + 1;
+      Node L, Rt;
+      L.min = nd.min;
+      L.max = nd.min + topSize - 1;
+      L.level = nd.level + 1;
+      int lid = (int)o.nodes.size();
+      if (topSize > o.leaf) {
+        L.leaf = false;
+        L.split = nd.min + topSize / 2 - 1;
+      } else {
+        L.leaf = true;
+        L.split = -1;
+      }
+      o.nodes.push_back(L);
+      o.nodes[id].left = lid;
+      if (!L.leaf) {
+        if ((int)lv.size() <= L.level) lv.resize(L.level + 1);
+        lv[L.level].push_back(lid);
+        go(o, lid, lv, lo);
+      } else {
+        lo.push_back(lid);
+        if (L.level > o.numLevels - 1) o.numLevels = L.level + 1;
+      }
+      Rt.min = nd.min + topSize;
+      Rt.max = nd.max;
+      Rt.level = nd.level + 1;
+      int rid = (int)o.nodes.size();
+      if (bottSize > o.leaf) {
+        Rt.leaf = false;
+        Rt.split = nd.max - bottSize / 2;
+      } else {
+        Rt.leaf = true;
+        Rt.split = -1;
+      }
+      o.nodes.push_back(Rt);
+      o.nodes[id].right = rid;
+      if (!Rt.leaf) {
+        if ((int)lv.size() <= Rt.level) lv.resize(Rt.level + 1);
+        lv[Rt.level].push_back(rid);
+        go(o, rid, lv, lo);
+      } else {
+        lo.push_back(rid);
+        if (Rt.level > o.numLevels - 1) o.numLevels = Rt.level + 1;
+      }
+    }
+  };
+  if (!root.leaf) R::go(o, 0, levelVec, leafOrder);
+  o.inner.clear();
+  for (auto& lv : levelVec)
+    for (int id : lv) o.inner.push_back(id);
+  o.leaves = leafOrder;
+  o.inner_pos.assign(o.nodes.size(), -1);
+  for (size_t p = 0; p < o.inner.size(); ++p) o.inner_pos[o.inner[p]] = (int)p;
+  o.leaf_pos.assign(o.nodes.size(), -1);
+  for (size_t p = 0; p < o.leaves.size(); ++p) o.leaf_pos[o.leaves[p]] = (int)p;
+  o.blocks.assign(2 * o.inner.size(), Block());
+  for (size_t p = 0; p < o.inner.size(); ++p) {
+    const Node& nd = o.nodes[o.inner[p]];
+    Block& t = o.blocks[2 * p];
+    t.r0 = nd.min;
+    t.c0 = nd.split + 1;
+    t.m = nd.split - nd.min + 1;
+    t.n = nd.max - nd.split;
+    Block& b = o.blocks[2 * p + 1];
+    b.r0 = nd.split + 1;
+    b.c0 = nd.min;
+    b.m = nd.max - nd.split;
+    b.n = nd.split - nd.min + 1;
+  }
+}
+
+// ------------------------------------------------------------------ ACA
+static double dot(const double* x, const double* y, int n) {
+  double s = 0.0;
+  for (int i = 0; i < n; ++i) s = s + x[i] * y[i];
+  return s;
+}
+
+// chooseNextRowCol (src/lowRank.cpp:291-298)
+static int choose_next(const std::vector<char>& chosen, const std::vector<double>& v,
+                       int minPivot) {
+  for (size_t i = 0; i < v.size(); ++i)
+    if (!chosen[i] && std::fabs(v[i]) > minPivot) return (int)i;
+  return -1;
+}
+
+// partialPivACA_LowRankApprox (src/lowRank.cpp:117-279).  minRank/maxRank
+// are -1 on the default tree (src/HODLR_Tree.cpp:44-47).
+void aca(const Oracle& o, Block& B, double tol, int minRank, int maxRank, int minPivot) {
+  const int m = B.m, n = B.n, min_i = B.r0, min_j = B.c0;
+  B.prow.clear();
+  B.pcol.clear();
+  B.margin = HUGE_VAL;
+  if (maxRank == 0) {
+    B.W = Mat(m, 1);
+    B.V = Mat(n, 1);
+    B.rank = 1;
+    B.iters = 0;
+    B.eps = 1;
+    return;
+  }
+  const int ub = std::min(m, n);
+  std::vector<std::vector<double>> W, V;  // columns
+  std::vector<char> chosenR(m, 0), chosenC(n, 0);
+  std::vector<double> rr(n), rc(m), s;
+  double frob2 = 0, eps = 1;
+  int cr = 0, cc = 0, nr = 0, k = 0, iters = 0;
+  auto note = [&](double e) {
+    double g = std::fabs(e - tol) / tol;
+    if (g < B.margin) B.margin = g;
+  };
+  while ((eps > tol || k < minRank) && k < ub) {
+    ++iters;
+    chosenR[cr] = 1;
+    const int gi = cr + min_i;
+    s.assign(n, 0.0);
+    for (int l = 0; l < k; ++l) {
+      double w = W[l][cr];
+      const double* vl = V[l].data();
+      for (int j = 0; j < n; ++j) s[j] = s[j] + w * vl[j];
+    }
+    for (int j = 0; j < n; ++j) rr[j] = o.entry(gi, j + min_j) - s[j];
+    int mi = 0;
+    double mv = std::fabs(rr[0]);
+    for (int j = 1; j < n; ++j)
+      if (std::fabs(rr[j]) > mv) { mv = std::fabs(rr[j]); mi = j; }
+    if (mv <= minPivot) {
+      int f = -1;
+      for (int i = 0; i < m; ++i)
+        if (!chosenR[i]) { f = i; break; }
+      if (f == -1) break;
+      cr = f;
+      continue;
+    }
+    if (!chosenC[mi]) {
+      cc = mi;
+    } else {
+      cc = choose_next(chosenC, rr, minPivot);
+      if (cc == -1) break;
+    }
+    chosenC[cc] = 1;
+    const int gj = cc + min_j;
+    double piv = 1 / rr[cc];
+    s.assign(m, 0.0);
+    for (int l = 0; l < k; ++l) {
+      double v = V[l][cc];
+      const double* wl = W[l].data();
+      for (int i = 0; i < m; ++i) s[i] = s[i] + v * wl[i];
+    }
+    for (int i = 0; i < m; ++i) rc[i] = o.entry(i + min_i, gj) - s[i];
+    mi = 0;
+    mv = std::fabs(rc[0]);
+    for (int i = 1; i < m; ++i)
+      if (std::fabs(rc[i]) > mv) { mv = std::fabs(rc[i]); mi = i; }
+    if (!chosenR[mi])
+      nr = mi;
+    else
+      nr = choose_next(chosenR, rc, minPivot);
+    if (nr == -1) break;
+    std::vector<double> wk(m);
+    for (int i = 0; i < m; ++i) wk[i] = piv * rc[i];
+    W.push_back(wk);
+    V.push_back(rr);
+    B.prow.push_back(cr);
+    B.pcol.push_back(cc);
+    double sumNorm = 0;
+    for (int j = 0; j < k; ++j)
+      sumNorm += dot(wk.data(), W[j].data(), m) * dot(V[j].data(), rr.data(), n);
+    double sw = dot(wk.data(), wk.data(), m), sv = dot(rr.data(), rr.data(), n);
+    frob2 += 2 * sumNorm + sw * sv;
+    double frob = std::sqrt(frob2);
+    eps = std::sqrt(sw) * std::sqrt(sv) / frob;
+    cr = nr;
+    k++;
+    if (k == maxRank) break;
+    if (k < ub && k >= minRank) note(eps);
+  }
+  B.iters = iters;
+  B.eps = eps;
+  B.rank = k;
+  if (k == 0) {
+    B.W = Mat(m, 1);
+    B.V = Mat(n, 1);
+    B.rank = 1;
+    return;
+  }
+  if (k >= ub - 1) {
+    if (n <= m) {
+      B.W = Mat(m, n);
+      for (int j = 0; j < n; ++j)
+        for (int i = 0; i < m; ++i) B.W(i, j) = o.entry(i + min_i, j + min_j);
+      B.V = Mat(n, n);
+      for (int j = 0; j < n; ++j) B.V(j, j) = 1.0;
+      B.rank = n;
+    } else {
+      B.W = Mat(m, m);
+      for (int j = 0; j < m; ++j) B.W(j, j) = 1.0;
+      B.V = Mat(n, m);
+      for (int j = 0; j < n; ++j)
+        for (int i = 0; i < m; ++i) B.V(j, i) = o.entry(i + min_i, j + min_j);
+      B.rank = m;
+    }
+    return;
+  }
+  B.W = Mat(m, k);
+  B.V = Mat(n, k);
+  for (int l = 0; l < k; ++l) {
+    std::memcpy(&B.W.a[(size_t)l * m], W[l].data(), sizeof(double) * m);
+    std::memcpy(&B.V.a[(size_t)l * n], V[l].data(), sizeof(double) * n);
+  }
+}
+
+template <class F>
+void parallel_for(int count, int nthreads, F f) {
+  if (nthreads <= 1 || count <= 1) {
+    for (int i = 0; i < count; ++i) f(i);
+    return;
+  }
+  std::atomic<int> next(0);
+  std::vector<std::thread> th;
+  for (int t = 0; t < nthreads; ++t)
+    th.emplace_back([&]() {
+      for (;;) {
+        int i = next.fetch_add(1);
+        if (i >= count) break;
+        f(i);
+      }
+    });
+  for (auto& t : th) t.join();
+}
+
+// storeLRinTree (src/HODLR_Matrix.cpp:274-338): leaves copy their diagonal
+// block, inner nodes compress their two off-diagonal blocks with ACA.  The
+// blocks are independent, so they are processed largest first on a pool.
+void compress(Oracle& o, int nthreads) {
+  std::vector<int> order(o.blocks.size());
+  for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    return (int64_t)o.blocks[a].m * o.blocks[a].n > (int64_t)o.blocks[b].m * o.blocks[b].n;
+  });
+  parallel_for((int)order.size(), nthreads, [&](int t) {
+    aca(o, o.blocks[order[t]], o.tol, -1, -1, o.minPivot);
+  });
+  o.leafMat.assign(o.leaves.size(), Mat());
+  parallel_for((int)o.leaves.size(), nthreads, [&](int p) {
+    const Node& nd = o.nodes[o.leaves[p]];
+    int s = nd.max - nd.min + 1;
+    Mat M(s, s);
+    for (int j = 0; j < s; ++j)
+      for (int i = 0; i < s; ++i) M(i, j) = o.entry(nd.min + i, nd.min + j);
+    o.leafMat[p] = M;
+  });
+  o.compressed = true;
+}
+
+// recLU_Factorize(rhs, node) (src/HODLR_Matrix.cpp:612-692)
+Mat rec_factor(Oracle& o, const Mat& rhs, int id) {
+  const Node& nd = o.nodes[id];
+  if (nd.leaf) {
+    int p = o.leaf_pos[id];
+    o.leafLU[p].factor(o.leafMat[p]);
+    return o.leafLU[p].solve(rhs);
+  }
+  int p = o.inner_pos[id];
+  const Block& T = o.blocks[2 * p];
+  const Block& Bt = o.blocks[2 * p + 1];
+  int st = nd.split - nd.min + 1, sb = nd.max - nd.split, c = rhs.c;
+  int kt = T.W.c, kb = Bt.W.c;
+  Mat topRHS(st, c + kt);
+  for (int j = 0; j < c; ++j)
+    for (int i = 0; i < st; ++i) topRHS(i, j) = rhs(i, j);
+  for (int j = 0; j < kt; ++j)
+    for (int i = 0; i < st; ++i) topRHS(i, c + j) = T.W(i, j);
+  Mat Xt = rec_factor(o, topRHS, nd.left);
+  Mat bottRHS(sb, c + kb);
+  for (int j = 0; j < c; ++j)
+    for (int i = 0; i < sb; ++i) bottRHS(i, j) = rhs(st + i, j);
+  for (int j = 0; j < kb; ++j)
+    for (int i = 0; i < sb; ++i) bottRHS(i, c + j) = Bt.W(i, j);
+  Mat Xb = rec_factor(o, bottRHS, nd.right);
+  Mat XtP(st, c), XbP(sb, c), tS(st, kt), bS(sb, kb);
+  for (int j = 0; j < c; ++j)
+    for (int i = 0; i < st; ++i) XtP(i, j) = Xt(i, j);
+  for (int j = 0; j < kt; ++j)
+    for (int i = 0; i < st; ++i) tS(i, j) = Xt(i, c + j);
+  for (int j = 0; j < c; ++j)
+    for (int i = 0; i < sb; ++i) XbP(i, j) = Xb(i, j);
+  for (int j = 0; j < kb; ++j)
+    for (int i = 0; i < sb; ++i) bS(i, j) = Xb(i, c + j);
+  o.topSolnLR[p] = tS;
+  o.bottSolnLR[p] = bS;
+  int rt = T.rank, rb = Bt.rank;  // == kt, kb
+  int sd = rt + rb;
+  Mat S(sd, sd);
+  for (int i = 0; i < rb; ++i) S(i, i) = 1.0;
+  for (int i = 0; i < rt; ++i) S(rb + i, rb + i) = 1.0;
+  Mat TR = matTmul(Bt.V, tS);  // k_b x k_t
+  Mat BL = matTmul(T.V, bS);   // k_t x k_b
+  for (int j = 0; j < rt; ++j)
+    for (int i = 0; i < rb; ++i) S(i, rb + j) = TR(i, j);
+  for (int j = 0; j < rb; ++j)
+    for (int i = 0; i < rt; ++i) S(rb + i, j) = BL(i, j);
+  o.schurLU[p].factor(S);
+  Mat top = matTmul(Bt.V, XtP), bot = matTmul(T.V, XbP);
+  Mat Z(sd, c);
+  for (int j = 0; j < c; ++j) {
+    for (int i = 0; i < rb; ++i) Z(i, j) = top(i, j);
+    for (int i = 0; i < rt; ++i) Z(rb + i, j) = bot(i, j);
+  }
+  Mat y = o.schurLU[p].solve(Z);
+  Mat yb(rt, c), yt(rb, c);
+  for (int j = 0; j < c; ++j) {
+    for (int i = 0; i < rt; ++i) yb(i, j) = y(rb + i, j);
+    for (int i = 0; i < rb; ++i) yt(i, j) = y(i, j);
+  }
+  Mat ut = matmul(tS, yb), ub = matmul(bS, yt);
+  Mat res(st + sb, c);
+  for (int j = 0; j < c; ++j) {
+    for (int i = 0; i < st; ++i) res(i, j) = XtP(i, j) - ut(i, j);
+    for (int i = 0; i < sb; ++i) res(st + i, j) = XbP(i, j) - ub(i, j);
+  }
+  return res;
+}
+
+// recLU_Solve(rhs, node) (src/HODLR_Matrix.cpp:694-755)
+Mat rec_solve(const Oracle& o, const Mat& rhs, int id) {
+  const Node& nd = o.nodes[id];
+  if (nd.leaf) return o.leafLU[o.leaf_pos[id]].solve(rhs);
+  int p = o.inner_pos[id];
+  const Block& T = o.blocks[2 * p];
+  const Block& Bt = o.blocks[2 * p + 1];
+  int st = nd.split - nd.min + 1, sb = nd.max - nd.split, c = rhs.c;
+  Mat rt_(st, c), rb_(sb, c);
+  for (int j = 0; j < c; ++j) {
+    for (int i = 0; i < st; ++i) rt_(i, j) = rhs(i, j);
+    for (int i = 0; i < sb; ++i) rb_(i, j) = rhs(st + i, j);
+  }
+  Mat xt = rec_solve(o, rt_, nd.left);
+  Mat xb = rec_solve(o, rb_, nd.right);
+  int rt = T.rank, rb = Bt.rank, sd = rt + rb;
+  Mat top = matTmul(Bt.V, xt), bot = matTmul(T.V, xb);
+  Mat Z(sd, c);
+  for (int j = 0; j < c; ++j) {
+    for (int i = 0; i < rb; ++i) Z(i, j) = top(i, j);
+    for (int i = 0; i < rt; ++i) Z(rb + i, j) = bot(i, j);
+  }
+  Mat y = o.schurLU[p].solve(Z);
+  Mat yb(rt, c), yt(rb, c);
+  for (int j = 0; j < c; ++j) {
+    for (int i = 0; i < rt; ++i) yb(i, j) = y(rb + i, j);
+    for (int i = 0; i < rb; ++i) yt(i, j) = y(i, j);
+  }
+  Mat ut = matmul(o.topSolnLR[p], yb), ub = matmul(o.bottSolnLR[p], yt);
+  Mat res(st + sb, c);
+  for (int j = 0; j < c; ++j) {
+    for (int i = 0; i < st; ++i) res(i, j) = xt(i, j) - ut(i, j);
+    for (int i = 0; i < sb; ++i) res(st + i, j) = xb(i, j) - ub(i, j);
+  }
+  return res;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------ C interface
+extern "C" {
+
+void* orc_create_kernel(int n, int dim, const double* pts, int ktype, double lscale,
+                        double shift, int diag_replace, double diag_value, int leaf) {
+  Oracle* o = new Oracle();
+  o->n = n;
+  o->dim = dim;
+  o->leaf = leaf;
+  o->dense = false;
+  o->pts.assign(pts, pts + (size_t)n * dim);
+  o->kp = hx_make_kparams(ktype, dim, lscale, shift, diag_replace, diag_value);
+  build_tree(*o);
+  return o;
+}
+
+void* orc_create_dense(int n, const double* A, int lda, int leaf) {
+  Oracle* o = new Oracle();
+  o->n = n;
+  o->leaf = leaf;
+  o->dense = true;
+  o->A.resize((size_t)n * n);
+  for (int j = 0; j < n; ++j)
+    std::memcpy(&o->A[(size_t)j * n], A + (size_t)j * lda, sizeof(double) * n);
+  build_tree(*o);
+  return o;
+}
+
+void orc_destroy(void* h) { delete (Oracle*)h; }
+
+void orc_set_lr(void* h, double tol, double minPivot) {
+  Oracle* o = (Oracle*)h;
+  o->tol = tol;
+  o->minPivot = (int)minPivot;  // the reference passes a double into an int parameter
+  o->compressed = o->factored = false;
+}
+
+int orc_compress(void* h, int nthreads) {
+  compress(*(Oracle*)h, nthreads);
+  return 0;
+}
+
+int orc_factorize(void* h) {
+  Oracle* o = (Oracle*)h;
+  if (!o->compressed) compress(*o, 1);
+  o->leafLU.assign(o->leaves.size(), LU());
+  o->schurLU.assign(o->inner.size(), LU());
+  o->topSolnLR.assign(o->inner.size(), Mat());
+  o->bottSolnLR.assign(o->inner.size(), Mat());
+  // recLU_Factorize() (src/HODLR_Matrix.cpp:505-518): dummy RHS LinSpaced(N,-2,2)
+  Mat dummy(o->n, 1);
+  for (int i = 0; i < o->n; ++i)
+    dummy(i, 0) = o->n > 1 ? -2.0 + 4.0 * i / (o->n - 1) : -2.0;
+  rec_factor(*o, dummy, 0);
+  o->factored = true;
+  int nz = 0;
+  for (auto& l : o->leafLU) nz += l.nzero;
+  for (auto& l : o->schurLU) nz += l.nzero;
+  return nz;
+}
+
+int orc_solve(void* h, int nrhs, const double* b, double* x) {
+  Oracle* o = (Oracle*)h;
+  if (!o->factored) orc_factorize(h);
+  Mat B(o->n, nrhs);
+  std::memcpy(B.a.data(), b, sizeof(double) * (size_t)o->n * nrhs);
+  Mat X = rec_solve(*o, B, 0);
+  std::memcpy(x, X.a.data(), sizeof(double) * (size_t)o->n * nrhs);
+  return 0;
+}
+
+int orc_num_levels(void* h) { return ((Oracle*)h)->numLevels; }
+int orc_num_inner(void* h) { return (int)((Oracle*)h)->inner.size(); }
+int orc_num_leaves(void* h) { return (int)((Oracle*)h)->leaves.size(); }
+
+void orc_inner_info(void* h, int p, int* level, int* mn, int* split, int* mx) {
+  const Node& nd = ((Oracle*)h)->nodes[((Oracle*)h)->inner[p]];
+  *level = nd.level;
+  *mn = nd.min;
+  *split = nd.split;
+  *mx = nd.max;
+}
+
+void orc_leaf_info(void* h, int p, int* level, int* mn, int* mx) {
+  const Node& nd = ((Oracle*)h)->nodes[((Oracle*)h)->leaves[p]];
+  *level = nd.level;
+  *mn = nd.min;
+  *mx = nd.max;
+}
+
+int orc_block_rank(void* h, int b) { return ((Oracle*)h)->blocks[b].rank; }
+int orc_block_iters(void* h, int b) { return ((Oracle*)h)->blocks[b].iters; }
+double orc_block_eps(void* h, int b) { return ((Oracle*)h)->blocks[b].eps; }
+double orc_block_margin(void* h, int b) { return ((Oracle*)h)->blocks[b].margin; }
+
+int orc_block_pivots(void* h, int b, int* rows, int* cols) {
+  const Block& B = ((Oracle*)h)->blocks[b];
+  for (size_t t = 0; t < B.prow.size(); ++t) {
+    rows[t] = B.prow[t];
+    cols[t] = B.pcol[t];
+  }
+  return (int)B.prow.size();
+}
+
+// W (m x rank) and V (n x rank), column-major.
+void orc_block_lowrank(void* h, int b, double* W, double* V) {
+  const Block& B = ((Oracle*)h)->blocks[b];
+  std::memcpy(W, B.W.a.data(), sizeof(double) * B.W.a.size());
+  std::memcpy(V, B.V.a.data(), sizeof(double) * B.V.a.size());
+}
+
+double orc_entry(void* h, int i, int j) { return ((Oracle*)h)->entry(i, j); }
+
+double orc_exp(double x) { return hx_exp(x); }
+
+// Full-kernel product Y = K X (kernelMatrix::operator*, src/kernel.cpp:27-35),
+// summing over k in order for each (i, j); rows spread over threads.
+void orc_kernel_matvec(void* h, int nrhs, const double* X, double* Y, int nthreads) {
+  const Oracle* o = (const Oracle*)h;
+  int n = o->n;
+  int chunks = (n + 63) / 64;
+  parallel_for(chunks, nthreads, [&](int c) {
+    int i0 = c * 64, i1 = std::min(n, i0 + 64);
+    for (int j = 0; j < nrhs; ++j)
+      for (int i = i0; i < i1; ++i) {
+        double s = 0.0;
+        for (int k = 0; k < n; ++k) s = s + o->entry(i, k) * X[(size_t)j * n + k];
+        Y[(size_t)j * n + i] = s;
+      }
+  });
+}
+
+}  // extern "C"

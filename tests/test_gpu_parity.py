@@ -1,0 +1,182 @@
+"""Parity of the CUDA path (through the C ABI) against the CPU oracle.
+
+Bit-exact: tree, ACA pivot sequences, ranks and the W/V factors (integer and
+pivot-deciding FP64 work).  Tolerance: solutions within 1e-10 relative
+difference of the oracle (the north-star bar for the FP64 path), residuals
+with the full kernel.  Blocks whose stopping test came within 1e-10 of the
+tolerance (a "near tie", where reduction order may decide the rank) are
+reported and excluded from the bit-exact rank comparison; the tests assert
+there are none on these inputs.
+"""
+import numpy as np
+import pytest
+
+from dense_hodlr_b200 import HODLR_Matrix, HODLRError, KernelSpec, kernelMatrix
+from dense_hodlr_b200.points import uniform_cube
+
+from .conftest import c1_points
+
+pytestmark = pytest.mark.gpu
+
+SOLVE_TOL = 1e-10  # relative difference vs the oracle, FP64 path
+
+
+def _pair(oracle_mod, pts, kind, l, shift, leaf, tol, diag_replace=False, diag_value=0.0):
+    g = HODLR_Matrix(pts.shape[1], pts.shape[1],
+                     KernelSpec(kind, l, shift, diag_replace, diag_value), pts, leaf)
+    g.set_LRTolerance(tol)
+    ktype = g_kind(kind)
+    o = oracle_mod.OracleHODLR.from_kernel(pts, ktype, l, shift=shift, leaf=leaf,
+                                           diag_replace=diag_replace, diag_value=diag_value)
+    o.set_lr(tol)
+    return g, o
+
+
+def g_kind(kind):
+    from dense_hodlr_b200.hodlr import _KERNEL_NAMES
+    return _KERNEL_NAMES[kind] if isinstance(kind, str) else kind
+
+
+def _compare_compression(g, o, check_factors=True):
+    g.storeLRinTree()
+    o.compress()
+    nb = g.num_blocks()
+    assert nb == o.num_blocks()
+    gr, orr = g.ranks(), o.ranks()
+    om = o.margins()
+    near = [b for b in range(nb) if g.margin(b)[1] > 0 or om[b] < 1e-10]
+    assert not near, f"near-tie blocks: {near}"
+    assert np.array_equal(gr, orr), np.nonzero(gr != orr)
+    inner = o.inner_nodes()
+    for b in range(nb):
+        info = g.block_info(b)
+        lvl, mn, sp, mx = inner[b // 2]
+        assert info["level"] == lvl
+        if b % 2 == 0:
+            assert (info["row0"], info["col0"], info["m"], info["n"]) == (mn, sp + 1, sp - mn + 1, mx - sp)
+        else:
+            assert (info["row0"], info["col0"], info["m"], info["n"]) == (sp + 1, mn, mx - sp, sp - mn + 1)
+        gp = g.pivots(b)
+        op = o.pivots(b)
+        assert np.array_equal(gp[0], op[0]) and np.array_equal(gp[1], op[1]), f"block {b}"
+        if check_factors:
+            W, V = g.lowrank(b)
+            Wo, Vo = o.lowrank(b, info["m"], info["n"])
+            assert np.array_equal(W, Wo), f"W of block {b}"
+            assert np.array_equal(V, Vo), f"V of block {b}"
+
+
+def test_c1_gaussian_1d_bit_exact(oracle_mod):
+    """N=4096 sorted uniform [-1,1], exp(-(dx)^2/0.1^2) + 1.0 delta, leaf 64, tol 1e-10."""
+    pts, rng = c1_points()
+    g, o = _pair(oracle_mod, pts, "gaussian", 0.1, 1.0, 64, 1e-10)
+    _compare_compression(g, o)
+    b = rng.standard_normal((4096, 1))
+    x = g.recLU_Solve(b)
+    xo = o.solve(b)
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= SOLVE_TOL
+    # dense FP64 LU oracle of the same K
+    K = np.exp(-((pts[0][:, None] - pts[0][None, :]) ** 2) / 0.01) + np.eye(4096)
+    xd = np.linalg.solve(K, b)
+    assert np.linalg.norm(x - xd) / np.linalg.norm(xd) < 1e-9
+    rel = g.residual(x, b)
+    assert rel.max() < 1e-9
+
+
+def test_uneven_2d_matern(oracle_mod):
+    """Uneven sizes exercise the left/right split asymmetry of createDefaultTree."""
+    pts = uniform_cube(3001, 2, 11)
+    g, o = _pair(oracle_mod, pts, "matern32", 0.2, 1e-2, 64, 1e-8)
+    _compare_compression(g, o)
+    b = np.random.default_rng(3).standard_normal((3001, 3))
+    x = g.recLU_Solve(b)
+    xo = o.solve(b)
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= SOLVE_TOL
+
+
+def test_3d_gaussian_group_levels(oracle_mod):
+    """3D Gaussian, leaf 128: top levels run with many CTAs per block."""
+    pts = uniform_cube(16384, 3, 5)
+    g, o = _pair(oracle_mod, pts, "gaussian", 0.3, 1e-1, 128, 1e-8)
+    _compare_compression(g, o, check_factors=False)
+    for b in (0, 1, 2, 5):  # the largest blocks, W/V bit for bit
+        info = g.block_info(b)
+        W, V = g.lowrank(b)
+        Wo, Vo = o.lowrank(b, info["m"], info["n"])
+        assert np.array_equal(W, Wo) and np.array_equal(V, Vo)
+    b = np.random.default_rng(4).standard_normal((16384, 4))
+    x = g.recLU_Solve(b)
+    xo = o.solve(b)
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= SOLVE_TOL
+
+
+def test_kernel_matvec_matches_oracle(oracle_mod):
+    pts = uniform_cube(5000, 3, 9)
+    g, o = _pair(oracle_mod, pts, "matern32", 0.1, 1e-2, 64, 1e-8)
+    x = np.random.default_rng(2).standard_normal((5000, 3))
+    import torch
+    xd = torch.from_numpy(np.asfortranarray(x).T.copy()).cuda()  # column-major = rows of x.T
+    yd = torch.empty_like(xd)
+    g.kernel_matvec_device(xd.data_ptr(), yd.data_ptr(), 3)
+    torch.cuda.synchronize()
+    y = yd.cpu().numpy().T
+    yo = o.kernel_matvec(x)
+    assert np.linalg.norm(y - yo) / np.linalg.norm(yo) < 1e-13
+
+
+def test_dense_input_inverse_multiquadric(oracle_mod):
+    """Reference test shape (test/test.cpp:112-129): dense 1D inverse multiquadric,
+    diagonal replaced by 0, leaf 30, tol 1e-8, solution error < 1e-6."""
+    n = 2000
+    x = np.linspace(-1.0, 1.0, n)
+    r = np.abs(x[:, None] - x[None, :])
+    A = 1.0 / np.sqrt(1.0 + r * r)
+    np.fill_diagonal(A, 0.0)
+    g = HODLR_Matrix(A, 30)
+    g.set_LRTolerance(1e-8)
+    o = oracle_mod.OracleHODLR.from_dense(A, leaf=30)
+    o.set_lr(1e-8)
+    _compare_compression(g, o)
+    xe = np.linspace(-2, 2, n)[:, None]
+    b = A @ xe
+    xs = g.recLU_Solve(b)
+    assert np.linalg.norm(xs - xe) / np.linalg.norm(xe) < 1e-6
+    xo = o.solve(b)
+    assert np.linalg.norm(xs - xo) / np.linalg.norm(xo) <= SOLVE_TOL
+
+
+def test_reference_random_exact_hodlr():
+    """Reference test shape (test/test.cpp:57-69): exact rank-10 HODLR, N=10000,
+    leaf 50, relative error < 1e-8 on x = LinSpaced(-2, 2)."""
+    from tests.test_oracle import exact_hodlr
+    n = 10000
+    A = exact_hodlr(n, 50, 10, seed=0)
+    g = HODLR_Matrix(A, 50)
+    xe = np.linspace(-2, 2, n)[:, None]
+    b = A @ xe
+    xs = g.recLU_Solve(b)
+    assert np.linalg.norm(xs - xe) / np.linalg.norm(xe) < 1e-8
+
+
+def test_tolerance_change_recompresses(oracle_mod):
+    pts, rng = c1_points(2048, 7)
+    g, o = _pair(oracle_mod, pts, "gaussian", 0.1, 1.0, 64, 1e-6)
+    g.storeLRinTree()
+    r1 = g.ranks().copy()
+    g.set_LRTolerance(1e-10)
+    o.set_lr(1e-10)
+    _compare_compression(g, o, check_factors=False)
+    assert g.ranks().sum() > r1.sum()
+
+
+def test_errors_are_status_codes():
+    with pytest.raises(HODLRError) as e:
+        HODLR_Matrix(100, 100, lambda i, j, d: 0.0, np.zeros((1, 100)), 30)
+    assert e.value.status == 4  # HODLR_ERR_UNSUPPORTED: host function pointer
+    pts, _ = c1_points(256, 1)
+    g = HODLR_Matrix(kernelMatrix(256, 256, KernelSpec("gaussian", 0.1, 1.0), pts), 32)
+    with pytest.raises(HODLRError) as e:
+        g.set_LRMethod("SVD")
+    assert e.value.status == 4
+    with pytest.raises(HODLRError):
+        g.recLU_Solve(np.zeros((10, 1)))

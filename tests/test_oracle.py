@@ -1,0 +1,266 @@
+"""CPU tests of the oracle: pinned to the reference's own test assertions, to
+an independent pure-Python restatement of ACA and of createDefaultTree, to a
+dense LU, and to the committed golden fixtures."""
+import math
+import os
+
+import numpy as np
+import pytest
+
+from .conftest import c1_points
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def exact_hodlr(n, leaf, rank, seed):
+    """createExactHODLR analogue (src/HODLR_Matrix.cpp:432-502): uniform [-1,1]
+    leaves and rank-`rank` off-diagonal blocks on the default tree, seeded."""
+    rng = np.random.default_rng(seed)
+    A = np.zeros((n, n))
+
+    def rec(mn, mx, split, is_root):
+        if split is None:
+            s = mx - mn + 1
+            A[mn:mx + 1, mn:mx + 1] = rng.uniform(-1, 1, (s, s))
+            return
+        t, b = split - mn + 1, mx - split
+        A[mn:split + 1, split + 1:mx + 1] = rng.uniform(-1, 1, (t, rank)) @ rng.uniform(-1, 1, (b, rank)).T
+        A[split + 1:mx + 1, mn:split + 1] = rng.uniform(-1, 1, (b, rank)) @ rng.uniform(-1, 1, (t, rank)).T
+        ls = mn + t // 2 - 1 if t > leaf else None
+        rs = mx - b // 2 if b > leaf else None
+        rec(mn, split, ls, False)
+        rec(split + 1, mx, rs, False)
+
+    if n < leaf:
+        A[:] = rng.uniform(-1, 1, (n, n))
+    else:
+        rec(0, n - 1, n // 2 - 1, True)
+    return A
+
+
+# ---------------------------------------------------------------- kfun.h
+def test_exp_within_one_ulp(oracle_mod):
+    xs = np.concatenate([np.linspace(-745.0, 709.7, 40001),
+                         np.random.default_rng(0).uniform(-40, 2, 20000),
+                         [0.0, -0.0, 1e-300, -1e-300, 0.5 * math.log(2), -0.5 * math.log(2)]])
+    worst = 0.0
+    for x in xs:
+        a, b = oracle_mod.hx_exp(x), math.exp(x)
+        if b >= 2.3e-308:
+            worst = max(worst, abs(a - b) / math.ulp(b))
+    assert worst <= 1.0
+    assert oracle_mod.hx_exp(-800.0) == 0.0
+    assert math.isinf(oracle_mod.hx_exp(710.0))
+    assert oracle_mod.hx_exp(0.0) == 1.0
+
+
+def test_kernel_entries_match_formulas(oracle_mod):
+    rng = np.random.default_rng(3)
+    pts = rng.uniform(0, 1, (3, 64))
+    l = 0.3
+    cases = [
+        (0, lambda r: np.exp(-r * r / (l * l))),
+        (1, lambda r: (1 + np.sqrt(3) * r / l) * np.exp(-np.sqrt(3) * r / l)),
+        (2, lambda r: 1 / np.sqrt(1 + r * r / (l * l))),
+        (3, lambda r: 1 + r * r / (l * l)),
+        (4, lambda r: np.exp(-r / l)),
+    ]
+    for kt, f in cases:
+        o = oracle_mod.OracleHODLR.from_kernel(pts, kt, l, shift=0.25, leaf=16)
+        for i, j in [(0, 1), (5, 40), (63, 2), (7, 7)]:
+            r = np.linalg.norm(pts[:, i] - pts[:, j])
+            ref = f(r) + (0.25 if i == j else 0.0)
+            assert abs(o.entry(i, j) - ref) <= 4e-16 * max(1.0, abs(ref))
+    o = oracle_mod.OracleHODLR.from_kernel(pts, 3, 1.0, leaf=16, diag_replace=True, diag_value=0.0)
+    assert o.entry(4, 4) == 0.0
+
+
+# ----------------------------------------------------------------- tree
+def py_default_tree(n, leaf):
+    """createDefaultTree (src/HODLR_Tree.cpp:33-132) restated independently."""
+    levels, leaves = {}, []
+    if n < leaf:
+        return levels, [(0, 0, n - 1)]
+
+    def rec(level, mn, mx, split):
+        levels.setdefault(level, []).append((level, mn, split, mx))
+        top, bott = split - mn + 1, mx - split
+        if top > leaf:
+            rec(level + 1, mn, mn + top - 1, mn + top // 2 - 1)
+        else:
+            leaves.append((level + 1, mn, mn + top - 1))
+        if bott > leaf:
+            rec(level + 1, mn + top, mx, mx - bott // 2)
+        else:
+            leaves.append((level + 1, mn + top, mx))
+
+    rec(0, 0, n - 1, n // 2 - 1)
+    return levels, leaves
+
+
+@pytest.mark.parametrize("n,leaf", [(4096, 64), (3001, 64), (1000, 30), (37, 30), (30, 30),
+                                    (29, 30), (262144, 128), (12936, 30)])
+def test_tree_matches_reference_rules(oracle_mod, n, leaf):
+    pts = np.linspace(0, 1, n)[None, :]
+    o = oracle_mod.OracleHODLR.from_kernel(pts, 0, 0.5, leaf=leaf)
+    levels, leaves = py_default_tree(n, leaf)
+    flat = [nd for lv in sorted(levels) for nd in levels[lv]]
+    assert o.inner_nodes() == flat
+    assert o.leaves() == leaves
+
+
+# ------------------------------------------------------------------ ACA
+def py_aca(entry, m, n, tol, min_pivot=0):
+    """partialPivACA_LowRankApprox (src/lowRank.cpp:117-279) restated in plain
+    Python floats (IEEE double, unfused), independent of the C oracle."""
+    ub = min(m, n)
+    W, V, prow, pcol = [], [], [], []
+    chR, chC = [False] * m, [False] * n
+    frob2, eps, cur, k = 0.0, 1.0, 0, 0
+    while eps > tol and k < ub:
+        chR[cur] = True
+        s = [0.0] * n
+        for l in range(k):
+            w = W[l][cur]
+            vl = V[l]
+            for j in range(n):
+                s[j] = s[j] + w * vl[j]
+        rr = [entry(cur, j) - s[j] for j in range(n)]
+        mi, mv = 0, abs(rr[0])
+        for j in range(1, n):
+            if abs(rr[j]) > mv:
+                mv, mi = abs(rr[j]), j
+        if mv <= min_pivot:
+            f = next((i for i in range(m) if not chR[i]), -1)
+            if f == -1:
+                break
+            cur = f
+            continue
+        if not chC[mi]:
+            cc = mi
+        else:
+            cc = next((j for j in range(n) if not chC[j] and abs(rr[j]) > min_pivot), -1)
+            if cc == -1:
+                break
+        chC[cc] = True
+        piv = 1 / rr[cc]
+        s = [0.0] * m
+        for l in range(k):
+            v = V[l][cc]
+            wl = W[l]
+            for i in range(m):
+                s[i] = s[i] + v * wl[i]
+        rc = [entry(i, cc) - s[i] for i in range(m)]
+        mi, mv = 0, abs(rc[0])
+        for i in range(1, m):
+            if abs(rc[i]) > mv:
+                mv, mi = abs(rc[i]), i
+        nr = mi if not chR[mi] else next((i for i in range(m) if not chR[i] and abs(rc[i]) > min_pivot), -1)
+        if nr == -1:
+            break
+        wk = [piv * c for c in rc]
+        W.append(wk)
+        V.append(rr)
+        prow.append(cur)
+        pcol.append(cc)
+
+        def dot(a, b):
+            t = 0.0
+            for x, y in zip(a, b):
+                t = t + x * y
+            return t
+        sum_norm = 0.0
+        for j in range(k):
+            sum_norm += dot(wk, W[j]) * dot(V[j], rr)
+        sw, sv = dot(wk, wk), dot(rr, rr)
+        frob2 += 2 * sum_norm + sw * sv
+        eps = math.sqrt(sw) * math.sqrt(sv) / math.sqrt(frob2)
+        cur = nr
+        k += 1
+    return k, prow, pcol, W, V
+
+
+def test_aca_matches_python_restatement(oracle_mod):
+    pts, _ = c1_points(256, 21)
+    o = oracle_mod.OracleHODLR.from_kernel(pts, 0, 0.1, shift=1.0, leaf=32)
+    o.set_lr(1e-10)
+    o.compress(1)
+    inner = o.inner_nodes()
+    ranks = o.ranks()
+    for b in range(o.num_blocks()):
+        lvl, mn, sp, mx = inner[b // 2]
+        r0, c0, m, n = (mn, sp + 1, sp - mn + 1, mx - sp) if b % 2 == 0 else (sp + 1, mn, mx - sp, sp - mn + 1)
+        k, prow, pcol, W, V = py_aca(lambda i, j: o.entry(r0 + i, c0 + j), m, n, 1e-10)
+        rows, cols = o.pivots(b)
+        assert list(rows) == prow and list(cols) == pcol
+        if k < min(m, n) - 1 and k > 0:
+            assert ranks[b] == k
+            Wo, Vo = o.lowrank(b, m, n)
+            assert np.array_equal(Wo, np.array(W).T) and np.array_equal(Vo, np.array(V).T)
+
+
+# -------------------------------------------------------- reference tests
+def test_reference_random_exact_hodlr(oracle_mod):
+    """test/test.cpp:57-69: exact rank-10 HODLR N=10000 leaf 50, rel. err < 1e-8."""
+    n = 10000
+    A = exact_hodlr(n, 50, 10, seed=0)
+    o = oracle_mod.OracleHODLR.from_dense(A, leaf=50)
+    xe = np.linspace(-2, 2, n)[:, None]
+    x = o.solve(A @ xe)
+    assert np.linalg.norm(x - xe) / np.linalg.norm(xe) < 1e-8
+
+
+def test_reference_inverse_multiquadric(oracle_mod):
+    """test/test.cpp:112-129: dense 1D inverse multiquadric on LinSpaced(-1,1),
+    diagonal 0, N=10000, leaf 30, tol 1e-8, rel. err < 1e-6."""
+    n = 10000
+    x = np.linspace(-1.0, 1.0, n)
+    r = np.abs(x[:, None] - x[None, :])
+    A = 1.0 / np.sqrt(1.0 + r * r)
+    np.fill_diagonal(A, 0.0)
+    o = oracle_mod.OracleHODLR.from_dense(A, leaf=30)
+    o.set_lr(1e-8)
+    xe = np.linspace(-2, 2, n)[:, None]
+    xs = o.solve(A @ xe)
+    assert np.linalg.norm(xs - xe) / np.linalg.norm(xe) < 1e-6
+
+
+def test_reference_quadratic_kernel_path(oracle_mod):
+    """test/test.cpp:565-576 (kernel-functor path): K_ij = (x_i-x_j)^2 + 1,
+    K_ii = 0, x = LinSpaced(-2,2), N=10000, leaf 30, default tol 1e-6.  The
+    reference prints the error without asserting; the oracle must solve it."""
+    n = 10000
+    x = np.linspace(-2.0, 2.0, n)
+    o = oracle_mod.OracleHODLR.from_kernel(x[None, :], 3, 1.0, leaf=30, diag_replace=True,
+                                           diag_value=0.0)
+    K = (x[:, None] - x[None, :]) ** 2 + 1.0
+    np.fill_diagonal(K, 0.0)
+    xs = o.solve(K @ x[:, None])
+    assert np.linalg.norm(xs[:, 0] - x) / np.linalg.norm(x) < 1e-6
+
+
+def test_c1_oracle_vs_dense_lu(oracle_mod):
+    pts, rng = c1_points()
+    o = oracle_mod.OracleHODLR.from_kernel(pts, 0, 0.1, shift=1.0, leaf=64)
+    o.set_lr(1e-10)
+    b = rng.standard_normal((4096, 1))
+    xs = o.solve(b)
+    K = np.exp(-((pts[0][:, None] - pts[0][None, :]) ** 2) / 0.01) + np.eye(4096)
+    xd = np.linalg.solve(K, b)
+    assert np.linalg.norm(xs - xd) / np.linalg.norm(xd) < 1e-9
+
+
+# --------------------------------------------------------------- golden
+def test_golden_c1_pivots_and_ranks(oracle_mod):
+    """The oracle reproduces the committed C1 fixture (pivots, ranks, iters)."""
+    g = np.load(os.path.join(GOLDEN, "c1_aca.npz"))
+    pts, _ = c1_points()
+    o = oracle_mod.OracleHODLR.from_kernel(pts, 0, 0.1, shift=1.0, leaf=64)
+    o.set_lr(1e-10)
+    o.compress()
+    assert np.array_equal(o.ranks(), g["ranks"])
+    assert np.array_equal(o.iters(), g["iters"])
+    rows = np.concatenate([o.pivots(b)[0] for b in range(o.num_blocks())])
+    cols = np.concatenate([o.pivots(b)[1] for b in range(o.num_blocks())])
+    assert np.array_equal(rows, g["prow"]) and np.array_equal(cols, g["pcol"])
+    assert np.array_equal(pts[0], g["points"])
