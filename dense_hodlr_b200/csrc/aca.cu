@@ -459,8 +459,10 @@ __global__ void __launch_bounds__(NT) aca_kernel(AcaLaunch L) {
     }
   }
   if (nonfinite) atomicOr(L.err, DEV_ERR_NONFINITE);
-  // Every CTA of the group reached the same state; CTA 0 records it.  The
-  // other CTAs read the state only at kernel start, before barrier 1.
+  // Every CTA of the group reached the same state; CTA 0 records it after a
+  // last barrier, so that no CTA of the group can still be about to read the
+  // entry state (a block that starts in post-processing has no barrier before).
+  if (status != ACA_ERROR && !group_sync(bar, G, gen, L.err)) status = ACA_ERROR;
   if (g == 0 && tid == 0) {
     st->k = k;
     st->cur = cur;
