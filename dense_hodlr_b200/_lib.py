@@ -42,6 +42,9 @@ SIGNATURES = {
     "hodlr_create_dense": (_I, [ctypes.POINTER(_H), _I, _PD, _I, _I]),
     "hodlr_create_fnptr": (_I, [ctypes.POINTER(_H), _I, _I, _V, _V, _I]),
     "hodlr_destroy": (None, [_H]),
+    "hodlr_reset": (_I, [_H]),
+    "hodlr_set_stream": (_I, [_H, _V]),
+    "hodlr_get_launch_count": (_I, [_H, ctypes.POINTER(ctypes.c_longlong)]),
     "hodlr_set_lr_tolerance": (_I, [_H, _D]),
     "hodlr_set_min_pivot": (_I, [_H, _D]),
     "hodlr_set_lr_method": (_I, [_H, ctypes.c_char_p]),

@@ -121,6 +121,8 @@ struct hodlr_handle_s {
   int blocks_cap = 0;
   unsigned* d_err = nullptr;
   cudaStream_t stream = nullptr;
+  cudaStream_t own_stream = nullptr;
+  long long nlaunch = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   int num_sms = 0;
   bool compressed = false, factored = false;
@@ -390,6 +392,7 @@ int run_aca(hodlr_t h, std::vector<AcaBlock>& blocks, int G, int nt, int kcap_ma
   CK(cudaEventRecord(h->ev0, h->stream));
   int rc = aca_launch(L, nt, kcap_max, G > 1, h->stream);
   if (rc) return cuda_fail(h, (cudaError_t)rc, "aca_launch");
+  h->nlaunch += 1;
   CK(cudaEventRecord(h->ev1, h->stream));
   CK(cudaEventSynchronize(h->ev1));
   float ms = 0;
@@ -586,6 +589,7 @@ int do_factorize(hodlr_t h) {
     L.err = h->d_err;
     int e = leaf_lu_launch(L, nl, h->smax, h->stream);
     if (e) return cuda_fail(h, (cudaError_t)e, "leaf_lu_launch");
+    h->nlaunch += 1;
   }
   // Y = [U panels of every level], zero padded
   if (h->C > 0) {
@@ -613,6 +617,7 @@ int do_factorize(hodlr_t h) {
       dim3 grid(std::min(64, (maxm + 255) / 256), nb, std::min(L.kmax, 64));
       y_init_kernel<<<grid, 256, 0, h->stream>>>(h->Y, N, L.coff, L.W, N, d_r0, d_m, d_rk, nb);
       CK(cudaGetLastError());
+      h->nlaunch += 1;
       CK(cudaStreamSynchronize(h->stream));
       dfree(d_r0);
       dfree(d_m);
@@ -630,6 +635,7 @@ int do_factorize(hodlr_t h) {
     S.ncols = (int)h->C;
     int e = leaf_solve_launch(S, nl, h->smax, h->stream);
     if (e) return cuda_fail(h, (cudaError_t)e, "leaf_solve_launch");
+    h->nlaunch += 1;
   }
   // levels bottom-up
   for (int l = (int)h->lv.size() - 1; l >= 0; --l) {
@@ -698,6 +704,7 @@ int do_factorize(hodlr_t h) {
     int e = gemm_tn_launch(L.tn.probs, L.tn.tiles, L.tn.ntiles, L.tn.nprob, h->ws,
                            L.tn.any_split, h->stream);
     if (e) return cuda_fail(h, (cudaError_t)e, "gemm_tn");
+    h->nlaunch += (L.tn.ntiles > 0) + (L.tn.ntiles > 0 && L.tn.any_split);
     SchurLaunch S;
     S.nodes = L.d_nodes;
     S.S = L.S;
@@ -707,9 +714,11 @@ int do_factorize(hodlr_t h) {
     S.err = h->d_err;
     e = schur_factor_launch(S, nn, h->stream);
     if (e) return cuda_fail(h, (cudaError_t)e, "schur_factor");
+    h->nlaunch += 2;
     if (L.coff > 0) {
       e = schur_solve_launch(S, nn, -1, L.coff, h->stream);
       if (e) return cuda_fail(h, (cudaError_t)e, "schur_solve");
+      h->nlaunch += 1;
       // Y[rows_h, 0:coff] -= Y[rows_h, coff : coff + rank(U_h)] * y_h
       std::vector<GemmProblem> up;
       for (int p = 0; p < nn; ++p) {
@@ -743,6 +752,7 @@ int do_factorize(hodlr_t h) {
       if (rc2) return rc2;
       e = gemm_nn_sub_launch(L.nn.probs, L.nn.tiles, L.nn.ntiles, h->stream);
       if (e) return cuda_fail(h, (cudaError_t)e, "gemm_nn_sub");
+      h->nlaunch += (L.nn.ntiles > 0);
     }
   }
   CK(cudaEventRecord(h->ev1, h->stream));
@@ -858,12 +868,14 @@ int solve_in_place(hodlr_t h, int nrhs) {
   S.ncols = nrhs;
   int e = leaf_solve_launch(S, (int)h->leaf_min.size(), h->smax, h->stream);
   if (e) return cuda_fail(h, (cudaError_t)e, "leaf_solve");
+  h->nlaunch += 1;
   for (int l = (int)h->lv.size() - 1; l >= 0; --l) {
     Level& L = h->lv[l];
     const int nn = (int)L.nmin.size();
     e = gemm_tn_launch(L.stn.probs, L.stn.tiles, L.stn.ntiles, L.stn.nprob, h->ws,
                        L.stn.any_split, h->stream);
     if (e) return cuda_fail(h, (cudaError_t)e, "solve gemm_tn");
+    h->nlaunch += (L.stn.ntiles > 0) + (L.stn.ntiles > 0 && L.stn.any_split);
     SchurLaunch SL;
     SL.nodes = L.d_snodes;
     SL.S = L.S;
@@ -875,6 +887,7 @@ int solve_in_place(hodlr_t h, int nrhs) {
     if (e) return cuda_fail(h, (cudaError_t)e, "solve schur");
     e = gemm_nn_sub_launch(L.snn.probs, L.snn.tiles, L.snn.ntiles, h->stream);
     if (e) return cuda_fail(h, (cudaError_t)e, "solve gemm_nn");
+    h->nlaunch += 1 + (L.snn.ntiles > 0);
   }
   return HODLR_OK;
 }
@@ -911,7 +924,8 @@ int init_common(hodlr_t h) {
   int coop = 0;
   CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
   if (!coop) return fail(h, HODLR_ERR_UNSUPPORTED, "device lacks cooperative launch");
-  CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
+  h->stream = h->own_stream;
   CK(cudaEventCreate(&h->ev0));
   CK(cudaEventCreate(&h->ev1));
   CK(dalloc(&h->d_err, 1));
@@ -1010,8 +1024,28 @@ void hodlr_destroy(hodlr_t h) {
   dfree(h->d_err);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
-  if (h->stream) cudaStreamDestroy(h->stream);
+  if (h->own_stream) cudaStreamDestroy(h->own_stream);
   delete h;
+}
+
+int hodlr_reset(hodlr_t h) {
+  if (!h) return HODLR_ERR_ARG;
+  free_compress(h);
+  h->t_lr = h->t_fact = h->t_solve = 0;
+  return HODLR_OK;
+}
+
+int hodlr_set_stream(hodlr_t h, void* stream) {
+  if (!h) return HODLR_ERR_ARG;
+  CK(cudaStreamSynchronize(h->stream));
+  h->stream = stream ? (cudaStream_t)stream : h->own_stream;
+  return HODLR_OK;
+}
+
+int hodlr_get_launch_count(hodlr_t h, long long* count) {
+  if (!h || !count) return HODLR_ERR_ARG;
+  *count = h->nlaunch;
+  return HODLR_OK;
 }
 
 int hodlr_set_lr_tolerance(hodlr_t h, double tol) {
@@ -1099,6 +1133,7 @@ int hodlr_kernel_matvec_device(hodlr_t h, int nrhs, const double* d_x, int ldx, 
   L.nrhs = nrhs;
   int e = kmatvec_launch(L, sp, h->stream);
   if (e) return cuda_fail(h, (cudaError_t)e, "kmatvec");
+  h->nlaunch += 1 + (sp > 1);
   CK(cudaStreamSynchronize(h->stream));
   return HODLR_OK;
 }

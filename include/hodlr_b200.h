@@ -70,6 +70,14 @@ int hodlr_create_fnptr(hodlr_t* out, int rows, int cols,
 
 void hodlr_destroy(hodlr_t h);
 
+/* reset_attributes() (src/HODLR_Matrix.cpp:1232-1246): discard the
+ * compression and the factorization so the next call recomputes them. */
+int hodlr_reset(hodlr_t h);
+
+/* Run all GPU work of the handle on `stream` (a cudaStream_t); NULL restores
+ * the handle's own stream.  The caller keeps ownership of the stream. */
+int hodlr_set_stream(hodlr_t h, void* stream);
+
 /* set_LRTolerance(double) (:222); default 1e-6.  A changed value discards the
  * compression and the factorization (reset_attributes,
  * src/HODLR_Matrix.cpp:1232-1257). */
@@ -126,6 +134,9 @@ int hodlr_get_block_margin(hodlr_t h, int block, double* margin, int* near);
  * time (seconds) and algorithmic bytes (one read of the W and V panels for
  * the residual and one for the norm update per step, plus the new columns). */
 int hodlr_get_aca_stats(hodlr_t h, int* launches, double* seconds, double* bytes);
+
+/* Number of kernels this handle has launched since it was created. */
+int hodlr_get_launch_count(hodlr_t h, long long* count);
 
 const char* hodlr_status_string(int status);
 const char* hodlr_last_error(hodlr_t h);

@@ -26,6 +26,7 @@
 // reduction orders inside Eigen are not pinned by any reference test.
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -277,7 +278,15 @@ static int choose_next(const std::vector<char>& chosen, const std::vector<double
 
 // partialPivACA_LowRankApprox (src/lowRank.cpp:117-279).  minRank/maxRank
 // are -1 on the default tree (src/HODLR_Tree.cpp:44-47).
-void aca(const Oracle& o, Block& B, double tol, int minRank, int maxRank, int minPivot) {
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// budget_s > 0 stops the loop after that many seconds (cost sampling only;
+// the block is then incomplete).  Returns false when stopped early.
+bool aca(const Oracle& o, Block& B, double tol, int minRank, int maxRank, int minPivot,
+         double budget_s = 0.0) {
+  const double t0 = budget_s > 0 ? now_s() : 0.0;
   const int m = B.m, n = B.n, min_i = B.r0, min_j = B.c0;
   B.prow.clear();
   B.pcol.clear();
@@ -288,7 +297,7 @@ void aca(const Oracle& o, Block& B, double tol, int minRank, int maxRank, int mi
     B.rank = 1;
     B.iters = 0;
     B.eps = 1;
-    return;
+    return true;
   }
   const int ub = std::min(m, n);
   std::vector<std::vector<double>> W, V;  // columns
@@ -301,6 +310,11 @@ void aca(const Oracle& o, Block& B, double tol, int minRank, int maxRank, int mi
     if (g < B.margin) B.margin = g;
   };
   while ((eps > tol || k < minRank) && k < ub) {
+    if (budget_s > 0 && now_s() - t0 > budget_s) {
+      B.iters = iters;
+      B.rank = k;
+      return false;
+    }
     ++iters;
     chosenR[cr] = 1;
     const int gi = cr + min_i;
@@ -373,7 +387,7 @@ void aca(const Oracle& o, Block& B, double tol, int minRank, int maxRank, int mi
     B.W = Mat(m, 1);
     B.V = Mat(n, 1);
     B.rank = 1;
-    return;
+    return true;
   }
   if (k >= ub - 1) {
     if (n <= m) {
@@ -391,7 +405,7 @@ void aca(const Oracle& o, Block& B, double tol, int minRank, int maxRank, int mi
         for (int i = 0; i < m; ++i) B.V(j, i) = o.entry(i + min_i, j + min_j);
       B.rank = m;
     }
-    return;
+    return true;
   }
   B.W = Mat(m, k);
   B.V = Mat(n, k);
@@ -399,6 +413,7 @@ void aca(const Oracle& o, Block& B, double tol, int minRank, int maxRank, int mi
     std::memcpy(&B.W.a[(size_t)l * m], W[l].data(), sizeof(double) * m);
     std::memcpy(&B.V.a[(size_t)l * n], V[l].data(), sizeof(double) * n);
   }
+  return true;
 }
 
 template <class F>
@@ -682,6 +697,74 @@ void orc_kernel_matvec(void* h, int nrhs, const double* X, double* Y, int nthrea
         Y[(size_t)j * n + i] = s;
       }
   });
+}
+
+// ------------------------------------------------------ cost sampling
+// Used only by the CPU-baseline leg of the benchmark: bounded runs of the
+// same operations on the workload's own blocks and sizes.
+
+// ACA of one block for at most budget_s seconds; returns iterations done,
+// *seconds the time taken, *finished whether the block completed.
+int orc_aca_block(void* h, int b, double budget_s, double* seconds, int* finished) {
+  Oracle* o = (Oracle*)h;
+  Block B = o->blocks[b];
+  double t0 = now_s();
+  bool done = aca(*o, B, o->tol, -1, -1, o->minPivot, budget_s);
+  *seconds = now_s() - t0;
+  *finished = done ? 1 : 0;
+  return B.iters;
+}
+
+// The work recLU_Factorize does at one inner node (src/HODLR_Matrix.cpp:
+// 661-687) on random data of the given sizes: V^T X products, S = [[I,.],[.,I]]
+// and its LU, the Schur solve and the two updates; c = columns riding along.
+// With solve_only the recLU_Solve node work (src/HODLR_Matrix.cpp:740-750).
+double orc_bench_node(int st, int sb, int kt, int kb, int c, int solve_only) {
+  const int ct = solve_only ? c : c + kt, cb = solve_only ? c : c + kb;
+  Mat Vt(sb, kt), Vb(st, kb), Xt(st, ct), Xb(sb, cb), tS(st, kt), bS(sb, kb);
+  for (auto* M : {&Vt, &Vb, &Xt, &Xb, &tS, &bS})
+    for (size_t i = 0; i < M->a.size(); ++i) M->a[i] = std::sin(0.37 * (double)i);
+  const int sd = kt + kb;
+  Mat Sm(sd, sd);
+  for (int i = 0; i < sd; ++i) Sm(i, i) = 1.0;
+  for (int j = 0; j < kt; ++j)
+    for (int i = 0; i < kb; ++i) Sm(i, kb + j) = 0.01 * std::sin(0.1 * i + 0.2 * j);
+  LU S;
+  if (solve_only) S.factor(Sm);  // factored once, outside the solve
+  double t0 = now_s();
+  Mat top = matTmul(Vb, Xt), bot = matTmul(Vt, Xb);
+  if (!solve_only) S.factor(Sm);
+  Mat Z(sd, c);
+  for (int j = 0; j < c; ++j) {
+    for (int i = 0; i < kb; ++i) Z(i, j) = top(i, j);
+    for (int i = 0; i < kt; ++i) Z(kb + i, j) = bot(i, j);
+  }
+  Mat y = S.solve(Z);
+  Mat yb(kt, c), yt(kb, c);
+  for (int j = 0; j < c; ++j) {
+    for (int i = 0; i < kt; ++i) yb(i, j) = y(kb + i, j);
+    for (int i = 0; i < kb; ++i) yt(i, j) = y(i, j);
+  }
+  Mat ut = matmul(tS, yb), ub = matmul(bS, yt);
+  double dt = now_s() - t0;
+  volatile double sink = (ut.a.empty() ? 0.0 : ut.a[0]) + (ub.a.empty() ? 0.0 : ub.a[0]);
+  (void)sink;
+  return dt;
+}
+
+// Leaf LU of an s x s block and its solve on c columns.
+double orc_bench_leaf(int s, int c) {
+  Mat A(s, s), B(s, c);
+  for (int j = 0; j < s; ++j)
+    for (int i = 0; i < s; ++i) A(i, j) = (i == j ? s : 0.0) + std::sin(0.1 * i + 0.3 * j);
+  for (size_t i = 0; i < B.a.size(); ++i) B.a[i] = std::cos(0.2 * (double)i);
+  double t0 = now_s();
+  LU L;
+  L.factor(A);
+  Mat X = L.solve(B);
+  volatile double sink = X.a[0];
+  (void)sink;
+  return now_s() - t0;
 }
 
 }  // extern "C"

@@ -57,6 +57,11 @@ def lib():
         L.orc_exp.argtypes = [ctypes.c_double]
         L.orc_exp.restype = ctypes.c_double
         L.orc_kernel_matvec.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp, ctypes.c_int]
+        L.orc_aca_block.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, _dp, _ip]
+        L.orc_bench_node.restype = ctypes.c_double
+        L.orc_bench_node.argtypes = [ctypes.c_int] * 6
+        L.orc_bench_leaf.restype = ctypes.c_double
+        L.orc_bench_leaf.argtypes = [ctypes.c_int] * 2
         _LIB = L
     return _LIB
 
@@ -166,6 +171,14 @@ class OracleHODLR:
         lib().orc_block_lowrank(self.h, b, _ptr(W), _ptr(V))
         return W, V
 
+    def aca_block_sample(self, b, budget_s):
+        """Run the ACA of block b for at most budget_s seconds (cost sampling)."""
+        secs = ctypes.c_double()
+        fin = ctypes.c_int()
+        it = lib().orc_aca_block(self.h, int(b), float(budget_s), ctypes.byref(secs),
+                                 ctypes.byref(fin))
+        return it, secs.value, bool(fin.value)
+
     def entry(self, i, j):
         return lib().orc_entry(self.h, i, j)
 
@@ -177,6 +190,14 @@ class OracleHODLR:
         lib().orc_kernel_matvec(self.h, x.shape[1], _ptr(x), _ptr(y),
                                 int(nthreads or os.cpu_count() or 1))
         return y
+
+
+def bench_node(st, sb, kt, kb, c, solve_only=False):
+    return lib().orc_bench_node(int(st), int(sb), int(kt), int(kb), int(c), int(solve_only))
+
+
+def bench_leaf(s, c):
+    return lib().orc_bench_leaf(int(s), int(c))
 
 
 def hx_exp(x):

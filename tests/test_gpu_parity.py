@@ -180,3 +180,25 @@ def test_errors_are_status_codes():
     assert e.value.status == 4
     with pytest.raises(HODLRError):
         g.recLU_Solve(np.zeros((10, 1)))
+
+
+def test_c2_full_size_ranks_and_pivots_match_fixture():
+    """The FP64-at-scale workload at full size (N=262144, 4094 blocks): every
+    block's rank, iteration count and pivot-sequence hash equals the oracle's
+    (tests/golden/c2_blocks.npz, made by tests/golden/make_golden.py --c2)."""
+    import os
+    from tests.golden.make_golden import pivot_hash
+    d = np.load(os.path.join(os.path.dirname(__file__), "golden", "c2_blocks.npz"))
+    pts = uniform_cube(262144, 2, 2024)
+    assert np.allclose([pts.sum(), (pts * pts).sum()], d["points_sum"], rtol=0, atol=1e-6)
+    g = HODLR_Matrix(262144, 262144, KernelSpec("matern32", 0.2, 1e-2), pts, 128)
+    g.set_LRTolerance(1e-8)
+    g.storeLRinTree()
+    ranks = g.ranks()
+    near = [b for b in range(g.num_blocks()) if g.margin(b)[1] > 0 or d["margin"][b] < 1e-10]
+    assert not near
+    assert np.array_equal(ranks, d["rank"])
+    iters = np.array([g.block_info(b)["iters"] for b in range(g.num_blocks())])
+    assert np.array_equal(iters, d["iters"])
+    hashes = np.array([pivot_hash(*g.pivots(b)) for b in range(g.num_blocks())], dtype=np.int64)
+    assert np.array_equal(hashes, d["pivot_hash"])
