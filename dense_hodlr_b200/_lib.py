@@ -45,6 +45,7 @@ SIGNATURES = {
     "hodlr_reset": (_I, [_H]),
     "hodlr_set_stream": (_I, [_H, _V]),
     "hodlr_get_launch_count": (_I, [_H, ctypes.POINTER(ctypes.c_longlong)]),
+    "hodlr_set_capacity_hint": (_I, [_H, _PI, _I]),
     "hodlr_set_lr_tolerance": (_I, [_H, _D]),
     "hodlr_set_min_pivot": (_I, [_H, _D]),
     "hodlr_set_lr_method": (_I, [_H, ctypes.c_char_p]),
@@ -53,6 +54,8 @@ SIGNATURES = {
     "hodlr_solve": (_I, [_H, _I, _PD, _I, _PD, _I]),
     "hodlr_solve_device": (_I, [_H, _I, _V, _I, _V, _I]),
     "hodlr_kernel_matvec_device": (_I, [_H, _I, _V, _I, _V, _I]),
+    "hodlr_solve_refined_device": (_I, [_H, _I, _V, _I, _V, _I, _D, _I, _PI, _PD]),
+    "hodlr_solve_refined": (_I, [_H, _I, _PD, _I, _PD, _I, _D, _I, _PI, _PD]),
     "hodlr_residual": (_I, [_H, _I, _PD, _I, _PD, _I, _PD]),
     "hodlr_get_times": (_I, [_H, _PD, _PD, _PD, _PD]),
     "hodlr_get_num_levels": (_I, [_H, _PI]),

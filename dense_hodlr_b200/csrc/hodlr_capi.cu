@@ -96,6 +96,7 @@ struct hodlr_handle_s {
   double tol = 1e-6;
   int minPivot = 0;
   std::vector<Level> lv;
+  std::vector<int> cap_hint;  // initial W/V columns per level (0 = default)
   std::vector<int> leaf_min, leaf_size;
   int* d_leaf_min = nullptr;
   int* d_leaf_size = nullptr;
@@ -111,6 +112,11 @@ struct hodlr_handle_s {
   int64_t z_cap = 0;
   double* X = nullptr;  // solve panel N x nrhs
   int x_cols = 0;
+  double* ir_b = nullptr;  // refinement: right-hand sides, iterate, K x, partial norms
+  double* ir_x = nullptr;
+  double* ir_y = nullptr;
+  double* ir_part = nullptr;
+  int ir_cols = 0;
   double* zs = nullptr;  // solve Schur right-hand sides
   int64_t zs_cap = 0;
   double* part = nullptr;
@@ -410,8 +416,10 @@ int do_compress(hodlr_t h) {
   h->aca_seconds = 0;
   h->aca_bytes = 0;
   const int init_cap = 64;
-  for (auto& L : h->lv) {
-    int cap = std::max(1, std::min(L.ub_max, init_cap));
+  for (size_t l = 0; l < h->lv.size(); ++l) {
+    Level& L = h->lv[l];
+    int want = (l < h->cap_hint.size() && h->cap_hint[l] > 0) ? h->cap_hint[l] : init_cap;
+    int cap = std::max(1, std::min(L.ub_max, want));
     int rc = grow_level(h, L, cap);
     if (rc) return rc;
     CK(dalloc(&L.cR, (size_t)N));
@@ -917,6 +925,140 @@ int do_solve_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double* d_x
   return check_dev_err(h, "solve");
 }
 
+constexpr int IR_BLOCKS = 256;
+
+// R = B - Y (stored in Y) and per-block partial sums of |R_c|^2 and |B_c|^2.
+__global__ void ir_residual_kernel(const double* B, double* Y, int64_t n, int nrhs,
+                                   double* part) {
+  __shared__ double red[2][8];
+  for (int c = 0; c < nrhs; ++c) {
+    double rr = 0.0, bb = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+      double b = B[c * n + i];
+      double r = b - Y[c * n + i];
+      Y[c * n + i] = r;
+      rr = fma(r, r, rr);
+      bb = fma(b, b, bb);
+    }
+    rr = warp_sum(rr);
+    bb = warp_sum(bb);
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+      red[0][w] = rr;
+      red[1][w] = bb;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double a = 0.0, d = 0.0;
+      for (int q = 0; q < (int)(blockDim.x >> 5); ++q) {
+        a += red[0][q];
+        d += red[1][q];
+      }
+      part[(int64_t)(2 * c) * gridDim.x + blockIdx.x] = a;
+      part[(int64_t)(2 * c + 1) * gridDim.x + blockIdx.x] = d;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void axpy_cols_kernel(double* X, const double* D, int64_t total) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x)
+    X[e] += D[e];
+}
+
+int kmatvec_dev(hodlr_t h, int nrhs, const double* d_x, int ldx, double* d_y, int ldy) {
+  int sp = kmatvec_splits(h->n, h->num_sms);
+  if (sp > 1) {
+    int rc = ensure_ws(h, (int64_t)sp * nrhs * h->n);
+    if (rc) return rc;
+  }
+  KmatvecLaunch L;
+  L.src = make_src(h);
+  L.X = d_x;
+  L.ldx = ldx;
+  L.Y = d_y;
+  L.ldy = ldy;
+  L.ws = h->ws;
+  L.n = h->n;
+  L.nrhs = nrhs;
+  int e = kmatvec_launch(L, sp, h->stream);
+  if (e) return cuda_fail(h, (cudaError_t)e, "kmatvec");
+  h->nlaunch += 1 + (sp > 1);
+  return HODLR_OK;
+}
+
+
+// Iterative refinement: x0 = M^-1 b, then x += M^-1 (b - K x) until
+// max_c ||b_c - K x_c|| / ||b_c|| <= tol or max_iter corrections.  b and x
+// are device pointers (ld n).  *iters = corrections applied.
+int refine_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double* d_x, int ldx,
+                  double tol, int max_iter, int* iters, double* relres) {
+  const int64_t N = h->n;
+  int rc = build_solve_plans(h, nrhs);
+  if (rc) return rc;
+  if (nrhs > h->ir_cols) {
+    dfree(h->ir_b);
+    dfree(h->ir_x);
+    dfree(h->ir_y);
+    dfree(h->ir_part);
+    CK(dalloc(&h->ir_b, (size_t)(N * nrhs)));
+    CK(dalloc(&h->ir_x, (size_t)(N * nrhs)));
+    CK(dalloc(&h->ir_y, (size_t)(N * nrhs)));
+    CK(dalloc(&h->ir_part, (size_t)(2 * nrhs * IR_BLOCKS)));
+    h->ir_cols = nrhs;
+  }
+  CK(cudaMemcpy2DAsync(h->ir_b, sizeof(double) * N, d_b, sizeof(double) * ldb,
+                       sizeof(double) * N, nrhs, cudaMemcpyDeviceToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->X, h->ir_b, sizeof(double) * N * nrhs, cudaMemcpyDeviceToDevice,
+                     h->stream));
+  rc = solve_in_place(h, nrhs);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(h->ir_x, h->X, sizeof(double) * N * nrhs, cudaMemcpyDeviceToDevice,
+                     h->stream));
+  std::vector<double> part((size_t)2 * nrhs * IR_BLOCKS);
+  double worst = HUGE_VAL;
+  int it = 0;
+  for (;; ++it) {
+    for (int c0 = 0; c0 < nrhs; c0 += 16) {
+      int nc = std::min(16, nrhs - c0);
+      rc = kmatvec_dev(h, nc, h->ir_x + c0 * N, (int)N, h->ir_y + c0 * N, (int)N);
+      if (rc) return rc;
+    }
+    ir_residual_kernel<<<IR_BLOCKS, 256, 0, h->stream>>>(h->ir_b, h->ir_y, N, nrhs, h->ir_part);
+    CK(cudaGetLastError());
+    h->nlaunch += 1;
+    CK(cudaMemcpyAsync(part.data(), h->ir_part, sizeof(double) * part.size(),
+                       cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    worst = 0.0;
+    for (int c = 0; c < nrhs; ++c) {
+      double a = 0.0, d = 0.0;
+      for (int q = 0; q < IR_BLOCKS; ++q) {
+        a += part[(size_t)(2 * c) * IR_BLOCKS + q];
+        d += part[(size_t)(2 * c + 1) * IR_BLOCKS + q];
+      }
+      double r = d > 0 ? std::sqrt(a / d) : std::sqrt(a);
+      if (relres) relres[c] = r;
+      worst = std::max(worst, r);
+    }
+    if (worst <= tol || it >= max_iter) break;
+    CK(cudaMemcpyAsync(h->X, h->ir_y, sizeof(double) * N * nrhs, cudaMemcpyDeviceToDevice,
+                       h->stream));
+    rc = solve_in_place(h, nrhs);
+    if (rc) return rc;
+    axpy_cols_kernel<<<1024, 256, 0, h->stream>>>(h->ir_x, h->X, N * nrhs);
+    CK(cudaGetLastError());
+    h->nlaunch += 1;
+  }
+  if (iters) *iters = it;
+  CK(cudaMemcpy2DAsync(d_x, sizeof(double) * ldx, h->ir_x, sizeof(double) * N,
+                       sizeof(double) * N, nrhs, cudaMemcpyDeviceToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return check_dev_err(h, "refine");
+}
+
 int init_common(hodlr_t h) {
   int dev = 0;
   CK(cudaGetDevice(&dev));
@@ -1018,6 +1160,10 @@ void hodlr_destroy(hodlr_t h) {
   dfree(h->Z);
   dfree(h->X);
   dfree(h->zs);
+  dfree(h->ir_b);
+  dfree(h->ir_x);
+  dfree(h->ir_y);
+  dfree(h->ir_part);
   dfree(h->part);
   dfree(h->bar);
   dfree(h->d_blocks);
@@ -1039,6 +1185,12 @@ int hodlr_set_stream(hodlr_t h, void* stream) {
   if (!h) return HODLR_ERR_ARG;
   CK(cudaStreamSynchronize(h->stream));
   h->stream = stream ? (cudaStream_t)stream : h->own_stream;
+  return HODLR_OK;
+}
+
+int hodlr_set_capacity_hint(hodlr_t h, const int* caps, int nlevels) {
+  if (!h || nlevels < 0 || (nlevels > 0 && !caps)) return HODLR_ERR_ARG;
+  h->cap_hint.assign(caps, caps + nlevels);
   return HODLR_OK;
 }
 
@@ -1117,25 +1269,54 @@ int hodlr_kernel_matvec_device(hodlr_t h, int nrhs, const double* d_x, int ldx, 
                                int ldy) {
   if (!h || nrhs < 1 || nrhs > 16 || !d_x || !d_y || ldx < h->n || ldy < h->n)
     return HODLR_ERR_ARG;
-  int sp = kmatvec_splits(h->n, h->num_sms);
-  if (sp > 1) {
-    int rc = ensure_ws(h, (int64_t)sp * nrhs * h->n);
-    if (rc) return rc;
-  }
-  KmatvecLaunch L;
-  L.src = make_src(h);
-  L.X = d_x;
-  L.ldx = ldx;
-  L.Y = d_y;
-  L.ldy = ldy;
-  L.ws = h->ws;
-  L.n = h->n;
-  L.nrhs = nrhs;
-  int e = kmatvec_launch(L, sp, h->stream);
-  if (e) return cuda_fail(h, (cudaError_t)e, "kmatvec");
-  h->nlaunch += 1 + (sp > 1);
+  int rc = kmatvec_dev(h, nrhs, d_x, ldx, d_y, ldy);
+  if (rc) return rc;
   CK(cudaStreamSynchronize(h->stream));
   return HODLR_OK;
+}
+
+int hodlr_solve_refined_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double* d_x,
+                               int ldx, double tol, int max_iter, int* iters, double* relres) {
+  if (!h || nrhs < 1 || !d_b || !d_x || ldb < h->n || ldx < h->n || !(tol >= 0) || max_iter < 0)
+    return HODLR_ERR_ARG;
+  int rc = hodlr_factorize(h);
+  if (rc) return rc;
+  CK(cudaEventRecord(h->ev0, h->stream));
+  rc = refine_device(h, nrhs, d_b, ldb, d_x, ldx, tol, max_iter, iters, relres);
+  if (rc) return rc;
+  CK(cudaEventRecord(h->ev1, h->stream));
+  CK(cudaEventSynchronize(h->ev1));
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+  h->t_solve = ms * 1e-3;
+  return HODLR_OK;
+}
+
+int hodlr_solve_refined(hodlr_t h, int nrhs, const double* b, int ldb, double* x, int ldx,
+                        double tol, int max_iter, int* iters, double* relres) {
+  if (!h || nrhs < 1 || !b || !x || ldb < h->n || ldx < h->n) return HODLR_ERR_ARG;
+  const int64_t N = h->n;
+  double *db = nullptr, *dx = nullptr;
+  CK(dalloc(&db, (size_t)(N * nrhs)));
+  cudaError_t e = dalloc(&dx, (size_t)(N * nrhs));
+  if (e != cudaSuccess) {
+    dfree(db);
+    return cuda_fail(h, e, "refine alloc");
+  }
+  int rc = HODLR_OK;
+  e = cudaMemcpy2D(db, sizeof(double) * N, b, sizeof(double) * ldb, sizeof(double) * N, nrhs,
+                   cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    rc = hodlr_solve_refined_device(h, nrhs, db, (int)N, dx, (int)N, tol, max_iter, iters,
+                                    relres);
+    if (!rc)
+      e = cudaMemcpy2D(x, sizeof(double) * ldx, dx, sizeof(double) * N, sizeof(double) * N,
+                       nrhs, cudaMemcpyDeviceToHost);
+  }
+  dfree(db);
+  dfree(dx);
+  if (e != cudaSuccess) return cuda_fail(h, e, "refine copy");
+  return rc;
 }
 
 int hodlr_residual(hodlr_t h, int nrhs, const double* b, int ldb, const double* x, int ldx,

@@ -1,0 +1,79 @@
+// Fast FP64 kernel entries for the full-kernel residual r = b - K x.
+//
+// The residual needs FP64-accurate entries (a few ulp), not entries that are
+// bit-identical to the ones ACA used, so it may contract into FMAs and use a
+// cheaper exponential.  exp here follows Tang's table-driven method (P. T. P.
+// Tang, "Table-driven implementation of the exponential function in IEEE
+// floating-point arithmetic", ACM TOMS 15(2), 1989): x = (64k + j) ln2/64 + r,
+// |r| <= ln2/128, e^x = 2^k * 2^(j/64) * e^r with e^r - 1 from its Taylor
+// series to degree 5 (truncation below 4e-17) and 2^(j/64) from a 64-entry
+// table (each entry correctly rounded, computed with exact arithmetic).
+#pragma once
+
+#include "kfun.h"
+
+// 2^(j/64), j = 0..63, correctly rounded.
+#define HX_TANG_TABLE_INIT { \
+    0x1.0000000000000p+0, 0x1.02c9a3e778061p+0, 0x1.059b0d3158574p+0, 0x1.0874518759bc8p+0, \
+    0x1.0b5586cf9890fp+0, 0x1.0e3ec32d3d1a2p+0, 0x1.11301d0125b51p+0, 0x1.1429aaea92de0p+0, \
+    0x1.172b83c7d517bp+0, 0x1.1a35beb6fcb75p+0, 0x1.1d4873168b9aap+0, 0x1.2063b88628cd6p+0, \
+    0x1.2387a6e756238p+0, 0x1.26b4565e27cddp+0, 0x1.29e9df51fdee1p+0, 0x1.2d285a6e4030bp+0, \
+    0x1.306fe0a31b715p+0, 0x1.33c08b26416ffp+0, 0x1.371a7373aa9cbp+0, 0x1.3a7db34e59ff7p+0, \
+    0x1.3dea64c123422p+0, 0x1.4160a21f72e2ap+0, 0x1.44e086061892dp+0, 0x1.486a2b5c13cd0p+0, \
+    0x1.4bfdad5362a27p+0, 0x1.4f9b2769d2ca7p+0, 0x1.5342b569d4f82p+0, 0x1.56f4736b527dap+0, \
+    0x1.5ab07dd485429p+0, 0x1.5e76f15ad2148p+0, 0x1.6247eb03a5585p+0, 0x1.6623882552225p+0, \
+    0x1.6a09e667f3bcdp+0, 0x1.6dfb23c651a2fp+0, 0x1.71f75e8ec5f74p+0, 0x1.75feb564267c9p+0, \
+    0x1.7a11473eb0187p+0, 0x1.7e2f336cf4e62p+0, 0x1.82589994cce13p+0, 0x1.868d99b4492edp+0, \
+    0x1.8ace5422aa0dbp+0, 0x1.8f1ae99157736p+0, 0x1.93737b0cdc5e5p+0, 0x1.97d829fde4e50p+0, \
+    0x1.9c49182a3f090p+0, 0x1.a0c667b5de565p+0, 0x1.a5503b23e255dp+0, 0x1.a9e6b5579fdbfp+0, \
+    0x1.ae89f995ad3adp+0, 0x1.b33a2b84f15fbp+0, 0x1.b7f76f2fb5e47p+0, 0x1.bcc1e904bc1d2p+0, \
+    0x1.c199bdd85529cp+0, 0x1.c67f12e57d14bp+0, 0x1.cb720dcef9069p+0, 0x1.d072d4a07897cp+0, \
+    0x1.d5818dcfba487p+0, 0x1.da9e603db3285p+0, 0x1.dfc97337b9b5fp+0, 0x1.e502ee78b3ff6p+0, \
+    0x1.ea4afa2a490dap+0, 0x1.efa1bee615a27p+0, 0x1.f50765b6e4540p+0, 0x1.fa7c1819e90d8p+0, \
+}
+
+static const double hx_tang_host[64] = HX_TANG_TABLE_INIT;
+
+// e^x with the 2^(j/64) table at `tab` (shared or global memory).
+HX_HD double hx_exp_tang(double x, const double* tab) {
+  const double INV_L = 0x1.71547652b82fep+6;  // 64 / ln2
+  const double L_HI = 0x1.62e42fe000000p-7;   // ln2/64, 29 significant bits
+  const double L_LO = 0x1.f473de6af278fp-36;
+  if (!(x > -745.2)) return x != x ? x : 0.0;
+  if (x > 709.78) return HUGE_VAL;
+  double nd = rint(x * INV_L);
+  int n = (int)nd;
+  double r = fma(-nd, L_LO, fma(-nd, L_HI, x));
+  // e^r - 1 = r + r^2 (1/2 + r (1/6 + r (1/24 + r/120)))
+  double p = fma(r, 0x1.1111111111111p-7, 0x1.5555555555555p-5);
+  p = fma(p, r, 0x1.5555555555555p-3);
+  p = fma(p, r, 0.5);
+  p = fma(p * r, r, r);
+  const int j = n & 63;
+  const int k = (n - j) >> 6;  // floor(n / 64)
+  const double t = tab[j];
+  double v = fma(t, p, t);
+  if (k < -1021) return (v * hx_pow2i(k + 600)) * hx_pow2i(-600);
+  if (k > 1023) return (v * 2.0) * hx_pow2i(k - 1);
+  return v * hx_pow2i(k);
+}
+
+// Kernel value of the squared distance, FP64-accurate (not bit-matched to ACA).
+HX_HD double hx_kernel_r2_fast(const hx_kparams& p, double r2, const double* tab) {
+  switch (p.type) {
+    case HX_KERNEL_GAUSSIAN:
+      return hx_exp_tang(r2 * p.a, tab);
+    case HX_KERNEL_MATERN32: {
+      double s = sqrt(r2) * p.a;
+      return (1.0 + s) * hx_exp_tang(-s, tab);
+    }
+    case HX_KERNEL_INV_MULTIQUADRIC:
+      return 1.0 / sqrt(fma(r2, p.a, 1.0));
+    case HX_KERNEL_QUADRATIC:
+      return fma(r2, p.a, 1.0);
+    case HX_KERNEL_EXPONENTIAL:
+      return hx_exp_tang(-sqrt(r2) * p.a, tab);
+    default:
+      return 0.0;
+  }
+}

@@ -1,39 +1,52 @@
 // Full-kernel product Y = K X in FP64 with every entry generated on the fly.
 // Replaces kernelMatrix::operator* (src/kernel.cpp:27-35), which the
 // reference uses for the residual ||K x - b|| / ||b|| (src/HODLR_Matrix.cpp:
-// 785-787).  Entries come from kfun.h, so they are the exact values ACA saw.
+// 785-787), and supplies the residual of iterative refinement.
 //
-// A CTA owns 128 rows (one per thread, NRHS accumulators in registers) and a
-// range of columns; column coordinates and X rows are staged through shared
-// memory 128 at a time.  Column ranges are split over gridDim.y when the row
-// tiles alone cannot fill the GPU; the partial sums are added in a fixed
-// order by kmatvec_reduce.
+// Compute-bound (FP64 pipe): about 25 FP64 operations per entry (distance,
+// sqrt / Tang exp from kfast.cuh) plus one FMA per right-hand side.  A CTA
+// owns 2 * KT rows (two per thread, sharing every staged column value), NR
+// accumulators per row in registers; column coordinates and X rows are staged
+// through shared memory KT at a time.  Column ranges are split over
+// gridDim.y when the row tiles alone cannot fill the GPU; the partial sums
+// are added in a fixed order by kmatvec_reduce.
 #include "common.cuh"
+#include "kfast.cuh"
 #include "kmatvec.h"
 
 namespace {
 
 constexpr int KT = 128;
+constexpr int RPT = 2;  // rows per thread
+
+__constant__ double c_tang[64] = HX_TANG_TABLE_INIT;
 
 template <int NR>
 __global__ void __launch_bounds__(KT) kmatvec_kernel(KmatvecLaunch L) {
   __shared__ double xs[3][KT];
   __shared__ double vs[NR][KT];
-  const int i = blockIdx.x * KT + threadIdx.x;
+  __shared__ double tab[64];
   const int n = L.n;
   const int nsplit = gridDim.y;
   const int per = ((n + nsplit - 1) / nsplit + KT - 1) / KT * KT;
   const int jb = blockIdx.y * per, je = min(n, jb + per);
-  const bool live = i < n;
   const int dim = L.src.kp.dim;
-  double xi[3] = {0.0, 0.0, 0.0};
-  if (live && !L.src.dense)
+  if (threadIdx.x < 64) tab[threadIdx.x] = c_tang[threadIdx.x];
+  int row[RPT];
+  bool live[RPT];
+  double xi[RPT][3];
+  double acc[RPT][NR];
+#pragma unroll
+  for (int q = 0; q < RPT; ++q) {
+    row[q] = blockIdx.x * (KT * RPT) + q * KT + threadIdx.x;
+    live[q] = row[q] < n;
 #pragma unroll
     for (int d = 0; d < 3; ++d)
-      if (d < dim) xi[d] = L.src.pts[d * L.src.ld + i];
-  double acc[NR];
+      xi[q][d] = (live[q] && !L.src.dense && d < dim) ? L.src.pts[d * L.src.ld + row[q]] : 0.0;
 #pragma unroll
-  for (int c = 0; c < NR; ++c) acc[c] = 0.0;
+    for (int c = 0; c < NR; ++c) acc[q][c] = 0.0;
+  }
+  const hx_kparams kp = L.src.kp;
   for (int j0 = jb; j0 < je; j0 += KT) {
     const int jn = min(KT, je - j0);
     __syncthreads();
@@ -48,39 +61,41 @@ __global__ void __launch_bounds__(KT) kmatvec_kernel(KmatvecLaunch L) {
         vs[c][threadIdx.x] = c < L.nrhs ? L.X[(int64_t)c * L.ldx + j] : 0.0;
     }
     __syncthreads();
-    if (live) {
-      for (int t = 0; t < jn; ++t) {
-        const int j = j0 + t;
+    for (int t = 0; t < jn; ++t) {
+      const int j = j0 + t;
+#pragma unroll
+      for (int q = 0; q < RPT; ++q) {
         double kij;
         if (L.src.dense) {
-          kij = L.src.A[(int64_t)j * L.src.ld + i];
-        } else if (i == j && L.src.kp.diag_replace) {
-          kij = L.src.kp.diag_value;
+          kij = live[q] ? L.src.A[(int64_t)j * L.src.ld + row[q]] : 0.0;
         } else {
           double r2 = 0.0;
 #pragma unroll
           for (int d = 0; d < 3; ++d)
             if (d < dim) {
-              double q = __dsub_rn(xi[d], xs[d][t]);
-              r2 = __dadd_rn(r2, __dmul_rn(q, q));
+              double dd = xi[q][d] - xs[d][t];
+              r2 = fma(dd, dd, r2);
             }
-          kij = hx_kernel_r2(L.src.kp, r2);
-          if (i == j) kij = __dadd_rn(kij, L.src.kp.shift);
+          kij = hx_kernel_r2_fast(kp, r2, tab);
+          if (row[q] == j) kij = kp.diag_replace ? kp.diag_value : kij + kp.shift;
         }
 #pragma unroll
-        for (int c = 0; c < NR; ++c) acc[c] = fma(kij, vs[c][t], acc[c]);
+        for (int c = 0; c < NR; ++c) acc[q][c] = fma(kij, vs[c][t], acc[q][c]);
       }
     }
   }
-  if (live)
+#pragma unroll
+  for (int q = 0; q < RPT; ++q) {
+    if (!live[q]) continue;
 #pragma unroll
     for (int c = 0; c < NR; ++c)
       if (c < L.nrhs) {
         if (nsplit == 1)
-          L.Y[(int64_t)c * L.ldy + i] = acc[c];
+          L.Y[(int64_t)c * L.ldy + row[q]] = acc[q][c];
         else
-          L.ws[((int64_t)blockIdx.y * L.nrhs + c) * n + i] = acc[c];
+          L.ws[((int64_t)blockIdx.y * L.nrhs + c) * n + row[q]] = acc[q][c];
       }
+  }
 }
 
 __global__ void kmatvec_reduce(KmatvecLaunch L, int nsplit) {
@@ -97,16 +112,16 @@ __global__ void kmatvec_reduce(KmatvecLaunch L, int nsplit) {
 }  // namespace
 
 int kmatvec_splits(int n, int num_sms) {
-  int tiles = (n + KT - 1) / KT;
-  int want = 4 * num_sms;
+  int tiles = (n + KT * RPT - 1) / (KT * RPT);
+  int want = 8 * num_sms;
   int sp = (want + tiles - 1) / tiles;
-  int maxsp = (n + 1023) / 1024;
+  int maxsp = (n + 2047) / 2048;
   if (sp > maxsp) sp = maxsp;
   return sp < 1 ? 1 : sp;
 }
 
 int kmatvec_launch(const KmatvecLaunch& L, int nsplit, cudaStream_t s) {
-  dim3 grid((L.n + KT - 1) / KT, nsplit);
+  dim3 grid((L.n + KT * RPT - 1) / (KT * RPT), nsplit);
   if (L.nrhs <= 1)
     kmatvec_kernel<1><<<grid, KT, 0, s>>>(L);
   else if (L.nrhs <= 4)

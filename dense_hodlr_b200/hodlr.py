@@ -153,6 +153,12 @@ class HODLR_Matrix:
     def set_LRMethod(self, method):
         _check(self._h, _L.lib().hodlr_set_lr_method(self._h, method.encode()))
 
+    def set_capacity_hint(self, caps):
+        """Initial low-rank columns per inner level (results do not depend on it)."""
+        a = np.ascontiguousarray(caps, dtype=np.int32)
+        _check(self._h, _L.lib().hodlr_set_capacity_hint(
+            self._h, a.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), len(a)))
+
     # ------------------------------------------------------------- solver
     def storeLRinTree(self):
         _check(self._h, _L.lib().hodlr_compress(self._h))
@@ -178,6 +184,31 @@ class HODLR_Matrix:
             print(f"Total Solve Time                 = {self.get_recLU_TotalTime()} seconds")
             print(f"Residual l2 Relative Error       = {rel.max()}")
         return x
+
+    def solve_refined(self, input_RHS, tol=1e-10, max_iter=20):
+        """recLU_Solve followed by iterative refinement with the full FP64
+        kernel residual; returns (x, corrections, per-column rel. residual)."""
+        b = _as_f64_fortran(input_RHS)
+        if b.shape[0] != self.n:
+            raise HODLRError(_L.ERR_ARG, "right-hand side has the wrong number of rows")
+        x = np.zeros_like(b, order="F")
+        rel = np.zeros(b.shape[1])
+        it = ctypes.c_int()
+        dp = ctypes.POINTER(ctypes.c_double)
+        _check(self._h, _L.lib().hodlr_solve_refined(self._h, b.shape[1], b.ctypes.data_as(dp),
+                                                     self.n, x.ctypes.data_as(dp), self.n,
+                                                     float(tol), int(max_iter), ctypes.byref(it),
+                                                     rel.ctypes.data_as(dp)))
+        return x, it.value, rel
+
+    def solve_refined_device(self, b_ptr, x_ptr, nrhs, tol=1e-10, max_iter=20):
+        rel = np.zeros(nrhs)
+        it = ctypes.c_int()
+        _check(self._h, _L.lib().hodlr_solve_refined_device(
+            self._h, int(nrhs), ctypes.c_void_p(b_ptr), self.n, ctypes.c_void_p(x_ptr), self.n,
+            float(tol), int(max_iter), ctypes.byref(it),
+            rel.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return it.value, rel
 
     def solve_device(self, b_ptr, x_ptr, nrhs, ldb=None, ldx=None):
         """recLU_Solve on device buffers (raw CUDA pointers)."""

@@ -100,6 +100,20 @@ int hodlr_solve(hodlr_t h, int nrhs, const double* b, int ldb, double* x, int ld
 int hodlr_solve_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double* d_x,
                        int ldx);
 
+/* Iterative refinement to a residual target: the direct recLU solve, then
+ * x += recLU_Solve(b - K x) with the full FP64 kernel residual
+ * (kernelMatrix::operator*, src/kernel.cpp:27-35) until
+ * max_c ||b_c - K x_c|| / ||b_c|| <= tol or max_iter corrections.  The
+ * reference offers refinement only for dense input (iterative_Solve,
+ * src/HODLR_Matrix.cpp:1138-1213, GMRES with the HODLR preconditioner);
+ * this is its kernel-matrix form.  *iters = corrections applied; relres[c]
+ * the final relative residual of column c.  Device pointers. */
+int hodlr_solve_refined_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double* d_x,
+                               int ldx, double tol, int max_iter, int* iters, double* relres);
+/* Same with host buffers. */
+int hodlr_solve_refined(hodlr_t h, int nrhs, const double* b, int ldb, double* x, int ldx,
+                        double tol, int max_iter, int* iters, double* relres);
+
 /* kernelMatrix::operator* (src/kernel.cpp:27-35): d_y = K d_x, FP64, entries
  * generated on the fly (device pointers). */
 int hodlr_kernel_matvec_device(hodlr_t h, int nrhs, const double* d_x, int ldx,
@@ -134,6 +148,13 @@ int hodlr_get_block_margin(hodlr_t h, int block, double* margin, int* near);
  * time (seconds) and algorithmic bytes (one read of the W and V panels for
  * the residual and one for the norm update per step, plus the new columns). */
 int hodlr_get_aca_stats(hodlr_t h, int* launches, double* seconds, double* bytes);
+
+/* Initial number of low-rank columns to allocate per inner level (caps[l],
+ * 0 = default).  ACA grows a level that needs more and resumes its blocks
+ * where they stopped, so a hint changes memory traffic, never results.  The
+ * reference grows W and V by doubling inside partialPivACA_LowRankApprox
+ * (src/lowRank.cpp:151-157). */
+int hodlr_set_capacity_hint(hodlr_t h, const int* caps, int nlevels);
 
 /* Number of kernels this handle has launched since it was created. */
 int hodlr_get_launch_count(hodlr_t h, long long* count);

@@ -35,6 +35,7 @@
 #include <vector>
 
 #include "../dense_hodlr_b200/csrc/kfun.h"
+#include "../dense_hodlr_b200/csrc/kfast.cuh"
 
 namespace {
 
@@ -681,6 +682,7 @@ void orc_block_lowrank(void* h, int b, double* W, double* V) {
 double orc_entry(void* h, int i, int j) { return ((Oracle*)h)->entry(i, j); }
 
 double orc_exp(double x) { return hx_exp(x); }
+double orc_exp_tang(double x) { return hx_exp_tang(x, hx_tang_host); }
 
 // Full-kernel product Y = K X (kernelMatrix::operator*, src/kernel.cpp:27-35),
 // summing over k in order for each (i, j); rows spread over threads.

@@ -56,6 +56,8 @@ def lib():
         L.orc_entry.restype = ctypes.c_double
         L.orc_exp.argtypes = [ctypes.c_double]
         L.orc_exp.restype = ctypes.c_double
+        L.orc_exp_tang.argtypes = [ctypes.c_double]
+        L.orc_exp_tang.restype = ctypes.c_double
         L.orc_kernel_matvec.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp, ctypes.c_int]
         L.orc_aca_block.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, _dp, _ip]
         L.orc_bench_node.restype = ctypes.c_double
@@ -202,3 +204,7 @@ def bench_leaf(s, c):
 
 def hx_exp(x):
     return lib().orc_exp(float(x))
+
+
+def hx_exp_tang(x):
+    return lib().orc_exp_tang(float(x))

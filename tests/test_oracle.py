@@ -54,6 +54,19 @@ def test_exp_within_one_ulp(oracle_mod):
     assert oracle_mod.hx_exp(0.0) == 1.0
 
 
+def test_tang_exp_within_two_ulp(oracle_mod):
+    """The table-driven exp of the residual path (kfast.cuh) against libm."""
+    xs = np.concatenate([np.linspace(-745.0, 709.7, 40001),
+                         np.random.default_rng(1).uniform(-40, 2, 20000)])
+    worst = 0.0
+    for x in xs:
+        a, b = oracle_mod.hx_exp_tang(x), math.exp(x)
+        if b >= 2.3e-308:
+            worst = max(worst, abs(a - b) / math.ulp(b))
+    assert worst <= 2.0
+    assert oracle_mod.hx_exp_tang(-800.0) == 0.0
+
+
 def test_kernel_entries_match_formulas(oracle_mod):
     rng = np.random.default_rng(3)
     pts = rng.uniform(0, 1, (3, 64))
