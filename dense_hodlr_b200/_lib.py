@@ -56,6 +56,8 @@ SIGNATURES = {
     "hodlr_kernel_matvec_device": (_I, [_H, _I, _V, _I, _V, _I]),
     "hodlr_solve_refined_device": (_I, [_H, _I, _V, _I, _V, _I, _D, _I, _PI, _PD]),
     "hodlr_solve_refined": (_I, [_H, _I, _PD, _I, _PD, _I, _D, _I, _PI, _PD]),
+    "hodlr_iterative_solve_device": (_I, [_H, _I, _V, _I, _V, _I, _D, _I, _I, _PI, _PD]),
+    "hodlr_iterative_solve": (_I, [_H, _I, _PD, _I, _PD, _I, _D, _I, _I, _PI, _PD]),
     "hodlr_residual": (_I, [_H, _I, _PD, _I, _PD, _I, _PD]),
     "hodlr_get_times": (_I, [_H, _PD, _PD, _PD, _PD]),
     "hodlr_get_num_levels": (_I, [_H, _PI]),

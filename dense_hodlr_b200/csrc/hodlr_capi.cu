@@ -117,6 +117,11 @@ struct hodlr_handle_s {
   double* ir_y = nullptr;
   double* ir_part = nullptr;
   int ir_cols = 0;
+  double* gm_V = nullptr;  // GMRES bases: (m+1) and m panels of N x nrhs
+  double* gm_Z = nullptr;
+  double* gm_h = nullptr;  // small device buffers of coefficients / partials
+  double* gm_part = nullptr;
+  int gm_m = 0, gm_cols = 0;
   double* zs = nullptr;  // solve Schur right-hand sides
   int64_t zs_cap = 0;
   double* part = nullptr;
@@ -1059,6 +1064,279 @@ int refine_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double* d_x, 
   return check_dev_err(h, "refine");
 }
 
+// ------------------------------------------------------------- GMRES
+constexpr int GM_BLOCKS = 256;
+
+// part[(i * nrhs + c) * GM_BLOCKS + blk] = sum over this block's rows of
+// V_i[:, c] . W[:, c] for i < nv (V_i = V + i * n * nrhs).
+__global__ void gm_dots_kernel(const double* V, int nv, const double* W, int64_t n, int nrhs,
+                               double* part) {
+  __shared__ double red[8];
+  const int i = blockIdx.y;
+  const double* Vi = V + (int64_t)i * n * nrhs;
+  for (int c = 0; c < nrhs; ++c) {
+    double a = 0.0;
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n;
+         r += (int64_t)gridDim.x * blockDim.x)
+      a = fma(Vi[c * n + r], W[c * n + r], a);
+    a = warp_sum(a);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = a;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int q = 0; q < (int)(blockDim.x >> 5); ++q) t += red[q];
+      part[((int64_t)i * nrhs + c) * gridDim.x + blockIdx.x] = t;
+    }
+    __syncthreads();
+  }
+}
+
+// out[k] = sum of the GM_BLOCKS partials of k (fixed order).
+__global__ void gm_sum_kernel(const double* part, int count, double* out) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
+    double t = 0.0;
+    for (int q = 0; q < GM_BLOCKS; ++q) t += part[(int64_t)k * GM_BLOCKS + q];
+    out[k] = t;
+  }
+}
+
+// W[:, c] -= sum_{i < nv} coef[i * nrhs + c] * V_i[:, c]
+__global__ void gm_sub_kernel(const double* V, int nv, const double* coef, double* W, int64_t n,
+                              int nrhs) {
+  const int64_t total = n * nrhs;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int c = (int)(e / n);
+    double w = W[e];
+    for (int i = 0; i < nv; ++i) w = fma(-coef[i * nrhs + c], V[(int64_t)i * total + e], w);
+    W[e] = w;
+  }
+}
+
+// Y[:, c] = X[:, c] * scale[c] (scale 0 gives an exact zero column)
+__global__ void gm_scale_kernel(const double* X, const double* scale, double* Y, int64_t n,
+                                int nrhs) {
+  const int64_t total = n * nrhs;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const double sc = scale[e / n];
+    Y[e] = sc == 0.0 ? 0.0 : X[e] * sc;
+  }
+}
+
+// Host-side launch helpers bound to the handle's stream.
+int gm_dots(hodlr_t h, const double* V, int nv, const double* W, int nrhs, std::vector<double>& out) {
+  const int64_t N = h->n;
+  gm_dots_kernel<<<dim3(GM_BLOCKS, nv), 256, 0, h->stream>>>(V, nv, W, N, nrhs, h->gm_part);
+  gm_sum_kernel<<<(nv * nrhs + 255) / 256, 256, 0, h->stream>>>(h->gm_part, nv * nrhs, h->gm_h);
+  CK(cudaGetLastError());
+  h->nlaunch += 2;
+  out.resize((size_t)nv * nrhs);
+  CK(cudaMemcpyAsync(out.data(), h->gm_h, sizeof(double) * nv * nrhs, cudaMemcpyDeviceToHost,
+                     h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return HODLR_OK;
+}
+
+int gm_sub(hodlr_t h, const double* V, int nv, const std::vector<double>& coef, double* W, int nrhs) {
+  const int64_t N = h->n;
+  CK(cudaMemcpyAsync(h->gm_h, coef.data(), sizeof(double) * nv * nrhs, cudaMemcpyHostToDevice,
+                     h->stream));
+  gm_sub_kernel<<<1024, 256, 0, h->stream>>>(V, nv, h->gm_h, W, N, nrhs);
+  CK(cudaGetLastError());
+  h->nlaunch += 1;
+  return HODLR_OK;
+}
+
+int gm_scale(hodlr_t h, const double* X, const std::vector<double>& sc, double* Y, int nrhs) {
+  const int64_t N = h->n;
+  CK(cudaMemcpyAsync(h->gm_h, sc.data(), sizeof(double) * nrhs, cudaMemcpyHostToDevice,
+                     h->stream));
+  gm_scale_kernel<<<1024, 256, 0, h->stream>>>(X, h->gm_h, Y, N, nrhs);
+  CK(cudaGetLastError());
+  h->nlaunch += 1;
+  return HODLR_OK;
+}
+
+// Restarted GMRES(m) on K x = b with the HODLR factor as a right
+// preconditioner (K M^-1 u = b, x = M^-1 u), all columns in lockstep so every
+// iteration costs one full-kernel product and one HODLR solve for all of
+// them.  Starts from the direct solve (the initial guess of iterative_Solve,
+// src/HODLR_Matrix.cpp:1169-1177) and stops when the true relative residual
+// max_c ||b_c - K x_c|| / ||b_c|| <= tol.  Classical Gram-Schmidt with one
+// re-orthogonalisation; Givens rotations as in IML's GMRES
+// (IML/include/gmres.h:83-153).
+int gmres_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double* d_x, int ldx,
+                 double tol, int max_iter, int m, int* iters, double* relres) {
+  const int64_t N = h->n;
+  int rc = build_solve_plans(h, nrhs);
+  if (rc) return rc;
+  if (nrhs > h->ir_cols) {
+    dfree(h->ir_b);
+    dfree(h->ir_x);
+    dfree(h->ir_y);
+    dfree(h->ir_part);
+    CK(dalloc(&h->ir_b, (size_t)(N * nrhs)));
+    CK(dalloc(&h->ir_x, (size_t)(N * nrhs)));
+    CK(dalloc(&h->ir_y, (size_t)(N * nrhs)));
+    CK(dalloc(&h->ir_part, (size_t)(2 * nrhs * IR_BLOCKS)));
+    h->ir_cols = nrhs;
+  }
+  if (m > h->gm_m || nrhs > h->gm_cols) {
+    dfree(h->gm_V);
+    dfree(h->gm_Z);
+    dfree(h->gm_h);
+    dfree(h->gm_part);
+    CK(dalloc(&h->gm_V, (size_t)((m + 1) * N * nrhs)));
+    CK(dalloc(&h->gm_Z, (size_t)(m * N * nrhs)));
+    CK(dalloc(&h->gm_h, (size_t)((m + 2) * nrhs)));
+    CK(dalloc(&h->gm_part, (size_t)((m + 2) * nrhs * GM_BLOCKS)));
+    h->gm_m = m;
+    h->gm_cols = nrhs;
+  }
+  const int64_t P = N * nrhs;
+  CK(cudaMemcpy2DAsync(h->ir_b, sizeof(double) * N, d_b, sizeof(double) * ldb,
+                       sizeof(double) * N, nrhs, cudaMemcpyDeviceToDevice, h->stream));
+  // x0 = M^-1 b
+  CK(cudaMemcpyAsync(h->X, h->ir_b, sizeof(double) * P, cudaMemcpyDeviceToDevice, h->stream));
+  rc = solve_in_place(h, nrhs);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(h->ir_x, h->X, sizeof(double) * P, cudaMemcpyDeviceToDevice, h->stream));
+  std::vector<double> bnorm, tmp, hcol, coef;
+  rc = gm_dots(h, h->ir_b, 1, h->ir_b, nrhs, bnorm);
+  if (rc) return rc;
+  for (auto& v : bnorm) v = v > 0 ? std::sqrt(v) : 1.0;
+  int total_it = 0;
+  std::vector<double> worst_res(nrhs, HUGE_VAL);
+  for (int cycle = 0;; ++cycle) {
+    // r = b - K x  -> ir_y ; beta = ||r||
+    for (int c0 = 0; c0 < nrhs; c0 += 16) {
+      int nc = std::min(16, nrhs - c0);
+      rc = kmatvec_dev(h, nc, h->ir_x + c0 * N, (int)N, h->ir_y + c0 * N, (int)N);
+      if (rc) return rc;
+    }
+    ir_residual_kernel<<<IR_BLOCKS, 256, 0, h->stream>>>(h->ir_b, h->ir_y, N, nrhs, h->ir_part);
+    CK(cudaGetLastError());
+    h->nlaunch += 1;
+    rc = gm_dots(h, h->ir_y, 1, h->ir_y, nrhs, tmp);
+    if (rc) return rc;
+    std::vector<double> beta(nrhs);
+    double worst = 0.0;
+    for (int c = 0; c < nrhs; ++c) {
+      beta[c] = std::sqrt(std::max(tmp[c], 0.0));
+      worst_res[c] = beta[c] / bnorm[c];
+      worst = std::max(worst, worst_res[c]);
+    }
+    if (worst <= tol || total_it >= max_iter) break;
+    // V0 = r / beta
+    std::vector<double> sc(nrhs);
+    for (int c = 0; c < nrhs; ++c) sc[c] = beta[c] > 0 ? 1.0 / beta[c] : 0.0;
+    rc = gm_scale(h, h->ir_y, sc, h->gm_V, nrhs);
+    if (rc) return rc;
+    // per-column Hessenberg (column-major (m+1) x m), rotations, rhs g
+    std::vector<double> H((size_t)(m + 1) * m * nrhs, 0.0), cs((size_t)m * nrhs),
+        sn((size_t)m * nrhs), g((size_t)(m + 1) * nrhs, 0.0);
+    for (int c = 0; c < nrhs; ++c) g[c] = beta[c];
+    std::vector<int> done(nrhs, 0), used(nrhs, 0);
+    for (int c = 0; c < nrhs; ++c)
+      if (worst_res[c] <= tol) done[c] = 1;
+    int j = 0;
+    for (; j < m && total_it < max_iter; ++j, ++total_it) {
+      double* Vj = h->gm_V + (int64_t)j * P;
+      double* Zj = h->gm_Z + (int64_t)j * P;
+      // Z_j = M^-1 V_j ; W = K Z_j
+      CK(cudaMemcpyAsync(h->X, Vj, sizeof(double) * P, cudaMemcpyDeviceToDevice, h->stream));
+      rc = solve_in_place(h, nrhs);
+      if (rc) return rc;
+      CK(cudaMemcpyAsync(Zj, h->X, sizeof(double) * P, cudaMemcpyDeviceToDevice, h->stream));
+      for (int c0 = 0; c0 < nrhs; c0 += 16) {
+        int nc = std::min(16, nrhs - c0);
+        rc = kmatvec_dev(h, nc, Zj + c0 * N, (int)N, h->ir_y + c0 * N, (int)N);
+        if (rc) return rc;
+      }
+      // classical Gram-Schmidt, twice
+      std::vector<double> hsum((size_t)(j + 1) * nrhs, 0.0);
+      for (int pass = 0; pass < 2; ++pass) {
+        rc = gm_dots(h, h->gm_V, j + 1, h->ir_y, nrhs, hcol);
+        if (rc) return rc;
+        for (int c = 0; c < nrhs; ++c)
+          if (done[c])
+            for (int i = 0; i <= j; ++i) hcol[(size_t)i * nrhs + c] = 0.0;
+        rc = gm_sub(h, h->gm_V, j + 1, hcol, h->ir_y, nrhs);
+        if (rc) return rc;
+        for (size_t q = 0; q < hsum.size(); ++q) hsum[q] += hcol[q];
+      }
+      rc = gm_dots(h, h->ir_y, 1, h->ir_y, nrhs, tmp);
+      if (rc) return rc;
+      std::vector<double> inv(nrhs, 0.0);
+      bool all_done = true;
+      for (int c = 0; c < nrhs; ++c) {
+        if (done[c]) continue;
+        double* Hc = &H[(size_t)c * (m + 1) * m];
+        for (int i = 0; i <= j; ++i) Hc[(size_t)j * (m + 1) + i] = hsum[(size_t)i * nrhs + c];
+        double hn = std::sqrt(std::max(tmp[c], 0.0));
+        Hc[(size_t)j * (m + 1) + j + 1] = hn;
+        inv[c] = hn > 0 ? 1.0 / hn : 0.0;
+        // apply previous rotations, then a new one
+        for (int i = 0; i < j; ++i) {
+          double a = Hc[(size_t)j * (m + 1) + i], b2 = Hc[(size_t)j * (m + 1) + i + 1];
+          double ci = cs[(size_t)c * m + i], si = sn[(size_t)c * m + i];
+          Hc[(size_t)j * (m + 1) + i] = ci * a + si * b2;
+          Hc[(size_t)j * (m + 1) + i + 1] = -si * a + ci * b2;
+        }
+        double a = Hc[(size_t)j * (m + 1) + j], b2 = Hc[(size_t)j * (m + 1) + j + 1];
+        double r = std::hypot(a, b2);
+        double ci = r > 0 ? a / r : 1.0, si = r > 0 ? b2 / r : 0.0;
+        cs[(size_t)c * m + j] = ci;
+        sn[(size_t)c * m + j] = si;
+        Hc[(size_t)j * (m + 1) + j] = r;
+        Hc[(size_t)j * (m + 1) + j + 1] = 0.0;
+        double gj = g[(size_t)j * nrhs + c];
+        g[(size_t)j * nrhs + c] = ci * gj;
+        g[(size_t)(j + 1) * nrhs + c] = -si * gj;
+        used[c] = j + 1;
+        // stop this column a little below tol; the true residual decides
+        if (std::fabs(g[(size_t)(j + 1) * nrhs + c]) <= 0.5 * tol * bnorm[c] || hn == 0.0)
+          done[c] = 1;
+        if (!done[c]) all_done = false;
+      }
+      rc = gm_scale(h, h->ir_y, inv, h->gm_V + (int64_t)(j + 1) * P, nrhs);
+      if (rc) return rc;
+      if (all_done) {
+        ++j;
+        ++total_it;
+        break;
+      }
+    }
+    // x += Z y, y from the triangular systems (per column)
+    std::vector<double> ycoef((size_t)m * nrhs, 0.0);
+    int nv = 0;
+    for (int c = 0; c < nrhs; ++c) {
+      const int k = used[c];
+      nv = std::max(nv, k);
+      const double* Hc = &H[(size_t)c * (m + 1) * m];
+      for (int i = k - 1; i >= 0; --i) {
+        double t = g[(size_t)i * nrhs + c];
+        for (int q = i + 1; q < k; ++q) t -= Hc[(size_t)q * (m + 1) + i] * ycoef[(size_t)q * nrhs + c];
+        ycoef[(size_t)i * nrhs + c] = Hc[(size_t)i * (m + 1) + i] != 0 ? t / Hc[(size_t)i * (m + 1) + i] : 0.0;
+      }
+    }
+    if (nv > 0) {
+      for (auto& v : ycoef) v = -v;  // gm_sub subtracts
+      rc = gm_sub(h, h->gm_Z, nv, ycoef, h->ir_x, nrhs);
+      if (rc) return rc;
+    }
+    (void)j;
+  }
+  if (iters) *iters = total_it;
+  if (relres)
+    for (int c = 0; c < nrhs; ++c) relres[c] = worst_res[c];
+  CK(cudaMemcpy2DAsync(d_x, sizeof(double) * ldx, h->ir_x, sizeof(double) * N,
+                       sizeof(double) * N, nrhs, cudaMemcpyDeviceToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return check_dev_err(h, "gmres");
+}
+
 int init_common(hodlr_t h) {
   int dev = 0;
   CK(cudaGetDevice(&dev));
@@ -1164,6 +1442,10 @@ void hodlr_destroy(hodlr_t h) {
   dfree(h->ir_x);
   dfree(h->ir_y);
   dfree(h->ir_part);
+  dfree(h->gm_V);
+  dfree(h->gm_Z);
+  dfree(h->gm_h);
+  dfree(h->gm_part);
   dfree(h->part);
   dfree(h->bar);
   dfree(h->d_blocks);
@@ -1290,6 +1572,52 @@ int hodlr_solve_refined_device(hodlr_t h, int nrhs, const double* d_b, int ldb, 
   CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
   h->t_solve = ms * 1e-3;
   return HODLR_OK;
+}
+
+int hodlr_iterative_solve_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double* d_x,
+                                 int ldx, double tol, int max_iter, int restart, int* iters,
+                                 double* relres) {
+  if (!h || nrhs < 1 || !d_b || !d_x || ldb < h->n || ldx < h->n || !(tol >= 0) ||
+      max_iter < 0 || restart < 1 || restart > 256)
+    return HODLR_ERR_ARG;
+  int rc = hodlr_factorize(h);
+  if (rc) return rc;
+  CK(cudaEventRecord(h->ev0, h->stream));
+  rc = gmres_device(h, nrhs, d_b, ldb, d_x, ldx, tol, max_iter, restart, iters, relres);
+  if (rc) return rc;
+  CK(cudaEventRecord(h->ev1, h->stream));
+  CK(cudaEventSynchronize(h->ev1));
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+  h->t_solve = ms * 1e-3;
+  return HODLR_OK;
+}
+
+int hodlr_iterative_solve(hodlr_t h, int nrhs, const double* b, int ldb, double* x, int ldx,
+                          double tol, int max_iter, int restart, int* iters, double* relres) {
+  if (!h || nrhs < 1 || !b || !x || ldb < h->n || ldx < h->n) return HODLR_ERR_ARG;
+  const int64_t N = h->n;
+  double *db = nullptr, *dx = nullptr;
+  CK(dalloc(&db, (size_t)(N * nrhs)));
+  cudaError_t e = dalloc(&dx, (size_t)(N * nrhs));
+  if (e != cudaSuccess) {
+    dfree(db);
+    return cuda_fail(h, e, "gmres alloc");
+  }
+  int rc = HODLR_OK;
+  e = cudaMemcpy2D(db, sizeof(double) * N, b, sizeof(double) * ldb, sizeof(double) * N, nrhs,
+                   cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    rc = hodlr_iterative_solve_device(h, nrhs, db, (int)N, dx, (int)N, tol, max_iter, restart,
+                                      iters, relres);
+    if (!rc)
+      e = cudaMemcpy2D(x, sizeof(double) * ldx, dx, sizeof(double) * N, sizeof(double) * N,
+                       nrhs, cudaMemcpyDeviceToHost);
+  }
+  dfree(db);
+  dfree(dx);
+  if (e != cudaSuccess) return cuda_fail(h, e, "gmres copy");
+  return rc;
 }
 
 int hodlr_solve_refined(hodlr_t h, int nrhs, const double* b, int ldb, double* x, int ldx,

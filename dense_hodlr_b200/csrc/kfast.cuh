@@ -41,8 +41,18 @@ HX_HD double hx_exp_tang(double x, const double* tab) {
   const double L_LO = 0x1.f473de6af278fp-36;
   if (!(x > -745.2)) return x != x ? x : 0.0;
   if (x > 709.78) return HUGE_VAL;
-  double nd = rint(x * INV_L);
-  int n = (int)nd;
+  // round-to-nearest integer by the 1.5 * 2^52 shifter: the sum's low word
+  // holds n, its difference with the shifter is n as a double
+  const double SHIFTER = 0x1.8p52;
+  double t0 = fma(x, INV_L, SHIFTER);
+  double nd = t0 - SHIFTER;
+#if defined(__CUDA_ARCH__)
+  int n = __double2loint(t0);
+#else
+  uint64_t tb;
+  memcpy(&tb, &t0, sizeof(tb));
+  int n = (int)(uint32_t)(tb & 0xffffffffu);
+#endif
   double r = fma(-nd, L_LO, fma(-nd, L_HI, x));
   // e^r - 1 = r + r^2 (1/2 + r (1/6 + r (1/24 + r/120)))
   double p = fma(r, 0x1.1111111111111p-7, 0x1.5555555555555p-5);

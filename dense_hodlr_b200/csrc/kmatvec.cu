@@ -61,6 +61,7 @@ __global__ void __launch_bounds__(KT) kmatvec_kernel(KmatvecLaunch L) {
         vs[c][threadIdx.x] = c < L.nrhs ? L.X[(int64_t)c * L.ldx + j] : 0.0;
     }
     __syncthreads();
+#pragma unroll 2
     for (int t = 0; t < jn; ++t) {
       const int j = j0 + t;
 #pragma unroll
@@ -69,6 +70,7 @@ __global__ void __launch_bounds__(KT) kmatvec_kernel(KmatvecLaunch L) {
         if (L.src.dense) {
           kij = live[q] ? L.src.A[(int64_t)j * L.src.ld + row[q]] : 0.0;
         } else {
+          // off-diagonal formula everywhere; the diagonal is corrected once below
           double r2 = 0.0;
 #pragma unroll
           for (int d = 0; d < 3; ++d)
@@ -77,16 +79,21 @@ __global__ void __launch_bounds__(KT) kmatvec_kernel(KmatvecLaunch L) {
               r2 = fma(dd, dd, r2);
             }
           kij = hx_kernel_r2_fast(kp, r2, tab);
-          if (row[q] == j) kij = kp.diag_replace ? kp.diag_value : kij + kp.shift;
         }
 #pragma unroll
         for (int c = 0; c < NR; ++c) acc[q][c] = fma(kij, vs[c][t], acc[q][c]);
       }
     }
   }
+  // K_ii = f(0) + shift (or the replaced value); f(0) = 1 for every family
+  const double dcorr = kp.diag_replace ? kp.diag_value - 1.0 : kp.shift;
 #pragma unroll
   for (int q = 0; q < RPT; ++q) {
     if (!live[q]) continue;
+    if (!L.src.dense && row[q] >= jb && row[q] < je)
+#pragma unroll
+      for (int c = 0; c < NR; ++c)
+        if (c < L.nrhs) acc[q][c] = fma(dcorr, L.X[(int64_t)c * L.ldx + row[q]], acc[q][c]);
 #pragma unroll
     for (int c = 0; c < NR; ++c)
       if (c < L.nrhs) {

@@ -201,6 +201,41 @@ class HODLR_Matrix:
                                                      rel.ctypes.data_as(dp)))
         return x, it.value, rel
 
+    def iterative_Solve(self, input_RHS, maxIterations=1000, stop_tolerance=1e-10,
+                        init_LRTolerance=None, input_LR_Method="partialPiv_ACA",
+                        directSolve_Method="recLU", restart=32):
+        """iterative_Solve (include/HODLR_Matrix.hpp:219): HODLR-preconditioned
+        GMRES from the recLU solution, to a true relative residual of
+        stop_tolerance.  Returns the solution like the reference; the iteration
+        count and residuals are kept in self.last_iterations / last_relres."""
+        if init_LRTolerance is not None:
+            self.set_LRTolerance(init_LRTolerance)
+        self.set_LRMethod(input_LR_Method)
+        if directSolve_Method != "recLU":
+            raise HODLRError(_L.ERR_UNSUPPORTED, "only the recLU direct solver is on the GPU path")
+        b = _as_f64_fortran(input_RHS)
+        if b.shape[0] != self.n:
+            raise HODLRError(_L.ERR_ARG, "right-hand side has the wrong number of rows")
+        x = np.zeros_like(b, order="F")
+        rel = np.zeros(b.shape[1])
+        it = ctypes.c_int()
+        dp = ctypes.POINTER(ctypes.c_double)
+        _check(self._h, _L.lib().hodlr_iterative_solve(
+            self._h, b.shape[1], b.ctypes.data_as(dp), self.n, x.ctypes.data_as(dp), self.n,
+            float(stop_tolerance), int(maxIterations), int(restart), ctypes.byref(it),
+            rel.ctypes.data_as(dp)))
+        self.last_iterations, self.last_relres = it.value, rel
+        return x
+
+    def iterative_solve_device(self, b_ptr, x_ptr, nrhs, tol=1e-10, max_iter=1000, restart=32):
+        rel = np.zeros(nrhs)
+        it = ctypes.c_int()
+        _check(self._h, _L.lib().hodlr_iterative_solve_device(
+            self._h, int(nrhs), ctypes.c_void_p(b_ptr), self.n, ctypes.c_void_p(x_ptr), self.n,
+            float(tol), int(max_iter), int(restart), ctypes.byref(it),
+            rel.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return it.value, rel
+
     def solve_refined_device(self, b_ptr, x_ptr, nrhs, tol=1e-10, max_iter=20):
         rel = np.zeros(nrhs)
         it = ctypes.c_int()

@@ -114,6 +114,21 @@ int hodlr_solve_refined_device(hodlr_t h, int nrhs, const double* d_b, int ldb, 
 int hodlr_solve_refined(hodlr_t h, int nrhs, const double* b, int ldb, double* x, int ldx,
                         double tol, int max_iter, int* iters, double* relres);
 
+/* iterative_Solve(rhs, maxIterations, stop_tolerance, ...) (:219,
+ * src/HODLR_Matrix.cpp:1138-1213): GMRES(restart) preconditioned by the HODLR
+ * factor, starting from the recLU solution.  The reference runs IML GMRES
+ * with left preconditioning on dense input only; here the preconditioner is
+ * applied on the right so that the stopping test is the true relative
+ * residual max_c ||b_c - K x_c|| / ||b_c|| <= tol, the full-kernel product
+ * is FP64 with entries generated on the fly, and all right-hand sides
+ * iterate together.  *iters = GMRES iterations (full-kernel products after
+ * the first residual).  Device pointers; the second form takes host buffers. */
+int hodlr_iterative_solve_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double* d_x,
+                                 int ldx, double tol, int max_iter, int restart, int* iters,
+                                 double* relres);
+int hodlr_iterative_solve(hodlr_t h, int nrhs, const double* b, int ldb, double* x, int ldx,
+                          double tol, int max_iter, int restart, int* iters, double* relres);
+
 /* kernelMatrix::operator* (src/kernel.cpp:27-35): d_y = K d_x, FP64, entries
  * generated on the fly (device pointers). */
 int hodlr_kernel_matvec_device(hodlr_t h, int nrhs, const double* d_x, int ldx,

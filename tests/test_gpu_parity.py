@@ -202,3 +202,23 @@ def test_c2_full_size_ranks_and_pivots_match_fixture():
     assert np.array_equal(iters, d["iters"])
     hashes = np.array([pivot_hash(*g.pivots(b)) for b in range(g.num_blocks())], dtype=np.int64)
     assert np.array_equal(hashes, d["pivot_hash"])
+
+
+def test_refinement_and_gmres_reach_residual_target():
+    """2D Matern with a small diagonal shift: the direct solve at tol 1e-8 is far
+    from 1e-10; refinement and HODLR-preconditioned GMRES both reach it with the
+    full FP64 kernel residual, GMRES in fewer full-kernel products."""
+    pts = uniform_cube(8192, 2, 31)
+    g = HODLR_Matrix(8192, 8192, KernelSpec("matern32", 0.2, 1e-2), pts, 128)
+    g.set_LRTolerance(1e-8)
+    b = np.random.default_rng(8).standard_normal((8192, 4))
+    x0 = g.recLU_Solve(b)
+    assert g.residual(x0, b).max() > 1e-8
+    x1, it1, rel1 = g.solve_refined(b, tol=1e-10, max_iter=60)
+    assert rel1.max() <= 1e-10 and g.residual(x1, b).max() <= 1.5e-10
+    x2 = g.iterative_Solve(b, 200, 1e-10)
+    assert g.last_relres.max() <= 1e-10
+    assert g.residual(x2, b).max() <= 1.5e-10
+    assert g.last_iterations <= it1
+    # same solution of the same system
+    assert np.linalg.norm(x1 - x2) / np.linalg.norm(x2) < 1e-7
