@@ -451,6 +451,25 @@ def run_profile_case(case):
         g.storeLRinTree()
         print(json.dumps({"case": case, "aca": g.aca_stats(), "lr_s": g.get_LR_ComputationTime(),
                           "max_rank": int(g.ranks().max())}))
+    elif case == "kmatvec-profile":
+        # N=65536 2D Matern-3/2, 8 right-hand sides: one full-kernel product
+        import torch
+        n = 65536
+        pts = uniform_cube(n, 2, SEED)
+        g = HODLR_Matrix(n, n, KernelSpec("matern32", LSCALE, SHIFT), pts, LEAF)
+        x = torch.randn(NRHS, n, dtype=torch.float64, device="cuda")
+        y = torch.empty_like(x)
+        for _ in range(3):
+            g.kernel_matvec_device(x.data_ptr(), y.data_ptr(), NRHS)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        g.kernel_matvec_device(x.data_ptr(), y.data_ptr(), NRHS)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        print(json.dumps({"case": case, "ms": ms, "entries_per_s": n * n / (ms / 1e3)}))
     else:
         raise SystemExit(f"unknown case {case}")
 

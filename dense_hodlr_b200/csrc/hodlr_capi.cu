@@ -725,11 +725,11 @@ int do_factorize(hodlr_t h) {
     S.R = h->Z;
     S.piv = L.piv;
     S.err = h->d_err;
-    e = schur_factor_launch(S, nn, h->stream);
+    e = schur_factor_launch(S, nn, L.max_sd, h->stream);
     if (e) return cuda_fail(h, (cudaError_t)e, "schur_factor");
     h->nlaunch += 2;
     if (L.coff > 0) {
-      e = schur_solve_launch(S, nn, -1, L.coff, h->stream);
+      e = schur_solve_launch(S, nn, -1, L.coff, L.max_sd, h->stream);
       if (e) return cuda_fail(h, (cudaError_t)e, "schur_solve");
       h->nlaunch += 1;
       // Y[rows_h, 0:coff] -= Y[rows_h, coff : coff + rank(U_h)] * y_h
@@ -896,7 +896,7 @@ int solve_in_place(hodlr_t h, int nrhs) {
     SL.R = h->zs;
     SL.piv = L.piv;
     SL.err = h->d_err;
-    e = schur_solve_launch(SL, nn, nrhs, nrhs, h->stream);
+    e = schur_solve_launch(SL, nn, nrhs, nrhs, L.max_sd, h->stream);
     if (e) return cuda_fail(h, (cudaError_t)e, "solve schur");
     e = gemm_nn_sub_launch(L.snn.probs, L.snn.tiles, L.snn.ntiles, h->stream);
     if (e) return cuda_fail(h, (cudaError_t)e, "solve gemm_nn");

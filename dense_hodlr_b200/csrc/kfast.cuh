@@ -68,21 +68,55 @@ HX_HD double hx_exp_tang(double x, const double* tab) {
   return v * hx_pow2i(k);
 }
 
+// e^x for x <= 0 without branches: x is clamped at -746 (e^x underflows to 0
+// there anyway) and 2^k is applied as two factors so that every scale factor
+// stays a normal number down to the subnormal range.
+HX_HD double hx_exp_tang_neg(double x, const double* tab) {
+  const double INV_L = 0x1.71547652b82fep+6;
+  const double L_HI = 0x1.62e42fe000000p-7;
+  const double L_LO = 0x1.f473de6af278fp-36;
+  const double SHIFTER = 0x1.8p52;
+  x = fmax(x, -746.0);
+  double t0 = fma(x, INV_L, SHIFTER);
+  double nd = t0 - SHIFTER;
+#if defined(__CUDA_ARCH__)
+  int n = __double2loint(t0);
+#else
+  uint64_t tb;
+  memcpy(&tb, &t0, sizeof(tb));
+  int n = (int)(uint32_t)(tb & 0xffffffffu);
+#endif
+  double r = fma(-nd, L_LO, fma(-nd, L_HI, x));
+  double p = fma(r, 0x1.1111111111111p-7, 0x1.5555555555555p-5);
+  p = fma(p, r, 0x1.5555555555555p-3);
+  p = fma(p, r, 0.5);
+  p = fma(p * r, r, r);
+  const int j = n & 63;
+  const int k = (n - j) >> 6;
+  const int k1 = k >> 1;
+  const double t = tab[j];
+  return (fma(t, p, t) * hx_pow2i(k1)) * hx_pow2i(k - k1);
+}
+
 // Kernel value of the squared distance, FP64-accurate (not bit-matched to ACA).
 HX_HD double hx_kernel_r2_fast(const hx_kparams& p, double r2, const double* tab) {
   switch (p.type) {
     case HX_KERNEL_GAUSSIAN:
-      return hx_exp_tang(r2 * p.a, tab);
+      return hx_exp_tang_neg(r2 * p.a, tab);
     case HX_KERNEL_MATERN32: {
+#if defined(__CUDA_ARCH__)
+      double s = r2 * rsqrt(fmax(r2, 1e-300)) * p.a;
+#else
       double s = sqrt(r2) * p.a;
-      return (1.0 + s) * hx_exp_tang(-s, tab);
+#endif
+      return (1.0 + s) * hx_exp_tang_neg(-s, tab);
     }
     case HX_KERNEL_INV_MULTIQUADRIC:
       return 1.0 / sqrt(fma(r2, p.a, 1.0));
     case HX_KERNEL_QUADRATIC:
       return fma(r2, p.a, 1.0);
     case HX_KERNEL_EXPONENTIAL:
-      return hx_exp_tang(-sqrt(r2) * p.a, tab);
+      return hx_exp_tang_neg(-sqrt(r2) * p.a, tab);
     default:
       return 0.0;
   }

@@ -5,7 +5,7 @@
 //
 // Compute-bound (FP64 pipe): about 25 FP64 operations per entry (distance,
 // sqrt / Tang exp from kfast.cuh) plus one FMA per right-hand side.  A CTA
-// owns 2 * KT rows (two per thread, sharing every staged column value), NR
+// owns RPT * KT rows (RPT per thread, sharing every staged column value), NR
 // accumulators per row in registers; column coordinates and X rows are staged
 // through shared memory KT at a time.  Column ranges are split over
 // gridDim.y when the row tiles alone cannot fill the GPU; the partial sums
@@ -17,7 +17,7 @@
 namespace {
 
 constexpr int KT = 128;
-constexpr int RPT = 2;  // rows per thread
+constexpr int RPT = 4;  // rows per thread
 
 __constant__ double c_tang[64] = HX_TANG_TABLE_INIT;
 

@@ -10,8 +10,9 @@
 //                     (src/HODLR_Matrix.cpp:626,703).
 //  schur_form_kernel  builds S = [[I, V_b^T K_t^-1 U_t], [V_t^T K_b^-1 U_b, I]]
 //                     (src/HODLR_Matrix.cpp:663-673) from the level product Z.
-//  dense_lu_kernel    factors each node's S in place (src/HODLR_Matrix.cpp:675).
-//  dense_lu_solve_kernel  y = S^-1 rhs (src/HODLR_Matrix.cpp:682,746).
+//  schur_lu_kernel    blocked partial-pivot LU of each node's S in place
+//                     (SchurLU = PartialPivLU(S), src/HODLR_Matrix.cpp:675).
+//  schur_solve_kernel y = S^-1 rhs by the stored LU (src/HODLR_Matrix.cpp:682,746).
 // Pivoting takes the first maximum |a| of the column, as PartialPivLU does.
 #include "common.cuh"
 #include "lu.h"
@@ -23,8 +24,6 @@ constexpr int LNT = 256;
 // ------------------------------------------------------------- leaf LU
 __global__ void __launch_bounds__(LNT) leaf_lu_kernel(LeafLULaunch L) {
   extern __shared__ double a[];  // s x s, leading dimension s | 1
-  __shared__ double red_v[LNT / 32];
-  __shared__ int red_i[LNT / 32];
   __shared__ int s_piv;
   const int leaf = blockIdx.x;
   const int r0 = L.leaf_min[leaf], s = L.leaf_size[leaf];
@@ -97,6 +96,70 @@ __global__ void __launch_bounds__(LNT) leaf_lu_kernel(LeafLULaunch L) {
   }
 }
 
+// ------------------------------------------------ blocked tile solves
+// x <- U^-1 L^-1 x for `ncol` columns of a tile in shared memory (x[c*ldx+i]),
+// where the unit-lower L and the upper U are read through `A(i, j)` (the
+// packed LU of an n x n matrix).  Diagonal blocks of BS rows are solved by one
+// thread per column; the rows below / above are updated by all threads.
+constexpr int BS = 16;
+
+struct SmemLU {
+  const double* a;
+  int lda;
+  __device__ double operator()(int i, int j) const { return a[j * lda + i]; }
+};
+struct GlobalLU {
+  const double* a;
+  int n;
+  __device__ double operator()(int i, int j) const { return __ldg(a + (int64_t)j * n + i); }
+};
+
+template <class LU>
+__device__ void lu_solve_tile(const LU& A, int n, double* x, int ldx, int ncol) {
+  const int tid = threadIdx.x, NT = blockDim.x;
+  for (int b0 = 0; b0 < n; b0 += BS) {  // forward, unit lower
+    const int be = min(n, b0 + BS);
+    for (int c = tid; c < ncol; c += NT) {
+      double* xc = x + c * ldx;
+      for (int i = b0 + 1; i < be; ++i) {
+        double t = xc[i];
+        for (int p = b0; p < i; ++p) t = fma(-A(i, p), xc[p], t);
+        xc[i] = t;
+      }
+    }
+    __syncthreads();
+    const int rem = n - be;
+    for (int e = tid; e < rem * ncol; e += NT) {
+      const int r = be + e % rem, c = e / rem;
+      double* xc = x + c * ldx;
+      double t = xc[r];
+      for (int p = b0; p < be; ++p) t = fma(-A(r, p), xc[p], t);
+      xc[r] = t;
+    }
+    __syncthreads();
+  }
+  for (int be = n; be > 0; be -= BS) {  // backward, upper
+    const int b0 = max(0, be - BS);
+    for (int c = tid; c < ncol; c += NT) {
+      double* xc = x + c * ldx;
+      for (int i = be - 1; i >= b0; --i) {
+        double t = xc[i];
+        for (int p = i + 1; p < be; ++p) t = fma(-A(i, p), xc[p], t);
+        xc[i] = t / A(i, i);
+      }
+    }
+    __syncthreads();
+    for (int e = tid; e < b0 * ncol; e += NT) {
+      const int r = e % b0, c = e / b0;
+      double* xc = x + c * ldx;
+      double t = xc[r];
+      for (int p = b0; p < be; ++p) t = fma(-A(r, p), xc[p], t);
+      xc[r] = t;
+    }
+    __syncthreads();
+  }
+}
+
 // ---------------------------------------------------------- leaf solve
 // X[leaf rows, c0 : c0+TC] <- U^-1 L^-1 P X.  One CTA per (leaf, column tile).
 template <int TC>
@@ -123,28 +186,7 @@ __global__ void __launch_bounds__(LNT) leaf_solve_kernel(LeafSolveLaunch L) {
     x[c * ldx + i] = L.X[(int64_t)(c0 + c) * L.ldx + r0 + perm[i]];
   }
   __syncthreads();
-  // thread layout: column c = tid % TC, row group rg = tid / TC
-  constexpr int RG = LNT / TC;
-  const int c = tid % TC, rg = tid / TC;
-  const bool active = c < ncol;
-  // forward: unit lower
-  for (int p = 0; p < s - 1; ++p) {
-    if (active) {
-      const double xp = x[c * ldx + p];
-      for (int i = p + 1 + rg; i < s; i += RG) x[c * ldx + i] = fma(-lu[p * lda + i], xp, x[c * ldx + i]);
-    }
-    __syncthreads();
-  }
-  // backward: upper
-  for (int p = s - 1; p >= 0; --p) {
-    if (active && rg == 0) x[c * ldx + p] = x[c * ldx + p] / lu[p * lda + p];
-    __syncthreads();
-    if (active) {
-      const double xp = x[c * ldx + p];
-      for (int i = rg; i < p; i += RG) x[c * ldx + i] = fma(-lu[p * lda + i], xp, x[c * ldx + i]);
-    }
-    __syncthreads();
-  }
+  lu_solve_tile(SmemLU{lu, lda}, s, x, ldx, ncol);
   for (int e = tid; e < s * ncol; e += LNT) {
     int i = e % s, cc = e / s;
     L.X[(int64_t)(c0 + cc) * L.ldx + r0 + i] = x[cc * ldx + i];
@@ -176,100 +218,184 @@ __global__ void schur_form_kernel(SchurLaunch L) {
 }
 
 // ------------------------------------------------------ dense batched LU
-// Right-looking LU of S in global memory (it stays in L2 for these sizes).
-__global__ void __launch_bounds__(LNT) dense_lu_kernel(SchurLaunch L) {
-  __shared__ int s_piv;
+// Blocked right-looking LU with row partial pivoting of each node's S, one CTA
+// per node, S in global memory (L2 resident).  Panels of PNB columns are
+// factored in shared memory; the trailing matrix is updated with 4x4 register
+// tiles.  The row interchanges of a panel are applied to the whole row, so the
+// packed result and `piv` are those of an unblocked partial-pivot LU with the
+// same pivot choices (LAPACK getrf convention).
+constexpr int SNT = 512;
+
+__global__ void __launch_bounds__(SNT) schur_lu_kernel(SchurLaunch L, int pnb) {
+  extern __shared__ double pan[];  // rows x pnb panel, leading dimension rows
+  __shared__ double red_v[SNT / 32];
+  __shared__ int red_i[SNT / 32];
+  __shared__ int lpiv[64];
   const int node = blockIdx.x;
   const SchurNode N = L.nodes[node];
   const int n = N.kb + N.kt;
   double* a = L.S + N.s_off;
   int* piv = L.piv + N.p_off;
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
   bool singular = false;
-  for (int p = 0; p < n; ++p) {
-    if (tid < 32) {
+  for (int j0 = 0; j0 < n; j0 += pnb) {
+    const int nb = min(pnb, n - j0), rows = n - j0;
+    for (int e = tid; e < rows * nb; e += SNT) {
+      int r = e % rows, c = e / rows;
+      pan[c * rows + r] = a[(int64_t)(j0 + c) * n + j0 + r];
+    }
+    __syncthreads();
+    for (int c = 0; c < nb; ++c) {
+      // pivot: first maximum |.| of panel column c, rows c..rows-1
       double bv = -1.0;
       int bi = INT_MAX;
-      for (int i = p + tid; i < n; i += 32) {
-        double v = fabs(a[(int64_t)p * n + i]);
+      for (int r = c + tid; r < rows; r += SNT) {
+        double v = fabs(pan[c * rows + r]);
         if (v > bv) {
           bv = v;
-          bi = i;
+          bi = r;
         }
       }
       warp_argmax(bv, bi);
-      if (tid == 0) {
-        s_piv = (bi == INT_MAX) ? p : bi;
-        piv[p] = s_piv;
+      if (lane == 0) {
+        red_v[w] = bv;
+        red_i[w] = bi;
+      }
+      __syncthreads();
+      if (w == 0) {
+        bv = lane < SNT / 32 ? red_v[lane] : -1.0;
+        bi = lane < SNT / 32 ? red_i[lane] : INT_MAX;
+        warp_argmax(bv, bi);
+        if (lane == 0) lpiv[c] = (bi == INT_MAX) ? c : bi;
+      }
+      __syncthreads();
+      const int q = lpiv[c];
+      if (q != c)
+        for (int cc = tid; cc < nb; cc += SNT) {
+          double t = pan[cc * rows + c];
+          pan[cc * rows + c] = pan[cc * rows + q];
+          pan[cc * rows + q] = t;
+        }
+      __syncthreads();
+      const double d = pan[c * rows + c];
+      if (d == 0.0) {
+        singular = true;
+        continue;
+      }
+      for (int r = c + 1 + tid; r < rows; r += SNT) pan[c * rows + r] /= d;
+      __syncthreads();
+      const int rr = rows - c - 1, cols = nb - c - 1;
+      for (int e = tid; e < rr * cols; e += SNT) {
+        int r = c + 1 + e % rr, cc = c + 1 + e / rr;
+        pan[cc * rows + r] = fma(-pan[c * rows + r], pan[cc * rows + c], pan[cc * rows + r]);
+      }
+      __syncthreads();
+    }
+    // panel back to global, pivots, interchanges outside the panel
+    for (int e = tid; e < rows * nb; e += SNT) {
+      int r = e % rows, c = e / rows;
+      a[(int64_t)(j0 + c) * n + j0 + r] = pan[c * rows + r];
+    }
+    if (tid < nb) piv[j0 + tid] = j0 + lpiv[tid];
+    for (int col = tid; col < n; col += SNT) {
+      if (col >= j0 && col < j0 + nb) continue;
+      double* ac = a + (int64_t)col * n;
+      for (int c = 0; c < nb; ++c) {
+        const int q = lpiv[c];
+        if (q != c) {
+          double t = ac[j0 + c];
+          ac[j0 + c] = ac[j0 + q];
+          ac[j0 + q] = t;
+        }
       }
     }
     __syncthreads();
-    const int q = s_piv;
-    if (q != p)
-      for (int j = tid; j < n; j += LNT) {
-        double t = a[(int64_t)j * n + p];
-        a[(int64_t)j * n + p] = a[(int64_t)j * n + q];
-        a[(int64_t)j * n + q] = t;
+    const int rest = n - j0 - nb;
+    if (rest > 0) {
+      // U12 = L11^-1 A12, one thread per column
+      for (int col = j0 + nb + tid; col < n; col += SNT) {
+        double* ac = a + (int64_t)col * n + j0;
+        for (int i = 1; i < nb; ++i) {
+          double t = ac[i];
+          for (int p = 0; p < i; ++p) t = fma(-pan[p * rows + i], ac[p], t);
+          ac[i] = t;
+        }
       }
-    __syncthreads();
-    const double d = a[(int64_t)p * n + p];
-    if (d == 0.0) {
-      singular = true;
-      continue;
+      __syncthreads();
+      // A22 -= L21 U12 with 4x4 register tiles
+      const int tr = (rest + 3) / 4;
+      for (int tt = tid; tt < tr * tr; tt += SNT) {
+        const int ti = (tt % tr) * 4, tj = (tt / tr) * 4;
+        double acc[4][4];
+#pragma unroll
+        for (int x = 0; x < 4; ++x)
+#pragma unroll
+          for (int y = 0; y < 4; ++y) acc[x][y] = 0.0;
+        for (int p = 0; p < nb; ++p) {
+          double l[4], u[4];
+#pragma unroll
+          for (int x = 0; x < 4; ++x) l[x] = (ti + x < rest) ? pan[p * rows + nb + ti + x] : 0.0;
+#pragma unroll
+          for (int y = 0; y < 4; ++y)
+            u[y] = (tj + y < rest) ? a[(int64_t)(j0 + nb + tj + y) * n + j0 + p] : 0.0;
+#pragma unroll
+          for (int x = 0; x < 4; ++x)
+#pragma unroll
+            for (int y = 0; y < 4; ++y) acc[x][y] = fma(l[x], u[y], acc[x][y]);
+        }
+#pragma unroll
+        for (int y = 0; y < 4; ++y) {
+          if (tj + y >= rest) continue;
+          double* ac = a + (int64_t)(j0 + nb + tj + y) * n + j0 + nb + ti;
+#pragma unroll
+          for (int x = 0; x < 4; ++x)
+            if (ti + x < rest) ac[x] -= acc[x][y];
+        }
+      }
+      __syncthreads();
     }
-    for (int i = p + 1 + tid; i < n; i += LNT) a[(int64_t)p * n + i] /= d;
-    __syncthreads();
-    const int rem = n - p - 1;
-    // column-by-column trailing update: warp w updates columns w, w+8, ...
-    const int w = tid >> 5, lane = tid & 31;
-    for (int jj = w; jj < rem; jj += LNT / 32) {
-      const int j = p + 1 + jj;
-      const double u = a[(int64_t)j * n + p];
-      if (u != 0.0)
-        for (int i = p + 1 + lane; i < n; i += 32)
-          a[(int64_t)j * n + i] = fma(-a[(int64_t)p * n + i], u, a[(int64_t)j * n + i]);
-    }
-    __syncthreads();
   }
   if (tid == 0 && singular) atomicOr(L.err, DEV_ERR_SINGULAR);
 }
 
-// y = S^-1 rhs for `ncols` right-hand sides stored in R (ld sd) at r_off;
-// one CTA per (node, column chunk), a warp per column.
-__global__ void __launch_bounds__(LNT) dense_lu_solve_kernel(SchurLaunch L, int ncols) {
+// y = S^-1 rhs for `ncols` right-hand sides stored in R (ld sd) at r_off
+// (ncols < 0: N.coff columns); one CTA per (node, tile of STC columns).
+constexpr int STC = 16;
+
+__global__ void __launch_bounds__(256) schur_solve_kernel(SchurLaunch L, int ncols) {
+  extern __shared__ double xs[];
   const int node = blockIdx.y;
   const SchurNode N = L.nodes[node];
   const int n = N.kb + N.kt;
+  const int cols = ncols < 0 ? N.coff : ncols;
+  const int c0 = blockIdx.x * STC;
+  if (c0 >= cols) return;
+  const int nc = min(STC, cols - c0);
   const double* a = L.S + N.s_off;
   const int* piv = L.piv + N.p_off;
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int cols = ncols < 0 ? N.coff : ncols;
-  for (int col = blockIdx.x * (LNT / 32) + w; col < cols; col += gridDim.x * (LNT / 32)) {
-    double* x = L.R + N.r_off + (int64_t)col * n;
-    // row interchanges, in order
-    if (lane == 0)
-      for (int p = 0; p < n; ++p) {
-        int q = piv[p];
-        if (q != p) {
-          double t = x[p];
-          x[p] = x[q];
-          x[q] = t;
-        }
-      }
-    __syncwarp();
+  const int ldx = n | 1;
+  double* R = L.R + N.r_off;
+  for (int e = threadIdx.x; e < n * nc; e += blockDim.x) {
+    int i = e % n, c = e / n;
+    xs[c * ldx + i] = R[(int64_t)(c0 + c) * n + i];
+  }
+  __syncthreads();
+  for (int c = threadIdx.x; c < nc; c += blockDim.x) {
+    double* xc = xs + c * ldx;
     for (int p = 0; p < n; ++p) {
-      const double xp = x[p];
-      __syncwarp();
-      for (int i = p + 1 + lane; i < n; i += 32) x[i] = fma(-a[(int64_t)p * n + i], xp, x[i]);
-      __syncwarp();
+      int q = piv[p];
+      if (q != p) {
+        double t = xc[p];
+        xc[p] = xc[q];
+        xc[q] = t;
+      }
     }
-    for (int p = n - 1; p >= 0; --p) {
-      if (lane == 0) x[p] = x[p] / a[(int64_t)p * n + p];
-      __syncwarp();
-      const double xp = x[p];
-      for (int i = lane; i < p; i += 32) x[i] = fma(-a[(int64_t)p * n + i], xp, x[i]);
-      __syncwarp();
-    }
+  }
+  __syncthreads();
+  lu_solve_tile(GlobalLU{a, n}, n, xs, ldx, nc);
+  for (int e = threadIdx.x; e < n * nc; e += blockDim.x) {
+    int i = e % n, c = e / n;
+    R[(int64_t)(c0 + c) * n + i] = xs[c * ldx + i];
   }
 }
 
@@ -301,18 +427,25 @@ int leaf_solve_launch(const LeafSolveLaunch& L, int nleaves, int smax, cudaStrea
   return (int)cudaGetLastError();
 }
 
-int schur_factor_launch(const SchurLaunch& L, int nnodes, cudaStream_t s) {
+int schur_factor_launch(const SchurLaunch& L, int nnodes, int max_sd, cudaStream_t s) {
   if (nnodes == 0) return 0;
   schur_form_kernel<<<nnodes, 256, 0, s>>>(L);
-  dense_lu_kernel<<<nnodes, LNT, 0, s>>>(L);
+  int pnb = 16;
+  while (pnb > 1 && (size_t)max_sd * pnb * sizeof(double) > 200 * 1024) pnb >>= 1;
+  size_t smem = (size_t)max_sd * pnb * sizeof(double);
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute(schur_lu_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  schur_lu_kernel<<<nnodes, SNT, smem, s>>>(L, pnb);
   return (int)cudaGetLastError();
 }
 
-int schur_solve_launch(const SchurLaunch& L, int nnodes, int ncols, int max_cols,
+int schur_solve_launch(const SchurLaunch& L, int nnodes, int ncols, int max_cols, int max_sd,
                        cudaStream_t s) {
   if (nnodes == 0 || max_cols <= 0) return 0;
-  int gx = (max_cols + (LNT / 32) - 1) / (LNT / 32);
-  if (gx > 64) gx = 64;
-  dense_lu_solve_kernel<<<dim3(gx, nnodes), LNT, 0, s>>>(L, ncols);
+  size_t smem = sizeof(double) * (size_t)(max_sd | 1) * STC;
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute(schur_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
+  schur_solve_kernel<<<dim3((max_cols + STC - 1) / STC, nnodes), 256, smem, s>>>(L, ncols);
   return (int)cudaGetLastError();
 }

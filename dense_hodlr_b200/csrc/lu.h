@@ -48,6 +48,6 @@ struct SchurLaunch {
 
 int leaf_lu_launch(const LeafLULaunch& L, int nleaves, int smax, cudaStream_t s);
 int leaf_solve_launch(const LeafSolveLaunch& L, int nleaves, int smax, cudaStream_t s);
-int schur_factor_launch(const SchurLaunch& L, int nnodes, cudaStream_t s);
-int schur_solve_launch(const SchurLaunch& L, int nnodes, int ncols, int max_cols,
+int schur_factor_launch(const SchurLaunch& L, int nnodes, int max_sd, cudaStream_t s);
+int schur_solve_launch(const SchurLaunch& L, int nnodes, int ncols, int max_cols, int max_sd,
                        cudaStream_t s);

@@ -58,6 +58,8 @@ def lib():
         L.orc_exp.restype = ctypes.c_double
         L.orc_exp_tang.argtypes = [ctypes.c_double]
         L.orc_exp_tang.restype = ctypes.c_double
+        L.orc_exp_tang_neg.argtypes = [ctypes.c_double]
+        L.orc_exp_tang_neg.restype = ctypes.c_double
         L.orc_kernel_matvec.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp, ctypes.c_int]
         L.orc_aca_block.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, _dp, _ip]
         L.orc_bench_node.restype = ctypes.c_double
@@ -208,3 +210,7 @@ def hx_exp(x):
 
 def hx_exp_tang(x):
     return lib().orc_exp_tang(float(x))
+
+
+def hx_exp_tang_neg(x):
+    return lib().orc_exp_tang_neg(float(x))
