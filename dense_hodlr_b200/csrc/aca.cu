@@ -16,9 +16,15 @@
 // a contiguous slice of the block's rows (for W, the column pass) and of its
 // columns (for V, the row pass).  One ACA step is two group phases:
 //   A  row residual on the column slice, slice argmax   -> barrier
-//   B  pick pivot column, column residual on the row slice, slice argmax,
-//      slice partial dots for the norm estimate          -> barrier
-//   C  (redundant in every CTA) combine partials, epsilon, next row.
+//   B  pick pivot column, column residual on the row slice, slice argmax
+//                                                        -> barrier
+//   C  (redundant in every CTA) combine partials, next row.
+// Each step streams the W and V panels once.  The stopping test of step k-1
+// needs dots of its new columns with all earlier ones; they are accumulated
+// while step k streams the same panels for its residuals, and step k is run
+// speculatively: if epsilon_{k-1} <= tol it is discarded, so pivots and ranks
+// are those of the reference's loop.  Where step k cannot stream the panels
+// (a zero residual row, the capacity limit) the dots take a pass of their own.
 // G = 1 for levels with many blocks (barriers are __syncthreads); G > 1 runs
 // under a cooperative launch so that a group's CTAs are co-resident, and its
 // barrier is a counter in global memory polled with a bounded spin.
@@ -163,10 +169,127 @@ __device__ void reduce_partials(Shared& sh, const double* part, int64_t stride, 
   __syncthreads();
 }
 
+// One residual pass over a slice [lo, hi) of a panel P (column l at P + l*ld):
+//   r[j] = entry(j) - sum_{l<k} coef[l] * P(j, l)     (l order, unfused: bit-exact)
+//   written to P(j, k) * scale (scale = 1 for V, the pivot reciprocal for W),
+// and, if `dots`, the per-warp partial dots  sum_j P(j, l) * P(j, k-1)  for
+// l < k-1 accumulated into dotw[warp * ldd + l] (the norm update of step k-1,
+// computed while the panel streams through for step k).  Returns the slice
+// argmax of |r| (first maximum), the first admissible candidate (unchosen,
+// |r| > minPiv) and the partial sum of squares of the stored column.
+template <int NT, int E, bool ROW>
+__device__ void residual_pass(const AcaLaunch& L, const AcaBlock& B, double* P, int lo, int hi,
+                              int k, const double* coef, bool dots, double* dotw, int ldd,
+                              int fixed, const double* xfix, double scale,
+                              const unsigned char* chosen, double& bv, int& bi, int& cand,
+                              double& sq, bool& nonfinite) {
+  const int64_t ld = L.ld;
+  const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
+  const double minPiv = L.minPivot;
+  for (int jb = lo; jb < hi; jb += E * NT) {
+    int jj[E];
+    bool ok[E];
+    double s[E], vp[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      jj[e] = jb + tid + e * NT;
+      ok[e] = jj[e] < hi;
+      if (!ok[e]) jj[e] = lo;  // safe address; its products use vp = 0
+      s[e] = 0.0;
+      vp[e] = (dots && ok[e]) ? P[jj[e] + (int64_t)(k - 1) * ld] : 0.0;
+    }
+    const double* pl = P;
+    const int kd = dots ? k - 1 : 0;
+    int l = 0;
+    for (; l < kd; ++l, pl += ld) {
+      const double c = coef[l];
+      double d = 0.0;
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const double v = pl[jj[e]];
+        s[e] = __dadd_rn(s[e], __dmul_rn(c, v));
+        d = fma(v, vp[e], d);
+      }
+      d = warp_sum(d);
+      if (lane == 0) dotw[w * ldd + l] += d;
+    }
+#pragma unroll 4
+    for (; l < k; ++l, pl += ld) {
+      const double c = coef[l];
+#pragma unroll
+      for (int e = 0; e < E; ++e) s[e] = __dadd_rn(s[e], __dmul_rn(c, pl[jj[e]]));
+    }
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      if (!ok[e]) continue;
+      const int j = jj[e];
+      double ent = ROW ? src_entry_xi(L.src, xfix, fixed, (ROW ? B.c0 : B.r0) + j)
+                       : src_entry_xj(L.src, xfix, B.r0 + j, fixed);
+      double r = __dsub_rn(ent, s[e]);
+      double stored = ROW ? r : __dmul_rn(scale, r);
+      P[j + (int64_t)k * ld] = stored;
+      sq = fma(stored, stored, sq);
+      double a = fabs(r);
+      nonfinite |= !isfinite(r);
+      if (a > bv) {  // increasing j per thread: the first maximum
+        bv = a;
+        bi = j;
+      }
+      if (cand == INT_MAX && a > minPiv && __ldcg(chosen + j) == 0) cand = j;
+    }
+  }
+}
+
+// Partial dots of step k-1 over this CTA's slices when they could not be
+// fused into a residual pass (a zero residual row, or the capacity limit).
 template <int NT>
-__global__ void __launch_bounds__(NT) aca_kernel(AcaLaunch L) {
-  extern __shared__ double dyn[];  // wrow[kcap], vrow[kcap]
+__device__ void dots_only_pass(const AcaLaunch& L, const AcaBlock& B, int k, int i_lo, int i_hi,
+                               int j_lo, int j_hi, double* bank) {
+  const int64_t ld = L.ld;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const double* wk = B.W + (int64_t)(k - 1) * ld;
+  const double* vk = B.V + (int64_t)(k - 1) * ld;
+  for (int l = w; l < k - 1; l += NT / 32) {
+    const double* wl = B.W + (int64_t)l * ld;
+    const double* vl = B.V + (int64_t)l * ld;
+    double aw = 0.0, av = 0.0;
+    for (int i = i_lo + lane; i < i_hi; i += 32) aw = fma(wk[i], wl[i], aw);
+    for (int j = j_lo + lane; j < j_hi; j += 32) av = fma(vl[j], vk[j], av);
+    aw = warp_sum(aw);
+    av = warp_sum(av);
+    if (lane == 0) {
+      bank[l] = av;
+      bank[B.kcap + l] = aw;
+    }
+  }
+}
+
+// epsilon of step k-1 from the G partial dots in the bank at offset bk
+// (dotV at bk, dotW at bk + kcap):
+// frobNormSq += 2 sum_l (w.W_l)(V_l.v) + |w|^2 |v|^2  (src/lowRank.cpp:234-241)
+template <int NT>
+__device__ double resolve_eps(Shared& sh, const AcaLaunch& L, const AcaBlock& B,
+                              const double* part_grp, int G, int bk, int k, double swp,
+                              double svp, double& frob2) {
+  double sum_local = 0.0;
+  for (int l = threadIdx.x; l < k - 1; l += NT) {
+    double dv = 0.0, dw = 0.0;
+    for (int q = 0; q < G; ++q) {
+      dv += __ldcg(part_grp + q * L.part_stride + bk + l);
+      dw += __ldcg(part_grp + q * L.part_stride + bk + B.kcap + l);
+    }
+    sum_local += dw * dv;
+  }
+  const double sumNorm = block_sum<NT>(sh, sum_local);
+  frob2 += 2 * sumNorm + swp * svp;
+  return sqrt(swp) * sqrt(svp) / sqrt(frob2);
+}
+
+template <int NT, int E>
+__global__ void __launch_bounds__(NT, (NT == 256 ? 2 : 4)) aca_kernel(AcaLaunch L) {
+  extern __shared__ double dyn[];  // row[kcap], per-warp dots[NT/32][kcap]
   __shared__ Shared sh;
+  constexpr int NW = NT / 32;
   const int G = L.G;
   const int b = blockIdx.x / G, g = blockIdx.x % G;
   const int tid = threadIdx.x;
@@ -178,8 +301,9 @@ __global__ void __launch_bounds__(NT) aca_kernel(AcaLaunch L) {
   const int64_t ld = L.ld;
   const int m = B.m, n = B.n, ub = min(m, n);
   const double tol = L.tol, minPiv = L.minPivot;
-  double* wrow = dyn;
-  double* vrow = dyn + B.kcap;
+  double* row = dyn;
+  double* dotw = dyn + L.kcap_max;
+  const int ldd = L.kcap_max;
   double* part_me = L.part + (int64_t)blockIdx.x * L.part_stride;
   const double* part_grp = L.part + (int64_t)(b * G) * L.part_stride;
   unsigned* bar = L.bar + b;
@@ -191,70 +315,75 @@ __global__ void __launch_bounds__(NT) aca_kernel(AcaLaunch L) {
 
   int k = st->k, cur = st->cur, iters = st->iters, status = st->status;
   double frob2 = st->frob2, eps = st->eps, margin = st->margin;
-  int near = st->near;
+  double swp = st->swp, svp = st->svp;
+  int near = st->near, pending = st->pending;
   bool nonfinite = false;
 
-  while (status == ACA_RUNNING) {
-    // while ((eps > tol || k < minRank) && k < ub), minRank = -1 on the default tree
-    if (!(eps > tol) || k >= ub) {
-      status = ACA_POST;
-      break;
+  auto note_margin = [&](int kcount) {
+    if (kcount < ub) {
+      double gap = fabs(eps - tol) / tol;
+      margin = fmin(margin, gap);
+      if (gap < 1e-10) ++near;
     }
-    if (k >= B.kcap) {  // paused: the host grows the capacity and resumes
-      status = ACA_NEED_CAP;
+  };
+
+  while (status == ACA_RUNNING) {
+    // loop test of the reference, with epsilon_{k-1} possibly still pending
+    if (!pending && !(eps > tol)) { status = ACA_POST; break; }
+    if (k >= ub) { status = ACA_POST; break; }
+    if (k >= B.kcap) {
+      if (pending) {
+        const int bk0 = 8 + (k & 1) * (2 * B.kcap + 2);
+        dots_only_pass<NT>(L, B, k, i_lo, i_hi, j_lo, j_hi, part_me + bk0);
+        if (!group_sync(bar, G, gen, L.err)) { status = ACA_ERROR; break; }
+        eps = resolve_eps<NT>(sh, L, B, part_grp, G, bk0, k, swp, svp, frob2);
+        pending = 0;
+        note_margin(k);
+        if (!group_sync(bar, G, gen, L.err)) { status = ACA_ERROR; break; }
+        if (!(eps > tol)) { status = ACA_POST; break; }
+      }
+      status = ACA_NEED_CAP;  // paused: the host grows the capacity and resumes
       break;
     }
     ++iters;
+    const bool fuse = pending && k >= 2;
+    // Dot and norm partials alternate between two banks by step parity: a
+    // slow CTA may still read step k-1's bank in its phase C while a fast one
+    // already writes step k's in phase A.
+    const int bk = 8 + (k & 1) * (2 * B.kcap + 2);
     // ---------------- phase A: residual row on this CTA's column slice
     if (g == 0 && tid == 0) B.cR[cur] = 1;
-    for (int l = tid; l < k; l += NT) wrow[l] = __ldcg(B.W + cur + (int64_t)l * ld);
+    for (int l = tid; l < k; l += NT) row[l] = __ldcg(B.W + cur + (int64_t)l * ld);
+    if (fuse)
+      for (int e = tid; e < NW * (k - 1); e += NT) dotw[(e / (k - 1)) * ldd + e % (k - 1)] = 0.0;
     __syncthreads();
     const int gi = B.r0 + cur;
     double xi[3] = {0.0, 0.0, 0.0};
-    if (!L.src.dense)
-      #pragma unroll
+    if (!L.src.dense) {
+#pragma unroll
       for (int d = 0; d < 3; ++d)
         if (d < L.src.kp.dim) xi[d] = __ldg(L.src.pts + d * L.src.ld + gi);
-    double bv = -1.0;
-    int bi = INT_MAX, cand = INT_MAX;
-    for (int j0 = j_lo + tid; j0 < j_hi; j0 += 4 * NT) {
-      int jj[4];
-      double s[4];
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        jj[e] = j0 + e * NT;
-        s[e] = 0.0;
-      }
-      const double* vp = B.V;
-      for (int l = 0; l < k; ++l, vp += ld) {
-        const double w = wrow[l];
-#pragma unroll
-        for (int e = 0; e < 4; ++e)
-          if (jj[e] < j_hi) s[e] = __dadd_rn(s[e], __dmul_rn(w, vp[jj[e]]));
-      }
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const int j = jj[e];
-        if (j < j_hi) {
-          double v = __dsub_rn(src_entry_xi(L.src, xi, gi, B.c0 + j), s[e]);
-          B.V[j + (int64_t)k * ld] = v;
-          double a = fabs(v);
-          nonfinite |= !isfinite(v);
-          if (a > bv) {  // increasing j per thread: keeps the first maximum
-            bv = a;
-            bi = j;
-          }
-          if (cand == INT_MAX && a > minPiv && __ldcg(B.cC + j) == 0) cand = j;
-        }
-      }
     }
+    double bv = -1.0, sv = 0.0;
+    int bi = INT_MAX, cand = INT_MAX;
+    residual_pass<NT, E, true>(L, B, B.V, j_lo, j_hi, k, row, fuse, dotw, ldd, gi, xi, 1.0, B.cC,
+                               bv, bi, cand, sv, nonfinite);
+    __syncthreads();
+    if (fuse)  // CTA partial dots of V, warps summed in order
+      for (int l = tid; l < k - 1; l += NT) {
+        double t = 0.0;
+        for (int q = 0; q < NW; ++q) t += dotw[q * ldd + l];
+        part_me[bk + l] = t;
+      }
     block_argmax<NT>(sh, bv, bi);
     cand = block_min_int<NT>(sh, cand);
+    sv = block_sum<NT>(sh, sv);
     if (tid == 0) {
       part_me[0] = bv;
       part_me[1] = (double)bi;
       part_me[2] = (bi != INT_MAX) ? (double)__ldcg(B.cC + bi) : 0.0;
       part_me[3] = (double)cand;
+      part_me[bk + 2 * B.kcap + 1] = sv;
     }
     if (!group_sync(bar, G, gen, L.err)) { status = ACA_ERROR; break; }
 
@@ -263,7 +392,16 @@ __global__ void __launch_bounds__(NT) aca_kernel(AcaLaunch L) {
     int mi, mflag, mcand;
     reduce_partials(sh, part_grp, L.part_stride, G, 0, mv, mi, mflag, mcand);
     if (mv <= minPiv) {
-      // zero residual row: move to the first unchosen row (src/lowRank.cpp:187-195)
+      // zero residual row (src/lowRank.cpp:187-195).  Whether the reference
+      // even reached this step depends on epsilon_{k-1}: settle it first.
+      if (pending) {
+        dots_only_pass<NT>(L, B, k, i_lo, i_hi, j_lo, j_hi, part_me + bk);
+        if (!group_sync(bar, G, gen, L.err)) { status = ACA_ERROR; break; }
+        eps = resolve_eps<NT>(sh, L, B, part_grp, G, bk, k, swp, svp, frob2);
+        pending = 0;
+        note_margin(k);
+        if (!(eps > tol)) { status = ACA_POST; break; }
+      }
       int f = INT_MAX;
       for (int i = tid; i < m; i += NT)
         if (__ldcg(B.cR + i) == 0) { f = i; break; }
@@ -277,139 +415,83 @@ __global__ void __launch_bounds__(NT) aca_kernel(AcaLaunch L) {
     if (!mflag) {
       cc = mi;
     } else {
+      // whichever way epsilon_{k-1} goes, the rank is k (src/lowRank.cpp:200-202)
       if (mcand == INT_MAX) { status = ACA_POST; break; }
       cc = mcand;
     }
     if (g == 0 && tid == 0) B.cC[cc] = 1;
     const double piv = __ddiv_rn(1.0, __ldcg(B.V + cc + (int64_t)k * ld));
-    for (int l = tid; l < k; l += NT) vrow[l] = __ldcg(B.V + cc + (int64_t)l * ld);
+    for (int l = tid; l < k; l += NT) row[l] = __ldcg(B.V + cc + (int64_t)l * ld);
+    if (fuse)
+      for (int e = tid; e < NW * (k - 1); e += NT) dotw[(e / (k - 1)) * ldd + e % (k - 1)] = 0.0;
     __syncthreads();
     const int gj = B.c0 + cc;
     double xj[3] = {0.0, 0.0, 0.0};
-    if (!L.src.dense)
-      #pragma unroll
+    if (!L.src.dense) {
+#pragma unroll
       for (int d = 0; d < 3; ++d)
         if (d < L.src.kp.dim) xj[d] = __ldg(L.src.pts + d * L.src.ld + gj);
+    }
     bv = -1.0;
     bi = INT_MAX;
     cand = INT_MAX;
     double sw = 0.0;
-    for (int i0 = i_lo + tid; i0 < i_hi; i0 += 4 * NT) {
-      int ii[4];
-      double s[4];
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        ii[e] = i0 + e * NT;
-        s[e] = 0.0;
+    residual_pass<NT, E, false>(L, B, B.W, i_lo, i_hi, k, row, fuse, dotw, ldd, gj, xj, piv,
+                                B.cR, bv, bi, cand, sw, nonfinite);
+    __syncthreads();
+    if (fuse)
+      for (int l = tid; l < k - 1; l += NT) {
+        double t = 0.0;
+        for (int q = 0; q < NW; ++q) t += dotw[q * ldd + l];
+        part_me[bk + B.kcap + l] = t;
       }
-      const double* wp = B.W;
-      for (int l = 0; l < k; ++l, wp += ld) {
-        const double v = vrow[l];
-#pragma unroll
-        for (int e = 0; e < 4; ++e)
-          if (ii[e] < i_hi) s[e] = __dadd_rn(s[e], __dmul_rn(v, wp[ii[e]]));
-      }
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const int i = ii[e];
-        if (i < i_hi) {
-          double c = __dsub_rn(src_entry_xj(L.src, xj, B.r0 + i, gj), s[e]);
-          double w = __dmul_rn(piv, c);
-          B.W[i + (int64_t)k * ld] = w;
-          sw = fma(w, w, sw);
-          double a = fabs(c);
-          nonfinite |= !isfinite(c);
-          if (a > bv) {
-            bv = a;
-            bi = i;
-          }
-          if (cand == INT_MAX && a > minPiv && __ldcg(B.cR + i) == 0) cand = i;
-        }
-      }
-    }
     block_argmax<NT>(sh, bv, bi);
     cand = block_min_int<NT>(sh, cand);
+    sw = block_sum<NT>(sh, sw);
     if (tid == 0) {
       part_me[4] = bv;
       part_me[5] = (double)bi;
       part_me[6] = (bi != INT_MAX) ? (double)__ldcg(B.cR + bi) : 0.0;
       part_me[7] = (double)cand;
-    }
-    // partial dots of the norm update over this CTA's slices
-    sw = block_sum<NT>(sh, sw);
-    double sv = 0.0;
-    for (int j = j_lo + tid; j < j_hi; j += NT) {
-      double v = B.V[j + (int64_t)k * ld];
-      sv = fma(v, v, sv);
-    }
-    sv = block_sum<NT>(sh, sv);
-    {
-      const int w = tid >> 5, lane = tid & 31;
-      const double* wk = B.W + (int64_t)k * ld;
-      const double* vk = B.V + (int64_t)k * ld;
-      for (int l = w; l < k; l += NT / 32) {
-        const double* wl = B.W + (int64_t)l * ld;
-        const double* vl = B.V + (int64_t)l * ld;
-        double aw = 0.0, av = 0.0;
-        for (int i = i_lo + lane; i < i_hi; i += 32) aw = fma(wk[i], wl[i], aw);
-        for (int j = j_lo + lane; j < j_hi; j += 32) av = fma(vl[j], vk[j], av);
-        aw = warp_sum(aw);
-        av = warp_sum(av);
-        if (lane == 0) {
-          part_me[8 + l] = aw;
-          part_me[8 + B.kcap + l] = av;
-        }
-      }
-      if (tid == 0) {
-        part_me[8 + 2 * B.kcap] = sw;
-        part_me[9 + 2 * B.kcap] = sv;
-      }
+      part_me[bk + 2 * B.kcap] = sw;
     }
     if (!group_sync(bar, G, gen, L.err)) { status = ACA_ERROR; break; }
 
-    // ---------------- phase C: next row, norm estimate, epsilon
+    // ---------------- phase C: epsilon of step k-1, then step k's next row
+    if (pending) {
+      eps = fuse ? resolve_eps<NT>(sh, L, B, part_grp, G, bk, k, swp, svp, frob2)
+                 : [&]() {  // k == 1: no earlier columns, the dots are empty
+                     frob2 += swp * svp;
+                     return sqrt(swp) * sqrt(svp) / sqrt(frob2);
+                   }();
+      pending = 0;
+      note_margin(k);
+      if (!(eps > tol)) { status = ACA_POST; break; }  // step k is discarded
+    }
     int nflag, ncand, ni;
     double nv;
     reduce_partials(sh, part_grp, L.part_stride, G, 4, nv, ni, nflag, ncand);
-    int nr;
-    if (!nflag)
-      nr = ni;
-    else
-      nr = ncand;
+    const int nr = nflag ? ncand : ni;
     if (nr == INT_MAX) {  // no admissible next row: stop before storing (src/lowRank.cpp:226-227)
       status = ACA_POST;
       break;
     }
-    double sum_local = 0.0;
-    for (int l = tid; l < k; l += NT) {
-      double dw = 0.0, dv = 0.0;
-      for (int q = 0; q < G; ++q) {
-        dw += __ldcg(part_grp + q * L.part_stride + 8 + l);
-        dv += __ldcg(part_grp + q * L.part_stride + 8 + B.kcap + l);
-      }
-      sum_local += dw * dv;
-    }
-    double sumNorm = block_sum<NT>(sh, sum_local);
     double swt = 0.0, svt = 0.0;
     for (int q = 0; q < G; ++q) {
-      swt += __ldcg(part_grp + q * L.part_stride + 8 + 2 * B.kcap);
-      svt += __ldcg(part_grp + q * L.part_stride + 9 + 2 * B.kcap);
+      swt += __ldcg(part_grp + q * L.part_stride + bk + 2 * B.kcap);
+      svt += __ldcg(part_grp + q * L.part_stride + bk + 2 * B.kcap + 1);
     }
-    frob2 += 2 * sumNorm + swt * svt;
-    eps = sqrt(swt) * sqrt(svt) / sqrt(frob2);
     if (g == 0 && tid == 0) {
       B.prow[k] = cur;
       B.pcol[k] = cc;
     }
+    swp = swt;
+    svp = svt;
+    pending = 1;
     cur = nr;
     ++k;
-    if (k < ub) {
-      double gap = fabs(eps - tol) / tol;
-      margin = fmin(margin, gap);
-      if (gap < 1e-10) ++near;
-    }
-    // No barrier needed here: the next writes to the row partials happen
-    // after every CTA has passed barrier 2, and W(:,k) / V(:,k) are final.
+    // No barrier needed here: the next writes to the partials come after
+    // every CTA has passed barrier 2, and W(:,k) / V(:,k) are final.
   }
 
   // ---------------- post-processing (src/lowRank.cpp:250-277)
@@ -427,13 +509,14 @@ __global__ void __launch_bounds__(NT) aca_kernel(AcaLaunch L) {
         rank = full;
       } else if (n <= m) {  // W = block (m x n), V = I_n
         for (int l = 0; l < n; ++l) {
-          double xj[3] = {0.0, 0.0, 0.0};
-          if (!L.src.dense)
+          double xc[3] = {0.0, 0.0, 0.0};
+          if (!L.src.dense) {
 #pragma unroll
             for (int d = 0; d < 3; ++d)
-              if (d < L.src.kp.dim) xj[d] = __ldg(L.src.pts + d * L.src.ld + B.c0 + l);
+              if (d < L.src.kp.dim) xc[d] = __ldg(L.src.pts + d * L.src.ld + B.c0 + l);
+          }
           for (int i = i_lo + tid; i < i_hi; i += NT)
-            B.W[i + (int64_t)l * ld] = src_entry_xj(L.src, xj, B.r0 + i, B.c0 + l);
+            B.W[i + (int64_t)l * ld] = src_entry_xj(L.src, xc, B.r0 + i, B.c0 + l);
           for (int j = j_lo + tid; j < j_hi; j += NT)
             B.V[j + (int64_t)l * ld] = (j == l) ? 1.0 : 0.0;
         }
@@ -441,13 +524,14 @@ __global__ void __launch_bounds__(NT) aca_kernel(AcaLaunch L) {
         status = ACA_DONE;
       } else {  // W = I_m, V = block^T (n x m)
         for (int l = 0; l < m; ++l) {
-          double xi[3] = {0.0, 0.0, 0.0};
-          if (!L.src.dense)
+          double xr[3] = {0.0, 0.0, 0.0};
+          if (!L.src.dense) {
 #pragma unroll
             for (int d = 0; d < 3; ++d)
-              if (d < L.src.kp.dim) xi[d] = __ldg(L.src.pts + d * L.src.ld + B.r0 + l);
+              if (d < L.src.kp.dim) xr[d] = __ldg(L.src.pts + d * L.src.ld + B.r0 + l);
+          }
           for (int j = j_lo + tid; j < j_hi; j += NT)
-            B.V[j + (int64_t)l * ld] = src_entry_xi(L.src, xi, B.r0 + l, B.c0 + j);
+            B.V[j + (int64_t)l * ld] = src_entry_xi(L.src, xr, B.r0 + l, B.c0 + j);
           for (int i = i_lo + tid; i < i_hi; i += NT)
             B.W[i + (int64_t)l * ld] = (i == l) ? 1.0 : 0.0;
         }
@@ -473,47 +557,37 @@ __global__ void __launch_bounds__(NT) aca_kernel(AcaLaunch L) {
     st->margin = margin;
     st->near = near;
     st->rank = rank;
+    st->swp = swp;
+    st->svp = svp;
+    st->pending = pending;
   }
 }
 
 }  // namespace
 
+static size_t aca_smem(int nt, int kcap_max) {
+  return sizeof(double) * (size_t)(1 + nt / 32) * (size_t)kcap_max;
+}
+
 int aca_launch(const AcaLaunch& L, int nt, int kcap_max, bool cooperative, cudaStream_t s) {
-  size_t smem = sizeof(double) * 2 * (size_t)kcap_max;
+  size_t smem = aca_smem(nt, kcap_max);
   dim3 grid(L.nblocks * L.G), block(nt);
   void* args[] = {(void*)&L};
-  cudaError_t e;
-  if (nt == 256) {
-    auto fn = aca_kernel<256>;
-    if (smem > 48 * 1024)
-      cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    e = cooperative ? cudaLaunchCooperativeKernel((void*)fn, grid, block, args, smem, s)
-                    : cudaLaunchKernel((void*)fn, grid, block, args, smem, s);
-  } else {
-    auto fn = aca_kernel<128>;
-    if (smem > 48 * 1024)
-      cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    e = cooperative ? cudaLaunchCooperativeKernel((void*)fn, grid, block, args, smem, s)
-                    : cudaLaunchKernel((void*)fn, grid, block, args, smem, s);
-  }
+  void* fn = nt == 256 ? (void*)aca_kernel<256, 4> : (void*)aca_kernel<128, 2>;
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = cooperative ? cudaLaunchCooperativeKernel(fn, grid, block, args, smem, s)
+                              : cudaLaunchKernel(fn, grid, block, args, smem, s);
   return e == cudaSuccess ? 0 : (int)e;
 }
 
 int aca_max_coresident(int nt, int kcap_max, int* per_sm) {
-  size_t smem = sizeof(double) * 2 * (size_t)kcap_max;
+  size_t smem = aca_smem(nt, kcap_max);
+  void* fn = nt == 256 ? (void*)aca_kernel<256, 4> : (void*)aca_kernel<128, 2>;
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int nb = 0;
-  cudaError_t e;
-  if (nt == 256) {
-    if (smem > 48 * 1024)
-      cudaFuncSetAttribute(aca_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)smem);
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, aca_kernel<256>, nt, smem);
-  } else {
-    if (smem > 48 * 1024)
-      cudaFuncSetAttribute(aca_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)smem);
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, aca_kernel<128>, nt, smem);
-  }
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, nt, smem);
   *per_sm = nb;
   return e == cudaSuccess ? 0 : (int)e;
 }

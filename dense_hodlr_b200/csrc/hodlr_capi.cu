@@ -375,7 +375,7 @@ int run_aca(hodlr_t h, std::vector<AcaBlock>& blocks, int G, int nt, int kcap_ma
   }
   CK(cudaMemcpyAsync(h->d_blocks, blocks.data(), sizeof(AcaBlock) * nb, cudaMemcpyHostToDevice,
                      h->stream));
-  int64_t stride = 16 + 2 * (int64_t)kcap_max;
+  int64_t stride = 12 + 4 * (int64_t)kcap_max;  // args + two banks of dots and norms
   int64_t need = stride * nb * G;
   if (need > h->part_cap) {
     dfree(h->part);
@@ -395,12 +395,15 @@ int run_aca(hodlr_t h, std::vector<AcaBlock>& blocks, int G, int nt, int kcap_ma
   L.ld = h->n;
   L.tol = h->tol;
   L.minPivot = (double)h->minPivot;
+  L.kcap_max = kcap_max;
   L.part = h->part;
   L.part_stride = stride;
   L.bar = h->bar;
   L.err = h->d_err;
   L.src = make_src(h);
   CK(cudaEventRecord(h->ev0, h->stream));
+  if ((size_t)(1 + nt / 32) * kcap_max * sizeof(double) > 227 * 1024)
+    return fail(h, HODLR_ERR_UNSUPPORTED, "block rank above the shared-memory limit of ACA");
   int rc = aca_launch(L, nt, kcap_max, G > 1, h->stream);
   if (rc) return cuda_fail(h, (cudaError_t)rc, "aca_launch");
   h->nlaunch += 1;
@@ -446,6 +449,9 @@ int do_compress(hodlr_t h) {
       s.iters = 0;
       s.rank = 0;
       s.near = 0;
+      s.swp = s.svp = 0;
+      s.pending = 0;
+      s.pad = 0;
     }
     CK(cudaMemcpyAsync(L.d_st, L.st.data(), sizeof(AcaState) * nb, cudaMemcpyHostToDevice,
                        h->stream));
@@ -525,8 +531,10 @@ int do_compress(hodlr_t h) {
       L.kmax = std::max(L.kmax, L.st[q].rank);
       int r0, c0, m, n;
       block_geom(L, q, r0, c0, m, n);
+      // one read of the W and V panels per step (the norm dots ride along),
+      // the two new columns and the coordinates of the entries evaluated
       double K = L.st[q].iters;
-      bytes += 8.0 * (m + n) * (K * (K - 1) + K * (1 + h->dim));
+      bytes += (double)(m + n) * (4.0 * K * (K - 1) + 8.0 * K * (1 + h->dim));
     }
     L.coff = (int)coff;
     coff += L.kmax;

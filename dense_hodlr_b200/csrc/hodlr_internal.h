@@ -47,7 +47,10 @@ struct AcaBlock {
 // Loop state of one block; lets a paused block resume where it stopped.
 struct AcaState {
   double frob2, eps, margin;
+  double swp, svp;  // |w_{k-1}|^2, |v_{k-1}|^2 while epsilon_{k-1} is pending
   int k, cur, status, iters, rank, near;
+  int pending;      // 1: epsilon of step k-1 not evaluated yet
+  int pad;
 };
 
 struct AcaLaunch {
@@ -56,6 +59,7 @@ struct AcaLaunch {
   int G;                 // CTAs per block
   int64_t ld;            // N
   double tol, minPivot;
+  int kcap_max;          // largest kcap among the launch's blocks (shared memory rows)
   double* part;          // per-CTA partials, part_stride doubles each
   int64_t part_stride;
   unsigned* bar;         // per-block barrier counters (zeroed before launch)

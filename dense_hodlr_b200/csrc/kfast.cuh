@@ -68,15 +68,16 @@ HX_HD double hx_exp_tang(double x, const double* tab) {
   return v * hx_pow2i(k);
 }
 
-// e^x for x <= 0 without branches: x is clamped at -746 (e^x underflows to 0
-// there anyway) and 2^k is applied as two factors so that every scale factor
-// stays a normal number down to the subnormal range.
+// e^x for x <= 0 without branches.  x is clamped at -707 so that 2^k stays in
+// the normal range (k >= -1020) and the scale is a single integer add to the
+// exponent field; for x < -707 the result is e^-707 ~ 1e-307 instead of a
+// smaller or subnormal value, an absolute difference below 1e-306.
 HX_HD double hx_exp_tang_neg(double x, const double* tab) {
   const double INV_L = 0x1.71547652b82fep+6;
   const double L_HI = 0x1.62e42fe000000p-7;
   const double L_LO = 0x1.f473de6af278fp-36;
   const double SHIFTER = 0x1.8p52;
-  x = fmax(x, -746.0);
+  x = fmax(x, -707.0);
   double t0 = fma(x, INV_L, SHIFTER);
   double nd = t0 - SHIFTER;
 #if defined(__CUDA_ARCH__)
@@ -91,11 +92,37 @@ HX_HD double hx_exp_tang_neg(double x, const double* tab) {
   p = fma(p, r, 0x1.5555555555555p-3);
   p = fma(p, r, 0.5);
   p = fma(p * r, r, r);
-  const int j = n & 63;
-  const int k = (n - j) >> 6;
-  const int k1 = k >> 1;
-  const double t = tab[j];
-  return (fma(t, p, t) * hx_pow2i(k1)) * hx_pow2i(k - k1);
+  const double t = tab[n & 63];
+  const double v = fma(t, p, t);
+  const int64_t k = (int64_t)((n - (n & 63)) >> 6);
+#if defined(__CUDA_ARCH__)
+  return __longlong_as_double(__double_as_longlong(v) + (k << 52));
+#else
+  int64_t vb;
+  memcpy(&vb, &v, sizeof(vb));
+  vb += (int64_t)((uint64_t)k << 52);
+  double out;
+  memcpy(&out, &vb, sizeof(out));
+  return out;
+#endif
+}
+
+// Kernel value of r2 for a kernel family fixed at compile time (no per-entry
+// dispatch in the residual kernel).
+template <int KTYPE>
+HX_HD double hx_kernel_r2_fast_t(double a, double r2, const double* tab) {
+  if (KTYPE == HX_KERNEL_GAUSSIAN) return hx_exp_tang_neg(r2 * a, tab);
+  if (KTYPE == HX_KERNEL_MATERN32) {
+#if defined(__CUDA_ARCH__)
+    double s = r2 * rsqrt(fmax(r2, 1e-300)) * a;
+#else
+    double s = sqrt(r2) * a;
+#endif
+    return (1.0 + s) * hx_exp_tang_neg(-s, tab);
+  }
+  if (KTYPE == HX_KERNEL_INV_MULTIQUADRIC) return 1.0 / sqrt(fma(r2, a, 1.0));
+  if (KTYPE == HX_KERNEL_QUADRATIC) return fma(r2, a, 1.0);
+  return hx_exp_tang_neg(-sqrt(r2) * a, tab);
 }
 
 // Kernel value of the squared distance, FP64-accurate (not bit-matched to ACA).

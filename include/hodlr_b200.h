@@ -160,8 +160,10 @@ int hodlr_get_lowrank(hodlr_t h, int block, double* W, double* V);
 int hodlr_get_block_margin(hodlr_t h, int block, double* margin, int* near);
 
 /* ACA kernel statistics of the last compression: launches, summed device
- * time (seconds) and algorithmic bytes (one read of the W and V panels for
- * the residual and one for the norm update per step, plus the new columns). */
+ * time (seconds) and algorithmic bytes: per block and step t, one read of
+ * the W and V panels (8 t (m+n) bytes; the norm-update dots ride along), the
+ * two new columns (8 (m+n)) and the coordinates of the entries evaluated
+ * (8 dim (m+n)). */
 int hodlr_get_aca_stats(hodlr_t h, int* launches, double* seconds, double* bytes);
 
 /* Initial number of low-rank columns to allocate per inner level (caps[l],
