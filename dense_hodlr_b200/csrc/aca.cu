@@ -179,14 +179,18 @@ __device__ void reduce_partials(Shared& sh, const double* part, int64_t stride, 
 // |r| > minPiv) and the partial sum of squares of the stored column.
 template <int NT, int E, bool ROW>
 __device__ void residual_pass(const AcaLaunch& L, const AcaBlock& B, double* P, int lo, int hi,
-                              int k, const double* coef, bool dots, double* dotw, int ldd,
-                              int fixed, const double* xfix, double scale,
-                              const unsigned char* chosen, double& bv, int& bi, int& cand,
-                              double& sq, bool& nonfinite) {
+                              int k, const double* __restrict__ coef, bool dots,
+                              double* __restrict__ dotw, int ldd, int fixed, const double* xfix,
+                              double scale, const unsigned char* chosen, double& bv, int& bi,
+                              int& cand, double& sq, bool& nonfinite) {
+  constexpr int U = 16 / E;  // panel columns per chunk: 16 loads in flight per thread
   const int64_t ld = L.ld;
   const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
   const double minPiv = L.minPivot;
-  for (int jb = lo; jb < hi; jb += E * NT) {
+  const double* __restrict__ Pr = P;  // columns < k are only read here
+  const int kd = dots ? k - 1 : 0;
+  bool first = true;
+  for (int jb = lo; jb < hi; jb += E * NT, first = false) {
     int jj[E];
     bool ok[E];
     double s[E], vp[E];
@@ -196,34 +200,62 @@ __device__ void residual_pass(const AcaLaunch& L, const AcaBlock& B, double* P, 
       ok[e] = jj[e] < hi;
       if (!ok[e]) jj[e] = lo;  // safe address; its products use vp = 0
       s[e] = 0.0;
-      vp[e] = (dots && ok[e]) ? P[jj[e] + (int64_t)(k - 1) * ld] : 0.0;
+      vp[e] = (dots && ok[e]) ? Pr[jj[e] + (int64_t)(k - 1) * ld] : 0.0;
     }
-    const double* pl = P;
-    const int kd = dots ? k - 1 : 0;
     int l = 0;
-    for (; l < kd; ++l, pl += ld) {
+    for (; l + U <= k; l += U) {
+      double v[U][E];
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+#pragma unroll
+        for (int e = 0; e < E; ++e) v[u][e] = Pr[jj[e] + (int64_t)(l + u) * ld];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const double c = coef[l + u];
+#pragma unroll
+        for (int e = 0; e < E; ++e) s[e] = __dadd_rn(s[e], __dmul_rn(c, v[u][e]));
+      }
+      if (dots) {
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          if (l + u >= kd) break;
+          double d = 0.0;
+#pragma unroll
+          for (int e = 0; e < E; ++e) d = fma(v[u][e], vp[e], d);
+          d = warp_sum(d);
+          if (lane == 0) {
+            if (first)
+              dotw[w * ldd + l + u] = d;
+            else
+              dotw[w * ldd + l + u] += d;
+          }
+        }
+      }
+    }
+    for (; l < k; ++l) {
       const double c = coef[l];
       double d = 0.0;
 #pragma unroll
       for (int e = 0; e < E; ++e) {
-        const double v = pl[jj[e]];
+        const double v = Pr[jj[e] + (int64_t)l * ld];
         s[e] = __dadd_rn(s[e], __dmul_rn(c, v));
         d = fma(v, vp[e], d);
       }
-      d = warp_sum(d);
-      if (lane == 0) dotw[w * ldd + l] += d;
-    }
-#pragma unroll 4
-    for (; l < k; ++l, pl += ld) {
-      const double c = coef[l];
-#pragma unroll
-      for (int e = 0; e < E; ++e) s[e] = __dadd_rn(s[e], __dmul_rn(c, pl[jj[e]]));
+      if (dots && l < kd) {
+        d = warp_sum(d);
+        if (lane == 0) {
+          if (first)
+            dotw[w * ldd + l] = d;
+          else
+            dotw[w * ldd + l] += d;
+        }
+      }
     }
 #pragma unroll
     for (int e = 0; e < E; ++e) {
       if (!ok[e]) continue;
       const int j = jj[e];
-      double ent = ROW ? src_entry_xi(L.src, xfix, fixed, (ROW ? B.c0 : B.r0) + j)
+      double ent = ROW ? src_entry_xi(L.src, xfix, fixed, B.c0 + j)
                        : src_entry_xj(L.src, xfix, B.r0 + j, fixed);
       double r = __dsub_rn(ent, s[e]);
       double stored = ROW ? r : __dmul_rn(scale, r);
@@ -354,7 +386,7 @@ __global__ void __launch_bounds__(NT, (NT == 256 ? 2 : 4)) aca_kernel(AcaLaunch 
     // ---------------- phase A: residual row on this CTA's column slice
     if (g == 0 && tid == 0) B.cR[cur] = 1;
     for (int l = tid; l < k; l += NT) row[l] = __ldcg(B.W + cur + (int64_t)l * ld);
-    if (fuse)
+    if (fuse && j_lo >= j_hi)  // an empty slice contributes zero dots
       for (int e = tid; e < NW * (k - 1); e += NT) dotw[(e / (k - 1)) * ldd + e % (k - 1)] = 0.0;
     __syncthreads();
     const int gi = B.r0 + cur;
@@ -400,7 +432,11 @@ __global__ void __launch_bounds__(NT, (NT == 256 ? 2 : 4)) aca_kernel(AcaLaunch 
         eps = resolve_eps<NT>(sh, L, B, part_grp, G, bk, k, swp, svp, frob2);
         pending = 0;
         note_margin(k);
-        if (!(eps > tol)) { status = ACA_POST; break; }
+        if (!(eps > tol)) {
+          --iters;
+          status = ACA_POST;
+          break;
+        }
       }
       int f = INT_MAX;
       for (int i = tid; i < m; i += NT)
@@ -422,7 +458,7 @@ __global__ void __launch_bounds__(NT, (NT == 256 ? 2 : 4)) aca_kernel(AcaLaunch 
     if (g == 0 && tid == 0) B.cC[cc] = 1;
     const double piv = __ddiv_rn(1.0, __ldcg(B.V + cc + (int64_t)k * ld));
     for (int l = tid; l < k; l += NT) row[l] = __ldcg(B.V + cc + (int64_t)l * ld);
-    if (fuse)
+    if (fuse && i_lo >= i_hi)
       for (int e = tid; e < NW * (k - 1); e += NT) dotw[(e / (k - 1)) * ldd + e % (k - 1)] = 0.0;
     __syncthreads();
     const int gj = B.c0 + cc;
@@ -466,7 +502,11 @@ __global__ void __launch_bounds__(NT, (NT == 256 ? 2 : 4)) aca_kernel(AcaLaunch 
                    }();
       pending = 0;
       note_margin(k);
-      if (!(eps > tol)) { status = ACA_POST; break; }  // step k is discarded
+      if (!(eps > tol)) {  // step k is discarded: the reference stopped before it
+        --iters;
+        status = ACA_POST;
+        break;
+      }
     }
     int nflag, ncand, ni;
     double nv;
