@@ -18,6 +18,8 @@
 //   S_l        per node (k_b + k_t)^2 capacitance LU + pivots
 #include <algorithm>
 #include <cmath>
+#include <map>
+#include <unordered_map>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -87,7 +89,65 @@ void block_geom(const Level& L, int q, int& r0, int& c0, int& m, int& n) {
 
 }  // namespace
 
+// Device memory cache of one handle.  Freed blocks go to `pending` and become
+// reusable only after the handle's stream has been synchronised, so a reused
+// block is never still read by an earlier kernel or host copy.
+struct DevPool {
+  std::multimap<size_t, void*> freeb, pending;
+  std::unordered_map<void*, size_t> size;
+  cudaError_t alloc(void** p, size_t bytes, cudaStream_t s) {
+    bytes = (bytes + 255) & ~(size_t)255;
+    for (int pass = 0; pass < 2; ++pass) {
+      auto it = freeb.lower_bound(bytes);
+      if (it != freeb.end() && it->first <= bytes + bytes / 4 + (1u << 20)) {
+        *p = it->second;
+        freeb.erase(it);
+        return cudaSuccess;
+      }
+      if (pass == 0 && !pending.empty()) {
+        cudaError_t e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return e;
+        freeb.insert(pending.begin(), pending.end());
+        pending.clear();
+      }
+    }
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e == cudaErrorMemoryAllocation) {  // give back the cache, retry once
+      cudaGetLastError();
+      cudaStreamSynchronize(s);
+      release_free();
+      for (auto& f : pending) {
+        cudaFree(f.second);
+        size.erase(f.second);
+      }
+      pending.clear();
+      e = cudaMalloc(p, bytes);
+    }
+    if (e == cudaSuccess) size[*p] = bytes;
+    return e;
+  }
+  void free(void* p) {
+    auto it = size.find(p);
+    if (it == size.end()) return;
+    pending.insert({it->second, p});
+  }
+  void release_free() {
+    for (auto& f : freeb) {
+      cudaFree(f.second);
+      size.erase(f.second);
+    }
+    freeb.clear();
+  }
+  void release_all() {
+    for (auto& f : size) cudaFree(f.first);
+    size.clear();
+    freeb.clear();
+    pending.clear();
+  }
+};
+
 struct hodlr_handle_s {
+  DevPool pool;
   int n = 0, leaf = 30, dim = 0;
   bool dense = false;
   hx_kparams kp{};
@@ -162,54 +222,54 @@ int cuda_fail(hodlr_t h, cudaError_t e, const char* where) {
   } while (0)
 
 template <class T>
-cudaError_t dalloc(T** p, size_t count) {
+cudaError_t dalloc(hodlr_t h, T** p, size_t count) {
   *p = nullptr;
   if (count == 0) return cudaSuccess;
-  return cudaMalloc((void**)p, sizeof(T) * count);
+  return h->pool.alloc((void**)p, sizeof(T) * count, h->stream);
 }
 
 template <class T>
-void dfree(T*& p) {
-  if (p) cudaFree((void*)p);
+void dfree(hodlr_t h, T*& p) {
+  if (p) h->pool.free((void*)p);
   p = nullptr;
 }
 
-void free_plan(DevPlan& p) {
-  dfree(p.probs);
-  dfree(p.tiles);
+void free_plan(hodlr_t h, DevPlan& p) {
+  dfree(h, p.probs);
+  dfree(h, p.tiles);
   p = DevPlan();
 }
 
 void free_factor(hodlr_t h) {
   for (auto& L : h->lv) {
-    dfree(L.S);
-    dfree(L.piv);
-    dfree(L.d_nodes);
-    dfree(L.d_snodes);
-    free_plan(L.tn);
-    free_plan(L.nn);
-    free_plan(L.stn);
-    free_plan(L.snn);
+    dfree(h, L.S);
+    dfree(h, L.piv);
+    dfree(h, L.d_nodes);
+    dfree(h, L.d_snodes);
+    free_plan(h, L.tn);
+    free_plan(h, L.nn);
+    free_plan(h, L.stn);
+    free_plan(h, L.snn);
     L.solve_nrhs = -1;
     L.nodes.clear();
   }
-  dfree(h->d_lu);
-  dfree(h->d_lu_off);
-  dfree(h->d_perm);
-  dfree(h->Y);
+  dfree(h, h->d_lu);
+  dfree(h, h->d_lu_off);
+  dfree(h, h->d_perm);
+  dfree(h, h->Y);
   h->factored = false;
 }
 
 void free_compress(hodlr_t h) {
   free_factor(h);
   for (auto& L : h->lv) {
-    dfree(L.W);
-    dfree(L.V);
-    dfree(L.cR);
-    dfree(L.cC);
-    dfree(L.prow);
-    dfree(L.pcol);
-    dfree(L.d_st);
+    dfree(h, L.W);
+    dfree(h, L.V);
+    dfree(h, L.cR);
+    dfree(h, L.cC);
+    dfree(h, L.prow);
+    dfree(h, L.pcol);
+    dfree(h, L.d_st);
     L.st.clear();
     L.kcap = 0;
   }
@@ -289,8 +349,8 @@ void build_tree(hodlr_t h) {
 
 int ensure_ws(hodlr_t h, int64_t elems) {
   if (elems <= h->ws_cap) return HODLR_OK;
-  dfree(h->ws);
-  CK(dalloc(&h->ws, (size_t)elems));
+  dfree(h, h->ws);
+  CK(dalloc(h, &h->ws, (size_t)elems));
   h->ws_cap = elems;
   return HODLR_OK;
 }
@@ -320,10 +380,10 @@ EntrySrc make_src(hodlr_t h) {
 int grow_level(hodlr_t h, Level& L, int cap) {
   const int64_t N = h->n;
   double *W2 = nullptr, *V2 = nullptr;
-  CK(dalloc(&W2, (size_t)(N * cap)));
-  cudaError_t e = dalloc(&V2, (size_t)(N * cap));
+  CK(dalloc(h, &W2, (size_t)(N * cap)));
+  cudaError_t e = dalloc(h, &V2, (size_t)(N * cap));
   if (e != cudaSuccess) {
-    dfree(W2);
+    dfree(h, W2);
     return cuda_fail(h, e, "grow_level");
   }
   if (L.W && L.kcap > 0) {
@@ -331,8 +391,8 @@ int grow_level(hodlr_t h, Level& L, int cap) {
     CK(cudaMemcpyAsync(V2, L.V, sizeof(double) * N * L.kcap, cudaMemcpyDeviceToDevice, h->stream));
   }
   CK(cudaStreamSynchronize(h->stream));
-  dfree(L.W);
-  dfree(L.V);
+  dfree(h, L.W);
+  dfree(h, L.V);
   L.W = W2;
   L.V = V2;
   L.kcap = cap;
@@ -369,8 +429,8 @@ int run_aca(hodlr_t h, std::vector<AcaBlock>& blocks, int G, int nt, int kcap_ma
   const int nb = (int)blocks.size();
   if (nb == 0) return HODLR_OK;
   if (nb > h->blocks_cap) {
-    dfree(h->d_blocks);
-    CK(dalloc(&h->d_blocks, (size_t)nb));
+    dfree(h, h->d_blocks);
+    CK(dalloc(h, &h->d_blocks, (size_t)nb));
     h->blocks_cap = nb;
   }
   CK(cudaMemcpyAsync(h->d_blocks, blocks.data(), sizeof(AcaBlock) * nb, cudaMemcpyHostToDevice,
@@ -378,13 +438,13 @@ int run_aca(hodlr_t h, std::vector<AcaBlock>& blocks, int G, int nt, int kcap_ma
   int64_t stride = 12 + 4 * (int64_t)kcap_max;  // args + two banks of dots and norms
   int64_t need = stride * nb * G;
   if (need > h->part_cap) {
-    dfree(h->part);
-    CK(dalloc(&h->part, (size_t)need));
+    dfree(h, h->part);
+    CK(dalloc(h, &h->part, (size_t)need));
     h->part_cap = need;
   }
   if (nb > h->bar_cap) {
-    dfree(h->bar);
-    CK(dalloc(&h->bar, (size_t)nb));
+    dfree(h, h->bar);
+    CK(dalloc(h, &h->bar, (size_t)nb));
     h->bar_cap = nb;
   }
   CK(cudaMemsetAsync(h->bar, 0, sizeof(unsigned) * nb, h->stream));
@@ -416,109 +476,159 @@ int run_aca(hodlr_t h, std::vector<AcaBlock>& blocks, int G, int nt, int kcap_ma
   return check_dev_err(h, "ACA");
 }
 
-int do_compress(hodlr_t h) {
-  if (h->compressed) return HODLR_OK;
-  free_compress(h);
+// Allocate the per-level arrays of level L with `cap` low-rank columns.
+int init_level(hodlr_t h, Level& L, int cap) {
   const int64_t N = h->n;
-  h->aca_launches = 0;
-  h->aca_seconds = 0;
-  h->aca_bytes = 0;
-  const int init_cap = 64;
-  for (size_t l = 0; l < h->lv.size(); ++l) {
-    Level& L = h->lv[l];
-    int want = (l < h->cap_hint.size() && h->cap_hint[l] > 0) ? h->cap_hint[l] : init_cap;
-    int cap = std::max(1, std::min(L.ub_max, want));
+  int rc = grow_level(h, L, std::max(1, std::min(L.ub_max, cap)));
+  if (rc) return rc;
+  CK(dalloc(h, &L.cR, (size_t)N));
+  CK(dalloc(h, &L.cC, (size_t)N));
+  CK(dalloc(h, &L.prow, (size_t)N));
+  CK(dalloc(h, &L.pcol, (size_t)N));
+  CK(cudaMemsetAsync(L.cR, 0, N, h->stream));
+  CK(cudaMemsetAsync(L.cC, 0, N, h->stream));
+  const int nb = L.nblocks();
+  CK(dalloc(h, &L.d_st, (size_t)nb));
+  L.st.assign(nb, AcaState());
+  for (auto& s : L.st) {
+    s.frob2 = 0;
+    s.eps = 1;
+    s.margin = HUGE_VAL;
+    s.swp = s.svp = 0;
+    s.k = 0;
+    s.cur = 0;
+    s.status = ACA_RUNNING;
+    s.iters = 0;
+    s.rank = 0;
+    s.near = 0;
+    s.pending = 0;
+    s.pad = 0;
+  }
+  CK(cudaMemcpyAsync(L.d_st, L.st.data(), sizeof(AcaState) * nb, cudaMemcpyHostToDevice,
+                     h->stream));
+  return HODLR_OK;
+}
+
+// Read the level's block states back; grow the level where blocks paused for
+// capacity and re-arm them.  *done = every block of the level finished.
+int sync_level(hodlr_t h, Level& L, bool* done) {
+  const int nb = L.nblocks();
+  CK(cudaMemcpyAsync(L.st.data(), L.d_st, sizeof(AcaState) * nb, cudaMemcpyDeviceToHost,
+                     h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  int need = 0;
+  *done = true;
+  for (auto& s : L.st) {
+    if (s.status == ACA_ERROR) return fail(h, HODLR_ERR_TIMEOUT, "ACA group failed");
+    if (s.status == ACA_NEED_CAP) need = std::max(need, L.kcap + std::max(32, L.kcap / 2));
+    if (s.status == ACA_NEED_CAP_POST) need = std::max(need, s.rank);
+    if (s.status != ACA_DONE) *done = false;
+  }
+  if (need > 0) {
+    int cap = std::min(std::max(need, L.kcap + 1), std::max(L.ub_max, L.kcap + 1));
     int rc = grow_level(h, L, cap);
     if (rc) return rc;
-    CK(dalloc(&L.cR, (size_t)N));
-    CK(dalloc(&L.cC, (size_t)N));
-    CK(dalloc(&L.prow, (size_t)N));
-    CK(dalloc(&L.pcol, (size_t)N));
-    CK(cudaMemsetAsync(L.cR, 0, N, h->stream));
-    CK(cudaMemsetAsync(L.cC, 0, N, h->stream));
-    const int nb = L.nblocks();
-    CK(dalloc(&L.d_st, (size_t)nb));
-    L.st.assign(nb, AcaState());
     for (auto& s : L.st) {
-      s.frob2 = 0;
-      s.eps = 1;
-      s.margin = HUGE_VAL;
-      s.k = 0;
-      s.cur = 0;
-      s.status = ACA_RUNNING;
-      s.iters = 0;
-      s.rank = 0;
-      s.near = 0;
-      s.swp = s.svp = 0;
-      s.pending = 0;
-      s.pad = 0;
+      if (s.status == ACA_NEED_CAP) s.status = ACA_RUNNING;
+      if (s.status == ACA_NEED_CAP_POST) s.status = ACA_POST;
     }
     CK(cudaMemcpyAsync(L.d_st, L.st.data(), sizeof(AcaState) * nb, cudaMemcpyHostToDevice,
                        h->stream));
   }
-  for (int round = 0; round < 64; ++round) {
+  return HODLR_OK;
+}
+
+int level_kmax(const Level& L) {
+  int k = 0;
+  for (auto& s : L.st) k = std::max(k, s.rank);
+  return k;
+}
+
+// storeLRinTree (src/HODLR_Matrix.cpp:257-272,274-430) for every block.
+// Levels with many blocks run together in one launch, one CTA per block
+// (G = 1); the top levels, with few large blocks, run one cooperative launch
+// each with a group of CTAs per block.  They go bottom-up so that each
+// level's W/V capacity can be sized from the ranks of the level below it
+// (ranks shrink down the tree); a level that needs more grows and resumes.
+int do_compress(hodlr_t h) {
+  if (h->compressed) return HODLR_OK;
+  free_compress(h);
+  h->aca_launches = 0;
+  h->aca_seconds = 0;
+  h->aca_bytes = 0;
+  const int nlev = (int)h->lv.size();
+  auto hint = [&](int l) {
+    return (l < (int)h->cap_hint.size() && h->cap_hint[l] > 0) ? h->cap_hint[l] : 0;
+  };
+  int per_sm = 0;
+  if (aca_max_coresident(256, 256, &per_sm))
+    return fail(h, HODLR_ERR_CUDA, "occupancy query failed");
+  const int P0 = std::max(1, per_sm) * h->num_sms;
+  std::vector<int> pooled_levels, group_levels;
+  for (int l = 0; l < nlev; ++l)
+    (h->lv[l].nblocks() * 2 > P0 ? pooled_levels : group_levels).push_back(l);
+  // 1. the many-block levels, together
+  for (int l : pooled_levels) {
+    int rc = init_level(h, h->lv[l], hint(l) ? hint(l) : 64);
+    if (rc) return rc;
+  }
+  for (int round = 0; round < 64 && !pooled_levels.empty(); ++round) {
     int kcap_max = 1;
-    for (auto& L : h->lv) kcap_max = std::max(kcap_max, L.kcap);
-    int per_sm256 = 0, per_sm128 = 0;
-    if (aca_max_coresident(256, kcap_max, &per_sm256) ||
-        aca_max_coresident(128, kcap_max, &per_sm128))
-      return fail(h, HODLR_ERR_CUDA, "occupancy query failed");
-    const int P = std::max(1, per_sm256) * h->num_sms;
-    std::vector<AcaBlock> pooled;
-    std::vector<std::pair<int64_t, AcaBlock>> pooled_sorted;
-    for (auto& L : h->lv) {
-      if (level_done(L)) continue;
-      const int nb = L.nblocks();
-      int G = P / nb;
-      if (G >= 2) {
-        L.G = G;
-        std::vector<AcaBlock> bl(nb);
-        for (int q = 0; q < nb; ++q) fill_block(h, L, q, bl[q]);
-        int rc = run_aca(h, bl, G, 256, kcap_max);
-        if (rc) return rc;
-      } else {
-        L.G = 1;
-        for (int q = 0; q < nb; ++q) {
-          if (L.st[q].status == ACA_DONE) continue;
-          AcaBlock B;
-          fill_block(h, L, q, B);
-          pooled_sorted.push_back({(int64_t)B.m * B.n, B});
-        }
+    std::vector<std::pair<int64_t, AcaBlock>> sorted;
+    for (int l : pooled_levels) {
+      Level& L = h->lv[l];
+      kcap_max = std::max(kcap_max, L.kcap);
+      L.G = 1;
+      for (int q = 0; q < L.nblocks(); ++q) {
+        if (L.st[q].status == ACA_DONE) continue;
+        AcaBlock B;
+        fill_block(h, L, q, B);
+        sorted.push_back({(int64_t)B.m * B.n, B});
       }
     }
-    std::stable_sort(pooled_sorted.begin(), pooled_sorted.end(),
+    if (sorted.empty()) break;
+    std::stable_sort(sorted.begin(), sorted.end(),
                      [](const std::pair<int64_t, AcaBlock>& a,
                         const std::pair<int64_t, AcaBlock>& b) { return a.first > b.first; });
-    for (auto& pb : pooled_sorted) pooled.push_back(pb.second);
-    if (!pooled.empty()) {
-      int rc = run_aca(h, pooled, 1, 128, kcap_max);
+    std::vector<AcaBlock> blocks;
+    for (auto& pb : sorted) blocks.push_back(pb.second);
+    int rc = run_aca(h, blocks, 1, 128, kcap_max);
+    if (rc) return rc;
+    bool all = true;
+    for (int l : pooled_levels) {
+      bool done;
+      rc = sync_level(h, h->lv[l], &done);
       if (rc) return rc;
+      all &= done;
     }
-    // read back states, grow where needed
-    bool all_done = true;
-    for (auto& L : h->lv) {
+    if (all) break;
+  }
+  // 2. the few-block levels, deepest first
+  int kmax_below = 0;
+  if (!pooled_levels.empty()) kmax_below = level_kmax(h->lv[pooled_levels.front()]);
+  for (auto it = group_levels.rbegin(); it != group_levels.rend(); ++it) {
+    const int l = *it;
+    Level& L = h->lv[l];
+    int guess = hint(l) ? hint(l) : std::max(64, (kmax_below * 3 + 1) / 2 + 16);
+    int rc = init_level(h, L, guess);
+    if (rc) return rc;
+    for (int round = 0; round < 64; ++round) {
+      int ps = 0;
+      if (aca_max_coresident(256, L.kcap, &ps))
+        return fail(h, HODLR_ERR_CUDA, "occupancy query failed");
       const int nb = L.nblocks();
-      CK(cudaMemcpy(L.st.data(), L.d_st, sizeof(AcaState) * nb, cudaMemcpyDeviceToHost));
-      int need = 0;
-      for (int q = 0; q < nb; ++q) {
-        auto& s = L.st[q];
-        if (s.status == ACA_ERROR) return fail(h, HODLR_ERR_TIMEOUT, "ACA group failed");
-        if (s.status == ACA_NEED_CAP) need = std::max(need, L.kcap * 2);
-        if (s.status == ACA_NEED_CAP_POST) need = std::max(need, s.rank);
-        if (s.status != ACA_DONE) all_done = false;
-      }
-      if (need > 0) {
-        int cap = std::min(std::max(need, L.kcap + 1), std::max(L.ub_max, L.kcap + 1));
-        int rc = grow_level(h, L, cap);
-        if (rc) return rc;
-        for (auto& s : L.st) {
-          if (s.status == ACA_NEED_CAP) s.status = ACA_RUNNING;
-          if (s.status == ACA_NEED_CAP_POST) s.status = ACA_POST;
-        }
-        CK(cudaMemcpy(L.d_st, L.st.data(), sizeof(AcaState) * nb, cudaMemcpyHostToDevice));
-      }
+      const int G = std::max(1, std::max(1, ps) * h->num_sms / nb);
+      L.G = G;
+      std::vector<AcaBlock> bl(nb);
+      for (int q = 0; q < nb; ++q) fill_block(h, L, q, bl[q]);
+      rc = run_aca(h, bl, G, G > 1 ? 256 : 128, L.kcap);
+      if (rc) return rc;
+      bool done;
+      rc = sync_level(h, L, &done);
+      if (rc) return rc;
+      if (done) break;
     }
-    if (all_done) break;
+    kmax_below = level_kmax(L);
   }
   for (auto& L : h->lv)
     if (!level_done(L)) return fail(h, HODLR_ERR_STATE, "ACA did not converge in 64 rounds");
@@ -549,19 +659,19 @@ int upload_plan(hodlr_t h, std::vector<GemmProblem>& probs, bool split, DevPlan&
   std::vector<int4> tiles;
   int64_t ws = 0;
   gemm_plan(probs, tiles, ws, split, 2 * h->num_sms * 4);
-  free_plan(out);
+  free_plan(h, out);
   out.nprob = (int)probs.size();
   out.ntiles = (int)tiles.size();
   out.ws_elems = ws;
   out.any_split = false;
   for (auto& p : probs) out.any_split |= p.splits > 1;
   if (out.nprob) {
-    CK(dalloc(&out.probs, (size_t)out.nprob));
+    CK(dalloc(h, &out.probs, (size_t)out.nprob));
     CK(cudaMemcpy(out.probs, probs.data(), sizeof(GemmProblem) * out.nprob,
                   cudaMemcpyHostToDevice));
   }
   if (out.ntiles) {
-    CK(dalloc(&out.tiles, (size_t)out.ntiles));
+    CK(dalloc(h, &out.tiles, (size_t)out.ntiles));
     CK(cudaMemcpy(out.tiles, tiles.data(), sizeof(int4) * out.ntiles, cudaMemcpyHostToDevice));
   }
   return ensure_ws(h, ws);
@@ -594,9 +704,9 @@ int do_factorize(hodlr_t h) {
     lu_off[p] = tot;
     tot += (int64_t)h->leaf_size[p] * h->leaf_size[p];
   }
-  CK(dalloc(&h->d_lu, (size_t)tot));
-  CK(dalloc(&h->d_lu_off, (size_t)nl));
-  CK(dalloc(&h->d_perm, (size_t)N));
+  CK(dalloc(h, &h->d_lu, (size_t)tot));
+  CK(dalloc(h, &h->d_lu_off, (size_t)nl));
+  CK(dalloc(h, &h->d_perm, (size_t)N));
   CK(cudaMemcpyAsync(h->d_lu_off, lu_off.data(), sizeof(int64_t) * nl, cudaMemcpyHostToDevice,
                      h->stream));
   {
@@ -614,7 +724,7 @@ int do_factorize(hodlr_t h) {
   }
   // Y = [U panels of every level], zero padded
   if (h->C > 0) {
-    CK(dalloc(&h->Y, (size_t)(N * h->C)));
+    CK(dalloc(h, &h->Y, (size_t)(N * h->C)));
     CK(cudaMemsetAsync(h->Y, 0, sizeof(double) * N * h->C, h->stream));
     for (auto& L : h->lv) {
       const int nb = L.nblocks();
@@ -627,9 +737,9 @@ int do_factorize(hodlr_t h) {
         rk[q] = level_rank(L, q);
       }
       int *d_r0 = nullptr, *d_m = nullptr, *d_rk = nullptr;
-      CK(dalloc(&d_r0, nb));
-      CK(dalloc(&d_m, nb));
-      CK(dalloc(&d_rk, nb));
+      CK(dalloc(h, &d_r0, nb));
+      CK(dalloc(h, &d_m, nb));
+      CK(dalloc(h, &d_rk, nb));
       CK(cudaMemcpyAsync(d_r0, r0s.data(), 4 * nb, cudaMemcpyHostToDevice, h->stream));
       CK(cudaMemcpyAsync(d_m, ms.data(), 4 * nb, cudaMemcpyHostToDevice, h->stream));
       CK(cudaMemcpyAsync(d_rk, rk.data(), 4 * nb, cudaMemcpyHostToDevice, h->stream));
@@ -640,9 +750,9 @@ int do_factorize(hodlr_t h) {
       CK(cudaGetLastError());
       h->nlaunch += 1;
       CK(cudaStreamSynchronize(h->stream));
-      dfree(d_r0);
-      dfree(d_m);
-      dfree(d_rk);
+      dfree(h, d_r0);
+      dfree(h, d_m);
+      dfree(h, d_rk);
     }
     // leaf solves on every column: Y <- blockdiag(leaf LU)^-1 Y
     LeafSolveLaunch S;
@@ -681,14 +791,14 @@ int do_factorize(hodlr_t h) {
       sn.p_off = p_tot;
       p_tot += sd;
     }
-    CK(dalloc(&L.S, (size_t)s_tot));
-    CK(dalloc(&L.piv, (size_t)p_tot));
-    CK(dalloc(&L.d_nodes, (size_t)nn));
+    CK(dalloc(h, &L.S, (size_t)s_tot));
+    CK(dalloc(h, &L.piv, (size_t)p_tot));
+    CK(dalloc(h, &L.d_nodes, (size_t)nn));
     CK(cudaMemcpyAsync(L.d_nodes, L.nodes.data(), sizeof(SchurNode) * nn,
                        cudaMemcpyHostToDevice, h->stream));
     if (z_tot > h->z_cap) {
-      dfree(h->Z);
-      CK(dalloc(&h->Z, (size_t)z_tot));
+      dfree(h, h->Z);
+      CK(dalloc(h, &h->Z, (size_t)z_tot));
       h->z_cap = z_tot;
     }
     // Z_h = V_h^T Y[rows_h, 0 : coff + rank(U_h)]
@@ -796,13 +906,13 @@ int build_solve_plans(hodlr_t h, int nrhs) {
     zs_tot = std::max(zs_tot, t);
   }
   if (zs_tot > h->zs_cap) {
-    dfree(h->zs);
-    CK(dalloc(&h->zs, (size_t)zs_tot));
+    dfree(h, h->zs);
+    CK(dalloc(h, &h->zs, (size_t)zs_tot));
     h->zs_cap = zs_tot;
   }
   if (nrhs > h->x_cols) {
-    dfree(h->X);
-    CK(dalloc(&h->X, (size_t)(N * nrhs)));
+    dfree(h, h->X);
+    CK(dalloc(h, &h->X, (size_t)(N * nrhs)));
     h->x_cols = nrhs;
   }
   for (auto& L : h->lv) {
@@ -814,8 +924,8 @@ int build_solve_plans(hodlr_t h, int nrhs) {
       s.r_off = off;
       off += (int64_t)(s.kb + s.kt) * nrhs;
     }
-    dfree(L.d_snodes);
-    CK(dalloc(&L.d_snodes, (size_t)nn));
+    dfree(h, L.d_snodes);
+    CK(dalloc(h, &L.d_snodes, (size_t)nn));
     CK(cudaMemcpy(L.d_snodes, sn.data(), sizeof(SchurNode) * nn, cudaMemcpyHostToDevice));
     std::vector<GemmProblem> tn, up;
     for (int p = 0; p < nn; ++p) {
@@ -1012,14 +1122,14 @@ int refine_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double* d_x, 
   int rc = build_solve_plans(h, nrhs);
   if (rc) return rc;
   if (nrhs > h->ir_cols) {
-    dfree(h->ir_b);
-    dfree(h->ir_x);
-    dfree(h->ir_y);
-    dfree(h->ir_part);
-    CK(dalloc(&h->ir_b, (size_t)(N * nrhs)));
-    CK(dalloc(&h->ir_x, (size_t)(N * nrhs)));
-    CK(dalloc(&h->ir_y, (size_t)(N * nrhs)));
-    CK(dalloc(&h->ir_part, (size_t)(2 * nrhs * IR_BLOCKS)));
+    dfree(h, h->ir_b);
+    dfree(h, h->ir_x);
+    dfree(h, h->ir_y);
+    dfree(h, h->ir_part);
+    CK(dalloc(h, &h->ir_b, (size_t)(N * nrhs)));
+    CK(dalloc(h, &h->ir_x, (size_t)(N * nrhs)));
+    CK(dalloc(h, &h->ir_y, (size_t)(N * nrhs)));
+    CK(dalloc(h, &h->ir_part, (size_t)(2 * nrhs * IR_BLOCKS)));
     h->ir_cols = nrhs;
   }
   CK(cudaMemcpy2DAsync(h->ir_b, sizeof(double) * N, d_b, sizeof(double) * ldb,
@@ -1180,25 +1290,25 @@ int gmres_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double* d_x, i
   int rc = build_solve_plans(h, nrhs);
   if (rc) return rc;
   if (nrhs > h->ir_cols) {
-    dfree(h->ir_b);
-    dfree(h->ir_x);
-    dfree(h->ir_y);
-    dfree(h->ir_part);
-    CK(dalloc(&h->ir_b, (size_t)(N * nrhs)));
-    CK(dalloc(&h->ir_x, (size_t)(N * nrhs)));
-    CK(dalloc(&h->ir_y, (size_t)(N * nrhs)));
-    CK(dalloc(&h->ir_part, (size_t)(2 * nrhs * IR_BLOCKS)));
+    dfree(h, h->ir_b);
+    dfree(h, h->ir_x);
+    dfree(h, h->ir_y);
+    dfree(h, h->ir_part);
+    CK(dalloc(h, &h->ir_b, (size_t)(N * nrhs)));
+    CK(dalloc(h, &h->ir_x, (size_t)(N * nrhs)));
+    CK(dalloc(h, &h->ir_y, (size_t)(N * nrhs)));
+    CK(dalloc(h, &h->ir_part, (size_t)(2 * nrhs * IR_BLOCKS)));
     h->ir_cols = nrhs;
   }
   if (m > h->gm_m || nrhs > h->gm_cols) {
-    dfree(h->gm_V);
-    dfree(h->gm_Z);
-    dfree(h->gm_h);
-    dfree(h->gm_part);
-    CK(dalloc(&h->gm_V, (size_t)((m + 1) * N * nrhs)));
-    CK(dalloc(&h->gm_Z, (size_t)(m * N * nrhs)));
-    CK(dalloc(&h->gm_h, (size_t)((m + 2) * nrhs)));
-    CK(dalloc(&h->gm_part, (size_t)((m + 2) * nrhs * GM_BLOCKS)));
+    dfree(h, h->gm_V);
+    dfree(h, h->gm_Z);
+    dfree(h, h->gm_h);
+    dfree(h, h->gm_part);
+    CK(dalloc(h, &h->gm_V, (size_t)((m + 1) * N * nrhs)));
+    CK(dalloc(h, &h->gm_Z, (size_t)(m * N * nrhs)));
+    CK(dalloc(h, &h->gm_h, (size_t)((m + 2) * nrhs)));
+    CK(dalloc(h, &h->gm_part, (size_t)((m + 2) * nrhs * GM_BLOCKS)));
     h->gm_m = m;
     h->gm_cols = nrhs;
   }
@@ -1356,13 +1466,13 @@ int init_common(hodlr_t h) {
   h->stream = h->own_stream;
   CK(cudaEventCreate(&h->ev0));
   CK(cudaEventCreate(&h->ev1));
-  CK(dalloc(&h->d_err, 1));
+  CK(dalloc(h, &h->d_err, 1));
   CK(cudaMemset(h->d_err, 0, sizeof(unsigned)));
   build_tree(h);
   const int nl = (int)h->leaf_min.size();
   if (h->smax > 160) return fail(h, HODLR_ERR_UNSUPPORTED, "leaf size above 160");
-  CK(dalloc(&h->d_leaf_min, (size_t)nl));
-  CK(dalloc(&h->d_leaf_size, (size_t)nl));
+  CK(dalloc(h, &h->d_leaf_min, (size_t)nl));
+  CK(dalloc(h, &h->d_leaf_size, (size_t)nl));
   CK(cudaMemcpy(h->d_leaf_min, h->leaf_min.data(), 4 * nl, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(h->d_leaf_size, h->leaf_size.data(), 4 * nl, cudaMemcpyHostToDevice));
   return HODLR_OK;
@@ -1387,7 +1497,7 @@ int hodlr_create_kernel(hodlr_t* out, int n, int dim, const double* pts,
                           k->diag_value);
   int rc = init_common(h);
   if (!rc) {
-    cudaError_t e = dalloc(&h->d_pts, (size_t)n * dim);
+    cudaError_t e = dalloc(h, &h->d_pts, (size_t)n * dim);
     if (e == cudaSuccess)
       e = cudaMemcpy(h->d_pts, pts, sizeof(double) * (size_t)n * dim, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) rc = cuda_fail(h, e, "points upload");
@@ -1410,7 +1520,7 @@ int hodlr_create_dense(hodlr_t* out, int n, const double* A, int lda, int leaf_s
   h->dense = true;
   int rc = init_common(h);
   if (!rc) {
-    cudaError_t e = dalloc(&h->d_A, (size_t)n * n);
+    cudaError_t e = dalloc(h, &h->d_A, (size_t)n * n);
     if (e == cudaSuccess)
       e = cudaMemcpy2D(h->d_A, sizeof(double) * n, A, sizeof(double) * lda, sizeof(double) * n,
                        n, cudaMemcpyHostToDevice);
@@ -1438,28 +1548,30 @@ int hodlr_create_fnptr(hodlr_t* out, int rows, int cols, double (*kernel)(int, i
 void hodlr_destroy(hodlr_t h) {
   if (!h) return;
   free_compress(h);
-  dfree(h->d_pts);
-  dfree(h->d_A);
-  dfree(h->d_leaf_min);
-  dfree(h->d_leaf_size);
-  dfree(h->ws);
-  dfree(h->Z);
-  dfree(h->X);
-  dfree(h->zs);
-  dfree(h->ir_b);
-  dfree(h->ir_x);
-  dfree(h->ir_y);
-  dfree(h->ir_part);
-  dfree(h->gm_V);
-  dfree(h->gm_Z);
-  dfree(h->gm_h);
-  dfree(h->gm_part);
-  dfree(h->part);
-  dfree(h->bar);
-  dfree(h->d_blocks);
-  dfree(h->d_err);
+  dfree(h, h->d_pts);
+  dfree(h, h->d_A);
+  dfree(h, h->d_leaf_min);
+  dfree(h, h->d_leaf_size);
+  dfree(h, h->ws);
+  dfree(h, h->Z);
+  dfree(h, h->X);
+  dfree(h, h->zs);
+  dfree(h, h->ir_b);
+  dfree(h, h->ir_x);
+  dfree(h, h->ir_y);
+  dfree(h, h->ir_part);
+  dfree(h, h->gm_V);
+  dfree(h, h->gm_Z);
+  dfree(h, h->gm_h);
+  dfree(h, h->gm_part);
+  dfree(h, h->part);
+  dfree(h, h->bar);
+  dfree(h, h->d_blocks);
+  dfree(h, h->d_err);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  h->pool.release_all();
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
   delete h;
 }
@@ -1606,10 +1718,10 @@ int hodlr_iterative_solve(hodlr_t h, int nrhs, const double* b, int ldb, double*
   if (!h || nrhs < 1 || !b || !x || ldb < h->n || ldx < h->n) return HODLR_ERR_ARG;
   const int64_t N = h->n;
   double *db = nullptr, *dx = nullptr;
-  CK(dalloc(&db, (size_t)(N * nrhs)));
-  cudaError_t e = dalloc(&dx, (size_t)(N * nrhs));
+  CK(dalloc(h, &db, (size_t)(N * nrhs)));
+  cudaError_t e = dalloc(h, &dx, (size_t)(N * nrhs));
   if (e != cudaSuccess) {
-    dfree(db);
+    dfree(h, db);
     return cuda_fail(h, e, "gmres alloc");
   }
   int rc = HODLR_OK;
@@ -1622,8 +1734,8 @@ int hodlr_iterative_solve(hodlr_t h, int nrhs, const double* b, int ldb, double*
       e = cudaMemcpy2D(x, sizeof(double) * ldx, dx, sizeof(double) * N, sizeof(double) * N,
                        nrhs, cudaMemcpyDeviceToHost);
   }
-  dfree(db);
-  dfree(dx);
+  dfree(h, db);
+  dfree(h, dx);
   if (e != cudaSuccess) return cuda_fail(h, e, "gmres copy");
   return rc;
 }
@@ -1633,10 +1745,10 @@ int hodlr_solve_refined(hodlr_t h, int nrhs, const double* b, int ldb, double* x
   if (!h || nrhs < 1 || !b || !x || ldb < h->n || ldx < h->n) return HODLR_ERR_ARG;
   const int64_t N = h->n;
   double *db = nullptr, *dx = nullptr;
-  CK(dalloc(&db, (size_t)(N * nrhs)));
-  cudaError_t e = dalloc(&dx, (size_t)(N * nrhs));
+  CK(dalloc(h, &db, (size_t)(N * nrhs)));
+  cudaError_t e = dalloc(h, &dx, (size_t)(N * nrhs));
   if (e != cudaSuccess) {
-    dfree(db);
+    dfree(h, db);
     return cuda_fail(h, e, "refine alloc");
   }
   int rc = HODLR_OK;
@@ -1649,8 +1761,8 @@ int hodlr_solve_refined(hodlr_t h, int nrhs, const double* b, int ldb, double* x
       e = cudaMemcpy2D(x, sizeof(double) * ldx, dx, sizeof(double) * N, sizeof(double) * N,
                        nrhs, cudaMemcpyDeviceToHost);
   }
-  dfree(db);
-  dfree(dx);
+  dfree(h, db);
+  dfree(h, dx);
   if (e != cudaSuccess) return cuda_fail(h, e, "refine copy");
   return rc;
 }
@@ -1660,10 +1772,10 @@ int hodlr_residual(hodlr_t h, int nrhs, const double* b, int ldb, const double* 
   if (!h || nrhs < 1 || !b || !x || !relres || ldb < h->n || ldx < h->n) return HODLR_ERR_ARG;
   const int64_t N = h->n;
   double *dx = nullptr, *dy = nullptr;
-  CK(dalloc(&dx, (size_t)(N * nrhs)));
-  cudaError_t e = dalloc(&dy, (size_t)(N * nrhs));
+  CK(dalloc(h, &dx, (size_t)(N * nrhs)));
+  cudaError_t e = dalloc(h, &dy, (size_t)(N * nrhs));
   if (e != cudaSuccess) {
-    dfree(dx);
+    dfree(h, dx);
     return cuda_fail(h, e, "residual alloc");
   }
   int rc = HODLR_OK;
@@ -1677,8 +1789,8 @@ int hodlr_residual(hodlr_t h, int nrhs, const double* b, int ldb, const double* 
     }
     if (!rc) e = cudaMemcpy(y.data(), dy, sizeof(double) * N * nrhs, cudaMemcpyDeviceToHost);
   }
-  dfree(dx);
-  dfree(dy);
+  dfree(h, dx);
+  dfree(h, dy);
   if (e != cudaSuccess) return cuda_fail(h, e, "residual");
   if (rc) return rc;
   for (int c = 0; c < nrhs; ++c) {
