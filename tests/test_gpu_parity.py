@@ -222,3 +222,20 @@ def test_refinement_and_gmres_reach_residual_target():
     assert g.last_iterations <= it1
     # same solution of the same system
     assert np.linalg.norm(x1 - x2) / np.linalg.norm(x2) < 1e-7
+
+
+def test_cpp_facade_drop_in(tmp_path):
+    """include/HODLR_Matrix.hpp compiled with g++ against libhodlr_b200.so and
+    run: the reference's kernel-path test shape, a dense solve and
+    iterative_Solve through the C++ drop-in class."""
+    import os
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    exe = tmp_path / "facade_test"
+    subprocess.run(["g++", "-O2", "-std=c++17", os.path.join(root, "tests", "cpp", "facade_test.cpp"),
+                    "-I", os.path.join(root, "include"), "-L", os.path.join(root, "dense_hodlr_b200"),
+                    "-lhodlr_b200", "-Wl,-rpath," + os.path.join(root, "dense_hodlr_b200"),
+                    "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=600)
+    print(out.stdout)
+    assert out.returncode == 0, out.stdout + out.stderr
