@@ -68,6 +68,8 @@ SIGNATURES = {
     "hodlr_get_lowrank": (_I, [_H, _I, _PD, _PD]),
     "hodlr_get_block_margin": (_I, [_H, _I, _PD, _PI]),
     "hodlr_get_aca_stats": (_I, [_H, _PI, _PD, _PD]),
+    "hodlr_kernel_matvec_noalloc": (_I, [_I, _I, _V, ctypes.POINTER(KernelDesc), _I, _V, _I, _V,
+                                         _I, _V]),
     "hodlr_status_string": (ctypes.c_char_p, [_I]),
     "hodlr_last_error": (ctypes.c_char_p, [_H]),
 }

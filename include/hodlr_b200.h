@@ -176,6 +176,29 @@ int hodlr_set_capacity_hint(hodlr_t h, const int* caps, int nlevels);
 /* Number of kernels this handle has launched since it was created. */
 int hodlr_get_launch_count(hodlr_t h, long long* count);
 
+/* Full-kernel FP64 product d_y = K d_x that allocates no device memory.  It
+ * has no counterpart in the reference.  It is for callers that cannot call
+ * cudaMalloc when they need K x: code running while a stream is captured into
+ * a CUDA graph, and applications whose memory manager has already reserved
+ * the device memory.  Such callers cannot create a handle (handles allocate),
+ * so this call takes the points (d_pts, dim x n, SoA, device memory), X and
+ * Y as caller-owned device buffers and runs on `stream` (NULL: the default
+ * stream), returning after the stream has finished the product.  Its scratch
+ * is a file-scope device array of HODLR_NOALLOC_SPLITS * HODLR_NOALLOC_MAX_ELEMS
+ * doubles (16 MiB) that every GPU loading the library holds until exit; hence
+ * the limit n * nrhs <= HODLR_NOALLOC_MAX_ELEMS, beyond which the call
+ * returns HODLR_ERR_ARG without launching.  The first call on a device looks
+ * up the array's device address (cudaGetSymbolAddress, with that device
+ * current): make that first call before any stream capture begins.  All calls
+ * share the array and it keeps the last call's contents (nothing in it needs
+ * to start at zero); calls whose kernels overlap on the GPU race on it, so
+ * issue them on one stream or serialise them. */
+#define HODLR_NOALLOC_SPLITS 4
+#define HODLR_NOALLOC_MAX_ELEMS 524288
+int hodlr_kernel_matvec_noalloc(int n, int dim, const double* d_pts,
+                                const hodlr_kernel_desc* kernel, int nrhs, const double* d_x,
+                                int ldx, double* d_y, int ldy, void* stream);
+
 const char* hodlr_status_string(int status);
 const char* hodlr_last_error(hodlr_t h);
 
