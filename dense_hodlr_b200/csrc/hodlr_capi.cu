@@ -157,6 +157,7 @@ struct hodlr_handle_s {
   int minPivot = 0;
   std::vector<Level> lv;
   std::vector<int> cap_hint;  // initial W/V columns per level (0 = default)
+  int gemm_prec = HODLR_GEMM_FP64;  // arithmetic of the Woodbury products
   std::vector<int> leaf_min, leaf_size;
   int* d_leaf_min = nullptr;
   int* d_leaf_size = nullptr;
@@ -658,7 +659,10 @@ int do_compress(hodlr_t h) {
 int upload_plan(hodlr_t h, std::vector<GemmProblem>& probs, bool split, DevPlan& out) {
   std::vector<int4> tiles;
   int64_t ws = 0;
-  gemm_plan(probs, tiles, ws, split, 2 * h->num_sms * 4);
+  if (h->gemm_prec == HODLR_GEMM_FP64)
+    gemm_plan(probs, tiles, ws, split, 2 * h->num_sms * 4);
+  else
+    umma_plan(probs, tiles, ws, split, 2 * h->num_sms * 4);
   free_plan(h, out);
   out.nprob = (int)probs.size();
   out.ntiles = (int)tiles.size();
@@ -678,6 +682,24 @@ int upload_plan(hodlr_t h, std::vector<GemmProblem>& probs, bool split, DevPlan&
 }
 
 int level_rank(const Level& L, int q) { return L.st[q].rank; }
+
+// Launch a planned TN / NN-sub group in the handle's arithmetic.
+int run_tn(hodlr_t h, const DevPlan& P) {
+  if (P.ntiles == 0) return 0;
+  h->nlaunch += 1 + (P.any_split ? 1 : 0);
+  if (h->gemm_prec == HODLR_GEMM_FP64)
+    return gemm_tn_launch(P.probs, P.tiles, P.ntiles, P.nprob, h->ws, P.any_split, h->stream);
+  return umma_tn_launch(h->gemm_prec, P.probs, P.tiles, P.ntiles, P.nprob, h->ws, P.any_split,
+                        h->d_err, h->stream);
+}
+
+int run_nn(hodlr_t h, const DevPlan& P) {
+  if (P.ntiles == 0) return 0;
+  h->nlaunch += 1;
+  if (h->gemm_prec == HODLR_GEMM_FP64)
+    return gemm_nn_sub_launch(P.probs, P.tiles, P.ntiles, h->stream);
+  return umma_nn_sub_launch(h->gemm_prec, P.probs, P.tiles, P.ntiles, h->d_err, h->stream);
+}
 
 __global__ void y_init_kernel(double* Y, int64_t ldy, int coff, const double* W, int64_t ldw,
                               const int* r0s, const int* ms, const int* ranks, int nb) {
@@ -832,10 +854,8 @@ int do_factorize(hodlr_t h) {
     }
     int rc2 = upload_plan(h, tn, true, L.tn);
     if (rc2) return rc2;
-    int e = gemm_tn_launch(L.tn.probs, L.tn.tiles, L.tn.ntiles, L.tn.nprob, h->ws,
-                           L.tn.any_split, h->stream);
+    int e = run_tn(h, L.tn);
     if (e) return cuda_fail(h, (cudaError_t)e, "gemm_tn");
-    h->nlaunch += (L.tn.ntiles > 0) + (L.tn.ntiles > 0 && L.tn.any_split);
     SchurLaunch S;
     S.nodes = L.d_nodes;
     S.S = L.S;
@@ -881,9 +901,8 @@ int do_factorize(hodlr_t h) {
       }
       rc2 = upload_plan(h, up, false, L.nn);
       if (rc2) return rc2;
-      e = gemm_nn_sub_launch(L.nn.probs, L.nn.tiles, L.nn.ntiles, h->stream);
+      e = run_nn(h, L.nn);
       if (e) return cuda_fail(h, (cudaError_t)e, "gemm_nn_sub");
-      h->nlaunch += (L.nn.ntiles > 0);
     }
   }
   CK(cudaEventRecord(h->ev1, h->stream));
@@ -1003,10 +1022,8 @@ int solve_in_place(hodlr_t h, int nrhs) {
   for (int l = (int)h->lv.size() - 1; l >= 0; --l) {
     Level& L = h->lv[l];
     const int nn = (int)L.nmin.size();
-    e = gemm_tn_launch(L.stn.probs, L.stn.tiles, L.stn.ntiles, L.stn.nprob, h->ws,
-                       L.stn.any_split, h->stream);
+    e = run_tn(h, L.stn);
     if (e) return cuda_fail(h, (cudaError_t)e, "solve gemm_tn");
-    h->nlaunch += (L.stn.ntiles > 0) + (L.stn.ntiles > 0 && L.stn.any_split);
     SchurLaunch SL;
     SL.nodes = L.d_snodes;
     SL.S = L.S;
@@ -1016,9 +1033,9 @@ int solve_in_place(hodlr_t h, int nrhs) {
     SL.err = h->d_err;
     e = schur_solve_launch(SL, nn, nrhs, nrhs, L.max_sd, h->stream);
     if (e) return cuda_fail(h, (cudaError_t)e, "solve schur");
-    e = gemm_nn_sub_launch(L.snn.probs, L.snn.tiles, L.snn.ntiles, h->stream);
+    h->nlaunch += 1;
+    e = run_nn(h, L.snn);
     if (e) return cuda_fail(h, (cudaError_t)e, "solve gemm_nn");
-    h->nlaunch += 1 + (L.snn.ntiles > 0);
   }
   return HODLR_OK;
 }
@@ -1588,6 +1605,79 @@ int hodlr_set_stream(hodlr_t h, void* stream) {
   CK(cudaStreamSynchronize(h->stream));
   h->stream = stream ? (cudaStream_t)stream : h->own_stream;
   return HODLR_OK;
+}
+
+int hodlr_set_precision(hodlr_t h, int precision) {
+  if (!h || precision < HODLR_PRECISION_FP64 || precision > HODLR_PRECISION_BF16)
+    return HODLR_ERR_ARG;
+  if (precision != h->gemm_prec) {
+    h->gemm_prec = precision;  // enum values coincide with HODLR_GEMM_*
+    free_factor(h);            // the compression is unchanged
+  }
+  return HODLR_OK;
+}
+
+int hodlr_gemm_device(int precision, int mode, int m, int n, int k, const double* A, int lda,
+                      const double* B, int ldb, double* C, int ldc, void* stream) {
+  if (precision < HODLR_PRECISION_FP64 || precision > HODLR_PRECISION_BF16 || mode < 0 ||
+      mode > 1 || m < 0 || n < 0 || k < 0 || !A || !B || !C || ldc < m ||
+      lda < (mode == 0 ? k : m) || ldb < k)
+    return HODLR_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  std::vector<GemmProblem> probs(1);
+  GemmProblem& p = probs[0];
+  p = GemmProblem{};
+  p.A = A;
+  p.B = B;
+  p.C = C;
+  p.M = m;
+  p.N = n;
+  p.K = k;
+  p.lda = lda;
+  p.ldb = ldb;
+  p.ldc = ldc;
+  std::vector<int4> tiles;
+  int64_t ws = 0;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (precision == HODLR_PRECISION_FP64)
+    gemm_plan(probs, tiles, ws, mode == 0, 8 * sms);
+  else
+    umma_plan(probs, tiles, ws, mode == 0, 8 * sms);
+  GemmProblem* dp = nullptr;
+  int4* dt = nullptr;
+  double* dws = nullptr;
+  unsigned* derr = nullptr;
+  int rc = HODLR_OK;
+  if (cudaMalloc(&dp, sizeof(GemmProblem)) != cudaSuccess ||
+      (tiles.size() && cudaMalloc(&dt, sizeof(int4) * tiles.size()) != cudaSuccess) ||
+      (ws && cudaMalloc(&dws, sizeof(double) * ws) != cudaSuccess) ||
+      cudaMalloc(&derr, sizeof(unsigned)) != cudaSuccess)
+    rc = HODLR_ERR_ALLOC;
+  if (!rc) {
+    cudaMemcpy(dp, probs.data(), sizeof(GemmProblem), cudaMemcpyHostToDevice);
+    if (tiles.size())
+      cudaMemcpy(dt, tiles.data(), sizeof(int4) * tiles.size(), cudaMemcpyHostToDevice);
+    cudaMemset(derr, 0, sizeof(unsigned));
+    const bool split = probs[0].splits > 1;
+    int e;
+    if (precision == HODLR_PRECISION_FP64)
+      e = mode == 0 ? gemm_tn_launch(dp, dt, (int)tiles.size(), 1, dws, split, s)
+                    : gemm_nn_sub_launch(dp, dt, (int)tiles.size(), s);
+    else
+      e = mode == 0 ? umma_tn_launch(precision, dp, dt, (int)tiles.size(), 1, dws, split, derr, s)
+                    : umma_nn_sub_launch(precision, dp, dt, (int)tiles.size(), derr, s);
+    if (e || cudaStreamSynchronize(s) != cudaSuccess) rc = HODLR_ERR_CUDA;
+    unsigned he = 0;
+    if (!rc && cudaMemcpy(&he, derr, sizeof(unsigned), cudaMemcpyDeviceToHost) == cudaSuccess && he)
+      rc = HODLR_ERR_TIMEOUT;
+  }
+  cudaFree(dp);
+  cudaFree(dt);
+  cudaFree(dws);
+  cudaFree(derr);
+  return rc;
 }
 
 int hodlr_set_capacity_hint(hodlr_t h, const int* caps, int nlevels) {

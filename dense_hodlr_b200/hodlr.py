@@ -153,6 +153,11 @@ class HODLR_Matrix:
     def set_LRMethod(self, method):
         _check(self._h, _L.lib().hodlr_set_lr_method(self._h, method.encode()))
 
+    def set_precision(self, precision):
+        """'fp64' (default), 'tf32' or 'bf16' for the Woodbury products."""
+        code = {"fp64": 0, "tf32": 1, "bf16": 2}[precision] if isinstance(precision, str) else int(precision)
+        _check(self._h, _L.lib().hodlr_set_precision(self._h, code))
+
     def set_capacity_hint(self, caps):
         """Initial low-rank columns per inner level (results do not depend on it)."""
         a = np.ascontiguousarray(caps, dtype=np.int32)

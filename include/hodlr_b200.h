@@ -173,6 +173,24 @@ int hodlr_get_aca_stats(hodlr_t h, int* launches, double* seconds, double* bytes
  * (src/lowRank.cpp:151-157). */
 int hodlr_set_capacity_hint(hodlr_t h, const int* caps, int nlevels);
 
+/* Arithmetic of the Woodbury products (V^T K^-1 U, V^T X and the updates)
+ * in the factorization and the solve.  FP64 (default) reproduces the
+ * reference; TF32 and BF16 run them on the tcgen05 tensor cores with FP32
+ * accumulation (the mixed-precision form) while leaf and capacitance LUs,
+ * their pivoting and the full-kernel residual stay FP64; GMRES
+ * (hodlr_iterative_solve) recovers full accuracy.  Changing it discards the
+ * factorization, not the compression. */
+#define HODLR_PRECISION_FP64 0
+#define HODLR_PRECISION_TF32 1
+#define HODLR_PRECISION_BF16 2
+int hodlr_set_precision(hodlr_t h, int precision);
+
+/* One product in the given arithmetic, device pointers, column-major:
+ * mode 0: C (m x n) = A^T B, A is k x m;  mode 1: C (m x n) -= A B, A is m x k;
+ * B is k x n.  The Woodbury GEMM kernels as a utility (and their test hook). */
+int hodlr_gemm_device(int precision, int mode, int m, int n, int k, const double* A, int lda,
+                      const double* B, int ldb, double* C, int ldc, void* stream);
+
 /* Number of kernels this handle has launched since it was created. */
 int hodlr_get_launch_count(hodlr_t h, long long* count);
 
