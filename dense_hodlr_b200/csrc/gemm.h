@@ -7,7 +7,7 @@
 #include <vector>
 
 // Arithmetic of the tensor-core path (umma_gemm.cu).
-enum { HODLR_GEMM_FP64 = 0, HODLR_GEMM_TF32 = 1, HODLR_GEMM_BF16 = 2 };
+enum { HODLR_GEMM_FP64 = 0, HODLR_GEMM_TF32 = 1, HODLR_GEMM_BF16 = 2, HODLR_GEMM_TF32X3 = 3 };
 
 // One product of a group.  TN: C (M x N) = A^T B with A K x M, B K x N.
 // NN-sub: C (M x N) -= A B with A M x K, B K x N.  All column-major.

@@ -1608,7 +1608,7 @@ int hodlr_set_stream(hodlr_t h, void* stream) {
 }
 
 int hodlr_set_precision(hodlr_t h, int precision) {
-  if (!h || precision < HODLR_PRECISION_FP64 || precision > HODLR_PRECISION_BF16)
+  if (!h || precision < HODLR_PRECISION_FP64 || precision > HODLR_PRECISION_TF32X3)
     return HODLR_ERR_ARG;
   if (precision != h->gemm_prec) {
     h->gemm_prec = precision;  // enum values coincide with HODLR_GEMM_*
@@ -1619,7 +1619,7 @@ int hodlr_set_precision(hodlr_t h, int precision) {
 
 int hodlr_gemm_device(int precision, int mode, int m, int n, int k, const double* A, int lda,
                       const double* B, int ldb, double* C, int ldc, void* stream) {
-  if (precision < HODLR_PRECISION_FP64 || precision > HODLR_PRECISION_BF16 || mode < 0 ||
+  if (precision < HODLR_PRECISION_FP64 || precision > HODLR_PRECISION_TF32X3 || mode < 0 ||
       mode > 1 || m < 0 || n < 0 || k < 0 || !A || !B || !C || ldc < m ||
       lda < (mode == 0 ? k : m) || ldb < k)
     return HODLR_ERR_ARG;

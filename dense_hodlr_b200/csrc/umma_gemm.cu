@@ -8,7 +8,7 @@
 // issues tcgen05.mma with the accumulator in tensor memory (FP32), and the
 // epilogue reads it back with tcgen05.ld and writes / subtracts FP64.
 //
-// CTA tile 128 x 64, K in stages of 64, two stage buffers: the MMAs of one
+// CTA tile 128 x 64, K in stages of 64 (32 for 3xTF32), two stage buffers: the MMAs of one
 // stage run while the threads stage the next; an mbarrier signalled by
 // tcgen05.commit tells when a buffer may be overwritten.  Every wait is
 // bounded; on a timeout the kernel records DEV_ERR_TIMEOUT, waits (bounded)
@@ -22,10 +22,18 @@ namespace {
 
 constexpr int UM = 128;   // tile rows (= TMEM lanes)
 constexpr int UN = 64;    // tile columns (= TMEM columns, fp32)
-constexpr int UK = 64;    // K per stage
 constexpr int UNT = 128;  // 4 warps: one per TMEM lane quarter
 constexpr unsigned kWaitLimit = 1u << 22;
 
+__device__ __forceinline__ float to_tf32(float f) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(f));
+  return __uint_as_float(r);
+}
+
+// Operand formats.  `parts` = 2 splits each operand into a TF32 head and a
+// TF32 tail (x = hi + lo); the product is hi*hi + hi*lo + lo*hi, which keeps
+// about FP32 accuracy (the error-compensated "3xTF32" scheme).
 template <int PREC>
 struct Fmt;
 template <>
@@ -33,20 +41,39 @@ struct Fmt<HODLR_GEMM_BF16> {  // kind::f16 with BF16 operands
   using T = __nv_bfloat16;
   static constexpr int per16 = 8;  // elements per 16-byte chunk
   static constexpr int mmak = 16;  // K of one MMA
+  static constexpr int uk = 64;    // K per stage
+  static constexpr int parts = 1;
   static constexpr uint32_t code = 1;
-  static __device__ __forceinline__ T cvt(double x) { return __double2bfloat16(x); }
+  static __device__ __forceinline__ void cvt(double x, T* hi, T* lo) {
+    *hi = __double2bfloat16(x);
+    (void)lo;
+  }
 };
 template <>
 struct Fmt<HODLR_GEMM_TF32> {  // kind::tf32, fp32 storage rounded to tf32
   using T = float;
   static constexpr int per16 = 4;
   static constexpr int mmak = 8;
+  static constexpr int uk = 64;
+  static constexpr int parts = 1;
   static constexpr uint32_t code = 2;
-  static __device__ __forceinline__ T cvt(double x) {
-    float f = (float)x;
-    uint32_t r;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(f));
-    return __uint_as_float(r);
+  static __device__ __forceinline__ void cvt(double x, T* hi, T* lo) {
+    *hi = to_tf32((float)x);
+    (void)lo;
+  }
+};
+template <>
+struct Fmt<HODLR_GEMM_TF32X3> {
+  using T = float;
+  static constexpr int per16 = 4;
+  static constexpr int mmak = 8;
+  static constexpr int uk = 32;
+  static constexpr int parts = 2;
+  static constexpr uint32_t code = 2;
+  static __device__ __forceinline__ void cvt(double x, T* hi, T* lo) {
+    const float h = to_tf32((float)x);
+    *hi = h;
+    *lo = to_tf32((float)(x - (double)h));
   }
 };
 
@@ -77,16 +104,19 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
   return false;
 }
 
-// Stage rows [r0, r0+R) x k [k0, k0+UK) of an operand into a K-major tile.
+// Stage rows [r0, r0+R) x k [k0, k0+uk) of an operand into a K-major tile
+// (and, for split formats, its tail into tile + R * uk elements).
 // KCONTIG: element (r, k) at src[k + r * ld]; else at src[r + k * ld].
 template <int PREC, int R, bool KCONTIG>
 __device__ __forceinline__ void stage_tile(uint8_t* tile, const double* __restrict__ src,
                                            int64_t ld, int r0, int rlim, int k0, int klim) {
   using F = Fmt<PREC>;
   using T = typename F::T;
+  constexpr int UK = F::uk;
   constexpr int CPR = UK / F::per16;  // chunks per row
   constexpr int SBO = CPR * 128;
   constexpr int TASKS = R * CPR;
+  constexpr int PART_BYTES = R * UK * (int)sizeof(T);
   for (int q = threadIdx.x; q < TASKS; q += UNT) {
     int r, c;
     if (KCONTIG) {  // a warp covers whole rows: contiguous k in memory
@@ -98,15 +128,17 @@ __device__ __forceinline__ void stage_tile(uint8_t* tile, const double* __restri
     }
     const int gr = r0 + r;
     alignas(16) T v[F::per16];
+    alignas(16) T w[F::per16];
 #pragma unroll
     for (int e = 0; e < F::per16; ++e) {
       const int gk = k0 + c * F::per16 + e;
       double x = 0.0;
       if (gr < rlim && gk < klim) x = KCONTIG ? src[gk + (int64_t)gr * ld] : src[gr + (int64_t)gk * ld];
-      v[e] = F::cvt(x);
+      F::cvt(x, &v[e], &w[e]);
     }
     uint8_t* dst = tile + (r >> 3) * SBO + c * 128 + (r & 7) * 16;
     *reinterpret_cast<uint4*>(dst) = *reinterpret_cast<const uint4*>(v);
+    if (F::parts == 2) *reinterpret_cast<uint4*>(dst + PART_BYTES) = *reinterpret_cast<const uint4*>(w);
   }
 }
 
@@ -115,10 +147,13 @@ __global__ void __launch_bounds__(UNT) umma_gemm_kernel(const GemmProblem* __res
                                                          const int4* __restrict__ tiles,
                                                          double* __restrict__ ws, unsigned* err) {
   using F = Fmt<PREC>;
+  constexpr int UK = F::uk;
   constexpr int CPR = UK / F::per16;
   constexpr int SBO = CPR * 128;
-  constexpr int A_BYTES = UM * UK * (int)sizeof(typename F::T);
-  constexpr int B_BYTES = UN * UK * (int)sizeof(typename F::T);
+  constexpr int A_PART = UM * UK * (int)sizeof(typename F::T);
+  constexpr int B_PART = UN * UK * (int)sizeof(typename F::T);
+  constexpr int A_BYTES = A_PART * F::parts;
+  constexpr int B_BYTES = B_PART * F::parts;
   extern __shared__ __align__(1024) uint8_t smem[];
   __shared__ __align__(8) uint64_t mbar[2];
   __shared__ uint32_t tmem_slot;
@@ -172,21 +207,26 @@ __global__ void __launch_bounds__(UNT) umma_gemm_kernel(const GemmProblem* __res
       const uint32_t a0 = smem_u32(A_s), b0 = smem_u32(B_s);
 #pragma unroll
       for (int kk = 0; kk < UK / F::mmak; ++kk) {
-        const uint64_t ad = smem_desc(a0 + kk * 256, 128, SBO);
-        const uint64_t bd = smem_desc(b0 + kk * 256, 128, SBO);
-        const uint32_t accum = (s > 0 || kk > 0) ? 1u : 0u;
-        if (PREC == HODLR_GEMM_BF16)
-          asm volatile(
-              "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-              "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
-              ::"r"(tmem), "l"(ad), "l"(bd), "r"(idesc), "r"(accum), "r"(0u), "r"(0u), "r"(0u),
-              "r"(0u));
-        else
-          asm volatile(
-              "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-              "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
-              ::"r"(tmem), "l"(ad), "l"(bd), "r"(idesc), "r"(accum), "r"(0u), "r"(0u), "r"(0u),
-              "r"(0u));
+        // (head, head), then for split formats (head, tail), (tail, head)
+#pragma unroll
+        for (int pp = 0; pp < (F::parts == 2 ? 3 : 1); ++pp) {
+          const uint32_t ao = (pp == 2) ? A_PART : 0u, bo = (pp == 1) ? B_PART : 0u;
+          const uint64_t ad = smem_desc(a0 + ao + kk * 256, 128, SBO);
+          const uint64_t bd = smem_desc(b0 + bo + kk * 256, 128, SBO);
+          const uint32_t accum = (s > 0 || kk > 0 || pp > 0) ? 1u : 0u;
+          if (PREC == HODLR_GEMM_BF16)
+            asm volatile(
+                "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+                ::"r"(tmem), "l"(ad), "l"(bd), "r"(idesc), "r"(accum), "r"(0u), "r"(0u), "r"(0u),
+                "r"(0u));
+          else
+            asm volatile(
+                "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+                ::"r"(tmem), "l"(ad), "l"(bd), "r"(idesc), "r"(accum), "r"(0u), "r"(0u), "r"(0u),
+                "r"(0u));
+        }
       }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
                    ::"r"(smem_u32(&mbar[buf])));
@@ -251,7 +291,7 @@ template <int PREC, bool TRANS_A, int MODE>
 int launch_umma(const GemmProblem* probs, const int4* tiles, int ntiles, double* ws, unsigned* err,
                 cudaStream_t s) {
   using F = Fmt<PREC>;
-  const size_t smem = 2 * (size_t)(UM + UN) * UK * sizeof(typename F::T);
+  const size_t smem = 2 * (size_t)(UM + UN) * F::uk * sizeof(typename F::T) * F::parts;
   auto fn = umma_gemm_kernel<PREC, TRANS_A, MODE>;
   cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   fn<<<ntiles, UNT, smem, s>>>(probs, tiles, ws, err);
@@ -290,7 +330,7 @@ void umma_plan(std::vector<GemmProblem>& probs, std::vector<int4>& tiles, int64_
       splits = std::max(1, std::min(want, p.K / 1024));
     }
     int kchunk = (p.K + splits - 1) / splits;
-    kchunk = ((kchunk + UK - 1) / UK) * UK;
+    kchunk = ((kchunk + 63) / 64) * 64;
     splits = (p.K + kchunk - 1) / kchunk;
     p.splits = splits;
     p.kchunk = splits > 1 ? kchunk : 0;
@@ -309,6 +349,8 @@ int umma_tn_launch(int prec, const GemmProblem* d_probs, const int4* d_tiles, in
   if (ntiles == 0) return 0;
   int e = prec == HODLR_GEMM_BF16
               ? launch_umma<HODLR_GEMM_BF16, true, 0>(d_probs, d_tiles, ntiles, d_ws, err, s)
+          : prec == HODLR_GEMM_TF32X3
+              ? launch_umma<HODLR_GEMM_TF32X3, true, 0>(d_probs, d_tiles, ntiles, d_ws, err, s)
               : launch_umma<HODLR_GEMM_TF32, true, 0>(d_probs, d_tiles, ntiles, d_ws, err, s);
   if (e) return e;
   if (any_split) umma_splitk_reduce<<<dim3(64, nprob), 256, 0, s>>>(d_probs, d_ws);
@@ -320,5 +362,7 @@ int umma_nn_sub_launch(int prec, const GemmProblem* d_probs, const int4* d_tiles
   if (ntiles == 0) return 0;
   return prec == HODLR_GEMM_BF16
              ? launch_umma<HODLR_GEMM_BF16, false, 1>(d_probs, d_tiles, ntiles, nullptr, err, s)
+         : prec == HODLR_GEMM_TF32X3
+             ? launch_umma<HODLR_GEMM_TF32X3, false, 1>(d_probs, d_tiles, ntiles, nullptr, err, s)
              : launch_umma<HODLR_GEMM_TF32, false, 1>(d_probs, d_tiles, ntiles, nullptr, err, s);
 }

@@ -154,8 +154,9 @@ class HODLR_Matrix:
         _check(self._h, _L.lib().hodlr_set_lr_method(self._h, method.encode()))
 
     def set_precision(self, precision):
-        """'fp64' (default), 'tf32' or 'bf16' for the Woodbury products."""
-        code = {"fp64": 0, "tf32": 1, "bf16": 2}[precision] if isinstance(precision, str) else int(precision)
+        """'fp64' (default), 'tf32', 'bf16' or 'tf32x3' for the Woodbury products."""
+        code = ({"fp64": 0, "tf32": 1, "bf16": 2, "tf32x3": 3}[precision]
+                if isinstance(precision, str) else int(precision))
         _check(self._h, _L.lib().hodlr_set_precision(self._h, code))
 
     def set_capacity_hint(self, caps):

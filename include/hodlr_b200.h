@@ -178,11 +178,15 @@ int hodlr_set_capacity_hint(hodlr_t h, const int* caps, int nlevels);
  * reference; TF32 and BF16 run them on the tcgen05 tensor cores with FP32
  * accumulation (the mixed-precision form) while leaf and capacitance LUs,
  * their pivoting and the full-kernel residual stay FP64; GMRES
- * (hodlr_iterative_solve) recovers full accuracy.  Changing it discards the
- * factorization, not the compression. */
+ * (hodlr_iterative_solve) recovers full accuracy when cond(K) * u is well
+ * below 1 (u = 4.9e-4 for TF32, 3.9e-3 for BF16).  TF32X3 splits each
+ * operand into TF32 head and tail and sums three tensor-core products
+ * (about FP32 accuracy, u ~ 1e-7) for ill-conditioned systems.  Changing it
+ * discards the factorization, not the compression. */
 #define HODLR_PRECISION_FP64 0
 #define HODLR_PRECISION_TF32 1
 #define HODLR_PRECISION_BF16 2
+#define HODLR_PRECISION_TF32X3 3
 int hodlr_set_precision(hodlr_t h, int precision);
 
 /* One product in the given arithmetic, device pointers, column-major:
