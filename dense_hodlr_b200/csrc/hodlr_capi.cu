@@ -356,11 +356,29 @@ int ensure_ws(hodlr_t h, int64_t elems) {
   return HODLR_OK;
 }
 
+// Host copies on the handle's stream.  The handle's own stream is a
+// non-blocking stream, so a synchronous cudaMemcpy (legacy default stream) is
+// not ordered with its kernels; every copy goes through these instead and
+// returns after the stream has drained.
+cudaError_t h2d(hodlr_t h, void* dst, const void* src, size_t bytes) {
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, h->stream);
+  return e != cudaSuccess ? e : cudaStreamSynchronize(h->stream);
+}
+cudaError_t d2h(hodlr_t h, void* dst, const void* src, size_t bytes) {
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, h->stream);
+  return e != cudaSuccess ? e : cudaStreamSynchronize(h->stream);
+}
+cudaError_t copy2d(hodlr_t h, void* dst, size_t dpitch, const void* src, size_t spitch,
+                   size_t width, size_t rows, cudaMemcpyKind kind) {
+  cudaError_t e = cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, rows, kind, h->stream);
+  return e != cudaSuccess ? e : cudaStreamSynchronize(h->stream);
+}
+
 int check_dev_err(hodlr_t h, const char* where) {
   unsigned e = 0;
-  CK(cudaMemcpy(&e, h->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost));
+  CK(d2h(h, &e, h->d_err, sizeof(unsigned)));
   if (e == 0) return HODLR_OK;
-  CK(cudaMemset(h->d_err, 0, sizeof(unsigned)));
+  CK(cudaMemsetAsync(h->d_err, 0, sizeof(unsigned), h->stream));
   if (e & DEV_ERR_TIMEOUT) return fail(h, HODLR_ERR_TIMEOUT, std::string(where) + ": device wait timed out");
   if (e & DEV_ERR_NONFINITE) return fail(h, HODLR_ERR_NONFINITE, std::string(where) + ": non-finite value");
   if (e & DEV_ERR_SINGULAR) return fail(h, HODLR_ERR_SINGULAR, std::string(where) + ": exact-zero pivot");
@@ -671,12 +689,11 @@ int upload_plan(hodlr_t h, std::vector<GemmProblem>& probs, bool split, DevPlan&
   for (auto& p : probs) out.any_split |= p.splits > 1;
   if (out.nprob) {
     CK(dalloc(h, &out.probs, (size_t)out.nprob));
-    CK(cudaMemcpy(out.probs, probs.data(), sizeof(GemmProblem) * out.nprob,
-                  cudaMemcpyHostToDevice));
+    CK(h2d(h, out.probs, probs.data(), sizeof(GemmProblem) * out.nprob));
   }
   if (out.ntiles) {
     CK(dalloc(h, &out.tiles, (size_t)out.ntiles));
-    CK(cudaMemcpy(out.tiles, tiles.data(), sizeof(int4) * out.ntiles, cudaMemcpyHostToDevice));
+    CK(h2d(h, out.tiles, tiles.data(), sizeof(int4) * out.ntiles));
   }
   return ensure_ws(h, ws);
 }
@@ -945,7 +962,7 @@ int build_solve_plans(hodlr_t h, int nrhs) {
     }
     dfree(h, L.d_snodes);
     CK(dalloc(h, &L.d_snodes, (size_t)nn));
-    CK(cudaMemcpy(L.d_snodes, sn.data(), sizeof(SchurNode) * nn, cudaMemcpyHostToDevice));
+    CK(h2d(h, L.d_snodes, sn.data(), sizeof(SchurNode) * nn));
     std::vector<GemmProblem> tn, up;
     for (int p = 0; p < nn; ++p) {
       const int sd = sn[p].kb + sn[p].kt;
@@ -1484,14 +1501,14 @@ int init_common(hodlr_t h) {
   CK(cudaEventCreate(&h->ev0));
   CK(cudaEventCreate(&h->ev1));
   CK(dalloc(h, &h->d_err, 1));
-  CK(cudaMemset(h->d_err, 0, sizeof(unsigned)));
+  CK(cudaMemsetAsync(h->d_err, 0, sizeof(unsigned), h->stream));
   build_tree(h);
   const int nl = (int)h->leaf_min.size();
   if (h->smax > 160) return fail(h, HODLR_ERR_UNSUPPORTED, "leaf size above 160");
   CK(dalloc(h, &h->d_leaf_min, (size_t)nl));
   CK(dalloc(h, &h->d_leaf_size, (size_t)nl));
-  CK(cudaMemcpy(h->d_leaf_min, h->leaf_min.data(), 4 * nl, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(h->d_leaf_size, h->leaf_size.data(), 4 * nl, cudaMemcpyHostToDevice));
+  CK(h2d(h, h->d_leaf_min, h->leaf_min.data(), 4 * nl));
+  CK(h2d(h, h->d_leaf_size, h->leaf_size.data(), 4 * nl));
   return HODLR_OK;
 }
 
@@ -1516,7 +1533,7 @@ int hodlr_create_kernel(hodlr_t* out, int n, int dim, const double* pts,
   if (!rc) {
     cudaError_t e = dalloc(h, &h->d_pts, (size_t)n * dim);
     if (e == cudaSuccess)
-      e = cudaMemcpy(h->d_pts, pts, sizeof(double) * (size_t)n * dim, cudaMemcpyHostToDevice);
+      e = h2d(h, h->d_pts, pts, sizeof(double) * (size_t)n * dim);
     if (e != cudaSuccess) rc = cuda_fail(h, e, "points upload");
   }
   if (rc) {
@@ -1539,8 +1556,8 @@ int hodlr_create_dense(hodlr_t* out, int n, const double* A, int lda, int leaf_s
   if (!rc) {
     cudaError_t e = dalloc(h, &h->d_A, (size_t)n * n);
     if (e == cudaSuccess)
-      e = cudaMemcpy2D(h->d_A, sizeof(double) * n, A, sizeof(double) * lda, sizeof(double) * n,
-                       n, cudaMemcpyHostToDevice);
+      e = copy2d(h, h->d_A, sizeof(double) * n, A, sizeof(double) * lda, sizeof(double) * n, n,
+                 cudaMemcpyHostToDevice);
     if (e != cudaSuccess) rc = cuda_fail(h, e, "matrix upload");
   }
   if (rc) {
@@ -1656,10 +1673,10 @@ int hodlr_gemm_device(int precision, int mode, int m, int n, int k, const double
       cudaMalloc(&derr, sizeof(unsigned)) != cudaSuccess)
     rc = HODLR_ERR_ALLOC;
   if (!rc) {
-    cudaMemcpy(dp, probs.data(), sizeof(GemmProblem), cudaMemcpyHostToDevice);
+    cudaMemcpyAsync(dp, probs.data(), sizeof(GemmProblem), cudaMemcpyHostToDevice, s);
     if (tiles.size())
-      cudaMemcpy(dt, tiles.data(), sizeof(int4) * tiles.size(), cudaMemcpyHostToDevice);
-    cudaMemset(derr, 0, sizeof(unsigned));
+      cudaMemcpyAsync(dt, tiles.data(), sizeof(int4) * tiles.size(), cudaMemcpyHostToDevice, s);
+    cudaMemsetAsync(derr, 0, sizeof(unsigned), s);
     const bool split = probs[0].splits > 1;
     int e;
     if (precision == HODLR_PRECISION_FP64)
@@ -1670,7 +1687,8 @@ int hodlr_gemm_device(int precision, int mode, int m, int n, int k, const double
                     : umma_nn_sub_launch(precision, dp, dt, (int)tiles.size(), derr, s);
     if (e || cudaStreamSynchronize(s) != cudaSuccess) rc = HODLR_ERR_CUDA;
     unsigned he = 0;
-    if (!rc && cudaMemcpy(&he, derr, sizeof(unsigned), cudaMemcpyDeviceToHost) == cudaSuccess && he)
+    if (!rc && cudaMemcpyAsync(&he, derr, sizeof(unsigned), cudaMemcpyDeviceToHost, s) == cudaSuccess &&
+        cudaStreamSynchronize(s) == cudaSuccess && he)
       rc = HODLR_ERR_TIMEOUT;
   }
   cudaFree(dp);
@@ -1815,14 +1833,14 @@ int hodlr_iterative_solve(hodlr_t h, int nrhs, const double* b, int ldb, double*
     return cuda_fail(h, e, "gmres alloc");
   }
   int rc = HODLR_OK;
-  e = cudaMemcpy2D(db, sizeof(double) * N, b, sizeof(double) * ldb, sizeof(double) * N, nrhs,
-                   cudaMemcpyHostToDevice);
+  e = copy2d(h, db, sizeof(double) * N, b, sizeof(double) * ldb, sizeof(double) * N, nrhs,
+             cudaMemcpyHostToDevice);
   if (e == cudaSuccess) {
     rc = hodlr_iterative_solve_device(h, nrhs, db, (int)N, dx, (int)N, tol, max_iter, restart,
                                       iters, relres);
     if (!rc)
-      e = cudaMemcpy2D(x, sizeof(double) * ldx, dx, sizeof(double) * N, sizeof(double) * N,
-                       nrhs, cudaMemcpyDeviceToHost);
+      e = copy2d(h, x, sizeof(double) * ldx, dx, sizeof(double) * N, sizeof(double) * N, nrhs,
+                 cudaMemcpyDeviceToHost);
   }
   dfree(h, db);
   dfree(h, dx);
@@ -1842,14 +1860,14 @@ int hodlr_solve_refined(hodlr_t h, int nrhs, const double* b, int ldb, double* x
     return cuda_fail(h, e, "refine alloc");
   }
   int rc = HODLR_OK;
-  e = cudaMemcpy2D(db, sizeof(double) * N, b, sizeof(double) * ldb, sizeof(double) * N, nrhs,
-                   cudaMemcpyHostToDevice);
+  e = copy2d(h, db, sizeof(double) * N, b, sizeof(double) * ldb, sizeof(double) * N, nrhs,
+             cudaMemcpyHostToDevice);
   if (e == cudaSuccess) {
     rc = hodlr_solve_refined_device(h, nrhs, db, (int)N, dx, (int)N, tol, max_iter, iters,
                                     relres);
     if (!rc)
-      e = cudaMemcpy2D(x, sizeof(double) * ldx, dx, sizeof(double) * N, sizeof(double) * N,
-                       nrhs, cudaMemcpyDeviceToHost);
+      e = copy2d(h, x, sizeof(double) * ldx, dx, sizeof(double) * N, sizeof(double) * N, nrhs,
+                 cudaMemcpyDeviceToHost);
   }
   dfree(h, db);
   dfree(h, dx);
@@ -1870,14 +1888,14 @@ int hodlr_residual(hodlr_t h, int nrhs, const double* b, int ldb, const double* 
   }
   int rc = HODLR_OK;
   std::vector<double> y((size_t)(N * nrhs));
-  e = cudaMemcpy2D(dx, sizeof(double) * N, x, sizeof(double) * ldx, sizeof(double) * N, nrhs,
-                   cudaMemcpyHostToDevice);
+  e = copy2d(h, dx, sizeof(double) * N, x, sizeof(double) * ldx, sizeof(double) * N, nrhs,
+             cudaMemcpyHostToDevice);
   if (e == cudaSuccess) {
     for (int c0 = 0; c0 < nrhs && !rc; c0 += 16) {
       int nc = std::min(16, nrhs - c0);
       rc = hodlr_kernel_matvec_device(h, nc, dx + c0 * N, (int)N, dy + c0 * N, (int)N);
     }
-    if (!rc) e = cudaMemcpy(y.data(), dy, sizeof(double) * N * nrhs, cudaMemcpyDeviceToHost);
+    if (!rc) e = d2h(h, y.data(), dy, sizeof(double) * N * nrhs);
   }
   dfree(h, dx);
   dfree(h, dy);
@@ -1969,8 +1987,8 @@ int hodlr_get_pivots(hodlr_t h, int block, int* rows, int* cols, int* count) {
   const int k = L.st[q].k;
   *count = k;
   if (k > 0) {
-    if (rows) CK(cudaMemcpy(rows, L.prow + r0, 4 * (size_t)k, cudaMemcpyDeviceToHost));
-    if (cols) CK(cudaMemcpy(cols, L.pcol + c0, 4 * (size_t)k, cudaMemcpyDeviceToHost));
+    if (rows) CK(d2h(h, rows, L.prow + r0, 4 * (size_t)k));
+    if (cols) CK(d2h(h, cols, L.pcol + c0, 4 * (size_t)k));
   }
   return HODLR_OK;
 }
@@ -1984,8 +2002,8 @@ int hodlr_get_lowrank(hodlr_t h, int block, double* W, double* V) {
   block_geom(L, q, r0, c0, m, n);
   const int r = L.st[q].rank;
   const int64_t N = h->n;
-  if (W) CK(cudaMemcpy2D(W, sizeof(double) * m, L.W + r0, sizeof(double) * N, sizeof(double) * m, r, cudaMemcpyDeviceToHost));
-  if (V) CK(cudaMemcpy2D(V, sizeof(double) * n, L.V + c0, sizeof(double) * N, sizeof(double) * n, r, cudaMemcpyDeviceToHost));
+  if (W) CK(copy2d(h, W, sizeof(double) * m, L.W + r0, sizeof(double) * N, sizeof(double) * m, r, cudaMemcpyDeviceToHost));
+  if (V) CK(copy2d(h, V, sizeof(double) * n, L.V + c0, sizeof(double) * N, sizeof(double) * n, r, cudaMemcpyDeviceToHost));
   return HODLR_OK;
 }
 

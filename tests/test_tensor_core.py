@@ -12,7 +12,8 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-TOL = {0: 1e-13, 1: 2e-3, 2: 1.5e-2, 3: 2e-6}  # FP64, TF32, BF16, 3xTF32
+# FP64, TF32, BF16, 3xTF32 (FP32 accumulation in tensor memory: ~1e-7 * sqrt(K))
+TOL = {0: 1e-13, 1: 2e-3, 2: 1.5e-2, 3: 2e-5}
 
 
 def _gemm(prec, mode, A, B, C):
