@@ -1126,8 +1126,9 @@ __global__ void axpy_cols_kernel(double* X, const double* D, int64_t total) {
 }
 
 int kmatvec_dev(hodlr_t h, int nrhs, const double* d_x, int ldx, double* d_y, int ldy) {
-  int sp = kmatvec_splits(h->n, h->num_sms);
-  if (sp > 1) {
+  const int sym = kmatvec_sym_slices(h->n, nrhs, h->dense);
+  const int sp = sym ? sym : kmatvec_splits(h->n, h->num_sms);
+  if (sym || sp > 1) {
     int rc = ensure_ws(h, (int64_t)sp * nrhs * h->n);
     if (rc) return rc;
   }
@@ -1140,9 +1141,9 @@ int kmatvec_dev(hodlr_t h, int nrhs, const double* d_x, int ldx, double* d_y, in
   L.ws = h->ws;
   L.n = h->n;
   L.nrhs = nrhs;
-  int e = kmatvec_launch(L, sp, h->stream);
+  int e = sym ? kmatvec_sym_launch(L, sym, h->stream) : kmatvec_launch(L, sp, h->stream);
   if (e) return cuda_fail(h, (cudaError_t)e, "kmatvec");
-  h->nlaunch += 1 + (sp > 1);
+  h->nlaunch += 1 + (sym || sp > 1);
   return HODLR_OK;
 }
 

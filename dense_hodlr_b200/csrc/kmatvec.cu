@@ -139,6 +139,226 @@ void launch_type(const KmatvecLaunch& L, dim3 grid, cudaStream_t s) {
   }
 }
 
+
+// ------------------------------------------------------------ symmetric form
+// K is symmetric entry for entry (the squared distance of i, j and of j, i
+// are the same sums of the same rounded squares), so one evaluation of K_ij
+// serves both y_i += K_ij x_j and y_j += K_ij x_i.  The points are cut into
+// 256-point tiles and the tiles into S splits; CTA (a, b), a <= b, takes every
+// tile pair (I in split a, J in split b), J >= I when a == b.  Its row sums
+// (rows of a) go to slice b of the workspace, its column sums (rows of b) to
+// slice a: every (slice, row) is written by exactly one CTA, in a fixed order,
+// and Y = sum over slices (kmatvec_reduce) is deterministic.  Diagonal tile
+// pairs (J == I) are evaluated in full with row sums only.
+//
+// Column sums without a cross-lane reduction per column: within a group of 32
+// columns, lane L handles column (s + L) mod 32 at step s and then hands its
+// column accumulator to lane L - 1, so each accumulator follows one column
+// around the warp and ends, after 32 steps, in the lane of that column.  The
+// four warps' group sums are added through shared memory (double-buffered
+// per group) and accumulated into the workspace.
+constexpr int ST = 256;  // tile edge (rows = columns)
+constexpr int SG = 32;   // rotation group
+constexpr int SYM_NT = 128;
+constexpr int SYM_RPT = ST / SYM_NT;
+constexpr int SYM_NW = SYM_NT / 32;
+
+template <int NR>
+struct SymPad {  // row stride of the staged X tile: an odd number of 16-byte units
+  static constexpr int VS = NR == 1 ? 1 : NR + 2;
+};
+
+template <int NR, int KTYPE, int DIM>
+__global__ void __launch_bounds__(SYM_NT, 3) kmatvec_sym_kernel(KmatvecLaunch L, int S, int tps) {
+  constexpr int VS = SymPad<NR>::VS;
+  __shared__ double xs[DIM][ST];
+  __shared__ __align__(16) double vs[ST][VS];
+  __shared__ __align__(16) double colw[2][SYM_NW][SG][VS];
+  __shared__ double tab[64];
+  const int n = L.n;
+  const int nT = (n + ST - 1) / ST;
+  int a, b;
+  {
+    const int nup = S * (S - 1) / 2;
+    int p = blockIdx.x;
+    if (p < nup) {
+      a = 0;
+      while (p >= S - 1 - a) {
+        p -= S - 1 - a;
+        ++a;
+      }
+      b = a + 1 + p;
+    } else {
+      a = b = p - nup;
+    }
+  }
+  const int ia0 = a * tps, ia1 = min(nT, ia0 + tps);
+  const int jb1 = min(nT, b * tps + tps);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (threadIdx.x < 64) tab[threadIdx.x] = c_tang[threadIdx.x];
+  const double ak = L.src.kp.a;
+  const int64_t slice = (int64_t)L.nrhs * n;
+  double* __restrict__ wsA = L.ws + (int64_t)a * slice;  // column sums (rows of split b)
+  double* __restrict__ wsB = L.ws + (int64_t)b * slice;  // row sums (rows of split a)
+  const hx_kparams kp = L.src.kp;
+  const double dcorr = kp.diag_replace ? kp.diag_value - 1.0 : kp.shift;
+
+  for (int I = ia0; I < ia1; ++I) {
+    int row[SYM_RPT];
+    bool live[SYM_RPT];
+    double xi[SYM_RPT][DIM];
+    double xv[SYM_RPT][NR];
+    double acc[SYM_RPT][NR];
+#pragma unroll
+    for (int q = 0; q < SYM_RPT; ++q) {
+      row[q] = I * ST + q * SYM_NT + threadIdx.x;
+      live[q] = row[q] < n;
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) xi[q][d] = live[q] ? L.src.pts[d * L.src.ld + row[q]] : 0.0;
+#pragma unroll
+      for (int c = 0; c < NR; ++c) {
+        xv[q][c] = (live[q] && c < L.nrhs) ? L.X[(int64_t)c * L.ldx + row[q]] : 0.0;
+        acc[q][c] = 0.0;
+      }
+    }
+    const int jstart = a == b ? I : b * tps;
+    for (int J = jstart; J < jb1; ++J) {
+      __syncthreads();  // every thread is done with the previous tile
+      for (int t = threadIdx.x; t < ST; t += SYM_NT) {
+        const int j = J * ST + t;
+        const bool ok = j < n;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) xs[d][t] = ok ? L.src.pts[d * L.src.ld + j] : 0.0;
+#pragma unroll
+        for (int c = 0; c < NR; ++c)
+          vs[t][c] = (ok && c < L.nrhs) ? L.X[(int64_t)c * L.ldx + j] : 0.0;
+      }
+      __syncthreads();
+      if (J == I) {  // diagonal tile pair: all entries, row sums only
+#pragma unroll 2
+        for (int t = 0; t < ST; ++t) {
+#pragma unroll
+          for (int q = 0; q < SYM_RPT; ++q) {
+            double r2 = 0.0;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+              const double dd = xi[q][d] - xs[d][t];
+              r2 = fma(dd, dd, r2);
+            }
+            const double k = hx_kernel_r2_fast_t<KTYPE>(ak, r2, tab);
+#pragma unroll
+            for (int c = 0; c < NR; ++c) acc[q][c] = fma(k, vs[t][c], acc[q][c]);
+          }
+        }
+        continue;
+      }
+      for (int g = 0; g < ST / SG; ++g) {
+        double cacc[NR];
+#pragma unroll
+        for (int c = 0; c < NR; ++c) cacc[c] = 0.0;
+#pragma unroll 2
+        for (int s = 0; s < SG; ++s) {
+          const int t = g * SG + ((s + lane) & (SG - 1));
+          double xj[DIM];
+#pragma unroll
+          for (int d = 0; d < DIM; ++d) xj[d] = xs[d][t];
+          double vj[NR];
+          if (NR == 1) {
+            vj[0] = vs[t][0];
+          } else {
+#pragma unroll
+            for (int c = 0; c < NR; c += 2) {
+              const double2 v2 = *reinterpret_cast<const double2*>(&vs[t][c]);
+              vj[c] = v2.x;
+              vj[c + 1] = v2.y;
+            }
+          }
+#pragma unroll
+          for (int q = 0; q < SYM_RPT; ++q) {
+            double r2 = 0.0;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+              const double dd = xi[q][d] - xj[d];
+              r2 = fma(dd, dd, r2);
+            }
+            const double k = hx_kernel_r2_fast_t<KTYPE>(ak, r2, tab);
+#pragma unroll
+            for (int c = 0; c < NR; ++c) {
+              acc[q][c] = fma(k, vj[c], acc[q][c]);
+              cacc[c] = fma(k, xv[q][c], cacc[c]);
+            }
+          }
+#pragma unroll
+          for (int c = 0; c < NR; ++c) cacc[c] = __shfl_sync(0xffffffffu, cacc[c], (lane + 1) & 31);
+        }
+        // lane L holds column g * SG + L of this warp's rows
+        double* cw = &colw[g & 1][w][lane][0];
+        if (NR == 1) {
+          cw[0] = cacc[0];
+        } else {
+#pragma unroll
+          for (int c = 0; c < NR; c += 2)
+            *reinterpret_cast<double2*>(&cw[c]) = make_double2(cacc[c], cacc[c + 1]);
+        }
+        __syncthreads();
+        for (int e = threadIdx.x; e < SG * NR; e += SYM_NT) {
+          const int tl = e % SG, c = e / SG;
+          const int j = J * ST + g * SG + tl;
+          if (c < L.nrhs && j < n) {
+            double sum = colw[g & 1][0][tl][c];
+#pragma unroll
+            for (int ww = 1; ww < SYM_NW; ++ww) sum += colw[g & 1][ww][tl][c];
+            double* dst = wsA + (int64_t)c * n + j;
+            *dst = I == ia0 ? sum : *dst + sum;
+          }
+        }
+      }
+    }
+    // row sums of tile I; in a diagonal block the earlier tiles' column sums
+    // are already there, and K_ii = f(0) + shift (or the replaced value)
+#pragma unroll
+    for (int q = 0; q < SYM_RPT; ++q) {
+      if (!live[q]) continue;
+#pragma unroll
+      for (int c = 0; c < NR; ++c) {
+        if (c >= L.nrhs) continue;
+        double v = acc[q][c];
+        if (a == b) v = fma(dcorr, xv[q][c], v);
+        double* dst = wsB + (int64_t)c * n + row[q];
+        *dst = (a == b && I != ia0) ? *dst + v : v;
+      }
+    }
+  }
+}
+
+template <int NR, int KTYPE>
+void launch_sym_dim(const KmatvecLaunch& L, int S, int tps, cudaStream_t s) {
+  const int grid = S * (S + 1) / 2;
+  if (L.src.kp.dim == 1)
+    kmatvec_sym_kernel<NR, KTYPE, 1><<<grid, SYM_NT, 0, s>>>(L, S, tps);
+  else if (L.src.kp.dim == 2)
+    kmatvec_sym_kernel<NR, KTYPE, 2><<<grid, SYM_NT, 0, s>>>(L, S, tps);
+  else
+    kmatvec_sym_kernel<NR, KTYPE, 3><<<grid, SYM_NT, 0, s>>>(L, S, tps);
+}
+
+template <int NR>
+void launch_sym_type(const KmatvecLaunch& L, int S, int tps, cudaStream_t s) {
+  switch (L.src.kp.type) {
+    case HX_KERNEL_GAUSSIAN: launch_sym_dim<NR, HX_KERNEL_GAUSSIAN>(L, S, tps, s); break;
+    case HX_KERNEL_MATERN32: launch_sym_dim<NR, HX_KERNEL_MATERN32>(L, S, tps, s); break;
+    case HX_KERNEL_INV_MULTIQUADRIC: launch_sym_dim<NR, HX_KERNEL_INV_MULTIQUADRIC>(L, S, tps, s); break;
+    case HX_KERNEL_QUADRATIC: launch_sym_dim<NR, HX_KERNEL_QUADRATIC>(L, S, tps, s); break;
+    default: launch_sym_dim<NR, HX_KERNEL_EXPONENTIAL>(L, S, tps, s); break;
+  }
+}
+
+// Tiles per split: about 96 splits (4656 CTAs) once there are enough tiles.
+int sym_tps(int n) {
+  const int nT = (n + ST - 1) / ST;
+  return nT <= 96 ? 1 : (nT + 95) / 96;
+}
+
 }  // namespace
 
 int kmatvec_splits(int n, int num_sms) {
@@ -163,5 +383,25 @@ int kmatvec_launch(const KmatvecLaunch& L, int nsplit, cudaStream_t s) {
   else
     return (int)cudaErrorInvalidValue;
   if (nsplit > 1) kmatvec_reduce<<<1024, 256, 0, s>>>(L, nsplit);
+  return (int)cudaGetLastError();
+}
+
+int kmatvec_sym_slices(int n, int nrhs, bool dense) {
+  if (dense || nrhs > 8 || n < 1) return 0;
+  const int nT = (n + ST - 1) / ST;
+  const int tps = sym_tps(n);
+  return (nT + tps - 1) / tps;
+}
+
+int kmatvec_sym_launch(const KmatvecLaunch& L, int S, cudaStream_t s) {
+  const int tps = sym_tps(L.n);
+  if (S != kmatvec_sym_slices(L.n, L.nrhs, L.src.dense) || S < 1) return (int)cudaErrorInvalidValue;
+  if (L.nrhs <= 1)
+    launch_sym_type<1>(L, S, tps, s);
+  else if (L.nrhs <= 4)
+    launch_sym_type<4>(L, S, tps, s);
+  else
+    launch_sym_type<8>(L, S, tps, s);
+  kmatvec_reduce<<<1024, 256, 0, s>>>(L, S);
   return (int)cudaGetLastError();
 }

@@ -18,3 +18,8 @@ struct KmatvecLaunch {
 
 int kmatvec_splits(int n, int num_sms);
 int kmatvec_launch(const KmatvecLaunch& L, int nsplit, cudaStream_t s);
+
+// Symmetric form (closed-form kernels, nrhs <= 8): number of workspace
+// slices (0 when it does not apply); L.ws must hold slices * nrhs * n.
+int kmatvec_sym_slices(int n, int nrhs, bool dense);
+int kmatvec_sym_launch(const KmatvecLaunch& L, int slices, cudaStream_t s);
