@@ -107,6 +107,32 @@ HX_HD double hx_exp_tang_neg(double x, const double* tab) {
 #endif
 }
 
+#if defined(__CUDA_ARCH__)
+// Square roots by Newton's method from the hardware reciprocal-square-root
+// approximation (rsqrt.approx.ftz.f64, relative error below 2^-20 on this
+// GPU).  One Newton step y <- y + y (1 - x y^2) / 2 on 1/sqrt(x) squares the
+// error (~2^-40); hx_sqrt_nr then applies one Heron correction to r = x y,
+// r <- r + (y / 2)(x - r^2), which gives sqrt(x) to within an ulp, and
+// hx_rsqrt_nr a second Newton step.  x must be a positive normal number.
+__device__ __forceinline__ double hx_rsqrt_seed(double x) {
+  double y;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  return y;
+}
+__device__ __forceinline__ double hx_rsqrt_step(double x, double y) {
+  const double e = fma(-(x * y), y, 1.0);  // 1 - x y^2
+  return fma(0.5 * y, e, y);
+}
+__device__ __forceinline__ double hx_sqrt_nr(double x) {
+  const double y = hx_rsqrt_step(x, hx_rsqrt_seed(x));
+  const double r = x * y;
+  return fma(0.5 * y, fma(-r, r, x), r);
+}
+__device__ __forceinline__ double hx_rsqrt_nr(double x) {
+  return hx_rsqrt_step(x, hx_rsqrt_step(x, hx_rsqrt_seed(x)));
+}
+#endif
+
 // Kernel value of r2 for a kernel family fixed at compile time (no per-entry
 // dispatch in the residual kernel).
 template <int KTYPE>
@@ -114,37 +140,20 @@ HX_HD double hx_kernel_r2_fast_t(double a, double r2, const double* tab) {
   if (KTYPE == HX_KERNEL_GAUSSIAN) return hx_exp_tang_neg(r2 * a, tab);
   if (KTYPE == HX_KERNEL_MATERN32) {
 #if defined(__CUDA_ARCH__)
-    double s = r2 * rsqrt(fmax(r2, 1e-300)) * a;
+    const double s = hx_sqrt_nr(fmax(r2, 1e-300)) * a;
 #else
-    double s = sqrt(r2) * a;
+    const double s = sqrt(r2) * a;
 #endif
-    return (1.0 + s) * hx_exp_tang_neg(-s, tab);
+    const double e = hx_exp_tang_neg(-s, tab);
+    return fma(e, s, e);  // (1 + s) e^-s
   }
+#if defined(__CUDA_ARCH__)
+  if (KTYPE == HX_KERNEL_INV_MULTIQUADRIC) return hx_rsqrt_nr(fma(r2, a, 1.0));
+  if (KTYPE == HX_KERNEL_QUADRATIC) return fma(r2, a, 1.0);
+  return hx_exp_tang_neg(-hx_sqrt_nr(fmax(r2, 1e-300)) * a, tab);
+#else
   if (KTYPE == HX_KERNEL_INV_MULTIQUADRIC) return 1.0 / sqrt(fma(r2, a, 1.0));
   if (KTYPE == HX_KERNEL_QUADRATIC) return fma(r2, a, 1.0);
   return hx_exp_tang_neg(-sqrt(r2) * a, tab);
-}
-
-// Kernel value of the squared distance, FP64-accurate (not bit-matched to ACA).
-HX_HD double hx_kernel_r2_fast(const hx_kparams& p, double r2, const double* tab) {
-  switch (p.type) {
-    case HX_KERNEL_GAUSSIAN:
-      return hx_exp_tang_neg(r2 * p.a, tab);
-    case HX_KERNEL_MATERN32: {
-#if defined(__CUDA_ARCH__)
-      double s = r2 * rsqrt(fmax(r2, 1e-300)) * p.a;
-#else
-      double s = sqrt(r2) * p.a;
 #endif
-      return (1.0 + s) * hx_exp_tang_neg(-s, tab);
-    }
-    case HX_KERNEL_INV_MULTIQUADRIC:
-      return 1.0 / sqrt(fma(r2, p.a, 1.0));
-    case HX_KERNEL_QUADRATIC:
-      return fma(r2, p.a, 1.0);
-    case HX_KERNEL_EXPONENTIAL:
-      return hx_exp_tang_neg(-sqrt(r2) * p.a, tab);
-    default:
-      return 0.0;
-  }
 }
