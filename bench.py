@@ -38,6 +38,9 @@ METRIC = "factor+solve s and solves/s, mixed vs FP64 GPU path, at rel residual â
 UNIT = "factor+solve/s"
 N_PTS, DIM, LSCALE, SHIFT, LEAF, TOL, NRHS, SEED = 262144, 2, 0.2, 1e-2, 128, 1e-8, 8, 2024
 RES_TOL, MAX_IR = 1e-10, 200
+# GMRES iterations to 1e-10 with this workload's FP64 HODLR preconditioner
+# (the reference's factors: same pivots and ranks) -- measured by the GPU path
+GMRES_ITERS_FP64 = 6
 WORKLOAD = ("FP64 at scale: N=262144 2D uniform [0,1]^2 k-d ordered, Matern-3/2 l=0.2 "
             "+1e-2*delta, leaf 128, partial-pivot ACA tol 1e-8, 8 RHS N(0,1), FP64")
 
@@ -57,18 +60,36 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def profiled_traffic():
-    """Per-launch DRAM bytes of the ACA kernel from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "aca_level_c2.md")
+def profiled_figure(name, key):
+    """A figure from a committed ncu summary under profiles/ (a 'key: value' line)."""
+    p = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(p):
         return None
     for line in open(p):
-        if line.strip().startswith("traffic_bytes_per_launch:"):
+        if line.strip().startswith(key + ":"):
             try:
-                return float(line.split(":", 1)[1].strip())
-            except ValueError:
+                return float(line.split(":", 1)[1].strip().split()[0])
+            except (ValueError, IndexError):
                 return None
     return None
+
+
+# FP64 FLOPs of the symmetric full-kernel product (kmatvec.cu / kfast.cuh),
+# FMA counted as 2: one Matern-3/2 entry in 2D costs 14 FMAs and 12 other FP64
+# operations (distance 2 sub + 1 mul + 1 fma; clamp; Newton square root 4 fma +
+# 4 mul; scale; Tang exp 1 clamp + 8 fma + 1 sub + 1 mul; (1+s)e^-s 1 fma) = 40
+# FLOPs, evaluated once per entry pair, plus 2 * nrhs FMAs (row and column
+# products) per evaluated entry.
+KMV_EVAL_FLOPS = 40
+
+
+def sym_slices(n):
+    """Workspace slices of the symmetric product (kmatvec.cu: 256-point tiles,
+    about 96 splits)."""
+    nt = -(-n // 256)
+    tps = 1 if nt <= 96 else -(-nt // 96)
+    return -(-nt // tps)
+FP64_LANES_PER_SM = 64
 
 
 class ClockSampler:
@@ -282,6 +303,36 @@ def run_ours(args, rank, world, local_rank):
     ms_max = float(t.item())
     clocks = clk.summary()
 
+    # mixed precision (3xTF32 tensor-core Woodbury products, FP64 leaf and
+    # capacitance LUs and residual) to the same accuracy.  TF32 and BF16
+    # factors stop being preconditioners at this shift (cond(K) * u > 1).
+    mixed = None
+    if not args.no_mixed:
+        g.set_precision("tf32x3")
+        for _ in range(1):
+            step()
+        torch.cuda.synchronize()
+        m0 = torch.cuda.Event(enable_timing=True)
+        m1 = torch.cuda.Event(enable_timing=True)
+        m_it, m_rel = [], []
+        m_steps = 2
+        m0.record(stream)
+        for _ in range(m_steps):
+            it, rel = step()
+            m_it.append(it)
+            m_rel.append(float(rel.max()))
+        m1.record(stream)
+        torch.cuda.synchronize()
+        m_ms = m0.elapsed_time(m1) / m_steps
+        mixed = {"precision": "tf32x3", "ms_per_step": m_ms, "steps": m_steps,
+                 "gmres_iterations": int(max(m_it)), "rel_residual": max(m_rel),
+                 "factor_s": g.get_recLU_FactorizationTime(),
+                 "speedup_vs_fp64": ms_max / m_ms,
+                 "note": ("TF32 and BF16 Woodbury products diverge on this system "
+                          "(Matern shift 1e-2: cond(K) * u_tf32 > 1); 3xTF32 converges")}
+        g.set_precision("fp64")
+        g.recLU_Compute()
+
     # direct solve only (no refinement), for the phase breakdown
     g.solve_device(b_d.data_ptr(), x_d.data_ptr(), NRHS)
     t_direct_solve = g.get_recLU_SolveTime()
@@ -329,7 +380,18 @@ def run_ours(args, rank, world, local_rank):
     aca_launch = float(np.mean(phase["aca_launches"]))
     hbm, peak_kind = peaks()
     achieved = aca_bytes / aca_s / 1e9
-    traffic = profiled_traffic()
+    ratio = profiled_figure("aca_kernel_matern2d_n131072.md", "traffic_to_algorithmic")
+    aca_per_launch = aca_bytes / max(aca_launch, 1.0)
+    traffic = ratio * aca_per_launch if ratio else None
+    # full-kernel product: FP64 FLOPs per launch over its event-timed duration
+    sm_mhz = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get("sm_max_mhz", 1965.0) \
+        if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else 1965.0
+    n_sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    fp64_peak = n_sms * FP64_LANES_PER_SM * 2 * sm_mhz * 1e6 / 1e12
+    evaluated = N_PTS * (N_PTS + 256) / 2.0
+    kmv_flops = evaluated * (KMV_EVAL_FLOPS + 4 * NRHS)
+    kmv_tf = kmv_flops / t_kmatvec / 1e12
+    kmv_dram_ref = profiled_figure("kmatvec_sym_matern2d_n65536.md", "dram_bytes_per_launch")
     out = {
         "metric": METRIC,
         "value": world * 1000.0 / ms_max,
@@ -364,14 +426,30 @@ def run_ours(args, rank, world, local_rank):
                 "h2d_bytes_per_step": int(pts.nbytes + b.nbytes),
                 "d2h_bytes_per_step": int(b.nbytes),
                 "dev_vs_host_solution_rel_diff": diff_dev_host},
-        "roofline": {"kernel": "aca_kernel (batched partial-pivot ACA, one launch per level group)",
-                     "bound": "hbm", "achieved": achieved, "peak": hbm,
-                     "peak_kind": f"{peak_kind} hbm_gbs (burst)", "unit": "GB/s",
-                     "frac": achieved / hbm,
-                     "traffic": traffic,
-                     "algorithmic_bytes_per_launch": aca_bytes / max(aca_launch, 1.0),
-                     "avg_launch_s": aca_s / max(aca_launch, 1.0),
-                     "launches_per_step": aca_launch},
+        "roofline": {"kernel": "kmatvec_sym_kernel (full-kernel FP64 product, 8 RHS; "
+                               "the largest share of the step)",
+                     "bound": "fp64", "achieved": kmv_tf, "peak": fp64_peak,
+                     "peak_kind": (f"nominal FP64 CUDA-core peak ({n_sms} SMs x 64 FMA/clk x 2 x "
+                                   f"{sm_mhz:.0f} MHz); no measured FP64 figure exists"),
+                     "unit": "TFLOP/s", "frac": kmv_tf / fp64_peak,
+                     "traffic": (kmv_dram_ref * (N_PTS * sym_slices(N_PTS))
+                                 / (65536.0 * sym_slices(65536)) if kmv_dram_ref else None),
+                     "traffic_note": ("DRAM bytes of the n=65536 capture scaled by slices x n "
+                                      "(the workspace writes); the kernel is compute-bound"),
+                     "algorithmic_flops_per_launch": kmv_flops,
+                     "avg_launch_s": t_kmatvec},
+        "roofline_aca": {"kernel": "aca_kernel (batched partial-pivot ACA, one launch per level "
+                                   "group)",
+                         "bound": "hbm", "achieved": achieved, "peak": hbm,
+                         "peak_kind": f"{peak_kind} hbm_gbs (burst)", "unit": "GB/s",
+                         "frac": achieved / hbm,
+                         "traffic": traffic,
+                         "traffic_note": ("DRAM/algorithmic ratio of the N=131072 capture "
+                                          "applied to this launch's algorithmic bytes"),
+                         "algorithmic_bytes_per_launch": aca_per_launch,
+                         "avg_launch_s": aca_s / max(aca_launch, 1.0),
+                         "launches_per_step": aca_launch},
+        "mixed": mixed,
         "clocks": clocks,
         "gpu_launches": int(n_launch),
     }
@@ -397,7 +475,7 @@ def run_reference(args):
     pts, _ = workload_inputs()
     blocks = reference_block_table(pts)
     times = []
-    ir = int(blocks[0].get("ir_iters", 4)) if blocks else 4
+    ir = GMRES_ITERS_FP64
     for it in range(args.warmup + args.steps):
         est = cpu_estimate(pts, blocks, args.ref_budget, threads=threads, ir_iters=ir)
         if it >= args.warmup:
@@ -482,6 +560,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision leg")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--ref-budget", type=float, default=6.0)
     args = ap.parse_args()
