@@ -46,6 +46,7 @@ SIGNATURES = {
     "hodlr_set_stream": (_I, [_H, _V]),
     "hodlr_get_launch_count": (_I, [_H, ctypes.POINTER(ctypes.c_longlong)]),
     "hodlr_set_capacity_hint": (_I, [_H, _PI, _I]),
+    "hodlr_trim_device_memory": (_I, []),
     "hodlr_set_precision": (_I, [_H, _I]),
     "hodlr_gemm_device": (_I, [_I, _I, _I, _I, _I, _V, _I, _V, _I, _V, _I, _V]),
     "hodlr_set_lr_tolerance": (_I, [_H, _D]),

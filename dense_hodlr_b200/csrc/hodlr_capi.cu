@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <cmath>
 #include <map>
+#include <mutex>
 #include <unordered_map>
 #include <cstdio>
 #include <cstring>
@@ -92,9 +93,46 @@ void block_geom(const Level& L, int q, int& r0, int& c0, int& m, int& n) {
 // Device memory cache of one handle.  Freed blocks go to `pending` and become
 // reusable only after the handle's stream has been synchronised, so a reused
 // block is never still read by an earlier kernel or host copy.
+// Device memory of every handle on a device comes from one stream-ordered
+// pool owned by the library (cudaMallocFromPoolAsync / cudaFreeAsync) whose
+// release threshold keeps freed memory reserved, so a new handle for the next
+// system reuses the previous one's arenas instead of paying cudaMalloc /
+// cudaFree for gigabytes.  hodlr_trim_device_memory hands it back.
+std::mutex g_pool_mu;
+std::map<int, cudaMemPool_t> g_pools;
+
+cudaMemPool_t device_pool() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  auto it = g_pools.find(dev);
+  if (it != g_pools.end()) return it->second;
+  cudaMemPoolProps props;
+  memset(&props, 0, sizeof(props));
+  props.allocType = cudaMemAllocationTypePinned;
+  props.handleTypes = cudaMemHandleTypeNone;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = dev;
+  cudaMemPool_t pool = nullptr;
+  if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) return nullptr;
+  uint64_t keep = UINT64_MAX;
+  cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  g_pools[dev] = pool;
+  return pool;
+}
+
+// Per-handle cache on top of the device pool: buffers freed by the handle are
+// reused by its next allocations of a similar size once its stream has
+// drained (pending -> free).
 struct DevPool {
+  cudaMemPool_t mp = nullptr;
   std::multimap<size_t, void*> freeb, pending;
   std::unordered_map<void*, size_t> size;
+  cudaError_t raw_alloc(void** p, size_t bytes, cudaStream_t s) {
+    if (!mp) mp = device_pool();
+    if (!mp) return cudaErrorMemoryAllocation;
+    return cudaMallocFromPoolAsync(p, bytes, mp, s);
+  }
   cudaError_t alloc(void** p, size_t bytes, cudaStream_t s) {
     bytes = (bytes + 255) & ~(size_t)255;
     for (int pass = 0; pass < 2; ++pass) {
@@ -111,17 +149,18 @@ struct DevPool {
         pending.clear();
       }
     }
-    cudaError_t e = cudaMalloc(p, bytes);
-    if (e == cudaErrorMemoryAllocation) {  // give back the cache, retry once
+    cudaError_t e = raw_alloc(p, bytes, s);
+    if (e == cudaErrorMemoryAllocation) {  // give back every cache, retry once
       cudaGetLastError();
-      cudaStreamSynchronize(s);
-      release_free();
+      release_free(s);
       for (auto& f : pending) {
-        cudaFree(f.second);
+        cudaFreeAsync(f.second, s);
         size.erase(f.second);
       }
       pending.clear();
-      e = cudaMalloc(p, bytes);
+      cudaStreamSynchronize(s);
+      cudaMemPoolTrimTo(mp, 0);
+      e = raw_alloc(p, bytes, s);
     }
     if (e == cudaSuccess) size[*p] = bytes;
     return e;
@@ -131,18 +170,19 @@ struct DevPool {
     if (it == size.end()) return;
     pending.insert({it->second, p});
   }
-  void release_free() {
+  void release_free(cudaStream_t s) {
     for (auto& f : freeb) {
-      cudaFree(f.second);
+      cudaFreeAsync(f.second, s);
       size.erase(f.second);
     }
     freeb.clear();
   }
-  void release_all() {
-    for (auto& f : size) cudaFree(f.first);
+  void release_all(cudaStream_t s) {
+    for (auto& f : size) cudaFreeAsync(f.first, s);
     size.clear();
     freeb.clear();
     pending.clear();
+    cudaStreamSynchronize(s);
   }
 };
 
@@ -1606,7 +1646,7 @@ void hodlr_destroy(hodlr_t h) {
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   if (h->stream) cudaStreamSynchronize(h->stream);
-  h->pool.release_all();
+  h->pool.release_all(h->stream);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
   delete h;
 }
@@ -1697,6 +1737,13 @@ int hodlr_gemm_device(int precision, int mode, int m, int n, int k, const double
   cudaFree(dws);
   cudaFree(derr);
   return rc;
+}
+
+int hodlr_trim_device_memory(void) {
+  cudaMemPool_t mp = device_pool();
+  if (!mp) return HODLR_ERR_CUDA;
+  if (cudaDeviceSynchronize() != cudaSuccess) return HODLR_ERR_CUDA;
+  return cudaMemPoolTrimTo(mp, 0) == cudaSuccess ? HODLR_OK : HODLR_ERR_CUDA;
 }
 
 int hodlr_set_capacity_hint(hodlr_t h, const int* caps, int nlevels) {

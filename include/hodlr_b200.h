@@ -173,6 +173,13 @@ int hodlr_get_aca_stats(hodlr_t h, int* launches, double* seconds, double* bytes
  * (src/lowRank.cpp:151-157). */
 int hodlr_set_capacity_hint(hodlr_t h, const int* caps, int nlevels);
 
+/* Device memory of all handles on the current device comes from one
+ * stream-ordered pool owned by the library; memory that hodlr_destroy frees
+ * stays reserved there for the next handle.  This returns it to the driver
+ * (after a device synchronise).  No reference counterpart: the reference
+ * allocates host memory per object. */
+int hodlr_trim_device_memory(void);
+
 /* Arithmetic of the Woodbury products (V^T K^-1 U, V^T X and the updates)
  * in the factorization and the solve.  FP64 (default) reproduces the
  * reference; TF32 and BF16 run them on the tcgen05 tensor cores with FP32
