@@ -36,6 +36,8 @@ _D = ctypes.c_double
 _PD = ctypes.POINTER(ctypes.c_double)
 _PI = ctypes.POINTER(ctypes.c_int)
 _V = ctypes.c_void_p
+_VP = ctypes.c_void_p
+_PF = ctypes.POINTER(ctypes.c_float)
 
 SIGNATURES = {
     "hodlr_create_kernel": (_I, [ctypes.POINTER(_H), _I, _I, _PD, ctypes.POINTER(KernelDesc), _I]),
@@ -47,6 +49,13 @@ SIGNATURES = {
     "hodlr_get_launch_count": (_I, [_H, ctypes.POINTER(ctypes.c_longlong)]),
     "hodlr_set_capacity_hint": (_I, [_H, _PI, _I]),
     "hodlr_trim_device_memory": (_I, []),
+    "hodlr_set_rank_model": (_I, [_H, _PF, _D]),
+    "hodlr_get_predicted_ranks": (_I, [_H, _PI]),
+    "hodlr_block_features": (_I, [_H, _D, _PF]),
+    "hodlr_mlp_scratch_floats": (_I, [_I, ctypes.POINTER(ctypes.c_longlong)]),
+    "hodlr_mlp_forward": (_I, [_VP, _VP, _I, _VP, _VP]),
+    "hodlr_mlp_train_step": (_I, [_VP, _VP, _VP, _VP, _VP, _I, _VP, ctypes.c_float, _I, _VP, _VP,
+                                  _VP]),
     "hodlr_set_precision": (_I, [_H, _I]),
     "hodlr_gemm_device": (_I, [_I, _I, _I, _I, _I, _V, _I, _V, _I, _V, _I, _V]),
     "hodlr_set_lr_tolerance": (_I, [_H, _D]),

@@ -27,7 +27,10 @@
 // (a zero residual row, the capacity limit) the dots take a pass of their own.
 // G = 1 for levels with many blocks (barriers are __syncthreads); G > 1 runs
 // under a cooperative launch so that a group's CTAs are co-resident, and its
-// barrier is a counter in global memory polled with a bounded spin.
+// barrier is a counter in global memory polled with a bounded spin.  Groups
+// are either all of size L.G (CTA c works on block c / G) or, with a CTA
+// table, of per-block size B.G starting at CTA B.g0 (sized from predicted
+// ranks so that a level's blocks finish together).
 #include "common.cuh"
 #include "hodlr_internal.h"
 
@@ -322,11 +325,14 @@ __global__ void __launch_bounds__(NT, (NT == 256 ? 2 : 4)) aca_kernel(AcaLaunch 
   extern __shared__ double dyn[];  // row[kcap], per-warp dots[NT/32][kcap]
   __shared__ Shared sh;
   constexpr int NW = NT / 32;
-  const int G = L.G;
-  const int b = blockIdx.x / G, g = blockIdx.x % G;
+  const int b = L.cta_block ? (blockIdx.x < (unsigned)L.ncta ? L.cta_block[blockIdx.x] : L.nblocks)
+                            : (int)(blockIdx.x / L.G);
   const int tid = threadIdx.x;
   if (b >= L.nblocks) return;
   const AcaBlock B = L.blocks[b];
+  const int G = L.cta_block ? B.G : L.G;
+  const int g = L.cta_block ? (int)blockIdx.x - B.g0 : (int)(blockIdx.x % L.G);
+  const int64_t grp0 = L.cta_block ? B.g0 : (int64_t)b * G;
   AcaState* st = B.st;
   if (st->status != ACA_RUNNING && st->status != ACA_POST) return;
 
@@ -337,7 +343,7 @@ __global__ void __launch_bounds__(NT, (NT == 256 ? 2 : 4)) aca_kernel(AcaLaunch 
   double* dotw = dyn + L.kcap_max;
   const int ldd = L.kcap_max;
   double* part_me = L.part + (int64_t)blockIdx.x * L.part_stride;
-  const double* part_grp = L.part + (int64_t)(b * G) * L.part_stride;
+  const double* part_grp = L.part + grp0 * L.part_stride;
   unsigned* bar = L.bar + b;
   unsigned gen = 0;
 
@@ -611,7 +617,7 @@ static size_t aca_smem(int nt, int kcap_max) {
 
 int aca_launch(const AcaLaunch& L, int nt, int kcap_max, bool cooperative, cudaStream_t s) {
   size_t smem = aca_smem(nt, kcap_max);
-  dim3 grid(L.nblocks * L.G), block(nt);
+  dim3 grid(L.cta_block ? L.ncta : L.nblocks * L.G), block(nt);
   void* args[] = {(void*)&L};
   void* fn = nt == 256 ? (void*)aca_kernel<256, 4> : (void*)aca_kernel<128, 2>;
   if (smem > 48 * 1024)

@@ -31,6 +31,7 @@
 #include "gemm.h"
 #include "kmatvec.h"
 #include "lu.h"
+#include "rank_mlp.h"
 
 int aca_launch(const AcaLaunch& L, int nt, int kcap_max, bool cooperative, cudaStream_t s);
 int aca_max_coresident(int nt, int kcap_max, int* per_sm);
@@ -188,6 +189,13 @@ struct DevPool {
 
 struct hodlr_handle_s {
   DevPool pool;
+  int* d_cta = nullptr;  // CTA -> block table of uneven ACA groups
+  int cta_cap = 0;
+  // rank predictor (rank_mlp.cu): FP32 parameter blob on the device, the
+  // length scale its features use, and the last predictions (block order)
+  float* d_model = nullptr;
+  double model_l = 0.0;
+  std::vector<int> pred;
   int n = 0, leaf = 30, dim = 0;
   bool dense = false;
   hx_kparams kp{};
@@ -475,6 +483,8 @@ void fill_block(hodlr_t h, Level& L, int q, AcaBlock& B) {
   B.n = n;
   B.kcap = L.kcap;
   B.level = 0;
+  B.g0 = 0;
+  B.G = 1;
 }
 
 bool level_done(const Level& L) {
@@ -484,9 +494,31 @@ bool level_done(const Level& L) {
 }
 
 // Run one ACA launch over `blocks` with group size G.
-int run_aca(hodlr_t h, std::vector<AcaBlock>& blocks, int G, int nt, int kcap_max) {
+// One ACA launch over `blocks`: groups of G CTAs each, or, with `groups`,
+// groups[i] CTAs for block i (a CTA table maps CTAs to blocks).
+int run_aca(hodlr_t h, std::vector<AcaBlock>& blocks, int G, int nt, int kcap_max,
+            const std::vector<int>* groups = nullptr) {
   const int nb = (int)blocks.size();
   if (nb == 0) return HODLR_OK;
+  int ncta = nb * G;
+  if (groups) {
+    ncta = 0;
+    for (int i = 0; i < nb; ++i) {
+      blocks[i].g0 = ncta;
+      blocks[i].G = (*groups)[i];
+      ncta += (*groups)[i];
+    }
+    std::vector<int> table((size_t)ncta);
+    for (int i = 0; i < nb; ++i)
+      for (int c = 0; c < blocks[i].G; ++c) table[(size_t)(blocks[i].g0 + c)] = i;
+    if (ncta > h->cta_cap) {
+      dfree(h, h->d_cta);
+      CK(dalloc(h, &h->d_cta, (size_t)ncta));
+      h->cta_cap = ncta;
+    }
+    CK(cudaMemcpyAsync(h->d_cta, table.data(), sizeof(int) * ncta, cudaMemcpyHostToDevice,
+                       h->stream));
+  }
   if (nb > h->blocks_cap) {
     dfree(h, h->d_blocks);
     CK(dalloc(h, &h->d_blocks, (size_t)nb));
@@ -495,7 +527,7 @@ int run_aca(hodlr_t h, std::vector<AcaBlock>& blocks, int G, int nt, int kcap_ma
   CK(cudaMemcpyAsync(h->d_blocks, blocks.data(), sizeof(AcaBlock) * nb, cudaMemcpyHostToDevice,
                      h->stream));
   int64_t stride = 12 + 4 * (int64_t)kcap_max;  // args + two banks of dots and norms
-  int64_t need = stride * nb * G;
+  int64_t need = stride * ncta;
   if (need > h->part_cap) {
     dfree(h, h->part);
     CK(dalloc(h, &h->part, (size_t)need));
@@ -520,10 +552,15 @@ int run_aca(hodlr_t h, std::vector<AcaBlock>& blocks, int G, int nt, int kcap_ma
   L.bar = h->bar;
   L.err = h->d_err;
   L.src = make_src(h);
+  L.cta_block = groups ? h->d_cta : nullptr;
+  L.ncta = ncta;
+  bool coop = G > 1;
+  if (groups)
+    for (int g : *groups) coop |= g > 1;
   CK(cudaEventRecord(h->ev0, h->stream));
   if ((size_t)(1 + nt / 32) * kcap_max * sizeof(double) > 227 * 1024)
     return fail(h, HODLR_ERR_UNSUPPORTED, "block rank above the shared-memory limit of ACA");
-  int rc = aca_launch(L, nt, kcap_max, G > 1, h->stream);
+  int rc = aca_launch(L, nt, kcap_max, coop, h->stream);
   if (rc) return cuda_fail(h, (cudaError_t)rc, "aca_launch");
   h->nlaunch += 1;
   CK(cudaEventRecord(h->ev1, h->stream));
@@ -609,6 +646,86 @@ int level_kmax(const Level& L) {
 // each with a group of CTAs per block.  They go bottom-up so that each
 // level's W/V capacity can be sized from the ranks of the level below it
 // (ranks shrink down the tree); a level that needs more grows and resumes.
+std::vector<int4> block_geoms(hodlr_t h) {
+  std::vector<int4> geom;
+  for (auto& L : h->lv)
+    for (int q = 0; q < L.nblocks(); ++q) {
+      int r0, c0, m, n;
+      block_geom(L, q, r0, c0, m, n);
+      geom.push_back(make_int4(r0, c0, m, n));
+    }
+  return geom;
+}
+
+// Features of every block (nb x HODLR_MLP_INPUTS, device) for length scale l.
+int block_features_dev(hodlr_t h, const std::vector<int4>& geom, double l, float* d_F) {
+  const int nb = (int)geom.size();
+  int4* d_geom = nullptr;
+  CK(dalloc(h, &d_geom, (size_t)nb));
+  CK(cudaMemcpyAsync(d_geom, geom.data(), sizeof(int4) * nb, cudaMemcpyHostToDevice, h->stream));
+  int e = block_features_launch(h->d_pts, h->n, h->dim, d_geom, nb, (float)std::log(l),
+                                (float)std::log(h->tol), d_F, h->stream);
+  if (e) return cuda_fail(h, (cudaError_t)e, "block features");
+  h->nlaunch += 1;
+  dfree(h, d_geom);
+  return HODLR_OK;
+}
+
+// Predicted ACA rank of every block (level-major order, as
+// hodlr_get_block_info numbers them) from the rank model: block features on
+// the device, the MLP forward, rank = exp(y) - 1 rounded and clamped.
+int predict_ranks(hodlr_t h) {
+  const std::vector<int4> geom = block_geoms(h);
+  const int nb = (int)geom.size();
+  h->pred.assign(nb, 0);
+  if (nb == 0) return HODLR_OK;
+  float *d_F = nullptr, *d_y = nullptr;
+  CK(dalloc(h, &d_F, (size_t)nb * HODLR_MLP_INPUTS));
+  CK(dalloc(h, &d_y, (size_t)nb));
+  int rc = block_features_dev(h, geom, h->model_l, d_F);
+  if (rc) return rc;
+  int e = mlp_forward_launch(h->d_model, d_F, nb, d_y, h->stream);
+  if (e) return cuda_fail(h, (cudaError_t)e, "rank prediction");
+  h->nlaunch += 1;
+  std::vector<float> y((size_t)nb);
+  CK(d2h(h, y.data(), d_y, sizeof(float) * nb));
+  dfree(h, d_F);
+  dfree(h, d_y);
+  for (int i = 0; i < nb; ++i) {
+    const double r = std::expm1((double)std::min(y[i], 20.0f));
+    const int ub = std::min(geom[i].z, geom[i].w);
+    h->pred[i] = std::max(0, std::min(ub, (int)std::lround(r)));
+  }
+  return HODLR_OK;
+}
+
+// CTAs per block of a level launch in proportion to the predicted ACA work
+// (m + n)(k + 1)^2, at least one each, P in total.
+std::vector<int> weighted_groups(const std::vector<double>& w, int P) {
+  const int nb = (int)w.size();
+  double W = 0;
+  for (double x : w) W += x;
+  std::vector<int> g(nb, 1);
+  if (nb == 0 || P <= nb || W <= 0) return g;
+  std::vector<std::pair<double, int>> rem;
+  int used = 0;
+  for (int i = 0; i < nb; ++i) {
+    const double raw = (double)P * w[i] / W;
+    g[i] = std::max(1, (int)raw);
+    used += g[i];
+    rem.push_back({raw - (int)raw, i});
+  }
+  while (used > P) {  // take back from the largest groups
+    int j = (int)(std::max_element(g.begin(), g.end()) - g.begin());
+    if (g[j] <= 1) break;
+    --g[j];
+    --used;
+  }
+  std::sort(rem.begin(), rem.end(), [](auto& a, auto& b) { return a.first > b.first; });
+  for (size_t t = 0; used < P && t < rem.size(); ++t, ++used) ++g[rem[t].second];
+  return g;
+}
+
 int do_compress(hodlr_t h) {
   if (h->compressed) return HODLR_OK;
   free_compress(h);
@@ -616,9 +733,28 @@ int do_compress(hodlr_t h) {
   h->aca_seconds = 0;
   h->aca_bytes = 0;
   const int nlev = (int)h->lv.size();
-  auto hint = [&](int l) {
-    return (l < (int)h->cap_hint.size() && h->cap_hint[l] > 0) ? h->cap_hint[l] : 0;
+  // predicted ranks, when a rank model is set: level capacities, the order
+  // of the pooled blocks and the CTA groups of the few-block levels follow
+  // them; ACA's stopping test still decides every rank (a block that needs
+  // more columns pauses and resumes after its level grows)
+  std::vector<int> lbase(nlev + 1, 0);
+  for (int l = 0; l < nlev; ++l) lbase[l + 1] = lbase[l] + h->lv[l].nblocks();
+  const bool have_pred = h->d_model != nullptr;
+  if (have_pred) {
+    int rc = predict_ranks(h);
+    if (rc) return rc;
+  }
+  auto pred = [&](int l, int q) { return h->pred[(size_t)(lbase[l] + q)]; };
+  auto pred_cap = [&](int l) {
+    int mx = 0;
+    for (int q = 0; q < h->lv[l].nblocks(); ++q) mx = std::max(mx, pred(l, q));
+    return std::max(16, ((mx + mx / 4 + 8) + 7) / 8 * 8);
   };
+  auto hint = [&](int l) {
+    if (l < (int)h->cap_hint.size() && h->cap_hint[l] > 0) return h->cap_hint[l];
+    return have_pred ? pred_cap(l) : 0;
+  };
+  auto pred_or = [&](int l, int q) -> int64_t { return have_pred ? pred(l, q) + 1 : 1; };
   int per_sm = 0;
   if (aca_max_coresident(256, 256, &per_sm))
     return fail(h, HODLR_ERR_CUDA, "occupancy query failed");
@@ -642,7 +778,8 @@ int do_compress(hodlr_t h) {
         if (L.st[q].status == ACA_DONE) continue;
         AcaBlock B;
         fill_block(h, L, q, B);
-        sorted.push_back({(int64_t)B.m * B.n, B});
+        const int64_t k1 = pred_or(l, q);
+        sorted.push_back({have_pred ? (int64_t)(B.m + B.n) * k1 * k1 : (int64_t)B.m * B.n, B});
       }
     }
     if (sorted.empty()) break;
@@ -676,11 +813,29 @@ int do_compress(hodlr_t h) {
       if (aca_max_coresident(256, L.kcap, &ps))
         return fail(h, HODLR_ERR_CUDA, "occupancy query failed");
       const int nb = L.nblocks();
-      const int G = std::max(1, std::max(1, ps) * h->num_sms / nb);
-      L.G = G;
-      std::vector<AcaBlock> bl(nb);
-      for (int q = 0; q < nb; ++q) fill_block(h, L, q, bl[q]);
-      rc = run_aca(h, bl, G, G > 1 ? 256 : 128, L.kcap);
+      const int P = std::max(1, ps) * h->num_sms;
+      if (have_pred && nb <= P) {  // groups sized by predicted work
+        std::vector<AcaBlock> bl;
+        std::vector<double> w;
+        for (int q = 0; q < nb; ++q) {
+          if (L.st[q].status == ACA_DONE) continue;
+          AcaBlock B;
+          fill_block(h, L, q, B);
+          const double k1 = (double)pred_or(l, q);
+          bl.push_back(B);
+          w.push_back((double)(B.m + B.n) * k1 * k1);
+        }
+        std::vector<int> groups = weighted_groups(w, P);
+        L.G = 0;
+        for (int g : groups) L.G = std::max(L.G, g);
+        rc = run_aca(h, bl, 1, 256, L.kcap, &groups);
+      } else {
+        const int G = std::max(1, P / nb);
+        L.G = G;
+        std::vector<AcaBlock> bl(nb);
+        for (int q = 0; q < nb; ++q) fill_block(h, L, q, bl[q]);
+        rc = run_aca(h, bl, G, G > 1 ? 256 : 128, L.kcap);
+      }
       if (rc) return rc;
       bool done;
       rc = sync_level(h, L, &done);
@@ -1642,6 +1797,8 @@ void hodlr_destroy(hodlr_t h) {
   dfree(h, h->part);
   dfree(h, h->bar);
   dfree(h, h->d_blocks);
+  dfree(h, h->d_cta);
+  dfree(h, h->d_model);
   dfree(h, h->d_err);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
@@ -1737,6 +1894,70 @@ int hodlr_gemm_device(int precision, int mode, int m, int n, int k, const double
   cudaFree(dws);
   cudaFree(derr);
   return rc;
+}
+
+int hodlr_set_rank_model(hodlr_t h, const float* params, double length_scale) {
+  if (!h) return HODLR_ERR_ARG;
+  if (!params) {
+    dfree(h, h->d_model);
+    return HODLR_OK;
+  }
+  if (h->dense) return fail(h, HODLR_ERR_UNSUPPORTED, "the rank model needs point coordinates");
+  if (!(length_scale > 0)) return HODLR_ERR_ARG;
+  for (int i = 0; i < HODLR_MLP_PARAMS; ++i)
+    if (!std::isfinite(params[i])) return fail(h, HODLR_ERR_ARG, "non-finite model parameter");
+  if (!h->d_model) CK(dalloc(h, &h->d_model, (size_t)HODLR_MLP_PARAMS));
+  CK(h2d(h, h->d_model, params, sizeof(float) * HODLR_MLP_PARAMS));
+  h->model_l = length_scale;
+  return HODLR_OK;
+}
+
+int hodlr_get_predicted_ranks(hodlr_t h, int* ranks) {
+  if (!h || !ranks) return HODLR_ERR_ARG;
+  if (!h->d_model) return fail(h, HODLR_ERR_STATE, "no rank model set");
+  int rc = predict_ranks(h);
+  if (rc) return rc;
+  std::copy(h->pred.begin(), h->pred.end(), ranks);
+  return HODLR_OK;
+}
+
+int hodlr_block_features(hodlr_t h, double length_scale, float* features) {
+  if (!h || !features || !(length_scale > 0)) return HODLR_ERR_ARG;
+  if (h->dense) return fail(h, HODLR_ERR_UNSUPPORTED, "block features need point coordinates");
+  const std::vector<int4> geom = block_geoms(h);
+  const int nb = (int)geom.size();
+  if (nb == 0) return HODLR_OK;
+  float* d_F = nullptr;
+  CK(dalloc(h, &d_F, (size_t)nb * HODLR_MLP_INPUTS));
+  int rc = block_features_dev(h, geom, length_scale, d_F);
+  if (rc) return rc;
+  CK(d2h(h, features, d_F, sizeof(float) * nb * HODLR_MLP_INPUTS));
+  dfree(h, d_F);
+  return HODLR_OK;
+}
+
+int hodlr_mlp_scratch_floats(int batch, long long* floats) {
+  if (batch < 1 || !floats) return HODLR_ERR_ARG;
+  *floats = (long long)batch * mlp_sample_floats();
+  return HODLR_OK;
+}
+
+int hodlr_mlp_forward(const float* d_params, const float* d_X, int batch, float* d_y,
+                      void* stream) {
+  if (!d_params || !d_X || !d_y || batch < 1) return HODLR_ERR_ARG;
+  int e = mlp_forward_launch(d_params, d_X, batch, d_y, (cudaStream_t)stream);
+  if (e || cudaStreamSynchronize((cudaStream_t)stream) != cudaSuccess) return HODLR_ERR_CUDA;
+  return HODLR_OK;
+}
+
+int hodlr_mlp_train_step(float* d_params, float* d_m1, float* d_m2, const float* d_X,
+                         const float* d_T, int batch, float* d_scratch, float lr, int step,
+                         float* d_grad, float* d_loss, void* stream) {
+  if (!d_params || !d_X || !d_T || !d_scratch || batch < 1) return HODLR_ERR_ARG;
+  if (lr > 0 && (!d_m1 || !d_m2 || step < 1)) return HODLR_ERR_ARG;
+  int e = mlp_train_launch(d_params, d_m1, d_m2, d_X, d_T, batch, d_scratch, lr, step, d_grad,
+                           d_loss, (cudaStream_t)stream);
+  return e ? HODLR_ERR_CUDA : HODLR_OK;
 }
 
 int hodlr_trim_device_memory(void) {

@@ -42,6 +42,7 @@ struct AcaBlock {
   int r0, c0, m, n;
   int kcap;           // columns available in W and V
   int level;
+  int g0, G;          // with a CTA table: first CTA of this block's group, group size
 };
 
 // Loop state of one block; lets a paused block resume where it stopped.
@@ -65,4 +66,6 @@ struct AcaLaunch {
   unsigned* bar;         // per-block barrier counters (zeroed before launch)
   unsigned* err;         // device error word
   EntrySrc src;
+  const int* cta_block;  // CTA -> block (groups of uneven size, AcaBlock::g0/G), or null
+  int ncta;              // CTAs of the launch when cta_block is set
 };

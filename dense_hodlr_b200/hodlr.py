@@ -348,6 +348,29 @@ class HODLR_Matrix:
                                                         ctypes.byref(n)))
         return m.value, n.value
 
+    # rank predictor (csrc/rank_mlp.cu)
+    def set_rank_model(self, params, length_scale):
+        """FP32 parameter blob of the rank MLP (None removes it) and the
+        kernel length scale of the log-l feature."""
+        if params is None:
+            _check(self._h, _L.lib().hodlr_set_rank_model(self._h, None, 0.0))
+            return
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        _check(self._h, _L.lib().hodlr_set_rank_model(
+            self._h, p.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), float(length_scale)))
+
+    def predicted_ranks(self):
+        out = np.zeros(self.num_blocks(), dtype=np.int32)
+        _check(self._h, _L.lib().hodlr_get_predicted_ranks(
+            self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int))))
+        return out
+
+    def block_features(self, length_scale):
+        out = np.zeros((self.num_blocks(), 14), dtype=np.float32)
+        _check(self._h, _L.lib().hodlr_block_features(
+            self._h, float(length_scale), out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+        return out
+
     def aca_stats(self):
         a, s, b = ctypes.c_int(), ctypes.c_double(), ctypes.c_double()
         _check(self._h, _L.lib().hodlr_get_aca_stats(self._h, ctypes.byref(a), ctypes.byref(s),

@@ -180,6 +180,47 @@ int hodlr_set_capacity_hint(hodlr_t h, const int* caps, int nlevels);
  * allocates host memory per object. */
 int hodlr_trim_device_memory(void);
 
+/* ------------------------------------------------------------------------
+ * Learned rank predictor.  No reference counterpart: the reference learns
+ * nothing and grows W and V by doubling as ACA runs
+ * (src/lowRank.cpp:151-157).  A 14-64-64-1 MLP with GELU, BF16 with FP32
+ * accumulation, maps a block's features -- the bounding-box centre (3) and
+ * extent (3) of its row cluster, then of its column cluster (axes beyond
+ * the points' dimension are 0), log l and log tol -- to log(1 + ACA rank).
+ * Parameters are one FP32 blob of HODLR_MLP_PARAMS floats:
+ * [mean(14) | inv_std(14) | W1 64x14 | b1(64) | W2 64x64 | b2(64) | W3(64) | b3],
+ * row-major weights; inputs are standardised as (x - mean) * inv_std.
+ * With a model set, hodlr_compress predicts every block's rank first and
+ * sizes each level's W/V capacity and each block's CTA group from the
+ * predictions; ACA's own stopping test still decides every rank.
+ * ------------------------------------------------------------------------ */
+#define HODLR_MLP_INPUTS 14
+#define HODLR_MLP_HIDDEN 64
+#define HODLR_MLP_PARAMS 5213
+
+/* Model for this handle (host blob; NULL removes it) and the kernel length
+ * scale its log l feature uses.  Point-coordinate handles only. */
+int hodlr_set_rank_model(hodlr_t h, const float* params, double length_scale);
+/* Predicted rank of every block, in hodlr_get_block_info order. */
+int hodlr_get_predicted_ranks(hodlr_t h, int* ranks);
+/* Features of every block (num_blocks x 14, row-major, host) for training. */
+int hodlr_block_features(hodlr_t h, double length_scale, float* features);
+
+/* Device-side MLP: forward y[b] = MLP(X[b, :]) for X row-major batch x 14;
+ * one training step (forward, backward, gradient summed over the batch in
+ * sample order; Adam with beta 0.9/0.999, eps 1e-8 when lr > 0, step >= 1)
+ * on loss 1/batch sum (y_b - T_b)^2, optional d_grad (trained parameters,
+ * HODLR_MLP_PARAMS - 28 floats, blob order after the standardisation) and
+ * d_loss (one float).  d_scratch holds hodlr_mlp_scratch_floats(batch)
+ * floats; d_m1 and d_m2 are the Adam moments of the trained parameters.
+ * The train step is asynchronous on `stream`. */
+int hodlr_mlp_scratch_floats(int batch, long long* floats);
+int hodlr_mlp_forward(const float* d_params, const float* d_X, int batch, float* d_y,
+                      void* stream);
+int hodlr_mlp_train_step(float* d_params, float* d_m1, float* d_m2, const float* d_X,
+                         const float* d_T, int batch, float* d_scratch, float lr, int step,
+                         float* d_grad, float* d_loss, void* stream);
+
 /* Arithmetic of the Woodbury products (V^T K^-1 U, V^T X and the updates)
  * in the factorization and the solve.  FP64 (default) reproduces the
  * reference; TF32 and BF16 run them on the tcgen05 tensor cores with FP32
