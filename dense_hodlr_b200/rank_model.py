@@ -1,0 +1,198 @@
+"""Rank predictor: training data from plain ACA, training and inference on
+the GPU through the CUDA kernels of csrc/rank_mlp.cu (hodlr_mlp_* entry
+points), and the trained models shipped with the package.
+
+Data: plain ACA (no model) on seeded 3D clouds -- uniform cube, 8-component
+Gaussian mixture with sigma 0.05, uniform on the unit sphere -- with the
+length scale log-uniform in [0.05, 0.5], ACA tol in {1e-6, 1e-8, 1e-10},
+leaf sizes 32 to 128 and N from 8192 to 32768; every off-diagonal block gives
+one (features, log(1 + rank)) pair.  One network per kernel family.
+
+    python -m dense_hodlr_b200.rank_model train --kernel matern32 \\
+        --pairs 200000 --out dense_hodlr_b200/rank_mlp_matern32.npz
+
+PyTorch only holds device memory and the stream; the arithmetic is in the
+project's kernels.
+"""
+import argparse
+import ctypes
+import json
+import os
+import time
+
+import numpy as np
+
+from . import _lib as _L
+from .hodlr import HODLR_Matrix, HODLRError, KernelSpec
+from .points import gaussian_mixture, uniform_cube, unit_sphere
+
+NI, NH = 14, 64
+NPARAM = 5213
+NTRAIN = NPARAM - 2 * NI
+HERE = os.path.dirname(os.path.abspath(__file__))
+CLOUDS = ("cube", "mixture", "sphere")
+
+
+def model_path(kind):
+    return os.path.join(HERE, f"rank_mlp_{kind}.npz")
+
+
+def load(kind_or_path):
+    """Parameter blob of a shipped model ('gaussian', 'matern32') or a file;
+    None if absent."""
+    p = kind_or_path if kind_or_path.endswith(".npz") else model_path(kind_or_path)
+    if not os.path.exists(p):
+        return None
+    return np.load(p)["params"].astype(np.float32)
+
+
+def cloud(name, n, seed):
+    if name == "cube":
+        return uniform_cube(n, 3, seed)
+    if name == "mixture":
+        return gaussian_mixture(n, seed, components=8, sigma=0.05)
+    return unit_sphere(n, seed)
+
+
+def block_dataset(pts, kind, l, tol, leaf):
+    """(features, log(1 + rank)) of every block of one plain compression."""
+    n = pts.shape[1]
+    g = HODLR_Matrix(n, n, KernelSpec(kind, l, 1e-2), pts, leaf)
+    g.set_LRTolerance(tol)
+    g.storeLRinTree()
+    return g.block_features(l), np.log1p(g.ranks().astype(np.float64)).astype(np.float32)
+
+
+def generate(kind, pairs, seed=0, max_seconds=900.0, log=None):
+    rng = np.random.default_rng(seed)
+    Fs, Ts = [], []
+    total, run = 0, 0
+    t0 = time.time()
+    while total < pairs and time.time() - t0 < max_seconds:
+        name = CLOUDS[run % 3]
+        n = int(rng.choice([8192, 16384, 32768]))
+        leaf = int(rng.choice([32, 64, 128]))
+        l = float(np.exp(rng.uniform(np.log(0.05), np.log(0.5))))
+        tol = float(rng.choice([1e-6, 1e-8, 1e-10]))
+        run += 1
+        try:
+            F, T = block_dataset(cloud(name, n, seed * 1000 + run), kind, l, tol, leaf)
+        except HODLRError as e:  # e.g. a rank beyond ACA's shared-memory limit
+            if log:
+                log(f"skip {name} n={n} leaf={leaf} l={l:.3f} tol={tol:g}: {e}")
+            continue
+        Fs.append(F)
+        Ts.append(T)
+        total += len(T)
+    return np.concatenate(Fs), np.concatenate(Ts)
+
+
+def init_params(X, T, seed=0):
+    rng = np.random.default_rng(seed)
+    p = np.zeros(NPARAM, np.float32)
+    mean = X.mean(0)
+    std = X.std(0)
+    std[std < 1e-6] = 1.0
+    p[0:NI] = mean
+    p[NI:2 * NI] = 1.0 / std
+    o = 2 * NI
+    p[o:o + NH * NI] = rng.standard_normal(NH * NI) * np.sqrt(2.0 / NI)
+    o += NH * NI + NH
+    p[o:o + NH * NH] = rng.standard_normal(NH * NH) * np.sqrt(2.0 / NH)
+    o += NH * NH + NH
+    p[o:o + NH] = rng.standard_normal(NH) * np.sqrt(1.0 / NH)
+    p[o + NH] = float(np.mean(T))
+    return p
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def train(X, T, epochs=40, batch=1024, lr=2e-3, seed=0, params=None, log=None):
+    """Adam on 1/B sum (y - t)^2 with a cosine learning rate; returns the
+    parameter blob and the per-epoch mean training loss."""
+    import torch
+    lib = _L.lib()
+    dev = torch.device("cuda")
+    stream = torch.cuda.current_stream(dev)
+    p = torch.from_numpy(init_params(X, T, seed) if params is None else params.copy()).to(dev)
+    m1 = torch.zeros(NTRAIN, dtype=torch.float32, device=dev)
+    m2 = torch.zeros_like(m1)
+    nsc = ctypes.c_longlong()
+    assert lib.hodlr_mlp_scratch_floats(batch, ctypes.byref(nsc)) == 0
+    S = torch.empty(nsc.value, dtype=torch.float32, device=dev)
+    Xd = torch.from_numpy(np.ascontiguousarray(X, np.float32)).to(dev)
+    Td = torch.from_numpy(np.ascontiguousarray(T, np.float32)).to(dev)
+    loss = torch.zeros(1, dtype=torch.float32, device=dev)
+    gen = torch.Generator(device="cpu").manual_seed(seed)
+    n = len(T)
+    steps = epochs * (n // batch)
+    t = 0
+    hist = []
+    for ep in range(epochs):
+        perm = torch.randperm(n, generator=gen).to(dev)
+        acc = torch.zeros(1, dtype=torch.float32, device=dev)
+        for s0 in range(0, n - batch + 1, batch):
+            idx = perm[s0:s0 + batch]
+            xb = Xd.index_select(0, idx).contiguous()
+            tb = Td.index_select(0, idx).contiguous()
+            t += 1
+            cur = 0.5 * lr * (1.0 + np.cos(np.pi * (t - 1) / max(1, steps)))
+            rc = lib.hodlr_mlp_train_step(_ptr(p), _ptr(m1), _ptr(m2), _ptr(xb), _ptr(tb), batch,
+                                          _ptr(S), ctypes.c_float(cur), t, None, _ptr(loss),
+                                          ctypes.c_void_p(stream.cuda_stream))
+            if rc:
+                raise HODLRError(rc, "hodlr_mlp_train_step")
+            acc += loss
+        hist.append(float(acc.item()) / max(1, n // batch))
+        if log:
+            log(f"epoch {ep + 1}/{epochs} loss {hist[-1]:.5f}")
+    return p.cpu().numpy(), hist
+
+
+def predict(params, X):
+    """log(1 + rank) predicted for feature rows X (GPU forward kernel)."""
+    import torch
+    lib = _L.lib()
+    dev = torch.device("cuda")
+    pd = torch.from_numpy(np.ascontiguousarray(params, np.float32)).to(dev)
+    Xd = torch.from_numpy(np.ascontiguousarray(X, np.float32)).to(dev)
+    y = torch.empty(len(X), dtype=torch.float32, device=dev)
+    rc = lib.hodlr_mlp_forward(_ptr(pd), _ptr(Xd), len(X), _ptr(y),
+                               ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream))
+    if rc:
+        raise HODLRError(rc, "hodlr_mlp_forward")
+    return y.cpu().numpy()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("cmd", choices=["train"])
+    ap.add_argument("--kernel", default="matern32", choices=["gaussian", "matern32"])
+    ap.add_argument("--pairs", type=int, default=200000)
+    ap.add_argument("--epochs", type=int, default=40)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--max-seconds", type=float, default=900.0, help="data generation budget")
+    ap.add_argument("--out", default=None)
+    ap.add_argument("--data-out", default=None, help="also save the (features, target) pairs")
+    a = ap.parse_args()
+    t0 = time.time()
+    X, T = generate(a.kernel, a.pairs, a.seed, a.max_seconds, log=print)
+    t1 = time.time()
+    hold = np.random.default_rng(a.seed + 7).random(len(T)) < 0.1
+    params, hist = train(X[~hold], T[~hold], epochs=a.epochs, seed=a.seed, log=print)
+    y = predict(params, X[hold])
+    meta = {"kernel": a.kernel, "pairs": int(len(T)), "epochs": a.epochs,
+            "train_loss": hist[-1], "holdout_mse": float(np.mean((y - T[hold]) ** 2)),
+            "holdout_median_abs_log_err": float(np.median(np.abs(y - T[hold]))),
+            "data_s": t1 - t0, "train_s": time.time() - t1}
+    print(json.dumps(meta))
+    out = a.out or model_path(a.kernel)
+    np.savez(out, params=params, meta=json.dumps(meta))
+    if a.data_out:
+        np.savez_compressed(a.data_out, X=X, T=T)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,159 @@
+"""Rank-predictor MLP: the oracle pinned by finite differences (CPU), the
+CUDA forward pass and gradients against the oracle, training, and what the
+shipped model gains ACA (GPU)."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from oracle import rank_mlp as orc
+
+NTRAIN = orc.NTRAIN
+
+
+def _random_params(seed, X):
+    rng = np.random.default_rng(seed)
+    p = np.zeros(orc.NPARAM, np.float32)
+    p[:14] = X.mean(0)
+    s = X.std(0)
+    s[s < 1e-6] = 1.0
+    p[14:28] = 1.0 / s
+    p[28:] = rng.standard_normal(orc.NPARAM - 28) * 0.3
+    return p
+
+
+def _features(n, seed):
+    rng = np.random.default_rng(seed)
+    X = np.zeros((n, 14), np.float32)
+    X[:, 0:3] = rng.uniform(0, 1, (n, 3))
+    X[:, 3:6] = rng.uniform(0, 0.5, (n, 3))
+    X[:, 6:9] = rng.uniform(0, 1, (n, 3))
+    X[:, 9:12] = rng.uniform(0, 0.5, (n, 3))
+    X[:, 12] = np.log(rng.uniform(0.05, 0.5, n))
+    X[:, 13] = np.log(rng.choice([1e-6, 1e-8, 1e-10], n))
+    return X
+
+
+def test_bf16_rounding_is_nearest_even():
+    vals = np.array([1.0, 1.0 + 2 ** -8, 1.0 + 2 ** -7 + 2 ** -8, 1.0 + 2 ** -9, -3.14159],
+                    np.float32)
+    got = orc.bf16(vals)
+    assert got[0] == 1.0
+    assert got[1] == 1.0                      # tie -> even
+    assert got[2] == 1.0 + 2 ** -6            # tie -> even (odd neighbour below)
+    assert got[3] == 1.0                      # below half an ulp
+    assert abs(got[4] + 3.14159) < 2 ** -7 * 4
+
+
+def test_oracle_gradient_matches_finite_differences():
+    X = _features(40, 1)
+    T = np.random.default_rng(2).uniform(0, 5, 40)
+    p = _random_params(3, X).astype(np.float64)
+    _, g = orc.loss_grad(p, X, T, bf16_round=False)
+    rng = np.random.default_rng(4)
+    for q in rng.choice(NTRAIN, 60, replace=False):
+        h = 1e-6
+        pp, pm = p.copy(), p.copy()
+        pp[28 + q] += h
+        pm[28 + q] -= h
+        fd = (orc.loss(pp, X, T, False) - orc.loss(pm, X, T, False)) / (2 * h)
+        assert abs(fd - g[q]) <= 1e-6 * (1 + abs(fd)), (q, fd, g[q])
+
+
+def _dev(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+@pytest.mark.gpu
+def test_mlp_forward_matches_oracle():
+    from dense_hodlr_b200 import _lib
+    import torch
+    X = _features(300, 5)
+    p = _random_params(6, X)
+    y = torch.empty(300, dtype=torch.float32, device="cuda")
+    assert _lib.lib().hodlr_mlp_forward(_ptr(_dev(p)), _ptr(_dev(X)), 300, _ptr(y), None) == 0
+    yo, _ = orc.forward(p, X)
+    err = np.abs(y.cpu().numpy() - yo) / (1 + np.abs(yo))
+    # bit-equal but for a hidden unit whose BF16 rounding flips with the last
+    # bit of erf (CUDA's erff against a correctly rounded erf)
+    assert np.mean(err > 1e-6) < 0.02, np.sort(err)[-10:]
+    assert err.max() < 2e-2
+
+
+@pytest.mark.gpu
+def test_mlp_gradient_matches_oracle():
+    """The CUDA backward pass (lr = 0: gradient only) against the oracle's,
+    BF16 rounding at the same points, FP32 vs FP64 accumulation."""
+    from dense_hodlr_b200 import _lib
+    import torch
+    lib = _lib.lib()
+    B = 512
+    X = _features(B, 7)
+    T = np.random.default_rng(8).uniform(0, 6, B).astype(np.float32)
+    p = _random_params(9, X)
+    n = ctypes.c_longlong()
+    assert lib.hodlr_mlp_scratch_floats(B, ctypes.byref(n)) == 0
+    S = torch.empty(n.value, dtype=torch.float32, device="cuda")
+    grad = torch.empty(NTRAIN, dtype=torch.float32, device="cuda")
+    loss = torch.empty(1, dtype=torch.float32, device="cuda")
+    pd = _dev(p)
+    assert lib.hodlr_mlp_train_step(_ptr(pd), None, None, _ptr(_dev(X)), _ptr(_dev(T)), B,
+                                    _ptr(S), ctypes.c_float(0.0), 0, _ptr(grad), _ptr(loss),
+                                    None) == 0
+    torch.cuda.synchronize()
+    lo, go = orc.loss_grad(p, X, T)
+    g = grad.cpu().numpy().astype(np.float64)
+    assert abs(loss.item() - lo) <= 1e-4 * lo
+    assert np.linalg.norm(g - go) / np.linalg.norm(go) < 1e-3
+    for a, b in ((0, 896), (896, 960), (960, 5056), (5056, 5120), (5120, 5184), (5184, 5185)):
+        assert np.linalg.norm(g[a:b] - go[a:b]) <= 2e-3 * np.linalg.norm(go[a:b]) + 1e-7
+    assert np.array_equal(pd.cpu().numpy(), p)  # lr = 0 leaves the parameters
+
+
+@pytest.mark.gpu
+def test_mlp_training_fits_a_smooth_target():
+    from dense_hodlr_b200 import rank_model
+    X = _features(20000, 10)
+    T = (2.0 + np.sin(3 * X[:, 0]) + X[:, 3] * 4 - 0.2 * X[:, 13]).astype(np.float32)
+    params, hist = rank_model.train(X, T, epochs=15, batch=512, lr=3e-3, seed=1)
+    assert hist[-1] < 0.05 * hist[0]
+    y = rank_model.predict(params, X[:1000])
+    assert np.mean((y - T[:1000]) ** 2) < 0.05
+
+
+@pytest.mark.gpu
+def test_rank_model_gain_on_held_out_cloud():
+    """The shipped Matern-3/2 model on a cloud it was not trained on: the
+    predictions track ACA's ranks, ACA's results are unchanged (its stopping
+    test decides), and the predicted capacities remove the W/V regrowth
+    relaunches of the plain bottom-up guess."""
+    from dense_hodlr_b200 import HODLR_Matrix, KernelSpec, _lib, rank_model
+    params = rank_model.load("matern32")
+    assert params is not None, "dense_hodlr_b200/rank_mlp_matern32.npz missing"
+    pts = rank_model.cloud("mixture", 32768, 987654)
+    spec = KernelSpec("matern32", 0.1, 1e-2)
+
+    def run(model):
+        g = HODLR_Matrix(32768, 32768, spec, pts, 64)
+        g.set_LRTolerance(1e-8)
+        if model is not None:
+            g.set_rank_model(model, 0.1)
+        g.storeLRinTree()  # warm the device pool
+        assert _lib.lib().hodlr_reset(g._h) == 0
+        g.storeLRinTree()
+        return g
+
+    g0, g1 = run(None), run(params)
+    r0, r1 = g0.ranks(), g1.ranks()
+    near = np.array([g0.margin(b)[0] < 1e-6 for b in range(g0.num_blocks())])
+    assert np.array_equal(r0[~near], r1[~near])
+    pred = g1.predicted_ranks()
+    err = np.abs(np.log1p(pred) - np.log1p(r0))
+    assert np.median(err) < 0.3, np.median(err)
+    s0, s1 = g0.aca_stats(), g1.aca_stats()
+    assert s1["launches"] <= s0["launches"], (s0, s1)
