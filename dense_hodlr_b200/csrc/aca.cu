@@ -322,7 +322,7 @@ __device__ double resolve_eps(Shared& sh, const AcaLaunch& L, const AcaBlock& B,
 
 template <int NT, int E>
 __global__ void __launch_bounds__(NT, (NT == 256 ? 2 : 4)) aca_kernel(AcaLaunch L) {
-  extern __shared__ double dyn[];  // row[kcap], per-warp dots[NT/32][kcap]
+  extern __shared__ double dyn[];  // row[kcap], then (unless L.dotg) per-warp dots[NT/32][kcap]
   __shared__ Shared sh;
   constexpr int NW = NT / 32;
   const int b = L.cta_block ? (blockIdx.x < (unsigned)L.ncta ? L.cta_block[blockIdx.x] : L.nblocks)
@@ -340,7 +340,9 @@ __global__ void __launch_bounds__(NT, (NT == 256 ? 2 : 4)) aca_kernel(AcaLaunch 
   const int m = B.m, n = B.n, ub = min(m, n);
   const double tol = L.tol, minPiv = L.minPivot;
   double* row = dyn;
-  double* dotw = dyn + L.kcap_max;
+  // per-warp dot partials: shared memory, or for large ranks this CTA's
+  // slice of global memory (same writers and order: only the footprint moves)
+  double* dotw = L.dotg ? L.dotg + (int64_t)blockIdx.x * L.dotg_stride : dyn + L.kcap_max;
   const int ldd = L.kcap_max;
   double* part_me = L.part + (int64_t)blockIdx.x * L.part_stride;
   const double* part_grp = L.part + grp0 * L.part_stride;
@@ -611,29 +613,48 @@ __global__ void __launch_bounds__(NT, (NT == 256 ? 2 : 4)) aca_kernel(AcaLaunch 
 
 }  // namespace
 
-static size_t aca_smem(int nt, int kcap_max) {
-  return sizeof(double) * (size_t)(1 + nt / 32) * (size_t)kcap_max;
+static size_t aca_smem(int nt, int kcap_max, bool global_dots) {
+  return sizeof(double) * (size_t)(global_dots ? 1 : 1 + nt / 32) * (size_t)kcap_max;
+}
+
+// The per-warp dot partials move to global memory once they would take more
+// than 100 KB of shared memory per CTA: beyond that fewer than two 256-thread
+// CTAs fit on an SM, and past 227 KB none would.
+bool aca_dots_global(int nt, int kcap_max) {
+  return aca_smem(nt, kcap_max, false) > 100 * 1024;
+}
+
+size_t aca_smem_bytes(int nt, int kcap_max) {
+  return aca_smem(nt, kcap_max, aca_dots_global(nt, kcap_max));
+}
+
+static int set_smem(void* fn, size_t smem) {
+  if (smem <= 48 * 1024) return 0;
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) cudaGetLastError();  // consume it: later launch checks stay clean
+  return (int)e;
 }
 
 int aca_launch(const AcaLaunch& L, int nt, int kcap_max, bool cooperative, cudaStream_t s) {
-  size_t smem = aca_smem(nt, kcap_max);
+  const size_t smem = aca_smem(nt, kcap_max, L.dotg != nullptr);
   dim3 grid(L.cta_block ? L.ncta : L.nblocks * L.G), block(nt);
   void* args[] = {(void*)&L};
   void* fn = nt == 256 ? (void*)aca_kernel<256, 4> : (void*)aca_kernel<128, 2>;
-  if (smem > 48 * 1024)
-    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (int e = set_smem(fn, smem)) return e;
   cudaError_t e = cooperative ? cudaLaunchCooperativeKernel(fn, grid, block, args, smem, s)
                               : cudaLaunchKernel(fn, grid, block, args, smem, s);
+  if (e != cudaSuccess) cudaGetLastError();
   return e == cudaSuccess ? 0 : (int)e;
 }
 
 int aca_max_coresident(int nt, int kcap_max, int* per_sm) {
-  size_t smem = aca_smem(nt, kcap_max);
+  const size_t smem = aca_smem_bytes(nt, kcap_max);
   void* fn = nt == 256 ? (void*)aca_kernel<256, 4> : (void*)aca_kernel<128, 2>;
-  if (smem > 48 * 1024)
-    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  *per_sm = 0;
+  if (int e = set_smem(fn, smem)) return e;
   int nb = 0;
   cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, nt, smem);
+  if (e != cudaSuccess) cudaGetLastError();
   *per_sm = nb;
   return e == cudaSuccess ? 0 : (int)e;
 }

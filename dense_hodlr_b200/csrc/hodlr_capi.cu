@@ -35,6 +35,8 @@
 
 int aca_launch(const AcaLaunch& L, int nt, int kcap_max, bool cooperative, cudaStream_t s);
 int aca_max_coresident(int nt, int kcap_max, int* per_sm);
+bool aca_dots_global(int nt, int kcap_max);
+size_t aca_smem_bytes(int nt, int kcap_max);
 
 namespace {
 
@@ -191,6 +193,8 @@ struct hodlr_handle_s {
   DevPool pool;
   int* d_cta = nullptr;  // CTA -> block table of uneven ACA groups
   int cta_cap = 0;
+  double* dotg = nullptr;  // ACA dot partials in global memory (large ranks)
+  int64_t dotg_cap = 0;
   // rank predictor (rank_mlp.cu): FP32 parameter blob on the device, the
   // length scale its features use, and the last predictions (block order)
   float* d_model = nullptr;
@@ -554,12 +558,24 @@ int run_aca(hodlr_t h, std::vector<AcaBlock>& blocks, int G, int nt, int kcap_ma
   L.src = make_src(h);
   L.cta_block = groups ? h->d_cta : nullptr;
   L.ncta = ncta;
+  L.dotg = nullptr;
+  L.dotg_stride = 0;
+  if (aca_smem_bytes(nt, kcap_max) > 227 * 1024)
+    return fail(h, HODLR_ERR_UNSUPPORTED, "block rank above the shared-memory limit of ACA");
+  if (aca_dots_global(nt, kcap_max)) {
+    L.dotg_stride = (int64_t)(nt / 32) * kcap_max;
+    const int64_t dneed = L.dotg_stride * ncta;
+    if (dneed > h->dotg_cap) {
+      dfree(h, h->dotg);
+      CK(dalloc(h, &h->dotg, (size_t)dneed));
+      h->dotg_cap = dneed;
+    }
+    L.dotg = h->dotg;
+  }
   bool coop = G > 1;
   if (groups)
     for (int g : *groups) coop |= g > 1;
   CK(cudaEventRecord(h->ev0, h->stream));
-  if ((size_t)(1 + nt / 32) * kcap_max * sizeof(double) > 227 * 1024)
-    return fail(h, HODLR_ERR_UNSUPPORTED, "block rank above the shared-memory limit of ACA");
   int rc = aca_launch(L, nt, kcap_max, coop, h->stream);
   if (rc) return cuda_fail(h, (cudaError_t)rc, "aca_launch");
   h->nlaunch += 1;
@@ -699,33 +715,6 @@ int predict_ranks(hodlr_t h) {
   return HODLR_OK;
 }
 
-// CTAs per block of a level launch in proportion to the predicted ACA work
-// (m + n)(k + 1)^2, at least one each, P in total.
-std::vector<int> weighted_groups(const std::vector<double>& w, int P) {
-  const int nb = (int)w.size();
-  double W = 0;
-  for (double x : w) W += x;
-  std::vector<int> g(nb, 1);
-  if (nb == 0 || P <= nb || W <= 0) return g;
-  std::vector<std::pair<double, int>> rem;
-  int used = 0;
-  for (int i = 0; i < nb; ++i) {
-    const double raw = (double)P * w[i] / W;
-    g[i] = std::max(1, (int)raw);
-    used += g[i];
-    rem.push_back({raw - (int)raw, i});
-  }
-  while (used > P) {  // take back from the largest groups
-    int j = (int)(std::max_element(g.begin(), g.end()) - g.begin());
-    if (g[j] <= 1) break;
-    --g[j];
-    --used;
-  }
-  std::sort(rem.begin(), rem.end(), [](auto& a, auto& b) { return a.first > b.first; });
-  for (size_t t = 0; used < P && t < rem.size(); ++t, ++used) ++g[rem[t].second];
-  return g;
-}
-
 int do_compress(hodlr_t h) {
   if (h->compressed) return HODLR_OK;
   free_compress(h);
@@ -733,10 +722,10 @@ int do_compress(hodlr_t h) {
   h->aca_seconds = 0;
   h->aca_bytes = 0;
   const int nlev = (int)h->lv.size();
-  // predicted ranks, when a rank model is set: level capacities, the order
-  // of the pooled blocks and the CTA groups of the few-block levels follow
-  // them; ACA's stopping test still decides every rank (a block that needs
-  // more columns pauses and resumes after its level grows)
+  // predicted ranks, when a rank model is set: level capacities and the
+  // order of the pooled blocks (largest predicted work first) follow them;
+  // ACA's stopping test still decides every rank (a block that needs more
+  // columns pauses and resumes after its level grows)
   std::vector<int> lbase(nlev + 1, 0);
   for (int l = 0; l < nlev; ++l) lbase[l + 1] = lbase[l] + h->lv[l].nblocks();
   const bool have_pred = h->d_model != nullptr;
@@ -813,29 +802,14 @@ int do_compress(hodlr_t h) {
       if (aca_max_coresident(256, L.kcap, &ps))
         return fail(h, HODLR_ERR_CUDA, "occupancy query failed");
       const int nb = L.nblocks();
-      const int P = std::max(1, ps) * h->num_sms;
-      if (have_pred && nb <= P) {  // groups sized by predicted work
-        std::vector<AcaBlock> bl;
-        std::vector<double> w;
-        for (int q = 0; q < nb; ++q) {
-          if (L.st[q].status == ACA_DONE) continue;
-          AcaBlock B;
-          fill_block(h, L, q, B);
-          const double k1 = (double)pred_or(l, q);
-          bl.push_back(B);
-          w.push_back((double)(B.m + B.n) * k1 * k1);
-        }
-        std::vector<int> groups = weighted_groups(w, P);
-        L.G = 0;
-        for (int g : groups) L.G = std::max(L.G, g);
-        rc = run_aca(h, bl, 1, 256, L.kcap, &groups);
-      } else {
-        const int G = std::max(1, P / nb);
-        L.G = G;
-        std::vector<AcaBlock> bl(nb);
-        for (int q = 0; q < nb; ++q) fill_block(h, L, q, bl[q]);
-        rc = run_aca(h, bl, G, G > 1 ? 256 : 128, L.kcap);
-      }
+      // equal groups: CTAs sized by predicted work measured 2-8% slower on
+      // 3D clouds than equal groups (per-step latency, not streamed bytes,
+      // sets a block's time)
+      const int G = std::max(1, std::max(1, ps) * h->num_sms / nb);
+      L.G = G;
+      std::vector<AcaBlock> bl(nb);
+      for (int q = 0; q < nb; ++q) fill_block(h, L, q, bl[q]);
+      rc = run_aca(h, bl, G, G > 1 ? 256 : 128, L.kcap);
       if (rc) return rc;
       bool done;
       rc = sync_level(h, L, &done);
@@ -1798,6 +1772,7 @@ void hodlr_destroy(hodlr_t h) {
   dfree(h, h->bar);
   dfree(h, h->d_blocks);
   dfree(h, h->d_cta);
+  dfree(h, h->dotg);
   dfree(h, h->d_model);
   dfree(h, h->d_err);
   if (h->ev0) cudaEventDestroy(h->ev0);

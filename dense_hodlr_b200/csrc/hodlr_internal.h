@@ -68,4 +68,6 @@ struct AcaLaunch {
   EntrySrc src;
   const int* cta_block;  // CTA -> block (groups of uneven size, AcaBlock::g0/G), or null
   int ncta;              // CTAs of the launch when cta_block is set
+  double* dotg;          // per-CTA per-warp dot partials in global memory (large ranks), or null
+  int64_t dotg_stride;   // doubles per CTA in dotg (NT/32 * kcap_max)
 };

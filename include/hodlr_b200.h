@@ -190,9 +190,9 @@ int hodlr_trim_device_memory(void);
  * Parameters are one FP32 blob of HODLR_MLP_PARAMS floats:
  * [mean(14) | inv_std(14) | W1 64x14 | b1(64) | W2 64x64 | b2(64) | W3(64) | b3],
  * row-major weights; inputs are standardised as (x - mean) * inv_std.
- * With a model set, hodlr_compress predicts every block's rank first and
- * sizes each level's W/V capacity and each block's CTA group from the
- * predictions; ACA's own stopping test still decides every rank.
+ * With a model set, hodlr_compress predicts every block's rank first, sizes
+ * each level's W/V capacity from the predictions and starts the largest
+ * predicted work first; ACA's own stopping test still decides every rank.
  * ------------------------------------------------------------------------ */
 #define HODLR_MLP_INPUTS 14
 #define HODLR_MLP_HIDDEN 64
