@@ -128,32 +128,38 @@ def test_mlp_training_fits_a_smooth_target():
 
 @pytest.mark.gpu
 def test_rank_model_gain_on_held_out_cloud():
-    """The shipped Matern-3/2 model on a cloud it was not trained on: the
-    predictions track ACA's ranks, ACA's results are unchanged (its stopping
-    test decides), and the predicted capacities remove the W/V regrowth
-    relaunches of the plain bottom-up guess."""
+    """The shipped Matern-3/2 model on a cloud it was not trained on (points
+    uniform on the sphere, N = 65536, l = 0.1, tol 1e-8).  Without it, each
+    level's W/V capacity is guessed from the level below and a level that
+    runs out is grown and its paused blocks relaunched; with it the
+    capacities come from the predicted ranks.  The gain: no relaunches for
+    regrowth (fewer ACA launches) at the same ACA time, with ACA's results
+    unchanged since its own stopping test decides every rank."""
     from dense_hodlr_b200 import HODLR_Matrix, KernelSpec, _lib, rank_model
     params = rank_model.load("matern32")
     assert params is not None, "dense_hodlr_b200/rank_mlp_matern32.npz missing"
-    pts = rank_model.cloud("mixture", 32768, 987654)
+    n = 65536
+    pts = rank_model.cloud("sphere", n, 777 + n)
     spec = KernelSpec("matern32", 0.1, 1e-2)
 
     def run(model):
-        g = HODLR_Matrix(32768, 32768, spec, pts, 64)
+        g = HODLR_Matrix(n, n, spec, pts, 64)
         g.set_LRTolerance(1e-8)
         if model is not None:
             g.set_rank_model(model, 0.1)
         g.storeLRinTree()  # warm the device pool
-        assert _lib.lib().hodlr_reset(g._h) == 0
-        g.storeLRinTree()
-        return g
+        t = []
+        for _ in range(2):
+            assert _lib.lib().hodlr_reset(g._h) == 0
+            g.storeLRinTree()
+            t.append(g.aca_stats()["seconds"])
+        return g, min(t)
 
-    g0, g1 = run(None), run(params)
-    r0, r1 = g0.ranks(), g1.ranks()
-    near = np.array([g0.margin(b)[0] < 1e-6 for b in range(g0.num_blocks())])
-    assert np.array_equal(r0[~near], r1[~near])
+    (g0, t0), (g1, t1) = run(None), run(params)
+    assert np.array_equal(g0.ranks(), g1.ranks())
+    r = g0.ranks()
     pred = g1.predicted_ranks()
-    err = np.abs(np.log1p(pred) - np.log1p(r0))
-    assert np.median(err) < 0.3, np.median(err)
-    s0, s1 = g0.aca_stats(), g1.aca_stats()
-    assert s1["launches"] <= s0["launches"], (s0, s1)
+    assert np.median(np.abs(np.log1p(pred) - np.log1p(r))) < 0.35
+    a0, a1 = g0.aca_stats()["launches"], g1.aca_stats()["launches"]
+    assert a1 < a0, (a0, a1)
+    assert t1 <= 1.05 * t0, (t0, t1)
