@@ -49,6 +49,10 @@ SIGNATURES = {
     "hodlr_get_launch_count": (_I, [_H, ctypes.POINTER(ctypes.c_longlong)]),
     "hodlr_set_capacity_hint": (_I, [_H, _PI, _I]),
     "hodlr_trim_device_memory": (_I, []),
+    "hodlr_create_forest": (_I, [ctypes.POINTER(_H), _I, _PI, _I, _PD, ctypes.POINTER(KernelDesc),
+                                 _I]),
+    "hodlr_get_num_systems": (_I, [_H, _PI]),
+    "hodlr_forest_refine_device": (_I, [_H, _I, _VP, _I, _VP, _I, _D, _I, _PI, _PD]),
     "hodlr_set_rank_model": (_I, [_H, _PF, _D]),
     "hodlr_get_predicted_ranks": (_I, [_H, _PI]),
     "hodlr_block_features": (_I, [_H, _D, _PF]),

@@ -185,7 +185,7 @@ __device__ void residual_pass(const AcaLaunch& L, const AcaBlock& B, double* P, 
                               int k, const double* __restrict__ coef, bool dots,
                               double* __restrict__ dotw, int ldd, int fixed, const double* xfix,
                               double scale, const unsigned char* chosen, double& bv, int& bi,
-                              int& cand, double& sq, bool& nonfinite) {
+                              int& cand, double& sq, bool& nonfinite, const EntrySrc& S) {
   constexpr int U = 16 / E;  // panel columns per chunk: 16 loads in flight per thread
   const int64_t ld = L.ld;
   const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
@@ -258,8 +258,8 @@ __device__ void residual_pass(const AcaLaunch& L, const AcaBlock& B, double* P, 
     for (int e = 0; e < E; ++e) {
       if (!ok[e]) continue;
       const int j = jj[e];
-      double ent = ROW ? src_entry_xi(L.src, xfix, fixed, B.c0 + j)
-                       : src_entry_xj(L.src, xfix, B.r0 + j, fixed);
+      double ent = ROW ? src_entry_xi(S, xfix, fixed, B.c0 + j)
+                       : src_entry_xj(S, xfix, B.r0 + j, fixed);
       double r = __dsub_rn(ent, s[e]);
       double stored = ROW ? r : __dmul_rn(scale, r);
       P[j + (int64_t)k * ld] = stored;
@@ -335,6 +335,7 @@ __global__ void __launch_bounds__(NT, (NT == 256 ? 2 : 4)) aca_kernel(AcaLaunch 
   const int64_t grp0 = L.cta_block ? B.g0 : (int64_t)b * G;
   AcaState* st = B.st;
   if (st->status != ACA_RUNNING && st->status != ACA_POST) return;
+  const EntrySrc S = src_for(S, B.r0);  // the kernel of this block's system
 
   const int64_t ld = L.ld;
   const int m = B.m, n = B.n, ub = min(m, n);
@@ -399,15 +400,15 @@ __global__ void __launch_bounds__(NT, (NT == 256 ? 2 : 4)) aca_kernel(AcaLaunch 
     __syncthreads();
     const int gi = B.r0 + cur;
     double xi[3] = {0.0, 0.0, 0.0};
-    if (!L.src.dense) {
+    if (!S.dense) {
 #pragma unroll
       for (int d = 0; d < 3; ++d)
-        if (d < L.src.kp.dim) xi[d] = __ldg(L.src.pts + d * L.src.ld + gi);
+        if (d < S.kp.dim) xi[d] = __ldg(S.pts + d * S.ld + gi);
     }
     double bv = -1.0, sv = 0.0;
     int bi = INT_MAX, cand = INT_MAX;
     residual_pass<NT, E, true>(L, B, B.V, j_lo, j_hi, k, row, fuse, dotw, ldd, gi, xi, 1.0, B.cC,
-                               bv, bi, cand, sv, nonfinite);
+                               bv, bi, cand, sv, nonfinite, S);
     __syncthreads();
     if (fuse)  // CTA partial dots of V, warps summed in order
       for (int l = tid; l < k - 1; l += NT) {
@@ -471,17 +472,17 @@ __global__ void __launch_bounds__(NT, (NT == 256 ? 2 : 4)) aca_kernel(AcaLaunch 
     __syncthreads();
     const int gj = B.c0 + cc;
     double xj[3] = {0.0, 0.0, 0.0};
-    if (!L.src.dense) {
+    if (!S.dense) {
 #pragma unroll
       for (int d = 0; d < 3; ++d)
-        if (d < L.src.kp.dim) xj[d] = __ldg(L.src.pts + d * L.src.ld + gj);
+        if (d < S.kp.dim) xj[d] = __ldg(S.pts + d * S.ld + gj);
     }
     bv = -1.0;
     bi = INT_MAX;
     cand = INT_MAX;
     double sw = 0.0;
     residual_pass<NT, E, false>(L, B, B.W, i_lo, i_hi, k, row, fuse, dotw, ldd, gj, xj, piv,
-                                B.cR, bv, bi, cand, sw, nonfinite);
+                                B.cR, bv, bi, cand, sw, nonfinite, S);
     __syncthreads();
     if (fuse)
       for (int l = tid; l < k - 1; l += NT) {
@@ -558,13 +559,13 @@ __global__ void __launch_bounds__(NT, (NT == 256 ? 2 : 4)) aca_kernel(AcaLaunch 
       } else if (n <= m) {  // W = block (m x n), V = I_n
         for (int l = 0; l < n; ++l) {
           double xc[3] = {0.0, 0.0, 0.0};
-          if (!L.src.dense) {
+          if (!S.dense) {
 #pragma unroll
             for (int d = 0; d < 3; ++d)
-              if (d < L.src.kp.dim) xc[d] = __ldg(L.src.pts + d * L.src.ld + B.c0 + l);
+              if (d < S.kp.dim) xc[d] = __ldg(S.pts + d * S.ld + B.c0 + l);
           }
           for (int i = i_lo + tid; i < i_hi; i += NT)
-            B.W[i + (int64_t)l * ld] = src_entry_xj(L.src, xc, B.r0 + i, B.c0 + l);
+            B.W[i + (int64_t)l * ld] = src_entry_xj(S, xc, B.r0 + i, B.c0 + l);
           for (int j = j_lo + tid; j < j_hi; j += NT)
             B.V[j + (int64_t)l * ld] = (j == l) ? 1.0 : 0.0;
         }
@@ -573,13 +574,13 @@ __global__ void __launch_bounds__(NT, (NT == 256 ? 2 : 4)) aca_kernel(AcaLaunch 
       } else {  // W = I_m, V = block^T (n x m)
         for (int l = 0; l < m; ++l) {
           double xr[3] = {0.0, 0.0, 0.0};
-          if (!L.src.dense) {
+          if (!S.dense) {
 #pragma unroll
             for (int d = 0; d < 3; ++d)
-              if (d < L.src.kp.dim) xr[d] = __ldg(L.src.pts + d * L.src.ld + B.r0 + l);
+              if (d < S.kp.dim) xr[d] = __ldg(S.pts + d * S.ld + B.r0 + l);
           }
           for (int j = j_lo + tid; j < j_hi; j += NT)
-            B.V[j + (int64_t)l * ld] = src_entry_xi(L.src, xr, B.r0 + l, B.c0 + j);
+            B.V[j + (int64_t)l * ld] = src_entry_xi(S, xr, B.r0 + l, B.c0 + j);
           for (int i = i_lo + tid; i < i_hi; i += NT)
             B.W[i + (int64_t)l * ld] = (i == l) ? 1.0 : 0.0;
         }

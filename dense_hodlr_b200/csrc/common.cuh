@@ -30,6 +30,14 @@ enum {
   DEV_ERR_SINGULAR = 4,     // an exact-zero LU pivot
 };
 
+// The entry source for blocks of the system that holds point i: in a forest
+// of independent systems each has its own kernel; otherwise s itself.
+HODLR_INLINE EntrySrc src_for(const EntrySrc& s, int i) {
+  EntrySrc t = s;
+  if (s.kps) t.kp = s.kps[__ldg(s.psys + i)];
+  return t;
+}
+
 HODLR_INLINE double src_entry(const EntrySrc& s, int i, int j) {
   if (s.dense) return __ldg(s.A + (int64_t)j * s.ld + i);
   return hx_entry(s.kp, s.pts, s.ld, i, j);

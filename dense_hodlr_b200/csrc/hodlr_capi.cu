@@ -191,6 +191,15 @@ struct DevPool {
 
 struct hodlr_handle_s {
   DevPool pool;
+  // forest of independent systems (hodlr_create_forest); nsys == 0: one system
+  int nsys = 0;
+  std::vector<int> sys_off;  // nsys + 1 point offsets
+  std::vector<hx_kparams> sys_kp;
+  hx_kparams* d_kps = nullptr;
+  int* d_psys = nullptr;
+  int4* d_fitems = nullptr;  // full-kernel product work items, by kernel family
+  int ftype_off[HX_FOREST_TYPES + 1] = {0};
+  double* d_fnorm = nullptr;  // per-system residual and right-hand-side norms
   int* d_cta = nullptr;  // CTA -> block table of uneven ACA groups
   int cta_cap = 0;
   double* dotg = nullptr;  // ACA dot partials in global memory (large ranks)
@@ -333,13 +342,12 @@ void free_compress(hodlr_t h) {
 // a child splits iff its size > leaf; a left-type child splits at
 // min + floor(s/2) - 1, a right-type child at max - floor(s/2).  Nodes of a
 // level are listed left to right (pre-order pushes), leaves in index order.
-void build_tree(hodlr_t h) {
-  h->lv.clear();
-  h->leaf_min.clear();
-  h->leaf_size.clear();
-  const int N = h->n, leaf = h->leaf;
+// The tree of one system on points [o, o + N): inner nodes appended level by
+// level (pre-order, left before right), leaves in index order.
+void build_subtree(hodlr_t h, int o, int N) {
+  const int leaf = h->leaf;
   if (N < leaf || N < 2) {
-    h->leaf_min.push_back(0);
+    h->leaf_min.push_back(o);
     h->leaf_size.push_back(N);
     return;
   }
@@ -347,7 +355,7 @@ void build_tree(hodlr_t h) {
     int level, mn, split, mx;
   };
   std::vector<Fr> stack;
-  stack.push_back({0, 0, N / 2 - 1, N - 1});
+  stack.push_back({0, o, o + N / 2 - 1, o + N - 1});
   auto push_inner = [&](const Fr& f) {
     if ((int)h->lv.size() <= f.level) h->lv.resize(f.level + 1);
     Level& L = h->lv[f.level];
@@ -371,7 +379,7 @@ void build_tree(hodlr_t h) {
   }
   // Walk the tree again to list the leaves in index order.
   std::vector<Fr> st2;
-  st2.push_back({0, 0, N / 2 - 1, N - 1});
+  st2.push_back({0, o, o + N / 2 - 1, o + N - 1});
   while (!st2.empty()) {
     Fr f = st2.back();
     st2.pop_back();
@@ -388,6 +396,20 @@ void build_tree(hodlr_t h) {
     st2.push_back(right);
     st2.push_back(left);
   }
+}
+
+// One tree, or a forest: every system's root sits at level 0, so a level's
+// blocks (and its ACA launch, its batched leaf LUs and GEMMs) span all
+// systems.
+void build_tree(hodlr_t h) {
+  h->lv.clear();
+  h->leaf_min.clear();
+  h->leaf_size.clear();
+  if (h->nsys == 0)
+    build_subtree(h, 0, h->n);
+  else
+    for (int q = 0; q < h->nsys; ++q)
+      build_subtree(h, h->sys_off[q], h->sys_off[q + 1] - h->sys_off[q]);
   for (auto& L : h->lv) {
     L.ub_max = 0;
     for (int q = 0; q < L.nblocks(); ++q) {
@@ -444,6 +466,8 @@ EntrySrc make_src(hodlr_t h) {
   s.ld = h->n;
   s.kp = h->kp;
   s.dense = h->dense ? 1 : 0;
+  s.kps = h->nsys ? h->d_kps : nullptr;
+  s.psys = h->nsys ? h->d_psys : nullptr;
   return s;
 }
 
@@ -1288,6 +1312,44 @@ __global__ void ir_residual_kernel(const double* B, double* Y, int64_t n, int nr
   }
 }
 
+// Forest refinement: per system s (one CTA) and column c, r = b - y over
+// the system's rows, out = (|r|^2, |b|^2); Y becomes r, or 0 for a system
+// already converged (its x is left as it is).
+__global__ void forest_residual_kernel(const double* B, double* Y, int64_t n, int nrhs,
+                                       const int* off, const unsigned char* done, double* out) {
+  __shared__ double red[2][8];
+  const int s = blockIdx.x;
+  const int r0 = off[s], r1 = off[s + 1];
+  for (int c = 0; c < nrhs; ++c) {
+    double rr = 0.0, bb = 0.0;
+    for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+      const double b = B[c * n + i];
+      const double r = b - Y[c * n + i];
+      Y[c * n + i] = done[s] ? 0.0 : r;
+      rr = fma(r, r, rr);
+      bb = fma(b, b, bb);
+    }
+    rr = warp_sum(rr);
+    bb = warp_sum(bb);
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+      red[0][w] = rr;
+      red[1][w] = bb;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double a = 0.0, d = 0.0;
+      for (int q = 0; q < (int)(blockDim.x >> 5); ++q) {
+        a += red[0][q];
+        d += red[1][q];
+      }
+      out[2 * ((int64_t)s * nrhs + c)] = a;
+      out[2 * ((int64_t)s * nrhs + c) + 1] = d;
+    }
+    __syncthreads();
+  }
+}
+
 __global__ void axpy_cols_kernel(double* X, const double* D, int64_t total) {
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
        e += (int64_t)gridDim.x * blockDim.x)
@@ -1295,6 +1357,21 @@ __global__ void axpy_cols_kernel(double* X, const double* D, int64_t total) {
 }
 
 int kmatvec_dev(hodlr_t h, int nrhs, const double* d_x, int ldx, double* d_y, int ldy) {
+  if (h->nsys) {  // forest: block-diagonal product
+    KmatvecLaunch L;
+    L.src = make_src(h);
+    L.X = d_x;
+    L.ldx = ldx;
+    L.Y = d_y;
+    L.ldy = ldy;
+    L.ws = nullptr;
+    L.n = h->n;
+    L.nrhs = nrhs;
+    int e = kmatvec_forest_launch(L, h->d_fitems, h->ftype_off, h->stream);
+    if (e) return cuda_fail(h, (cudaError_t)e, "forest kmatvec");
+    for (int t = 0; t < HX_FOREST_TYPES; ++t) h->nlaunch += h->ftype_off[t + 1] > h->ftype_off[t];
+    return HODLR_OK;
+  }
   const int sym = kmatvec_sym_slices(h->n, nrhs, h->dense);
   const int sp = sym ? sym : kmatvec_splits(h->n, h->num_sms);
   if (sym || sp > 1) {
@@ -1384,6 +1461,92 @@ int refine_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double* d_x, 
                        sizeof(double) * N, nrhs, cudaMemcpyDeviceToDevice, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   return check_dev_err(h, "refine");
+}
+
+// Iterative refinement of a forest with a stopping test per system:
+// x0 = M^-1 b, then x += M^-1 (b - K x) on the systems whose
+// max_c ||b_c - K x_c|| / ||b_c|| (over the system's rows) is still above
+// tol.  relres: nsys x nrhs, system-major.
+int forest_refine_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double* d_x, int ldx,
+                         double tol, int max_iter, int* iters, double* relres) {
+  const int64_t N = h->n;
+  const int S = h->nsys;
+  int rc = build_solve_plans(h, nrhs);
+  if (rc) return rc;
+  if (nrhs > h->ir_cols) {
+    dfree(h, h->ir_b);
+    dfree(h, h->ir_x);
+    dfree(h, h->ir_y);
+    dfree(h, h->ir_part);
+    CK(dalloc(h, &h->ir_b, (size_t)(N * nrhs)));
+    CK(dalloc(h, &h->ir_x, (size_t)(N * nrhs)));
+    CK(dalloc(h, &h->ir_y, (size_t)(N * nrhs)));
+    CK(dalloc(h, &h->ir_part, (size_t)(2 * nrhs * IR_BLOCKS)));
+    h->ir_cols = nrhs;
+  }
+  double* d_out = nullptr;
+  unsigned char* d_done = nullptr;
+  int* d_off = nullptr;
+  CK(dalloc(h, &d_out, (size_t)2 * S * nrhs));
+  CK(dalloc(h, &d_done, (size_t)S));
+  CK(dalloc(h, &d_off, (size_t)S + 1));
+  CK(cudaMemcpyAsync(d_off, h->sys_off.data(), sizeof(int) * (S + 1), cudaMemcpyHostToDevice,
+                     h->stream));
+  CK(cudaMemsetAsync(d_done, 0, (size_t)S, h->stream));
+  CK(cudaMemcpy2DAsync(h->ir_b, sizeof(double) * N, d_b, sizeof(double) * ldb,
+                       sizeof(double) * N, nrhs, cudaMemcpyDeviceToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->X, h->ir_b, sizeof(double) * N * nrhs, cudaMemcpyDeviceToDevice,
+                     h->stream));
+  rc = solve_in_place(h, nrhs);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(h->ir_x, h->X, sizeof(double) * N * nrhs, cudaMemcpyDeviceToDevice,
+                     h->stream));
+  std::vector<double> out((size_t)2 * S * nrhs);
+  std::vector<unsigned char> done((size_t)S, 0);
+  int it = 0;
+  for (;; ++it) {
+    for (int c0 = 0; c0 < nrhs; c0 += 16) {
+      int nc = std::min(16, nrhs - c0);
+      rc = kmatvec_dev(h, nc, h->ir_x + c0 * N, (int)N, h->ir_y + c0 * N, (int)N);
+      if (rc) return rc;
+    }
+    forest_residual_kernel<<<S, 256, 0, h->stream>>>(h->ir_b, h->ir_y, N, nrhs, d_off, d_done,
+                                                     d_out);
+    CK(cudaGetLastError());
+    h->nlaunch += 1;
+    CK(d2h(h, out.data(), d_out, sizeof(double) * out.size()));
+    bool all = true;
+    for (int q = 0; q < S; ++q) {
+      double worst = 0.0;
+      for (int c = 0; c < nrhs; ++c) {
+        const double a = out[2 * ((size_t)q * nrhs + c)], d = out[2 * ((size_t)q * nrhs + c) + 1];
+        const double r = d > 0 ? std::sqrt(a / d) : std::sqrt(a);
+        if (!done[q] && relres) relres[(size_t)q * nrhs + c] = r;
+        worst = std::max(worst, r);
+      }
+      if (!done[q] && !(worst > tol)) done[q] = 1;
+      all &= done[q] != 0;
+    }
+    if (all || it >= max_iter) break;
+    // systems that converged in this pass still take this correction (their
+    // residual rows were written); from the next pass on they are frozen
+    CK(cudaMemcpyAsync(h->X, h->ir_y, sizeof(double) * N * nrhs, cudaMemcpyDeviceToDevice,
+                       h->stream));
+    rc = solve_in_place(h, nrhs);
+    if (rc) return rc;
+    axpy_cols_kernel<<<1024, 256, 0, h->stream>>>(h->ir_x, h->X, N * nrhs);
+    CK(cudaGetLastError());
+    h->nlaunch += 1;
+    CK(cudaMemcpyAsync(d_done, done.data(), (size_t)S, cudaMemcpyHostToDevice, h->stream));
+  }
+  if (iters) *iters = it;
+  CK(cudaMemcpy2DAsync(d_x, sizeof(double) * ldx, h->ir_x, sizeof(double) * N,
+                       sizeof(double) * N, nrhs, cudaMemcpyDeviceToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  dfree(h, d_out);
+  dfree(h, d_done);
+  dfree(h, d_off);
+  return check_dev_err(h, "forest refine");
 }
 
 // ------------------------------------------------------------- GMRES
@@ -1738,6 +1901,96 @@ int hodlr_create_dense(hodlr_t* out, int n, const double* A, int lda, int leaf_s
   return HODLR_OK;
 }
 
+int hodlr_create_forest(hodlr_t* out, int nsys, const int* sizes, int dim, const double* pts,
+                        const hodlr_kernel_desc* kernels, int leaf_size) {
+  if (!out || nsys < 1 || !sizes || dim < 1 || dim > 3 || !pts || !kernels || leaf_size < 1)
+    return HODLR_ERR_ARG;
+  int64_t total = 0;
+  for (int q = 0; q < nsys; ++q) {
+    if (sizes[q] < 1) return HODLR_ERR_ARG;
+    const hodlr_kernel_desc& k = kernels[q];
+    if (k.type < 0 || k.type > 4 || !(k.length_scale > 0)) return HODLR_ERR_ARG;
+    total += sizes[q];
+  }
+  if (total > INT32_MAX / 2) return HODLR_ERR_ARG;
+  *out = nullptr;
+  hodlr_t h = new hodlr_handle_s();
+  h->n = (int)total;
+  h->dim = dim;
+  h->leaf = leaf_size;
+  h->nsys = nsys;
+  h->sys_off.assign((size_t)nsys + 1, 0);
+  for (int q = 0; q < nsys; ++q) {
+    h->sys_off[q + 1] = h->sys_off[q] + sizes[q];
+    const hodlr_kernel_desc& k = kernels[q];
+    h->sys_kp.push_back(hx_make_kparams(k.type, dim, k.length_scale, k.diag_shift,
+                                        k.diag_replace, k.diag_value));
+  }
+  h->kp = h->sys_kp[0];
+  int rc = init_common(h);
+  if (!rc) {
+    // point -> system, and the product's work items: 256-row tiles grouped by
+    // kernel family, largest systems first
+    std::vector<int> psys((size_t)total);
+    std::vector<std::vector<std::pair<int, int4>>> byt(HX_FOREST_TYPES);
+    for (int q = 0; q < nsys; ++q) {
+      const int o = h->sys_off[q], e = h->sys_off[q + 1];
+      for (int i = o; i < e; ++i) psys[(size_t)i] = q;
+      for (int r = o; r < e; r += HX_FOREST_TILE)
+        byt[kernels[q].type].push_back({e - o, make_int4(r, o, e, q)});
+    }
+    std::vector<int4> items;
+    for (int t = 0; t < HX_FOREST_TYPES; ++t) {
+      std::stable_sort(byt[t].begin(), byt[t].end(),
+                       [](const std::pair<int, int4>& a, const std::pair<int, int4>& b) {
+                         return a.first > b.first;
+                       });
+      h->ftype_off[t] = (int)items.size();
+      for (auto& pi : byt[t]) items.push_back(pi.second);
+    }
+    h->ftype_off[HX_FOREST_TYPES] = (int)items.size();
+    cudaError_t e = dalloc(h, &h->d_pts, (size_t)total * dim);
+    if (e == cudaSuccess) e = h2d(h, h->d_pts, pts, sizeof(double) * (size_t)total * dim);
+    if (e == cudaSuccess) e = dalloc(h, &h->d_kps, (size_t)nsys);
+    if (e == cudaSuccess) e = h2d(h, h->d_kps, h->sys_kp.data(), sizeof(hx_kparams) * nsys);
+    if (e == cudaSuccess) e = dalloc(h, &h->d_psys, (size_t)total);
+    if (e == cudaSuccess) e = h2d(h, h->d_psys, psys.data(), sizeof(int) * (size_t)total);
+    if (e == cudaSuccess) e = dalloc(h, &h->d_fitems, items.size());
+    if (e == cudaSuccess) e = h2d(h, h->d_fitems, items.data(), sizeof(int4) * items.size());
+    if (e != cudaSuccess) rc = cuda_fail(h, e, "forest upload");
+  }
+  if (rc) {
+    hodlr_destroy(h);
+    return rc;
+  }
+  *out = h;
+  return HODLR_OK;
+}
+
+int hodlr_get_num_systems(hodlr_t h, int* nsys) {
+  if (!h || !nsys) return HODLR_ERR_ARG;
+  *nsys = h->nsys ? h->nsys : 1;
+  return HODLR_OK;
+}
+
+int hodlr_forest_refine_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double* d_x,
+                               int ldx, double tol, int max_iter, int* iters, double* relres) {
+  if (!h || nrhs < 1 || !d_b || !d_x || ldb < h->n || ldx < h->n || !(tol >= 0) || max_iter < 0)
+    return HODLR_ERR_ARG;
+  if (!h->nsys) return fail(h, HODLR_ERR_STATE, "not a forest (hodlr_create_forest)");
+  int rc = hodlr_factorize(h);
+  if (rc) return rc;
+  CK(cudaEventRecord(h->ev0, h->stream));
+  rc = forest_refine_device(h, nrhs, d_b, ldb, d_x, ldx, tol, max_iter, iters, relres);
+  if (rc) return rc;
+  CK(cudaEventRecord(h->ev1, h->stream));
+  CK(cudaEventSynchronize(h->ev1));
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+  h->t_solve = ms * 1e-3;
+  return HODLR_OK;
+}
+
 int hodlr_create_fnptr(hodlr_t* out, int rows, int cols, double (*kernel)(int, int, void*),
                        void* data, int leaf_size) {
   (void)rows;
@@ -1773,6 +2026,10 @@ void hodlr_destroy(hodlr_t h) {
   dfree(h, h->d_blocks);
   dfree(h, h->d_cta);
   dfree(h, h->dotg);
+  dfree(h, h->d_kps);
+  dfree(h, h->d_psys);
+  dfree(h, h->d_fitems);
+  dfree(h, h->d_fnorm);
   dfree(h, h->d_model);
   dfree(h, h->d_err);
   if (h->ev0) cudaEventDestroy(h->ev0);
@@ -1878,6 +2135,7 @@ int hodlr_set_rank_model(hodlr_t h, const float* params, double length_scale) {
     return HODLR_OK;
   }
   if (h->dense) return fail(h, HODLR_ERR_UNSUPPORTED, "the rank model needs point coordinates");
+  if (h->nsys) return fail(h, HODLR_ERR_UNSUPPORTED, "the rank model takes one length scale, not a forest");
   if (!(length_scale > 0)) return HODLR_ERR_ARG;
   for (int i = 0; i < HODLR_MLP_PARAMS; ++i)
     if (!std::isfinite(params[i])) return fail(h, HODLR_ERR_ARG, "non-finite model parameter");

@@ -14,6 +14,9 @@ struct EntrySrc {
   int64_t ld;         // = n
   hx_kparams kp;
   int dense;
+  // forest of independent systems: kernel of system psys[i] (null for one system)
+  const hx_kparams* kps;
+  const int* psys;
 };
 
 // ----------------------------------------------------------------- ACA

@@ -359,6 +359,98 @@ int sym_tps(int n) {
   return nT <= 96 ? 1 : (nT + 95) / 96;
 }
 
+// ------------------------------------------------------------ forest form
+// Block-diagonal product over a forest of independent systems.  Work item
+// (x, y, z, w) = rows [x, min(x + 2*KT, z)) of system w against its columns
+// [y, z), with system w's kernel (L.src.kps[w]); one launch per kernel family
+// present, items largest system first.  Every row is owned by one CTA and
+// written once: no workspace, deterministic.
+template <int NR, int KTYPE, int DIM>
+__global__ void __launch_bounds__(KT) kmatvec_forest_kernel(KmatvecLaunch L,
+                                                            const int4* __restrict__ items) {
+  __shared__ double xs[DIM][KT];
+  __shared__ double vs[NR][KT];
+  __shared__ double tab[64];
+  const int4 it = items[blockIdx.x];
+  const hx_kparams kp = L.src.kps[it.w];
+  if (threadIdx.x < 64) tab[threadIdx.x] = c_tang[threadIdx.x];
+  int row[RPT];
+  bool live[RPT];
+  double xi[RPT][DIM];
+  double acc[RPT][NR];
+#pragma unroll
+  for (int q = 0; q < RPT; ++q) {
+    row[q] = it.x + q * KT + threadIdx.x;
+    live[q] = row[q] < it.z;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) xi[q][d] = live[q] ? L.src.pts[d * L.src.ld + row[q]] : 0.0;
+#pragma unroll
+    for (int c = 0; c < NR; ++c) acc[q][c] = 0.0;
+  }
+  for (int j0 = it.y; j0 < it.z; j0 += KT) {
+    const int jn = min(KT, it.z - j0);
+    __syncthreads();
+    if (threadIdx.x < jn) {
+      const int j = j0 + threadIdx.x;
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) xs[d][threadIdx.x] = L.src.pts[d * L.src.ld + j];
+#pragma unroll
+      for (int c = 0; c < NR; ++c)
+        vs[c][threadIdx.x] = c < L.nrhs ? L.X[(int64_t)c * L.ldx + j] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll 2
+    for (int t = 0; t < jn; ++t) {
+#pragma unroll
+      for (int q = 0; q < RPT; ++q) {
+        double r2 = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+          const double dd = xi[q][d] - xs[d][t];
+          r2 = fma(dd, dd, r2);
+        }
+        const double kij = hx_kernel_r2_fast_t<KTYPE>(kp.a, r2, tab);
+#pragma unroll
+        for (int c = 0; c < NR; ++c) acc[q][c] = fma(kij, vs[c][t], acc[q][c]);
+      }
+    }
+  }
+  const double dcorr = kp.diag_replace ? kp.diag_value - 1.0 : kp.shift;
+#pragma unroll
+  for (int q = 0; q < RPT; ++q) {
+    if (!live[q]) continue;
+#pragma unroll
+    for (int c = 0; c < NR; ++c)
+      if (c < L.nrhs)
+        L.Y[(int64_t)c * L.ldy + row[q]] =
+            fma(dcorr, L.X[(int64_t)c * L.ldx + row[q]], acc[q][c]);
+  }
+}
+
+template <int NR, int KTYPE>
+void launch_forest_dim(const KmatvecLaunch& L, const int4* items, int count, cudaStream_t s) {
+  if (L.src.kp.dim == 1)
+    kmatvec_forest_kernel<NR, KTYPE, 1><<<count, KT, 0, s>>>(L, items);
+  else if (L.src.kp.dim == 2)
+    kmatvec_forest_kernel<NR, KTYPE, 2><<<count, KT, 0, s>>>(L, items);
+  else
+    kmatvec_forest_kernel<NR, KTYPE, 3><<<count, KT, 0, s>>>(L, items);
+}
+
+template <int NR>
+void launch_forest_type(const KmatvecLaunch& L, int type, const int4* items, int count,
+                        cudaStream_t s) {
+  switch (type) {
+    case HX_KERNEL_GAUSSIAN: launch_forest_dim<NR, HX_KERNEL_GAUSSIAN>(L, items, count, s); break;
+    case HX_KERNEL_MATERN32: launch_forest_dim<NR, HX_KERNEL_MATERN32>(L, items, count, s); break;
+    case HX_KERNEL_INV_MULTIQUADRIC:
+      launch_forest_dim<NR, HX_KERNEL_INV_MULTIQUADRIC>(L, items, count, s);
+      break;
+    case HX_KERNEL_QUADRATIC: launch_forest_dim<NR, HX_KERNEL_QUADRATIC>(L, items, count, s); break;
+    default: launch_forest_dim<NR, HX_KERNEL_EXPONENTIAL>(L, items, count, s); break;
+  }
+}
+
 }  // namespace
 
 int kmatvec_splits(int n, int num_sms) {
@@ -403,5 +495,24 @@ int kmatvec_sym_launch(const KmatvecLaunch& L, int S, cudaStream_t s) {
   else
     launch_sym_type<8>(L, S, tps, s);
   kmatvec_reduce<<<1024, 256, 0, s>>>(L, S);
+  return (int)cudaGetLastError();
+}
+
+int kmatvec_forest_launch(const KmatvecLaunch& L, const int4* d_items, const int* type_off,
+                          cudaStream_t s) {
+  if (L.nrhs < 1 || L.nrhs > 16) return (int)cudaErrorInvalidValue;
+  for (int t = 0; t < HX_FOREST_TYPES; ++t) {
+    const int count = type_off[t + 1] - type_off[t];
+    if (count <= 0) continue;
+    const int4* items = d_items + type_off[t];
+    if (L.nrhs <= 1)
+      launch_forest_type<1>(L, t, items, count, s);
+    else if (L.nrhs <= 4)
+      launch_forest_type<4>(L, t, items, count, s);
+    else if (L.nrhs <= 8)
+      launch_forest_type<8>(L, t, items, count, s);
+    else
+      launch_forest_type<16>(L, t, items, count, s);
+  }
   return (int)cudaGetLastError();
 }

@@ -30,10 +30,11 @@ __global__ void __launch_bounds__(LNT) leaf_lu_kernel(LeafLULaunch L) {
   const int lda = s | 1;
   const int tid = threadIdx.x;
   int* perm = L.perm + r0;  // final row permutation, local indices
+  const EntrySrc S = src_for(L.src, r0);  // the kernel of this leaf's system
   // assemble
   for (int e = tid; e < s * s; e += LNT) {
     int i = e % s, j = e / s;
-    a[j * lda + i] = src_entry(L.src, r0 + i, r0 + j);
+    a[j * lda + i] = src_entry(S, r0 + i, r0 + j);
   }
   for (int i = tid; i < s; i += LNT) perm[i] = i;
   __syncthreads();

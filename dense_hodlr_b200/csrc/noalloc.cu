@@ -69,6 +69,8 @@ extern "C" int hodlr_kernel_matvec_noalloc(int n, int dim, const double* d_pts,
   L.src.kp = hx_make_kparams(kernel->type, dim, kernel->length_scale, kernel->diag_shift,
                              kernel->diag_replace, kernel->diag_value);
   L.src.dense = 0;
+  L.src.kps = nullptr;
+  L.src.psys = nullptr;
   L.X = d_x;
   L.ldx = ldx;
   L.Y = d_y;

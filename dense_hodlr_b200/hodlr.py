@@ -348,6 +348,54 @@ class HODLR_Matrix:
                                                         ctypes.byref(n)))
         return m.value, n.value
 
+    # forests of independent systems
+    @classmethod
+    def forest(cls, systems, leaf=64):
+        """One handle for many independent systems: `systems` is a list of
+        (points dim_q x n_q, KernelSpec).  Points of lower dimension are
+        padded with zero coordinates; rows and columns of system q are
+        [offsets[q], offsets[q+1]) of the block-diagonal matrix."""
+        lib = _L.lib()
+        dim = max(np.atleast_2d(p).shape[0] for p, _ in systems)
+        sizes = np.array([np.atleast_2d(p).shape[1] for p, _ in systems], dtype=np.int32)
+        pts = np.zeros((dim, int(sizes.sum())), dtype=np.float64)
+        o = 0
+        for p, _ in systems:
+            p = np.atleast_2d(np.asarray(p, dtype=np.float64))
+            pts[:p.shape[0], o:o + p.shape[1]] = p
+            o += p.shape[1]
+        descs = (_L.KernelDesc * len(systems))(*[k.desc() for _, k in systems])
+        h = ctypes.c_void_p()
+        rc = lib.hodlr_create_forest(ctypes.byref(h), len(systems),
+                                     sizes.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), dim,
+                                     pts.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), descs,
+                                     int(leaf))
+        _check(None, rc)
+        self = cls.__new__(cls)
+        self.printResultInfo = False
+        self._h = h
+        self.n = int(sizes.sum())
+        self.leaf = leaf
+        self.offsets = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+        return self
+
+    def num_systems(self):
+        n = ctypes.c_int()
+        _check(self._h, _L.lib().hodlr_get_num_systems(self._h, ctypes.byref(n)))
+        return n.value
+
+    def forest_refine_device(self, d_b, d_x, nrhs, tol=1e-10, max_iter=50):
+        """Direct solve + refinement to a per-system residual target on device
+        buffers (column-major n x nrhs); returns (corrections, relres nsys x nrhs)."""
+        ns = self.num_systems()
+        it = ctypes.c_int()
+        rel = np.zeros(ns * nrhs, dtype=np.float64)
+        _check(self._h, _L.lib().hodlr_forest_refine_device(
+            self._h, int(nrhs), ctypes.c_void_p(d_b), self.n, ctypes.c_void_p(d_x), self.n,
+            float(tol), int(max_iter), ctypes.byref(it),
+            rel.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return it.value, rel.reshape(ns, nrhs)
+
     # rank predictor (csrc/rank_mlp.cu)
     def set_rank_model(self, params, length_scale):
         """FP32 parameter blob of the rank MLP (None removes it) and the

@@ -181,6 +181,28 @@ int hodlr_set_capacity_hint(hodlr_t h, const int* caps, int nlevels);
 int hodlr_trim_device_memory(void);
 
 /* ------------------------------------------------------------------------
+ * Forests of independent systems.  No reference counterpart: the reference
+ * solves one HODLR_Matrix per object.  nsys systems with sizes[q] points
+ * each, concatenated in pts (dim x sum(sizes), SoA, each system's points
+ * contiguous and ordered as the caller wants its tree), kernels[q] the
+ * kernel of system q (point dimensions below `dim` are padded with zeros by
+ * the caller).  Every system gets the tree the reference would build for it
+ * alone; all systems' roots sit at level 0, so each level's ACA launch,
+ * batched leaf LUs, GEMMs and capacitance LUs span all systems, and the
+ * full-kernel product is block diagonal.  Every entry point above works on a
+ * forest (global point and row indices; the matrix is block diagonal).
+ * ------------------------------------------------------------------------ */
+int hodlr_create_forest(hodlr_t* out, int nsys, const int* sizes, int dim, const double* pts,
+                        const hodlr_kernel_desc* kernels, int leaf_size);
+int hodlr_get_num_systems(hodlr_t h, int* nsys);
+/* Factor (if needed), direct solve, then iterative refinement with the FP64
+ * residual until every system q has max_c ||b_c - K x_c|| / ||b_c|| <= tol
+ * over its own rows (or max_iter corrections).  relres: nsys x nrhs,
+ * system-major; a converged system's x is left unchanged afterwards. */
+int hodlr_forest_refine_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double* d_x,
+                               int ldx, double tol, int max_iter, int* iters, double* relres);
+
+/* ------------------------------------------------------------------------
  * Learned rank predictor.  No reference counterpart: the reference learns
  * nothing and grows W and V by doubling as ACA runs
  * (src/lowRank.cpp:151-157).  A 14-64-64-1 MLP with GELU, BF16 with FP32
