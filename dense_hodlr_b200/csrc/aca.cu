@@ -335,7 +335,7 @@ __global__ void __launch_bounds__(NT, (NT == 256 ? 2 : 4)) aca_kernel(AcaLaunch 
   const int64_t grp0 = L.cta_block ? B.g0 : (int64_t)b * G;
   AcaState* st = B.st;
   if (st->status != ACA_RUNNING && st->status != ACA_POST) return;
-  const EntrySrc S = src_for(S, B.r0);  // the kernel of this block's system
+  const EntrySrc S = src_for(L.src, B.r0);  // the kernel of this block's system
 
   const int64_t ld = L.ld;
   const int m = B.m, n = B.n, ub = min(m, n);
