@@ -548,8 +548,108 @@ def run_profile_case(case):
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
         print(json.dumps({"case": case, "ms": ms, "entries_per_s": n * n / (ms / 1e3)}))
+    elif case.startswith("batched"):
+        print(json.dumps(run_batched(case)))
     else:
         raise SystemExit(f"unknown case {case}")
+
+
+def batched_systems(nsys, seed=SEED):
+    """The uneven-systems workload: N log-uniform in [1024, 32768], 1D or 2D
+    uniform points (alternating), Gaussian or Matern-3/2 (50/50), l
+    log-uniform in [0.05, 0.5], diagonal shift log-uniform in [1e-2, 1]."""
+    from dense_hodlr_b200 import KernelSpec
+    from dense_hodlr_b200.points import uniform_1d_sorted, uniform_cube
+    rng = np.random.default_rng(seed)
+    out = []
+    for q in range(nsys):
+        n = int(np.exp(rng.uniform(np.log(1024), np.log(32768))))
+        p = uniform_1d_sorted(n, 0.0, 1.0, seed + 7 * q) if q % 2 else uniform_cube(n, 2, seed + 7 * q)
+        kind = "gaussian" if rng.random() < 0.5 else "matern32"
+        l = float(np.exp(rng.uniform(np.log(0.05), np.log(0.5))))
+        sh = float(np.exp(rng.uniform(np.log(1e-2), np.log(1.0))))
+        out.append((p, KernelSpec(kind, l, sh)))
+    return out
+
+
+def run_batched(case):
+    """Uneven batch, case 'batched[:nsys[:max_points_per_forest[:precision]]]'.
+    Systems are sorted by size and packed into forests (waves) of at most
+    max_points points, each forest one handle whose level launches span its
+    systems; per wave: compress, factor, direct solve and refinement until
+    every system's residual is <= 1e-10.  The same systems one handle each
+    (every 8th, scaled by 8) give the unbatched time."""
+    import torch
+    from dense_hodlr_b200 import HODLR_Matrix, _lib
+    parts = case.split(":")
+    nsys = int(parts[1]) if len(parts) > 1 else 512
+    cap = int(parts[2]) if len(parts) > 2 else 1_200_000
+    prec = parts[3] if len(parts) > 3 else "fp64"
+    systems = batched_systems(nsys)
+    order = sorted(range(nsys), key=lambda q: -systems[q][0].shape[1])
+    waves, cur, npts = [], [], 0
+    for q in order:
+        n = systems[q][0].shape[1]
+        if cur and npts + n > cap:
+            waves.append(cur)
+            cur, npts = [], 0
+        cur.append(q)
+        npts += n
+    if cur:
+        waves.append(cur)
+    rng = np.random.default_rng(SEED + 3)
+    total_pts = sum(p.shape[1] for p, _ in systems)
+    res = {"case": "batched", "systems": nsys, "points": int(total_pts), "waves": len(waves),
+           "max_points_per_forest": cap, "precision": prec}
+
+    def run_waves(timed):
+        worst, its, t_total = 0.0, [], 0.0
+        for w in waves:
+            F = HODLR_Matrix.forest([systems[q] for q in w], leaf=64)
+            F.set_LRTolerance(1e-8)
+            if prec != "fp64":
+                F.set_precision(prec)
+            b = torch.from_numpy(rng.standard_normal(F.n)).cuda()
+            x = torch.empty_like(b)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            F.storeLRinTree()
+            F.recLU_Compute()
+            it, rel = F.forest_refine_device(b.data_ptr(), x.data_ptr(), 1, tol=1e-10, max_iter=100)
+            torch.cuda.synchronize()
+            t_total += time.perf_counter() - t0
+            worst = max(worst, float(rel.max()))
+            its.append(it)
+            del F
+        return t_total, worst, its
+
+    run_waves(False)  # warm-up: device pool, modules
+    t, worst, its = run_waves(True)
+    res.update({"seconds": t, "systems_per_s": nsys / t, "max_rel_residual": worst,
+                "refine_corrections_per_wave": its})
+    # one handle per system, every 8th system, scaled by 8
+    t1 = 0.0
+    sample = list(range(0, nsys, 8))
+    for q in sample:
+        p, k = systems[q]
+        n = p.shape[1]
+        b = torch.from_numpy(rng.standard_normal(n)).cuda()
+        x = torch.empty_like(b)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        g = HODLR_Matrix(n, n, k, p, 64)
+        g.set_LRTolerance(1e-8)
+        if prec != "fp64":
+            g.set_precision(prec)
+        g.storeLRinTree()
+        g.recLU_Compute()
+        g.solve_refined_device(b.data_ptr(), x.data_ptr(), 1, tol=1e-10, max_iter=100)
+        torch.cuda.synchronize()
+        t1 += time.perf_counter() - t0
+        del g
+    res["one_handle_per_system_seconds"] = t1 * nsys / len(sample)
+    res["speedup_vs_one_handle_per_system"] = res["one_handle_per_system_seconds"] / t
+    return res
 
 
 def main():
