@@ -548,6 +548,20 @@ def run_profile_case(case):
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
         print(json.dumps({"case": case, "ms": ms, "entries_per_s": n * n / (ms / 1e3)}))
+    elif case == "factor-profile":
+        # the FP64-at-scale workload: one compression, then one factorization
+        # (the launches after the aca_kernel ones) and one 8-RHS direct solve
+        import torch
+        pts, b = workload_inputs()
+        g = HODLR_Matrix(N_PTS, N_PTS, KernelSpec("matern32", LSCALE, SHIFT), pts, LEAF)
+        g.set_LRTolerance(TOL)
+        g.storeLRinTree()
+        g.recLU_Compute()
+        b_d = torch.from_numpy(np.ascontiguousarray(b.T)).cuda()
+        x_d = torch.empty_like(b_d)
+        g.solve_device(b_d.data_ptr(), x_d.data_ptr(), NRHS)
+        print(json.dumps({"case": case, "factor_s": g.get_recLU_FactorizationTime(),
+                          "solve_s": g.get_recLU_SolveTime()}))
     elif case.startswith("batched"):
         print(json.dumps(run_batched(case)))
     else:

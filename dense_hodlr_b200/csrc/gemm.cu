@@ -16,12 +16,19 @@ namespace {
 constexpr int BM = 64, BN = 64, BK = 16, NT = 256;
 
 // mode: 0 store C = A^T B (or split partial), 1 C -= A B
+//
+// Thread (tx, ty) of the 16 x 16 grid owns rows tx + 16 i and columns
+// ty + 16 j of the 64 x 64 tile, so a warp reads and writes 16 consecutive
+// rows of two columns (coalesced C traffic: the update of the ancestor
+// columns is most of the bytes).  The next k tile is loaded into registers
+// while the current one is consumed (two shared-memory buffers, one barrier
+// per tile).  Each output is still one FMA chain in k order.
 template <bool TRANS_A, int MODE>
 __global__ void __launch_bounds__(NT) gemm_kernel(const GemmProblem* __restrict__ probs,
                                                   const int4* __restrict__ tiles,
                                                   double* __restrict__ ws) {
-  __shared__ double As[BK][BM + 2];
-  __shared__ double Bs[BK][BN + 2];
+  __shared__ double As[2][BK][BM + 2];
+  __shared__ double Bs[2][BK][BN + 2];
   const int4 t = tiles[blockIdx.x];
   const GemmProblem P = probs[t.x];
   const int m0 = t.y * BM, n0 = t.z * BN;
@@ -29,66 +36,90 @@ __global__ void __launch_bounds__(NT) gemm_kernel(const GemmProblem* __restrict_
   const int kchunk = P.kchunk > 0 ? P.kchunk : P.K;
   const int kb = ks * kchunk, ke = min(P.K, kb + kchunk);
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  constexpr int LA = (BK * BM) / NT, LB = (BK * BN) / NT;
   double acc[4][4];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
 
-  for (int k0 = kb; k0 < ke; k0 += BK) {
-    // A tile -> As[kk][mm]
+  double ra[LA], rb[LB];
+  auto load = [&](int k0) {
 #pragma unroll
-    for (int r = 0; r < (BK * BM) / NT; ++r) {
-      int e = threadIdx.x + r * NT;
+    for (int r = 0; r < LA; ++r) {
+      const int e = threadIdx.x + r * NT;
       int kk, mm;
-      double v = 0.0;
       if (TRANS_A) {  // A is K x M (column-major): contiguous along k
         kk = e % BK;
         mm = e / BK;
-        int gk = k0 + kk, gm = m0 + mm;
-        if (gk < ke && gm < P.M) v = __ldg(P.A + (int64_t)gm * P.lda + gk);
       } else {  // A is M x K: contiguous along m
         mm = e % BM;
         kk = e / BM;
-        int gk = k0 + kk, gm = m0 + mm;
-        if (gk < ke && gm < P.M) v = __ldg(P.A + (int64_t)gk * P.lda + gm);
       }
-      As[kk][mm] = v;
-    }
-    // B tile (K x N, column-major) -> Bs[kk][nn]
-#pragma unroll
-    for (int r = 0; r < (BK * BN) / NT; ++r) {
-      int e = threadIdx.x + r * NT;
-      int kk = e % BK, nn = e / BK;
-      int gk = k0 + kk, gn = n0 + nn;
+      const int gk = k0 + kk, gm = m0 + mm;
       double v = 0.0;
-      if (gk < ke && gn < P.N) v = __ldg(P.B + (int64_t)gn * P.ldb + gk);
-      Bs[kk][nn] = v;
+      if (gk < ke && gm < P.M)
+        v = TRANS_A ? __ldg(P.A + (int64_t)gm * P.lda + gk) : __ldg(P.A + (int64_t)gk * P.lda + gm);
+      ra[r] = v;
     }
-    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < LB; ++r) {  // B (K x N, column-major)
+      const int e = threadIdx.x + r * NT;
+      const int kk = e % BK, nn = e / BK;
+      const int gk = k0 + kk, gn = n0 + nn;
+      rb[r] = (gk < ke && gn < P.N) ? __ldg(P.B + (int64_t)gn * P.ldb + gk) : 0.0;
+    }
+  };
+  auto store = [&](int buf) {
+#pragma unroll
+    for (int r = 0; r < LA; ++r) {
+      const int e = threadIdx.x + r * NT;
+      if (TRANS_A)
+        As[buf][e % BK][e / BK] = ra[r];
+      else
+        As[buf][e / BM][e % BM] = ra[r];
+    }
+#pragma unroll
+    for (int r = 0; r < LB; ++r) {
+      const int e = threadIdx.x + r * NT;
+      Bs[buf][e % BK][e / BK] = rb[r];
+    }
+  };
+
+  int buf = 0;
+  if (kb < ke) {
+    load(kb);
+    store(0);
+  }
+  __syncthreads();
+  for (int k0 = kb; k0 < ke; k0 += BK) {
+    const bool more = k0 + BK < ke;
+    if (more) load(k0 + BK);  // in flight while this tile is consumed
 #pragma unroll
     for (int kk = 0; kk < BK; ++kk) {
       double a[4], b[4];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = As[kk][ty * 4 + i];
+      for (int i = 0; i < 4; ++i) a[i] = As[buf][kk][tx + 16 * i];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx * 4 + j];
+      for (int j = 0; j < 4; ++j) b[j] = Bs[buf][kk][ty + 16 * j];
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
     }
+    if (more) store(buf ^ 1);  // the other buffer: last read before the previous barrier
     __syncthreads();
+    buf ^= 1;
   }
   // epilogue
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    int gm = m0 + ty * 4 + i;
-    if (gm >= P.M) continue;
+  for (int j = 0; j < 4; ++j) {
+    const int gn = n0 + ty + 16 * j;
+    if (gn >= P.N) continue;
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      int gn = n0 + tx * 4 + j;
-      if (gn >= P.N) continue;
+    for (int i = 0; i < 4; ++i) {
+      const int gm = m0 + tx + 16 * i;
+      if (gm >= P.M) continue;
       if (MODE == 1) {
         double* c = P.C + (int64_t)gn * P.ldc + gm;
         *c = *c - acc[i][j];
