@@ -15,7 +15,7 @@ namespace {
 
 constexpr int BM = 64, BN = 64, BK = 16, NT = 256;
 
-// mode: 0 store C = A^T B (or split partial), 1 C -= A B
+// mode: 0 store C = A^T B (or split partial), 1 C -= A B, 2 store C = A B
 //
 // Thread (tx, ty) of the 16 x 16 grid owns rows tx + 16 i and columns
 // ty + 16 j of the 64 x 64 tile, so a warp reads and writes 16 consecutive
@@ -123,7 +123,7 @@ __global__ void __launch_bounds__(NT) gemm_kernel(const GemmProblem* __restrict_
       if (MODE == 1) {
         double* c = P.C + (int64_t)gn * P.ldc + gm;
         *c = *c - acc[i][j];
-      } else if (P.splits > 1) {
+      } else if (MODE == 0 && P.splits > 1) {
         ws[P.ws_off + ((int64_t)ks * P.N + gn) * P.M + gm] = acc[i][j];
       } else {
         P.C[(int64_t)gn * P.ldc + gm] = acc[i][j];
@@ -153,6 +153,12 @@ int gemm_tn_launch(const GemmProblem* d_probs, const int4* d_tiles, int ntiles, 
   if (ntiles == 0) return 0;
   gemm_kernel<true, 0><<<ntiles, NT, 0, s>>>(d_probs, d_tiles, d_ws);
   if (any_split) splitk_reduce_kernel<<<dim3(64, nprob), 256, 0, s>>>(d_probs, nprob, d_ws);
+  return (int)cudaGetLastError();
+}
+
+int gemm_nn_launch(const GemmProblem* d_probs, const int4* d_tiles, int ntiles, cudaStream_t s) {
+  if (ntiles == 0) return 0;
+  gemm_kernel<false, 2><<<ntiles, NT, 0, s>>>(d_probs, d_tiles, nullptr);
   return (int)cudaGetLastError();
 }
 

@@ -921,6 +921,14 @@ __global__ void y_init_kernel(double* Y, int64_t ldy, int coff, const double* W,
       Y[(int64_t)(coff + c) * ldy + r0 + i] = W[(int64_t)c * ldw + r0 + i];
 }
 
+// Identity blocks on the leaves' diagonal of an N x smax panel (zeroed):
+// X[r0 + i, i] = 1 for every leaf (r0, s), i < s.
+__global__ void leaf_identity_kernel(double* X, int64_t ldx, const int* leaf_min,
+                                     const int* leaf_size) {
+  const int r0 = leaf_min[blockIdx.x], s = leaf_size[blockIdx.x];
+  for (int i = threadIdx.x; i < s; i += blockDim.x) X[r0 + i + (int64_t)i * ldx] = 1.0;
+}
+
 int do_factorize(hodlr_t h) {
   if (h->factored) return HODLR_OK;
   int rc = do_compress(h);
@@ -986,19 +994,60 @@ int do_factorize(hodlr_t h) {
       dfree(h, d_m);
       dfree(h, d_rk);
     }
-    // leaf solves on every column: Y <- blockdiag(leaf LU)^-1 Y
+    // Y <- blockdiag(leaf)^-1 Y on every column.  Each leaf's inverse is
+    // formed once (its LU applied to identity columns, smax columns in all)
+    // and applied as a grouped GEMM, Y_new = A_leaf^-1 Y: C columns of
+    // triangular substitution per leaf become one pass of dense products.
+    const int sm = h->smax;
+    double *Xinv = nullptr, *Y2 = nullptr;
+    CK(dalloc(h, &Xinv, (size_t)(N * sm)));
+    CK(dalloc(h, &Y2, (size_t)(N * h->C)));
+    CK(cudaMemsetAsync(Xinv, 0, sizeof(double) * N * sm, h->stream));
+    leaf_identity_kernel<<<nl, 128, 0, h->stream>>>(Xinv, N, h->d_leaf_min, h->d_leaf_size);
+    CK(cudaGetLastError());
     LeafSolveLaunch S;
     S.leaf_min = h->d_leaf_min;
     S.leaf_size = h->d_leaf_size;
     S.lu_off = h->d_lu_off;
     S.lu = h->d_lu;
     S.perm = h->d_perm;
-    S.X = h->Y;
+    S.X = Xinv;
     S.ldx = N;
-    S.ncols = (int)h->C;
-    int e = leaf_solve_launch(S, nl, h->smax, h->stream);
+    S.ncols = sm;
+    int e = leaf_solve_launch(S, nl, sm, h->stream);
     if (e) return cuda_fail(h, (cudaError_t)e, "leaf_solve_launch");
-    h->nlaunch += 1;
+    std::vector<GemmProblem> probs;
+    for (int p = 0; p < nl; ++p) {
+      const int r0 = h->leaf_min[p], s = h->leaf_size[p];
+      GemmProblem g{};
+      g.A = Xinv + r0;
+      g.B = h->Y + r0;
+      g.C = Y2 + r0;
+      g.M = s;
+      g.N = (int)h->C;
+      g.K = s;
+      g.lda = (int)N;
+      g.ldb = (int)N;
+      g.ldc = (int)N;
+      probs.push_back(g);
+    }
+    std::vector<int4> tiles;
+    int64_t ws = 0;
+    gemm_plan(probs, tiles, ws, false, 0);
+    GemmProblem* d_probs = nullptr;
+    int4* d_tiles = nullptr;
+    CK(dalloc(h, &d_probs, probs.size()));
+    CK(dalloc(h, &d_tiles, tiles.size()));
+    CK(h2d(h, d_probs, probs.data(), sizeof(GemmProblem) * probs.size()));
+    CK(h2d(h, d_tiles, tiles.data(), sizeof(int4) * tiles.size()));
+    e = gemm_nn_launch(d_probs, d_tiles, (int)tiles.size(), h->stream);
+    if (e) return cuda_fail(h, (cudaError_t)e, "leaf inverse product");
+    h->nlaunch += 3;
+    dfree(h, h->Y);
+    h->Y = Y2;
+    dfree(h, Xinv);
+    dfree(h, d_probs);
+    dfree(h, d_tiles);
   }
   // levels bottom-up
   for (int l = (int)h->lv.size() - 1; l >= 0; --l) {
