@@ -159,9 +159,15 @@ void launch_type(const KmatvecLaunch& L, dim3 grid, cudaStream_t s) {
 // per group) and accumulated into the workspace.
 constexpr int ST = 256;  // tile edge (rows = columns)
 constexpr int SG = 32;   // rotation group
-constexpr int SYM_NT = 128;
-constexpr int SYM_RPT = ST / SYM_NT;
-constexpr int SYM_NW = SYM_NT / 32;
+// rows per thread: 4 for 8 right-hand sides (halves the rotation shuffles and
+// X loads per evaluated entry), else 2
+template <int NR>
+struct SymCfg {
+  static constexpr int RPT = NR == 8 ? 4 : 2;
+  static constexpr int NT = ST / RPT;
+  static constexpr int NW = NT / 32;
+  static constexpr int MINB = NR == 8 ? 4 : 3;
+};
 
 template <int NR>
 struct SymPad {  // row stride of the staged X tile: an odd number of 16-byte units
@@ -169,7 +175,9 @@ struct SymPad {  // row stride of the staged X tile: an odd number of 16-byte un
 };
 
 template <int NR, int KTYPE, int DIM>
-__global__ void __launch_bounds__(SYM_NT, 3) kmatvec_sym_kernel(KmatvecLaunch L, int S, int tps) {
+__global__ void __launch_bounds__(SymCfg<NR>::NT, SymCfg<NR>::MINB)
+    kmatvec_sym_kernel(KmatvecLaunch L, int S, int tps) {
+  constexpr int SYM_RPT = SymCfg<NR>::RPT, SYM_NT = SymCfg<NR>::NT, SYM_NW = SymCfg<NR>::NW;
   constexpr int VS = SymPad<NR>::VS;
   __shared__ double xs[DIM][ST];
   __shared__ __align__(16) double vs[ST][VS];
@@ -335,11 +343,11 @@ template <int NR, int KTYPE>
 void launch_sym_dim(const KmatvecLaunch& L, int S, int tps, cudaStream_t s) {
   const int grid = S * (S + 1) / 2;
   if (L.src.kp.dim == 1)
-    kmatvec_sym_kernel<NR, KTYPE, 1><<<grid, SYM_NT, 0, s>>>(L, S, tps);
+    kmatvec_sym_kernel<NR, KTYPE, 1><<<grid, SymCfg<NR>::NT, 0, s>>>(L, S, tps);
   else if (L.src.kp.dim == 2)
-    kmatvec_sym_kernel<NR, KTYPE, 2><<<grid, SYM_NT, 0, s>>>(L, S, tps);
+    kmatvec_sym_kernel<NR, KTYPE, 2><<<grid, SymCfg<NR>::NT, 0, s>>>(L, S, tps);
   else
-    kmatvec_sym_kernel<NR, KTYPE, 3><<<grid, SYM_NT, 0, s>>>(L, S, tps);
+    kmatvec_sym_kernel<NR, KTYPE, 3><<<grid, SymCfg<NR>::NT, 0, s>>>(L, S, tps);
 }
 
 template <int NR>
