@@ -562,10 +562,61 @@ def run_profile_case(case):
         g.solve_device(b_d.data_ptr(), x_d.data_ptr(), NRHS)
         print(json.dumps({"case": case, "factor_s": g.get_recLU_FactorizationTime(),
                           "solve_s": g.get_recLU_SolveTime()}))
+    elif case.startswith("c3"):
+        print(json.dumps(run_c3(case)))
     elif case.startswith("batched"):
         print(json.dumps(run_batched(case)))
     else:
         raise SystemExit(f"unknown case {case}")
+
+
+def run_c3(case):
+    """The mixed-precision configuration at a reduced size, case 'c3[:N]'
+    (default N = 131072; its 2^20 size needs O(N K^2) = terabytes of ACA panel
+    traffic at the top level): N points uniform in [0,1]^3, k-d ordered,
+    Gaussian exp(-r^2/0.3^2) + 0.1 on the diagonal, leaf 128, ACA tol 1e-8,
+    16 right-hand sides, GMRES on the FP64 residual to 1e-10, with the
+    Woodbury products in FP64, TF32, BF16 and 3xTF32."""
+    import torch
+    from dense_hodlr_b200 import HODLR_Matrix, KernelSpec, _lib
+    from dense_hodlr_b200.points import uniform_cube
+    parts = case.split(":")
+    n = int(parts[1]) if len(parts) > 1 else 131072
+    nrhs = 16
+    pts = uniform_cube(n, 3, SEED)
+    b = np.random.default_rng(SEED + 1).standard_normal((n, nrhs))
+    b_d = torch.from_numpy(np.ascontiguousarray(b.T)).cuda()
+    x_d = torch.empty_like(b_d)
+    g = HODLR_Matrix(n, n, KernelSpec("gaussian", 0.3, 0.1), pts, 128)
+    g.set_LRTolerance(1e-8)
+    lib = _lib.lib()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    g.storeLRinTree()
+    out = {"case": "c3", "n": n, "nrhs": nrhs, "lr_s": g.get_LR_ComputationTime(),
+           "max_rank": int(g.ranks().max()), "runs": {}}
+    x64 = None
+    for prec in ("fp64", "tf32", "bf16", "tf32x3", "fp64"):
+        g.set_precision(prec)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        g.recLU_Compute()
+        tf = g.get_recLU_FactorizationTime()
+        g.solve_device(b_d.data_ptr(), x_d.data_ptr(), nrhs)
+        xd = x_d.cpu().numpy().T.copy()
+        it, rel = g.iterative_solve_device(b_d.data_ptr(), x_d.data_ptr(), nrhs, tol=1e-10,
+                                           max_iter=60, restart=32)
+        torch.cuda.synchronize()
+        total = time.perf_counter() - t0
+        if prec == "fp64" and x64 is None:
+            x64 = xd
+        out["runs"][prec] = {"factor_s": tf, "gmres_s": g.get_recLU_SolveTime(),
+                             "factor_solve_s": total, "gmres_iterations": int(it),
+                             "rel_residual": float(rel.max()),
+                             "direct_solve_rel_diff_vs_fp64": float(
+                                 np.linalg.norm(xd - x64) / np.linalg.norm(x64))}
+        print(json.dumps({prec: out["runs"][prec]}), flush=True)
+    return out
 
 
 def batched_systems(nsys, seed=SEED):

@@ -999,9 +999,10 @@ int do_factorize(hodlr_t h) {
     // and applied as a grouped GEMM, Y_new = A_leaf^-1 Y: C columns of
     // triangular substitution per leaf become one pass of dense products.
     const int sm = h->smax;
+    const int CH = (int)std::min<int64_t>(h->C, 512);  // Y columns per product pass
     double *Xinv = nullptr, *Y2 = nullptr;
     CK(dalloc(h, &Xinv, (size_t)(N * sm)));
-    CK(dalloc(h, &Y2, (size_t)(N * h->C)));
+    CK(dalloc(h, &Y2, (size_t)(N * CH)));
     CK(cudaMemsetAsync(Xinv, 0, sizeof(double) * N * sm, h->stream));
     leaf_identity_kernel<<<nl, 128, 0, h->stream>>>(Xinv, N, h->d_leaf_min, h->d_leaf_size);
     CK(cudaGetLastError());
@@ -1016,35 +1017,41 @@ int do_factorize(hodlr_t h) {
     S.ncols = sm;
     int e = leaf_solve_launch(S, nl, sm, h->stream);
     if (e) return cuda_fail(h, (cudaError_t)e, "leaf_solve_launch");
-    std::vector<GemmProblem> probs;
-    for (int p = 0; p < nl; ++p) {
-      const int r0 = h->leaf_min[p], s = h->leaf_size[p];
-      GemmProblem g{};
-      g.A = Xinv + r0;
-      g.B = h->Y + r0;
-      g.C = Y2 + r0;
-      g.M = s;
-      g.N = (int)h->C;
-      g.K = s;
-      g.lda = (int)N;
-      g.ldb = (int)N;
-      g.ldc = (int)N;
-      probs.push_back(g);
-    }
-    std::vector<int4> tiles;
-    int64_t ws = 0;
-    gemm_plan(probs, tiles, ws, false, 0);
+    // in passes of CH columns through an N x CH buffer (memory: N * CH, not N * C)
     GemmProblem* d_probs = nullptr;
     int4* d_tiles = nullptr;
-    CK(dalloc(h, &d_probs, probs.size()));
-    CK(dalloc(h, &d_tiles, tiles.size()));
-    CK(h2d(h, d_probs, probs.data(), sizeof(GemmProblem) * probs.size()));
-    CK(h2d(h, d_tiles, tiles.data(), sizeof(int4) * tiles.size()));
-    e = gemm_nn_launch(d_probs, d_tiles, (int)tiles.size(), h->stream);
-    if (e) return cuda_fail(h, (cudaError_t)e, "leaf inverse product");
-    h->nlaunch += 3;
-    dfree(h, h->Y);
-    h->Y = Y2;
+    CK(dalloc(h, &d_probs, (size_t)nl));
+    for (int64_t c0 = 0; c0 < h->C; c0 += CH) {
+      const int nc = (int)std::min<int64_t>(CH, h->C - c0);
+      std::vector<GemmProblem> probs;
+      for (int p = 0; p < nl; ++p) {
+        const int r0 = h->leaf_min[p], s = h->leaf_size[p];
+        GemmProblem g{};
+        g.A = Xinv + r0;
+        g.B = h->Y + r0 + c0 * N;
+        g.C = Y2 + r0;
+        g.M = s;
+        g.N = nc;
+        g.K = s;
+        g.lda = (int)N;
+        g.ldb = (int)N;
+        g.ldc = (int)N;
+        probs.push_back(g);
+      }
+      std::vector<int4> tiles;
+      int64_t ws = 0;
+      gemm_plan(probs, tiles, ws, false, 0);
+      if (c0 == 0) CK(dalloc(h, &d_tiles, tiles.size()));  // the same count every full pass
+      CK(h2d(h, d_probs, probs.data(), sizeof(GemmProblem) * probs.size()));
+      CK(h2d(h, d_tiles, tiles.data(), sizeof(int4) * tiles.size()));
+      e = gemm_nn_launch(d_probs, d_tiles, (int)tiles.size(), h->stream);
+      if (e) return cuda_fail(h, (cudaError_t)e, "leaf inverse product");
+      CK(cudaMemcpyAsync(h->Y + c0 * N, Y2, sizeof(double) * N * nc, cudaMemcpyDeviceToDevice,
+                         h->stream));
+      h->nlaunch += 1;
+    }
+    h->nlaunch += 2;
+    dfree(h, Y2);
     dfree(h, Xinv);
     dfree(h, d_probs);
     dfree(h, d_tiles);
