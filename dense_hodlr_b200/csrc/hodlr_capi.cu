@@ -191,6 +191,15 @@ struct DevPool {
 
 struct hodlr_handle_s {
   DevPool pool;
+  // the direct solve as a CUDA graph, replayed while its key is unchanged
+  cudaGraphExec_t sg_exec = nullptr;
+  int sg_nrhs = -1;
+  cudaStream_t sg_stream = nullptr;
+  const void* sg_key[4] = {nullptr, nullptr, nullptr, nullptr};
+  long sg_gen = -1;
+  long long sg_launches = 0;
+  bool sg_off = false;  // capture refused once: direct launches from then on
+  long factor_gen = 0;
   // forest of independent systems (hodlr_create_forest); nsys == 0: one system
   int nsys = 0;
   std::vector<int> sys_off;  // nsys + 1 point offsets
@@ -302,7 +311,15 @@ void free_plan(hodlr_t h, DevPlan& p) {
   p = DevPlan();
 }
 
+void drop_solve_graph(hodlr_t h) {
+  if (h->sg_exec) cudaGraphExecDestroy(h->sg_exec);
+  h->sg_exec = nullptr;
+  h->sg_nrhs = -1;
+}
+
 void free_factor(hodlr_t h) {
+  drop_solve_graph(h);
+  ++h->factor_gen;
   for (auto& L : h->lv) {
     dfree(h, L.S);
     dfree(h, L.piv);
@@ -1306,6 +1323,49 @@ int solve_in_place(hodlr_t h, int nrhs) {
   return HODLR_OK;
 }
 
+// solve_in_place through a CUDA graph: captured on first use, replayed while
+// the right-hand-side count, stream, buffers, precision and factorization
+// are the same (one launch instead of ~4 per level).
+int solve_fast(hodlr_t h, int nrhs) {
+  if (h->sg_off) return solve_in_place(h, nrhs);
+  const void* key[4] = {h->X, h->zs, h->ws, (const void*)(intptr_t)(h->gemm_prec + 1)};
+  bool same = h->sg_exec && h->sg_nrhs == nrhs && h->sg_stream == h->stream &&
+              h->sg_gen == h->factor_gen;
+  for (int i = 0; i < 4 && same; ++i) same = key[i] == h->sg_key[i];
+  if (!same) {
+    drop_solve_graph(h);
+    const long long before = h->nlaunch;
+    if (cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+      cudaGetLastError();
+      h->sg_off = true;
+      return solve_in_place(h, nrhs);
+    }
+    int rc = solve_in_place(h, nrhs);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+    cudaGraphExec_t ex = nullptr;
+    if (!rc && e == cudaSuccess && g) e = cudaGraphInstantiate(&ex, g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (rc || e != cudaSuccess || !ex) {  // not capturable here: launch directly
+      cudaGetLastError();
+      h->sg_off = true;
+      h->nlaunch = before;
+      h->err.clear();
+      return solve_in_place(h, nrhs);
+    }
+    h->sg_exec = ex;
+    h->sg_nrhs = nrhs;
+    h->sg_stream = h->stream;
+    h->sg_gen = h->factor_gen;
+    for (int i = 0; i < 4; ++i) h->sg_key[i] = key[i];
+    h->sg_launches = h->nlaunch - before;
+    h->nlaunch = before;
+  }
+  CK(cudaGraphLaunch(h->sg_exec, h->stream));
+  h->nlaunch += h->sg_launches;
+  return HODLR_OK;
+}
+
 int do_solve_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double* d_x, int ldx,
                     bool host_io) {
   int rc = do_factorize(h);
@@ -1318,7 +1378,7 @@ int do_solve_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double* d_x
   CK(cudaEventRecord(h->ev0, h->stream));
   CK(cudaMemcpy2DAsync(h->X, sizeof(double) * N, d_b, sizeof(double) * ldb, sizeof(double) * N,
                        nrhs, kin, h->stream));
-  rc = solve_in_place(h, nrhs);
+  rc = solve_fast(h, nrhs);
   if (rc) return rc;
   CK(cudaMemcpy2DAsync(d_x, sizeof(double) * ldx, h->X, sizeof(double) * N, sizeof(double) * N,
                        nrhs, kout, h->stream));
@@ -1473,7 +1533,7 @@ int refine_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double* d_x, 
                        sizeof(double) * N, nrhs, cudaMemcpyDeviceToDevice, h->stream));
   CK(cudaMemcpyAsync(h->X, h->ir_b, sizeof(double) * N * nrhs, cudaMemcpyDeviceToDevice,
                      h->stream));
-  rc = solve_in_place(h, nrhs);
+  rc = solve_fast(h, nrhs);
   if (rc) return rc;
   CK(cudaMemcpyAsync(h->ir_x, h->X, sizeof(double) * N * nrhs, cudaMemcpyDeviceToDevice,
                      h->stream));
@@ -1506,7 +1566,7 @@ int refine_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double* d_x, 
     if (worst <= tol || it >= max_iter) break;
     CK(cudaMemcpyAsync(h->X, h->ir_y, sizeof(double) * N * nrhs, cudaMemcpyDeviceToDevice,
                        h->stream));
-    rc = solve_in_place(h, nrhs);
+    rc = solve_fast(h, nrhs);
     if (rc) return rc;
     axpy_cols_kernel<<<1024, 256, 0, h->stream>>>(h->ir_x, h->X, N * nrhs);
     CK(cudaGetLastError());
@@ -1553,7 +1613,7 @@ int forest_refine_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double
                        sizeof(double) * N, nrhs, cudaMemcpyDeviceToDevice, h->stream));
   CK(cudaMemcpyAsync(h->X, h->ir_b, sizeof(double) * N * nrhs, cudaMemcpyDeviceToDevice,
                      h->stream));
-  rc = solve_in_place(h, nrhs);
+  rc = solve_fast(h, nrhs);
   if (rc) return rc;
   CK(cudaMemcpyAsync(h->ir_x, h->X, sizeof(double) * N * nrhs, cudaMemcpyDeviceToDevice,
                      h->stream));
@@ -1588,7 +1648,7 @@ int forest_refine_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double
     // residual rows were written); from the next pass on they are frozen
     CK(cudaMemcpyAsync(h->X, h->ir_y, sizeof(double) * N * nrhs, cudaMemcpyDeviceToDevice,
                        h->stream));
-    rc = solve_in_place(h, nrhs);
+    rc = solve_fast(h, nrhs);
     if (rc) return rc;
     axpy_cols_kernel<<<1024, 256, 0, h->stream>>>(h->ir_x, h->X, N * nrhs);
     CK(cudaGetLastError());
@@ -1740,7 +1800,7 @@ int gmres_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double* d_x, i
                        sizeof(double) * N, nrhs, cudaMemcpyDeviceToDevice, h->stream));
   // x0 = M^-1 b
   CK(cudaMemcpyAsync(h->X, h->ir_b, sizeof(double) * P, cudaMemcpyDeviceToDevice, h->stream));
-  rc = solve_in_place(h, nrhs);
+  rc = solve_fast(h, nrhs);
   if (rc) return rc;
   CK(cudaMemcpyAsync(h->ir_x, h->X, sizeof(double) * P, cudaMemcpyDeviceToDevice, h->stream));
   std::vector<double> bnorm, tmp, hcol, coef;
@@ -1787,7 +1847,7 @@ int gmres_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double* d_x, i
       double* Zj = h->gm_Z + (int64_t)j * P;
       // Z_j = M^-1 V_j ; W = K Z_j
       CK(cudaMemcpyAsync(h->X, Vj, sizeof(double) * P, cudaMemcpyDeviceToDevice, h->stream));
-      rc = solve_in_place(h, nrhs);
+      rc = solve_fast(h, nrhs);
       if (rc) return rc;
       CK(cudaMemcpyAsync(Zj, h->X, sizeof(double) * P, cudaMemcpyDeviceToDevice, h->stream));
       for (int c0 = 0; c0 < nrhs; c0 += 16) {
@@ -2106,6 +2166,7 @@ int hodlr_reset(hodlr_t h) {
 int hodlr_set_stream(hodlr_t h, void* stream) {
   if (!h) return HODLR_ERR_ARG;
   CK(cudaStreamSynchronize(h->stream));
+  drop_solve_graph(h);
   h->stream = stream ? (cudaStream_t)stream : h->own_stream;
   return HODLR_OK;
 }

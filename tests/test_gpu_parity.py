@@ -266,3 +266,28 @@ def test_cpp_facade_drop_in(tmp_path):
     out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=600)
     print(out.stdout)
     assert out.returncode == 0, out.stdout + out.stderr
+
+
+def test_solve_graph_replay_is_bit_identical():
+    """The direct solve is captured as a CUDA graph on first use and replayed
+    afterwards: replays give the same bits as the first (captured) run and as
+    a fresh handle's solve."""
+    import torch
+    pts = uniform_cube(20000, 2, 21)
+    spec = KernelSpec("matern32", 0.2, 1e-2)
+    g = HODLR_Matrix(20000, 20000, spec, pts, 128)
+    g.set_LRTolerance(1e-8)
+    rng = np.random.default_rng(4)
+    b1, b2 = (torch.from_numpy(rng.standard_normal((3, 20000))).cuda() for _ in range(2))
+    x = [torch.empty_like(b1) for _ in range(3)]
+    g.solve_device(b1.data_ptr(), x[0].data_ptr(), 3)   # captured
+    g.solve_device(b2.data_ptr(), x[1].data_ptr(), 3)   # replayed
+    g.solve_device(b1.data_ptr(), x[2].data_ptr(), 3)   # replayed
+    torch.cuda.synchronize()
+    assert torch.equal(x[0], x[2])
+    f = HODLR_Matrix(20000, 20000, spec, pts, 128)
+    f.set_LRTolerance(1e-8)
+    y = torch.empty_like(b2)
+    f.solve_device(b2.data_ptr(), y.data_ptr(), 3)
+    torch.cuda.synchronize()
+    assert torch.equal(x[1], y)
