@@ -107,29 +107,61 @@ HX_HD double hx_exp_tang_neg(double x, const double* tab) {
 #endif
 }
 
-#if defined(__CUDA_ARCH__)
+#if defined(__CUDACC__)
 // Square roots by Newton's method from the hardware reciprocal-square-root
 // approximation (rsqrt.approx.ftz.f64, relative error below 2^-20 on this
 // GPU).  One Newton step y <- y + y (1 - x y^2) / 2 on 1/sqrt(x) squares the
-// error (~2^-40); hx_sqrt_nr then applies one Heron correction to r = x y,
-// r <- r + (y / 2)(x - r^2), which gives sqrt(x) to within an ulp, and
-// hx_rsqrt_nr a second Newton step.  x must be a positive normal number.
+// error (~2^-40), and hx_rsqrt_nr takes a second one.  x must be a positive
+// normal number.
 __device__ __forceinline__ double hx_rsqrt_seed(double x) {
   double y;
+#if defined(__CUDA_ARCH__)
   asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+#else
+  y = 1.0 / sqrt(x);
+#endif
   return y;
 }
 __device__ __forceinline__ double hx_rsqrt_step(double x, double y) {
   const double e = fma(-(x * y), y, 1.0);  // 1 - x y^2
   return fma(0.5 * y, e, y);
 }
+// sqrt(x): r0 = x y0 from the seed (relative error e ~ 2^-20), then two
+// Heron corrections r <- r + h (x - r^2) with the fixed h = y0 / 2 ~ 1/(2r):
+// each multiplies the error by about e (2^-40, then 2^-60, below rounding).
 __device__ __forceinline__ double hx_sqrt_nr(double x) {
-  const double y = hx_rsqrt_step(x, hx_rsqrt_seed(x));
-  const double r = x * y;
-  return fma(0.5 * y, fma(-r, r, x), r);
+  const double y0 = hx_rsqrt_seed(x);
+  const double h = 0.5 * y0;
+  double r = x * y0;
+  r = fma(h, fma(-r, r, x), r);
+  return fma(h, fma(-r, r, x), r);
 }
 __device__ __forceinline__ double hx_rsqrt_nr(double x) {
   return hx_rsqrt_step(x, hx_rsqrt_step(x, hx_rsqrt_seed(x)));
+}
+#endif
+
+#if defined(__CUDACC__)
+// Coordinates scaled by c = hx_point_scale<KTYPE>(a) turn the kernel into a
+// function of the scaled squared distance alone (hx_kernel_unit_t): one
+// multiply per point instead of one per entry.
+template <int KTYPE>
+__device__ __forceinline__ double hx_point_scale(double a) {
+  if (KTYPE == HX_KERNEL_GAUSSIAN) return sqrt(-a);
+  if (KTYPE == HX_KERNEL_MATERN32 || KTYPE == HX_KERNEL_EXPONENTIAL) return a;
+  return sqrt(a);  // inverse multiquadric, quadratic
+}
+template <int KTYPE>
+__device__ __forceinline__ double hx_kernel_unit_t(double r2, const double* tab) {
+  if (KTYPE == HX_KERNEL_GAUSSIAN) return hx_exp_tang_neg(-r2, tab);
+  if (KTYPE == HX_KERNEL_MATERN32) {
+    const double s = hx_sqrt_nr(fmax(r2, 1e-300));
+    const double e = hx_exp_tang_neg(-s, tab);
+    return fma(e, s, e);  // (1 + s) e^-s
+  }
+  if (KTYPE == HX_KERNEL_INV_MULTIQUADRIC) return hx_rsqrt_nr(1.0 + r2);
+  if (KTYPE == HX_KERNEL_QUADRATIC) return 1.0 + r2;
+  return hx_exp_tang_neg(-hx_sqrt_nr(fmax(r2, 1e-300)), tab);
 }
 #endif
 

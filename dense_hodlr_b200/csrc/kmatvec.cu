@@ -204,7 +204,7 @@ __global__ void __launch_bounds__(SymCfg<NR>::NT, SymCfg<NR>::MINB)
   const int jb1 = min(nT, b * tps + tps);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   if (threadIdx.x < 64) tab[threadIdx.x] = c_tang[threadIdx.x];
-  const double ak = L.src.kp.a;
+  const double cs = hx_point_scale<KTYPE>(L.src.kp.a);  // coordinates scaled once
   const int64_t slice = (int64_t)L.nrhs * n;
   double* __restrict__ wsA = L.ws + (int64_t)a * slice;  // column sums (rows of split b)
   double* __restrict__ wsB = L.ws + (int64_t)b * slice;  // row sums (rows of split a)
@@ -222,7 +222,7 @@ __global__ void __launch_bounds__(SymCfg<NR>::NT, SymCfg<NR>::MINB)
       row[q] = I * ST + q * SYM_NT + threadIdx.x;
       live[q] = row[q] < n;
 #pragma unroll
-      for (int d = 0; d < DIM; ++d) xi[q][d] = live[q] ? L.src.pts[d * L.src.ld + row[q]] : 0.0;
+      for (int d = 0; d < DIM; ++d) xi[q][d] = live[q] ? cs * L.src.pts[d * L.src.ld + row[q]] : 0.0;
 #pragma unroll
       for (int c = 0; c < NR; ++c) {
         xv[q][c] = (live[q] && c < L.nrhs) ? L.X[(int64_t)c * L.ldx + row[q]] : 0.0;
@@ -236,7 +236,7 @@ __global__ void __launch_bounds__(SymCfg<NR>::NT, SymCfg<NR>::MINB)
         const int j = J * ST + t;
         const bool ok = j < n;
 #pragma unroll
-        for (int d = 0; d < DIM; ++d) xs[d][t] = ok ? L.src.pts[d * L.src.ld + j] : 0.0;
+        for (int d = 0; d < DIM; ++d) xs[d][t] = ok ? cs * L.src.pts[d * L.src.ld + j] : 0.0;
 #pragma unroll
         for (int c = 0; c < NR; ++c)
           vs[t][c] = (ok && c < L.nrhs) ? L.X[(int64_t)c * L.ldx + j] : 0.0;
@@ -253,7 +253,7 @@ __global__ void __launch_bounds__(SymCfg<NR>::NT, SymCfg<NR>::MINB)
               const double dd = xi[q][d] - xs[d][t];
               r2 = fma(dd, dd, r2);
             }
-            const double k = hx_kernel_r2_fast_t<KTYPE>(ak, r2, tab);
+            const double k = hx_kernel_unit_t<KTYPE>(r2, tab);
 #pragma unroll
             for (int c = 0; c < NR; ++c) acc[q][c] = fma(k, vs[t][c], acc[q][c]);
           }
@@ -289,7 +289,7 @@ __global__ void __launch_bounds__(SymCfg<NR>::NT, SymCfg<NR>::MINB)
               const double dd = xi[q][d] - xj[d];
               r2 = fma(dd, dd, r2);
             }
-            const double k = hx_kernel_r2_fast_t<KTYPE>(ak, r2, tab);
+            const double k = hx_kernel_unit_t<KTYPE>(r2, tab);
 #pragma unroll
             for (int c = 0; c < NR; ++c) {
               acc[q][c] = fma(k, vj[c], acc[q][c]);
