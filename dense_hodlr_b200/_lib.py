@@ -52,6 +52,7 @@ SIGNATURES = {
     "hodlr_create_forest": (_I, [ctypes.POINTER(_H), _I, _PI, _I, _PD, ctypes.POINTER(KernelDesc),
                                  _I]),
     "hodlr_get_num_systems": (_I, [_H, _PI]),
+    "hodlr_set_index_tree": (_I, [_H, _I, _PI, _PI, _PI]),
     "hodlr_forest_refine_device": (_I, [_H, _I, _VP, _I, _VP, _I, _D, _I, _PI, _PD]),
     "hodlr_set_rank_model": (_I, [_H, _PF, _D]),
     "hodlr_get_predicted_ranks": (_I, [_H, _PI]),

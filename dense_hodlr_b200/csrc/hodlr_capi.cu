@@ -231,6 +231,9 @@ struct hodlr_handle_s {
   std::vector<int> leaf_min, leaf_size;
   int* d_leaf_min = nullptr;
   int* d_leaf_size = nullptr;
+  // user index tree (hodlr_set_index_tree): pre-order nodes, split index and
+  // child indices (-1: none)
+  std::vector<int> ut_split, ut_left, ut_right;
   int64_t* d_lu_off = nullptr;
   double* d_lu = nullptr;
   int* d_perm = nullptr;
@@ -415,6 +418,73 @@ void build_subtree(hodlr_t h, int o, int N) {
   }
 }
 
+// ---- user index trees (userTree_To_HODLRTree, src/HODLR_Tree.cpp:207-327)
+void push_inner_node(hodlr_t h, int level, int mn, int split, int mx) {
+  if ((int)h->lv.size() <= level) h->lv.resize(level + 1);
+  Level& L = h->lv[level];
+  L.nmin.push_back(mn);
+  L.nsplit.push_back(split);
+  L.nmax.push_back(mx);
+}
+
+// An inner node with a given split and the default rules below it
+// (createDefaultTree from that node): a child splits iff its size exceeds the
+// leaf size, the left-type child with floor(s/2) rows on top, the right-type
+// child with ceil(s/2).
+void grow_default(hodlr_t h, int level, int mn, int split, int mx) {
+  push_inner_node(h, level, mn, split, mx);
+  const int top = split - mn + 1, bott = mx - split;
+  if (top > h->leaf) {
+    grow_default(h, level + 1, mn, mn + top / 2 - 1, split);
+  } else {
+    h->leaf_min.push_back(mn);
+    h->leaf_size.push_back(top);
+  }
+  if (bott > h->leaf) {
+    grow_default(h, level + 1, split + 1, mx - bott / 2, mx);
+  } else {
+    h->leaf_min.push_back(split + 1);
+    h->leaf_size.push_back(bott);
+  }
+}
+
+// Node [mn, mx] of user node u: a leaf when it is no larger than the leaf size
+// and has no split; otherwise split where u says, with u's children, or, if
+// u has none, default children (the right one with floor(s/2) rows on top,
+// as the reference builds them).  Returns false for an invalid user tree.
+bool user_subtree(hodlr_t h, int level, int mn, int mx, int u, std::vector<char>& seen) {
+  if (u < 0 || u >= (int)h->ut_split.size() || seen[u]) return false;
+  seen[u] = 1;
+  const int size = mx - mn + 1, sp = h->ut_split[u];
+  if (size <= h->leaf && sp == -1) {
+    h->leaf_min.push_back(mn);
+    h->leaf_size.push_back(size);
+    return true;
+  }
+  if (sp < mn || sp >= mx) return false;
+  push_inner_node(h, level, mn, sp, mx);
+  const int l = h->ut_left[u], r = h->ut_right[u];
+  if (l < 0 && r < 0) {
+    const int ls = sp - mn + 1, rs = mx - sp;
+    if (ls > h->leaf) {
+      grow_default(h, level + 1, mn, mn + ls / 2 - 1, sp);
+    } else {
+      h->leaf_min.push_back(mn);
+      h->leaf_size.push_back(ls);
+    }
+    if (rs > h->leaf) {
+      grow_default(h, level + 1, sp + 1, sp + rs / 2, mx);
+    } else {
+      h->leaf_min.push_back(sp + 1);
+      h->leaf_size.push_back(rs);
+    }
+    return true;
+  }
+  if (l < 0 || r < 0) return false;
+  return user_subtree(h, level + 1, mn, sp, l, seen) &&
+         user_subtree(h, level + 1, sp + 1, mx, r, seen);
+}
+
 // One tree, or a forest: every system's root sits at level 0, so a level's
 // blocks (and its ACA launch, its batched leaf LUs and GEMMs) span all
 // systems.
@@ -422,7 +492,15 @@ void build_tree(hodlr_t h) {
   h->lv.clear();
   h->leaf_min.clear();
   h->leaf_size.clear();
-  if (h->nsys == 0)
+  if (h->nsys == 0 && !h->ut_split.empty()) {
+    std::vector<char> seen(h->ut_split.size(), 0);
+    if (!user_subtree(h, 0, 0, h->n - 1, 0, seen)) {  // invalid: the caller restores
+      h->lv.clear();
+      h->leaf_min.clear();
+      h->leaf_size.clear();
+      return;
+    }
+  } else if (h->nsys == 0)
     build_subtree(h, 0, h->n);
   else
     for (int q = 0; q < h->nsys; ++q)
@@ -2081,6 +2159,36 @@ int hodlr_create_forest(hodlr_t* out, int nsys, const int* sizes, int dim, const
   }
   *out = h;
   return HODLR_OK;
+}
+
+int hodlr_set_index_tree(hodlr_t h, int nnodes, const int* split, const int* left,
+                         const int* right) {
+  if (!h || nnodes < 0 || (nnodes > 0 && (!split || !left || !right))) return HODLR_ERR_ARG;
+  if (h->nsys) return fail(h, HODLR_ERR_UNSUPPORTED, "user index trees are for one system");
+  CK(cudaStreamSynchronize(h->stream));
+  free_compress(h);
+  h->compressed = false;
+  h->ut_split.assign(split, split + nnodes);
+  h->ut_left.assign(left, left + nnodes);
+  h->ut_right.assign(right, right + nnodes);
+  build_tree(h);
+  int rc = HODLR_OK;
+  if (h->leaf_min.empty() || h->smax > 160) {
+    rc = fail(h, h->leaf_min.empty() ? HODLR_ERR_ARG : HODLR_ERR_UNSUPPORTED,
+              h->leaf_min.empty() ? "invalid user index tree" : "leaf size above 160");
+    h->ut_split.clear();
+    h->ut_left.clear();
+    h->ut_right.clear();
+    build_tree(h);  // back to the default tree
+  }
+  const int nl = (int)h->leaf_min.size();
+  dfree(h, h->d_leaf_min);
+  dfree(h, h->d_leaf_size);
+  CK(dalloc(h, &h->d_leaf_min, (size_t)nl));
+  CK(dalloc(h, &h->d_leaf_size, (size_t)nl));
+  CK(h2d(h, h->d_leaf_min, h->leaf_min.data(), 4 * nl));
+  CK(h2d(h, h->d_leaf_size, h->leaf_size.data(), 4 * nl));
+  return rc;
 }
 
 int hodlr_get_num_systems(hodlr_t h, int* nsys) {

@@ -379,6 +379,14 @@ class HODLR_Matrix:
         self.offsets = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
         return self
 
+    def set_index_tree(self, split, left, right):
+        """User index tree in pre-order (node 0 = root): split row per node (-1:
+        none), child node indices (-1: none; both -1 = default subtrees)."""
+        sp, lf, rt = (np.ascontiguousarray(a, dtype=np.int32) for a in (split, left, right))
+        pi = ctypes.POINTER(ctypes.c_int)
+        _check(self._h, _L.lib().hodlr_set_index_tree(self._h, len(sp), sp.ctypes.data_as(pi),
+                                                      lf.ctypes.data_as(pi), rt.ctypes.data_as(pi)))
+
     def num_systems(self):
         n = ctypes.c_int()
         _check(self._h, _L.lib().hodlr_get_num_systems(self._h, ctypes.byref(n)))

@@ -195,6 +195,20 @@ int hodlr_trim_device_memory(void);
 int hodlr_create_forest(hodlr_t* out, int nsys, const int* sizes, int dim, const double* pts,
                         const hodlr_kernel_desc* kernels, int leaf_size);
 int hodlr_get_num_systems(hodlr_t h, int* nsys);
+
+/* User index tree, replacing the constructors that take a user_IndexTree
+ * (include/HODLR_Matrix.hpp:85,184; built by userTree_To_HODLRTree,
+ * src/HODLR_Tree.cpp:207-327).  Nodes in pre-order, node 0 the root covering
+ * all rows: split[i] is the last row of node i's top half (-1: none; a node
+ * no larger than the leaf size with no split is a leaf), left[i] and
+ * right[i] its child nodes (both -1: default subtrees below, the right one
+ * with floor(s/2) rows on top as in the reference).  The per-node rank bounds
+ * and low-rank method of user_IndexTree::node are not taken: partial-pivot
+ * ACA with the handle's tolerance on every block.  Discards any compression;
+ * one-system handles only.  Invalid trees return HODLR_ERR_ARG and leave the
+ * default tree. */
+int hodlr_set_index_tree(hodlr_t h, int nnodes, const int* split, const int* left,
+                         const int* right);
 /* Factor (if needed), direct solve, then iterative refinement with the FP64
  * residual until every system q has max_c ||b_c - K x_c|| / ||b_c|| <= tol
  * over its own rows (or max_iter corrections).  relres: nsys x nrhs,

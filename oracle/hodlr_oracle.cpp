@@ -166,6 +166,13 @@ struct Oracle {
 // createDefaultTree (src/HODLR_Tree.cpp:33-132): the root is a leaf iff
 // N < leaf; a child splits iff its size > leaf; a left-type child splits at
 // min + floor(s/2) - 1, a right-type child at max - floor(s/2).
+void finish_tree(Oracle& o, const std::vector<std::vector<int>>& levelVec,
+                 const std::vector<int>& leafOrder);
+
+// Children of inner node `id` by the default rules, recursively (pre-order,
+// left before right): the createDefaultTree recursion below a node.
+void default_children(Oracle& o, int id, std::vector<std::vector<int>>& lv, std::vector<int>& lo);
+
 void build_tree(Oracle& o) {
   o.nodes.clear();
   std::vector<std::vector<int>> levelVec;
@@ -238,6 +245,118 @@ void build_tree(Oracle& o) {
     }
   };
   if (!root.leaf) R::go(o, 0, levelVec, leafOrder);
+  finish_tree(o, levelVec, leafOrder);
+}
+
+void default_children(Oracle& o, int id, std::vector<std::vector<int>>& lv, std::vector<int>& lo) {
+  // the same recursion as build_tree's, started from an existing inner node
+  Node nd = o.nodes[id];
+  int topSize = nd.split - nd.min + 1;
+  int bottSize = nd.max - nd.split;
+  if (nd.level > o.numLevels - 1) o.numLevels = nd.level + 1;
+  Node L, Rt;
+  L.min = nd.min;
+  L.max = nd.min + topSize - 1;
+  L.level = nd.level + 1;
+  L.leaf = !(topSize > o.leaf);
+  L.split = L.leaf ? -1 : nd.min + topSize / 2 - 1;
+  int lid = (int)o.nodes.size();
+  o.nodes.push_back(L);
+  o.nodes[id].left = lid;
+  if (!L.leaf) {
+    if ((int)lv.size() <= L.level) lv.resize(L.level + 1);
+    lv[L.level].push_back(lid);
+    default_children(o, lid, lv, lo);
+  } else {
+    lo.push_back(lid);
+    if (L.level > o.numLevels - 1) o.numLevels = L.level + 1;
+  }
+  Rt.min = nd.min + topSize;
+  Rt.max = nd.max;
+  Rt.level = nd.level + 1;
+  Rt.leaf = !(bottSize > o.leaf);
+  Rt.split = Rt.leaf ? -1 : nd.max - bottSize / 2;
+  int rid = (int)o.nodes.size();
+  o.nodes.push_back(Rt);
+  o.nodes[id].right = rid;
+  if (!Rt.leaf) {
+    if ((int)lv.size() <= Rt.level) lv.resize(Rt.level + 1);
+    lv[Rt.level].push_back(rid);
+    default_children(o, rid, lv, lo);
+  } else {
+    lo.push_back(rid);
+    if (Rt.level > o.numLevels - 1) o.numLevels = Rt.level + 1;
+  }
+}
+
+// userTree_To_HODLRTree (src/HODLR_Tree.cpp:207-327): a node no larger than
+// the leaf size with no user split is a leaf; otherwise it splits at the user
+// split; without user children both children follow the default rules, the
+// right one split at split + floor(s/2) (src/HODLR_Tree.cpp:300-303).
+bool user_tree(Oracle& o, const int* usplit, const int* uleft, const int* uright, int nn,
+               int level, int mn, int mx, int u, std::vector<char>& seen,
+               std::vector<std::vector<int>>& lv, std::vector<int>& lo) {
+  if (u < 0 || u >= nn || seen[u]) return false;
+  seen[u] = 1;
+  if (level > o.numLevels - 1) o.numLevels = level + 1;
+  const int size = mx - mn + 1, sp = usplit[u];
+  Node nd;
+  nd.level = level;
+  nd.min = mn;
+  nd.max = mx;
+  int id = (int)o.nodes.size();
+  if (size <= o.leaf && sp == -1) {
+    nd.leaf = true;
+    nd.split = -1;
+    o.nodes.push_back(nd);
+    lo.push_back(id);
+    return true;
+  }
+  if (sp < mn || sp >= mx) return false;
+  nd.leaf = false;
+  nd.split = sp;
+  o.nodes.push_back(nd);
+  if ((int)lv.size() <= level) lv.resize(level + 1);
+  lv[level].push_back(id);
+  const int l = uleft[u], r = uright[u];
+  if (l < 0 && r < 0) {
+    const int ls = sp - mn + 1, rs = mx - sp;
+    Node L, Rt;
+    L.level = Rt.level = level + 1;
+    L.min = mn;
+    L.max = sp;
+    L.leaf = ls <= o.leaf;
+    L.split = L.leaf ? -1 : mn + ls / 2 - 1;
+    Rt.min = sp + 1;
+    Rt.max = mx;
+    Rt.leaf = rs <= o.leaf;
+    Rt.split = Rt.leaf ? -1 : sp + rs / 2;
+    if (level + 1 > o.numLevels - 1) o.numLevels = level + 2;
+    for (int side = 0; side < 2; ++side) {
+      const Node c = side == 0 ? L : Rt;
+      int cid = (int)o.nodes.size();
+      o.nodes.push_back(c);
+      if (side == 0) o.nodes[id].left = cid; else o.nodes[id].right = cid;
+      if (c.leaf) {
+        lo.push_back(cid);
+      } else {
+        if ((int)lv.size() <= c.level) lv.resize(c.level + 1);
+        lv[c.level].push_back(cid);
+        default_children(o, cid, lv, lo);
+      }
+    }
+    return true;
+  }
+  if (l < 0 || r < 0) return false;
+  o.nodes[id].left = (int)o.nodes.size();
+  if (!user_tree(o, usplit, uleft, uright, nn, level + 1, mn, sp, l, seen, lv, lo)) return false;
+  o.nodes[id].right = (int)o.nodes.size();
+  return user_tree(o, usplit, uleft, uright, nn, level + 1, sp + 1, mx, r, seen, lv, lo);
+}
+
+// Level order, positions and the off-diagonal blocks of a built tree.
+void finish_tree(Oracle& o, const std::vector<std::vector<int>>& levelVec,
+                 const std::vector<int>& leafOrder) {
   o.inner.clear();
   for (auto& lv : levelVec)
     for (int id : lv) o.inner.push_back(id);
@@ -597,6 +716,24 @@ void* orc_create_dense(int n, const double* A, int lda, int leaf) {
 }
 
 void orc_destroy(void* h) { delete (Oracle*)h; }
+
+// User index tree (nodes in pre-order, node 0 the root); 0 = ok, 1 = invalid
+// (the default tree is kept).
+int orc_set_user_tree(void* h, int nn, const int* split, const int* left, const int* right) {
+  Oracle& o = *(Oracle*)h;
+  o.nodes.clear();
+  o.numLevels = 1;
+  std::vector<std::vector<int>> lv;
+  std::vector<int> lo;
+  std::vector<char> seen((size_t)std::max(nn, 1), 0);
+  if (nn < 1 || !user_tree(o, split, left, right, nn, 0, 0, o.n - 1, 0, seen, lv, lo)) {
+    build_tree(o);
+    return 1;
+  }
+  finish_tree(o, lv, lo);
+  o.compressed = o.factored = false;
+  return 0;
+}
 
 void orc_set_lr(void* h, double tol, double minPivot) {
   Oracle* o = (Oracle*)h;

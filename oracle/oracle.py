@@ -37,6 +37,8 @@ def lib():
         L.orc_create_dense.restype = ctypes.c_void_p
         L.orc_create_dense.argtypes = [ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int]
         L.orc_destroy.argtypes = [ctypes.c_void_p]
+        L.orc_set_user_tree.argtypes = [ctypes.c_void_p, ctypes.c_int, _ip, _ip, _ip]
+        L.orc_set_user_tree.restype = ctypes.c_int
         L.orc_set_lr.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double]
         L.orc_compress.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.orc_factorize.argtypes = [ctypes.c_void_p]
@@ -103,6 +105,11 @@ class OracleHODLR:
         if getattr(self, "h", None):
             lib().orc_destroy(self.h)
             self.h = None
+
+    def set_user_tree(self, split, left, right):
+        """User index tree in pre-order; returns 0, or 1 if invalid."""
+        a = [np.ascontiguousarray(v, dtype=np.int32) for v in (split, left, right)]
+        return lib().orc_set_user_tree(self.h, len(a[0]), *[x.ctypes.data_as(_ip) for x in a])
 
     def set_lr(self, tol, min_pivot=0.0):
         lib().orc_set_lr(self.h, float(tol), float(min_pivot))
