@@ -379,6 +379,19 @@ class HODLR_Matrix:
         self.offsets = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
         return self
 
+    def logAbsDeterminant(self):
+        """log|det K| from the factorization (src/HODLR_Matrix.cpp:1666)."""
+        v, sg = ctypes.c_double(), ctypes.c_int()
+        _check(self._h, _L.lib().hodlr_logdet(self._h, ctypes.byref(v), ctypes.byref(sg)))
+        return v.value
+
+    def determinant(self):
+        """det K (with the sign of the pivoting permutations); overflows to
+        inf for large matrices -- prefer logAbsDeterminant."""
+        v, sg = ctypes.c_double(), ctypes.c_int()
+        _check(self._h, _L.lib().hodlr_logdet(self._h, ctypes.byref(v), ctypes.byref(sg)))
+        return sg.value * float(np.exp(v.value))
+
     def set_index_tree(self, split, left, right):
         """User index tree in pre-order (node 0 = root): split row per node (-1:
         none), child node indices (-1: none; both -1 = default subtrees)."""

@@ -196,6 +196,14 @@ int hodlr_create_forest(hodlr_t* out, int nsys, const int* sizes, int dim, const
                         const hodlr_kernel_desc* kernels, int leaf_size);
 int hodlr_get_num_systems(hodlr_t h, int* nsys);
 
+/* log|det K| and the sign of det K from the factorization (factors first if
+ * needed): the product of the leaf determinants and of every node's
+ * capacitance determinant.  Replaces logAbsDeterminant() / determinant()
+ * (include/HODLR_Matrix.hpp:248-249; src/HODLR_Matrix.cpp:1661-1697, which
+ * reach the same determinant through recSM_Factorize and perturbI nodes; its
+ * signed value omits the row permutations, this one does not). */
+int hodlr_logdet(hodlr_t h, double* log_abs_det, int* sign);
+
 /* User index tree, replacing the constructors that take a user_IndexTree
  * (include/HODLR_Matrix.hpp:85,184; built by userTree_To_HODLRTree,
  * src/HODLR_Tree.cpp:207-327).  Nodes in pre-order, node 0 the root covering
