@@ -385,6 +385,12 @@ class HODLR_Matrix:
         _check(self._h, _L.lib().hodlr_logdet(self._h, ctypes.byref(v), ctypes.byref(sg)))
         return v.value
 
+    def slogdet(self):
+        """(sign, log|det K|), like numpy.linalg.slogdet."""
+        v, sg = ctypes.c_double(), ctypes.c_int()
+        _check(self._h, _L.lib().hodlr_logdet(self._h, ctypes.byref(v), ctypes.byref(sg)))
+        return sg.value, v.value
+
     def determinant(self):
         """det K (with the sign of the pivoting permutations); overflows to
         inf for large matrices -- prefer logAbsDeterminant."""

@@ -306,5 +306,5 @@ def test_log_determinant_matches_dense(kind, l, shift):
     K += shift * np.eye(n)
     sgn, ld = np.linalg.slogdet(K)
     assert abs(g.logAbsDeterminant() - ld) <= 1e-9 * abs(ld)
-    d = g.determinant()
-    assert np.sign(d) == sgn
+    s2, ld2 = g.slogdet()  # determinant() itself under/overflows at this size
+    assert s2 == sgn and ld2 == g.logAbsDeterminant()
