@@ -15,6 +15,7 @@
 #ifndef HODLR_B200_HODLR_MATRIX_HPP
 #define HODLR_B200_HODLR_MATRIX_HPP
 
+#include <cmath>
 #include <cstdio>
 #include <stdexcept>
 #include <string>
@@ -72,6 +73,74 @@ inline void check(hodlr_t h, int status, const char* where) {
 
 }  // namespace hodlr_b200
 
+// user_IndexTree (reference include/user_IndexTree.hpp:7-38): a user-defined
+// splitting scheme.  splitIndex is the last row of a node's top half (-1:
+// none); children may be left NULL for default subtrees below.  The rank
+// bounds and per-node low-rank method must keep their defaults (-1, and the
+// empty string or "partialPiv_ACA"): the GPU path runs partial-pivot ACA with
+// the matrix's tolerance on every block.
+class user_IndexTree {
+ public:
+  struct node {
+    node* left = nullptr;
+    node* right = nullptr;
+    int splitIndex = -1;
+    int topOffDiag_minRank = -1;
+    int bottOffDiag_minRank = -1;
+    int topOffDiag_maxRank = -1;
+    int bottOffDiag_maxRank = -1;
+    std::string LR_Method;
+  };
+  node* rootNode = nullptr;
+
+  user_IndexTree() = default;
+  user_IndexTree(const user_IndexTree&) = delete;
+  user_IndexTree& operator=(const user_IndexTree&) = delete;
+  ~user_IndexTree() { freeTree(rootNode); }
+  void setChildren_NULL(node* parent) {
+    parent->left = nullptr;
+    parent->right = nullptr;
+  }
+  void printTree() const { printTree(rootNode, 0); }
+
+  // pre-order arrays for hodlr_set_index_tree
+  void flatten(std::vector<int>& split, std::vector<int>& left, std::vector<int>& right) const {
+    split.clear();
+    left.clear();
+    right.clear();
+    if (rootNode) add(rootNode, split, left, right);
+  }
+
+ private:
+  static int add(const node* nd, std::vector<int>& split, std::vector<int>& left,
+                 std::vector<int>& right) {
+    if (nd->topOffDiag_minRank != -1 || nd->bottOffDiag_minRank != -1 ||
+        nd->topOffDiag_maxRank != -1 || nd->bottOffDiag_maxRank != -1 ||
+        !(nd->LR_Method.empty() || nd->LR_Method == "partialPiv_ACA"))
+      throw hodlr_b200::Error(HODLR_ERR_UNSUPPORTED,
+                              "user tree rank bounds / low-rank methods are not on the GPU path");
+    const int id = (int)split.size();
+    split.push_back(nd->splitIndex);
+    left.push_back(-1);
+    right.push_back(-1);
+    if (nd->left) left[id] = add(nd->left, split, left, right);
+    if (nd->right) right[id] = add(nd->right, split, left, right);
+    return id;
+  }
+  static void freeTree(node* nd) {
+    if (!nd) return;
+    freeTree(nd->left);
+    freeTree(nd->right);
+    delete nd;
+  }
+  static void printTree(const node* nd, int depth) {
+    if (!nd) return;
+    std::printf("%*ssplit %d\n", 2 * depth, "", nd->splitIndex);
+    printTree(nd->left, depth + 1);
+    printTree(nd->right, depth + 1);
+  }
+};
+
 class HODLR_Matrix {
  public:
   bool printResultInfo = false;
@@ -118,6 +187,23 @@ class HODLR_Matrix {
                       hodlr_create_kernel(&h_, numRows, dim, pts, &kernel, inputSizeThreshold),
                       "HODLR_Matrix(kernel)");
     n_ = numRows;
+  }
+
+  // With a user_IndexTree (reference :85 dense, :184 kernel)
+  HODLR_Matrix(const hodlr_b200::Matrix& A, int inputSizeThreshold, user_IndexTree& input_IndexTree)
+      : HODLR_Matrix(A, inputSizeThreshold) {
+    set_tree(input_IndexTree);
+  }
+#ifdef HODLR_B200_HAVE_EIGEN
+  HODLR_Matrix(Eigen::MatrixXd& A, int inputSizeThreshold, user_IndexTree& input_IndexTree)
+      : HODLR_Matrix(A, inputSizeThreshold) {
+    set_tree(input_IndexTree);
+  }
+#endif
+  HODLR_Matrix(int numRows, int numCols, const hodlr_kernel_desc& kernel, const double* pts,
+               int dim, int inputSizeThreshold, user_IndexTree& input_IndexTree)
+      : HODLR_Matrix(numRows, numCols, kernel, pts, dim, inputSizeThreshold) {
+    set_tree(input_IndexTree);
   }
 
   HODLR_Matrix(const HODLR_Matrix&) = delete;
@@ -177,6 +263,20 @@ class HODLR_Matrix {
   }
 #endif
 
+  // determinant() / logAbsDeterminant()  (reference :248-249)
+  double logAbsDeterminant() {
+    double v = 0;
+    int sign = 1;
+    hodlr_b200::check(h_, hodlr_logdet(h_, &v, &sign), "logAbsDeterminant");
+    return v;
+  }
+  double determinant() {
+    double v = 0;
+    int sign = 1;
+    hodlr_b200::check(h_, hodlr_logdet(h_, &v, &sign), "determinant");
+    return sign * std::exp(v);
+  }
+
   // ------------------------------------------------------------- getters
   double get_LR_ComputationTime() const { return times()[0]; }
   double get_recLU_FactorizationTime() const { return times()[1]; }
@@ -192,6 +292,15 @@ class HODLR_Matrix {
   hodlr_t h_ = nullptr;
   int n_ = 0;
   int last_iterations_ = 0;
+
+  void set_tree(const user_IndexTree& t) {
+    std::vector<int> split, left, right;
+    t.flatten(split, left, right);
+    hodlr_b200::check(h_,
+                      hodlr_set_index_tree(h_, (int)split.size(), split.data(), left.data(),
+                                           right.data()),
+                      "user_IndexTree");
+  }
 
   void solve_raw(int rows, int nrhs, const double* b, double* x) {
     if (rows != n_) throw hodlr_b200::Error(HODLR_ERR_ARG, "right-hand side has the wrong number of rows");

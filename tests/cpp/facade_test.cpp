@@ -72,6 +72,37 @@ int main() {
     std::printf("iterative_Solve rel. error %g after %d iterations\n", e2, H.last_iterations());
     fails += !(e2 < 1e-9);
   }
+  // user_IndexTree (reference :184) and logAbsDeterminant (:249): a root split
+  // off-centre with default subtrees; the solution and the determinant agree
+  // with the default tree's
+  {
+    const int n = 3000;
+    Matrix X = Matrix::LinSpaced(n, -1, 1);
+    hodlr_kernel_desc k{HODLR_KERNEL_GAUSSIAN, 0.1, 1.0, 0, 0.0};
+    user_IndexTree t;
+    t.rootNode = new user_IndexTree::node();
+    t.rootNode->splitIndex = 999;
+    HODLR_Matrix Ku(n, n, k, X.data(), 1, 64, t);
+    HODLR_Matrix Kd(n, n, k, X.data(), 1, 64);
+    Ku.set_LRTolerance(1e-12);
+    Kd.set_LRTolerance(1e-12);
+    Matrix b(n, 1);
+    for (int i = 0; i < n; ++i) b(i, 0) = std::sin(3.0 * i);
+    double e = rel_err(Ku.recLU_Solve(b), Kd.recLU_Solve(b));
+    double du = Ku.logAbsDeterminant(), dd = Kd.logAbsDeterminant();
+    std::printf("user tree: solution diff %g, log|det| %.12g vs %.12g\n", e, du, dd);
+    fails += !(e < 1e-9) + !(std::fabs(du - dd) < 1e-8 * std::fabs(dd));
+    user_IndexTree bounded;
+    bounded.rootNode = new user_IndexTree::node();
+    bounded.rootNode->splitIndex = 999;
+    bounded.rootNode->topOffDiag_maxRank = 5;
+    try {
+      HODLR_Matrix Kb(n, n, k, X.data(), 1, 64, bounded);
+      fails += 1;
+    } catch (const hodlr_b200::Error& err) {
+      fails += (err.status() != HODLR_ERR_UNSUPPORTED);
+    }
+  }
   try {
     HODLR_Matrix bad(10, 10, [](int, int, void*) { return 0.0; }, nullptr, 30);
     fails += 1;
