@@ -199,8 +199,14 @@ void gemm_plan(std::vector<GemmProblem>& probs, std::vector<int4>& tiles, int64_
       p.ws_off = ws_elems;
       ws_elems += (int64_t)splits * p.M * p.N;
     }
+    // grouped raster: column tiles in groups of GW, row tiles outer within a
+    // group, so an A tile is reused from L2 by GW consecutive CTAs and a
+    // group's B tiles by every row tile (each tile computes the same values
+    // in any order)
+    constexpr int GW = 8;
     for (int ks = 0; ks < splits; ++ks)
-      for (int j = 0; j < tn; ++j)
-        for (int i = 0; i < tm; ++i) tiles.push_back(make_int4((int)q, i, j, ks));
+      for (int jg = 0; jg < tn; jg += GW)
+        for (int i = 0; i < tm; ++i)
+          for (int j = jg; j < std::min(tn, jg + GW); ++j) tiles.push_back(make_int4((int)q, i, j, ks));
   }
 }
