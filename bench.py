@@ -559,12 +559,16 @@ def run_profile_case(case):
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
         print(json.dumps({"case": case, "ms": ms, "entries_per_s": n * n / (ms / 1e3)}))
-    elif case == "factor-profile":
-        # the FP64-at-scale workload: one compression, then one factorization
-        # (the launches after the aca_kernel ones) and one 8-RHS direct solve
+    elif case.startswith("factor-profile"):
+        # the FP64-at-scale workload (or its first N points' cloud at a smaller
+        # N, 'factor-profile:N'): one compression, then one factorization (the
+        # launches after the aca_kernel ones) and one 8-RHS direct solve
         import torch
-        pts, b = workload_inputs()
-        g = HODLR_Matrix(N_PTS, N_PTS, KernelSpec("matern32", LSCALE, SHIFT), pts, LEAF)
+        from dense_hodlr_b200.points import uniform_cube
+        n = int(case.split(":")[1]) if ":" in case else N_PTS
+        pts = uniform_cube(n, DIM, SEED) if n != N_PTS else workload_inputs()[0]
+        b = np.random.default_rng(SEED + 1).standard_normal((n, NRHS))
+        g = HODLR_Matrix(n, n, KernelSpec("matern32", LSCALE, SHIFT), pts, LEAF)
         g.set_LRTolerance(TOL)
         g.storeLRinTree()
         g.recLU_Compute()
