@@ -86,6 +86,20 @@ __global__ void __launch_bounds__(NT) gemm_kernel(const GemmProblem* __restrict_
     }
   };
 
+  // NN-subtract: the C tile is read before the k loop (it does not change
+  // there), so its load overlaps the products instead of stalling the epilogue
+  double cold[4][4];
+  if (MODE == 1) {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int gn = n0 + ty + 16 * j;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int gm = m0 + tx + 16 * i;
+        cold[i][j] = (gn < P.N && gm < P.M) ? P.C[(int64_t)gn * P.ldc + gm] : 0.0;
+      }
+    }
+  }
   int buf = 0;
   if (kb < ke) {
     load(kb);
@@ -121,8 +135,7 @@ __global__ void __launch_bounds__(NT) gemm_kernel(const GemmProblem* __restrict_
       const int gm = m0 + tx + 16 * i;
       if (gm >= P.M) continue;
       if (MODE == 1) {
-        double* c = P.C + (int64_t)gn * P.ldc + gm;
-        *c = *c - acc[i][j];
+        P.C[(int64_t)gn * P.ldc + gm] = cold[i][j] - acc[i][j];
       } else if (MODE == 0 && P.splits > 1) {
         ws[P.ws_off + ((int64_t)ks * P.N + gn) * P.M + gm] = acc[i][j];
       } else {
