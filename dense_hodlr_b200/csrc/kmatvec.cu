@@ -247,7 +247,7 @@ __global__ void __launch_bounds__(SymCfg<NR>::NT, SymCfg<NR>::MINB)
         for (int t = 0; t < ST; ++t) {
 #pragma unroll
           for (int q = 0; q < SYM_RPT; ++q) {
-            double r2 = 0.0;
+            double r2 = HX_R2_FLOOR;
 #pragma unroll
             for (int d = 0; d < DIM; ++d) {
               const double dd = xi[q][d] - xs[d][t];
@@ -283,7 +283,7 @@ __global__ void __launch_bounds__(SymCfg<NR>::NT, SymCfg<NR>::MINB)
           }
 #pragma unroll
           for (int q = 0; q < SYM_RPT; ++q) {
-            double r2 = 0.0;
+            double r2 = HX_R2_FLOOR;
 #pragma unroll
             for (int d = 0; d < DIM; ++d) {
               const double dd = xi[q][d] - xj[d];
@@ -336,6 +336,229 @@ __global__ void __launch_bounds__(SymCfg<NR>::NT, SymCfg<NR>::MINB)
         *dst = (a == b && I != ia0) ? *dst + v : v;
       }
     }
+  }
+}
+
+// ---------------------------------------- symmetric form, 8 right-hand sides
+// The same tile-pair schedule and workspace ownership as kmatvec_sym_kernel,
+// with the per-entry products on the FP64 tensor-core instruction
+// mma.m8n8k4.f64 (D[8x8] += A[8x4] B[4x8]; lane l holds A[l/4][l%4],
+// B[l%4][l/4] and D[l/4][2(l%4) .. +1]).  Warp w of 8 owns rows
+// 32w .. 32w+31 of tile I as four 8-row chunks and walks tile J in 8-column
+// chunks.  In a chunk lane (g, t) evaluates e0 = K[g][t] and e1 = K[g][t+4]:
+//   row sums    Y_I[rows][rhs] += K[rows][cols] X_J[cols][rhs]: A = e0, e1;
+//   column sums Y_J[cols][rhs] += K^T[cols][rows] X_I[rows][rhs]: A needs
+//               K[t][g], K[t+4][g], the transpose, which goes through a
+//               per-warp shared-memory buffer (two 8-byte stores, one 16-byte
+//               load per lane).
+// Each warp's column sums of a chunk are stored per warp; after every 32
+// columns the CTA adds the eight warps' sums in warp order into the
+// workspace slice, so every (slice, row) still has one writer in a fixed
+// order.  The FP64 work per entry is the entry itself plus 16 FMAs inside
+// the MMAs, as in the FMA form, with half the instructions and a quarter of
+// the registers.
+constexpr int MMA_NT = 256;  // 8 warps
+constexpr int MMA_VSP = ST + 8;  // padded row stride of the staged X tile
+
+__device__ __forceinline__ void dmma_884(double (&d)[2], double a, double b) {
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
+
+// staged position of tile column u: chunk c = u / 8 keeps its 8 columns, and
+// columns t and t + 4 of a chunk sit side by side (one 16-byte load per lane)
+__device__ __forceinline__ int mma_pos(int u) { return (u & ~7) + 2 * (u & 3) + ((u >> 2) & 1); }
+
+// dynamic shared memory of the kernel, in doubles
+template <int DIM>
+struct MmaSmem {
+  static constexpr int XS = 0;                        // [DIM][ST] column coordinates
+  static constexpr int VS = XS + DIM * ST;            // [8][MMA_VSP] X_J by rhs
+  static constexpr int TR = VS + 8 * MMA_VSP;         // [8 warps][2][4 row chunks][64]
+  static constexpr int CW = TR + 8 * 2 * 4 * 64;      // [2][8 warps][8 rhs][34]
+  static constexpr int TAB = CW + 2 * 8 * 8 * 34;     // [64]
+  static constexpr size_t BYTES = (size_t)(TAB + 64) * sizeof(double);
+};
+
+template <int KTYPE, int DIM>
+__global__ void __launch_bounds__(MMA_NT, 2)
+    kmatvec_sym_mma_kernel(KmatvecLaunch L, int S, int tps) {
+  extern __shared__ __align__(16) double mma_smem[];
+  using M = MmaSmem<DIM>;
+  double(*xs)[ST] = reinterpret_cast<double(*)[ST]>(mma_smem + M::XS);
+  double(*vsT)[MMA_VSP] = reinterpret_cast<double(*)[MMA_VSP]>(mma_smem + M::VS);
+  double(*tr)[2][4][64] = reinterpret_cast<double(*)[2][4][64]>(mma_smem + M::TR);
+  double(*colw)[8][8][34] = reinterpret_cast<double(*)[8][8][34]>(mma_smem + M::CW);
+  double* tab = mma_smem + M::TAB;
+  const int n = L.n;
+  const int nT = (n + ST - 1) / ST;
+  int a, b;
+  {
+    const int nup = S * (S - 1) / 2;
+    int p = blockIdx.x;
+    if (p < nup) {
+      a = 0;
+      while (p >= S - 1 - a) {
+        p -= S - 1 - a;
+        ++a;
+      }
+      b = a + 1 + p;
+    } else {
+      a = b = p - nup;
+    }
+  }
+  const int ia0 = a * tps, ia1 = min(nT, ia0 + tps);
+  const int jb1 = min(nT, b * tps + tps);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  if (threadIdx.x < 64) tab[threadIdx.x] = c_tang[threadIdx.x];
+  const double cs = hx_point_scale<KTYPE>(L.src.kp.a);
+  const int64_t slice = (int64_t)L.nrhs * n;
+  double* __restrict__ wsA = L.ws + (int64_t)a * slice;
+  double* __restrict__ wsB = L.ws + (int64_t)b * slice;
+  const hx_kparams kp = L.src.kp;
+  const double dcorr = kp.diag_replace ? kp.diag_value - 1.0 : kp.shift;
+  const int wsl = 8 * t + 2 * (g & 3) + (g >> 2);  // where this lane's K[g][t] goes
+
+  for (int I = ia0; I < ia1; ++I) {
+    const int rbase = I * ST + 32 * w;
+    double xr[4][DIM];        // coordinates of row g of each chunk
+    double xi0[4], xi1[4];    // X_I[row t][rhs g], X_I[row t + 4][rhs g]
+    double accR[4][2];        // Y_I[row g][rhs 2t, 2t + 1]
+#pragma unroll
+    for (int rc = 0; rc < 4; ++rc) {
+      const int r = rbase + 8 * rc + g;
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) xr[rc][d] = r < n ? cs * L.src.pts[d * L.src.ld + r] : 0.0;
+      const int r0 = rbase + 8 * rc + t, r1 = r0 + 4;
+      const bool cg = g < L.nrhs;
+      xi0[rc] = (cg && r0 < n) ? L.X[(int64_t)g * L.ldx + r0] : 0.0;
+      xi1[rc] = (cg && r1 < n) ? L.X[(int64_t)g * L.ldx + r1] : 0.0;
+      accR[rc][0] = accR[rc][1] = 0.0;
+    }
+    const int jstart = a == b ? I : b * tps;
+    for (int J = jstart; J < jb1; ++J) {
+      __syncthreads();  // every thread is done with the previous tile
+      {
+        const int u = threadIdx.x, j = J * ST + u, pu = mma_pos(u);
+        const bool ok = j < n;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) xs[d][pu] = ok ? cs * L.src.pts[d * L.src.ld + j] : 0.0;
+#pragma unroll
+        for (int c = 0; c < 8; ++c) vsT[c][pu] = (ok && c < L.nrhs) ? L.X[(int64_t)c * L.ldx + j] : 0.0;
+      }
+      __syncthreads();
+      const bool diag = J == I;  // diagonal tile pair: all entries, row sums only
+      for (int grp = 0; grp < ST / 32; ++grp) {
+#pragma unroll 1
+        for (int c4 = 0; c4 < 4; ++c4) {
+          const int cc = grp * 4 + c4;
+          const int p0 = 8 * cc + 2 * t;
+          double xc0[DIM], xc1[DIM];
+#pragma unroll
+          for (int d = 0; d < DIM; ++d) {
+            const double2 v = *reinterpret_cast<const double2*>(&xs[d][p0]);
+            xc0[d] = v.x;
+            xc1[d] = v.y;
+          }
+          const double2 xb = *reinterpret_cast<const double2*>(&vsT[g][p0]);
+          double e0[4], e1[4];
+#pragma unroll
+          for (int rc = 0; rc < 4; ++rc) {
+            double s0 = HX_R2_FLOOR, s1 = HX_R2_FLOOR;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+              const double d0 = xr[rc][d] - xc0[d], d1 = xr[rc][d] - xc1[d];
+              s0 = fma(d0, d0, s0);
+              s1 = fma(d1, d1, s1);
+            }
+            e0[rc] = hx_kernel_unit_t<KTYPE>(s0, tab);
+            e1[rc] = hx_kernel_unit_t<KTYPE>(s1, tab);
+            dmma_884(accR[rc], e0[rc], xb.x);
+            dmma_884(accR[rc], e1[rc], xb.y);
+          }
+          if (diag) continue;
+          double* tb = &tr[w][cc & 1][0][0];
+#pragma unroll
+          for (int rc = 0; rc < 4; ++rc) {
+            tb[rc * 64 + wsl] = e0[rc];
+            tb[rc * 64 + 32 + wsl] = e1[rc];
+          }
+          __syncwarp();
+          double accC[2] = {0.0, 0.0};  // Y_J[col g][rhs 2t, 2t + 1], this warp's rows
+#pragma unroll
+          for (int rc = 0; rc < 4; ++rc) {
+            const double2 v = *reinterpret_cast<const double2*>(&tb[rc * 64 + 8 * g + 2 * t]);
+            dmma_884(accC, v.x, xi0[rc]);
+            dmma_884(accC, v.y, xi1[rc]);
+          }
+          colw[grp & 1][w][2 * t][8 * c4 + g] = accC[0];
+          colw[grp & 1][w][2 * t + 1][8 * c4 + g] = accC[1];
+        }
+        if (diag) continue;
+        __syncthreads();
+        {
+          const int col = threadIdx.x & 31, c = threadIdx.x >> 5;
+          const int j = J * ST + grp * 32 + col;
+          if (c < L.nrhs && j < n) {
+            double sum = colw[grp & 1][0][c][col];
+#pragma unroll
+            for (int ww = 1; ww < 8; ++ww) sum += colw[grp & 1][ww][c][col];
+            double* dst = wsA + (int64_t)c * n + j;
+            *dst = I == ia0 ? sum : *dst + sum;
+          }
+        }
+      }
+    }
+    // row sums of tile I; in a diagonal block the earlier tiles' column sums
+    // are already there, and K_ii = f(0) + shift (or the replaced value)
+#pragma unroll
+    for (int rc = 0; rc < 4; ++rc) {
+      const int r = rbase + 8 * rc + g;
+      if (r >= n) continue;
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const int c = 2 * t + q;
+        if (c >= L.nrhs) continue;
+        double v = accR[rc][q];
+        if (a == b) v = fma(dcorr, L.X[(int64_t)c * L.ldx + r], v);
+        double* dst = wsB + (int64_t)c * n + r;
+        *dst = (a == b && I != ia0) ? *dst + v : v;
+      }
+    }
+  }
+}
+
+template <int KTYPE, int DIM>
+void launch_sym_mma_dim(const KmatvecLaunch& L, int S, int tps, cudaStream_t s) {
+  static bool attr_set = false;  // the opt-in above 48 KB, once per instance
+  if (!attr_set) {
+    cudaFuncSetAttribute(kmatvec_sym_mma_kernel<KTYPE, DIM>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MmaSmem<DIM>::BYTES);
+    attr_set = true;
+  }
+  const int grid = S * (S + 1) / 2;
+  kmatvec_sym_mma_kernel<KTYPE, DIM><<<grid, MMA_NT, MmaSmem<DIM>::BYTES, s>>>(L, S, tps);
+}
+
+template <int KTYPE>
+void launch_sym_mma(const KmatvecLaunch& L, int S, int tps, cudaStream_t s) {
+  if (L.src.kp.dim == 1)
+    launch_sym_mma_dim<KTYPE, 1>(L, S, tps, s);
+  else if (L.src.kp.dim == 2)
+    launch_sym_mma_dim<KTYPE, 2>(L, S, tps, s);
+  else
+    launch_sym_mma_dim<KTYPE, 3>(L, S, tps, s);
+}
+
+void launch_sym_mma_type(const KmatvecLaunch& L, int S, int tps, cudaStream_t s) {
+  switch (L.src.kp.type) {
+    case HX_KERNEL_GAUSSIAN: launch_sym_mma<HX_KERNEL_GAUSSIAN>(L, S, tps, s); break;
+    case HX_KERNEL_MATERN32: launch_sym_mma<HX_KERNEL_MATERN32>(L, S, tps, s); break;
+    case HX_KERNEL_INV_MULTIQUADRIC: launch_sym_mma<HX_KERNEL_INV_MULTIQUADRIC>(L, S, tps, s); break;
+    case HX_KERNEL_QUADRATIC: launch_sym_mma<HX_KERNEL_QUADRATIC>(L, S, tps, s); break;
+    default: launch_sym_mma<HX_KERNEL_EXPONENTIAL>(L, S, tps, s); break;
   }
 }
 
@@ -501,7 +724,7 @@ int kmatvec_sym_launch(const KmatvecLaunch& L, int S, cudaStream_t s) {
   else if (L.nrhs <= 4)
     launch_sym_type<4>(L, S, tps, s);
   else
-    launch_sym_type<8>(L, S, tps, s);
+    launch_sym_mma_type(L, S, tps, s);
   kmatvec_reduce<<<1024, 256, 0, s>>>(L, S);
   return (int)cudaGetLastError();
 }
