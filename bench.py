@@ -75,12 +75,14 @@ def profiled_figure(name, key):
 
 
 # FP64 FLOPs of the symmetric full-kernel product (kmatvec.cu / kfast.cuh),
-# FMA counted as 2: one Matern-3/2 entry in 2D costs 14 FMAs and 12 other FP64
-# operations (distance 2 sub + 1 mul + 1 fma; clamp; Newton square root 4 fma +
-# 4 mul; scale; Tang exp 1 clamp + 8 fma + 1 sub + 1 mul; (1+s)e^-s 1 fma) = 40
-# FLOPs, evaluated once per entry pair, plus 2 * nrhs FMAs (row and column
-# products) per evaluated entry.
-KMV_EVAL_FLOPS = 40
+# FMA counted as 2, as the kernel executes them: one Matern-3/2 entry in 2D is
+# the distance (2 sub + 2 fma from the floor), the square root from the
+# hardware seed (2 mul + 3 fma), Tang's exp (1 clamp, 1 fma + 1 sub for the
+# index, 2 fma for the reduction, 3 fma + 1 mul for the polynomial, 1 fma for
+# the table scale) and (1+s)e^-s (1 fma): 13 FMAs + 7 other = 33 FLOPs,
+# evaluated once per entry pair, plus 2 * nrhs FMAs (row and column products,
+# inside mma.m8n8k4.f64 for 8 right-hand sides) per evaluated entry.
+KMV_EVAL_FLOPS = 33
 
 
 def sym_slices(n):
@@ -437,11 +439,12 @@ def run_ours(args, rank, world, local_rank):
                 "h2d_bytes_per_step": int(pts.nbytes + b.nbytes),
                 "d2h_bytes_per_step": int(b.nbytes),
                 "dev_vs_host_solution_rel_diff": diff_dev_host},
-        "roofline": {"kernel": "kmatvec_sym_kernel (full-kernel FP64 product, 8 RHS; "
-                               "the largest share of the step)",
+        "roofline": {"kernel": "kmatvec_sym_mma_kernel (full-kernel FP64 product, 8 RHS, "
+                               "products on mma.m8n8k4.f64; the largest share of the step)",
                      "bound": "fp64", "achieved": kmv_tf, "peak": fp64_peak,
-                     "peak_kind": (f"nominal FP64 CUDA-core peak ({n_sms} SMs x 64 FMA/clk x 2 x "
-                                   f"{sm_mhz:.0f} MHz); no measured FP64 figure exists"),
+                     "peak_kind": (f"nominal FP64 peak ({n_sms} SMs x 64 FMA/clk x 2 x "
+                                   f"{sm_mhz:.0f} MHz), shared by FP64 FMAs and FP64 MMAs; "
+                                   "no measured FP64 figure exists"),
                      "unit": "TFLOP/s", "frac": kmv_tf / fp64_peak,
                      "traffic": (kmv_dram_ref * (N_PTS * sym_slices(N_PTS))
                                  / (65536.0 * sym_slices(65536)) if kmv_dram_ref else None),

@@ -20,18 +20,18 @@ namespace {
 constexpr int KT = 128;
 constexpr int RPT = 2;  // rows per thread
 
-__constant__ double c_tang[64] = HX_TANG_TABLE_INIT;
+__constant__ double c_tang[HX_TANG_TABLE_SIZE] = HX_TANG_TABLE_INIT;
 
 template <int NR, int KTYPE, int DIM>
 __global__ void __launch_bounds__(KT) kmatvec_kernel(KmatvecLaunch L) {
   __shared__ double xs[DIM > 0 ? DIM : 1][KT];
   __shared__ double vs[NR][KT];
-  __shared__ double tab[64];
+  __shared__ double tab[HX_TANG_TABLE_SIZE];
   const int n = L.n;
   const int nsplit = gridDim.y;
   const int per = ((n + nsplit - 1) / nsplit + KT - 1) / KT * KT;
   const int jb = blockIdx.y * per, je = min(n, jb + per);
-  if (threadIdx.x < 64) tab[threadIdx.x] = c_tang[threadIdx.x];
+  for (int i = threadIdx.x; i < HX_TANG_TABLE_SIZE; i += blockDim.x) tab[i] = c_tang[i];
   int row[RPT];
   bool live[RPT];
   double xi[RPT][DIM > 0 ? DIM : 1];
@@ -182,7 +182,7 @@ __global__ void __launch_bounds__(SymCfg<NR>::NT, SymCfg<NR>::MINB)
   __shared__ double xs[DIM][ST];
   __shared__ __align__(16) double vs[ST][VS];
   __shared__ __align__(16) double colw[2][SYM_NW][SG][VS];
-  __shared__ double tab[64];
+  __shared__ double tab[HX_TANG_TABLE_SIZE];
   const int n = L.n;
   const int nT = (n + ST - 1) / ST;
   int a, b;
@@ -203,7 +203,7 @@ __global__ void __launch_bounds__(SymCfg<NR>::NT, SymCfg<NR>::MINB)
   const int ia0 = a * tps, ia1 = min(nT, ia0 + tps);
   const int jb1 = min(nT, b * tps + tps);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  if (threadIdx.x < 64) tab[threadIdx.x] = c_tang[threadIdx.x];
+  for (int i = threadIdx.x; i < HX_TANG_TABLE_SIZE; i += blockDim.x) tab[i] = c_tang[i];
   const double cs = hx_point_scale<KTYPE>(L.src.kp.a);  // coordinates scaled once
   const int64_t slice = (int64_t)L.nrhs * n;
   double* __restrict__ wsA = L.ws + (int64_t)a * slice;  // column sums (rows of split b)
@@ -351,12 +351,16 @@ __global__ void __launch_bounds__(SymCfg<NR>::NT, SymCfg<NR>::MINB)
 //               K[t][g], K[t+4][g], the transpose, which goes through a
 //               per-warp shared-memory buffer (two 8-byte stores, one 16-byte
 //               load per lane).
-// Each warp's column sums of a chunk are stored per warp; after every 32
-// columns the CTA adds the eight warps' sums in warp order into the
-// workspace slice, so every (slice, row) still has one writer in a fixed
-// order.  The FP64 work per entry is the entry itself plus 16 FMAs inside
-// the MMAs, as in the FMA form, with half the instructions and a quarter of
-// the registers.
+// The chunks are software-pipelined: the column MMAs of chunk c - 1 (its
+// transpose written and warp-synchronised in the previous step) are issued
+// beside the entries of chunk c, so their dependent chain hides under the
+// entry arithmetic; two transpose buffers suffice because a step reads the
+// previous buffer before its own warp barrier.  Each warp's column sums of a
+// chunk are stored per warp; after every 32 columns the CTA adds the eight
+// warps' sums in warp order into the workspace slice, so every (slice, row)
+// still has one writer in a fixed order.  The FP64 work per entry is the
+// entry itself plus 16 FMAs inside the MMAs, as in the FMA form, with half
+// the instructions and half the registers.
 constexpr int MMA_NT = 256;  // 8 warps
 constexpr int MMA_VSP = ST + 8;  // padded row stride of the staged X tile
 
@@ -377,8 +381,8 @@ struct MmaSmem {
   static constexpr int VS = XS + DIM * ST;            // [8][MMA_VSP] X_J by rhs
   static constexpr int TR = VS + 8 * MMA_VSP;         // [8 warps][2][4 row chunks][64]
   static constexpr int CW = TR + 8 * 2 * 4 * 64;      // [2][8 warps][8 rhs][34]
-  static constexpr int TAB = CW + 2 * 8 * 8 * 34;     // [64]
-  static constexpr size_t BYTES = (size_t)(TAB + 64) * sizeof(double);
+  static constexpr int TAB = CW + 2 * 8 * 8 * 34;     // [HX_TANG_TABLE_SIZE]
+  static constexpr size_t BYTES = (size_t)(TAB + HX_TANG_TABLE_SIZE) * sizeof(double);
 };
 
 template <int KTYPE, int DIM>
@@ -412,7 +416,7 @@ __global__ void __launch_bounds__(MMA_NT, 2)
   const int jb1 = min(nT, b * tps + tps);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int g = lane >> 2, t = lane & 3;
-  if (threadIdx.x < 64) tab[threadIdx.x] = c_tang[threadIdx.x];
+  for (int i = threadIdx.x; i < HX_TANG_TABLE_SIZE; i += blockDim.x) tab[i] = c_tang[i];
   const double cs = hx_point_scale<KTYPE>(L.src.kp.a);
   const int64_t slice = (int64_t)L.nrhs * n;
   double* __restrict__ wsA = L.ws + (int64_t)a * slice;
@@ -449,67 +453,104 @@ __global__ void __launch_bounds__(MMA_NT, 2)
         for (int c = 0; c < 8; ++c) vsT[c][pu] = (ok && c < L.nrhs) ? L.X[(int64_t)c * L.ldx + j] : 0.0;
       }
       __syncthreads();
-      const bool diag = J == I;  // diagonal tile pair: all entries, row sums only
-      for (int grp = 0; grp < ST / 32; ++grp) {
-#pragma unroll 1
-        for (int c4 = 0; c4 < 4; ++c4) {
-          const int cc = grp * 4 + c4;
-          const int p0 = 8 * cc + 2 * t;
-          double xc0[DIM], xc1[DIM];
+      // entries of chunk cc and their row sums
+      auto chunk = [&](int cc, double (&e0)[4], double (&e1)[4]) {
+        const int p0 = 8 * cc + 2 * t;
+        double xc0[DIM], xc1[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+          const double2 v = *reinterpret_cast<const double2*>(&xs[d][p0]);
+          xc0[d] = v.x;
+          xc1[d] = v.y;
+        }
+        const double2 xb = *reinterpret_cast<const double2*>(&vsT[g][p0]);
+#pragma unroll
+        for (int rc = 0; rc < 4; ++rc) {
+          double s0 = HX_R2_FLOOR, s1 = HX_R2_FLOOR;
 #pragma unroll
           for (int d = 0; d < DIM; ++d) {
-            const double2 v = *reinterpret_cast<const double2*>(&xs[d][p0]);
-            xc0[d] = v.x;
-            xc1[d] = v.y;
+            const double d0 = xr[rc][d] - xc0[d], d1 = xr[rc][d] - xc1[d];
+            s0 = fma(d0, d0, s0);
+            s1 = fma(d1, d1, s1);
           }
-          const double2 xb = *reinterpret_cast<const double2*>(&vsT[g][p0]);
-          double e0[4], e1[4];
-#pragma unroll
-          for (int rc = 0; rc < 4; ++rc) {
-            double s0 = HX_R2_FLOOR, s1 = HX_R2_FLOOR;
-#pragma unroll
-            for (int d = 0; d < DIM; ++d) {
-              const double d0 = xr[rc][d] - xc0[d], d1 = xr[rc][d] - xc1[d];
-              s0 = fma(d0, d0, s0);
-              s1 = fma(d1, d1, s1);
-            }
-            e0[rc] = hx_kernel_unit_t<KTYPE>(s0, tab);
-            e1[rc] = hx_kernel_unit_t<KTYPE>(s1, tab);
-            dmma_884(accR[rc], e0[rc], xb.x);
-            dmma_884(accR[rc], e1[rc], xb.y);
-          }
-          if (diag) continue;
-          double* tb = &tr[w][cc & 1][0][0];
-#pragma unroll
-          for (int rc = 0; rc < 4; ++rc) {
-            tb[rc * 64 + wsl] = e0[rc];
-            tb[rc * 64 + 32 + wsl] = e1[rc];
-          }
-          __syncwarp();
-          double accC[2] = {0.0, 0.0};  // Y_J[col g][rhs 2t, 2t + 1], this warp's rows
-#pragma unroll
-          for (int rc = 0; rc < 4; ++rc) {
-            const double2 v = *reinterpret_cast<const double2*>(&tb[rc * 64 + 8 * g + 2 * t]);
-            dmma_884(accC, v.x, xi0[rc]);
-            dmma_884(accC, v.y, xi1[rc]);
-          }
-          colw[grp & 1][w][2 * t][8 * c4 + g] = accC[0];
-          colw[grp & 1][w][2 * t + 1][8 * c4 + g] = accC[1];
+          e0[rc] = hx_kernel_unit_t<KTYPE>(s0, tab);
+          e1[rc] = hx_kernel_unit_t<KTYPE>(s1, tab);
+          dmma_884(accR[rc], e0[rc], xb.x);
+          dmma_884(accR[rc], e1[rc], xb.y);
         }
-        if (diag) continue;
-        __syncthreads();
-        {
-          const int col = threadIdx.x & 31, c = threadIdx.x >> 5;
-          const int j = J * ST + grp * 32 + col;
-          if (c < L.nrhs && j < n) {
-            double sum = colw[grp & 1][0][c][col];
+      };
+      auto put_tr = [&](int buf, const double (&e0)[4], const double (&e1)[4]) {
+        double* tb = &tr[w][buf][0][0];
 #pragma unroll
-            for (int ww = 1; ww < 8; ++ww) sum += colw[grp & 1][ww][c][col];
-            double* dst = wsA + (int64_t)c * n + j;
-            *dst = I == ia0 ? sum : *dst + sum;
-          }
+        for (int rc = 0; rc < 4; ++rc) {
+          tb[rc * 64 + wsl] = e0[rc];
+          tb[rc * 64 + 32 + wsl] = e1[rc];
+        }
+      };
+      auto get_tr = [&](int buf, double2 (&v)[4]) {
+        const double* tb = &tr[w][buf][0][0];
+#pragma unroll
+        for (int rc = 0; rc < 4; ++rc) v[rc] = *reinterpret_cast<const double2*>(&tb[rc * 64 + 8 * g + 2 * t]);
+      };
+      // column sums of chunk cc over this warp's rows, into the group buffer
+      auto col_sums = [&](int cc, const double2 (&v)[4]) {
+        double accC[2] = {0.0, 0.0};
+#pragma unroll
+        for (int rc = 0; rc < 4; ++rc) {
+          dmma_884(accC, v[rc].x, xi0[rc]);
+          dmma_884(accC, v[rc].y, xi1[rc]);
+        }
+        colw[(cc >> 2) & 1][w][2 * t][8 * (cc & 3) + g] = accC[0];
+        colw[(cc >> 2) & 1][w][2 * t + 1][8 * (cc & 3) + g] = accC[1];
+      };
+      auto reduce_group = [&](int grp) {
+        const int col = threadIdx.x & 31, c = threadIdx.x >> 5;
+        const int j = J * ST + grp * 32 + col;
+        if (c < L.nrhs && j < n) {
+          double sum = colw[grp & 1][0][c][col];
+#pragma unroll
+          for (int ww = 1; ww < 8; ++ww) sum += colw[grp & 1][ww][c][col];
+          double* dst = wsA + (int64_t)c * n + j;
+          *dst = I == ia0 ? sum : *dst + sum;
+        }
+      };
+      if (J == I) {  // diagonal tile pair: all entries, row sums only
+#pragma unroll 1
+        for (int cc = 0; cc < ST / 8; ++cc) {
+          double e0[4], e1[4];
+          chunk(cc, e0, e1);
+        }
+        continue;
+      }
+      // software pipeline: the column sums of chunk cc - 1 (entries already
+      // transposed) run beside the entries of chunk cc
+      {
+        double e0[4], e1[4];
+        chunk(0, e0, e1);
+        put_tr(0, e0, e1);
+        __syncwarp();
+      }
+#pragma unroll 1
+      for (int cc = 1; cc < ST / 8; ++cc) {
+        double2 v[4];
+        get_tr((cc - 1) & 1, v);
+        double e0[4], e1[4];
+        chunk(cc, e0, e1);
+        col_sums(cc - 1, v);
+        put_tr(cc & 1, e0, e1);
+        __syncwarp();
+        if ((cc & 3) == 0) {
+          __syncthreads();
+          reduce_group((cc >> 2) - 1);
         }
       }
+      {
+        double2 v[4];
+        get_tr(1, v);
+        col_sums(ST / 8 - 1, v);
+      }
+      __syncthreads();
+      reduce_group(ST / 32 - 1);
     }
     // row sums of tile I; in a diagonal block the earlier tiles' column sums
     // are already there, and K_ii = f(0) + shift (or the replaced value)
@@ -601,10 +642,10 @@ __global__ void __launch_bounds__(KT) kmatvec_forest_kernel(KmatvecLaunch L,
                                                             const int4* __restrict__ items) {
   __shared__ double xs[DIM][KT];
   __shared__ double vs[NR][KT];
-  __shared__ double tab[64];
+  __shared__ double tab[HX_TANG_TABLE_SIZE];
   const int4 it = items[blockIdx.x];
   const hx_kparams kp = L.src.kps[it.w];
-  if (threadIdx.x < 64) tab[threadIdx.x] = c_tang[threadIdx.x];
+  for (int i = threadIdx.x; i < HX_TANG_TABLE_SIZE; i += blockDim.x) tab[i] = c_tang[i];
   int row[RPT];
   bool live[RPT];
   double xi[RPT][DIM];

@@ -821,6 +821,7 @@ double orc_entry(void* h, int i, int j) { return ((Oracle*)h)->entry(i, j); }
 double orc_exp(double x) { return hx_exp(x); }
 double orc_exp_tang(double x) { return hx_exp_tang(x, hx_tang_host); }
 double orc_exp_tang_neg(double x) { return hx_exp_tang_neg(x, hx_tang_host); }
+double orc_tang_entry(int j) { return j >= 0 && j < HX_TANG_TABLE_SIZE ? hx_tang_host[j] : 0.0; }
 
 // Full-kernel product Y = K X (kernelMatrix::operator*, src/kernel.cpp:27-35),
 // summing over k in order for each (i, j); rows spread over threads.

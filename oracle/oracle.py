@@ -62,6 +62,8 @@ def lib():
         L.orc_exp_tang.restype = ctypes.c_double
         L.orc_exp_tang_neg.argtypes = [ctypes.c_double]
         L.orc_exp_tang_neg.restype = ctypes.c_double
+        L.orc_tang_entry.argtypes = [ctypes.c_int]
+        L.orc_tang_entry.restype = ctypes.c_double
         L.orc_kernel_matvec.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp, ctypes.c_int]
         L.orc_aca_block.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, _dp, _ip]
         L.orc_bench_node.restype = ctypes.c_double
@@ -221,3 +223,8 @@ def hx_exp_tang(x):
 
 def hx_exp_tang_neg(x):
     return lib().orc_exp_tang_neg(float(x))
+
+
+def tang_entry(j):
+    """Entry j of the 2^(j/256) table of the residual path's exp (kfast.cuh)."""
+    return lib().orc_tang_entry(int(j))

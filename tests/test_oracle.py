@@ -54,6 +54,16 @@ def test_exp_within_one_ulp(oracle_mod):
     assert oracle_mod.hx_exp(0.0) == 1.0
 
 
+def test_tang_table_correctly_rounded(oracle_mod):
+    """Every entry of the 2^(j/256) table is the double nearest to the exact
+    value (computed here with 80-digit decimal arithmetic)."""
+    from decimal import Decimal, getcontext
+    getcontext().prec = 80
+    ln2 = Decimal(2).ln()
+    for j in range(256):
+        assert oracle_mod.tang_entry(j) == float((ln2 * j / 256).exp()), j
+
+
 def test_tang_exp_within_two_ulp(oracle_mod):
     """The table-driven exp of the residual path (kfast.cuh) against libm."""
     xs = np.concatenate([np.linspace(-745.0, 709.7, 40001),
