@@ -404,7 +404,7 @@ def run_ours(args, rank, world, local_rank):
     evaluated = N_PTS * (N_PTS + 256) / 2.0
     kmv_flops = evaluated * (KMV_EVAL_FLOPS + 4 * NRHS)
     kmv_tf = kmv_flops / t_kmatvec / 1e12
-    kmv_dram_ref = profiled_figure("kmatvec_sym_matern2d_n65536.md", "dram_bytes_per_launch")
+    kmv_dram_ref = profiled_figure("kmatvec_sym_mma_matern2d_n65536.md", "dram_bytes_per_launch")
     out = {
         "metric": METRIC,
         "value": job_rate(ms_max, world),
