@@ -42,6 +42,8 @@ _PF = ctypes.POINTER(ctypes.c_float)
 SIGNATURES = {
     "hodlr_create_kernel": (_I, [ctypes.POINTER(_H), _I, _I, _PD, ctypes.POINTER(KernelDesc), _I]),
     "hodlr_create_dense": (_I, [ctypes.POINTER(_H), _I, _PD, _I, _I]),
+    "hodlr_create_dense_device": (_I, [ctypes.POINTER(_H), _I, _I, ctypes.POINTER(_VP),
+                                       ctypes.POINTER(ctypes.c_int64)]),
     "hodlr_create_fnptr": (_I, [ctypes.POINTER(_H), _I, _I, _V, _V, _I]),
     "hodlr_destroy": (None, [_H]),
     "hodlr_reset": (_I, [_H]),

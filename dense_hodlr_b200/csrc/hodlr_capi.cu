@@ -2144,6 +2144,34 @@ int hodlr_create_dense(hodlr_t* out, int n, const double* A, int lda, int leaf_s
   return HODLR_OK;
 }
 
+int hodlr_create_dense_device(hodlr_t* out, int n, int leaf_size, double** dA, int64_t* ld) {
+  if (!out || n <= 0 || leaf_size < 1 || !dA || !ld) return HODLR_ERR_ARG;
+  *out = nullptr;
+  *dA = nullptr;
+  *ld = 0;
+  hodlr_t h = new hodlr_handle_s();
+  h->n = n;
+  h->dim = 0;
+  h->leaf = leaf_size;
+  h->dense = true;
+  int rc = init_common(h);
+  if (!rc) {
+    cudaError_t e = dalloc(h, &h->d_A, (size_t)n * n);
+    // the stream-ordered allocation is complete before the caller's fill,
+    // which may run on any stream
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) rc = cuda_fail(h, e, "matrix allocation");
+  }
+  if (rc) {
+    hodlr_destroy(h);
+    return rc;
+  }
+  *dA = h->d_A;
+  *ld = n;
+  *out = h;
+  return HODLR_OK;
+}
+
 int hodlr_create_forest(hodlr_t* out, int nsys, const int* sizes, int dim, const double* pts,
                         const hodlr_kernel_desc* kernels, int leaf_size) {
   if (!out || nsys < 1 || !sizes || dim < 1 || dim > 3 || !pts || !kernels || leaf_size < 1)

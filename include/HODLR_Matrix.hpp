@@ -8,7 +8,9 @@
 //    prints and calls exit(EXIT_FAILURE);
 //  * a host function-pointer kernel cannot run on the GPU: that constructor
 //    throws HODLR_ERR_UNSUPPORTED; pass a closed-form kernel of points instead
-//    (hodlr_kernel_desc + coordinates), or a dense matrix;
+//    (hodlr_kernel_desc + coordinates), a dense matrix, or (compiled with
+//    nvcc) a functor with a __device__ operator()(int i, int j), evaluated on
+//    the GPU into a stored n x n matrix;
 //  * only the "partialPiv_ACA" low-rank method and the recLU solver exist.
 // Without Eigen the matrices are hodlr_b200::Matrix (column-major); with
 // Eigen on the include path the Eigen::MatrixXd overloads are added.
@@ -23,6 +25,12 @@
 #include <vector>
 
 #include "hodlr_b200.h"
+
+#if defined(__CUDACC__)
+#include <cuda_runtime.h>
+
+#include <type_traits>
+#endif
 
 #if defined(__has_include)
 #if __has_include(<Eigen/Dense>)
@@ -141,6 +149,19 @@ class user_IndexTree {
   }
 };
 
+#if defined(__CUDACC__)
+namespace detail {
+// A[i + j ld] = f(i, j): one thread per row, coalesced in i; grid.y strides
+// over the columns.
+template <class F>
+__global__ void fill_from_functor(F f, double* A, int64_t ld, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int j = blockIdx.y; j < n; j += gridDim.y) A[(int64_t)j * ld + i] = f(i, j);
+}
+}  // namespace detail
+#endif
+
 class HODLR_Matrix {
  public:
   bool printResultInfo = false;
@@ -176,6 +197,39 @@ class HODLR_Matrix {
                                          inputSizeThreshold),
                       "HODLR_Matrix(kernel function)");
   }
+
+#if defined(__CUDACC__)
+  // HODLR_Matrix(int, int, double (*)(int,int,void*), void*, int)  (reference :162)
+  // as a device functor: kernel(i, j) is a __device__ (or __host__ __device__)
+  // call operator over data the functor reaches on the device.  It is
+  // evaluated once per entry by a kernel compiled in the caller's translation
+  // unit into an n x n matrix the handle owns (n^2 doubles of HBM); from
+  // there compression, factorization and solves are those of the dense
+  // constructor, and the entries are exactly what the functor returns.
+  template <class KernelFunctor,
+            class = typename std::enable_if<std::is_class<KernelFunctor>::value>::type>
+  HODLR_Matrix(int numRows, int numCols, KernelFunctor kernel, int inputSizeThreshold = 30) {
+    if (numRows != numCols)
+      throw hodlr_b200::Error(HODLR_ERR_ARG, "only square kernel matrices form a HODLR tree");
+    double* dA = nullptr;
+    int64_t ld = 0;
+    hodlr_b200::check(nullptr,
+                      hodlr_create_dense_device(&h_, numRows, inputSizeThreshold, &dA, &ld),
+                      "HODLR_Matrix(kernel functor)");
+    n_ = numRows;
+    const unsigned gy = numRows < 65535 ? (unsigned)numRows : 65535u;
+    detail::fill_from_functor<<<dim3((unsigned)((numRows + 255) / 256), gy), 256>>>(kernel, dA, ld,
+                                                                                     numRows);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+    if (e != cudaSuccess) {
+      hodlr_destroy(h_);
+      h_ = nullptr;
+      throw hodlr_b200::Error(HODLR_ERR_CUDA, std::string("kernel functor fill: ") +
+                                                  cudaGetErrorString(e));
+    }
+  }
+#endif
 
   // The GPU form of the kernel constructor: K_ij = f(|x_i - x_j|) for points
   // pts (dim x numRows, SoA, host memory; copied).

@@ -62,6 +62,17 @@ int hodlr_create_kernel(hodlr_t* out, int n, int dim, const double* pts,
 int hodlr_create_dense(hodlr_t* out, int n, const double* A, int lda, int leaf_size);
 
 /* HODLR_Matrix(int, int, double (*)(int,int,void*), void*, int)     (:162)
+ * in its device-functor form: a dense handle whose n x n column-major FP64
+ * matrix lives in device memory owned by the handle, left uninitialised.
+ * *dA receives its address and *ld its leading dimension (n).  The caller
+ * writes every entry K(i, j) = dA[i + j * ld] on the device (the C++ facade
+ * launches a kernel evaluating a __device__ functor, compiled in the caller's
+ * translation unit) and completes that work before the next call on the
+ * handle; from then on the handle behaves as hodlr_create_dense's.  Memory
+ * is n^2 doubles: entries are stored, not regenerated. */
+int hodlr_create_dense_device(hodlr_t* out, int n, int leaf_size, double** dA, int64_t* ld);
+
+/* HODLR_Matrix(int, int, double (*)(int,int,void*), void*, int)     (:162)
  * with an arbitrary host function: returns HODLR_ERR_UNSUPPORTED, because a
  * host function pointer cannot be evaluated by GPU kernels.  Use
  * hodlr_create_kernel (closed-form kernels) or hodlr_create_dense. */

@@ -270,6 +270,27 @@ def test_cpp_facade_drop_in(tmp_path):
     assert out.returncode == 0, out.stdout + out.stderr
 
 
+def test_cpp_device_functor_constructor(tmp_path):
+    """The device-functor form of HODLR_Matrix(int, int, kernel, data, leaf)
+    (include/HODLR_Matrix.hpp, compiled with nvcc): a functor returning the
+    library's closed-form entries gives the closed-form constructor's ranks and
+    solution; a kernel without a closed form solves to a small residual."""
+    import os
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    exe = tmp_path / "functor_test"
+    subprocess.run(["nvcc", "-gencode", "arch=compute_100a,code=sm_100a", "-O2", "-std=c++17",
+                    os.path.join(root, "tests", "cpp", "functor_test.cu"),
+                    "-I", os.path.join(root, "include"),
+                    "-I", os.path.join(root, "dense_hodlr_b200", "csrc"),
+                    "-L", os.path.join(root, "dense_hodlr_b200"), "-lhodlr_b200",
+                    "-Xlinker", "-rpath", "-Xlinker", os.path.join(root, "dense_hodlr_b200"),
+                    "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=600)
+    print(out.stdout)
+    assert out.returncode == 0, out.stdout + out.stderr
+
+
 def test_solve_graph_replay_is_bit_identical():
     """The direct solve is captured as a CUDA graph on first use and replayed
     afterwards: replays give the same bits as the first (captured) run and as
