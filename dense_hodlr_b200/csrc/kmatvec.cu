@@ -3,14 +3,17 @@
 // reference uses for the residual ||K x - b|| / ||b|| (src/HODLR_Matrix.cpp:
 // 785-787), and supplies the residual of iterative refinement and GMRES.
 //
-// Compute-bound on the FP64 pipe: the distance, rsqrt / Tang exp from
-// kfast.cuh (specialised per kernel family at compile time, so an entry costs
-// ~25 FP64 instructions and no dispatch) and one FMA per right-hand side.  A
-// CTA owns RPT * KT rows (RPT per thread, sharing every staged column value),
-// NR accumulators per row in registers; column coordinates and X rows are
-// staged through shared memory KT at a time.  Column ranges are split over
-// gridDim.y when the row tiles alone cannot fill the GPU; the partial sums
-// are added in a fixed order by kmatvec_reduce.
+// Bound by the FP64 units: the distance, square root and Tang exp from
+// kfast.cuh (specialised per kernel family at compile time, no dispatch) and
+// two products per right-hand side and evaluated entry.  Four forms:
+//   kmatvec_kernel          row by row (dense input, the no-alloc entry, up to
+//                           16 right-hand sides); column ranges split over
+//                           gridDim.y, partial sums added in a fixed order;
+//   kmatvec_sym_kernel      each entry evaluated once for K_ij and K_ji,
+//                           1 to 4 right-hand sides, FMAs;
+//   kmatvec_sym_mma_kernel  the same for 5 to 8 right-hand sides with the
+//                           products on mma.m8n8k4.f64;
+//   kmatvec_forest_kernel   block-diagonal product over a forest of systems.
 #include "common.cuh"
 #include "kfast.cuh"
 #include "kmatvec.h"
@@ -159,14 +162,15 @@ void launch_type(const KmatvecLaunch& L, dim3 grid, cudaStream_t s) {
 // per group) and accumulated into the workspace.
 constexpr int ST = 256;  // tile edge (rows = columns)
 constexpr int SG = 32;   // rotation group
-// rows per thread: 4 for 8 right-hand sides (halves the rotation shuffles and
-// X loads per evaluated entry), else 2
+// 1 to 4 right-hand sides (more go to kmatvec_sym_mma_kernel): 2 rows per
+// thread, 128 threads
 template <int NR>
 struct SymCfg {
-  static constexpr int RPT = NR == 8 ? 4 : 2;
+  static_assert(NR == 1 || NR == 4, "the FMA form serves 1 to 4 right-hand sides");
+  static constexpr int RPT = 2;
   static constexpr int NT = ST / RPT;
   static constexpr int NW = NT / 32;
-  static constexpr int MINB = NR == 8 ? 4 : 3;
+  static constexpr int MINB = 3;
 };
 
 template <int NR>
@@ -573,12 +577,12 @@ __global__ void __launch_bounds__(MMA_NT, 2)
 
 template <int KTYPE, int DIM>
 void launch_sym_mma_dim(const KmatvecLaunch& L, int S, int tps, cudaStream_t s) {
-  static bool attr_set = false;  // the opt-in above 48 KB, once per instance
-  if (!attr_set) {
-    cudaFuncSetAttribute(kmatvec_sym_mma_kernel<KTYPE, DIM>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MmaSmem<DIM>::BYTES);
-    attr_set = true;
-  }
+  // the opt-in above 48 KB of shared memory, once per instance (thread-safe
+  // static initialisation); a failure shows as the launch's error
+  static const cudaError_t attr = cudaFuncSetAttribute(
+      kmatvec_sym_mma_kernel<KTYPE, DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      (int)MmaSmem<DIM>::BYTES);
+  (void)attr;
   const int grid = S * (S + 1) / 2;
   kmatvec_sym_mma_kernel<KTYPE, DIM><<<grid, MMA_NT, MmaSmem<DIM>::BYTES, s>>>(L, S, tps);
 }
