@@ -359,10 +359,105 @@ __global__ void __launch_bounds__(SNT) schur_lu_kernel(SchurLaunch L, int pnb) {
   if (tid == 0 && singular) atomicOr(L.err, DEV_ERR_SINGULAR);
 }
 
+// x <- U^-1 L^-1 x for `ncol` columns in shared memory (x[c*ldx+i]) with the
+// packed LU of an n x n matrix in global memory (column-major, ld n): the
+// capacitance matrices, up to a few thousand rows, with few columns per CTA.
+// Diagonal blocks of GB rows: one warp per column substitutes with the
+// block's row of A in registers (lane = row) and each solved value broadcast
+// by a shuffle, so the sequential chain is shuffles and FMAs, not memory
+// loads.  Rows outside the block: one thread per row loads its GB entries of
+// A once and updates every column.  The forward sweep performs exactly the
+// operations of a row-by-row substitution, in the same order (ascending
+// column); the backward sweep subtracts within a diagonal block in
+// descending column order.
+constexpr int GB = 32;
+
+__device__ void lu_solve_global(const double* __restrict__ a, int n, double* x, int ldx,
+                                int ncol) {
+  const int tid = threadIdx.x, NT = blockDim.x;
+  const int lane = tid & 31, wid = tid >> 5, NW = NT >> 5;
+  for (int b0 = 0; b0 < n; b0 += GB) {  // forward, unit lower
+    const int nb = min(GB, n - b0), be = b0 + nb;
+    if (wid < ncol) {
+      double ar[GB];  // A(b0 + lane, b0 + p), p < lane
+#pragma unroll
+      for (int p = 0; p < GB; ++p)
+        ar[p] = (p < lane && lane < nb) ? __ldg(a + (int64_t)(b0 + p) * n + b0 + lane) : 0.0;
+      for (int c = wid; c < ncol; c += NW) {
+        double* xc = x + c * ldx + b0;
+        double t = lane < nb ? xc[lane] : 0.0;
+#pragma unroll
+        for (int p = 0; p < GB - 1; ++p) {
+          const double xp = __shfl_sync(0xffffffffu, t, p);
+          if (p < lane) t = fma(-ar[p], xp, t);
+        }
+        if (lane < nb) xc[lane] = t;
+      }
+    }
+    __syncthreads();
+    for (int r = be + tid; r < n; r += NT) {
+      double ar[GB];  // A(r, b0 + p)
+#pragma unroll
+      for (int p = 0; p < GB; ++p) ar[p] = p < nb ? __ldg(a + (int64_t)(b0 + p) * n + r) : 0.0;
+      for (int c = 0; c < ncol; ++c) {
+        double* xc = x + c * ldx;
+        double t = xc[r];
+#pragma unroll
+        for (int p = 0; p < GB; ++p)
+          if (p < nb) t = fma(-ar[p], xc[b0 + p], t);
+        xc[r] = t;
+      }
+    }
+    __syncthreads();
+  }
+  for (int be = n; be > 0; be -= GB) {  // backward, upper
+    const int b0 = max(0, be - GB), nb = be - b0;
+    if (wid < ncol) {
+      double ar[GB];  // A(b0 + lane, b0 + p), p > lane
+#pragma unroll
+      for (int p = 0; p < GB; ++p)
+        ar[p] = (lane < p && p < nb) ? __ldg(a + (int64_t)(b0 + p) * n + b0 + lane) : 0.0;
+      const double ad = lane < nb ? __ldg(a + (int64_t)(b0 + lane) * n + b0 + lane) : 1.0;
+      for (int c = wid; c < ncol; c += NW) {
+        double* xc = x + c * ldx + b0;
+        double t = lane < nb ? xc[lane] : 0.0;
+#pragma unroll
+        for (int p = GB - 1; p >= 0; --p) {
+          if (p >= nb) continue;  // the same for every lane
+          if (lane == p) t = t / ad;
+          const double xp = __shfl_sync(0xffffffffu, t, p);
+          if (lane < p) t = fma(-ar[p], xp, t);
+        }
+        if (lane < nb) xc[lane] = t;
+      }
+    }
+    __syncthreads();
+    for (int r = tid; r < b0; r += NT) {
+      double ar[GB];  // A(r, b0 + p)
+#pragma unroll
+      for (int p = 0; p < GB; ++p) ar[p] = p < nb ? __ldg(a + (int64_t)(b0 + p) * n + r) : 0.0;
+      for (int c = 0; c < ncol; ++c) {
+        double* xc = x + c * ldx;
+        double t = xc[r];
+#pragma unroll
+        for (int p = 0; p < GB; ++p)
+          if (p < nb) t = fma(-ar[p], xc[b0 + p], t);
+        xc[r] = t;
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // y = S^-1 rhs for `ncols` right-hand sides stored in R (ld sd) at r_off
 // (ncols < 0: N.coff columns); one CTA per (node, tile of STC columns).
+// WARP_SUBST selects lu_solve_global, whose short sequential chains suit the
+// solve (one CTA per node, latency-bound at the top levels); the ancestor
+// columns of the factorization (many CTAs per node, throughput-bound) keep
+// the 32-register blocked tile solve.
 constexpr int STC = 16;
 
+template <bool WARP_SUBST>
 __global__ void __launch_bounds__(256) schur_solve_kernel(SchurLaunch L, int ncols) {
   extern __shared__ double xs[];
   const int node = blockIdx.y;
@@ -393,7 +488,10 @@ __global__ void __launch_bounds__(256) schur_solve_kernel(SchurLaunch L, int nco
     }
   }
   __syncthreads();
-  lu_solve_tile(GlobalLU{a, n}, n, xs, ldx, nc);
+  if (WARP_SUBST)
+    lu_solve_global(a, n, xs, ldx, nc);
+  else
+    lu_solve_tile(GlobalLU{a, n}, n, xs, ldx, nc);
   for (int e = threadIdx.x; e < n * nc; e += blockDim.x) {
     int i = e % n, c = e / n;
     R[(int64_t)(c0 + c) * n + i] = xs[c * ldx + i];
@@ -444,9 +542,17 @@ int schur_solve_launch(const SchurLaunch& L, int nnodes, int ncols, int max_cols
                        cudaStream_t s) {
   if (nnodes == 0 || max_cols <= 0) return 0;
   size_t smem = sizeof(double) * (size_t)(max_sd | 1) * STC;
-  if (smem > 48 * 1024)
-    cudaFuncSetAttribute(schur_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)smem);
-  schur_solve_kernel<<<dim3((max_cols + STC - 1) / STC, nnodes), 256, smem, s>>>(L, ncols);
+  const dim3 grid((max_cols + STC - 1) / STC, nnodes);
+  if (ncols >= 0) {
+    if (smem > 48 * 1024)
+      cudaFuncSetAttribute(schur_solve_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem);
+    schur_solve_kernel<true><<<grid, 256, smem, s>>>(L, ncols);
+  } else {
+    if (smem > 48 * 1024)
+      cudaFuncSetAttribute(schur_solve_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem);
+    schur_solve_kernel<false><<<grid, 256, smem, s>>>(L, ncols);
+  }
   return (int)cudaGetLastError();
 }
