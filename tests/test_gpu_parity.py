@@ -2,7 +2,7 @@
 
 Bit-exact: tree, ACA pivot sequences, ranks and the W/V factors (integer and
 pivot-deciding FP64 work).  Tolerance: solutions within 1e-10 relative
-difference of the oracle (the north-star bar for the FP64 path), residuals
+difference of the oracle (the parity bar of the FP64 path), residuals
 with the full kernel.  Blocks whose stopping test came within 1e-10 of the
 tolerance (a "near tie", where reduction order may decide the rank) are
 reported and excluded from the bit-exact rank comparison; the tests assert
