@@ -131,6 +131,7 @@ def test_kernel_matvec_matches_oracle(oracle_mod):
     (9000, 3, "inv_multiquadric", 4, False),
     (4097, 3, "gaussian", 8, False),     # tensor-core form, 3D, one row past a tile
     (1300, 1, "matern32", 6, False),     # tensor-core form, 1D, 6 of 8 columns live
+    (100, 2, "matern32", 8, False),      # tensor-core form, one partial tile (diagonal pair only)
 ])
 def test_symmetric_kernel_matvec(oracle_mod, n, dim, kind, nrhs, diag_replace):
     """The symmetric full-kernel product (each entry evaluated once for both
