@@ -14,10 +14,12 @@ ERR_SINGULAR = 5
 ERR_STATE = 6
 ERR_NONFINITE = 7
 ERR_TIMEOUT = 8
+ERR_IO = 9
 
 _STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "device memory exhausted",
            4: "unsupported on the GPU path", 5: "exact-zero pivot", 6: "call out of order",
-           7: "non-finite value", 8: "device wait timed out"}
+           7: "non-finite value", 8: "device wait timed out",
+           9: "file could not be read or written"}
 
 
 def status_string(s):
@@ -44,6 +46,9 @@ SIGNATURES = {
     "hodlr_create_dense": (_I, [ctypes.POINTER(_H), _I, _PD, _I, _I]),
     "hodlr_create_dense_device": (_I, [ctypes.POINTER(_H), _I, _I, ctypes.POINTER(_VP),
                                        ctypes.POINTER(ctypes.c_int64)]),
+    "hodlr_matrix_file_dims": (_I, [ctypes.c_char_p, _PI, _PI]),
+    "hodlr_read_matrix_file": (_I, [ctypes.c_char_p, _I, _I, _PD, _I]),
+    "hodlr_write_matrix_file": (_I, [ctypes.c_char_p, _I, _I, _PD, _I]),
     "hodlr_create_fnptr": (_I, [ctypes.POINTER(_H), _I, _I, _V, _V, _I]),
     "hodlr_destroy": (None, [_H]),
     "hodlr_reset": (_I, [_H]),

@@ -2879,6 +2879,7 @@ const char* hodlr_status_string(int s) {
     case HODLR_ERR_STATE: return "call out of order";
     case HODLR_ERR_NONFINITE: return "non-finite value";
     case HODLR_ERR_TIMEOUT: return "device wait timed out";
+    case HODLR_ERR_IO: return "file could not be read or written";
     default: return "unknown status";
   }
 }

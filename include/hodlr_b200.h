@@ -30,6 +30,7 @@ typedef struct hodlr_handle_s* hodlr_t;
 #define HODLR_ERR_STATE 6       /* call out of order */
 #define HODLR_ERR_NONFINITE 7   /* a NaN/Inf matrix entry or residual */
 #define HODLR_ERR_TIMEOUT 8     /* a bounded device wait gave up */
+#define HODLR_ERR_IO 9          /* a file could not be opened, read or written */
 
 /* kernel families: K_ij = f(r_ij) (+ shift on the diagonal) */
 #define HODLR_KERNEL_GAUSSIAN 0          /* exp(-r^2/l^2) */
@@ -300,6 +301,17 @@ int hodlr_gemm_device(int precision, int mode, int m, int n, int k, const double
 
 /* Number of kernels this handle has launched since it was created. */
 int hodlr_get_launch_count(hodlr_t h, long long* count);
+
+/* Dense-matrix files of the reference's binary format (include/matrixIO.hpp:38-53,
+ * saveMatrixXdToBinary / readBinaryIntoMatrixXd, src/matrixIO.cpp:159-202):
+ * two native int32 (rows, cols), then rows x cols FP64 values row by row.
+ * Matrices here are column-major with leading dimension lda.  Host-only: no
+ * GPU is needed.  HODLR_ERR_IO: the file cannot be opened, is short, or its
+ * header holds negative sizes; HODLR_ERR_ARG: null pointers, lda < rows, or
+ * (read) sizes other than the file's. */
+int hodlr_matrix_file_dims(const char* path, int* rows, int* cols);
+int hodlr_read_matrix_file(const char* path, int rows, int cols, double* A, int lda);
+int hodlr_write_matrix_file(const char* path, int rows, int cols, const double* A, int lda);
 
 /* Full-kernel FP64 product d_y = K d_x that allocates no device memory.  It
  * has no counterpart in the reference.  It is for callers that cannot call

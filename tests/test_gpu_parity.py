@@ -175,6 +175,35 @@ def test_dense_input_inverse_multiquadric(oracle_mod):
     assert np.linalg.norm(xs - xo) / np.linalg.norm(xo) <= SOLVE_TOL
 
 
+def test_dense_input_from_matrix_file(oracle_mod, tmp_path):
+    """Dense input through the reference's binary matrix file
+    (saveMatrixXdToBinary / readBinaryIntoMatrixXd, src/matrixIO.cpp:159-202):
+    a Gaussian 1D matrix written to a file, read back by the C ABI, compressed
+    and solved on the GPU, against the oracle on the same entries, bit for bit
+    in pivots and ranks, so no kernel-function rounding enters the parity."""
+    import ctypes
+    from dense_hodlr_b200 import _lib
+    from dense_hodlr_b200.matrix_io import saveMatrixXdToBinary
+    n = 3000
+    x = np.sort(np.random.default_rng(8).uniform(-1.0, 1.0, n))
+    A = np.exp(-((x[:, None] - x[None, :]) / 0.1) ** 2) + np.eye(n)
+    path = tmp_path / "k.bin"
+    saveMatrixXdToBinary(A, path)
+    F = np.zeros((n, n), order="F")
+    lib = _lib.lib()
+    assert lib.hodlr_read_matrix_file(str(path).encode(), n, n,
+                                      F.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), n) == 0
+    assert np.array_equal(F, A)
+    g = HODLR_Matrix(F, 64)
+    g.set_LRTolerance(1e-10)
+    o = oracle_mod.OracleHODLR.from_dense(A, leaf=64)
+    o.set_lr(1e-10)
+    _compare_compression(g, o)
+    b = np.random.default_rng(9).standard_normal((n, 2))
+    xs, xo = g.recLU_Solve(b), o.solve(b)
+    assert np.linalg.norm(xs - xo) / np.linalg.norm(xo) <= SOLVE_TOL
+
+
 def test_reference_random_exact_hodlr():
     """Reference test shape (test/test.cpp:57-69): exact rank-10 HODLR, N=10000,
     leaf 50, relative error < 1e-8 on x = LinSpaced(-2, 2)."""
