@@ -577,12 +577,11 @@ __global__ void __launch_bounds__(MMA_NT, 2)
 
 template <int KTYPE, int DIM>
 void launch_sym_mma_dim(const KmatvecLaunch& L, int S, int tps, cudaStream_t s) {
-  // the opt-in above 48 KB of shared memory, once per instance (thread-safe
-  // static initialisation); a failure shows as the launch's error
-  static const cudaError_t attr = cudaFuncSetAttribute(
-      kmatvec_sym_mma_kernel<KTYPE, DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-      (int)MmaSmem<DIM>::BYTES);
-  (void)attr;
+  // the opt-in above 48 KB of shared memory, for the current device (set on
+  // every launch, as the attribute is per device); a failure shows as the
+  // launch's error
+  cudaFuncSetAttribute(kmatvec_sym_mma_kernel<KTYPE, DIM>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MmaSmem<DIM>::BYTES);
   const int grid = S * (S + 1) / 2;
   kmatvec_sym_mma_kernel<KTYPE, DIM><<<grid, MMA_NT, MmaSmem<DIM>::BYTES, s>>>(L, S, tps);
 }
