@@ -71,3 +71,17 @@ def test_no_cpu_fallback_without_gpu(gpu_lib):
     with pytest.raises(HODLRError) as e:
         HODLR_Matrix(64, 64, KernelSpec("gaussian", 0.1, 1.0), np.linspace(0, 1, 64)[None, :], 16)
     assert e.value.status == 2  # HODLR_ERR_CUDA
+
+
+def test_device_functor_facade_compiles(gpu_lib, tmp_path):
+    """The device-functor constructor of include/HODLR_Matrix.hpp and its test
+    program build with nvcc for sm_100a (run by the GPU suite)."""
+    import subprocess
+    exe = tmp_path / "functor_test"
+    subprocess.run(["nvcc", "-gencode", "arch=compute_100a,code=sm_100a", "-O1", "-std=c++17",
+                    os.path.join(ROOT, "tests", "cpp", "functor_test.cu"),
+                    "-I", os.path.join(ROOT, "include"),
+                    "-I", os.path.join(ROOT, "dense_hodlr_b200", "csrc"),
+                    "-L", os.path.join(ROOT, "dense_hodlr_b200"), "-lhodlr_b200",
+                    "-o", str(exe)], check=True, timeout=600)
+    assert exe.exists()
