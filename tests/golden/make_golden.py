@@ -7,7 +7,8 @@ oracle restatement after it has passed the reference's own test assertions
 
 c1_aca.npz  pivots, ranks and iteration counts of the 1D workload: N=4096
             sorted uniform points on [-1,1] (numpy default_rng seed 1),
-            K = exp(-(dx)^2/0.1^2) + 1.0*delta, leaf 64, ACA tol 1e-10.
+            K = exp(-(dx)^2/0.1^2) + 1.0*delta, leaf 64, ACA tol 1e-10;
+            and per block a hash of the exact FP64 bytes of its W and V.
 c2_blocks.npz  per block: level, size, rank, iterations, stopping margin and
             a hash of the pivot sequence, for the FP64-at-scale workload:
             N=262144 uniform [0,1]^2 (dense_hodlr_b200.points.uniform_cube,
@@ -38,6 +39,21 @@ def pivot_hash(rows, cols):
     return np.int64(h.astype(np.int64))
 
 
+def factor_hash(W, V):
+    """First 8 bytes of the SHA-256 of the FP64 bytes of W then V (column-major),
+    as a signed 64-bit integer: pins the low-rank factors bit for bit."""
+    import hashlib
+    d = hashlib.sha256(np.asfortranarray(W).tobytes(order="F")
+                       + np.asfortranarray(V).tobytes(order="F")).digest()
+    return np.frombuffer(d[:8], dtype=np.int64)[0]
+
+
+def block_shape(inner, b):
+    """(m, n) of block b: 2p is node p's top block, 2p+1 its bottom block."""
+    lv, mn, sp, mx = inner[b // 2]
+    return (sp - mn + 1, mx - sp) if b % 2 == 0 else (mx - sp, sp - mn + 1)
+
+
 def c1():
     rng = np.random.default_rng(1)
     pts = np.sort(rng.uniform(-1.0, 1.0, 4096))[None, :]
@@ -47,9 +63,12 @@ def c1():
     nb = o.num_blocks()
     prow = np.concatenate([o.pivots(b)[0] for b in range(nb)])
     pcol = np.concatenate([o.pivots(b)[1] for b in range(nb)])
+    inner = o.inner_nodes()
+    wv = np.array([factor_hash(*o.lowrank(b, *block_shape(inner, b))) for b in range(nb)],
+                  dtype=np.int64)
     out = os.path.join(HERE, "c1_aca.npz")
     np.savez_compressed(out, points=pts[0], ranks=o.ranks(), iters=o.iters(), prow=prow,
-                        pcol=pcol)
+                        pcol=pcol, wv_hash=wv)
     print(out, "blocks", nb, "pivots", len(prow))
 
 

@@ -241,6 +241,28 @@ def test_errors_are_status_codes():
         g.recLU_Solve(np.zeros((10, 1)))
 
 
+def test_golden_c1_fixture():
+    """The CUDA path against the committed C1 fixture directly (tests/golden/
+    c1_aca.npz, made by tests/golden/make_golden.py): ranks, iteration counts,
+    pivot sequences and the exact bytes of every block's W and V."""
+    import os
+    from tests.golden.make_golden import factor_hash
+    d = np.load(os.path.join(os.path.dirname(__file__), "golden", "c1_aca.npz"))
+    pts, _ = c1_points()
+    assert np.array_equal(pts[0], d["points"])
+    g = HODLR_Matrix(4096, 4096, KernelSpec("gaussian", 0.1, 1.0), pts, 64)
+    g.set_LRTolerance(1e-10)
+    g.storeLRinTree()
+    nb = g.num_blocks()
+    assert np.array_equal(g.ranks(), d["ranks"])
+    assert np.array_equal([g.block_info(b)["iters"] for b in range(nb)], d["iters"])
+    rows = np.concatenate([g.pivots(b)[0] for b in range(nb)])
+    cols = np.concatenate([g.pivots(b)[1] for b in range(nb)])
+    assert np.array_equal(rows, d["prow"]) and np.array_equal(cols, d["pcol"])
+    wv = np.array([factor_hash(*g.lowrank(b)) for b in range(nb)], dtype=np.int64)
+    assert np.array_equal(wv, d["wv_hash"])
+
+
 def test_c2_full_size_ranks_and_pivots_match_fixture():
     """The FP64-at-scale workload at full size (N=262144, 4094 blocks): every
     block's rank, iteration count and pivot-sequence hash equals the oracle's

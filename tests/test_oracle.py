@@ -282,7 +282,8 @@ def test_c1_oracle_vs_dense_lu(oracle_mod):
 
 # --------------------------------------------------------------- golden
 def test_golden_c1_pivots_and_ranks(oracle_mod):
-    """The oracle reproduces the committed C1 fixture (pivots, ranks, iters)."""
+    """The oracle reproduces the committed C1 fixture (pivots, ranks, iters and
+    the bytes of every block's W and V)."""
     g = np.load(os.path.join(GOLDEN, "c1_aca.npz"))
     pts, _ = c1_points()
     o = oracle_mod.OracleHODLR.from_kernel(pts, 0, 0.1, shift=1.0, leaf=64)
@@ -294,3 +295,7 @@ def test_golden_c1_pivots_and_ranks(oracle_mod):
     cols = np.concatenate([o.pivots(b)[1] for b in range(o.num_blocks())])
     assert np.array_equal(rows, g["prow"]) and np.array_equal(cols, g["pcol"])
     assert np.array_equal(pts[0], g["points"])
+    from tests.golden.make_golden import block_shape, factor_hash
+    inner = o.inner_nodes()
+    wv = [factor_hash(*o.lowrank(b, *block_shape(inner, b))) for b in range(o.num_blocks())]
+    assert np.array_equal(np.array(wv, dtype=np.int64), g["wv_hash"])
