@@ -94,6 +94,23 @@ def test_uneven_2d_matern(oracle_mod):
     assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= SOLVE_TOL
 
 
+@pytest.mark.parametrize("kind,dim,n,l,shift,replace,value", [
+    ("exponential", 2, 6000, 0.3, 0.5, False, 0.0),
+    ("inv_multiquadric", 3, 5000, 0.5, 0.0, True, 2.0),
+    ("quadratic", 1, 4000, 1.0, 0.0, True, 0.0),  # the reference's kernel test shape: K_ii = 0
+])
+def test_other_kernel_families_bit_exact(oracle_mod, kind, dim, n, l, shift, replace, value):
+    """The remaining closed-form kernels through ACA and the solve: pivots,
+    ranks and W/V bit for bit against the oracle, solutions within 1e-10."""
+    pts = uniform_cube(n, dim, 40 + dim)
+    g, o = _pair(oracle_mod, pts, kind, l, shift, 64, 1e-8, replace, value)
+    _compare_compression(g, o)
+    b = np.random.default_rng(n).standard_normal((n, 2))
+    x = g.recLU_Solve(b)
+    xo = o.solve(b)
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= SOLVE_TOL
+
+
 def test_3d_gaussian_group_levels(oracle_mod):
     """3D Gaussian, leaf 128: top levels run with many CTAs per block."""
     pts = uniform_cube(16384, 3, 5)
