@@ -229,6 +229,31 @@ def test_aca_matches_python_restatement(oracle_mod):
             assert np.array_equal(Wo, np.array(W).T) and np.array_equal(Vo, np.array(V).T)
 
 
+def test_aca_min_pivot_matches_python_restatement(oracle_mod):
+    """The skip-row path (src/lowRank.cpp:187-195) and the pivot fallbacks with
+    minPivot > 0: dense 10 * Gaussian + I, minPivot 2.5 (truncated to 2 as the
+    reference passes it to an int), against the Python restatement."""
+    rng = np.random.default_rng(22)
+    x = np.sort(rng.uniform(-1.0, 1.0, 256))
+    A = 10.0 * np.exp(-((x[:, None] - x[None, :]) / 0.1) ** 2) + np.eye(256)
+    o = oracle_mod.OracleHODLR.from_dense(A, leaf=32)
+    o.set_lr(1e-10, 2.5)
+    o.compress(1)
+    inner = o.inner_nodes()
+    skipped = 0
+    for b in range(o.num_blocks()):
+        lvl, mn, sp, mx = inner[b // 2]
+        r0, c0, m, n = (mn, sp + 1, sp - mn + 1, mx - sp) if b % 2 == 0 else (sp + 1, mn, mx - sp, sp - mn + 1)
+        k, prow, pcol, W, V = py_aca(lambda i, j: A[r0 + i, c0 + j], m, n, 1e-10, min_pivot=2)
+        rows, cols = o.pivots(b)
+        assert list(rows) == prow and list(cols) == pcol, b
+        skipped += o.iters()[b] - k
+        if 0 < k < min(m, n) - 1:
+            Wo, Vo = o.lowrank(b, m, n)
+            assert np.array_equal(Wo, np.array(W).T) and np.array_equal(Vo, np.array(V).T)
+    assert skipped > 0  # the path under test ran
+
+
 # -------------------------------------------------------- reference tests
 def test_reference_random_exact_hodlr(oracle_mod):
     """test/test.cpp:57-69: exact rank-10 HODLR N=10000 leaf 50, rel. err < 1e-8."""
