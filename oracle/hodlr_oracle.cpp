@@ -121,10 +121,14 @@ struct Node {
   int level, min, split, max;  // split == last row of the top half
   int left = -1, right = -1;   // child indices: >= 0 inner node, < 0 leaf (-1-id)
   bool leaf;
+  // ACA rank bounds of the top and bottom blocks (user_IndexTree::node,
+  // include/user_IndexTree.hpp:14-17); -1: none
+  int tmin = -1, bmin = -1, tmax = -1, bmax = -1;
 };
 
 struct Block {  // one off-diagonal block and its ACA result
   int r0 = 0, c0 = 0, m = 0, n = 0;
+  int minRank = -1, maxRank = -1;  // the node's bounds for this block
   int rank = 0, iters = 0;
   Mat W, V;
   std::vector<int> prow, pcol;
@@ -293,9 +297,12 @@ void default_children(Oracle& o, int id, std::vector<std::vector<int>>& lv, std:
 // the leaf size with no user split is a leaf; otherwise it splits at the user
 // split; without user children both children follow the default rules, the
 // right one split at split + floor(s/2) (src/HODLR_Tree.cpp:300-303).
-bool user_tree(Oracle& o, const int* usplit, const int* uleft, const int* uright, int nn,
-               int level, int mn, int mx, int u, std::vector<char>& seen,
-               std::vector<std::vector<int>>& lv, std::vector<int>& lo) {
+// A user inner node carries its rank bounds (src/HODLR_Tree.cpp:241-244; ub:
+// top min, bottom min, top max, bottom max per user node, or null).
+bool user_tree(Oracle& o, const int* usplit, const int* uleft, const int* uright,
+               const int* const* ub, int nn, int level, int mn, int mx, int u,
+               std::vector<char>& seen, std::vector<std::vector<int>>& lv,
+               std::vector<int>& lo) {
   if (u < 0 || u >= nn || seen[u]) return false;
   seen[u] = 1;
   if (level > o.numLevels - 1) o.numLevels = level + 1;
@@ -315,6 +322,12 @@ bool user_tree(Oracle& o, const int* usplit, const int* uleft, const int* uright
   if (sp < mn || sp >= mx) return false;
   nd.leaf = false;
   nd.split = sp;
+  if (ub) {
+    nd.tmin = ub[0][u];
+    nd.bmin = ub[1][u];
+    nd.tmax = ub[2][u];
+    nd.bmax = ub[3][u];
+  }
   o.nodes.push_back(nd);
   if ((int)lv.size() <= level) lv.resize(level + 1);
   lv[level].push_back(id);
@@ -349,9 +362,10 @@ bool user_tree(Oracle& o, const int* usplit, const int* uleft, const int* uright
   }
   if (l < 0 || r < 0) return false;
   o.nodes[id].left = (int)o.nodes.size();
-  if (!user_tree(o, usplit, uleft, uright, nn, level + 1, mn, sp, l, seen, lv, lo)) return false;
+  if (!user_tree(o, usplit, uleft, uright, ub, nn, level + 1, mn, sp, l, seen, lv, lo))
+    return false;
   o.nodes[id].right = (int)o.nodes.size();
-  return user_tree(o, usplit, uleft, uright, nn, level + 1, sp + 1, mx, r, seen, lv, lo);
+  return user_tree(o, usplit, uleft, uright, ub, nn, level + 1, sp + 1, mx, r, seen, lv, lo);
 }
 
 // Level order, positions and the off-diagonal blocks of a built tree.
@@ -373,11 +387,15 @@ void finish_tree(Oracle& o, const std::vector<std::vector<int>>& levelVec,
     t.c0 = nd.split + 1;
     t.m = nd.split - nd.min + 1;
     t.n = nd.max - nd.split;
+    t.minRank = nd.tmin;
+    t.maxRank = nd.tmax;
     Block& b = o.blocks[2 * p + 1];
     b.r0 = nd.split + 1;
     b.c0 = nd.min;
     b.m = nd.max - nd.split;
     b.n = nd.split - nd.min + 1;
+    b.minRank = nd.bmin;
+    b.maxRank = nd.bmax;
   }
 }
 
@@ -565,7 +583,8 @@ void compress(Oracle& o, int nthreads) {
     return (int64_t)o.blocks[a].m * o.blocks[a].n > (int64_t)o.blocks[b].m * o.blocks[b].n;
   });
   parallel_for((int)order.size(), nthreads, [&](int t) {
-    aca(o, o.blocks[order[t]], o.tol, -1, -1, o.minPivot);
+    Block& B = o.blocks[order[t]];
+    aca(o, B, o.tol, B.minRank, B.maxRank, o.minPivot);
   });
   o.leafMat.assign(o.leaves.size(), Mat());
   parallel_for((int)o.leaves.size(), nthreads, [&](int p) {
@@ -719,20 +738,30 @@ void orc_destroy(void* h) { delete (Oracle*)h; }
 
 // User index tree (nodes in pre-order, node 0 the root); 0 = ok, 1 = invalid
 // (the default tree is kept).
-int orc_set_user_tree(void* h, int nn, const int* split, const int* left, const int* right) {
+// userTree_To_HODLRTree with the user nodes' rank bounds (each of tmin, bmin,
+// tmax, bmax: nn values, -1 for none; all four null: no bounds).
+int orc_set_user_tree_bounds(void* h, int nn, const int* split, const int* left,
+                             const int* right, const int* tmin, const int* bmin,
+                             const int* tmax, const int* bmax) {
   Oracle& o = *(Oracle*)h;
   o.nodes.clear();
   o.numLevels = 1;
   std::vector<std::vector<int>> lv;
   std::vector<int> lo;
   std::vector<char> seen((size_t)std::max(nn, 1), 0);
-  if (nn < 1 || !user_tree(o, split, left, right, nn, 0, 0, o.n - 1, 0, seen, lv, lo)) {
+  const int* ubv[4] = {tmin, bmin, tmax, bmax};
+  const int* const* ub = (tmin && bmin && tmax && bmax) ? ubv : nullptr;
+  if (nn < 1 || !user_tree(o, split, left, right, ub, nn, 0, 0, o.n - 1, 0, seen, lv, lo)) {
     build_tree(o);
     return 1;
   }
   finish_tree(o, lv, lo);
   o.compressed = o.factored = false;
   return 0;
+}
+
+int orc_set_user_tree(void* h, int nn, const int* split, const int* left, const int* right) {
+  return orc_set_user_tree_bounds(h, nn, split, left, right, nullptr, nullptr, nullptr, nullptr);
 }
 
 void orc_set_lr(void* h, double tol, double minPivot) {

@@ -39,6 +39,8 @@ def lib():
         L.orc_destroy.argtypes = [ctypes.c_void_p]
         L.orc_set_user_tree.argtypes = [ctypes.c_void_p, ctypes.c_int, _ip, _ip, _ip]
         L.orc_set_user_tree.restype = ctypes.c_int
+        L.orc_set_user_tree_bounds.argtypes = [ctypes.c_void_p, ctypes.c_int] + [_ip] * 7
+        L.orc_set_user_tree_bounds.restype = ctypes.c_int
         L.orc_set_lr.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double]
         L.orc_compress.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.orc_factorize.argtypes = [ctypes.c_void_p]
@@ -108,10 +110,17 @@ class OracleHODLR:
             lib().orc_destroy(self.h)
             self.h = None
 
-    def set_user_tree(self, split, left, right):
-        """User index tree in pre-order; returns 0, or 1 if invalid."""
+    def set_user_tree(self, split, left, right, bounds=None):
+        """User index tree in pre-order; returns 0, or 1 if invalid.  bounds:
+        (top min, bottom min, top max, bottom max) rank bounds per user node
+        (user_IndexTree::node, -1 for none), or None."""
         a = [np.ascontiguousarray(v, dtype=np.int32) for v in (split, left, right)]
-        return lib().orc_set_user_tree(self.h, len(a[0]), *[x.ctypes.data_as(_ip) for x in a])
+        if bounds is None:
+            return lib().orc_set_user_tree(self.h, len(a[0]), *[x.ctypes.data_as(_ip) for x in a])
+        b = [np.ascontiguousarray(v, dtype=np.int32) for v in bounds]
+        assert len(b) == 4 and all(len(v) == len(a[0]) for v in b)
+        return lib().orc_set_user_tree_bounds(self.h, len(a[0]),
+                                              *[x.ctypes.data_as(_ip) for x in a + b])
 
     def set_lr(self, tol, min_pivot=0.0):
         lib().orc_set_lr(self.h, float(tol), float(min_pivot))

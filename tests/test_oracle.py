@@ -140,14 +140,17 @@ def test_tree_matches_reference_rules(oracle_mod, n, leaf):
 
 
 # ------------------------------------------------------------------ ACA
-def py_aca(entry, m, n, tol, min_pivot=0):
+def py_aca(entry, m, n, tol, min_pivot=0, min_rank=-1, max_rank=-1):
     """partialPivACA_LowRankApprox (src/lowRank.cpp:117-279) restated in plain
-    Python floats (IEEE double, unfused), independent of the C oracle."""
+    Python floats (IEEE double, unfused), independent of the C oracle; with
+    its minRank / maxRank arguments (maxRank 0: zero factors, :120-125)."""
     ub = min(m, n)
     W, V, prow, pcol = [], [], [], []
+    if max_rank == 0:
+        return 0, prow, pcol, W, V
     chR, chC = [False] * m, [False] * n
     frob2, eps, cur, k = 0.0, 1.0, 0, 0
-    while eps > tol and k < ub:
+    while (eps > tol or k < min_rank) and k < ub:
         chR[cur] = True
         s = [0.0] * n
         for l in range(k):
@@ -207,6 +210,8 @@ def py_aca(entry, m, n, tol, min_pivot=0):
         eps = math.sqrt(sw) * math.sqrt(sv) / math.sqrt(frob2)
         cur = nr
         k += 1
+        if k == max_rank:
+            break
     return k, prow, pcol, W, V
 
 

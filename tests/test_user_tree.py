@@ -24,6 +24,49 @@ def test_oracle_user_tree_shape(oracle_mod):
     assert o.set_user_tree([999, 499], [1, -1], [-1, -1]) == 1  # one child only
 
 
+def test_oracle_user_tree_rank_bounds(oracle_mod):
+    """Per-node ACA rank bounds of a user tree (user_IndexTree::node
+    topOffDiag_minRank ... bottOffDiag_maxRank, copied to the HODLR node at
+    src/HODLR_Tree.cpp:241-244 and passed to ACA at src/HODLR_Matrix.cpp:330-331):
+    each bounded block against the Python ACA restatement with those bounds;
+    the default subtrees keep no bounds."""
+    from tests.test_oracle import py_aca
+    pts = uniform_cube(800, 2, 4)
+    o = oracle_mod.OracleHODLR.from_kernel(pts, 1, 0.2, shift=1e-2, leaf=64)
+    o.set_lr(1e-8)
+    tree = ([399, 199, 599], [1, -1, -1], [2, -1, -1])
+    # per user node: top min, bottom min, top max, bottom max (unbounded ranks of the
+    # six blocks are 109, 103, 63, 59, 60, 57)
+    bounds = ([-1, -1, 75], [120, -1, -1], [5, 0, -1], [-1, -1, 3])
+    assert o.set_user_tree(*tree, bounds=bounds) == 0
+    o.compress(1)
+    inner = o.inner_nodes()
+    assert inner[:3] == [(0, 0, 399, 799), (1, 0, 199, 399), (1, 400, 599, 799)]
+    ranks = o.ranks()
+    for p, (tmin, bmin, tmax, bmax) in enumerate(zip(*bounds)):
+        lvl, mn, sp, mx = inner[p]
+        for b, lo, hi in ((2 * p, tmin, tmax), (2 * p + 1, bmin, bmax)):
+            r0, c0, m, n = (mn, sp + 1, sp - mn + 1, mx - sp) if b % 2 == 0 else (sp + 1, mn, mx - sp, sp - mn + 1)
+            k, prow, pcol, W, V = py_aca(lambda i, j: o.entry(r0 + i, c0 + j), m, n, 1e-8,
+                                         min_rank=lo, max_rank=hi)
+            rows, cols = o.pivots(b)
+            assert list(rows) == prow and list(cols) == pcol, b
+            assert ranks[b] == (1 if k == 0 else k), b
+            if k > 0:
+                Wo, Vo = o.lowrank(b, m, n)
+                assert np.array_equal(Wo, np.array(W).T) and np.array_equal(Vo, np.array(V).T)
+    assert ranks[0] == 5 and ranks[1] >= 120 and ranks[2] == 1 and ranks[4] >= 75
+    assert ranks[5] == 3
+    # the same tree without bounds: the bounded blocks change, the rest do not
+    o2 = oracle_mod.OracleHODLR.from_kernel(pts, 1, 0.2, shift=1e-2, leaf=64)
+    o2.set_lr(1e-8)
+    assert o2.set_user_tree(*tree) == 0
+    o2.compress(1)
+    r2 = o2.ranks()
+    assert r2[0] > 5 and r2[1] < 120 and r2[4] < 75
+    assert np.array_equal(ranks[6:], r2[6:])
+
+
 @pytest.mark.gpu
 def test_user_tree_matches_oracle(oracle_mod):
     from dense_hodlr_b200 import HODLR_Matrix, HODLRError, KernelSpec
