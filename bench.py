@@ -580,61 +580,97 @@ def run_profile_case(case):
         g.solve_device(b_d.data_ptr(), x_d.data_ptr(), NRHS)
         print(json.dumps({"case": case, "factor_s": g.get_recLU_FactorizationTime(),
                           "solve_s": g.get_recLU_SolveTime()}))
-    elif case.startswith("c3"):
-        print(json.dumps(run_c3(case)))
+    elif case.split(":")[0] in SCALE_CONFIGS:
+        print(json.dumps(run_scale(case)))
     elif case.startswith("batched"):
         print(json.dumps(run_batched(case)))
     else:
         raise SystemExit(f"unknown case {case}")
 
 
-def run_c3(case):
-    """The mixed-precision configuration at a reduced size, case 'c3[:N]'
-    (default N = 131072; its 2^20 size needs O(N K^2) = terabytes of ACA panel
-    traffic at the top level): N points uniform in [0,1]^3, k-d ordered,
-    Gaussian exp(-r^2/0.3^2) + 0.1 on the diagonal, leaf 128, ACA tol 1e-8,
-    16 right-hand sides, GMRES on the FP64 residual to 1e-10, with the
-    Woodbury products in FP64, TF32, BF16 and 3xTF32."""
+# The two 2^20-point configurations: (points, kernel, length scale, shift,
+# leaf, ACA tolerance, right-hand sides).
+SCALE_CONFIGS = {
+    # mixed precision with refinement: 3D uniform cube, Gaussian
+    "c3": dict(cloud="cube", kernel="gaussian", l=0.3, shift=0.1, leaf=128, tol=1e-8, nrhs=16),
+    # the end-to-end target: unit sphere, Matern-3/2, ACA tol 1e-10
+    "c5": dict(cloud="sphere", kernel="matern32", l=0.1, shift=1e-2, leaf=128, tol=1e-10,
+               nrhs=1),
+}
+
+
+def scale_points(cloud, n, seed=SEED):
+    from dense_hodlr_b200.points import uniform_cube, unit_sphere
+    return uniform_cube(n, 3, seed) if cloud == "cube" else unit_sphere(n, seed)
+
+
+def run_scale(case):
+    """One of the 2^20-point configurations, case '<c3|c5>[:N[:prec,prec,...]]'
+    (default N = 2^20, precisions fp64 then tf32x3,tf32,bf16): compression
+    once (FP64 ACA), then per precision of the Woodbury products the
+    factorization, a direct solve and HODLR-preconditioned GMRES on the FP64
+    full-kernel residual to 1e-10.  One JSON line per phase (flushed), so a
+    run cut short still reports what it finished."""
     import torch
-    from dense_hodlr_b200 import HODLR_Matrix, KernelSpec, _lib
-    from dense_hodlr_b200.points import uniform_cube
+    from dense_hodlr_b200 import HODLR_Matrix, KernelSpec
     parts = case.split(":")
-    n = int(parts[1]) if len(parts) > 1 else 131072
-    nrhs = 16
-    pts = uniform_cube(n, 3, SEED)
+    cfg = SCALE_CONFIGS[parts[0]]
+    n = int(parts[1]) if len(parts) > 1 and parts[1] else 1 << 20
+    precs = parts[2].split(",") if len(parts) > 2 else ["fp64", "tf32x3", "tf32", "bf16"]
+    nrhs = cfg["nrhs"]
+
+    def emit(d):
+        free, total = torch.cuda.mem_get_info()
+        d["device_used_gb"] = round((total - free) / 1e9, 2)
+        print(json.dumps(d), flush=True)
+
+    pts = scale_points(cfg["cloud"], n)
     b = np.random.default_rng(SEED + 1).standard_normal((n, nrhs))
     b_d = torch.from_numpy(np.ascontiguousarray(b.T)).cuda()
     x_d = torch.empty_like(b_d)
-    g = HODLR_Matrix(n, n, KernelSpec("gaussian", 0.3, 0.1), pts, 128)
-    g.set_LRTolerance(1e-8)
-    lib = _lib.lib()
+    g = HODLR_Matrix(n, n, KernelSpec(cfg["kernel"], cfg["l"], cfg["shift"]), pts, cfg["leaf"])
+    g.set_LRTolerance(cfg["tol"])
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     g.storeLRinTree()
-    out = {"case": "c3", "n": n, "nrhs": nrhs, "lr_s": g.get_LR_ComputationTime(),
-           "max_rank": int(g.ranks().max()), "runs": {}}
+    lr_wall = time.perf_counter() - t0
+    blocks = gather_blocks(g)
+    nlev = max(bk["level"] for bk in blocks) + 1
+    st = g.aca_stats()
+    emit({"case": parts[0], "n": n, "nrhs": nrhs, "phase": "compress",
+          "lr_s": g.get_LR_ComputationTime(), "lr_wall_s": lr_wall, "aca": st,
+          "aca_gbs": st["bytes"] / max(st["seconds"], 1e-12) / 1e9,
+          "kmax_per_level": [max(bk["rank"] for bk in blocks if bk["level"] == lv)
+                             for lv in range(nlev)],
+          "iters_max_per_level": [max(bk["iters"] for bk in blocks if bk["level"] == lv)
+                                  for lv in range(nlev)]})
     x64 = None
-    for prec in ("fp64", "tf32", "bf16", "tf32x3", "fp64"):
+    for prec in precs:
         g.set_precision(prec)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         g.recLU_Compute()
         tf = g.get_recLU_FactorizationTime()
         g.solve_device(b_d.data_ptr(), x_d.data_ptr(), nrhs)
+        ts = g.get_recLU_SolveTime()
         xd = x_d.cpu().numpy().T.copy()
+        if prec == "fp64" and x64 is None:
+            x64 = xd
+        emit({"case": parts[0], "n": n, "precision": prec, "phase": "factor",
+              "factor_s": tf, "direct_solve_s": ts})
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
         it, rel = g.iterative_solve_device(b_d.data_ptr(), x_d.data_ptr(), nrhs, tol=1e-10,
                                            max_iter=60, restart=32)
         torch.cuda.synchronize()
-        total = time.perf_counter() - t0
-        if prec == "fp64" and x64 is None:
-            x64 = xd
-        out["runs"][prec] = {"factor_s": tf, "gmres_s": g.get_recLU_SolveTime(),
-                             "factor_solve_s": total, "gmres_iterations": int(it),
-                             "rel_residual": float(rel.max()),
-                             "direct_solve_rel_diff_vs_fp64": float(
-                                 np.linalg.norm(xd - x64) / np.linalg.norm(x64))}
-        print(json.dumps({prec: out["runs"][prec]}), flush=True)
-    return out
+        t_gm = time.perf_counter() - t1
+        emit({"case": parts[0], "n": n, "precision": prec, "phase": "gmres",
+              "gmres_s": t_gm, "gmres_iterations": int(it), "rel_residual": float(rel.max()),
+              "factor_plus_gmres_s": time.perf_counter() - t0,
+              "direct_solve_rel_diff_vs_fp64": (float(np.linalg.norm(xd - x64) /
+                                                      np.linalg.norm(x64))
+                                                if x64 is not None else None)})
+    return {"case": parts[0], "n": n, "done": True}
 
 
 def batched_systems(nsys, seed=SEED):

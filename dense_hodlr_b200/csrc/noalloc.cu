@@ -1,13 +1,15 @@
 // Full-kernel product Y = K X that allocates no device memory.
 //
-// Some callers cannot call cudaMalloc at the point where they need K x: code
-// running while a stream is being captured into a CUDA graph (allocation is
-// not a stream operation and is refused during capture), and applications
-// whose memory manager has reserved all device memory up front (a framework's
-// caching allocator, a fixed real-time budget).  A HODLR handle allocates on
-// creation, so they cannot use hodlr_kernel_matvec_device.  This entry point
-// takes the points, X and Y as caller-owned device buffers and keeps its only
-// scratch -- the partial sums of the column splits of kmatvec.cu -- in the
+// Some callers cannot call cudaMalloc when they need K x.  An application
+// whose memory manager has reserved the device memory up front (a caching
+// allocator that holds the GPU, a fixed budget set at start-up) would see a
+// new allocation fail or push it over its budget.  A plugin hosted by such a
+// framework is often not allowed to allocate behind the framework's back.
+// And latency-bound code avoids cudaMalloc/cudaFree because they can
+// synchronise the device.  A HODLR handle allocates on creation, so these
+// callers cannot use hodlr_kernel_matvec_device.  This entry point takes the
+// points, X and Y as caller-owned device buffers and keeps its only scratch
+// -- the partial sums of the column splits of kmatvec.cu -- in the
 // file-scope array below, which every GPU that loads the library holds until
 // the process exits.
 #include <mutex>
@@ -18,10 +20,10 @@
 
 namespace {
 
-constexpr int kNoallocSplits = 4;  // column splits at most; partials = splits * n * nrhs
-
-// Shared by every call on a device; holds the last call's partial sums.
-static __device__ __align__(256) double g_noalloc_scratch[kNoallocSplits * HODLR_NOALLOC_MAX_ELEMS];
+// Shared by every call on a device; holds the last call's partial sums
+// (HODLR_NOALLOC_SPLITS column splits at most, splits * n * nrhs doubles).
+static __device__ __align__(256) double
+    g_noalloc_scratch[HODLR_NOALLOC_SPLITS * HODLR_NOALLOC_MAX_ELEMS];
 
 constexpr int kMaxDevices = 64;
 double* g_scratch_addr[kMaxDevices] = {nullptr};
@@ -53,6 +55,10 @@ extern "C" int hodlr_kernel_matvec_noalloc(int n, int dim, const double* d_pts,
     return HODLR_ERR_ARG;
   if (kernel->type < 0 || kernel->type > 4 || !(kernel->length_scale > 0)) return HODLR_ERR_ARG;
   if ((int64_t)n * nrhs > HODLR_NOALLOC_MAX_ELEMS) return HODLR_ERR_ARG;  // scratch limit
+  // An error left pending by the caller's earlier CUDA work would be read
+  // (and cleared) by the launch check below and reported as this call's:
+  // leave it pending for its owner and launch nothing.
+  if (cudaPeekAtLastError() != cudaSuccess) return HODLR_ERR_STATE;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return HODLR_ERR_CUDA;
   double* scratch = nullptr;
@@ -61,7 +67,7 @@ extern "C" int hodlr_kernel_matvec_noalloc(int n, int dim, const double* d_pts,
   if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
     return HODLR_ERR_CUDA;
   int nsplit = kmatvec_splits(n, sms);
-  if (nsplit > kNoallocSplits) nsplit = kNoallocSplits;
+  if (nsplit > HODLR_NOALLOC_SPLITS) nsplit = HODLR_NOALLOC_SPLITS;
   KmatvecLaunch L;
   L.src.pts = d_pts;
   L.src.A = nullptr;

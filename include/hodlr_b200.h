@@ -315,21 +315,26 @@ int hodlr_write_matrix_file(const char* path, int rows, int cols, const double* 
 
 /* Full-kernel FP64 product d_y = K d_x that allocates no device memory.  It
  * has no counterpart in the reference.  It is for callers that cannot call
- * cudaMalloc when they need K x: code running while a stream is captured into
- * a CUDA graph, and applications whose memory manager has already reserved
- * the device memory.  Such callers cannot create a handle (handles allocate),
- * so this call takes the points (d_pts, dim x n, SoA, device memory), X and
- * Y as caller-owned device buffers and runs on `stream` (NULL: the default
- * stream), returning after the stream has finished the product.  Its scratch
- * is a file-scope device array of HODLR_NOALLOC_SPLITS * HODLR_NOALLOC_MAX_ELEMS
- * doubles (16 MiB) that every GPU loading the library holds until exit; hence
- * the limit n * nrhs <= HODLR_NOALLOC_MAX_ELEMS, beyond which the call
- * returns HODLR_ERR_ARG without launching.  The first call on a device looks
- * up the array's device address (cudaGetSymbolAddress, with that device
- * current): make that first call before any stream capture begins.  All calls
- * share the array and it keeps the last call's contents (nothing in it needs
- * to start at zero); calls whose kernels overlap on the GPU race on it, so
- * issue them on one stream or serialise them. */
+ * cudaMalloc when they need K x: applications whose memory manager has
+ * already reserved the device memory (a new allocation would fail or break
+ * their budget), plugins that must not allocate behind their host
+ * framework's allocator, and latency-bound code that avoids cudaMalloc
+ * because it can synchronise the device.  Such callers cannot create a
+ * handle (handles allocate), so this call takes the points (d_pts, dim x n,
+ * SoA, device memory), X and Y as caller-owned device buffers, runs on
+ * `stream` (NULL: the default stream) and returns after synchronising that
+ * stream.  Its scratch is a file-scope device array of
+ * HODLR_NOALLOC_SPLITS * HODLR_NOALLOC_MAX_ELEMS doubles (16 MiB) that every
+ * GPU loading the library holds until exit; hence the limit
+ * n * nrhs <= HODLR_NOALLOC_MAX_ELEMS, beyond which the call returns
+ * HODLR_ERR_ARG without launching.  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress, with that device current):
+ * make that first call before any stream capture begins.  All calls share
+ * the array and it keeps the last call's contents (nothing in it needs to
+ * start at zero); calls whose kernels overlap on the GPU race on it, so
+ * issue them on one stream or serialise them.  A CUDA error already pending
+ * from the caller's earlier work is left pending and the call returns
+ * HODLR_ERR_STATE without launching. */
 #define HODLR_NOALLOC_SPLITS 4
 #define HODLR_NOALLOC_MAX_ELEMS 524288
 int hodlr_kernel_matvec_noalloc(int n, int dim, const double* d_pts,

@@ -95,15 +95,38 @@ struct LU {
   }
 };
 
-// C = A^T B
+// C = A^T B.  Every C(i, j) is summed over k in order; four of them are
+// accumulated side by side (independent chains, the same sums).
 Mat matTmul(const Mat& A, const Mat& B) {
   Mat C(A.c, B.c);
-  for (int j = 0; j < B.c; ++j)
-    for (int i = 0; i < A.c; ++i) {
+  const int K = A.r;
+  for (int j = 0; j < B.c; ++j) {
+    const double* b = &B.a[(size_t)j * B.r];
+    int i = 0;
+    for (; i + 4 <= A.c; i += 4) {
+      const double* a0 = &A.a[(size_t)i * K];
+      const double* a1 = a0 + K;
+      const double* a2 = a1 + K;
+      const double* a3 = a2 + K;
+      double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+      for (int k = 0; k < K; ++k) {
+        const double bk = b[k];
+        s0 = s0 + a0[k] * bk;
+        s1 = s1 + a1[k] * bk;
+        s2 = s2 + a2[k] * bk;
+        s3 = s3 + a3[k] * bk;
+      }
+      C(i, j) = s0;
+      C(i + 1, j) = s1;
+      C(i + 2, j) = s2;
+      C(i + 3, j) = s3;
+    }
+    for (; i < A.c; ++i) {
       double s = 0.0;
-      for (int k = 0; k < A.r; ++k) s = s + A(k, i) * B(k, j);
+      for (int k = 0; k < K; ++k) s = s + A(k, i) * b[k];
       C(i, j) = s;
     }
+  }
   return C;
 }
 // C = A B
@@ -598,8 +621,11 @@ void compress(Oracle& o, int nthreads) {
   o.compressed = true;
 }
 
-// recLU_Factorize(rhs, node) (src/HODLR_Matrix.cpp:612-692)
-Mat rec_factor(Oracle& o, const Mat& rhs, int id) {
+// recLU_Factorize(rhs, node) (src/HODLR_Matrix.cpp:612-692).  The two
+// child recursions touch disjoint nodes and rows, so with spawn > 1 the top
+// child runs on a thread of its own (spawn halves per level): the results
+// are those of the sequential recursion, bit for bit.
+Mat rec_factor(Oracle& o, const Mat& rhs, int id, int spawn = 1) {
   const Node& nd = o.nodes[id];
   if (nd.leaf) {
     int p = o.leaf_pos[id];
@@ -616,13 +642,20 @@ Mat rec_factor(Oracle& o, const Mat& rhs, int id) {
     for (int i = 0; i < st; ++i) topRHS(i, j) = rhs(i, j);
   for (int j = 0; j < kt; ++j)
     for (int i = 0; i < st; ++i) topRHS(i, c + j) = T.W(i, j);
-  Mat Xt = rec_factor(o, topRHS, nd.left);
   Mat bottRHS(sb, c + kb);
   for (int j = 0; j < c; ++j)
     for (int i = 0; i < sb; ++i) bottRHS(i, j) = rhs(st + i, j);
   for (int j = 0; j < kb; ++j)
     for (int i = 0; i < sb; ++i) bottRHS(i, c + j) = Bt.W(i, j);
-  Mat Xb = rec_factor(o, bottRHS, nd.right);
+  Mat Xt, Xb;
+  if (spawn > 1) {
+    std::thread tt([&]() { Xt = rec_factor(o, topRHS, nd.left, spawn / 2); });
+    Xb = rec_factor(o, bottRHS, nd.right, spawn - spawn / 2);
+    tt.join();
+  } else {
+    Xt = rec_factor(o, topRHS, nd.left);
+    Xb = rec_factor(o, bottRHS, nd.right);
+  }
   Mat XtP(st, c), XbP(sb, c), tS(st, kt), bS(sb, kb);
   for (int j = 0; j < c; ++j)
     for (int i = 0; i < st; ++i) XtP(i, j) = Xt(i, j);
@@ -667,8 +700,9 @@ Mat rec_factor(Oracle& o, const Mat& rhs, int id) {
   return res;
 }
 
-// recLU_Solve(rhs, node) (src/HODLR_Matrix.cpp:694-755)
-Mat rec_solve(const Oracle& o, const Mat& rhs, int id) {
+// recLU_Solve(rhs, node) (src/HODLR_Matrix.cpp:694-755); spawn as in
+// rec_factor.
+Mat rec_solve(const Oracle& o, const Mat& rhs, int id, int spawn = 1) {
   const Node& nd = o.nodes[id];
   if (nd.leaf) return o.leafLU[o.leaf_pos[id]].solve(rhs);
   int p = o.inner_pos[id];
@@ -680,8 +714,15 @@ Mat rec_solve(const Oracle& o, const Mat& rhs, int id) {
     for (int i = 0; i < st; ++i) rt_(i, j) = rhs(i, j);
     for (int i = 0; i < sb; ++i) rb_(i, j) = rhs(st + i, j);
   }
-  Mat xt = rec_solve(o, rt_, nd.left);
-  Mat xb = rec_solve(o, rb_, nd.right);
+  Mat xt, xb;
+  if (spawn > 1) {
+    std::thread tt([&]() { xt = rec_solve(o, rt_, nd.left, spawn / 2); });
+    xb = rec_solve(o, rb_, nd.right, spawn - spawn / 2);
+    tt.join();
+  } else {
+    xt = rec_solve(o, rt_, nd.left);
+    xb = rec_solve(o, rb_, nd.right);
+  }
   int rt = T.rank, rb = Bt.rank, sd = rt + rb;
   Mat top = matTmul(Bt.V, xt), bot = matTmul(T.V, xb);
   Mat Z(sd, c);
@@ -776,7 +817,7 @@ int orc_compress(void* h, int nthreads) {
   return 0;
 }
 
-int orc_factorize(void* h) {
+int orc_factorize_mt(void* h, int nthreads) {
   Oracle* o = (Oracle*)h;
   if (!o->compressed) compress(*o, 1);
   o->leafLU.assign(o->leaves.size(), LU());
@@ -787,7 +828,7 @@ int orc_factorize(void* h) {
   Mat dummy(o->n, 1);
   for (int i = 0; i < o->n; ++i)
     dummy(i, 0) = o->n > 1 ? -2.0 + 4.0 * i / (o->n - 1) : -2.0;
-  rec_factor(*o, dummy, 0);
+  rec_factor(*o, dummy, 0, std::max(1, nthreads));
   o->factored = true;
   int nz = 0;
   for (auto& l : o->leafLU) nz += l.nzero;
@@ -795,14 +836,20 @@ int orc_factorize(void* h) {
   return nz;
 }
 
-int orc_solve(void* h, int nrhs, const double* b, double* x) {
+int orc_factorize(void* h) { return orc_factorize_mt(h, 1); }
+
+int orc_solve_mt(void* h, int nrhs, const double* b, double* x, int nthreads) {
   Oracle* o = (Oracle*)h;
-  if (!o->factored) orc_factorize(h);
+  if (!o->factored) orc_factorize_mt(h, nthreads);
   Mat B(o->n, nrhs);
   std::memcpy(B.a.data(), b, sizeof(double) * (size_t)o->n * nrhs);
-  Mat X = rec_solve(*o, B, 0);
+  Mat X = rec_solve(*o, B, 0, std::max(1, nthreads));
   std::memcpy(x, X.a.data(), sizeof(double) * (size_t)o->n * nrhs);
   return 0;
+}
+
+int orc_solve(void* h, int nrhs, const double* b, double* x) {
+  return orc_solve_mt(h, nrhs, b, x, 1);
 }
 
 int orc_num_levels(void* h) { return ((Oracle*)h)->numLevels; }

@@ -44,7 +44,9 @@ def lib():
         L.orc_set_lr.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double]
         L.orc_compress.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.orc_factorize.argtypes = [ctypes.c_void_p]
+        L.orc_factorize_mt.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.orc_solve.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp]
+        L.orc_solve_mt.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp, ctypes.c_int]
         for f in ("orc_num_levels", "orc_num_inner", "orc_num_leaves"):
             getattr(L, f).argtypes = [ctypes.c_void_p]
         L.orc_inner_info.argtypes = [ctypes.c_void_p, ctypes.c_int, _ip, _ip, _ip, _ip]
@@ -128,15 +130,17 @@ class OracleHODLR:
     def compress(self, nthreads=None):
         lib().orc_compress(self.h, int(nthreads or os.cpu_count() or 1))
 
-    def factorize(self):
-        return lib().orc_factorize(self.h)
+    def factorize(self, nthreads=1):
+        """recLU_Factorize; nthreads > 1 runs sibling subtrees on threads
+        (same results as the sequential recursion)."""
+        return lib().orc_factorize_mt(self.h, int(nthreads))
 
-    def solve(self, b):
+    def solve(self, b, nthreads=1):
         b = np.asfortranarray(b, dtype=np.float64)
         if b.ndim == 1:
             b = b.reshape(-1, 1, order="F")
         x = np.zeros_like(b, order="F")
-        lib().orc_solve(self.h, b.shape[1], _ptr(b), _ptr(x))
+        lib().orc_solve_mt(self.h, b.shape[1], _ptr(b), _ptr(x), int(nthreads))
         return x
 
     # tree / block introspection

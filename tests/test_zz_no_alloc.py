@@ -1,11 +1,12 @@
 """The allocation-free full-kernel product (hodlr_kernel_matvec_noalloc).
 
-It serves callers that cannot allocate device memory at the point of use --
-code running inside a CUDA-graph stream capture, or under a memory manager
-that has already reserved the GPU -- by keeping its scratch in a static device
-array.  This file is collected last so that a run stopping at the first
-failure has already run every other test; it passes on its own in a fresh
-process as well as after the rest of the suite.
+It serves callers that cannot allocate device memory when they need K x --
+an application whose memory manager has already reserved the GPU, a plugin
+that must not allocate behind its host framework, latency-bound code that
+avoids cudaMalloc's device synchronisation -- by keeping its scratch in a
+static device array.  This file is collected last so that a run stopping at
+the first failure has already run every other test; it passes on its own in a
+fresh process as well as after the rest of the suite.
 """
 import ctypes
 
@@ -50,6 +51,43 @@ def test_noalloc_matvec_matches_handle_matvec_twice():
         got = y_d.cpu().numpy()
         assert np.isfinite(got).all()
         assert np.linalg.norm(got - ref) / np.linalg.norm(ref) <= TOL, f"call {call}"
+
+
+def test_noalloc_matvec_matches_oracle_and_allocates_nothing(oracle_mod):
+    """Against the CPU oracle's K x directly, and with the device's free memory
+    and torch's allocator unchanged across calls (after a first call, which
+    loads the module and with it the static scratch)."""
+    import torch
+
+    from dense_hodlr_b200 import KernelSpec
+    from dense_hodlr_b200 import _lib
+    from dense_hodlr_b200.points import uniform_cube
+
+    lib = _lib.lib()
+    n, dim, nrhs = 6000, 3, 2
+    pts = uniform_cube(n, dim, 23)
+    spec = KernelSpec("gaussian", 0.3, 0.1)
+    o = oracle_mod.OracleHODLR.from_kernel(pts, 0, 0.3, shift=0.1, leaf=64)
+    pts_d = torch.from_numpy(pts).cuda()
+    desc = spec.desc()
+    rng = np.random.default_rng(9)
+    x = rng.standard_normal((n, nrhs))
+    x_d = torch.from_numpy(np.ascontiguousarray(x.T)).cuda()
+    y_d = torch.empty_like(x_d)
+    assert _run_noalloc(lib, n, dim, pts_d, desc, nrhs, x_d, y_d) == 0  # first call: set-up
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    alloc0 = torch.cuda.memory_allocated()
+    ref = o.kernel_matvec(x)
+    for call in range(2):
+        y_d.fill_(float("nan"))
+        assert _run_noalloc(lib, n, dim, pts_d, desc, nrhs, x_d, y_d) == 0, f"call {call}"
+        torch.cuda.synchronize()
+        got = y_d.cpu().numpy().T
+        assert np.linalg.norm(got - ref) / np.linalg.norm(ref) <= TOL, f"call {call}"
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
+    assert torch.cuda.memory_allocated() == alloc0
 
 
 def test_noalloc_rejects_sizes_beyond_its_scratch():
