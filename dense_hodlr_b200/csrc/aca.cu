@@ -629,9 +629,14 @@ size_t aca_smem_bytes(int nt, int kcap_max) {
   return aca_smem(nt, kcap_max, aca_dots_global(nt, kcap_max));
 }
 
+// Dynamic shared memory above 48 KB, and the largest shared-memory carveout:
+// the occupancy query that sizes a cooperative launch and the launch itself
+// then see the same per-SM capacity.
 static int set_smem(void* fn, size_t smem) {
-  if (smem <= 48 * 1024) return 0;
-  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                       (int)cudaSharedmemCarveoutMaxShared);
+  if (e == cudaSuccess && smem > 48 * 1024)
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) cudaGetLastError();  // consume it: later launch checks stay clean
   return (int)e;
 }

@@ -279,6 +279,10 @@ struct hodlr_handle_s {
 
 namespace {
 
+// Internal status (never returned by the C ABI): a cooperative launch was
+// refused as too large and may be retried with fewer CTAs.
+constexpr int HODLR_ERR_RETRY_SMALLER = 1000;
+
 int fail(hodlr_t h, int code, const std::string& msg) {
   if (h) h->err = msg;
   return code;
@@ -696,6 +700,7 @@ int run_aca(hodlr_t h, std::vector<AcaBlock>& blocks, int G, int nt, int kcap_ma
     for (int g : *groups) coop |= g > 1;
   CK(cudaEventRecord(h->ev0, h->stream));
   int rc = aca_launch(L, nt, kcap_max, coop, h->stream);
+  if (rc == (int)cudaErrorCooperativeLaunchTooLarge) return HODLR_ERR_RETRY_SMALLER;
   if (rc) return cuda_fail(h, (cudaError_t)rc, "aca_launch");
   h->nlaunch += 1;
   CK(cudaEventRecord(h->ev1, h->stream));
@@ -924,11 +929,16 @@ int do_compress(hodlr_t h) {
       // equal groups: CTAs sized by predicted work measured 2-8% slower on
       // 3D clouds than equal groups (per-step latency, not streamed bytes,
       // sets a block's time)
-      const int G = std::max(1, std::max(1, ps) * h->num_sms / nb);
-      L.G = G;
+      int G = std::max(1, std::max(1, ps) * h->num_sms / nb);
       std::vector<AcaBlock> bl(nb);
-      for (int q = 0; q < nb; ++q) fill_block(h, L, q, bl[q]);
-      rc = run_aca(h, bl, G, G > 1 ? 256 : 128, L.kcap);
+      for (;;) {  // a cooperative launch the driver refuses is retried with half the groups
+        L.G = G;
+        for (int q = 0; q < nb; ++q) fill_block(h, L, q, bl[q]);
+        rc = run_aca(h, bl, G, G > 1 ? 256 : 128, L.kcap);
+        if (rc != HODLR_ERR_RETRY_SMALLER) break;
+        if (G == 1) return fail(h, HODLR_ERR_CUDA, "aca_launch: cooperative launch refused");
+        G = std::max(1, G / 2);
+      }
       if (rc) return rc;
       bool done;
       rc = sync_level(h, L, &done);
@@ -1273,9 +1283,11 @@ int do_factorize(hodlr_t h) {
     S.R = h->Z;
     S.piv = L.piv;
     S.err = h->d_err;
-    e = schur_factor_launch(S, nn, L.max_sd, h->stream);
+    std::vector<int> sds(nn);
+    for (int p = 0; p < nn; ++p) sds[p] = L.nodes[p].kb + L.nodes[p].kt;
+    e = schur_factor_launch(S, nn, sds.data(), h->stream);
     if (e) return cuda_fail(h, (cudaError_t)e, "schur_factor");
-    h->nlaunch += 2;
+    h->nlaunch += schur_factor_launches(sds.data(), nn);
     if (L.coff > 0) {
       e = schur_solve_launch(S, nn, -1, L.coff, L.max_sd, h->stream);
       if (e) return cuda_fail(h, (cudaError_t)e, "schur_solve");

@@ -14,6 +14,9 @@
 //                     (SchurLU = PartialPivLU(S), src/HODLR_Matrix.cpp:675).
 //  schur_solve_kernel y = S^-1 rhs by the stored LU (src/HODLR_Matrix.cpp:682,746).
 // Pivoting takes the first maximum |a| of the column, as PartialPivLU does.
+#include <algorithm>
+#include <vector>
+
 #include "common.cuh"
 #include "lu.h"
 
@@ -219,28 +222,25 @@ __global__ void schur_form_kernel(SchurLaunch L) {
 }
 
 // ------------------------------------------------------ dense batched LU
-// Blocked right-looking LU with row partial pivoting of each node's S, one CTA
-// per node, S in global memory (L2 resident).  Panels of PNB columns are
-// factored in shared memory; the trailing matrix is updated with 4x4 register
-// tiles.  The row interchanges of a panel are applied to the whole row, so the
-// packed result and `piv` are those of an unblocked partial-pivot LU with the
-// same pivot choices (LAPACK getrf convention).
+// Blocked right-looking LU with row partial pivoting, S in global memory (L2
+// resident).  Panels of PNB columns are factored in shared memory; the
+// trailing matrix is updated with 4x4 register tiles.  The row interchanges
+// of a panel are applied to the whole row, so the packed result and `piv`
+// are those of an unblocked partial-pivot LU with the same pivot choices
+// (LAPACK getrf convention).
 constexpr int SNT = 512;
 
-__global__ void __launch_bounds__(SNT) schur_lu_kernel(SchurLaunch L, int pnb) {
-  extern __shared__ double pan[];  // rows x pnb panel, leading dimension rows
-  __shared__ double red_v[SNT / 32];
-  __shared__ int red_i[SNT / 32];
-  __shared__ int lpiv[64];
-  const int node = blockIdx.x;
-  const SchurNode N = L.nodes[node];
-  const int n = N.kb + N.kt;
-  double* a = L.S + N.s_off;
-  int* piv = L.piv + N.p_off;
+// One CTA factors columns [jlo, jhi) of the n x n matrix a (columns < jlo
+// final, their interchanges already applied to columns >= jlo): the pivots of
+// those columns go to piv, their interchanges are applied to the columns of
+// [jlo, jhi) only, and the columns >= jhi are not touched.  jlo = 0,
+// jhi = n is the whole LU.
+__device__ bool lu_columns(double* a, int n, int* piv, int jlo, int jhi, int pnb, double* pan,
+                           double* red_v, int* red_i, int* lpiv) {
   const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
   bool singular = false;
-  for (int j0 = 0; j0 < n; j0 += pnb) {
-    const int nb = min(pnb, n - j0), rows = n - j0;
+  for (int j0 = jlo; j0 < jhi; j0 += pnb) {
+    const int nb = min(pnb, jhi - j0), rows = n - j0;
     for (int e = tid; e < rows * nb; e += SNT) {
       int r = e % rows, c = e / rows;
       pan[c * rows + r] = a[(int64_t)(j0 + c) * n + j0 + r];
@@ -292,13 +292,13 @@ __global__ void __launch_bounds__(SNT) schur_lu_kernel(SchurLaunch L, int pnb) {
       }
       __syncthreads();
     }
-    // panel back to global, pivots, interchanges outside the panel
+    // panel back to global, pivots, interchanges in the other columns of the range
     for (int e = tid; e < rows * nb; e += SNT) {
       int r = e % rows, c = e / rows;
       a[(int64_t)(j0 + c) * n + j0 + r] = pan[c * rows + r];
     }
     if (tid < nb) piv[j0 + tid] = j0 + lpiv[tid];
-    for (int col = tid; col < n; col += SNT) {
+    for (int col = jlo + tid; col < jhi; col += SNT) {
       if (col >= j0 && col < j0 + nb) continue;
       double* ac = a + (int64_t)col * n;
       for (int c = 0; c < nb; ++c) {
@@ -311,10 +311,11 @@ __global__ void __launch_bounds__(SNT) schur_lu_kernel(SchurLaunch L, int pnb) {
       }
     }
     __syncthreads();
-    const int rest = n - j0 - nb;
-    if (rest > 0) {
+    const int rest = n - j0 - nb;      // trailing rows
+    const int crest = jhi - j0 - nb;   // trailing columns inside the range
+    if (rest > 0 && crest > 0) {
       // U12 = L11^-1 A12, one thread per column
-      for (int col = j0 + nb + tid; col < n; col += SNT) {
+      for (int col = j0 + nb + tid; col < jhi; col += SNT) {
         double* ac = a + (int64_t)col * n + j0;
         for (int i = 1; i < nb; ++i) {
           double t = ac[i];
@@ -324,8 +325,8 @@ __global__ void __launch_bounds__(SNT) schur_lu_kernel(SchurLaunch L, int pnb) {
       }
       __syncthreads();
       // A22 -= L21 U12 with 4x4 register tiles
-      const int tr = (rest + 3) / 4;
-      for (int tt = tid; tt < tr * tr; tt += SNT) {
+      const int tr = (rest + 3) / 4, tc = (crest + 3) / 4;
+      for (int tt = tid; tt < tr * tc; tt += SNT) {
         const int ti = (tt % tr) * 4, tj = (tt / tr) * 4;
         double acc[4][4];
 #pragma unroll
@@ -338,7 +339,7 @@ __global__ void __launch_bounds__(SNT) schur_lu_kernel(SchurLaunch L, int pnb) {
           for (int x = 0; x < 4; ++x) l[x] = (ti + x < rest) ? pan[p * rows + nb + ti + x] : 0.0;
 #pragma unroll
           for (int y = 0; y < 4; ++y)
-            u[y] = (tj + y < rest) ? a[(int64_t)(j0 + nb + tj + y) * n + j0 + p] : 0.0;
+            u[y] = (tj + y < crest) ? a[(int64_t)(j0 + nb + tj + y) * n + j0 + p] : 0.0;
 #pragma unroll
           for (int x = 0; x < 4; ++x)
 #pragma unroll
@@ -346,7 +347,7 @@ __global__ void __launch_bounds__(SNT) schur_lu_kernel(SchurLaunch L, int pnb) {
         }
 #pragma unroll
         for (int y = 0; y < 4; ++y) {
-          if (tj + y >= rest) continue;
+          if (tj + y >= crest) continue;
           double* ac = a + (int64_t)(j0 + nb + tj + y) * n + j0 + nb + ti;
 #pragma unroll
           for (int x = 0; x < 4; ++x)
@@ -356,7 +357,138 @@ __global__ void __launch_bounds__(SNT) schur_lu_kernel(SchurLaunch L, int pnb) {
       __syncthreads();
     }
   }
-  if (tid == 0 && singular) atomicOr(L.err, DEV_ERR_SINGULAR);
+  return singular;
+}
+
+// Whole LU of every node with sd < big_sd, one CTA per node (larger nodes are
+// left to the multi-CTA path below).
+__global__ void __launch_bounds__(SNT) schur_lu_kernel(SchurLaunch L, int pnb, int big_sd) {
+  extern __shared__ double pan[];  // rows x pnb panel, leading dimension rows
+  __shared__ double red_v[SNT / 32];
+  __shared__ int red_i[SNT / 32];
+  __shared__ int lpiv[64];
+  const SchurNode N = L.nodes[blockIdx.x];
+  const int n = N.kb + N.kt;
+  if (n >= big_sd) return;
+  const bool singular =
+      lu_columns(L.S + N.s_off, n, L.piv + N.p_off, 0, n, pnb, pan, red_v, red_i, lpiv);
+  if (threadIdx.x == 0 && singular) atomicOr(L.err, DEV_ERR_SINGULAR);
+}
+
+// ------------------------------------------- multi-CTA LU of large nodes
+// Right-looking, outer panels of BNB columns.  Per panel j0, for every large
+// node (its index in BigNodes): (1) one CTA factors the panel columns
+// [j0, j0+BNB) with lu_columns; (2) many CTAs apply the panel's interchanges
+// to every other column and form U12 = L11^-1 A12 right of the panel; (3)
+// A22 -= L21 U12 in 64 x 64 tiles over all SMs.  The pivot choices are the
+// column-wise first maxima, as in the one-CTA kernel.
+constexpr int BNB = 32;
+constexpr int BIG_MAX = 64;
+struct BigNodes {
+  int idx[BIG_MAX];
+  int count;
+};
+
+__global__ void __launch_bounds__(SNT) big_panel_kernel(SchurLaunch L, BigNodes B, int j0, int pnb) {
+  extern __shared__ double pan[];
+  __shared__ double red_v[SNT / 32];
+  __shared__ int red_i[SNT / 32];
+  __shared__ int lpiv[64];
+  const SchurNode N = L.nodes[B.idx[blockIdx.x]];
+  const int n = N.kb + N.kt;
+  if (j0 >= n) return;
+  const bool singular = lu_columns(L.S + N.s_off, n, L.piv + N.p_off, j0, min(n, j0 + BNB), pnb,
+                                   pan, red_v, red_i, lpiv);
+  if (threadIdx.x == 0 && singular) atomicOr(L.err, DEV_ERR_SINGULAR);
+}
+
+// One thread per column outside the panel: the panel's interchanges, then
+// (right of the panel) the unit-lower solve with L11.
+__global__ void __launch_bounds__(256) big_swap_trsm_kernel(SchurLaunch L, BigNodes B, int j0) {
+  __shared__ double l11[BNB][BNB + 1];
+  __shared__ int sp[BNB];
+  const SchurNode N = L.nodes[B.idx[blockIdx.y]];
+  const int n = N.kb + N.kt;
+  if (j0 >= n) return;
+  const int nb = min(BNB, n - j0);
+  double* a = L.S + N.s_off;
+  const int* piv = L.piv + N.p_off;
+  for (int e = threadIdx.x; e < BNB * BNB; e += blockDim.x) {
+    const int i = e % BNB, p = e / BNB;
+    l11[i][p] = (i < nb && p < nb) ? a[(int64_t)(j0 + p) * n + j0 + i] : 0.0;
+  }
+  if (threadIdx.x < BNB) sp[threadIdx.x] = threadIdx.x < nb ? piv[j0 + threadIdx.x] : 0;
+  __syncthreads();
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= n || (col >= j0 && col < j0 + nb)) return;
+  double* ac = a + (int64_t)col * n;
+  for (int c = 0; c < nb; ++c) {
+    const int q = sp[c];
+    if (q != j0 + c) {
+      const double t = ac[j0 + c];
+      ac[j0 + c] = ac[q];
+      ac[q] = t;
+    }
+  }
+  if (col < j0) return;
+  double u[BNB];
+#pragma unroll
+  for (int i = 0; i < BNB; ++i) u[i] = i < nb ? ac[j0 + i] : 0.0;
+#pragma unroll
+  for (int i = 1; i < BNB; ++i)
+#pragma unroll
+    for (int p = 0; p < i; ++p) u[i] = fma(-l11[i][p], u[p], u[i]);
+#pragma unroll
+  for (int i = 0; i < BNB; ++i)
+    if (i < nb) ac[j0 + i] = u[i];
+}
+
+// A22 -= L21 U12: CTA (ti, tj, node) owns a 64 x 64 tile, 256 threads with
+// 4 x 4 outputs each; L21 and U12 tiles staged in shared memory.
+constexpr int BT = 64;
+__global__ void __launch_bounds__(256) big_update_kernel(SchurLaunch L, BigNodes B, int j0) {
+  __shared__ double ls[BNB][BT + 1];  // L21 tile, [p][row]
+  __shared__ double us[BNB][BT + 1];  // U12 tile, [p][col]
+  const SchurNode N = L.nodes[B.idx[blockIdx.z]];
+  const int n = N.kb + N.kt;
+  const int r0 = j0 + BNB + blockIdx.x * BT, c0 = j0 + BNB + blockIdx.y * BT;
+  if (r0 >= n || c0 >= n) return;
+  double* a = L.S + N.s_off;
+  for (int e = threadIdx.x; e < BNB * BT; e += blockDim.x) {
+    const int i = e % BT, p = e / BT;
+    ls[p][i] = r0 + i < n ? a[(int64_t)(j0 + p) * n + r0 + i] : 0.0;
+    us[p][i] = c0 + i < n ? a[(int64_t)(c0 + i) * n + j0 + p] : 0.0;
+  }
+  __syncthreads();
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;  // rows tx + 16x, cols ty + 16y
+  double acc[4][4];
+#pragma unroll
+  for (int x = 0; x < 4; ++x)
+#pragma unroll
+    for (int y = 0; y < 4; ++y) acc[x][y] = 0.0;
+#pragma unroll 8
+  for (int p = 0; p < BNB; ++p) {
+    double l[4], u[4];
+#pragma unroll
+    for (int x = 0; x < 4; ++x) l[x] = ls[p][tx + 16 * x];
+#pragma unroll
+    for (int y = 0; y < 4; ++y) u[y] = us[p][ty + 16 * y];
+#pragma unroll
+    for (int x = 0; x < 4; ++x)
+#pragma unroll
+      for (int y = 0; y < 4; ++y) acc[x][y] = fma(l[x], u[y], acc[x][y]);
+  }
+#pragma unroll
+  for (int y = 0; y < 4; ++y) {
+    const int c = c0 + ty + 16 * y;
+    if (c >= n) continue;
+    double* ac = a + (int64_t)c * n;
+#pragma unroll
+    for (int x = 0; x < 4; ++x) {
+      const int r = r0 + tx + 16 * x;
+      if (r < n) ac[r] -= acc[x][y];
+    }
+  }
 }
 
 // x <- U^-1 L^-1 x for `ncol` columns in shared memory (x[c*ldx+i]) with the
@@ -457,23 +589,30 @@ __device__ void lu_solve_global(const double* __restrict__ a, int n, double* x, 
 // the 32-register blocked tile solve.
 constexpr int STC = 16;
 
+// tc columns per CTA (STC, or fewer where a column tile would not fit in
+// shared memory); in_smem == false: the columns are solved in place in
+// global memory (capacitance matrices too large for even one column).
 template <bool WARP_SUBST>
-__global__ void __launch_bounds__(256) schur_solve_kernel(SchurLaunch L, int ncols) {
-  extern __shared__ double xs[];
+__global__ void __launch_bounds__(256) schur_solve_kernel(SchurLaunch L, int ncols, int tc,
+                                                          bool in_smem) {
+  extern __shared__ double xs_smem[];
   const int node = blockIdx.y;
   const SchurNode N = L.nodes[node];
   const int n = N.kb + N.kt;
   const int cols = ncols < 0 ? N.coff : ncols;
-  const int c0 = blockIdx.x * STC;
+  const int c0 = blockIdx.x * tc;
   if (c0 >= cols) return;
-  const int nc = min(STC, cols - c0);
+  const int nc = min(tc, cols - c0);
   const double* a = L.S + N.s_off;
   const int* piv = L.piv + N.p_off;
-  const int ldx = n | 1;
   double* R = L.R + N.r_off;
-  for (int e = threadIdx.x; e < n * nc; e += blockDim.x) {
-    int i = e % n, c = e / n;
-    xs[c * ldx + i] = R[(int64_t)(c0 + c) * n + i];
+  const int ldx = in_smem ? (n | 1) : n;
+  double* xs = in_smem ? xs_smem : R + (int64_t)c0 * n;
+  if (in_smem) {
+    for (int e = threadIdx.x; e < n * nc; e += blockDim.x) {
+      int i = e % n, c = e / n;
+      xs[c * ldx + i] = R[(int64_t)(c0 + c) * n + i];
+    }
   }
   __syncthreads();
   for (int c = threadIdx.x; c < nc; c += blockDim.x) {
@@ -492,9 +631,11 @@ __global__ void __launch_bounds__(256) schur_solve_kernel(SchurLaunch L, int nco
     lu_solve_global(a, n, xs, ldx, nc);
   else
     lu_solve_tile(GlobalLU{a, n}, n, xs, ldx, nc);
-  for (int e = threadIdx.x; e < n * nc; e += blockDim.x) {
-    int i = e % n, c = e / n;
-    R[(int64_t)(c0 + c) * n + i] = xs[c * ldx + i];
+  if (in_smem) {
+    for (int e = threadIdx.x; e < n * nc; e += blockDim.x) {
+      int i = e % n, c = e / n;
+      R[(int64_t)(c0 + c) * n + i] = xs[c * ldx + i];
+    }
   }
 }
 
@@ -526,33 +667,99 @@ int leaf_solve_launch(const LeafSolveLaunch& L, int nleaves, int smax, cudaStrea
   return (int)cudaGetLastError();
 }
 
-int schur_factor_launch(const SchurLaunch& L, int nnodes, int max_sd, cudaStream_t s) {
+// Inner panel width for rows x pnb doubles of shared memory (<= 200 KB).
+static int panel_width(int rows) {
+  int pnb = 16;
+  while (pnb > 1 && (size_t)rows * pnb * sizeof(double) > 200 * 1024) pnb >>= 1;
+  return pnb;
+}
+
+int schur_factor_launch(const SchurLaunch& L, int nnodes, const int* sd, cudaStream_t s) {
   if (nnodes == 0) return 0;
   schur_form_kernel<<<nnodes, 256, 0, s>>>(L);
-  int pnb = 16;
-  while (pnb > 1 && (size_t)max_sd * pnb * sizeof(double) > 200 * 1024) pnb >>= 1;
-  size_t smem = (size_t)max_sd * pnb * sizeof(double);
-  if (smem > 48 * 1024)
-    cudaFuncSetAttribute(schur_lu_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  schur_lu_kernel<<<nnodes, SNT, smem, s>>>(L, pnb);
+  int small_max = 0, big_max = 0;
+  std::vector<int> big;
+  for (int i = 0; i < nnodes; ++i) {
+    if (sd[i] >= SCHUR_BIG_SD) {
+      big.push_back(i);
+      big_max = std::max(big_max, sd[i]);
+    } else {
+      small_max = std::max(small_max, sd[i]);
+    }
+  }
+  if (small_max > 0) {
+    const int pnb = panel_width(small_max);
+    size_t smem = (size_t)small_max * pnb * sizeof(double);
+    if (smem > 48 * 1024)
+      cudaFuncSetAttribute(schur_lu_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem);
+    schur_lu_kernel<<<nnodes, SNT, smem, s>>>(L, pnb, SCHUR_BIG_SD);
+  }
+  for (size_t b0 = 0; b0 < big.size(); b0 += BIG_MAX) {
+    BigNodes B;
+    B.count = (int)std::min<size_t>(BIG_MAX, big.size() - b0);
+    int mx = 0;
+    for (int i = 0; i < B.count; ++i) {
+      B.idx[i] = big[b0 + i];
+      mx = std::max(mx, sd[big[b0 + i]]);
+    }
+    const int pnb = std::min(BNB, panel_width(mx));
+    const size_t smem = (size_t)mx * pnb * sizeof(double);
+    if (smem > 48 * 1024)
+      cudaFuncSetAttribute(big_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem);
+    for (int j0 = 0; j0 < mx; j0 += BNB) {
+      big_panel_kernel<<<B.count, SNT, smem, s>>>(L, B, j0, pnb);
+      big_swap_trsm_kernel<<<dim3((mx + 255) / 256, B.count), 256, 0, s>>>(L, B, j0);
+      const int rest = mx - j0 - BNB;
+      if (rest > 0) {
+        const int t = (rest + BT - 1) / BT;
+        big_update_kernel<<<dim3(t, t, B.count), 256, 0, s>>>(L, B, j0);
+      }
+    }
+  }
   return (int)cudaGetLastError();
+}
+
+int schur_factor_launches(const int* sd, int nnodes) {
+  int n = 1, small = 0, mx = 0, big = 0;
+  for (int i = 0; i < nnodes; ++i) {
+    if (sd[i] >= SCHUR_BIG_SD) {
+      ++big;
+      mx = std::max(mx, sd[i]);
+    } else {
+      small = 1;
+    }
+  }
+  n += small;
+  if (big) {
+    const int batches = (big + BIG_MAX - 1) / BIG_MAX;
+    for (int j0 = 0; j0 < mx; j0 += BNB) n += batches * (mx - j0 - BNB > 0 ? 3 : 2);
+  }
+  return n;
 }
 
 int schur_solve_launch(const SchurLaunch& L, int nnodes, int ncols, int max_cols, int max_sd,
                        cudaStream_t s) {
   if (nnodes == 0 || max_cols <= 0) return 0;
-  size_t smem = sizeof(double) * (size_t)(max_sd | 1) * STC;
-  const dim3 grid((max_cols + STC - 1) / STC, nnodes);
+  // columns per CTA: STC, fewer when a tile of them would exceed the
+  // shared-memory budget, none (in place in global memory) past one column
+  const size_t col_bytes = sizeof(double) * (size_t)(max_sd | 1);
+  constexpr size_t kBudget = 200 * 1024;
+  const int tc = (int)std::max<size_t>(1, std::min<size_t>(STC, kBudget / col_bytes));
+  const bool in_smem = col_bytes <= kBudget;
+  const size_t smem = in_smem ? col_bytes * tc : 0;
+  const dim3 grid((max_cols + tc - 1) / tc, nnodes);
   if (ncols >= 0) {
     if (smem > 48 * 1024)
       cudaFuncSetAttribute(schur_solve_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem);
-    schur_solve_kernel<true><<<grid, 256, smem, s>>>(L, ncols);
+    schur_solve_kernel<true><<<grid, 256, smem, s>>>(L, ncols, tc, in_smem);
   } else {
     if (smem > 48 * 1024)
       cudaFuncSetAttribute(schur_solve_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem);
-    schur_solve_kernel<false><<<grid, 256, smem, s>>>(L, ncols);
+    schur_solve_kernel<false><<<grid, 256, smem, s>>>(L, ncols, tc, in_smem);
   }
   return (int)cudaGetLastError();
 }

@@ -48,6 +48,13 @@ struct SchurLaunch {
 
 int leaf_lu_launch(const LeafLULaunch& L, int nleaves, int smax, cudaStream_t s);
 int leaf_solve_launch(const LeafSolveLaunch& L, int nleaves, int smax, cudaStream_t s);
-int schur_factor_launch(const SchurLaunch& L, int nnodes, int max_sd, cudaStream_t s);
+// Capacitance matrices of at least this size are factored by the multi-CTA
+// blocked LU (panel, swap + triangular solve, tiled trailing update per 32
+// columns); smaller ones by one CTA each.
+constexpr int SCHUR_BIG_SD = 768;
+// sd: host array of the nodes' capacitance sizes (kb + kt), in node order.
+int schur_factor_launch(const SchurLaunch& L, int nnodes, const int* sd, cudaStream_t s);
+// Kernel launches schur_factor_launch makes for these sizes.
+int schur_factor_launches(const int* sd, int nnodes);
 int schur_solve_launch(const SchurLaunch& L, int nnodes, int ncols, int max_cols, int max_sd,
                        cudaStream_t s);

@@ -31,6 +31,9 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <condition_variable>
+#include <functional>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -423,10 +426,104 @@ void finish_tree(Oracle& o, const std::vector<std::vector<int>>& levelVec,
 }
 
 // ------------------------------------------------------------------ ACA
+// Persistent worker threads for parallel_for: a call costs a wake-up, not
+// thread creation (ACA calls it three times per step).  One call runs at a
+// time; a call made while another runs (from a worker, or from a second host
+// thread) runs serially.  The pool is never destroyed: its threads block on
+// a condition variable until the process exits.
+class Pool {
+ public:
+  template <class F>
+  void run(int count, int nthreads, F& f) {
+    std::unique_lock<std::mutex> rl(run_mu_, std::try_to_lock);
+    if (!rl.owns_lock()) {
+      for (int i = 0; i < count; ++i) f(i);
+      return;
+    }
+    const int want = std::min(nthreads, count) - 1;
+    std::function<void(int)> job = [&f](int i) { f(i); };
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      while ((int)workers_.size() < want) {
+        const int id = (int)workers_.size();
+        workers_.emplace_back([this, id]() { loop(id); });
+        workers_.back().detach();
+      }
+      job_ = &job;
+      count_ = count;
+      next_.store(0);
+      want_ = want;
+      finished_ = 0;
+      ++gen_;
+    }
+    cv_.notify_all();
+    for (int i = next_.fetch_add(1); i < count; i = next_.fetch_add(1)) job(i);
+    std::unique_lock<std::mutex> lk(mu_);
+    done_cv_.wait(lk, [&]() { return finished_ == want_; });
+    job_ = nullptr;
+  }
+
+ private:
+  void loop(int id) {
+    long seen = 0;
+    for (;;) {
+      std::unique_lock<std::mutex> lk(mu_);
+      cv_.wait(lk, [&]() { return gen_ != seen; });
+      seen = gen_;
+      if (id >= want_) continue;
+      const std::function<void(int)>* job = job_;
+      const int count = count_;
+      lk.unlock();
+      for (int i = next_.fetch_add(1); i < count; i = next_.fetch_add(1)) (*job)(i);
+      lk.lock();
+      if (++finished_ == want_) done_cv_.notify_all();
+    }
+  }
+  std::mutex run_mu_, mu_;
+  std::condition_variable cv_, done_cv_;
+  std::vector<std::thread> workers_;
+  const std::function<void(int)>* job_ = nullptr;
+  int count_ = 0, want_ = 0, finished_ = 0;
+  long gen_ = 0;
+  std::atomic<int> next_{0};
+};
+
+Pool& pool() {
+  static Pool* p = new Pool();  // never destroyed (see Pool)
+  return *p;
+}
+
+template <class F>
+void parallel_for(int count, int nthreads, F f) {
+  if (nthreads <= 1 || count <= 1) {
+    for (int i = 0; i < count; ++i) f(i);
+    return;
+  }
+  pool().run(count, nthreads, f);
+}
+
 static double dot(const double* x, const double* y, int n) {
   double s = 0.0;
   for (int i = 0; i < n; ++i) s = s + x[i] * y[i];
   return s;
+}
+
+// Four dots x . y_q side by side: each summed in order, as dot() would
+// (x * y_q and y_q * x round alike).
+static void dot4(const double* x, const double* y0, const double* y1, const double* y2,
+                 const double* y3, int n, double* out) {
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+  for (int i = 0; i < n; ++i) {
+    const double xi = x[i];
+    s0 = s0 + xi * y0[i];
+    s1 = s1 + xi * y1[i];
+    s2 = s2 + xi * y2[i];
+    s3 = s3 + xi * y3[i];
+  }
+  out[0] = s0;
+  out[1] = s1;
+  out[2] = s2;
+  out[3] = s3;
 }
 
 // chooseNextRowCol (src/lowRank.cpp:291-298)
@@ -445,8 +542,11 @@ double now_s() {
 
 // budget_s > 0 stops the loop after that many seconds (cost sampling only;
 // the block is then incomplete).  Returns false when stopped early.
+// nth > 1 spreads the element loops and the independent dot products of a
+// step over nth threads; every sum keeps its order, so the results do not
+// depend on nth.
 bool aca(const Oracle& o, Block& B, double tol, int minRank, int maxRank, int minPivot,
-         double budget_s = 0.0) {
+         double budget_s = 0.0, int nth = 1) {
   const double t0 = budget_s > 0 ? now_s() : 0.0;
   const int m = B.m, n = B.n, min_i = B.r0, min_j = B.c0;
   B.prow.clear();
@@ -480,12 +580,15 @@ bool aca(const Oracle& o, Block& B, double tol, int minRank, int maxRank, int mi
     chosenR[cr] = 1;
     const int gi = cr + min_i;
     s.assign(n, 0.0);
-    for (int l = 0; l < k; ++l) {
-      double w = W[l][cr];
-      const double* vl = V[l].data();
-      for (int j = 0; j < n; ++j) s[j] = s[j] + w * vl[j];
-    }
-    for (int j = 0; j < n; ++j) rr[j] = o.entry(gi, j + min_j) - s[j];
+    parallel_for((n + 1023) / 1024, nth, [&](int c) {
+      const int j0 = c * 1024, j1 = std::min(n, j0 + 1024);
+      for (int l = 0; l < k; ++l) {
+        double w = W[l][cr];
+        const double* vl = V[l].data();
+        for (int j = j0; j < j1; ++j) s[j] = s[j] + w * vl[j];
+      }
+      for (int j = j0; j < j1; ++j) rr[j] = o.entry(gi, j + min_j) - s[j];
+    });
     int mi = 0;
     double mv = std::fabs(rr[0]);
     for (int j = 1; j < n; ++j)
@@ -508,12 +611,15 @@ bool aca(const Oracle& o, Block& B, double tol, int minRank, int maxRank, int mi
     const int gj = cc + min_j;
     double piv = 1 / rr[cc];
     s.assign(m, 0.0);
-    for (int l = 0; l < k; ++l) {
-      double v = V[l][cc];
-      const double* wl = W[l].data();
-      for (int i = 0; i < m; ++i) s[i] = s[i] + v * wl[i];
-    }
-    for (int i = 0; i < m; ++i) rc[i] = o.entry(i + min_i, gj) - s[i];
+    parallel_for((m + 1023) / 1024, nth, [&](int c) {
+      const int i0 = c * 1024, i1 = std::min(m, i0 + 1024);
+      for (int l = 0; l < k; ++l) {
+        double v = V[l][cc];
+        const double* wl = W[l].data();
+        for (int i = i0; i < i1; ++i) s[i] = s[i] + v * wl[i];
+      }
+      for (int i = i0; i < i1; ++i) rc[i] = o.entry(i + min_i, gj) - s[i];
+    });
     mi = 0;
     mv = std::fabs(rc[0]);
     for (int i = 1; i < m; ++i)
@@ -529,9 +635,24 @@ bool aca(const Oracle& o, Block& B, double tol, int minRank, int maxRank, int mi
     V.push_back(rr);
     B.prow.push_back(cr);
     B.pcol.push_back(cc);
+    // the 2k dots, each summed in order; then sumNorm in j order
+    std::vector<double> dw(k), dv(k);
+    parallel_for((k + 3) / 4, nth, [&](int t) {
+      const int j = 4 * t, c = std::min(4, k - j);
+      if (c == 4) {
+        dot4(wk.data(), W[j].data(), W[j + 1].data(), W[j + 2].data(), W[j + 3].data(), m,
+             &dw[j]);
+        dot4(rr.data(), V[j].data(), V[j + 1].data(), V[j + 2].data(), V[j + 3].data(), n,
+             &dv[j]);
+      } else {
+        for (int q = j; q < j + c; ++q) {
+          dw[q] = dot(wk.data(), W[q].data(), m);
+          dv[q] = dot(V[q].data(), rr.data(), n);
+        }
+      }
+    });
     double sumNorm = 0;
-    for (int j = 0; j < k; ++j)
-      sumNorm += dot(wk.data(), W[j].data(), m) * dot(V[j].data(), rr.data(), n);
+    for (int j = 0; j < k; ++j) sumNorm += dw[j] * dv[j];
     double sw = dot(wk.data(), wk.data(), m), sv = dot(rr.data(), rr.data(), n);
     frob2 += 2 * sumNorm + sw * sv;
     double frob = std::sqrt(frob2);
@@ -577,24 +698,6 @@ bool aca(const Oracle& o, Block& B, double tol, int minRank, int maxRank, int mi
   return true;
 }
 
-template <class F>
-void parallel_for(int count, int nthreads, F f) {
-  if (nthreads <= 1 || count <= 1) {
-    for (int i = 0; i < count; ++i) f(i);
-    return;
-  }
-  std::atomic<int> next(0);
-  std::vector<std::thread> th;
-  for (int t = 0; t < nthreads; ++t)
-    th.emplace_back([&]() {
-      for (;;) {
-        int i = next.fetch_add(1);
-        if (i >= count) break;
-        f(i);
-      }
-    });
-  for (auto& t : th) t.join();
-}
 
 // storeLRinTree (src/HODLR_Matrix.cpp:274-338): leaves copy their diagonal
 // block, inner nodes compress their two off-diagonal blocks with ACA.  The
@@ -605,8 +708,18 @@ void compress(Oracle& o, int nthreads) {
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
     return (int64_t)o.blocks[a].m * o.blocks[a].n > (int64_t)o.blocks[b].m * o.blocks[b].n;
   });
-  parallel_for((int)order.size(), nthreads, [&](int t) {
+  // the largest blocks (fewer of their size than threads) one at a time with
+  // threads inside the block, the rest on a pool of whole blocks
+  int nbig = 0;
+  while (nthreads > 1 && nbig < (int)order.size() &&
+         (int64_t)(o.blocks[order[nbig]].m + o.blocks[order[nbig]].n) * nthreads >= 2LL * o.n)
+    ++nbig;
+  for (int t = 0; t < nbig; ++t) {
     Block& B = o.blocks[order[t]];
+    aca(o, B, o.tol, B.minRank, B.maxRank, o.minPivot, 0.0, nthreads);
+  }
+  parallel_for((int)order.size() - nbig, nthreads, [&](int t) {
+    Block& B = o.blocks[order[nbig + t]];
     aca(o, B, o.tol, B.minRank, B.maxRank, o.minPivot);
   });
   o.leafMat.assign(o.leaves.size(), Mat());
@@ -901,12 +1014,16 @@ double orc_tang_entry(int j) { return j >= 0 && j < HX_TANG_TABLE_SIZE ? hx_tang
 
 // Full-kernel product Y = K X (kernelMatrix::operator*, src/kernel.cpp:27-35),
 // summing over k in order for each (i, j); rows spread over threads.
-void orc_kernel_matvec(void* h, int nrhs, const double* X, double* Y, int nthreads) {
+// Rows [row0, row0 + nrows) of Y only (ld n): every row costs the same, so
+// the time of a row sample scales exactly to the full product.
+void orc_kernel_matvec_rows(void* h, int nrhs, const double* X, double* Y, int row0, int nrows,
+                            int nthreads) {
   const Oracle* o = (const Oracle*)h;
   int n = o->n;
-  int chunks = (n + 63) / 64;
+  const int end = std::min(n, row0 + nrows);
+  int chunks = (end - row0 + 63) / 64;
   parallel_for(chunks, nthreads, [&](int c) {
-    int i0 = c * 64, i1 = std::min(n, i0 + 64);
+    int i0 = row0 + c * 64, i1 = std::min(end, i0 + 64);
     for (int j = 0; j < nrhs; ++j)
       for (int i = i0; i < i1; ++i) {
         double s = 0.0;
@@ -916,17 +1033,28 @@ void orc_kernel_matvec(void* h, int nrhs, const double* X, double* Y, int nthrea
   });
 }
 
+void orc_kernel_matvec(void* h, int nrhs, const double* X, double* Y, int nthreads) {
+  orc_kernel_matvec_rows(h, nrhs, X, Y, 0, ((const Oracle*)h)->n, nthreads);
+}
+
 // ------------------------------------------------------ cost sampling
 // Used only by the CPU-baseline leg of the benchmark: bounded runs of the
 // same operations on the workload's own blocks and sizes.
 
 // ACA of one block for at most budget_s seconds; returns iterations done,
 // *seconds the time taken, *finished whether the block completed.
+int orc_aca_block_mt(void* h, int b, double budget_s, double* seconds, int* finished,
+                     int nthreads);
 int orc_aca_block(void* h, int b, double budget_s, double* seconds, int* finished) {
+  return orc_aca_block_mt(h, b, budget_s, seconds, finished, 1);
+}
+
+int orc_aca_block_mt(void* h, int b, double budget_s, double* seconds, int* finished,
+                     int nthreads) {
   Oracle* o = (Oracle*)h;
   Block B = o->blocks[b];
   double t0 = now_s();
-  bool done = aca(*o, B, o->tol, -1, -1, o->minPivot, budget_s);
+  bool done = aca(*o, B, o->tol, -1, -1, o->minPivot, budget_s, nthreads);
   *seconds = now_s() - t0;
   *finished = done ? 1 : 0;
   return B.iters;

@@ -69,7 +69,11 @@ def lib():
         L.orc_tang_entry.argtypes = [ctypes.c_int]
         L.orc_tang_entry.restype = ctypes.c_double
         L.orc_kernel_matvec.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp, ctypes.c_int]
+        L.orc_kernel_matvec_rows.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp,
+                                             ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.orc_aca_block.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, _dp, _ip]
+        L.orc_aca_block_mt.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, _dp, _ip,
+                                       ctypes.c_int]
         L.orc_bench_node.restype = ctypes.c_double
         L.orc_bench_node.argtypes = [ctypes.c_int] * 6
         L.orc_bench_leaf.restype = ctypes.c_double
@@ -197,12 +201,12 @@ class OracleHODLR:
         lib().orc_block_lowrank(self.h, b, _ptr(W), _ptr(V))
         return W, V
 
-    def aca_block_sample(self, b, budget_s):
+    def aca_block_sample(self, b, budget_s, nthreads=1):
         """Run the ACA of block b for at most budget_s seconds (cost sampling)."""
         secs = ctypes.c_double()
         fin = ctypes.c_int()
-        it = lib().orc_aca_block(self.h, int(b), float(budget_s), ctypes.byref(secs),
-                                 ctypes.byref(fin))
+        it = lib().orc_aca_block_mt(self.h, int(b), float(budget_s), ctypes.byref(secs),
+                                    ctypes.byref(fin), int(nthreads))
         return it, secs.value, bool(fin.value)
 
     def entry(self, i, j):
@@ -215,6 +219,16 @@ class OracleHODLR:
         y = np.zeros_like(x, order="F")
         lib().orc_kernel_matvec(self.h, x.shape[1], _ptr(x), _ptr(y),
                                 int(nthreads or os.cpu_count() or 1))
+        return y
+
+    def kernel_matvec_rows(self, x, row0, nrows, nthreads=None):
+        """Rows [row0, row0 + nrows) of K x (the other rows of the result are 0)."""
+        x = np.asfortranarray(x, dtype=np.float64)
+        if x.ndim == 1:
+            x = x.reshape(-1, 1, order="F")
+        y = np.zeros_like(x, order="F")
+        lib().orc_kernel_matvec_rows(self.h, x.shape[1], _ptr(x), _ptr(y), int(row0),
+                                     int(nrows), int(nthreads or os.cpu_count() or 1))
         return y
 
 

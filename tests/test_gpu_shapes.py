@@ -1,0 +1,96 @@
+"""GPU parity at reduced size for the configurations measured at 2^20 points,
+and for the minPivot skip-row path of ACA.
+
+* The sphere / Matern-3/2 shape (unit sphere, l = 0.1, shift 1e-2, leaf 128,
+  ACA tol 1e-10): its ranks make the top capacitance matrices large enough
+  for the multi-CTA blocked LU (sd >= SCHUR_BIG_SD = 768).
+* The cube / Gaussian shape (l = 0.3, shift 0.1, leaf 128, tol 1e-8) with 16
+  right-hand sides, through HODLR-preconditioned GMRES in every precision of
+  the Woodbury products.
+* minPivot >= 1 (src/lowRank.cpp:187-195 skip path, :197-203 and :217-227
+  fallbacks): dense 10 * Gaussian + I with minPivot 2.5 (truncated to 2, as
+  the reference passes it to an int).
+
+Bit-exact: pivots, ranks, iteration counts and the W/V factors of the
+largest blocks.  Solutions within 1e-10 of the oracle's.
+"""
+import numpy as np
+import pytest
+
+from dense_hodlr_b200 import HODLR_Matrix, KernelSpec
+from dense_hodlr_b200.points import uniform_cube, unit_sphere
+
+from .test_gpu_parity import SOLVE_TOL, _compare_compression, _pair
+
+pytestmark = pytest.mark.gpu
+
+BIG_SD = 768  # SCHUR_BIG_SD in csrc/lu.h
+
+
+def _device_gmres(g, b, tol=1e-10, max_iter=60):
+    import torch
+    b_d = torch.from_numpy(np.ascontiguousarray(b.T)).cuda()
+    x_d = torch.empty_like(b_d)
+    it, rel = g.iterative_solve_device(b_d.data_ptr(), x_d.data_ptr(), b.shape[1], tol=tol,
+                                       max_iter=max_iter, restart=32)
+    return it, rel, x_d.cpu().numpy().T
+
+
+def test_sphere_matern_tol_1e10_bit_exact_and_large_capacitance(oracle_mod):
+    n = 16384
+    pts = unit_sphere(n, 31)
+    g, o = _pair(oracle_mod, pts, "matern32", 0.1, 1e-2, 128, 1e-10)
+    _compare_compression(g, o, check_factors=False)
+    assert np.array_equal([g.block_info(b)["iters"] for b in range(g.num_blocks())], o.iters())
+    for b in (0, 1, 2, 3):
+        info = g.block_info(b)
+        W, V = g.lowrank(b)
+        Wo, Vo = o.lowrank(b, info["m"], info["n"])
+        assert np.array_equal(W, Wo) and np.array_equal(V, Vo), b
+    r = g.ranks()
+    assert r[0] + r[1] >= BIG_SD  # the root's capacitance LU takes the multi-CTA path
+    b = np.random.default_rng(6).standard_normal((n, 2))
+    x = g.recLU_Solve(b)
+    xo = o.solve(b, nthreads=8)
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= SOLVE_TOL
+    it, rel, xg = _device_gmres(g, b)
+    assert rel.max() <= 1e-10
+    assert np.all(g.residual(xg, b) <= 1e-10)
+
+
+@pytest.mark.parametrize("n,leaf", [(256, 32), (4096, 64)])
+def test_min_pivot_skip_rows_bit_exact(oracle_mod, n, leaf):
+    rng = np.random.default_rng(22)
+    x = np.sort(rng.uniform(-1.0, 1.0, n))
+    A = 10.0 * np.exp(-((x[:, None] - x[None, :]) / 0.1) ** 2) + np.eye(n)
+    g = HODLR_Matrix(A, leaf)
+    g.set_LRTolerance(1e-10)
+    g.set_minPivot(2.5)
+    o = oracle_mod.OracleHODLR.from_dense(A, leaf=leaf)
+    o.set_lr(1e-10, 2.5)
+    _compare_compression(g, o)
+    giters = np.array([g.block_info(b)["iters"] for b in range(g.num_blocks())])
+    assert np.array_equal(giters, o.iters())
+    assert (o.iters() > np.minimum(o.ranks(), o.iters())).any()  # rows were skipped
+    bvec = np.random.default_rng(3).standard_normal((n, 2))
+    xs, xo = g.recLU_Solve(bvec), o.solve(bvec)
+    assert np.linalg.norm(xs - xo) / np.linalg.norm(xo) <= SOLVE_TOL
+
+
+def test_cube_gaussian_16_rhs_gmres_every_precision(oracle_mod):
+    n, nrhs = 16384, 16
+    pts = uniform_cube(n, 3, 5)
+    g, o = _pair(oracle_mod, pts, "gaussian", 0.3, 1e-1, 128, 1e-8)
+    g.storeLRinTree()
+    o.compress()
+    assert np.array_equal(g.ranks(), o.ranks())
+    b = np.random.default_rng(12).standard_normal((n, nrhs))
+    xo = o.solve(b, nthreads=8)
+    x64 = g.recLU_Solve(b)
+    assert np.linalg.norm(x64 - xo) / np.linalg.norm(xo) <= SOLVE_TOL
+    for prec in ("fp64", "tf32x3", "tf32", "bf16"):
+        g.set_precision(prec)
+        g.recLU_Compute()
+        it, rel, x = _device_gmres(g, b)
+        assert rel.max() <= 1e-10, (prec, it, rel.max())
+        assert np.all(g.residual(x, b) <= 1e-10), prec
