@@ -52,6 +52,13 @@ def workload_inputs():
     return pts, b
 
 
+def workload_config(world):
+    return {"workload": WORKLOAD, "n": N_PTS, "dim": DIM, "kernel": "matern32",
+            "length_scale": LSCALE, "diag_shift": SHIFT, "leaf": LEAF, "aca_tol": TOL,
+            "nrhs": NRHS, "precision": "fp64", "parallelism": f"replicas{world}",
+            "l2": "no flush: W/V/Y panels (GBs) exceed the 126 MB L2"}
+
+
 def peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -145,84 +152,43 @@ class ClockSampler:
 
 
 # --------------------------------------------------------------- CPU leg
-def cpu_estimate(pts, blocks, budget_s, threads=1, ir_iters=0):
-    """Bounded-sample estimate of the reference algorithm's factor+solve time
-    on this host, using the CPU oracle port.
+def cpu_reference_step(pts, b, threads, kmv_rows=1024):
+    """The reference algorithm's recLU path on the host cores, measured in
+    full on the workload: storeLRinTree (partial-pivot ACA of every block and
+    the leaf blocks), recLU_Factorize and recLU_Solve of every right-hand side
+    -- the reference's recLU_TotalTime (src/HODLR_Matrix.cpp:757-775).  It
+    runs the CPU oracle, the restatement of the reference (the reference needs
+    Eigen, absent here), on `threads` threads: blocks, leaves and sibling
+    subtrees in parallel, the largest blocks with threads inside.
 
-    ACA: each level's first blocks are compressed by the oracle for a share of
-    the budget; the measured time per unit of ACA work, (m+n)*sum_t(20 + t),
-    is applied to every block's actual iteration count.  Factorization and
-    solve: the per-node work of recLU_Factorize / recLU_Solve and the leaf
-    LU + panel solve are run on random data of the workload's sizes (inner
-    node sizes scaled down where needed; that work is linear in the node size)
-    and multiplied by the node and leaf counts.  threads > 1 divides each
-    level's work by min(threads, blocks of the level), the best a block-
-    parallel port could do.
-    """
+    The direct solution does not reach the 1e-10 residual (the reference's
+    recLU_Solve stops there).  Reaching it takes HODLR-preconditioned GMRES
+    with the full-kernel product, O(N^2) entry evaluations per product on the
+    CPU; one product is timed on the first kmv_rows rows (every row costs the
+    same) and scaled by N / kmv_rows.  That estimate is reported beside the
+    measurement, never inside it."""
     from oracle import oracle as orc
     orc.build()
+    n = pts.shape[1]
     o = orc.OracleHODLR.from_kernel(pts, 1, LSCALE, shift=SHIFT, leaf=LEAF)
     o.set_lr(TOL)
-    levels = sorted({b["level"] for b in blocks})
-    alpha = 20.0
-
-    def work(K, m, n):
-        return (m + n) * (alpha * K + K * (K - 1) / 2.0)
-
-    t_start = time.time()
-    aca_budget = 0.6 * budget_s
-    per_level = aca_budget / max(1, len(levels))
-    t_aca = 0.0
-    for lv in levels:
-        idx = [i for i, b in enumerate(blocks) if b["level"] == lv]
-        spent, wdone = 0.0, 0.0
-        for i in idx:
-            if spent >= per_level:
-                break
-            it, secs, fin = o.aca_block_sample(i, per_level - spent)
-            spent += secs
-            wdone += work(it, blocks[i]["m"], blocks[i]["n"])
-        coef = spent / max(wdone, 1.0)
-        lvl_work = sum(work(blocks[i]["iters"], blocks[i]["m"], blocks[i]["n"]) for i in idx)
-        t_aca += coef * lvl_work / max(1, min(threads, len(idx)))
-    # factorization + solve: per-level node work and leaves
-    ranks_by_level = {lv: [b["rank"] for b in blocks if b["level"] == lv] for lv in levels}
-    mean_rank = {lv: float(np.mean(r)) for lv, r in ranks_by_level.items()}
-    t_fact = t_solve = 0.0
-    for lv in levels:
-        nn = len(ranks_by_level[lv]) // 2
-        s = N_PTS // (2 ** lv)
-        k = int(round(mean_rank[lv]))
-        c = 1 + int(round(sum(mean_rank[x] for x in levels if x < lv)))
-        half = s // 2
-        scale = max(1, half // 1024)
-        hs = max(1, half // scale)
-        base = orc.bench_node(2, 2, k, k, c)  # the s-independent part (S LU and solve)
-        tn = orc.bench_node(hs, hs, k, k, c)
-        t_node = scale * (tn - base) + base
-        t_fact += nn * t_node / max(1, min(threads, nn))
-        bs = orc.bench_node(2, 2, k, k, NRHS, True)
-        ts = orc.bench_node(hs, hs, k, k, NRHS, True)
-        t_solve += nn * (scale * (ts - bs) + bs) / max(1, min(threads, nn))
-    c_all = 1 + int(round(sum(mean_rank.values())))
-    nleaves = N_PTS // LEAF
-    t_leaf = orc.bench_leaf(LEAF, c_all)
-    t_fact += nleaves * t_leaf / max(1, min(threads, nleaves))
-    t_leaf_s = orc.bench_leaf(LEAF, NRHS)
-    t_solve += nleaves * t_leaf_s / max(1, min(threads, nleaves))
-    # full-kernel residual: the oracle's K x on a subset of the points, scaled
-    # by (N / n_sub)^2 (entry count); one per refinement pass plus the check
-    n_sub = 4096
-    osub = orc.OracleHODLR.from_kernel(np.ascontiguousarray(pts[:, :n_sub]), 1, LSCALE,
-                                       shift=SHIFT, leaf=LEAF)
-    xs = np.random.default_rng(0).standard_normal((n_sub, NRHS))
-    t0 = time.time()
-    osub.kernel_matvec(xs, nthreads=1)
-    t_kmv = (time.time() - t0) * (N_PTS / n_sub) ** 2 / max(1, threads)
-    t_refine = (ir_iters + 1) * t_kmv + ir_iters * t_solve
-    total = t_aca + t_fact + t_solve + t_refine
-    return {"seconds": total, "aca_s": t_aca, "factor_s": t_fact, "solve_s": t_solve,
-            "refine_s": t_refine, "kmatvec_s": t_kmv, "sample_wall_s": time.time() - t_start}
+    t0 = time.perf_counter()
+    o.compress(threads)
+    t1 = time.perf_counter()
+    o.factorize(threads)
+    t2 = time.perf_counter()
+    x = o.solve(b, threads)
+    t3 = time.perf_counter()
+    y = o.kernel_matvec_rows(x, 0, kmv_rows, threads)
+    t4 = time.perf_counter()
+    r = b[:kmv_rows] - y[:kmv_rows]
+    kmv_s = (t4 - t3) * n / kmv_rows
+    return {"compress_s": t1 - t0, "factor_s": t2 - t1, "solve_s": t3 - t2,
+            "total_s": t3 - t0, "threads": threads,
+            "direct_rel_residual_rows": float(np.linalg.norm(r) / np.linalg.norm(b[:kmv_rows])),
+            "kmatvec_s_estimate": kmv_s, "kmatvec_rows_timed": kmv_rows,
+            "to_1e-10_s_estimate": (t3 - t0) + (GMRES_ITERS_FP64 + 1) * kmv_s
+                                   + GMRES_ITERS_FP64 * (t3 - t2)}
 
 
 def cpu_model():
@@ -316,6 +282,7 @@ def run_ours(args, rank, world, local_rank):
         e1.record(stream)
         torch.cuda.synchronize()
     n_launch = launches() - l0
+    x_dev = x_d.cpu().numpy().T.copy()  # the last timed step's solution (device path)
     ms = e0.elapsed_time(e1) / args.steps
     ms_max = slowest_rank(ms, world, dev)
     clocks = clk.summary()
@@ -385,7 +352,8 @@ def run_ours(args, rank, world, local_rank):
     # accuracy (outside the timed region): full-kernel FP64 residual
     relres = g.residual(x_host, b)
     relres_direct = g.residual(x_direct, b)
-    diff_dev_host = 0.0
+    # the same solve through the host-buffer C ABI path against the device path
+    diff_dev_host = float(np.linalg.norm(x_host - x_dev) / np.linalg.norm(x_dev))
 
     blocks = gather_blocks(g)
     aca_bytes = float(np.mean(phase["aca_bytes"]))
@@ -418,10 +386,7 @@ def run_ours(args, rank, world, local_rank):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic (seeded uniform 2D cloud, k-d ordered; N(0,1) right-hand sides)",
-        "config": {"workload": WORKLOAD, "n": N_PTS, "dim": DIM, "kernel": "matern32",
-                   "length_scale": LSCALE, "diag_shift": SHIFT, "leaf": LEAF, "aca_tol": TOL,
-                   "nrhs": NRHS, "precision": "fp64", "parallelism": f"replicas{world}",
-                   "l2": "no flush: W/V/Y panels (GBs) exceed the 126 MB L2"},
+        "config": workload_config(world),
         "factor_solve_s": ms_max / 1000.0,
         "phases_s": {"lr": float(np.mean(phase["lr"])), "factor": float(np.mean(phase["fact"])),
                      "solve_refine": float(np.mean(phase["solve"])),
@@ -468,60 +433,58 @@ def run_ours(args, rank, world, local_rank):
         "gpu_launches": int(n_launch),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        est = cpu_estimate(pts, blocks, args.cpu_budget, threads=1,
-                           ir_iters=int(max(phase["ir"])))
+        threads = os.cpu_count() or 1
+        c = cpu_reference_step(pts, b, threads)
         out["cpu_baseline"] = {
-            "value": 1.0 / est["seconds"], "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": (f"CPU oracle (restatement; reference unbuildable without Eigen) on "
-                       f"{cpu_model()}: bounded ACA runs on each level's first blocks "
-                       f"+ node/leaf recLU work at the workload's sizes, "
-                       f"{est['sample_wall_s']:.1f} s of CPU work, extrapolated to the full "
-                       f"factor+solve+refinement ({est['seconds']:.1f} s: ACA {est['aca_s']:.1f}, "
-                       f"factor {est['factor_s']:.1f}, solve {est['solve_s']:.2f}, refinement "
-                       f"{est['refine_s']:.1f} of which K x {est['kmatvec_s']:.1f} per pass)"),
-            "extrapolated": True,
+            "value": 1.0 / c["total_s"], "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": (f"the whole workload's recLU path (compression, factorization and the "
+                       f"8-RHS direct solve: the reference's recLU_TotalTime) by the CPU oracle "
+                       f"(restatement; the reference needs Eigen) on {threads} threads of "
+                       f"{cpu_model()}, measured once: {c['total_s']:.1f} s (compress "
+                       f"{c['compress_s']:.1f}, factor {c['factor_s']:.1f}, solve "
+                       f"{c['solve_s']:.2f}); direct residual {c['direct_rel_residual_rows']:.1e} "
+                       f"on the first {c['kmatvec_rows_timed']} rows, not 1e-10"),
+            "measured": c,
         }
     return out
 
 
 def run_reference(args):
+    """The reference arm: the reference algorithm's recLU path on the host
+    cores (cpu_reference_step), one measured step over the whole workload --
+    its compression, factorization and direct solve (recLU_TotalTime).  The
+    line's steps / ms_per_step are those of the step that ran; --steps and
+    --warmup do not apply (one pass over the workload takes about a minute on
+    16 cores).  The reference's path stops at the direct solve, whose residual
+    (printed) is far above 1e-10, so this value is a conservative stand-in for
+    the metric: its time to 1e-10 (refinement products estimated from a timed
+    row sample) is printed beside it."""
     threads = os.cpu_count() or 1
-    pts, _ = workload_inputs()
-    blocks = reference_block_table(pts)
-    times = []
-    ir = GMRES_ITERS_FP64
-    for it in range(args.warmup + args.steps):
-        est = cpu_estimate(pts, blocks, args.ref_budget, threads=threads, ir_iters=ir)
-        if it >= args.warmup:
-            times.append(est["seconds"])
-    T = float(np.mean(times))
+    pts, b = workload_inputs()
+    t0 = time.perf_counter()
+    c = cpu_reference_step(pts, b, threads)
+    wall = time.perf_counter() - t0
+    T = c["total_s"]
     return {
         "metric": METRIC, "impl": "reference", "value": 1.0 / T, "unit": UNIT, "n_gpus": 1,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": T * 1000.0,
+        "steps": 1, "warmup": 0, "ms_per_step": T * 1000.0,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded uniform 2D cloud, k-d ordered)",
-        "config": {"workload": WORKLOAD, "n": N_PTS, "leaf": LEAF, "aca_tol": TOL, "nrhs": NRHS},
+        "data": "synthetic (seeded uniform 2D cloud, k-d ordered; N(0,1) right-hand sides)",
+        "config": workload_config(1),
         "cpu_baseline": {"value": 1.0 / T, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": (f"CPU oracle port of the reference algorithm on {cpu_model()}, "
-                                    f"{threads} threads (block-parallel), bounded sample per step "
-                                    f"extrapolated to the full factor+solve"),
-                         "extrapolated": True},
+                         "sample": (f"the whole workload, once: compression + factorization + "
+                                    f"8-RHS direct solve (recLU_TotalTime) by the CPU oracle "
+                                    f"(restatement of the reference, which needs Eigen) on "
+                                    f"{threads} threads of {cpu_model()}")},
         "e2e": {"value": 1.0 / T, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "measured": c,
+        "note": (f"steps/warmup requested {args.steps}/{args.warmup}; one measured pass ran "
+                 f"({wall:.1f} s with the residual sample).  The direct solve reaches "
+                 f"{c['direct_rel_residual_rows']:.1e}, not 1e-10; reaching 1e-10 would take "
+                 f"about {c['to_1e-10_s_estimate']:.0f} s ({GMRES_ITERS_FP64} GMRES iterations "
+                 f"with O(N^2) kernel products, estimated from a timed "
+                 f"{c['kmatvec_rows_timed']}-row sample)"),
     }
-
-
-def reference_block_table(pts):
-    """Block sizes, ranks and iteration counts of the workload from the CPU
-    oracle: a full compression with all host threads is too slow at this
-    size, so the table is read from tests-independent fixtures when present,
-    else estimated by compressing the first subtree levels."""
-    from oracle import oracle as orc
-    fix = os.path.join(ROOT, "tests", "golden", "c2_blocks.npz")
-    if os.path.exists(fix):
-        d = np.load(fix)
-        return [dict(level=int(a), m=int(m), n=int(n), rank=int(r), iters=int(i))
-                for a, m, n, r, i in zip(d["level"], d["m"], d["n"], d["rank"], d["iters"])]
-    raise RuntimeError("tests/golden/c2_blocks.npz missing")
 
 
 def run_profile_case(case):
@@ -780,8 +743,6 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision leg")
-    ap.add_argument("--cpu-budget", type=float, default=20.0)
-    ap.add_argument("--ref-budget", type=float, default=6.0)
     args = ap.parse_args()
     if args.case:
         run_profile_case(args.case)

@@ -98,48 +98,84 @@ struct LU {
   }
 };
 
-// C = A^T B.  Every C(i, j) is summed over k in order; four of them are
-// accumulated side by side (independent chains, the same sums).
+// Dense products of the factorization and solve (Eigen's GEMM in the
+// reference: its summation order is not pinned by any reference test, and
+// the factor/solve parity is checked at 1e-10, not bit for bit).  Fixed,
+// deterministic orders, written for the vector units: 4-lane partial sums.
+typedef double v4d __attribute__((vector_size(32)));
+
+static inline v4d load4(const double* p) {
+  v4d v;
+  std::memcpy(&v, p, sizeof(v));
+  return v;
+}
+static inline double hsum(v4d v) { return (v[0] + v[1]) + (v[2] + v[3]); }
+
+// C = A^T B: 4 x 4 blocks of C, each entry a 4-lane sum over k (lane k mod 4)
+// then the lanes, then the k tail in order.
 Mat matTmul(const Mat& A, const Mat& B) {
   Mat C(A.c, B.c);
-  const int K = A.r;
-  for (int j = 0; j < B.c; ++j) {
-    const double* b = &B.a[(size_t)j * B.r];
-    int i = 0;
-    for (; i + 4 <= A.c; i += 4) {
-      const double* a0 = &A.a[(size_t)i * K];
-      const double* a1 = a0 + K;
-      const double* a2 = a1 + K;
-      const double* a3 = a2 + K;
-      double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-      for (int k = 0; k < K; ++k) {
-        const double bk = b[k];
-        s0 = s0 + a0[k] * bk;
-        s1 = s1 + a1[k] * bk;
-        s2 = s2 + a2[k] * bk;
-        s3 = s3 + a3[k] * bk;
+  const int K = A.r, K4 = K & ~3;
+  auto col = [&](const Mat& M, int j) { return &M.a[(size_t)j * M.r]; };
+  for (int j0 = 0; j0 < B.c; j0 += 4) {
+    const int nj = std::min(4, B.c - j0);
+    for (int i0 = 0; i0 < A.c; i0 += 4) {
+      const int ni = std::min(4, A.c - i0);
+      v4d acc[4][4];
+      for (int x = 0; x < 4; ++x)
+        for (int y = 0; y < 4; ++y) acc[x][y] = v4d{0, 0, 0, 0};
+      const double* a[4];
+      const double* b[4];
+      for (int x = 0; x < 4; ++x) a[x] = col(A, i0 + std::min(x, ni - 1));
+      for (int y = 0; y < 4; ++y) b[y] = col(B, j0 + std::min(y, nj - 1));
+      for (int k = 0; k < K4; k += 4) {
+        v4d av[4], bv[4];
+        for (int x = 0; x < 4; ++x) av[x] = load4(a[x] + k);
+        for (int y = 0; y < 4; ++y) bv[y] = load4(b[y] + k);
+        for (int x = 0; x < 4; ++x)
+          for (int y = 0; y < 4; ++y) acc[x][y] += av[x] * bv[y];
       }
-      C(i, j) = s0;
-      C(i + 1, j) = s1;
-      C(i + 2, j) = s2;
-      C(i + 3, j) = s3;
-    }
-    for (; i < A.c; ++i) {
-      double s = 0.0;
-      for (int k = 0; k < K; ++k) s = s + A(k, i) * b[k];
-      C(i, j) = s;
+      for (int y = 0; y < nj; ++y)
+        for (int x = 0; x < ni; ++x) {
+          double s = hsum(acc[x][y]);
+          for (int k = K4; k < K; ++k) s = s + a[x][k] * b[y][k];
+          C(i0 + x, j0 + y) = s;
+        }
     }
   }
   return C;
 }
-// C = A B
+
+// C = A B: four columns of C at a time, each updated column by column of A
+// (k in order), rows in vector lanes.
 Mat matmul(const Mat& A, const Mat& B) {
   Mat C(A.r, B.c);
-  for (int j = 0; j < B.c; ++j)
-    for (int k = 0; k < A.c; ++k) {
-      double b = B(k, j);
-      for (int i = 0; i < A.r; ++i) C(i, j) = C(i, j) + A(i, k) * b;
+  const int R = A.r;
+  for (int j0 = 0; j0 < B.c; j0 += 4) {
+    const int nj = std::min(4, B.c - j0);
+    double* c[4];
+    for (int y = 0; y < 4; ++y) c[y] = &C.a[(size_t)(j0 + std::min(y, nj - 1)) * R];
+    if (nj == 4) {
+      for (int k = 0; k < A.c; ++k) {
+        const double* ak = &A.a[(size_t)k * R];
+        const double b0 = B(k, j0), b1 = B(k, j0 + 1), b2 = B(k, j0 + 2), b3 = B(k, j0 + 3);
+        for (int i = 0; i < R; ++i) {
+          const double x = ak[i];
+          c[0][i] = c[0][i] + x * b0;
+          c[1][i] = c[1][i] + x * b1;
+          c[2][i] = c[2][i] + x * b2;
+          c[3][i] = c[3][i] + x * b3;
+        }
+      }
+    } else {
+      for (int y = 0; y < nj; ++y)
+        for (int k = 0; k < A.c; ++k) {
+          const double* ak = &A.a[(size_t)k * R];
+          const double b = B(k, j0 + y);
+          for (int i = 0; i < R; ++i) c[y][i] = c[y][i] + ak[i] * b;
+        }
     }
+  }
   return C;
 }
 
