@@ -275,6 +275,186 @@ __device__ void residual_pass(const AcaLaunch& L, const AcaBlock& B, double* P, 
   }
 }
 
+// ---------------------------------------------------------------- bulk-copy ring
+// The group levels stream their panel slices through shared memory: a ring
+// of TMA_S tiles, each TMA_BC panel columns x TMA_BR rows, filled by
+// cp.async.bulk copies (one per column) that complete on the tile's `full`
+// mbarrier; every warp releases a tile on its `empty` mbarrier and thread 0
+// then refills it with the tile TMA_S ahead.  Rows start on an even global
+// index so that every copy is 16-byte aligned (requires an even N).
+constexpr int TMA_BC = 4;
+constexpr int TMA_S = 4;
+constexpr int TMA_NT = 256, TMA_E = 4, TMA_BR = TMA_NT * TMA_E;
+constexpr size_t TMA_RING_BYTES = sizeof(double) * TMA_S * TMA_BC * TMA_BR;  // 128 KB
+
+struct Ring {
+  double* buf;      // TMA_S tiles of TMA_BC x TMA_BR doubles, column u at u * TMA_BR
+  uint64_t* full;   // per tile: its copies landed (1 arrival + transaction bytes)
+  uint64_t* empty;  // per tile: every warp is done with it (NT / 32 arrivals)
+  uint32_t t;       // tiles this CTA has consumed (the same in every thread)
+};
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait on an mbarrier phase.  On giving up it raises DEV_ERR_TIMEOUT
+// and returns; once the error word is set, later waits give up at once, so a
+// failed launch ends quickly (its next group barrier fails).
+__device__ void mbar_wait_bounded(uint64_t* bar, uint32_t parity, unsigned* err) {
+  for (uint32_t polls = 0;; ++polls) {
+    if (mbar_try(bar, parity)) return;
+    if (polls >= (1u << 20) || (polls >= 64 && *(volatile unsigned*)err)) {
+      atomicOr(err, DEV_ERR_TIMEOUT);
+      return;
+    }
+    if (polls >= 64) __nanosleep(64);
+  }
+}
+
+// Thread 0: tile gt of the ring, `nc` columns from column l0 of P, `count`
+// rows from row0 (count even, row0 on an even global row).
+__device__ void ring_issue(Ring& R, uint32_t gt, const double* P, int64_t ld, int row0, int count,
+                           int l0, int nc, unsigned* err) {
+  const int slot = (int)(gt % TMA_S);
+  if (gt >= (uint32_t)TMA_S) mbar_wait_bounded(&R.empty[slot], ((gt / TMA_S) + 1) & 1, err);
+  const uint32_t bytes = (uint32_t)count * (uint32_t)sizeof(double);
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
+                   smem_addr(&R.full[slot])),
+               "r"(bytes * (uint32_t)nc)
+               : "memory");
+  double* dst = R.buf + (size_t)slot * TMA_BC * TMA_BR;
+  for (int u = 0; u < nc; ++u)
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+            "r"(smem_addr(dst + u * TMA_BR)),
+        "l"(P + row0 + (int64_t)(l0 + u) * ld), "r"(bytes), "r"(smem_addr(&R.full[slot]))
+        : "memory");
+}
+
+// residual_pass with the panel slice streamed through the ring.  gbase: the
+// global row of P[0] (the block's first column for V, first row for W).
+// The same arithmetic as residual_pass, element for element: the residual
+// sums in l order with separately rounded products and sums, the argmax in
+// increasing index per thread; the fused dots add their chunk partials in a
+// GPU order, as there.
+template <int NT, int E, bool ROW>
+__device__ void residual_pass_ring(const AcaLaunch& L, const AcaBlock& B, double* P, int lo,
+                                   int hi, int k, const double* __restrict__ coef, bool dots,
+                                   double* __restrict__ dotw, int ldd, int fixed,
+                                   const double* xfix, double scale, const unsigned char* chosen,
+                                   double& bv, int& bi, int& cand, double& sq, bool& nonfinite,
+                                   const EntrySrc& S, Ring& R, int gbase) {
+  static_assert(NT * E == TMA_BR, "one chunk is one ring tile high");
+  if (lo >= hi) return;
+  const int64_t ld = L.ld;
+  const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
+  const double minPiv = L.minPivot;
+  const int x0 = lo - ((gbase + lo) & 1);  // first chunk row: even global index
+  const int nchunks = (hi - x0 + TMA_BR - 1) / TMA_BR;
+  const int tpc = (k + TMA_BC - 1) / TMA_BC;  // tiles per chunk
+  const uint32_t T = (uint32_t)nchunks * (uint32_t)tpc;
+  const int kd = dots ? k - 1 : 0;
+  auto issue = [&](uint32_t i) {
+    const int c = (int)(i / tpc), l0 = (int)(i % tpc) * TMA_BC;
+    const int row0 = x0 + c * TMA_BR;
+    const int count = (min(TMA_BR, hi - row0) + 1) & ~1;
+    ring_issue(R, R.t + i, P, ld, row0, count, l0, min(TMA_BC, k - l0), L.err);
+  };
+  if (tid == 0 && T > 0) {
+    // this CTA's earlier generic stores to the panel (after the caller's
+    // __syncthreads) before the bulk copies read it
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+    for (uint32_t i = 0; i < T && i < (uint32_t)TMA_S; ++i) issue(i);
+  }
+  uint32_t i = 0;
+  for (int c = 0; c < nchunks; ++c) {
+    const int jb = x0 + c * TMA_BR;
+    int jj[E];
+    bool ok[E];
+    double s[E], vp[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      jj[e] = jb + tid + e * NT;
+      ok[e] = jj[e] >= lo && jj[e] < hi;
+      s[e] = 0.0;
+      vp[e] = (dots && ok[e]) ? P[jj[e] + (int64_t)(k - 1) * ld] : 0.0;
+    }
+    for (int l0 = 0; l0 < k; l0 += TMA_BC, ++i) {
+      const uint32_t gt = R.t + i;
+      const int slot = (int)(gt % TMA_S);
+      mbar_wait_bounded(&R.full[slot], (gt / TMA_S) & 1, L.err);
+      const double* tile = R.buf + (size_t)slot * TMA_BC * TMA_BR;
+      const int nc = min(TMA_BC, k - l0);
+      double v[TMA_BC][E];
+#pragma unroll
+      for (int u = 0; u < TMA_BC; ++u)
+#pragma unroll
+        for (int e = 0; e < E; ++e)
+          v[u][e] = (u < nc && ok[e]) ? tile[u * TMA_BR + tid + e * NT] : 0.0;
+#pragma unroll
+      for (int u = 0; u < TMA_BC; ++u) {
+        if (u >= nc) break;
+        const double cf = coef[l0 + u];
+#pragma unroll
+        for (int e = 0; e < E; ++e) s[e] = __dadd_rn(s[e], __dmul_rn(cf, v[u][e]));
+      }
+      if (dots) {
+#pragma unroll
+        for (int u = 0; u < TMA_BC; ++u) {
+          if (l0 + u >= kd) break;
+          double d = 0.0;
+#pragma unroll
+          for (int e = 0; e < E; ++e) d = fma(v[u][e], vp[e], d);
+          d = warp_sum(d);
+          if (lane == 0) {
+            if (c == 0)
+              dotw[w * ldd + l0 + u] = d;
+            else
+              dotw[w * ldd + l0 + u] += d;
+          }
+        }
+      }
+      __syncwarp();
+      if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(
+                                      smem_addr(&R.empty[slot]))
+                                  : "memory");
+      if (tid == 0 && i + TMA_S < T) issue(i + TMA_S);
+    }
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      if (!ok[e]) continue;
+      const int j = jj[e];
+      double ent = ROW ? src_entry_xi(S, xfix, fixed, B.c0 + j)
+                       : src_entry_xj(S, xfix, B.r0 + j, fixed);
+      double r = __dsub_rn(ent, s[e]);
+      double stored = ROW ? r : __dmul_rn(scale, r);
+      P[j + (int64_t)k * ld] = stored;
+      sq = fma(stored, stored, sq);
+      double a = fabs(r);
+      nonfinite |= !isfinite(r);
+      if (a > bv) {
+        bv = a;
+        bi = j;
+      }
+      if (cand == INT_MAX && a > minPiv && __ldcg(chosen + j) == 0) cand = j;
+    }
+  }
+  R.t += T;
+}
+
 // Partial dots of step k-1 over this CTA's slices when they could not be
 // fused into a residual pass (a zero residual row, or the capacity limit).
 template <int NT>
@@ -320,10 +500,16 @@ __device__ double resolve_eps(Shared& sh, const AcaLaunch& L, const AcaBlock& B,
   return sqrt(swp) * sqrt(svp) / sqrt(frob2);
 }
 
-template <int NT, int E>
-__global__ void __launch_bounds__(NT, (NT == 256 ? 2 : 4)) aca_kernel(AcaLaunch L) {
-  extern __shared__ double dyn[];  // row[kcap], then (unless L.dotg) per-warp dots[NT/32][kcap]
+// RING: the residual passes stream their panel slices through the bulk-copy
+// ring (group levels of an even N); the dynamic shared memory then starts
+// with the ring's TMA_RING_BYTES.
+template <int NT, int E, bool RING>
+__global__ void __launch_bounds__(NT, (RING ? 1 : (NT == 256 ? 2 : 4))) aca_kernel(AcaLaunch L) {
+  extern __shared__ __align__(128) double dyn_all[];
   __shared__ Shared sh;
+  __shared__ __align__(8) uint64_t ring_full[TMA_S], ring_empty[TMA_S];
+  double* dyn = RING ? dyn_all + TMA_RING_BYTES / sizeof(double) : dyn_all;
+  // dyn: row[kcap], then (unless L.dotg) per-warp dots[NT/32][kcap]
   constexpr int NW = NT / 32;
   const int b = L.cta_block ? (blockIdx.x < (unsigned)L.ncta ? L.cta_block[blockIdx.x] : L.nblocks)
                             : (int)(blockIdx.x / L.G);
@@ -359,6 +545,18 @@ __global__ void __launch_bounds__(NT, (NT == 256 ? 2 : 4)) aca_kernel(AcaLaunch 
   double swp = st->swp, svp = st->svp;
   int near = st->near, pending = st->pending;
   bool nonfinite = false;
+  Ring ring{dyn_all, ring_full, ring_empty, 0};
+  if (RING) {
+    if (tid == 0) {
+      for (int q = 0; q < TMA_S; ++q) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&ring_full[q])));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&ring_empty[q])),
+                     "r"(NT / 32));
+      }
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+  }
 
   auto note_margin = [&](int kcount) {
     if (kcount < ub) {
@@ -407,8 +605,12 @@ __global__ void __launch_bounds__(NT, (NT == 256 ? 2 : 4)) aca_kernel(AcaLaunch 
     }
     double bv = -1.0, sv = 0.0;
     int bi = INT_MAX, cand = INT_MAX;
-    residual_pass<NT, E, true>(L, B, B.V, j_lo, j_hi, k, row, fuse, dotw, ldd, gi, xi, 1.0, B.cC,
-                               bv, bi, cand, sv, nonfinite, S);
+    if constexpr (RING)
+      residual_pass_ring<NT, E, true>(L, B, B.V, j_lo, j_hi, k, row, fuse, dotw, ldd, gi, xi, 1.0,
+                                      B.cC, bv, bi, cand, sv, nonfinite, S, ring, B.c0);
+    else
+      residual_pass<NT, E, true>(L, B, B.V, j_lo, j_hi, k, row, fuse, dotw, ldd, gi, xi, 1.0,
+                                 B.cC, bv, bi, cand, sv, nonfinite, S);
     __syncthreads();
     if (fuse)  // CTA partial dots of V, warps summed in order
       for (int l = tid; l < k - 1; l += NT) {
@@ -481,8 +683,12 @@ __global__ void __launch_bounds__(NT, (NT == 256 ? 2 : 4)) aca_kernel(AcaLaunch 
     bi = INT_MAX;
     cand = INT_MAX;
     double sw = 0.0;
-    residual_pass<NT, E, false>(L, B, B.W, i_lo, i_hi, k, row, fuse, dotw, ldd, gj, xj, piv,
-                                B.cR, bv, bi, cand, sw, nonfinite, S);
+    if constexpr (RING)
+      residual_pass_ring<NT, E, false>(L, B, B.W, i_lo, i_hi, k, row, fuse, dotw, ldd, gj, xj,
+                                       piv, B.cR, bv, bi, cand, sw, nonfinite, S, ring, B.r0);
+    else
+      residual_pass<NT, E, false>(L, B, B.W, i_lo, i_hi, k, row, fuse, dotw, ldd, gj, xj, piv,
+                                  B.cR, bv, bi, cand, sw, nonfinite, S);
     __syncthreads();
     if (fuse)
       for (int l = tid; l < k - 1; l += NT) {
@@ -614,19 +820,27 @@ __global__ void __launch_bounds__(NT, (NT == 256 ? 2 : 4)) aca_kernel(AcaLaunch 
 
 }  // namespace
 
-static size_t aca_smem(int nt, int kcap_max, bool global_dots) {
-  return sizeof(double) * (size_t)(global_dots ? 1 : 1 + nt / 32) * (size_t)kcap_max;
+static size_t aca_smem(int nt, int kcap_max, bool global_dots, bool ring) {
+  return (ring ? TMA_RING_BYTES : 0) +
+         sizeof(double) * (size_t)(global_dots ? 1 : 1 + nt / 32) * (size_t)kcap_max;
 }
 
 // The per-warp dot partials move to global memory once they would take more
-// than 100 KB of shared memory per CTA: beyond that fewer than two 256-thread
-// CTAs fit on an SM, and past 227 KB none would.
-bool aca_dots_global(int nt, int kcap_max) {
-  return aca_smem(nt, kcap_max, false) > 100 * 1024;
+// than 100 KB of shared memory per CTA (without the ring: beyond that fewer
+// than two 256-thread CTAs fit on an SM), or with the ring once the CTA's
+// shared memory would pass 220 KB.
+bool aca_dots_global(int nt, int kcap_max, bool ring) {
+  return ring ? aca_smem(nt, kcap_max, false, true) > 220 * 1024
+              : aca_smem(nt, kcap_max, false, false) > 100 * 1024;
 }
 
-size_t aca_smem_bytes(int nt, int kcap_max) {
-  return aca_smem(nt, kcap_max, aca_dots_global(nt, kcap_max));
+size_t aca_smem_bytes(int nt, int kcap_max, bool ring) {
+  return aca_smem(nt, kcap_max, aca_dots_global(nt, kcap_max, ring), ring);
+}
+
+static void* aca_fn(int nt, bool ring) {
+  if (ring) return (void*)aca_kernel<TMA_NT, TMA_E, true>;
+  return nt == 256 ? (void*)aca_kernel<256, 4, false> : (void*)aca_kernel<128, 2, false>;
 }
 
 // Dynamic shared memory above 48 KB, and the largest shared-memory carveout:
@@ -642,10 +856,12 @@ static int set_smem(void* fn, size_t smem) {
 }
 
 int aca_launch(const AcaLaunch& L, int nt, int kcap_max, bool cooperative, cudaStream_t s) {
-  const size_t smem = aca_smem(nt, kcap_max, L.dotg != nullptr);
+  const bool ring = L.ring != 0;
+  if (ring && (nt != TMA_NT || (L.ld & 1))) return (int)cudaErrorInvalidValue;
+  const size_t smem = aca_smem(nt, kcap_max, L.dotg != nullptr, ring);
   dim3 grid(L.cta_block ? L.ncta : L.nblocks * L.G), block(nt);
   void* args[] = {(void*)&L};
-  void* fn = nt == 256 ? (void*)aca_kernel<256, 4> : (void*)aca_kernel<128, 2>;
+  void* fn = aca_fn(nt, ring);
   if (int e = set_smem(fn, smem)) return e;
   cudaError_t e = cooperative ? cudaLaunchCooperativeKernel(fn, grid, block, args, smem, s)
                               : cudaLaunchKernel(fn, grid, block, args, smem, s);
@@ -653,9 +869,9 @@ int aca_launch(const AcaLaunch& L, int nt, int kcap_max, bool cooperative, cudaS
   return e == cudaSuccess ? 0 : (int)e;
 }
 
-int aca_max_coresident(int nt, int kcap_max, int* per_sm) {
-  const size_t smem = aca_smem_bytes(nt, kcap_max);
-  void* fn = nt == 256 ? (void*)aca_kernel<256, 4> : (void*)aca_kernel<128, 2>;
+int aca_max_coresident(int nt, int kcap_max, bool ring, int* per_sm) {
+  const size_t smem = aca_smem_bytes(nt, kcap_max, ring);
+  void* fn = aca_fn(nt, ring);
   *per_sm = 0;
   if (int e = set_smem(fn, smem)) return e;
   int nb = 0;

@@ -34,9 +34,9 @@
 #include "rank_mlp.h"
 
 int aca_launch(const AcaLaunch& L, int nt, int kcap_max, bool cooperative, cudaStream_t s);
-int aca_max_coresident(int nt, int kcap_max, int* per_sm);
-bool aca_dots_global(int nt, int kcap_max);
-size_t aca_smem_bytes(int nt, int kcap_max);
+int aca_max_coresident(int nt, int kcap_max, bool ring, int* per_sm);
+bool aca_dots_global(int nt, int kcap_max, bool ring);
+size_t aca_smem_bytes(int nt, int kcap_max, bool ring);
 
 namespace {
 
@@ -63,6 +63,10 @@ struct Level {
   std::vector<AcaState> st;
   int G = 1;
   int kmax = 0, coff = 0;
+  // K^-1 U of the level's blocks (N x kmax, ld N): its own allocation, or
+  // (y_alias) the first kmax columns of W, overwritten in place
+  double* Yl = nullptr;
+  bool y_alias = false;
   // factorization
   double* S = nullptr;
   int* piv = nullptr;
@@ -228,6 +232,7 @@ struct hodlr_handle_s {
   std::vector<Level> lv;
   std::vector<int> cap_hint;  // initial W/V columns per level (0 = default)
   int gemm_prec = HODLR_GEMM_FP64;  // arithmetic of the Woodbury products
+  bool aca_ring = true;  // group-level ACA panels through the bulk-copy ring
   std::vector<int> leaf_min, leaf_size;
   int* d_leaf_min = nullptr;
   int* d_leaf_size = nullptr;
@@ -238,8 +243,11 @@ struct hodlr_handle_s {
   double* d_lu = nullptr;
   int* d_perm = nullptr;
   int smax = 0;
-  double* Y = nullptr;
-  int64_t C = 0;
+  int64_t C = 0;  // sum over levels of kmax: the columns of all K^-1 U panels
+  // factor in place: -1 only when a separate K^-1 U panel cannot be
+  // allocated, 0 never, 1 always (hodlr_set_factor_in_place)
+  int in_place = -1;
+  bool w_consumed = false;  // some level's W holds K^-1 U: recompress before refactoring
   double* ws = nullptr;  // GEMM split-K / kmatvec workspace
   int64_t ws_cap = 0;
   double* Z = nullptr;  // per-level Schur right-hand sides (factor)
@@ -342,7 +350,13 @@ void free_factor(hodlr_t h) {
   dfree(h, h->d_lu);
   dfree(h, h->d_lu_off);
   dfree(h, h->d_perm);
-  dfree(h, h->Y);
+  for (auto& L : h->lv) {
+    if (!L.y_alias) dfree(h, L.Yl);
+    L.Yl = nullptr;
+    L.y_alias = false;
+  }
+  if (h->w_consumed) h->compressed = false;  // the U panels are gone: compress again
+  h->w_consumed = false;
   h->factored = false;
 }
 
@@ -624,7 +638,7 @@ bool level_done(const Level& L) {
 // One ACA launch over `blocks`: groups of G CTAs each, or, with `groups`,
 // groups[i] CTAs for block i (a CTA table maps CTAs to blocks).
 int run_aca(hodlr_t h, std::vector<AcaBlock>& blocks, int G, int nt, int kcap_max,
-            const std::vector<int>* groups = nullptr) {
+            bool ring = false, const std::vector<int>* groups = nullptr) {
   const int nb = (int)blocks.size();
   if (nb == 0) return HODLR_OK;
   int ncta = nb * G;
@@ -683,9 +697,10 @@ int run_aca(hodlr_t h, std::vector<AcaBlock>& blocks, int G, int nt, int kcap_ma
   L.ncta = ncta;
   L.dotg = nullptr;
   L.dotg_stride = 0;
-  if (aca_smem_bytes(nt, kcap_max) > 227 * 1024)
+  L.ring = ring ? 1 : 0;
+  if (aca_smem_bytes(nt, kcap_max, ring) > 227 * 1024)
     return fail(h, HODLR_ERR_UNSUPPORTED, "block rank above the shared-memory limit of ACA");
-  if (aca_dots_global(nt, kcap_max)) {
+  if (aca_dots_global(nt, kcap_max, ring)) {
     L.dotg_stride = (int64_t)(nt / 32) * kcap_max;
     const int64_t dneed = L.dotg_stride * ncta;
     if (dneed > h->dotg_cap) {
@@ -869,7 +884,7 @@ int do_compress(hodlr_t h) {
   };
   auto pred_or = [&](int l, int q) -> int64_t { return have_pred ? pred(l, q) + 1 : 1; };
   int per_sm = 0;
-  if (aca_max_coresident(256, 256, &per_sm))
+  if (aca_max_coresident(256, 256, false, &per_sm))
     return fail(h, HODLR_ERR_CUDA, "occupancy query failed");
   const int P0 = std::max(1, per_sm) * h->num_sms;
   std::vector<int> pooled_levels, group_levels;
@@ -922,10 +937,16 @@ int do_compress(hodlr_t h) {
     int rc = init_level(h, L, guess);
     if (rc) return rc;
     for (int round = 0; round < 64; ++round) {
-      int ps = 0;
-      if (aca_max_coresident(256, L.kcap, &ps))
-        return fail(h, HODLR_ERR_CUDA, "occupancy query failed");
+      // the group levels stream their panels through the bulk-copy ring
+      // (16-byte aligned columns need an even N) while that still leaves at
+      // least two of its one-per-SM CTAs to every block
       const int nb = L.nblocks();
+      int ps = 0, ps_ring = 0;
+      if (aca_max_coresident(256, L.kcap, false, &ps) ||
+          aca_max_coresident(256, L.kcap, true, &ps_ring))
+        return fail(h, HODLR_ERR_CUDA, "occupancy query failed");
+      const bool ring = h->aca_ring && (h->n % 2 == 0) && ps_ring * h->num_sms >= 2 * nb;
+      if (ring) ps = ps_ring;
       // equal groups: CTAs sized by predicted work measured 2-8% slower on
       // 3D clouds than equal groups (per-step latency, not streamed bytes,
       // sets a block's time)
@@ -934,7 +955,7 @@ int do_compress(hodlr_t h) {
       for (;;) {  // a cooperative launch the driver refuses is retried with half the groups
         L.G = G;
         for (int q = 0; q < nb; ++q) fill_block(h, L, q, bl[q]);
-        rc = run_aca(h, bl, G, G > 1 ? 256 : 128, L.kcap);
+        rc = run_aca(h, bl, G, G > 1 || ring ? 256 : 128, L.kcap, ring);
         if (rc != HODLR_ERR_RETRY_SMALLER) break;
         if (G == 1) return fail(h, HODLR_ERR_CUDA, "aca_launch: cooperative launch refused");
         G = std::max(1, G / 2);
@@ -1016,14 +1037,18 @@ int run_nn(hodlr_t h, const DevPlan& P) {
   return umma_nn_sub_launch(h->gemm_prec, P.probs, P.tiles, P.ntiles, h->d_err, h->stream);
 }
 
-__global__ void y_init_kernel(double* Y, int64_t ldy, int coff, const double* W, int64_t ldw,
-                              const int* r0s, const int* ms, const int* ranks, int nb) {
+// Y_l[rows of block q, c] = W_l[rows, c] for c < rank(q), 0 for rank(q) <= c
+// < kmax.  With Y == W (in place) only the padding is written.
+__global__ void y_init_kernel(double* Y, const double* W, int64_t ld, int kmax, const int* r0s,
+                              const int* ms, const int* ranks, int nb) {
   int q = blockIdx.y;
   if (q >= nb) return;
   const int r0 = r0s[q], m = ms[q], rank = ranks[q];
-  for (int c = blockIdx.z; c < rank; c += gridDim.z)
+  for (int c = blockIdx.z; c < kmax; c += gridDim.z) {
+    if (c < rank && Y == W) continue;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x)
-      Y[(int64_t)(coff + c) * ldy + r0 + i] = W[(int64_t)c * ldw + r0 + i];
+      Y[(int64_t)c * ld + r0 + i] = c < rank ? W[(int64_t)c * ld + r0 + i] : 0.0;
+  }
 }
 
 // log|det| pieces of the factorization: per leaf LU (column-major s x s,
@@ -1085,9 +1110,9 @@ __global__ void leaf_identity_kernel(double* X, int64_t ldx, const int* leaf_min
 
 int do_factorize(hodlr_t h) {
   if (h->factored) return HODLR_OK;
+  free_factor(h);  // first: a factorization that overwrote W also drops the compression
   int rc = do_compress(h);
   if (rc) return rc;
-  free_factor(h);
   const int64_t N = h->n;
   CK(cudaEventRecord(h->ev0, h->stream));
   // leaves: assemble + LU
@@ -1116,11 +1141,11 @@ int do_factorize(hodlr_t h) {
     if (e) return cuda_fail(h, (cudaError_t)e, "leaf_lu_launch");
     h->nlaunch += 1;
   }
-  // Y = [U panels of every level], zero padded
+  // Y_l = the U panel of every level, zero padded to kmax columns: its own
+  // allocation, or W_l itself (in place) when that cannot be had
   if (h->C > 0) {
-    CK(dalloc(h, &h->Y, (size_t)(N * h->C)));
-    CK(cudaMemsetAsync(h->Y, 0, sizeof(double) * N * h->C, h->stream));
     for (auto& L : h->lv) {
+      if (L.kmax == 0) continue;
       const int nb = L.nblocks();
       std::vector<int> r0s(nb), ms(nb), rk(nb);
       for (int q = 0; q < nb; ++q) {
@@ -1129,6 +1154,20 @@ int do_factorize(hodlr_t h) {
         r0s[q] = r0;
         ms[q] = m;
         rk[q] = level_rank(L, q);
+      }
+      L.y_alias = h->in_place == 1;
+      if (!L.y_alias) {
+        cudaError_t ea = dalloc(h, &L.Yl, (size_t)(N * L.kmax));
+        if (ea == cudaErrorMemoryAllocation && h->in_place == -1) {
+          cudaGetLastError();
+          L.y_alias = true;
+        } else if (ea != cudaSuccess) {
+          return cuda_fail(h, ea, "K^-1 U panel");
+        }
+      }
+      if (L.y_alias) {
+        L.Yl = L.W;
+        h->w_consumed = true;
       }
       int *d_r0 = nullptr, *d_m = nullptr, *d_rk = nullptr;
       CK(dalloc(h, &d_r0, nb));
@@ -1140,7 +1179,7 @@ int do_factorize(hodlr_t h) {
       int maxm = 0;
       for (int m : ms) maxm = std::max(maxm, m);
       dim3 grid(std::min(64, (maxm + 255) / 256), nb, std::min(L.kmax, 64));
-      y_init_kernel<<<grid, 256, 0, h->stream>>>(h->Y, N, L.coff, L.W, N, d_r0, d_m, d_rk, nb);
+      y_init_kernel<<<grid, 256, 0, h->stream>>>(L.Yl, L.W, N, L.kmax, d_r0, d_m, d_rk, nb);
       CK(cudaGetLastError());
       h->nlaunch += 1;
       CK(cudaStreamSynchronize(h->stream));
@@ -1150,10 +1189,11 @@ int do_factorize(hodlr_t h) {
     }
     // Y <- blockdiag(leaf)^-1 Y on every column.  Each leaf's inverse is
     // formed once (its LU applied to identity columns, smax columns in all)
-    // and applied as a grouped GEMM, Y_new = A_leaf^-1 Y: C columns of
+    // and applied as a grouped GEMM, Y_new = A_leaf^-1 Y: the columns of
     // triangular substitution per leaf become one pass of dense products.
     const int sm = h->smax;
-    const int CH = (int)std::min<int64_t>(h->C, 512);  // Y columns per product pass
+    int CH = 1;  // Y columns per product pass
+    for (auto& L : h->lv) CH = std::max(CH, std::min(L.kmax, 512));
     double *Xinv = nullptr, *Y2 = nullptr;
     CK(dalloc(h, &Xinv, (size_t)(N * sm)));
     CK(dalloc(h, &Y2, (size_t)(N * CH)));
@@ -1171,38 +1211,45 @@ int do_factorize(hodlr_t h) {
     S.ncols = sm;
     int e = leaf_solve_launch(S, nl, sm, h->stream);
     if (e) return cuda_fail(h, (cudaError_t)e, "leaf_solve_launch");
-    // in passes of CH columns through an N x CH buffer (memory: N * CH, not N * C)
+    // per level, in passes of CH columns through an N x CH buffer
     GemmProblem* d_probs = nullptr;
     int4* d_tiles = nullptr;
+    size_t tiles_cap = 0;
     CK(dalloc(h, &d_probs, (size_t)nl));
-    for (int64_t c0 = 0; c0 < h->C; c0 += CH) {
-      const int nc = (int)std::min<int64_t>(CH, h->C - c0);
-      std::vector<GemmProblem> probs;
-      for (int p = 0; p < nl; ++p) {
-        const int r0 = h->leaf_min[p], s = h->leaf_size[p];
-        GemmProblem g{};
-        g.A = Xinv + r0;
-        g.B = h->Y + r0 + c0 * N;
-        g.C = Y2 + r0;
-        g.M = s;
-        g.N = nc;
-        g.K = s;
-        g.lda = (int)N;
-        g.ldb = (int)N;
-        g.ldc = (int)N;
-        probs.push_back(g);
+    for (auto& L : h->lv) {
+      for (int c0 = 0; c0 < L.kmax; c0 += CH) {
+        const int nc = std::min(CH, L.kmax - c0);
+        std::vector<GemmProblem> probs;
+        for (int p = 0; p < nl; ++p) {
+          const int r0 = h->leaf_min[p], s = h->leaf_size[p];
+          GemmProblem g{};
+          g.A = Xinv + r0;
+          g.B = L.Yl + r0 + (int64_t)c0 * N;
+          g.C = Y2 + r0;
+          g.M = s;
+          g.N = nc;
+          g.K = s;
+          g.lda = (int)N;
+          g.ldb = (int)N;
+          g.ldc = (int)N;
+          probs.push_back(g);
+        }
+        std::vector<int4> tiles;
+        int64_t ws = 0;
+        gemm_plan(probs, tiles, ws, false, 0);
+        if (tiles.size() > tiles_cap) {
+          dfree(h, d_tiles);
+          CK(dalloc(h, &d_tiles, tiles.size()));
+          tiles_cap = tiles.size();
+        }
+        CK(h2d(h, d_probs, probs.data(), sizeof(GemmProblem) * probs.size()));
+        CK(h2d(h, d_tiles, tiles.data(), sizeof(int4) * tiles.size()));
+        e = gemm_nn_launch(d_probs, d_tiles, (int)tiles.size(), h->stream);
+        if (e) return cuda_fail(h, (cudaError_t)e, "leaf inverse product");
+        CK(cudaMemcpyAsync(L.Yl + (int64_t)c0 * N, Y2, sizeof(double) * N * nc,
+                           cudaMemcpyDeviceToDevice, h->stream));
+        h->nlaunch += 1;
       }
-      std::vector<int4> tiles;
-      int64_t ws = 0;
-      gemm_plan(probs, tiles, ws, false, 0);
-      if (c0 == 0) CK(dalloc(h, &d_tiles, tiles.size()));  // the same count every full pass
-      CK(h2d(h, d_probs, probs.data(), sizeof(GemmProblem) * probs.size()));
-      CK(h2d(h, d_tiles, tiles.data(), sizeof(int4) * tiles.size()));
-      e = gemm_nn_launch(d_probs, d_tiles, (int)tiles.size(), h->stream);
-      if (e) return cuda_fail(h, (cudaError_t)e, "leaf inverse product");
-      CK(cudaMemcpyAsync(h->Y + c0 * N, Y2, sizeof(double) * N * nc, cudaMemcpyDeviceToDevice,
-                         h->stream));
-      h->nlaunch += 1;
     }
     h->nlaunch += 2;
     dfree(h, Y2);
@@ -1243,34 +1290,44 @@ int do_factorize(hodlr_t h) {
       CK(dalloc(h, &h->Z, (size_t)z_tot));
       h->z_cap = z_tot;
     }
-    // Z_h = V_h^T Y[rows_h, 0 : coff + rank(U_h)]
+    // Z_h = V_h^T [Y_0 .. Y_{l-1} | own U columns of Y_l] on the node's rows:
+    // Z columns [coff_a, coff_a + kmax_a) from level a < l, then the own
+    // rank(U_h) columns at coff_l, one grouped-GEMM problem per panel
     std::vector<GemmProblem> tn;
     for (int p = 0; p < nn; ++p) {
       const SchurNode& sn = L.nodes[p];
       const int sd = sn.kb + sn.kt;
       const int mn = L.nmin[p], sp = L.nsplit[p], mx = L.nmax[p];
-      GemmProblem a{};
-      a.A = L.V + mn;  // V of the bottom block lives on the top rows
-      a.M = sn.kb;
-      a.K = sp - mn + 1;
-      a.lda = (int)N;
-      a.B = h->Y + mn;
-      a.N = L.coff + sn.kt;
-      a.ldb = (int)N;
-      a.C = h->Z + sn.z_off;
-      a.ldc = sd;
-      tn.push_back(a);
-      GemmProblem b{};
-      b.A = L.V + sp + 1;  // V of the top block lives on the bottom rows
-      b.M = sn.kt;
-      b.K = mx - sp;
-      b.lda = (int)N;
-      b.B = h->Y + sp + 1;
-      b.N = L.coff + sn.kb;
-      b.ldb = (int)N;
-      b.C = h->Z + sn.z_off + sn.kb;
-      b.ldc = sd;
-      tn.push_back(b);
+      for (int a = 0; a <= l; ++a) {
+        const Level& A = h->lv[a];
+        const int ncols_t = a < l ? A.kmax : sn.kt, ncols_b = a < l ? A.kmax : sn.kb;
+        if (ncols_t > 0 && sn.kb > 0) {
+          GemmProblem t{};
+          t.A = L.V + mn;  // V of the bottom block lives on the top rows
+          t.M = sn.kb;
+          t.K = sp - mn + 1;
+          t.lda = (int)N;
+          t.B = A.Yl + mn;
+          t.N = ncols_t;
+          t.ldb = (int)N;
+          t.C = h->Z + sn.z_off + (int64_t)A.coff * sd;
+          t.ldc = sd;
+          tn.push_back(t);
+        }
+        if (ncols_b > 0 && sn.kt > 0) {
+          GemmProblem b{};
+          b.A = L.V + sp + 1;  // V of the top block lives on the bottom rows
+          b.M = sn.kt;
+          b.K = mx - sp;
+          b.lda = (int)N;
+          b.B = A.Yl + sp + 1;
+          b.N = ncols_b;
+          b.ldb = (int)N;
+          b.C = h->Z + sn.z_off + (int64_t)A.coff * sd + sn.kb;
+          b.ldc = sd;
+          tn.push_back(b);
+        }
+      }
     }
     int rc2 = upload_plan(h, tn, true, L.tn);
     if (rc2) return rc2;
@@ -1292,34 +1349,43 @@ int do_factorize(hodlr_t h) {
       e = schur_solve_launch(S, nn, -1, L.coff, L.max_sd, h->stream);
       if (e) return cuda_fail(h, (cudaError_t)e, "schur_solve");
       h->nlaunch += 1;
-      // Y[rows_h, 0:coff] -= Y[rows_h, coff : coff + rank(U_h)] * y_h
+      // Y_a[rows_h] -= Y_l[rows_h, 0 : rank(U_h)] * y_h[:, level a's columns]
+      // for every ancestor level a < l
       std::vector<GemmProblem> up;
       for (int p = 0; p < nn; ++p) {
         const SchurNode& sn = L.nodes[p];
         const int sd = sn.kb + sn.kt;
         const int mn = L.nmin[p], sp = L.nsplit[p], mx = L.nmax[p];
-        GemmProblem a{};
-        a.C = h->Y + mn;
-        a.ldc = (int)N;
-        a.A = h->Y + mn + (int64_t)L.coff * N;
-        a.lda = (int)N;
-        a.M = sp - mn + 1;
-        a.K = sn.kt;
-        a.B = h->Z + sn.z_off + sn.kb;
-        a.ldb = sd;
-        a.N = L.coff;
-        up.push_back(a);
-        GemmProblem b{};
-        b.C = h->Y + sp + 1;
-        b.ldc = (int)N;
-        b.A = h->Y + sp + 1 + (int64_t)L.coff * N;
-        b.lda = (int)N;
-        b.M = mx - sp;
-        b.K = sn.kb;
-        b.B = h->Z + sn.z_off;
-        b.ldb = sd;
-        b.N = L.coff;
-        up.push_back(b);
+        for (int a = 0; a < l; ++a) {
+          const Level& A = h->lv[a];
+          if (A.kmax == 0) continue;
+          if (sn.kt > 0) {
+            GemmProblem t{};
+            t.C = A.Yl + mn;
+            t.ldc = (int)N;
+            t.A = L.Yl + mn;
+            t.lda = (int)N;
+            t.M = sp - mn + 1;
+            t.K = sn.kt;
+            t.B = h->Z + sn.z_off + sn.kb + (int64_t)A.coff * sd;
+            t.ldb = sd;
+            t.N = A.kmax;
+            up.push_back(t);
+          }
+          if (sn.kb > 0) {
+            GemmProblem b{};
+            b.C = A.Yl + sp + 1;
+            b.ldc = (int)N;
+            b.A = L.Yl + sp + 1;
+            b.lda = (int)N;
+            b.M = mx - sp;
+            b.K = sn.kb;
+            b.B = h->Z + sn.z_off + (int64_t)A.coff * sd;
+            b.ldb = sd;
+            b.N = A.kmax;
+            up.push_back(b);
+          }
+        }
       }
       rc2 = upload_plan(h, up, false, L.nn);
       if (rc2) return rc2;
@@ -1397,7 +1463,7 @@ int build_solve_plans(hodlr_t h, int nrhs) {
       GemmProblem c{};
       c.C = h->X + mn;
       c.ldc = (int)N;
-      c.A = h->Y + mn + (int64_t)L.coff * N;
+      c.A = L.Yl + mn;
       c.lda = (int)N;
       c.M = sp - mn + 1;
       c.K = sn[p].kt;
@@ -1408,7 +1474,7 @@ int build_solve_plans(hodlr_t h, int nrhs) {
       GemmProblem d{};
       d.C = h->X + sp + 1;
       d.ldc = (int)N;
-      d.A = h->Y + sp + 1 + (int64_t)L.coff * N;
+      d.A = L.Yl + sp + 1;
       d.lda = (int)N;
       d.M = mx - sp;
       d.K = sn[p].kb;
@@ -2413,7 +2479,7 @@ int hodlr_set_precision(hodlr_t h, int precision) {
     return HODLR_ERR_ARG;
   if (precision != h->gemm_prec) {
     h->gemm_prec = precision;  // enum values coincide with HODLR_GEMM_*
-    free_factor(h);            // the compression is unchanged
+    free_factor(h);  // the compression is kept, unless the factorization overwrote W
   }
   return HODLR_OK;
 }
@@ -2557,6 +2623,29 @@ int hodlr_trim_device_memory(void) {
 int hodlr_set_capacity_hint(hodlr_t h, const int* caps, int nlevels) {
   if (!h || nlevels < 0 || (nlevels > 0 && !caps)) return HODLR_ERR_ARG;
   h->cap_hint.assign(caps, caps + nlevels);
+  return HODLR_OK;
+}
+
+int hodlr_set_aca_streaming(hodlr_t h, int on) {
+  if (!h || on < 0 || on > 1) return HODLR_ERR_ARG;
+  h->aca_ring = on != 0;
+  return HODLR_OK;
+}
+
+int hodlr_set_factor_in_place(hodlr_t h, int mode) {
+  if (!h || mode < -1 || mode > 1) return HODLR_ERR_ARG;
+  if (mode != h->in_place) {
+    h->in_place = mode;
+    free_factor(h);
+  }
+  return HODLR_OK;
+}
+
+int hodlr_get_factor_in_place(hodlr_t h, int* levels) {
+  if (!h || !levels) return HODLR_ERR_ARG;
+  int c = 0;
+  for (auto& L : h->lv) c += L.y_alias ? 1 : 0;
+  *levels = c;
   return HODLR_OK;
 }
 
@@ -2853,6 +2942,8 @@ int hodlr_get_lowrank(hodlr_t h, int block, double* W, double* V) {
   int l, q;
   if (!h || !locate(h, block, l, q)) return HODLR_ERR_ARG;
   if (!h->compressed) return fail(h, HODLR_ERR_STATE, "not compressed");
+  if (h->lv[l].y_alias)
+    return fail(h, HODLR_ERR_STATE, "W of this level was overwritten by the in-place factorization");
   Level& L = h->lv[l];
   int r0, c0, m, n;
   block_geom(L, q, r0, c0, m, n);

@@ -73,4 +73,5 @@ struct AcaLaunch {
   int ncta;              // CTAs of the launch when cta_block is set
   double* dotg;          // per-CTA per-warp dot partials in global memory (large ranks), or null
   int64_t dotg_stride;   // doubles per CTA in dotg (NT/32 * kcap_max)
+  int ring;              // 1: panel slices streamed by bulk copies (256 threads, even ld)
 };

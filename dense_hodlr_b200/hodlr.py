@@ -165,6 +165,20 @@ class HODLR_Matrix:
         _check(self._h, _L.lib().hodlr_set_capacity_hint(
             self._h, a.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), len(a)))
 
+    def set_aca_streaming(self, on):
+        """Top-level ACA panels through the bulk-copy ring (1, default) or per-thread loads (0)."""
+        _check(self._h, _L.lib().hodlr_set_aca_streaming(self._h, int(bool(on))))
+
+    def set_factor_in_place(self, mode):
+        """K^-1 U over the U panels: 1 always, 0 never, -1 (default) only when
+        separate memory cannot be allocated (hodlr_set_factor_in_place)."""
+        _check(self._h, _L.lib().hodlr_set_factor_in_place(self._h, int(mode)))
+
+    def factor_in_place_levels(self):
+        v = ctypes.c_int()
+        _check(self._h, _L.lib().hodlr_get_factor_in_place(self._h, ctypes.byref(v)))
+        return v.value
+
     # ------------------------------------------------------------- solver
     def storeLRinTree(self):
         _check(self._h, _L.lib().hodlr_compress(self._h))

@@ -299,6 +299,26 @@ int hodlr_set_precision(hodlr_t h, int precision);
 int hodlr_gemm_device(int precision, int mode, int m, int n, int k, const double* A, int lda,
                       const double* B, int ldb, double* C, int ldc, void* stream);
 
+/* Memory of the factorization (no counterpart in the reference, which keeps
+ * U and K^-1 U side by side in each node, include/HODLR_Tree.hpp:41-58).
+ * K^-1 U of a level needs N x kmax doubles.  mode 1: it overwrites the
+ * level's U panel (W) in place; mode 0: it always gets its own memory
+ * (HODLR_ERR_ALLOC if there is none); mode -1 (default): its own memory when
+ * that can be allocated, else in place.  Results are the same.  Once a level
+ * is factored in place its W is gone: hodlr_get_lowrank returns
+ * HODLR_ERR_STATE for its blocks, and a refactorization (another precision)
+ * compresses again.  hodlr_get_factor_in_place reports how many levels the
+ * last factorization overwrote. */
+int hodlr_set_factor_in_place(hodlr_t h, int mode);
+
+/* How the ACA of the few-block top levels reads its W/V panel slices (no
+ * counterpart in the reference): on = 1 (default) streams them through a
+ * shared-memory ring filled by bulk copies (used when N is even), 0 loads
+ * them per thread.  Pivots, ranks and W/V are the same either way; the
+ * setting applies from the next compression. */
+int hodlr_set_aca_streaming(hodlr_t h, int on);
+int hodlr_get_factor_in_place(hodlr_t h, int* levels);
+
 /* Number of kernels this handle has launched since it was created. */
 int hodlr_get_launch_count(hodlr_t h, long long* count);
 

@@ -94,3 +94,34 @@ def test_cube_gaussian_16_rhs_gmres_every_precision(oracle_mod):
         it, rel, x = _device_gmres(g, b)
         assert rel.max() <= 1e-10, (prec, it, rel.max())
         assert np.all(g.residual(x, b) <= 1e-10), prec
+
+
+def test_factor_in_place_matches_separate_panels(oracle_mod):
+    """K^-1 U written over the U panels (hodlr_set_factor_in_place(1)) gives the
+    solution of the separate-panel factorization; the overwritten W is
+    refused afterwards, and another precision compresses again."""
+    n = 8192
+    pts = uniform_cube(n, 2, 19)
+    g, o = _pair(oracle_mod, pts, "matern32", 0.2, 1e-2, 64, 1e-8)
+    b = np.random.default_rng(2).standard_normal((n, 3))
+    g.set_factor_in_place(0)
+    x0 = g.recLU_Solve(b)
+    assert g.factor_in_place_levels() == 0
+    W0, V0 = g.lowrank(0)
+    g.set_factor_in_place(1)
+    x1 = g.recLU_Solve(b)
+    assert g.factor_in_place_levels() == g.num_levels()
+    assert np.linalg.norm(x1 - x0) / np.linalg.norm(x0) <= 1e-13
+    xo = o.solve(b, nthreads=8)
+    assert np.linalg.norm(x1 - xo) / np.linalg.norm(xo) <= SOLVE_TOL
+    from dense_hodlr_b200 import HODLRError
+    with pytest.raises(HODLRError):
+        g.lowrank(0)
+    g.set_precision("tf32x3")  # refactor: the U panels are compressed again
+    it, rel, _ = _device_gmres(g, b)
+    assert rel.max() <= 1e-10
+    g.set_precision("fp64")
+    g.set_factor_in_place(0)
+    g.recLU_Compute()
+    W2, V2 = g.lowrank(0)
+    assert np.array_equal(W0, W2) and np.array_equal(V0, V2)
