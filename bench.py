@@ -543,12 +543,111 @@ def run_profile_case(case):
         g.solve_device(b_d.data_ptr(), x_d.data_ptr(), NRHS)
         print(json.dumps({"case": case, "factor_s": g.get_recLU_FactorizationTime(),
                           "solve_s": g.get_recLU_SolveTime()}))
+    elif case.startswith("tune"):
+        run_tune(case)
+    elif case.startswith("aca-ab"):
+        print(json.dumps(run_aca_ab(case)))
     elif case.split(":")[0] in SCALE_CONFIGS:
         print(json.dumps(run_scale(case)))
     elif case.startswith("batched"):
         print(json.dumps(run_batched(case)))
     else:
         raise SystemExit(f"unknown case {case}")
+
+
+def run_tune(case):
+    """Sweep of the preconditioner's compression tolerance and Woodbury
+    precision on one configuration, case 'tune:<c3|c5|c2>:N[:tols[:precs]]'
+    (tols and precs comma-separated): for each ACA tolerance one compression,
+    then per precision the factorization and GMRES on the FP64 full-kernel
+    residual to 1e-10.  One JSON line per (tolerance, precision), flushed."""
+    import torch
+    from dense_hodlr_b200 import HODLR_Matrix, KernelSpec
+    parts = case.split(":")
+    cfg = parts[1]
+    n = int(parts[2])
+    tols = [float(t) for t in parts[3].split(",")] if len(parts) > 3 else [1e-10, 1e-8, 1e-6, 1e-4]
+    precs = parts[4].split(",") if len(parts) > 4 else ["fp64", "tf32x3", "tf32", "bf16"]
+    if cfg == "c2":
+        from dense_hodlr_b200.points import uniform_cube
+        pts = uniform_cube(n, DIM, SEED)
+        spec, leaf, nrhs = KernelSpec("matern32", LSCALE, SHIFT), LEAF, NRHS
+    else:
+        c = SCALE_CONFIGS[cfg]
+        pts = scale_points(c["cloud"], n)
+        spec, leaf, nrhs = KernelSpec(c["kernel"], c["l"], c["shift"]), c["leaf"], c["nrhs"]
+    b = np.random.default_rng(SEED + 1).standard_normal((n, nrhs))
+    b_d = torch.from_numpy(np.ascontiguousarray(b.T)).cuda()
+    x_d = torch.empty_like(b_d)
+    g = HODLR_Matrix(n, n, spec, pts, leaf)
+    for tol in tols:
+        g.set_precision("fp64")
+        g.set_LRTolerance(tol)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        g.storeLRinTree()
+        t_lr = time.perf_counter() - t0
+        kmax = int(g.ranks().max())
+        for prec in precs:
+            g.set_precision(prec)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            g.recLU_Compute()
+            t_f = time.perf_counter() - t0
+            t0 = time.perf_counter()
+            try:
+                it, rel = g.iterative_solve_device(b_d.data_ptr(), x_d.data_ptr(), nrhs,
+                                                   tol=1e-10, max_iter=80, restart=40)
+                err = None
+            except Exception as e:  # a factor too poor to precondition
+                it, rel, err = -1, np.array([np.inf]), str(e)
+            torch.cuda.synchronize()
+            t_g = time.perf_counter() - t0
+            print(json.dumps({"case": "tune", "cfg": cfg, "n": n, "aca_tol": tol,
+                              "precision": prec, "compress_s": t_lr, "kmax": kmax,
+                              "factor_s": t_f, "gmres_s": t_g, "gmres_iterations": int(it),
+                              "rel_residual": float(rel.max()),
+                              "total_s": t_lr + t_f + t_g, "error": err}), flush=True)
+
+
+def run_aca_ab(case):
+    """ACA with the top levels' panels streamed through the bulk-copy ring
+    against per-thread loads, case 'aca-ab[:N[:cfg]]' (default: the FP64
+    workload's cloud at N = 262144; cfg 'c5' for the sphere / Matern tol 1e-10
+    shape): one compression each way (after a warm-up), the ACA time and
+    algorithmic GB/s of each, and whether ranks and pivots agree."""
+    from dense_hodlr_b200 import HODLR_Matrix, KernelSpec
+    parts = case.split(":")
+    n = int(parts[1]) if len(parts) > 1 and parts[1] else N_PTS
+    cfg = parts[2] if len(parts) > 2 else "c2"
+    if cfg == "c5":
+        c = SCALE_CONFIGS["c5"]
+        pts = scale_points(c["cloud"], n)
+        spec, leaf, tol = KernelSpec(c["kernel"], c["l"], c["shift"]), c["leaf"], c["tol"]
+    else:
+        from dense_hodlr_b200.points import uniform_cube
+        pts = uniform_cube(n, DIM, SEED)
+        spec, leaf, tol = KernelSpec("matern32", LSCALE, SHIFT), LEAF, TOL
+    out = {"case": "aca-ab", "n": n, "cfg": cfg}
+    res = {}
+    for on in (1, 0, 1):
+        g = HODLR_Matrix(n, n, spec, pts, leaf)
+        g.set_LRTolerance(tol)
+        g.set_aca_streaming(on)
+        g.storeLRinTree()
+        st = g.aca_stats()
+        res[on] = (g.ranks(), [g.pivots(b) for b in range(min(g.num_blocks(), 64))])
+        out[f"stream{on}"] = {"aca_s": st["seconds"], "launches": st["launches"],
+                              "gbs": st["bytes"] / st["seconds"] / 1e9,
+                              "lr_s": g.get_LR_ComputationTime(),
+                              "max_rank": int(g.ranks().max())}
+        del g
+    r1, p1 = res[1]
+    r0, p0 = res[0]
+    out["ranks_equal"] = bool(np.array_equal(r1, r0))
+    out["pivots_equal"] = all(np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+                              for a, b in zip(p1, p0))
+    return out
 
 
 # The two 2^20-point configurations: (points, kernel, length scale, shift,

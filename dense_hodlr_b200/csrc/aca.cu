@@ -44,8 +44,10 @@ struct Shared {
   int bcast_i[8];
 };
 
-// Group barrier.  gen counts the barriers this CTA has passed.
-__device__ bool group_sync(unsigned* bar, int G, unsigned& gen, unsigned* err) {
+// Group barrier.  gen counts the barriers this CTA has passed.  It gives up
+// after L.spin_limit polls (or once another CTA has raised the error word).
+__device__ bool group_sync(const AcaLaunch& L, unsigned* bar, int G, unsigned& gen,
+                           unsigned* err) {
   __syncthreads();
   if (G == 1) return true;
   __shared__ int s_fail;
@@ -53,10 +55,10 @@ __device__ bool group_sync(unsigned* bar, int G, unsigned& gen, unsigned* err) {
     s_fail = 0;
     __threadfence();
     atomicAdd(bar, 1u);
-    unsigned target = (gen + 1) * (unsigned)G;
+    unsigned target = (gen + 1) * (unsigned)G + L.bar_extra;
     unsigned polls = 0;
     while (ld_acquire_u32(bar) < target) {
-      if (++polls > HODLR_SPIN_LIMIT || *(volatile unsigned*)err) {
+      if (++polls > L.spin_limit || *(volatile unsigned*)err) {
         atomicOr(err, DEV_ERR_TIMEOUT);
         s_fail = 1;
         break;
@@ -574,11 +576,11 @@ __global__ void __launch_bounds__(NT, (RING ? 1 : (NT == 256 ? 2 : 4))) aca_kern
       if (pending) {
         const int bk0 = 8 + (k & 1) * (2 * B.kcap + 2);
         dots_only_pass<NT>(L, B, k, i_lo, i_hi, j_lo, j_hi, part_me + bk0);
-        if (!group_sync(bar, G, gen, L.err)) { status = ACA_ERROR; break; }
+        if (!group_sync(L, bar, G, gen, L.err)) { status = ACA_ERROR; break; }
         eps = resolve_eps<NT>(sh, L, B, part_grp, G, bk0, k, swp, svp, frob2);
         pending = 0;
         note_margin(k);
-        if (!group_sync(bar, G, gen, L.err)) { status = ACA_ERROR; break; }
+        if (!group_sync(L, bar, G, gen, L.err)) { status = ACA_ERROR; break; }
         if (!(eps > tol)) { status = ACA_POST; break; }
       }
       status = ACA_NEED_CAP;  // paused: the host grows the capacity and resumes
@@ -628,7 +630,7 @@ __global__ void __launch_bounds__(NT, (RING ? 1 : (NT == 256 ? 2 : 4))) aca_kern
       part_me[3] = (double)cand;
       part_me[bk + 2 * B.kcap + 1] = sv;
     }
-    if (!group_sync(bar, G, gen, L.err)) { status = ACA_ERROR; break; }
+    if (!group_sync(L, bar, G, gen, L.err)) { status = ACA_ERROR; break; }
 
     // ---------------- phase B: pivot column, residual column on the row slice
     double mv;
@@ -639,7 +641,7 @@ __global__ void __launch_bounds__(NT, (RING ? 1 : (NT == 256 ? 2 : 4))) aca_kern
       // even reached this step depends on epsilon_{k-1}: settle it first.
       if (pending) {
         dots_only_pass<NT>(L, B, k, i_lo, i_hi, j_lo, j_hi, part_me + bk);
-        if (!group_sync(bar, G, gen, L.err)) { status = ACA_ERROR; break; }
+        if (!group_sync(L, bar, G, gen, L.err)) { status = ACA_ERROR; break; }
         eps = resolve_eps<NT>(sh, L, B, part_grp, G, bk, k, swp, svp, frob2);
         pending = 0;
         note_margin(k);
@@ -655,7 +657,7 @@ __global__ void __launch_bounds__(NT, (RING ? 1 : (NT == 256 ? 2 : 4))) aca_kern
       f = block_min_int<NT>(sh, f);
       if (f == INT_MAX) { status = ACA_POST; break; }
       cur = f;
-      if (!group_sync(bar, G, gen, L.err)) { status = ACA_ERROR; break; }
+      if (!group_sync(L, bar, G, gen, L.err)) { status = ACA_ERROR; break; }
       continue;
     }
     int cc;
@@ -706,7 +708,7 @@ __global__ void __launch_bounds__(NT, (RING ? 1 : (NT == 256 ? 2 : 4))) aca_kern
       part_me[7] = (double)cand;
       part_me[bk + 2 * B.kcap] = sw;
     }
-    if (!group_sync(bar, G, gen, L.err)) { status = ACA_ERROR; break; }
+    if (!group_sync(L, bar, G, gen, L.err)) { status = ACA_ERROR; break; }
 
     // ---------------- phase C: epsilon of step k-1, then step k's next row
     if (pending) {
@@ -801,7 +803,7 @@ __global__ void __launch_bounds__(NT, (RING ? 1 : (NT == 256 ? 2 : 4))) aca_kern
   // Every CTA of the group reached the same state; CTA 0 records it after a
   // last barrier, so that no CTA of the group can still be about to read the
   // entry state (a block that starts in post-processing has no barrier before).
-  if (status != ACA_ERROR && !group_sync(bar, G, gen, L.err)) status = ACA_ERROR;
+  if (status != ACA_ERROR && !group_sync(L, bar, G, gen, L.err)) status = ACA_ERROR;
   if (g == 0 && tid == 0) {
     st->k = k;
     st->cur = cur;

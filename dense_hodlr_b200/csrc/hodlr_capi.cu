@@ -233,6 +233,8 @@ struct hodlr_handle_s {
   std::vector<int> cap_hint;  // initial W/V columns per level (0 = default)
   int gemm_prec = HODLR_GEMM_FP64;  // arithmetic of the Woodbury products
   bool aca_ring = true;  // group-level ACA panels through the bulk-copy ring
+  unsigned spin_limit = 0;       // polls of an ACA group barrier (0: HODLR_SPIN_LIMIT)
+  bool bar_unreachable = false;  // ACA group barriers wait for one arrival too many
   std::vector<int> leaf_min, leaf_size;
   int* d_leaf_min = nullptr;
   int* d_leaf_size = nullptr;
@@ -698,6 +700,8 @@ int run_aca(hodlr_t h, std::vector<AcaBlock>& blocks, int G, int nt, int kcap_ma
   L.dotg = nullptr;
   L.dotg_stride = 0;
   L.ring = ring ? 1 : 0;
+  L.spin_limit = h->spin_limit ? h->spin_limit : HODLR_SPIN_LIMIT;
+  L.bar_extra = h->bar_unreachable ? 1u : 0u;
   if (aca_smem_bytes(nt, kcap_max, ring) > 227 * 1024)
     return fail(h, HODLR_ERR_UNSUPPORTED, "block rank above the shared-memory limit of ACA");
   if (aca_dots_global(nt, kcap_max, ring)) {
@@ -2623,6 +2627,13 @@ int hodlr_trim_device_memory(void) {
 int hodlr_set_capacity_hint(hodlr_t h, const int* caps, int nlevels) {
   if (!h || nlevels < 0 || (nlevels > 0 && !caps)) return HODLR_ERR_ARG;
   h->cap_hint.assign(caps, caps + nlevels);
+  return HODLR_OK;
+}
+
+int hodlr_set_wait_limit(hodlr_t h, unsigned polls, int unreachable) {
+  if (!h || unreachable < 0 || unreachable > 1) return HODLR_ERR_ARG;
+  h->spin_limit = polls;
+  h->bar_unreachable = unreachable != 0;
   return HODLR_OK;
 }
 

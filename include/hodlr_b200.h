@@ -317,6 +317,15 @@ int hodlr_set_factor_in_place(hodlr_t h, int mode);
  * them per thread.  Pivots, ranks and W/V are the same either way; the
  * setting applies from the next compression. */
 int hodlr_set_aca_streaming(hodlr_t h, int on);
+
+/* Bounded device waits (no counterpart in the reference).  The CTAs of one
+ * ACA block group meet at a barrier in global memory; a barrier that is not
+ * complete after `polls` polls (0: the default, 2^26) gives up, the launch
+ * ends and the call returns HODLR_ERR_TIMEOUT, leaving the handle usable.
+ * unreachable = 1 makes every such barrier wait for one arrival more than
+ * its group has -- a wait nothing completes -- so that this path can be
+ * tested; set it back to 0 for normal work. */
+int hodlr_set_wait_limit(hodlr_t h, unsigned polls, int unreachable);
 int hodlr_get_factor_in_place(hodlr_t h, int* levels);
 
 /* Number of kernels this handle has launched since it was created. */
