@@ -64,6 +64,7 @@ SIGNATURES = {
                                  _I]),
     "hodlr_get_num_systems": (_I, [_H, _PI]),
     "hodlr_set_index_tree": (_I, [_H, _I, _PI, _PI, _PI]),
+    "hodlr_set_index_tree_bounds": (_I, [_H, _I, _PI, _PI, _PI, _PI, _PI, _PI, _PI]),
     "hodlr_logdet": (_I, [_H, _PD, _PI]),
     "hodlr_forest_refine_device": (_I, [_H, _I, _VP, _I, _VP, _I, _D, _I, _PI, _PD]),
     "hodlr_set_rank_model": (_I, [_H, _PF, _D]),

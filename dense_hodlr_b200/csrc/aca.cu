@@ -560,8 +560,10 @@ __global__ void __launch_bounds__(NT, (RING ? 1 : (NT == 256 ? 2 : 4))) aca_kern
     __syncthreads();
   }
 
+  const int minR = B.minRank, maxR = B.maxRank;  // -1: none (src/lowRank.cpp:149,244-247)
+  if (status == ACA_RUNNING && k == 0 && maxR == 0) status = ACA_POST;  // zero columns, rank 1
   auto note_margin = [&](int kcount) {
-    if (kcount < ub) {
+    if (kcount < ub && kcount >= minR) {
       double gap = fabs(eps - tol) / tol;
       margin = fmin(margin, gap);
       if (gap < 1e-10) ++near;
@@ -570,7 +572,7 @@ __global__ void __launch_bounds__(NT, (RING ? 1 : (NT == 256 ? 2 : 4))) aca_kern
 
   while (status == ACA_RUNNING) {
     // loop test of the reference, with epsilon_{k-1} possibly still pending
-    if (!pending && !(eps > tol)) { status = ACA_POST; break; }
+    if (!pending && !(eps > tol) && k >= minR) { status = ACA_POST; break; }
     if (k >= ub) { status = ACA_POST; break; }
     if (k >= B.kcap) {
       if (pending) {
@@ -581,7 +583,7 @@ __global__ void __launch_bounds__(NT, (RING ? 1 : (NT == 256 ? 2 : 4))) aca_kern
         pending = 0;
         note_margin(k);
         if (!group_sync(L, bar, G, gen, L.err)) { status = ACA_ERROR; break; }
-        if (!(eps > tol)) { status = ACA_POST; break; }
+        if (!(eps > tol) && k >= minR) { status = ACA_POST; break; }
       }
       status = ACA_NEED_CAP;  // paused: the host grows the capacity and resumes
       break;
@@ -645,7 +647,7 @@ __global__ void __launch_bounds__(NT, (RING ? 1 : (NT == 256 ? 2 : 4))) aca_kern
         eps = resolve_eps<NT>(sh, L, B, part_grp, G, bk, k, swp, svp, frob2);
         pending = 0;
         note_margin(k);
-        if (!(eps > tol)) {
+        if (!(eps > tol) && k >= minR) {
           --iters;
           status = ACA_POST;
           break;
@@ -719,7 +721,7 @@ __global__ void __launch_bounds__(NT, (RING ? 1 : (NT == 256 ? 2 : 4))) aca_kern
                    }();
       pending = 0;
       note_margin(k);
-      if (!(eps > tol)) {  // step k is discarded: the reference stopped before it
+      if (!(eps > tol) && k >= minR) {  // step k is discarded: the reference stopped before it
         --iters;
         status = ACA_POST;
         break;
@@ -747,6 +749,11 @@ __global__ void __launch_bounds__(NT, (RING ? 1 : (NT == 256 ? 2 : 4))) aca_kern
     pending = 1;
     cur = nr;
     ++k;
+    if (k == maxR) {  // the rank ceiling: stop without the last epsilon (src/lowRank.cpp:244-247)
+      pending = 0;
+      status = ACA_POST;
+      break;
+    }
     // No barrier needed here: the next writes to the partials come after
     // every CTA has passed barrier 2, and W(:,k) / V(:,k) are final.
   }

@@ -50,6 +50,9 @@ struct DevPlan {  // a grouped GEMM uploaded to the device
 
 struct Level {
   std::vector<int> nmin, nsplit, nmax;  // inner nodes of this level
+  // per node: rank bounds of its top and bottom blocks (-1: none; set by a
+  // user index tree, user_IndexTree::node, include/user_IndexTree.hpp)
+  std::vector<int> tmin, bmin, tmax, bmax;
   int nblocks() const { return 2 * (int)nmin.size(); }
   int ub_max = 0;  // largest min(m, n) of the level's blocks
   int kcap = 0;
@@ -241,6 +244,7 @@ struct hodlr_handle_s {
   // user index tree (hodlr_set_index_tree): pre-order nodes, split index and
   // child indices (-1: none)
   std::vector<int> ut_split, ut_left, ut_right;
+  std::vector<int> ut_tmin, ut_bmin, ut_tmax, ut_bmax;  // per user node, or empty
   int64_t* d_lu_off = nullptr;
   double* d_lu = nullptr;
   int* d_perm = nullptr;
@@ -378,6 +382,19 @@ void free_compress(hodlr_t h) {
   h->compressed = false;
 }
 
+void push_inner_node(hodlr_t h, int level, int mn, int split, int mx, int u = -1) {
+  if ((int)h->lv.size() <= level) h->lv.resize(level + 1);
+  Level& L = h->lv[level];
+  L.nmin.push_back(mn);
+  L.nsplit.push_back(split);
+  L.nmax.push_back(mx);
+  const bool b = u >= 0 && !h->ut_tmin.empty();
+  L.tmin.push_back(b ? h->ut_tmin[u] : -1);
+  L.bmin.push_back(b ? h->ut_bmin[u] : -1);
+  L.tmax.push_back(b ? h->ut_tmax[u] : -1);
+  L.bmax.push_back(b ? h->ut_bmax[u] : -1);
+}
+
 // createDefaultTree (src/HODLR_Tree.cpp:33-132): root is a leaf iff N < leaf;
 // a child splits iff its size > leaf; a left-type child splits at
 // min + floor(s/2) - 1, a right-type child at max - floor(s/2).  Nodes of a
@@ -396,13 +413,7 @@ void build_subtree(hodlr_t h, int o, int N) {
   };
   std::vector<Fr> stack;
   stack.push_back({0, o, o + N / 2 - 1, o + N - 1});
-  auto push_inner = [&](const Fr& f) {
-    if ((int)h->lv.size() <= f.level) h->lv.resize(f.level + 1);
-    Level& L = h->lv[f.level];
-    L.nmin.push_back(f.mn);
-    L.nsplit.push_back(f.split);
-    L.nmax.push_back(f.mx);
-  };
+  auto push_inner = [&](const Fr& f) { push_inner_node(h, f.level, f.mn, f.split, f.mx); };
   // explicit pre-order, left before right
   while (!stack.empty()) {
     Fr f = stack.back();
@@ -439,13 +450,6 @@ void build_subtree(hodlr_t h, int o, int N) {
 }
 
 // ---- user index trees (userTree_To_HODLRTree, src/HODLR_Tree.cpp:207-327)
-void push_inner_node(hodlr_t h, int level, int mn, int split, int mx) {
-  if ((int)h->lv.size() <= level) h->lv.resize(level + 1);
-  Level& L = h->lv[level];
-  L.nmin.push_back(mn);
-  L.nsplit.push_back(split);
-  L.nmax.push_back(mx);
-}
 
 // An inner node with a given split and the default rules below it
 // (createDefaultTree from that node): a child splits iff its size exceeds the
@@ -482,7 +486,7 @@ bool user_subtree(hodlr_t h, int level, int mn, int mx, int u, std::vector<char>
     return true;
   }
   if (sp < mn || sp >= mx) return false;
-  push_inner_node(h, level, mn, sp, mx);
+  push_inner_node(h, level, mn, sp, mx, u);
   const int l = h->ut_left[u], r = h->ut_right[u];
   if (l < 0 && r < 0) {
     const int ls = sp - mn + 1, rs = mx - sp;
@@ -628,6 +632,9 @@ void fill_block(hodlr_t h, Level& L, int q, AcaBlock& B) {
   B.level = 0;
   B.g0 = 0;
   B.G = 1;
+  const int p = q >> 1;
+  B.minRank = (q & 1) ? L.bmin[p] : L.tmin[p];
+  B.maxRank = (q & 1) ? L.bmax[p] : L.tmax[p];
 }
 
 bool level_done(const Level& L) {
@@ -2322,7 +2329,16 @@ int hodlr_create_forest(hodlr_t* out, int nsys, const int* sizes, int dim, const
 
 int hodlr_set_index_tree(hodlr_t h, int nnodes, const int* split, const int* left,
                          const int* right) {
+  return hodlr_set_index_tree_bounds(h, nnodes, split, left, right, nullptr, nullptr, nullptr,
+                                     nullptr);
+}
+
+int hodlr_set_index_tree_bounds(hodlr_t h, int nnodes, const int* split, const int* left,
+                                const int* right, const int* top_min, const int* bott_min,
+                                const int* top_max, const int* bott_max) {
   if (!h || nnodes < 0 || (nnodes > 0 && (!split || !left || !right))) return HODLR_ERR_ARG;
+  const bool bounds = top_min || bott_min || top_max || bott_max;
+  if (bounds && !(top_min && bott_min && top_max && bott_max)) return HODLR_ERR_ARG;
   if (h->nsys) return fail(h, HODLR_ERR_UNSUPPORTED, "user index trees are for one system");
   CK(cudaStreamSynchronize(h->stream));
   free_compress(h);
@@ -2330,6 +2346,17 @@ int hodlr_set_index_tree(hodlr_t h, int nnodes, const int* split, const int* lef
   h->ut_split.assign(split, split + nnodes);
   h->ut_left.assign(left, left + nnodes);
   h->ut_right.assign(right, right + nnodes);
+  if (bounds) {
+    h->ut_tmin.assign(top_min, top_min + nnodes);
+    h->ut_bmin.assign(bott_min, bott_min + nnodes);
+    h->ut_tmax.assign(top_max, top_max + nnodes);
+    h->ut_bmax.assign(bott_max, bott_max + nnodes);
+  } else {
+    h->ut_tmin.clear();
+    h->ut_bmin.clear();
+    h->ut_tmax.clear();
+    h->ut_bmax.clear();
+  }
   build_tree(h);
   int rc = HODLR_OK;
   if (h->leaf_min.empty() || h->smax > 160) {
@@ -2338,6 +2365,10 @@ int hodlr_set_index_tree(hodlr_t h, int nnodes, const int* split, const int* lef
     h->ut_split.clear();
     h->ut_left.clear();
     h->ut_right.clear();
+    h->ut_tmin.clear();
+    h->ut_bmin.clear();
+    h->ut_tmax.clear();
+    h->ut_bmax.clear();
     build_tree(h);  // back to the default tree
   }
   const int nl = (int)h->leaf_min.size();

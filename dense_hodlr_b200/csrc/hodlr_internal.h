@@ -46,6 +46,7 @@ struct AcaBlock {
   int kcap;           // columns available in W and V
   int level;
   int g0, G;          // with a CTA table: first CTA of this block's group, group size
+  int minRank, maxRank;  // the node's rank bounds for this block (-1: none)
 };
 
 // Loop state of one block; lets a paused block resume where it stopped.

@@ -412,13 +412,24 @@ class HODLR_Matrix:
         _check(self._h, _L.lib().hodlr_logdet(self._h, ctypes.byref(v), ctypes.byref(sg)))
         return sg.value * float(np.exp(v.value))
 
-    def set_index_tree(self, split, left, right):
+    def set_index_tree(self, split, left, right, bounds=None):
         """User index tree in pre-order (node 0 = root): split row per node (-1:
-        none), child node indices (-1: none; both -1 = default subtrees)."""
+        none), child node indices (-1: none; both -1 = default subtrees).
+        bounds: (top min, bottom min, top max, bottom max) rank bounds per user
+        node (user_IndexTree::node; -1 for none), or None."""
         sp, lf, rt = (np.ascontiguousarray(a, dtype=np.int32) for a in (split, left, right))
         pi = ctypes.POINTER(ctypes.c_int)
-        _check(self._h, _L.lib().hodlr_set_index_tree(self._h, len(sp), sp.ctypes.data_as(pi),
-                                                      lf.ctypes.data_as(pi), rt.ctypes.data_as(pi)))
+        if bounds is None:
+            _check(self._h, _L.lib().hodlr_set_index_tree(
+                self._h, len(sp), sp.ctypes.data_as(pi), lf.ctypes.data_as(pi),
+                rt.ctypes.data_as(pi)))
+            return
+        bs = [np.ascontiguousarray(a, dtype=np.int32) for a in bounds]
+        if len(bs) != 4 or any(len(a) != len(sp) for a in bs):
+            raise HODLRError(_L.ERR_ARG, "bounds: four arrays, one value per user node")
+        _check(self._h, _L.lib().hodlr_set_index_tree_bounds(
+            self._h, len(sp), sp.ctypes.data_as(pi), lf.ctypes.data_as(pi),
+            rt.ctypes.data_as(pi), *[a.ctypes.data_as(pi) for a in bs]))
 
     def num_systems(self):
         n = ctypes.c_int()

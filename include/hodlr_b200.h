@@ -222,13 +222,22 @@ int hodlr_logdet(hodlr_t h, double* log_abs_det, int* sign);
  * all rows: split[i] is the last row of node i's top half (-1: none; a node
  * no larger than the leaf size with no split is a leaf), left[i] and
  * right[i] its child nodes (both -1: default subtrees below, the right one
- * with floor(s/2) rows on top as in the reference).  The per-node rank bounds
- * and low-rank method of user_IndexTree::node are not taken: partial-pivot
- * ACA with the handle's tolerance on every block.  Discards any compression;
- * one-system handles only.  Invalid trees return HODLR_ERR_ARG and leave the
- * default tree. */
+ * with floor(s/2) rows on top as in the reference).  The low-rank method of
+ * user_IndexTree::node is not taken: partial-pivot ACA with the handle's
+ * tolerance on every block.  Discards any compression; one-system handles
+ * only.  Invalid trees return HODLR_ERR_ARG and leave the default tree. */
 int hodlr_set_index_tree(hodlr_t h, int nnodes, const int* split, const int* left,
                          const int* right);
+/* The same with user_IndexTree::node's rank bounds (include/user_IndexTree.hpp:
+ * topOffDiag_minRank, bottOffDiag_minRank, topOffDiag_maxRank,
+ * bottOffDiag_maxRank; src/HODLR_Tree.cpp:241-244), one value per user node,
+ * -1 for none: ACA continues while the rank is below the minimum (even past
+ * the tolerance) and stops at the maximum (src/lowRank.cpp:149,244-247).
+ * Nodes of the default subtrees below a user leaf take no bounds.  All four
+ * arrays or none. */
+int hodlr_set_index_tree_bounds(hodlr_t h, int nnodes, const int* split, const int* left,
+                                const int* right, const int* top_min, const int* bott_min,
+                                const int* top_max, const int* bott_max);
 /* Factor (if needed), direct solve, then iterative refinement with the FP64
  * residual until every system q has max_c ||b_c - K x_c|| / ||b_c|| <= tol
  * over its own rows (or max_iter corrections).  relres: nsys x nrhs,

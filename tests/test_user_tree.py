@@ -88,3 +88,32 @@ def test_user_tree_matches_oracle(oracle_mod):
     with pytest.raises(HODLRError):
         g.set_index_tree([5000], [-1], [-1])
     assert g.num_blocks() == n_default
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n,leaf", [(800, 64), (20000, 128)])
+def test_user_tree_rank_bounds_match_oracle(oracle_mod, n, leaf):
+    """Per-node rank bounds on the GPU (hodlr_set_index_tree_bounds): minRank
+    keeps ACA going past the tolerance, maxRank stops it, maxRank 0 gives the
+    zero rank-1 block -- pivots, ranks and W/V bit for bit against the oracle,
+    which is pinned to the Python ACA restatement with the same bounds.  The
+    larger case puts bounded blocks on the grouped (multi-CTA) top levels."""
+    from dense_hodlr_b200 import HODLR_Matrix, KernelSpec
+    from tests.test_gpu_parity import SOLVE_TOL, _compare_compression
+    pts = uniform_cube(n, 2, 4)
+    half, q = n // 2 - 1, n // 4
+    tree = ([half, q - 1, half + q], [1, -1, -1], [2, -1, -1])
+    bounds = ([-1, -1, 75], [120, -1, -1], [5, 0, -1], [-1, -1, 3])
+    g = HODLR_Matrix(n, n, KernelSpec("matern32", 0.2, 1e-2), pts, leaf)
+    g.set_LRTolerance(1e-8)
+    g.set_index_tree(*tree, bounds=bounds)
+    o = oracle_mod.OracleHODLR.from_kernel(pts, 1, 0.2, shift=1e-2, leaf=leaf)
+    o.set_lr(1e-8)
+    assert o.set_user_tree(*tree, bounds=bounds) == 0
+    _compare_compression(g, o)
+    r = g.ranks()
+    assert r[0] == 5 and r[1] >= 120 and r[2] == 1 and r[4] >= 75 and r[5] == 3
+    b = np.random.default_rng(5).standard_normal((n, 2))
+    x = g.recLU_Solve(b)
+    xo = o.solve(b, nthreads=8)
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= SOLVE_TOL
