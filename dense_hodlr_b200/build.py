@@ -10,7 +10,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libhodlr_b200.so")
-SOURCES = ["aca.cu", "gemm.cu", "lu.cu", "kmatvec.cu", "hodlr_capi.cu", "noalloc.cu", "umma_gemm.cu", "rank_mlp.cu",
+SOURCES = ["aca.cu", "gemm.cu", "lu.cu", "kmatvec.cu", "handle.cu", "tree.cu", "compress.cu",
+           "factor.cu", "solve.cu", "hodlr_capi.cu", "noalloc.cu", "umma_gemm.cu", "rank_mlp.cu",
            "matrix_io.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",

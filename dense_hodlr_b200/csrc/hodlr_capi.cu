@@ -1,2183 +1,8 @@
-// Host orchestration and C ABI of the B200 HODLR solver (include/hodlr_b200.h).
-//
-// Replaces, for the recLU path, HODLR_Matrix (include/HODLR_Matrix.hpp:38-413,
-// src/HODLR_Matrix.cpp) and HODLR_Tree::createDefaultTree
-// (src/HODLR_Tree.cpp:33-132).  The pointer tree of the reference becomes
-// level arrays; the recursions of recLU_Factorize / recLU_Solve
-// (src/HODLR_Matrix.cpp:612-755) become bottom-up sweeps over levels in which
-// every node of a level is processed by one batched launch.
-//
-// HBM layout (N = matrix size, column-major, leading dimension N):
-//   pts        dim x N coordinates (SoA)            or A  N x N dense input
-//   W_l, V_l   N x kcap_l per inner level l: the blocks of a level tile the
-//              rows (W) and the columns (V) of the matrix exactly once
-//   Y          N x C, C = sum_l kmax_l: level l occupies columns
-//              [coff_l, coff_l + kmax_l); after the factorization it holds
-//              K^-1 U for every node (topDiagSoln_LR / bottDiagSoln_LR)
-//   leaf LU    sum over leaves of s^2, plus a row permutation (N ints)
-//   S_l        per node (k_b + k_t)^2 capacitance LU + pivots
-#include <algorithm>
-#include <cmath>
-#include <map>
-#include <mutex>
-#include <unordered_map>
-#include <cstdio>
-#include <cstring>
-#include <string>
-#include <vector>
-
-#include "../../include/hodlr_b200.h"
-#include "common.cuh"
-#include "gemm.h"
-#include "kmatvec.h"
-#include "lu.h"
-#include "rank_mlp.h"
-
-int aca_launch(const AcaLaunch& L, int nt, int kcap_max, bool cooperative, cudaStream_t s);
-int aca_max_coresident(int nt, int kcap_max, bool ring, int* per_sm);
-bool aca_dots_global(int nt, int kcap_max, bool ring);
-size_t aca_smem_bytes(int nt, int kcap_max, bool ring);
-
-namespace {
-
-struct DevPlan {  // a grouped GEMM uploaded to the device
-  GemmProblem* probs = nullptr;
-  int4* tiles = nullptr;
-  int nprob = 0, ntiles = 0;
-  int64_t ws_elems = 0;
-  bool any_split = false;
-};
-
-struct Level {
-  std::vector<int> nmin, nsplit, nmax;  // inner nodes of this level
-  // per node: rank bounds of its top and bottom blocks (-1: none; set by a
-  // user index tree, user_IndexTree::node, include/user_IndexTree.hpp)
-  std::vector<int> tmin, bmin, tmax, bmax;
-  int nblocks() const { return 2 * (int)nmin.size(); }
-  int ub_max = 0;  // largest min(m, n) of the level's blocks
-  int kcap = 0;
-  double* W = nullptr;
-  double* V = nullptr;
-  unsigned char* cR = nullptr;
-  unsigned char* cC = nullptr;
-  int* prow = nullptr;
-  int* pcol = nullptr;
-  AcaState* d_st = nullptr;
-  std::vector<AcaState> st;
-  int G = 1;
-  int kmax = 0, coff = 0;
-  // K^-1 U of the level's blocks (N x kmax, ld N): its own allocation, or
-  // (y_alias) the first kmax columns of W, overwritten in place
-  double* Yl = nullptr;
-  bool y_alias = false;
-  // factorization
-  double* S = nullptr;
-  int* piv = nullptr;
-  SchurNode* d_nodes = nullptr;
-  std::vector<SchurNode> nodes;
-  int max_sd = 0;
-  DevPlan tn, nn;          // factor GEMMs
-  int solve_nrhs = -1;     // nrhs the solve plans were built for
-  DevPlan stn, snn;        // solve GEMMs
-  SchurNode* d_snodes = nullptr;  // solve: r_off into the solve buffer
-  int64_t zs_elems = 0;
-};
-
-void block_geom(const Level& L, int q, int& r0, int& c0, int& m, int& n) {
-  int p = q >> 1;
-  if ((q & 1) == 0) {  // top off-diagonal: rows [min, split], cols [split+1, max]
-    r0 = L.nmin[p];
-    c0 = L.nsplit[p] + 1;
-    m = L.nsplit[p] - L.nmin[p] + 1;
-    n = L.nmax[p] - L.nsplit[p];
-  } else {  // bottom off-diagonal: rows [split+1, max], cols [min, split]
-    r0 = L.nsplit[p] + 1;
-    c0 = L.nmin[p];
-    m = L.nmax[p] - L.nsplit[p];
-    n = L.nsplit[p] - L.nmin[p] + 1;
-  }
-}
-
-}  // namespace
-
-// Device memory cache of one handle.  Freed blocks go to `pending` and become
-// reusable only after the handle's stream has been synchronised, so a reused
-// block is never still read by an earlier kernel or host copy.
-// Device memory of every handle on a device comes from one stream-ordered
-// pool owned by the library (cudaMallocFromPoolAsync / cudaFreeAsync) whose
-// release threshold keeps freed memory reserved, so a new handle for the next
-// system reuses the previous one's arenas instead of paying cudaMalloc /
-// cudaFree for gigabytes.  hodlr_trim_device_memory hands it back.
-std::mutex g_pool_mu;
-std::map<int, cudaMemPool_t> g_pools;
-
-cudaMemPool_t device_pool() {
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
-  std::lock_guard<std::mutex> lk(g_pool_mu);
-  auto it = g_pools.find(dev);
-  if (it != g_pools.end()) return it->second;
-  cudaMemPoolProps props;
-  memset(&props, 0, sizeof(props));
-  props.allocType = cudaMemAllocationTypePinned;
-  props.handleTypes = cudaMemHandleTypeNone;
-  props.location.type = cudaMemLocationTypeDevice;
-  props.location.id = dev;
-  cudaMemPool_t pool = nullptr;
-  if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) return nullptr;
-  uint64_t keep = UINT64_MAX;
-  cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
-  g_pools[dev] = pool;
-  return pool;
-}
-
-// Per-handle cache on top of the device pool: buffers freed by the handle are
-// reused by its next allocations of a similar size once its stream has
-// drained (pending -> free).
-struct DevPool {
-  cudaMemPool_t mp = nullptr;
-  std::multimap<size_t, void*> freeb, pending;
-  std::unordered_map<void*, size_t> size;
-  cudaError_t raw_alloc(void** p, size_t bytes, cudaStream_t s) {
-    if (!mp) mp = device_pool();
-    if (!mp) return cudaErrorMemoryAllocation;
-    return cudaMallocFromPoolAsync(p, bytes, mp, s);
-  }
-  cudaError_t alloc(void** p, size_t bytes, cudaStream_t s) {
-    bytes = (bytes + 255) & ~(size_t)255;
-    for (int pass = 0; pass < 2; ++pass) {
-      auto it = freeb.lower_bound(bytes);
-      if (it != freeb.end() && it->first <= bytes + bytes / 4 + (1u << 20)) {
-        *p = it->second;
-        freeb.erase(it);
-        return cudaSuccess;
-      }
-      if (pass == 0 && !pending.empty()) {
-        cudaError_t e = cudaStreamSynchronize(s);
-        if (e != cudaSuccess) return e;
-        freeb.insert(pending.begin(), pending.end());
-        pending.clear();
-      }
-    }
-    cudaError_t e = raw_alloc(p, bytes, s);
-    if (e == cudaErrorMemoryAllocation) {  // give back every cache, retry once
-      cudaGetLastError();
-      release_free(s);
-      for (auto& f : pending) {
-        cudaFreeAsync(f.second, s);
-        size.erase(f.second);
-      }
-      pending.clear();
-      cudaStreamSynchronize(s);
-      cudaMemPoolTrimTo(mp, 0);
-      e = raw_alloc(p, bytes, s);
-    }
-    if (e == cudaSuccess) size[*p] = bytes;
-    return e;
-  }
-  void free(void* p) {
-    auto it = size.find(p);
-    if (it == size.end()) return;
-    pending.insert({it->second, p});
-  }
-  void release_free(cudaStream_t s) {
-    for (auto& f : freeb) {
-      cudaFreeAsync(f.second, s);
-      size.erase(f.second);
-    }
-    freeb.clear();
-  }
-  void release_all(cudaStream_t s) {
-    for (auto& f : size) cudaFreeAsync(f.first, s);
-    size.clear();
-    freeb.clear();
-    pending.clear();
-    cudaStreamSynchronize(s);
-  }
-};
-
-struct hodlr_handle_s {
-  DevPool pool;
-  // the direct solve as a CUDA graph, replayed while its key is unchanged
-  cudaGraphExec_t sg_exec = nullptr;
-  int sg_nrhs = -1;
-  cudaStream_t sg_stream = nullptr;
-  const void* sg_key[4] = {nullptr, nullptr, nullptr, nullptr};
-  long sg_gen = -1;
-  long long sg_launches = 0;
-  bool sg_off = false;  // capture refused once: direct launches from then on
-  long factor_gen = 0;
-  // forest of independent systems (hodlr_create_forest); nsys == 0: one system
-  int nsys = 0;
-  std::vector<int> sys_off;  // nsys + 1 point offsets
-  std::vector<hx_kparams> sys_kp;
-  hx_kparams* d_kps = nullptr;
-  int* d_psys = nullptr;
-  int4* d_fitems = nullptr;  // full-kernel product work items, by kernel family
-  int ftype_off[HX_FOREST_TYPES + 1] = {0};
-  double* d_fnorm = nullptr;  // per-system residual and right-hand-side norms
-  int* d_cta = nullptr;  // CTA -> block table of uneven ACA groups
-  int cta_cap = 0;
-  double* dotg = nullptr;  // ACA dot partials in global memory (large ranks)
-  int64_t dotg_cap = 0;
-  // rank predictor (rank_mlp.cu): FP32 parameter blob on the device, the
-  // length scale its features use, and the last predictions (block order)
-  float* d_model = nullptr;
-  double model_l = 0.0;
-  std::vector<int> pred;
-  int n = 0, leaf = 30, dim = 0;
-  bool dense = false;
-  hx_kparams kp{};
-  double* d_pts = nullptr;
-  double* d_A = nullptr;
-  double tol = 1e-6;
-  int minPivot = 0;
-  std::vector<Level> lv;
-  std::vector<int> cap_hint;  // initial W/V columns per level (0 = default)
-  int gemm_prec = HODLR_GEMM_FP64;  // arithmetic of the Woodbury products
-  bool aca_ring = true;  // group-level ACA panels through the bulk-copy ring
-  unsigned spin_limit = 0;       // polls of an ACA group barrier (0: HODLR_SPIN_LIMIT)
-  bool bar_unreachable = false;  // ACA group barriers wait for one arrival too many
-  std::vector<int> leaf_min, leaf_size;
-  int* d_leaf_min = nullptr;
-  int* d_leaf_size = nullptr;
-  // user index tree (hodlr_set_index_tree): pre-order nodes, split index and
-  // child indices (-1: none)
-  std::vector<int> ut_split, ut_left, ut_right;
-  std::vector<int> ut_tmin, ut_bmin, ut_tmax, ut_bmax;  // per user node, or empty
-  int64_t* d_lu_off = nullptr;
-  double* d_lu = nullptr;
-  int* d_perm = nullptr;
-  int smax = 0;
-  int64_t C = 0;  // sum over levels of kmax: the columns of all K^-1 U panels
-  // factor in place: -1 only when a separate K^-1 U panel cannot be
-  // allocated, 0 never, 1 always (hodlr_set_factor_in_place)
-  int in_place = -1;
-  bool w_consumed = false;  // some level's W holds K^-1 U: recompress before refactoring
-  double* ws = nullptr;  // GEMM split-K / kmatvec workspace
-  int64_t ws_cap = 0;
-  double* Z = nullptr;  // per-level Schur right-hand sides (factor)
-  int64_t z_cap = 0;
-  double* X = nullptr;  // solve panel N x nrhs
-  int x_cols = 0;
-  double* ir_b = nullptr;  // refinement: right-hand sides, iterate, K x, partial norms
-  double* ir_x = nullptr;
-  double* ir_y = nullptr;
-  double* ir_part = nullptr;
-  int ir_cols = 0;
-  double* gm_V = nullptr;  // GMRES bases: (m+1) and m panels of N x nrhs
-  double* gm_Z = nullptr;
-  double* gm_h = nullptr;  // small device buffers of coefficients / partials
-  double* gm_part = nullptr;
-  int gm_m = 0, gm_cols = 0;
-  double* zs = nullptr;  // solve Schur right-hand sides
-  int64_t zs_cap = 0;
-  double* part = nullptr;
-  int64_t part_cap = 0;
-  unsigned* bar = nullptr;
-  int bar_cap = 0;
-  AcaBlock* d_blocks = nullptr;
-  int blocks_cap = 0;
-  unsigned* d_err = nullptr;
-  cudaStream_t stream = nullptr;
-  cudaStream_t own_stream = nullptr;
-  long long nlaunch = 0;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  int num_sms = 0;
-  bool compressed = false, factored = false;
-  double t_lr = 0, t_fact = 0, t_solve = 0, t_total = 0;
-  int aca_launches = 0;
-  double aca_seconds = 0, aca_bytes = 0;
-  std::string err;
-};
-
-namespace {
-
-// Internal status (never returned by the C ABI): a cooperative launch was
-// refused as too large and may be retried with fewer CTAs.
-constexpr int HODLR_ERR_RETRY_SMALLER = 1000;
-
-int fail(hodlr_t h, int code, const std::string& msg) {
-  if (h) h->err = msg;
-  return code;
-}
-
-int cuda_fail(hodlr_t h, cudaError_t e, const char* where) {
-  return fail(h, e == cudaErrorMemoryAllocation ? HODLR_ERR_ALLOC : HODLR_ERR_CUDA,
-              std::string(where) + ": " + cudaGetErrorString(e));
-}
-
-#define CK(call)                                               \
-  do {                                                         \
-    cudaError_t e__ = (call);                                  \
-    if (e__ != cudaSuccess) return cuda_fail(h, e__, #call);   \
-  } while (0)
-
-template <class T>
-cudaError_t dalloc(hodlr_t h, T** p, size_t count) {
-  *p = nullptr;
-  if (count == 0) return cudaSuccess;
-  return h->pool.alloc((void**)p, sizeof(T) * count, h->stream);
-}
-
-template <class T>
-void dfree(hodlr_t h, T*& p) {
-  if (p) h->pool.free((void*)p);
-  p = nullptr;
-}
-
-void free_plan(hodlr_t h, DevPlan& p) {
-  dfree(h, p.probs);
-  dfree(h, p.tiles);
-  p = DevPlan();
-}
-
-void drop_solve_graph(hodlr_t h) {
-  if (h->sg_exec) cudaGraphExecDestroy(h->sg_exec);
-  h->sg_exec = nullptr;
-  h->sg_nrhs = -1;
-}
-
-void free_factor(hodlr_t h) {
-  drop_solve_graph(h);
-  ++h->factor_gen;
-  for (auto& L : h->lv) {
-    dfree(h, L.S);
-    dfree(h, L.piv);
-    dfree(h, L.d_nodes);
-    dfree(h, L.d_snodes);
-    free_plan(h, L.tn);
-    free_plan(h, L.nn);
-    free_plan(h, L.stn);
-    free_plan(h, L.snn);
-    L.solve_nrhs = -1;
-    L.nodes.clear();
-  }
-  dfree(h, h->d_lu);
-  dfree(h, h->d_lu_off);
-  dfree(h, h->d_perm);
-  for (auto& L : h->lv) {
-    if (!L.y_alias) dfree(h, L.Yl);
-    L.Yl = nullptr;
-    L.y_alias = false;
-  }
-  if (h->w_consumed) h->compressed = false;  // the U panels are gone: compress again
-  h->w_consumed = false;
-  h->factored = false;
-}
-
-void free_compress(hodlr_t h) {
-  free_factor(h);
-  for (auto& L : h->lv) {
-    dfree(h, L.W);
-    dfree(h, L.V);
-    dfree(h, L.cR);
-    dfree(h, L.cC);
-    dfree(h, L.prow);
-    dfree(h, L.pcol);
-    dfree(h, L.d_st);
-    L.st.clear();
-    L.kcap = 0;
-  }
-  h->compressed = false;
-}
-
-void push_inner_node(hodlr_t h, int level, int mn, int split, int mx, int u = -1) {
-  if ((int)h->lv.size() <= level) h->lv.resize(level + 1);
-  Level& L = h->lv[level];
-  L.nmin.push_back(mn);
-  L.nsplit.push_back(split);
-  L.nmax.push_back(mx);
-  const bool b = u >= 0 && !h->ut_tmin.empty();
-  L.tmin.push_back(b ? h->ut_tmin[u] : -1);
-  L.bmin.push_back(b ? h->ut_bmin[u] : -1);
-  L.tmax.push_back(b ? h->ut_tmax[u] : -1);
-  L.bmax.push_back(b ? h->ut_bmax[u] : -1);
-}
-
-// createDefaultTree (src/HODLR_Tree.cpp:33-132): root is a leaf iff N < leaf;
-// a child splits iff its size > leaf; a left-type child splits at
-// min + floor(s/2) - 1, a right-type child at max - floor(s/2).  Nodes of a
-// level are listed left to right (pre-order pushes), leaves in index order.
-// The tree of one system on points [o, o + N): inner nodes appended level by
-// level (pre-order, left before right), leaves in index order.
-void build_subtree(hodlr_t h, int o, int N) {
-  const int leaf = h->leaf;
-  if (N < leaf || N < 2) {
-    h->leaf_min.push_back(o);
-    h->leaf_size.push_back(N);
-    return;
-  }
-  struct Fr {
-    int level, mn, split, mx;
-  };
-  std::vector<Fr> stack;
-  stack.push_back({0, o, o + N / 2 - 1, o + N - 1});
-  auto push_inner = [&](const Fr& f) { push_inner_node(h, f.level, f.mn, f.split, f.mx); };
-  // explicit pre-order, left before right
-  while (!stack.empty()) {
-    Fr f = stack.back();
-    stack.pop_back();
-    push_inner(f);
-    int top = f.split - f.mn + 1, bott = f.mx - f.split;
-    Fr right{f.level + 1, f.mn + top, -1, f.mx};
-    Fr left{f.level + 1, f.mn, -1, f.mn + top - 1};
-    bool rsplit = bott > leaf, lsplit = top > leaf;
-    if (rsplit) right.split = f.mx - bott / 2;
-    if (lsplit) left.split = f.mn + top / 2 - 1;
-    if (rsplit) stack.push_back(right);
-    if (lsplit) stack.push_back(left);
-  }
-  // Walk the tree again to list the leaves in index order.
-  std::vector<Fr> st2;
-  st2.push_back({0, o, o + N / 2 - 1, o + N - 1});
-  while (!st2.empty()) {
-    Fr f = st2.back();
-    st2.pop_back();
-    if (f.split < 0) {
-      h->leaf_min.push_back(f.mn);
-      h->leaf_size.push_back(f.mx - f.mn + 1);
-      continue;
-    }
-    int top = f.split - f.mn + 1, bott = f.mx - f.split;
-    Fr right{f.level + 1, f.mn + top, -1, f.mx};
-    Fr left{f.level + 1, f.mn, -1, f.mn + top - 1};
-    if (bott > leaf) right.split = f.mx - bott / 2;
-    if (top > leaf) left.split = f.mn + top / 2 - 1;
-    st2.push_back(right);
-    st2.push_back(left);
-  }
-}
-
-// ---- user index trees (userTree_To_HODLRTree, src/HODLR_Tree.cpp:207-327)
-
-// An inner node with a given split and the default rules below it
-// (createDefaultTree from that node): a child splits iff its size exceeds the
-// leaf size, the left-type child with floor(s/2) rows on top, the right-type
-// child with ceil(s/2).
-void grow_default(hodlr_t h, int level, int mn, int split, int mx) {
-  push_inner_node(h, level, mn, split, mx);
-  const int top = split - mn + 1, bott = mx - split;
-  if (top > h->leaf) {
-    grow_default(h, level + 1, mn, mn + top / 2 - 1, split);
-  } else {
-    h->leaf_min.push_back(mn);
-    h->leaf_size.push_back(top);
-  }
-  if (bott > h->leaf) {
-    grow_default(h, level + 1, split + 1, mx - bott / 2, mx);
-  } else {
-    h->leaf_min.push_back(split + 1);
-    h->leaf_size.push_back(bott);
-  }
-}
-
-// Node [mn, mx] of user node u: a leaf when it is no larger than the leaf size
-// and has no split; otherwise split where u says, with u's children, or, if
-// u has none, default children (the right one with floor(s/2) rows on top,
-// as the reference builds them).  Returns false for an invalid user tree.
-bool user_subtree(hodlr_t h, int level, int mn, int mx, int u, std::vector<char>& seen) {
-  if (u < 0 || u >= (int)h->ut_split.size() || seen[u]) return false;
-  seen[u] = 1;
-  const int size = mx - mn + 1, sp = h->ut_split[u];
-  if (size <= h->leaf && sp == -1) {
-    h->leaf_min.push_back(mn);
-    h->leaf_size.push_back(size);
-    return true;
-  }
-  if (sp < mn || sp >= mx) return false;
-  push_inner_node(h, level, mn, sp, mx, u);
-  const int l = h->ut_left[u], r = h->ut_right[u];
-  if (l < 0 && r < 0) {
-    const int ls = sp - mn + 1, rs = mx - sp;
-    if (ls > h->leaf) {
-      grow_default(h, level + 1, mn, mn + ls / 2 - 1, sp);
-    } else {
-      h->leaf_min.push_back(mn);
-      h->leaf_size.push_back(ls);
-    }
-    if (rs > h->leaf) {
-      grow_default(h, level + 1, sp + 1, sp + rs / 2, mx);
-    } else {
-      h->leaf_min.push_back(sp + 1);
-      h->leaf_size.push_back(rs);
-    }
-    return true;
-  }
-  if (l < 0 || r < 0) return false;
-  return user_subtree(h, level + 1, mn, sp, l, seen) &&
-         user_subtree(h, level + 1, sp + 1, mx, r, seen);
-}
-
-// One tree, or a forest: every system's root sits at level 0, so a level's
-// blocks (and its ACA launch, its batched leaf LUs and GEMMs) span all
-// systems.
-void build_tree(hodlr_t h) {
-  h->lv.clear();
-  h->leaf_min.clear();
-  h->leaf_size.clear();
-  if (h->nsys == 0 && !h->ut_split.empty()) {
-    std::vector<char> seen(h->ut_split.size(), 0);
-    if (!user_subtree(h, 0, 0, h->n - 1, 0, seen)) {  // invalid: the caller restores
-      h->lv.clear();
-      h->leaf_min.clear();
-      h->leaf_size.clear();
-      return;
-    }
-  } else if (h->nsys == 0)
-    build_subtree(h, 0, h->n);
-  else
-    for (int q = 0; q < h->nsys; ++q)
-      build_subtree(h, h->sys_off[q], h->sys_off[q + 1] - h->sys_off[q]);
-  for (auto& L : h->lv) {
-    L.ub_max = 0;
-    for (int q = 0; q < L.nblocks(); ++q) {
-      int r0, c0, m, n;
-      block_geom(L, q, r0, c0, m, n);
-      L.ub_max = std::max(L.ub_max, std::min(m, n));
-    }
-  }
-  h->smax = 0;
-  for (int s : h->leaf_size) h->smax = std::max(h->smax, s);
-}
-
-int ensure_ws(hodlr_t h, int64_t elems) {
-  if (elems <= h->ws_cap) return HODLR_OK;
-  dfree(h, h->ws);
-  CK(dalloc(h, &h->ws, (size_t)elems));
-  h->ws_cap = elems;
-  return HODLR_OK;
-}
-
-// Host copies on the handle's stream.  The handle's own stream is a
-// non-blocking stream, so a synchronous cudaMemcpy (legacy default stream) is
-// not ordered with its kernels; every copy goes through these instead and
-// returns after the stream has drained.
-cudaError_t h2d(hodlr_t h, void* dst, const void* src, size_t bytes) {
-  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, h->stream);
-  return e != cudaSuccess ? e : cudaStreamSynchronize(h->stream);
-}
-cudaError_t d2h(hodlr_t h, void* dst, const void* src, size_t bytes) {
-  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, h->stream);
-  return e != cudaSuccess ? e : cudaStreamSynchronize(h->stream);
-}
-cudaError_t copy2d(hodlr_t h, void* dst, size_t dpitch, const void* src, size_t spitch,
-                   size_t width, size_t rows, cudaMemcpyKind kind) {
-  cudaError_t e = cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, rows, kind, h->stream);
-  return e != cudaSuccess ? e : cudaStreamSynchronize(h->stream);
-}
-
-int check_dev_err(hodlr_t h, const char* where) {
-  unsigned e = 0;
-  CK(d2h(h, &e, h->d_err, sizeof(unsigned)));
-  if (e == 0) return HODLR_OK;
-  CK(cudaMemsetAsync(h->d_err, 0, sizeof(unsigned), h->stream));
-  if (e & DEV_ERR_TIMEOUT) return fail(h, HODLR_ERR_TIMEOUT, std::string(where) + ": device wait timed out");
-  if (e & DEV_ERR_NONFINITE) return fail(h, HODLR_ERR_NONFINITE, std::string(where) + ": non-finite value");
-  if (e & DEV_ERR_SINGULAR) return fail(h, HODLR_ERR_SINGULAR, std::string(where) + ": exact-zero pivot");
-  return fail(h, HODLR_ERR_CUDA, where);
-}
-
-EntrySrc make_src(hodlr_t h) {
-  EntrySrc s;
-  s.pts = h->d_pts;
-  s.A = h->d_A;
-  s.ld = h->n;
-  s.kp = h->kp;
-  s.dense = h->dense ? 1 : 0;
-  s.kps = h->nsys ? h->d_kps : nullptr;
-  s.psys = h->nsys ? h->d_psys : nullptr;
-  return s;
-}
-
-// Grow level L to `cap` columns, keeping the first `keep` columns.
-int grow_level(hodlr_t h, Level& L, int cap) {
-  const int64_t N = h->n;
-  double *W2 = nullptr, *V2 = nullptr;
-  CK(dalloc(h, &W2, (size_t)(N * cap)));
-  cudaError_t e = dalloc(h, &V2, (size_t)(N * cap));
-  if (e != cudaSuccess) {
-    dfree(h, W2);
-    return cuda_fail(h, e, "grow_level");
-  }
-  if (L.W && L.kcap > 0) {
-    CK(cudaMemcpyAsync(W2, L.W, sizeof(double) * N * L.kcap, cudaMemcpyDeviceToDevice, h->stream));
-    CK(cudaMemcpyAsync(V2, L.V, sizeof(double) * N * L.kcap, cudaMemcpyDeviceToDevice, h->stream));
-  }
-  CK(cudaStreamSynchronize(h->stream));
-  dfree(h, L.W);
-  dfree(h, L.V);
-  L.W = W2;
-  L.V = V2;
-  L.kcap = cap;
-  return HODLR_OK;
-}
-
-void fill_block(hodlr_t h, Level& L, int q, AcaBlock& B) {
-  int r0, c0, m, n;
-  block_geom(L, q, r0, c0, m, n);
-  (void)h;
-  B.st = L.d_st + q;
-  B.W = L.W + r0;
-  B.V = L.V + c0;
-  B.cR = L.cR + r0;
-  B.cC = L.cC + c0;
-  B.prow = L.prow + r0;
-  B.pcol = L.pcol + c0;
-  B.r0 = r0;
-  B.c0 = c0;
-  B.m = m;
-  B.n = n;
-  B.kcap = L.kcap;
-  B.level = 0;
-  B.g0 = 0;
-  B.G = 1;
-  const int p = q >> 1;
-  B.minRank = (q & 1) ? L.bmin[p] : L.tmin[p];
-  B.maxRank = (q & 1) ? L.bmax[p] : L.tmax[p];
-}
-
-bool level_done(const Level& L) {
-  for (auto& s : L.st)
-    if (s.status != ACA_DONE) return false;
-  return true;
-}
-
-// Run one ACA launch over `blocks` with group size G.
-// One ACA launch over `blocks`: groups of G CTAs each, or, with `groups`,
-// groups[i] CTAs for block i (a CTA table maps CTAs to blocks).
-int run_aca(hodlr_t h, std::vector<AcaBlock>& blocks, int G, int nt, int kcap_max,
-            bool ring = false, const std::vector<int>* groups = nullptr) {
-  const int nb = (int)blocks.size();
-  if (nb == 0) return HODLR_OK;
-  int ncta = nb * G;
-  if (groups) {
-    ncta = 0;
-    for (int i = 0; i < nb; ++i) {
-      blocks[i].g0 = ncta;
-      blocks[i].G = (*groups)[i];
-      ncta += (*groups)[i];
-    }
-    std::vector<int> table((size_t)ncta);
-    for (int i = 0; i < nb; ++i)
-      for (int c = 0; c < blocks[i].G; ++c) table[(size_t)(blocks[i].g0 + c)] = i;
-    if (ncta > h->cta_cap) {
-      dfree(h, h->d_cta);
-      CK(dalloc(h, &h->d_cta, (size_t)ncta));
-      h->cta_cap = ncta;
-    }
-    CK(cudaMemcpyAsync(h->d_cta, table.data(), sizeof(int) * ncta, cudaMemcpyHostToDevice,
-                       h->stream));
-  }
-  if (nb > h->blocks_cap) {
-    dfree(h, h->d_blocks);
-    CK(dalloc(h, &h->d_blocks, (size_t)nb));
-    h->blocks_cap = nb;
-  }
-  CK(cudaMemcpyAsync(h->d_blocks, blocks.data(), sizeof(AcaBlock) * nb, cudaMemcpyHostToDevice,
-                     h->stream));
-  int64_t stride = 12 + 4 * (int64_t)kcap_max;  // args + two banks of dots and norms
-  int64_t need = stride * ncta;
-  if (need > h->part_cap) {
-    dfree(h, h->part);
-    CK(dalloc(h, &h->part, (size_t)need));
-    h->part_cap = need;
-  }
-  if (nb > h->bar_cap) {
-    dfree(h, h->bar);
-    CK(dalloc(h, &h->bar, (size_t)nb));
-    h->bar_cap = nb;
-  }
-  CK(cudaMemsetAsync(h->bar, 0, sizeof(unsigned) * nb, h->stream));
-  AcaLaunch L;
-  L.blocks = h->d_blocks;
-  L.nblocks = nb;
-  L.G = G;
-  L.ld = h->n;
-  L.tol = h->tol;
-  L.minPivot = (double)h->minPivot;
-  L.kcap_max = kcap_max;
-  L.part = h->part;
-  L.part_stride = stride;
-  L.bar = h->bar;
-  L.err = h->d_err;
-  L.src = make_src(h);
-  L.cta_block = groups ? h->d_cta : nullptr;
-  L.ncta = ncta;
-  L.dotg = nullptr;
-  L.dotg_stride = 0;
-  L.ring = ring ? 1 : 0;
-  L.spin_limit = h->spin_limit ? h->spin_limit : HODLR_SPIN_LIMIT;
-  L.bar_extra = h->bar_unreachable ? 1u : 0u;
-  if (aca_smem_bytes(nt, kcap_max, ring) > 227 * 1024)
-    return fail(h, HODLR_ERR_UNSUPPORTED, "block rank above the shared-memory limit of ACA");
-  if (aca_dots_global(nt, kcap_max, ring)) {
-    L.dotg_stride = (int64_t)(nt / 32) * kcap_max;
-    const int64_t dneed = L.dotg_stride * ncta;
-    if (dneed > h->dotg_cap) {
-      dfree(h, h->dotg);
-      CK(dalloc(h, &h->dotg, (size_t)dneed));
-      h->dotg_cap = dneed;
-    }
-    L.dotg = h->dotg;
-  }
-  bool coop = G > 1;
-  if (groups)
-    for (int g : *groups) coop |= g > 1;
-  CK(cudaEventRecord(h->ev0, h->stream));
-  int rc = aca_launch(L, nt, kcap_max, coop, h->stream);
-  if (rc == (int)cudaErrorCooperativeLaunchTooLarge) return HODLR_ERR_RETRY_SMALLER;
-  if (rc) return cuda_fail(h, (cudaError_t)rc, "aca_launch");
-  h->nlaunch += 1;
-  CK(cudaEventRecord(h->ev1, h->stream));
-  CK(cudaEventSynchronize(h->ev1));
-  float ms = 0;
-  CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
-  h->aca_seconds += ms * 1e-3;
-  h->aca_launches += 1;
-  return check_dev_err(h, "ACA");
-}
-
-// Allocate the per-level arrays of level L with `cap` low-rank columns.
-int init_level(hodlr_t h, Level& L, int cap) {
-  const int64_t N = h->n;
-  int rc = grow_level(h, L, std::max(1, std::min(L.ub_max, cap)));
-  if (rc) return rc;
-  CK(dalloc(h, &L.cR, (size_t)N));
-  CK(dalloc(h, &L.cC, (size_t)N));
-  CK(dalloc(h, &L.prow, (size_t)N));
-  CK(dalloc(h, &L.pcol, (size_t)N));
-  CK(cudaMemsetAsync(L.cR, 0, N, h->stream));
-  CK(cudaMemsetAsync(L.cC, 0, N, h->stream));
-  const int nb = L.nblocks();
-  CK(dalloc(h, &L.d_st, (size_t)nb));
-  L.st.assign(nb, AcaState());
-  for (auto& s : L.st) {
-    s.frob2 = 0;
-    s.eps = 1;
-    s.margin = HUGE_VAL;
-    s.swp = s.svp = 0;
-    s.k = 0;
-    s.cur = 0;
-    s.status = ACA_RUNNING;
-    s.iters = 0;
-    s.rank = 0;
-    s.near = 0;
-    s.pending = 0;
-    s.pad = 0;
-  }
-  CK(cudaMemcpyAsync(L.d_st, L.st.data(), sizeof(AcaState) * nb, cudaMemcpyHostToDevice,
-                     h->stream));
-  return HODLR_OK;
-}
-
-// Read the level's block states back; grow the level where blocks paused for
-// capacity and re-arm them.  *done = every block of the level finished.
-int sync_level(hodlr_t h, Level& L, bool* done) {
-  const int nb = L.nblocks();
-  CK(cudaMemcpyAsync(L.st.data(), L.d_st, sizeof(AcaState) * nb, cudaMemcpyDeviceToHost,
-                     h->stream));
-  CK(cudaStreamSynchronize(h->stream));
-  int need = 0;
-  *done = true;
-  for (auto& s : L.st) {
-    if (s.status == ACA_ERROR) return fail(h, HODLR_ERR_TIMEOUT, "ACA group failed");
-    if (s.status == ACA_NEED_CAP) need = std::max(need, L.kcap + std::max(32, L.kcap / 2));
-    if (s.status == ACA_NEED_CAP_POST) need = std::max(need, s.rank);
-    if (s.status != ACA_DONE) *done = false;
-  }
-  if (need > 0) {
-    int cap = std::min(std::max(need, L.kcap + 1), std::max(L.ub_max, L.kcap + 1));
-    int rc = grow_level(h, L, cap);
-    if (rc) return rc;
-    for (auto& s : L.st) {
-      if (s.status == ACA_NEED_CAP) s.status = ACA_RUNNING;
-      if (s.status == ACA_NEED_CAP_POST) s.status = ACA_POST;
-    }
-    CK(cudaMemcpyAsync(L.d_st, L.st.data(), sizeof(AcaState) * nb, cudaMemcpyHostToDevice,
-                       h->stream));
-  }
-  return HODLR_OK;
-}
-
-int level_kmax(const Level& L) {
-  int k = 0;
-  for (auto& s : L.st) k = std::max(k, s.rank);
-  return k;
-}
-
-// storeLRinTree (src/HODLR_Matrix.cpp:257-272,274-430) for every block.
-// Levels with many blocks run together in one launch, one CTA per block
-// (G = 1); the top levels, with few large blocks, run one cooperative launch
-// each with a group of CTAs per block.  They go bottom-up so that each
-// level's W/V capacity can be sized from the ranks of the level below it
-// (ranks shrink down the tree); a level that needs more grows and resumes.
-std::vector<int4> block_geoms(hodlr_t h) {
-  std::vector<int4> geom;
-  for (auto& L : h->lv)
-    for (int q = 0; q < L.nblocks(); ++q) {
-      int r0, c0, m, n;
-      block_geom(L, q, r0, c0, m, n);
-      geom.push_back(make_int4(r0, c0, m, n));
-    }
-  return geom;
-}
-
-// Features of every block (nb x HODLR_MLP_INPUTS, device) for length scale l.
-int block_features_dev(hodlr_t h, const std::vector<int4>& geom, double l, float* d_F) {
-  const int nb = (int)geom.size();
-  int4* d_geom = nullptr;
-  CK(dalloc(h, &d_geom, (size_t)nb));
-  CK(cudaMemcpyAsync(d_geom, geom.data(), sizeof(int4) * nb, cudaMemcpyHostToDevice, h->stream));
-  int e = block_features_launch(h->d_pts, h->n, h->dim, d_geom, nb, (float)std::log(l),
-                                (float)std::log(h->tol), d_F, h->stream);
-  if (e) return cuda_fail(h, (cudaError_t)e, "block features");
-  h->nlaunch += 1;
-  dfree(h, d_geom);
-  return HODLR_OK;
-}
-
-// Predicted ACA rank of every block (level-major order, as
-// hodlr_get_block_info numbers them) from the rank model: block features on
-// the device, the MLP forward, rank = exp(y) - 1 rounded and clamped.
-int predict_ranks(hodlr_t h) {
-  const std::vector<int4> geom = block_geoms(h);
-  const int nb = (int)geom.size();
-  h->pred.assign(nb, 0);
-  if (nb == 0) return HODLR_OK;
-  float *d_F = nullptr, *d_y = nullptr;
-  CK(dalloc(h, &d_F, (size_t)nb * HODLR_MLP_INPUTS));
-  CK(dalloc(h, &d_y, (size_t)nb));
-  int rc = block_features_dev(h, geom, h->model_l, d_F);
-  if (rc) return rc;
-  int e = mlp_forward_launch(h->d_model, d_F, nb, d_y, h->stream);
-  if (e) return cuda_fail(h, (cudaError_t)e, "rank prediction");
-  h->nlaunch += 1;
-  std::vector<float> y((size_t)nb);
-  CK(d2h(h, y.data(), d_y, sizeof(float) * nb));
-  dfree(h, d_F);
-  dfree(h, d_y);
-  for (int i = 0; i < nb; ++i) {
-    const double r = std::expm1((double)std::min(y[i], 20.0f));
-    const int ub = std::min(geom[i].z, geom[i].w);
-    h->pred[i] = std::max(0, std::min(ub, (int)std::lround(r)));
-  }
-  return HODLR_OK;
-}
-
-int do_compress(hodlr_t h) {
-  if (h->compressed) return HODLR_OK;
-  free_compress(h);
-  h->aca_launches = 0;
-  h->aca_seconds = 0;
-  h->aca_bytes = 0;
-  const int nlev = (int)h->lv.size();
-  // predicted ranks, when a rank model is set: level capacities and the
-  // order of the pooled blocks (largest predicted work first) follow them;
-  // ACA's stopping test still decides every rank (a block that needs more
-  // columns pauses and resumes after its level grows)
-  std::vector<int> lbase(nlev + 1, 0);
-  for (int l = 0; l < nlev; ++l) lbase[l + 1] = lbase[l] + h->lv[l].nblocks();
-  const bool have_pred = h->d_model != nullptr;
-  if (have_pred) {
-    int rc = predict_ranks(h);
-    if (rc) return rc;
-  }
-  auto pred = [&](int l, int q) { return h->pred[(size_t)(lbase[l] + q)]; };
-  auto pred_cap = [&](int l) {
-    int mx = 0;
-    for (int q = 0; q < h->lv[l].nblocks(); ++q) mx = std::max(mx, pred(l, q));
-    return std::max(16, ((mx + mx / 4 + 8) + 7) / 8 * 8);
-  };
-  auto hint = [&](int l) {
-    if (l < (int)h->cap_hint.size() && h->cap_hint[l] > 0) return h->cap_hint[l];
-    return have_pred ? pred_cap(l) : 0;
-  };
-  auto pred_or = [&](int l, int q) -> int64_t { return have_pred ? pred(l, q) + 1 : 1; };
-  int per_sm = 0;
-  if (aca_max_coresident(256, 256, false, &per_sm))
-    return fail(h, HODLR_ERR_CUDA, "occupancy query failed");
-  const int P0 = std::max(1, per_sm) * h->num_sms;
-  std::vector<int> pooled_levels, group_levels;
-  for (int l = 0; l < nlev; ++l)
-    (h->lv[l].nblocks() * 2 > P0 ? pooled_levels : group_levels).push_back(l);
-  // 1. the many-block levels, together
-  for (int l : pooled_levels) {
-    int rc = init_level(h, h->lv[l], hint(l) ? hint(l) : 64);
-    if (rc) return rc;
-  }
-  for (int round = 0; round < 64 && !pooled_levels.empty(); ++round) {
-    int kcap_max = 1;
-    std::vector<std::pair<int64_t, AcaBlock>> sorted;
-    for (int l : pooled_levels) {
-      Level& L = h->lv[l];
-      kcap_max = std::max(kcap_max, L.kcap);
-      L.G = 1;
-      for (int q = 0; q < L.nblocks(); ++q) {
-        if (L.st[q].status == ACA_DONE) continue;
-        AcaBlock B;
-        fill_block(h, L, q, B);
-        const int64_t k1 = pred_or(l, q);
-        sorted.push_back({have_pred ? (int64_t)(B.m + B.n) * k1 * k1 : (int64_t)B.m * B.n, B});
-      }
-    }
-    if (sorted.empty()) break;
-    std::stable_sort(sorted.begin(), sorted.end(),
-                     [](const std::pair<int64_t, AcaBlock>& a,
-                        const std::pair<int64_t, AcaBlock>& b) { return a.first > b.first; });
-    std::vector<AcaBlock> blocks;
-    for (auto& pb : sorted) blocks.push_back(pb.second);
-    int rc = run_aca(h, blocks, 1, 128, kcap_max);
-    if (rc) return rc;
-    bool all = true;
-    for (int l : pooled_levels) {
-      bool done;
-      rc = sync_level(h, h->lv[l], &done);
-      if (rc) return rc;
-      all &= done;
-    }
-    if (all) break;
-  }
-  // 2. the few-block levels, deepest first
-  int kmax_below = 0;
-  if (!pooled_levels.empty()) kmax_below = level_kmax(h->lv[pooled_levels.front()]);
-  for (auto it = group_levels.rbegin(); it != group_levels.rend(); ++it) {
-    const int l = *it;
-    Level& L = h->lv[l];
-    int guess = hint(l) ? hint(l) : std::max(64, (kmax_below * 3 + 1) / 2 + 16);
-    int rc = init_level(h, L, guess);
-    if (rc) return rc;
-    for (int round = 0; round < 64; ++round) {
-      // the group levels stream their panels through the bulk-copy ring
-      // (16-byte aligned columns need an even N) while that still leaves at
-      // least two of its one-per-SM CTAs to every block
-      const int nb = L.nblocks();
-      int ps = 0, ps_ring = 0;
-      if (aca_max_coresident(256, L.kcap, false, &ps) ||
-          aca_max_coresident(256, L.kcap, true, &ps_ring))
-        return fail(h, HODLR_ERR_CUDA, "occupancy query failed");
-      const bool ring = h->aca_ring && (h->n % 2 == 0) && ps_ring * h->num_sms >= 2 * nb;
-      if (ring) ps = ps_ring;
-      // equal groups: CTAs sized by predicted work measured 2-8% slower on
-      // 3D clouds than equal groups (per-step latency, not streamed bytes,
-      // sets a block's time)
-      int G = std::max(1, std::max(1, ps) * h->num_sms / nb);
-      std::vector<AcaBlock> bl(nb);
-      for (;;) {  // a cooperative launch the driver refuses is retried with half the groups
-        L.G = G;
-        for (int q = 0; q < nb; ++q) fill_block(h, L, q, bl[q]);
-        rc = run_aca(h, bl, G, G > 1 || ring ? 256 : 128, L.kcap, ring);
-        if (rc != HODLR_ERR_RETRY_SMALLER) break;
-        if (G == 1) return fail(h, HODLR_ERR_CUDA, "aca_launch: cooperative launch refused");
-        G = std::max(1, G / 2);
-      }
-      if (rc) return rc;
-      bool done;
-      rc = sync_level(h, L, &done);
-      if (rc) return rc;
-      if (done) break;
-    }
-    kmax_below = level_kmax(L);
-  }
-  for (auto& L : h->lv)
-    if (!level_done(L)) return fail(h, HODLR_ERR_STATE, "ACA did not converge in 64 rounds");
-  // ranks, level widths, column offsets, algorithmic bytes
-  int64_t coff = 0;
-  double bytes = 0;
-  for (auto& L : h->lv) {
-    L.kmax = 0;
-    for (int q = 0; q < L.nblocks(); ++q) {
-      L.kmax = std::max(L.kmax, L.st[q].rank);
-      int r0, c0, m, n;
-      block_geom(L, q, r0, c0, m, n);
-      // one read of the W and V panels per step (the norm dots ride along),
-      // the two new columns and the coordinates of the entries evaluated
-      double K = L.st[q].iters;
-      bytes += (double)(m + n) * (4.0 * K * (K - 1) + 8.0 * K * (1 + h->dim));
-    }
-    L.coff = (int)coff;
-    coff += L.kmax;
-  }
-  h->C = coff;
-  h->aca_bytes = bytes;
-  h->compressed = true;
-  return HODLR_OK;
-}
-
-int upload_plan(hodlr_t h, std::vector<GemmProblem>& probs, bool split, DevPlan& out) {
-  std::vector<int4> tiles;
-  int64_t ws = 0;
-  if (h->gemm_prec == HODLR_GEMM_FP64)
-    gemm_plan(probs, tiles, ws, split, 2 * h->num_sms * 4);
-  else
-    umma_plan(probs, tiles, ws, split, 2 * h->num_sms * 4);
-  free_plan(h, out);
-  out.nprob = (int)probs.size();
-  out.ntiles = (int)tiles.size();
-  out.ws_elems = ws;
-  out.any_split = false;
-  for (auto& p : probs) out.any_split |= p.splits > 1;
-  if (out.nprob) {
-    CK(dalloc(h, &out.probs, (size_t)out.nprob));
-    CK(h2d(h, out.probs, probs.data(), sizeof(GemmProblem) * out.nprob));
-  }
-  if (out.ntiles) {
-    CK(dalloc(h, &out.tiles, (size_t)out.ntiles));
-    CK(h2d(h, out.tiles, tiles.data(), sizeof(int4) * out.ntiles));
-  }
-  return ensure_ws(h, ws);
-}
-
-int level_rank(const Level& L, int q) { return L.st[q].rank; }
-
-// Launch a planned TN / NN-sub group in the handle's arithmetic.
-int run_tn(hodlr_t h, const DevPlan& P) {
-  if (P.ntiles == 0) return 0;
-  h->nlaunch += 1 + (P.any_split ? 1 : 0);
-  if (h->gemm_prec == HODLR_GEMM_FP64)
-    return gemm_tn_launch(P.probs, P.tiles, P.ntiles, P.nprob, h->ws, P.any_split, h->stream);
-  return umma_tn_launch(h->gemm_prec, P.probs, P.tiles, P.ntiles, P.nprob, h->ws, P.any_split,
-                        h->d_err, h->stream);
-}
-
-int run_nn(hodlr_t h, const DevPlan& P) {
-  if (P.ntiles == 0) return 0;
-  h->nlaunch += 1;
-  if (h->gemm_prec == HODLR_GEMM_FP64)
-    return gemm_nn_sub_launch(P.probs, P.tiles, P.ntiles, h->stream);
-  return umma_nn_sub_launch(h->gemm_prec, P.probs, P.tiles, P.ntiles, h->d_err, h->stream);
-}
-
-// Y_l[rows of block q, c] = W_l[rows, c] for c < rank(q), 0 for rank(q) <= c
-// < kmax.  With Y == W (in place) only the padding is written.
-__global__ void y_init_kernel(double* Y, const double* W, int64_t ld, int kmax, const int* r0s,
-                              const int* ms, const int* ranks, int nb) {
-  int q = blockIdx.y;
-  if (q >= nb) return;
-  const int r0 = r0s[q], m = ms[q], rank = ranks[q];
-  for (int c = blockIdx.z; c < kmax; c += gridDim.z) {
-    if (c < rank && Y == W) continue;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x)
-      Y[(int64_t)c * ld + r0 + i] = c < rank ? W[(int64_t)c * ld + r0 + i] : 0.0;
-  }
-}
-
-// log|det| pieces of the factorization: per leaf LU (column-major s x s,
-// final row permutation perm) and per capacitance LU (sd x sd, LAPACK-style
-// swaps piv): out = (sum_i log|u_ii|, #u_ii < 0, permutation parity).
-__global__ void leaf_logdet_kernel(const double* lu, const int64_t* lu_off, const int* leaf_min,
-                                   const int* leaf_size, const int* perm, double* out) {
-  if (threadIdx.x != 0) return;
-  const int q = blockIdx.x, s = leaf_size[q];
-  const double* g = lu + lu_off[q];
-  const int* pm = perm + leaf_min[q];
-  double sum = 0.0;
-  int neg = 0;
-  for (int i = 0; i < s; ++i) {
-    const double d = g[(int64_t)i * s + i];
-    sum += log(fabs(d));
-    neg += d < 0.0;
-  }
-  unsigned char seen[160];
-  for (int i = 0; i < s; ++i) seen[i] = 0;
-  int cycles = 0;
-  for (int i = 0; i < s; ++i) {
-    if (seen[i]) continue;
-    ++cycles;
-    for (int j = i; !seen[j]; j = pm[j]) seen[j] = 1;
-  }
-  out[3 * q] = sum;
-  out[3 * q + 1] = neg;
-  out[3 * q + 2] = (s - cycles) & 1;
-}
-
-__global__ void schur_logdet_kernel(const SchurNode* nodes, const double* S, const int* piv,
-                                    double* out) {
-  if (threadIdx.x != 0) return;
-  const SchurNode N = nodes[blockIdx.x];
-  const int n = N.kb + N.kt;
-  const double* a = S + N.s_off;
-  const int* p = piv + N.p_off;
-  double sum = 0.0;
-  int neg = 0, swaps = 0;
-  for (int i = 0; i < n; ++i) {
-    const double d = a[(int64_t)i * n + i];
-    sum += log(fabs(d));
-    neg += d < 0.0;
-    swaps += p[i] != i;
-  }
-  out[3 * blockIdx.x] = sum;
-  out[3 * blockIdx.x + 1] = neg;
-  out[3 * blockIdx.x + 2] = swaps & 1;
-}
-
-// Identity blocks on the leaves' diagonal of an N x smax panel (zeroed):
-// X[r0 + i, i] = 1 for every leaf (r0, s), i < s.
-__global__ void leaf_identity_kernel(double* X, int64_t ldx, const int* leaf_min,
-                                     const int* leaf_size) {
-  const int r0 = leaf_min[blockIdx.x], s = leaf_size[blockIdx.x];
-  for (int i = threadIdx.x; i < s; i += blockDim.x) X[r0 + i + (int64_t)i * ldx] = 1.0;
-}
-
-int do_factorize(hodlr_t h) {
-  if (h->factored) return HODLR_OK;
-  free_factor(h);  // first: a factorization that overwrote W also drops the compression
-  int rc = do_compress(h);
-  if (rc) return rc;
-  const int64_t N = h->n;
-  CK(cudaEventRecord(h->ev0, h->stream));
-  // leaves: assemble + LU
-  const int nl = (int)h->leaf_min.size();
-  std::vector<int64_t> lu_off(nl);
-  int64_t tot = 0;
-  for (int p = 0; p < nl; ++p) {
-    lu_off[p] = tot;
-    tot += (int64_t)h->leaf_size[p] * h->leaf_size[p];
-  }
-  CK(dalloc(h, &h->d_lu, (size_t)tot));
-  CK(dalloc(h, &h->d_lu_off, (size_t)nl));
-  CK(dalloc(h, &h->d_perm, (size_t)N));
-  CK(cudaMemcpyAsync(h->d_lu_off, lu_off.data(), sizeof(int64_t) * nl, cudaMemcpyHostToDevice,
-                     h->stream));
-  {
-    LeafLULaunch L;
-    L.leaf_min = h->d_leaf_min;
-    L.leaf_size = h->d_leaf_size;
-    L.lu_off = h->d_lu_off;
-    L.lu = h->d_lu;
-    L.perm = h->d_perm;
-    L.src = make_src(h);
-    L.err = h->d_err;
-    int e = leaf_lu_launch(L, nl, h->smax, h->stream);
-    if (e) return cuda_fail(h, (cudaError_t)e, "leaf_lu_launch");
-    h->nlaunch += 1;
-  }
-  // Y_l = the U panel of every level, zero padded to kmax columns: its own
-  // allocation, or W_l itself (in place) when that cannot be had
-  if (h->C > 0) {
-    for (auto& L : h->lv) {
-      if (L.kmax == 0) continue;
-      const int nb = L.nblocks();
-      std::vector<int> r0s(nb), ms(nb), rk(nb);
-      for (int q = 0; q < nb; ++q) {
-        int r0, c0, m, n;
-        block_geom(L, q, r0, c0, m, n);
-        r0s[q] = r0;
-        ms[q] = m;
-        rk[q] = level_rank(L, q);
-      }
-      L.y_alias = h->in_place == 1;
-      if (!L.y_alias) {
-        cudaError_t ea = dalloc(h, &L.Yl, (size_t)(N * L.kmax));
-        if (ea == cudaErrorMemoryAllocation && h->in_place == -1) {
-          cudaGetLastError();
-          L.y_alias = true;
-        } else if (ea != cudaSuccess) {
-          return cuda_fail(h, ea, "K^-1 U panel");
-        }
-      }
-      if (L.y_alias) {
-        L.Yl = L.W;
-        h->w_consumed = true;
-      }
-      int *d_r0 = nullptr, *d_m = nullptr, *d_rk = nullptr;
-      CK(dalloc(h, &d_r0, nb));
-      CK(dalloc(h, &d_m, nb));
-      CK(dalloc(h, &d_rk, nb));
-      CK(cudaMemcpyAsync(d_r0, r0s.data(), 4 * nb, cudaMemcpyHostToDevice, h->stream));
-      CK(cudaMemcpyAsync(d_m, ms.data(), 4 * nb, cudaMemcpyHostToDevice, h->stream));
-      CK(cudaMemcpyAsync(d_rk, rk.data(), 4 * nb, cudaMemcpyHostToDevice, h->stream));
-      int maxm = 0;
-      for (int m : ms) maxm = std::max(maxm, m);
-      dim3 grid(std::min(64, (maxm + 255) / 256), nb, std::min(L.kmax, 64));
-      y_init_kernel<<<grid, 256, 0, h->stream>>>(L.Yl, L.W, N, L.kmax, d_r0, d_m, d_rk, nb);
-      CK(cudaGetLastError());
-      h->nlaunch += 1;
-      CK(cudaStreamSynchronize(h->stream));
-      dfree(h, d_r0);
-      dfree(h, d_m);
-      dfree(h, d_rk);
-    }
-    // Y <- blockdiag(leaf)^-1 Y on every column.  Each leaf's inverse is
-    // formed once (its LU applied to identity columns, smax columns in all)
-    // and applied as a grouped GEMM, Y_new = A_leaf^-1 Y: the columns of
-    // triangular substitution per leaf become one pass of dense products.
-    const int sm = h->smax;
-    int CH = 1;  // Y columns per product pass
-    for (auto& L : h->lv) CH = std::max(CH, std::min(L.kmax, 512));
-    double *Xinv = nullptr, *Y2 = nullptr;
-    CK(dalloc(h, &Xinv, (size_t)(N * sm)));
-    CK(dalloc(h, &Y2, (size_t)(N * CH)));
-    CK(cudaMemsetAsync(Xinv, 0, sizeof(double) * N * sm, h->stream));
-    leaf_identity_kernel<<<nl, 128, 0, h->stream>>>(Xinv, N, h->d_leaf_min, h->d_leaf_size);
-    CK(cudaGetLastError());
-    LeafSolveLaunch S;
-    S.leaf_min = h->d_leaf_min;
-    S.leaf_size = h->d_leaf_size;
-    S.lu_off = h->d_lu_off;
-    S.lu = h->d_lu;
-    S.perm = h->d_perm;
-    S.X = Xinv;
-    S.ldx = N;
-    S.ncols = sm;
-    int e = leaf_solve_launch(S, nl, sm, h->stream);
-    if (e) return cuda_fail(h, (cudaError_t)e, "leaf_solve_launch");
-    // per level, in passes of CH columns through an N x CH buffer
-    GemmProblem* d_probs = nullptr;
-    int4* d_tiles = nullptr;
-    size_t tiles_cap = 0;
-    CK(dalloc(h, &d_probs, (size_t)nl));
-    for (auto& L : h->lv) {
-      for (int c0 = 0; c0 < L.kmax; c0 += CH) {
-        const int nc = std::min(CH, L.kmax - c0);
-        std::vector<GemmProblem> probs;
-        for (int p = 0; p < nl; ++p) {
-          const int r0 = h->leaf_min[p], s = h->leaf_size[p];
-          GemmProblem g{};
-          g.A = Xinv + r0;
-          g.B = L.Yl + r0 + (int64_t)c0 * N;
-          g.C = Y2 + r0;
-          g.M = s;
-          g.N = nc;
-          g.K = s;
-          g.lda = (int)N;
-          g.ldb = (int)N;
-          g.ldc = (int)N;
-          probs.push_back(g);
-        }
-        std::vector<int4> tiles;
-        int64_t ws = 0;
-        gemm_plan(probs, tiles, ws, false, 0);
-        if (tiles.size() > tiles_cap) {
-          dfree(h, d_tiles);
-          CK(dalloc(h, &d_tiles, tiles.size()));
-          tiles_cap = tiles.size();
-        }
-        CK(h2d(h, d_probs, probs.data(), sizeof(GemmProblem) * probs.size()));
-        CK(h2d(h, d_tiles, tiles.data(), sizeof(int4) * tiles.size()));
-        e = gemm_nn_launch(d_probs, d_tiles, (int)tiles.size(), h->stream);
-        if (e) return cuda_fail(h, (cudaError_t)e, "leaf inverse product");
-        CK(cudaMemcpyAsync(L.Yl + (int64_t)c0 * N, Y2, sizeof(double) * N * nc,
-                           cudaMemcpyDeviceToDevice, h->stream));
-        h->nlaunch += 1;
-      }
-    }
-    h->nlaunch += 2;
-    dfree(h, Y2);
-    dfree(h, Xinv);
-    dfree(h, d_probs);
-    dfree(h, d_tiles);
-  }
-  // levels bottom-up
-  for (int l = (int)h->lv.size() - 1; l >= 0; --l) {
-    Level& L = h->lv[l];
-    const int nn = (int)L.nmin.size();
-    L.nodes.resize(nn);
-    int64_t s_tot = 0, z_tot = 0, p_tot = 0;
-    L.max_sd = 0;
-    for (int p = 0; p < nn; ++p) {
-      SchurNode& sn = L.nodes[p];
-      sn.kt = level_rank(L, 2 * p);
-      sn.kb = level_rank(L, 2 * p + 1);
-      sn.coff = L.coff;
-      sn.pad = 0;
-      const int sd = sn.kb + sn.kt;
-      L.max_sd = std::max(L.max_sd, sd);
-      sn.s_off = s_tot;
-      s_tot += (int64_t)sd * sd;
-      sn.z_off = z_tot;
-      sn.r_off = z_tot;
-      z_tot += (int64_t)sd * (L.coff + std::max(sn.kb, sn.kt));
-      sn.p_off = p_tot;
-      p_tot += sd;
-    }
-    CK(dalloc(h, &L.S, (size_t)s_tot));
-    CK(dalloc(h, &L.piv, (size_t)p_tot));
-    CK(dalloc(h, &L.d_nodes, (size_t)nn));
-    CK(cudaMemcpyAsync(L.d_nodes, L.nodes.data(), sizeof(SchurNode) * nn,
-                       cudaMemcpyHostToDevice, h->stream));
-    if (z_tot > h->z_cap) {
-      dfree(h, h->Z);
-      CK(dalloc(h, &h->Z, (size_t)z_tot));
-      h->z_cap = z_tot;
-    }
-    // Z_h = V_h^T [Y_0 .. Y_{l-1} | own U columns of Y_l] on the node's rows:
-    // Z columns [coff_a, coff_a + kmax_a) from level a < l, then the own
-    // rank(U_h) columns at coff_l, one grouped-GEMM problem per panel
-    std::vector<GemmProblem> tn;
-    for (int p = 0; p < nn; ++p) {
-      const SchurNode& sn = L.nodes[p];
-      const int sd = sn.kb + sn.kt;
-      const int mn = L.nmin[p], sp = L.nsplit[p], mx = L.nmax[p];
-      for (int a = 0; a <= l; ++a) {
-        const Level& A = h->lv[a];
-        const int ncols_t = a < l ? A.kmax : sn.kt, ncols_b = a < l ? A.kmax : sn.kb;
-        if (ncols_t > 0 && sn.kb > 0) {
-          GemmProblem t{};
-          t.A = L.V + mn;  // V of the bottom block lives on the top rows
-          t.M = sn.kb;
-          t.K = sp - mn + 1;
-          t.lda = (int)N;
-          t.B = A.Yl + mn;
-          t.N = ncols_t;
-          t.ldb = (int)N;
-          t.C = h->Z + sn.z_off + (int64_t)A.coff * sd;
-          t.ldc = sd;
-          tn.push_back(t);
-        }
-        if (ncols_b > 0 && sn.kt > 0) {
-          GemmProblem b{};
-          b.A = L.V + sp + 1;  // V of the top block lives on the bottom rows
-          b.M = sn.kt;
-          b.K = mx - sp;
-          b.lda = (int)N;
-          b.B = A.Yl + sp + 1;
-          b.N = ncols_b;
-          b.ldb = (int)N;
-          b.C = h->Z + sn.z_off + (int64_t)A.coff * sd + sn.kb;
-          b.ldc = sd;
-          tn.push_back(b);
-        }
-      }
-    }
-    int rc2 = upload_plan(h, tn, true, L.tn);
-    if (rc2) return rc2;
-    int e = run_tn(h, L.tn);
-    if (e) return cuda_fail(h, (cudaError_t)e, "gemm_tn");
-    SchurLaunch S;
-    S.nodes = L.d_nodes;
-    S.S = L.S;
-    S.Z = h->Z;
-    S.R = h->Z;
-    S.piv = L.piv;
-    S.err = h->d_err;
-    std::vector<int> sds(nn);
-    for (int p = 0; p < nn; ++p) sds[p] = L.nodes[p].kb + L.nodes[p].kt;
-    e = schur_factor_launch(S, nn, sds.data(), h->stream);
-    if (e) return cuda_fail(h, (cudaError_t)e, "schur_factor");
-    h->nlaunch += schur_factor_launches(sds.data(), nn);
-    if (L.coff > 0) {
-      e = schur_solve_launch(S, nn, -1, L.coff, L.max_sd, h->stream);
-      if (e) return cuda_fail(h, (cudaError_t)e, "schur_solve");
-      h->nlaunch += 1;
-      // Y_a[rows_h] -= Y_l[rows_h, 0 : rank(U_h)] * y_h[:, level a's columns]
-      // for every ancestor level a < l
-      std::vector<GemmProblem> up;
-      for (int p = 0; p < nn; ++p) {
-        const SchurNode& sn = L.nodes[p];
-        const int sd = sn.kb + sn.kt;
-        const int mn = L.nmin[p], sp = L.nsplit[p], mx = L.nmax[p];
-        for (int a = 0; a < l; ++a) {
-          const Level& A = h->lv[a];
-          if (A.kmax == 0) continue;
-          if (sn.kt > 0) {
-            GemmProblem t{};
-            t.C = A.Yl + mn;
-            t.ldc = (int)N;
-            t.A = L.Yl + mn;
-            t.lda = (int)N;
-            t.M = sp - mn + 1;
-            t.K = sn.kt;
-            t.B = h->Z + sn.z_off + sn.kb + (int64_t)A.coff * sd;
-            t.ldb = sd;
-            t.N = A.kmax;
-            up.push_back(t);
-          }
-          if (sn.kb > 0) {
-            GemmProblem b{};
-            b.C = A.Yl + sp + 1;
-            b.ldc = (int)N;
-            b.A = L.Yl + sp + 1;
-            b.lda = (int)N;
-            b.M = mx - sp;
-            b.K = sn.kb;
-            b.B = h->Z + sn.z_off + (int64_t)A.coff * sd;
-            b.ldb = sd;
-            b.N = A.kmax;
-            up.push_back(b);
-          }
-        }
-      }
-      rc2 = upload_plan(h, up, false, L.nn);
-      if (rc2) return rc2;
-      e = run_nn(h, L.nn);
-      if (e) return cuda_fail(h, (cudaError_t)e, "gemm_nn_sub");
-    }
-  }
-  CK(cudaEventRecord(h->ev1, h->stream));
-  CK(cudaEventSynchronize(h->ev1));
-  float ms = 0;
-  CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
-  h->t_fact = ms * 1e-3;
-  rc = check_dev_err(h, "factorize");
-  if (rc) return rc;
-  h->factored = true;
-  return HODLR_OK;
-}
-
-int build_solve_plans(hodlr_t h, int nrhs) {
-  const int64_t N = h->n;
-  int64_t zs_tot = 0;
-  for (auto& L : h->lv) {
-    int64_t t = 0;
-    for (auto& sn : L.nodes) t += (int64_t)(sn.kb + sn.kt) * nrhs;
-    zs_tot = std::max(zs_tot, t);
-  }
-  if (zs_tot > h->zs_cap) {
-    dfree(h, h->zs);
-    CK(dalloc(h, &h->zs, (size_t)zs_tot));
-    h->zs_cap = zs_tot;
-  }
-  if (nrhs > h->x_cols) {
-    dfree(h, h->X);
-    CK(dalloc(h, &h->X, (size_t)(N * nrhs)));
-    h->x_cols = nrhs;
-  }
-  for (auto& L : h->lv) {
-    if (L.solve_nrhs == nrhs) continue;
-    const int nn = (int)L.nmin.size();
-    std::vector<SchurNode> sn = L.nodes;
-    int64_t off = 0;
-    for (auto& s : sn) {
-      s.r_off = off;
-      off += (int64_t)(s.kb + s.kt) * nrhs;
-    }
-    dfree(h, L.d_snodes);
-    CK(dalloc(h, &L.d_snodes, (size_t)nn));
-    CK(h2d(h, L.d_snodes, sn.data(), sizeof(SchurNode) * nn));
-    std::vector<GemmProblem> tn, up;
-    for (int p = 0; p < nn; ++p) {
-      const int sd = sn[p].kb + sn[p].kt;
-      const int mn = L.nmin[p], sp = L.nsplit[p], mx = L.nmax[p];
-      GemmProblem a{};
-      a.A = L.V + mn;
-      a.M = sn[p].kb;
-      a.K = sp - mn + 1;
-      a.lda = (int)N;
-      a.B = h->X + mn;
-      a.N = nrhs;
-      a.ldb = (int)N;
-      a.C = h->zs + sn[p].r_off;
-      a.ldc = sd;
-      tn.push_back(a);
-      GemmProblem b{};
-      b.A = L.V + sp + 1;
-      b.M = sn[p].kt;
-      b.K = mx - sp;
-      b.lda = (int)N;
-      b.B = h->X + sp + 1;
-      b.N = nrhs;
-      b.ldb = (int)N;
-      b.C = h->zs + sn[p].r_off + sn[p].kb;
-      b.ldc = sd;
-      tn.push_back(b);
-      GemmProblem c{};
-      c.C = h->X + mn;
-      c.ldc = (int)N;
-      c.A = L.Yl + mn;
-      c.lda = (int)N;
-      c.M = sp - mn + 1;
-      c.K = sn[p].kt;
-      c.B = h->zs + sn[p].r_off + sn[p].kb;
-      c.ldb = sd;
-      c.N = nrhs;
-      up.push_back(c);
-      GemmProblem d{};
-      d.C = h->X + sp + 1;
-      d.ldc = (int)N;
-      d.A = L.Yl + sp + 1;
-      d.lda = (int)N;
-      d.M = mx - sp;
-      d.K = sn[p].kb;
-      d.B = h->zs + sn[p].r_off;
-      d.ldb = sd;
-      d.N = nrhs;
-      up.push_back(d);
-    }
-    int rc = upload_plan(h, tn, true, L.stn);
-    if (rc) return rc;
-    rc = upload_plan(h, up, false, L.snn);
-    if (rc) return rc;
-    L.solve_nrhs = nrhs;
-  }
-  return HODLR_OK;
-}
-
-// x <- K_HODLR^-1 b, with b already in h->X (N x nrhs, ld N).
-int solve_in_place(hodlr_t h, int nrhs) {
-  const int64_t N = h->n;
-  LeafSolveLaunch S;
-  S.leaf_min = h->d_leaf_min;
-  S.leaf_size = h->d_leaf_size;
-  S.lu_off = h->d_lu_off;
-  S.lu = h->d_lu;
-  S.perm = h->d_perm;
-  S.X = h->X;
-  S.ldx = N;
-  S.ncols = nrhs;
-  int e = leaf_solve_launch(S, (int)h->leaf_min.size(), h->smax, h->stream);
-  if (e) return cuda_fail(h, (cudaError_t)e, "leaf_solve");
-  h->nlaunch += 1;
-  for (int l = (int)h->lv.size() - 1; l >= 0; --l) {
-    Level& L = h->lv[l];
-    const int nn = (int)L.nmin.size();
-    e = run_tn(h, L.stn);
-    if (e) return cuda_fail(h, (cudaError_t)e, "solve gemm_tn");
-    SchurLaunch SL;
-    SL.nodes = L.d_snodes;
-    SL.S = L.S;
-    SL.Z = nullptr;
-    SL.R = h->zs;
-    SL.piv = L.piv;
-    SL.err = h->d_err;
-    e = schur_solve_launch(SL, nn, nrhs, nrhs, L.max_sd, h->stream);
-    if (e) return cuda_fail(h, (cudaError_t)e, "solve schur");
-    h->nlaunch += 1;
-    e = run_nn(h, L.snn);
-    if (e) return cuda_fail(h, (cudaError_t)e, "solve gemm_nn");
-  }
-  return HODLR_OK;
-}
-
-// solve_in_place through a CUDA graph: captured on first use, replayed while
-// the right-hand-side count, stream, buffers, precision and factorization
-// are the same (one launch instead of ~4 per level).
-int solve_fast(hodlr_t h, int nrhs) {
-  if (h->sg_off) return solve_in_place(h, nrhs);
-  const void* key[4] = {h->X, h->zs, h->ws, (const void*)(intptr_t)(h->gemm_prec + 1)};
-  bool same = h->sg_exec && h->sg_nrhs == nrhs && h->sg_stream == h->stream &&
-              h->sg_gen == h->factor_gen;
-  for (int i = 0; i < 4 && same; ++i) same = key[i] == h->sg_key[i];
-  if (!same) {
-    drop_solve_graph(h);
-    const long long before = h->nlaunch;
-    if (cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
-      cudaGetLastError();
-      h->sg_off = true;
-      return solve_in_place(h, nrhs);
-    }
-    int rc = solve_in_place(h, nrhs);
-    cudaGraph_t g = nullptr;
-    cudaError_t e = cudaStreamEndCapture(h->stream, &g);
-    cudaGraphExec_t ex = nullptr;
-    if (!rc && e == cudaSuccess && g) e = cudaGraphInstantiate(&ex, g, 0);
-    if (g) cudaGraphDestroy(g);
-    if (rc || e != cudaSuccess || !ex) {  // not capturable here: launch directly
-      cudaGetLastError();
-      h->sg_off = true;
-      h->nlaunch = before;
-      h->err.clear();
-      return solve_in_place(h, nrhs);
-    }
-    h->sg_exec = ex;
-    h->sg_nrhs = nrhs;
-    h->sg_stream = h->stream;
-    h->sg_gen = h->factor_gen;
-    for (int i = 0; i < 4; ++i) h->sg_key[i] = key[i];
-    h->sg_launches = h->nlaunch - before;
-    h->nlaunch = before;
-  }
-  CK(cudaGraphLaunch(h->sg_exec, h->stream));
-  h->nlaunch += h->sg_launches;
-  return HODLR_OK;
-}
-
-int do_solve_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double* d_x, int ldx,
-                    bool host_io) {
-  int rc = do_factorize(h);
-  if (rc) return rc;
-  rc = build_solve_plans(h, nrhs);
-  if (rc) return rc;
-  const int64_t N = h->n;
-  cudaMemcpyKind kin = host_io ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
-  cudaMemcpyKind kout = host_io ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
-  CK(cudaEventRecord(h->ev0, h->stream));
-  CK(cudaMemcpy2DAsync(h->X, sizeof(double) * N, d_b, sizeof(double) * ldb, sizeof(double) * N,
-                       nrhs, kin, h->stream));
-  rc = solve_fast(h, nrhs);
-  if (rc) return rc;
-  CK(cudaMemcpy2DAsync(d_x, sizeof(double) * ldx, h->X, sizeof(double) * N, sizeof(double) * N,
-                       nrhs, kout, h->stream));
-  CK(cudaEventRecord(h->ev1, h->stream));
-  CK(cudaEventSynchronize(h->ev1));
-  float ms = 0;
-  CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
-  h->t_solve = ms * 1e-3;
-  h->t_total = h->t_lr + h->t_fact + h->t_solve;
-  return check_dev_err(h, "solve");
-}
-
-constexpr int IR_BLOCKS = 256;
-
-// R = B - Y (stored in Y) and per-block partial sums of |R_c|^2 and |B_c|^2.
-__global__ void ir_residual_kernel(const double* B, double* Y, int64_t n, int nrhs,
-                                   double* part) {
-  __shared__ double red[2][8];
-  for (int c = 0; c < nrhs; ++c) {
-    double rr = 0.0, bb = 0.0;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * blockDim.x) {
-      double b = B[c * n + i];
-      double r = b - Y[c * n + i];
-      Y[c * n + i] = r;
-      rr = fma(r, r, rr);
-      bb = fma(b, b, bb);
-    }
-    rr = warp_sum(rr);
-    bb = warp_sum(bb);
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (lane == 0) {
-      red[0][w] = rr;
-      red[1][w] = bb;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double a = 0.0, d = 0.0;
-      for (int q = 0; q < (int)(blockDim.x >> 5); ++q) {
-        a += red[0][q];
-        d += red[1][q];
-      }
-      part[(int64_t)(2 * c) * gridDim.x + blockIdx.x] = a;
-      part[(int64_t)(2 * c + 1) * gridDim.x + blockIdx.x] = d;
-    }
-    __syncthreads();
-  }
-}
-
-// Forest refinement: per system s (one CTA) and column c, r = b - y over
-// the system's rows, out = (|r|^2, |b|^2); Y becomes r, or 0 for a system
-// already converged (its x is left as it is).
-__global__ void forest_residual_kernel(const double* B, double* Y, int64_t n, int nrhs,
-                                       const int* off, const unsigned char* done, double* out) {
-  __shared__ double red[2][8];
-  const int s = blockIdx.x;
-  const int r0 = off[s], r1 = off[s + 1];
-  for (int c = 0; c < nrhs; ++c) {
-    double rr = 0.0, bb = 0.0;
-    for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
-      const double b = B[c * n + i];
-      const double r = b - Y[c * n + i];
-      Y[c * n + i] = done[s] ? 0.0 : r;
-      rr = fma(r, r, rr);
-      bb = fma(b, b, bb);
-    }
-    rr = warp_sum(rr);
-    bb = warp_sum(bb);
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (lane == 0) {
-      red[0][w] = rr;
-      red[1][w] = bb;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double a = 0.0, d = 0.0;
-      for (int q = 0; q < (int)(blockDim.x >> 5); ++q) {
-        a += red[0][q];
-        d += red[1][q];
-      }
-      out[2 * ((int64_t)s * nrhs + c)] = a;
-      out[2 * ((int64_t)s * nrhs + c) + 1] = d;
-    }
-    __syncthreads();
-  }
-}
-
-__global__ void axpy_cols_kernel(double* X, const double* D, int64_t total) {
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
-       e += (int64_t)gridDim.x * blockDim.x)
-    X[e] += D[e];
-}
-
-int kmatvec_dev(hodlr_t h, int nrhs, const double* d_x, int ldx, double* d_y, int ldy) {
-  if (h->nsys) {  // forest: block-diagonal product
-    KmatvecLaunch L;
-    L.src = make_src(h);
-    L.X = d_x;
-    L.ldx = ldx;
-    L.Y = d_y;
-    L.ldy = ldy;
-    L.ws = nullptr;
-    L.n = h->n;
-    L.nrhs = nrhs;
-    int e = kmatvec_forest_launch(L, h->d_fitems, h->ftype_off, h->stream);
-    if (e) return cuda_fail(h, (cudaError_t)e, "forest kmatvec");
-    for (int t = 0; t < HX_FOREST_TYPES; ++t) h->nlaunch += h->ftype_off[t + 1] > h->ftype_off[t];
-    return HODLR_OK;
-  }
-  const int sym = kmatvec_sym_slices(h->n, nrhs, h->dense);
-  const int sp = sym ? sym : kmatvec_splits(h->n, h->num_sms);
-  if (sym || sp > 1) {
-    int rc = ensure_ws(h, (int64_t)sp * nrhs * h->n);
-    if (rc) return rc;
-  }
-  KmatvecLaunch L;
-  L.src = make_src(h);
-  L.X = d_x;
-  L.ldx = ldx;
-  L.Y = d_y;
-  L.ldy = ldy;
-  L.ws = h->ws;
-  L.n = h->n;
-  L.nrhs = nrhs;
-  int e = sym ? kmatvec_sym_launch(L, sym, h->stream) : kmatvec_launch(L, sp, h->stream);
-  if (e) return cuda_fail(h, (cudaError_t)e, "kmatvec");
-  h->nlaunch += 1 + (sym || sp > 1);
-  return HODLR_OK;
-}
-
-
-// Iterative refinement: x0 = M^-1 b, then x += M^-1 (b - K x) until
-// max_c ||b_c - K x_c|| / ||b_c|| <= tol or max_iter corrections.  b and x
-// are device pointers (ld n).  *iters = corrections applied.
-int refine_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double* d_x, int ldx,
-                  double tol, int max_iter, int* iters, double* relres) {
-  const int64_t N = h->n;
-  int rc = build_solve_plans(h, nrhs);
-  if (rc) return rc;
-  if (nrhs > h->ir_cols) {
-    dfree(h, h->ir_b);
-    dfree(h, h->ir_x);
-    dfree(h, h->ir_y);
-    dfree(h, h->ir_part);
-    CK(dalloc(h, &h->ir_b, (size_t)(N * nrhs)));
-    CK(dalloc(h, &h->ir_x, (size_t)(N * nrhs)));
-    CK(dalloc(h, &h->ir_y, (size_t)(N * nrhs)));
-    CK(dalloc(h, &h->ir_part, (size_t)(2 * nrhs * IR_BLOCKS)));
-    h->ir_cols = nrhs;
-  }
-  CK(cudaMemcpy2DAsync(h->ir_b, sizeof(double) * N, d_b, sizeof(double) * ldb,
-                       sizeof(double) * N, nrhs, cudaMemcpyDeviceToDevice, h->stream));
-  CK(cudaMemcpyAsync(h->X, h->ir_b, sizeof(double) * N * nrhs, cudaMemcpyDeviceToDevice,
-                     h->stream));
-  rc = solve_fast(h, nrhs);
-  if (rc) return rc;
-  CK(cudaMemcpyAsync(h->ir_x, h->X, sizeof(double) * N * nrhs, cudaMemcpyDeviceToDevice,
-                     h->stream));
-  std::vector<double> part((size_t)2 * nrhs * IR_BLOCKS);
-  double worst = HUGE_VAL;
-  int it = 0;
-  for (;; ++it) {
-    for (int c0 = 0; c0 < nrhs; c0 += 16) {
-      int nc = std::min(16, nrhs - c0);
-      rc = kmatvec_dev(h, nc, h->ir_x + c0 * N, (int)N, h->ir_y + c0 * N, (int)N);
-      if (rc) return rc;
-    }
-    ir_residual_kernel<<<IR_BLOCKS, 256, 0, h->stream>>>(h->ir_b, h->ir_y, N, nrhs, h->ir_part);
-    CK(cudaGetLastError());
-    h->nlaunch += 1;
-    CK(cudaMemcpyAsync(part.data(), h->ir_part, sizeof(double) * part.size(),
-                       cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
-    worst = 0.0;
-    for (int c = 0; c < nrhs; ++c) {
-      double a = 0.0, d = 0.0;
-      for (int q = 0; q < IR_BLOCKS; ++q) {
-        a += part[(size_t)(2 * c) * IR_BLOCKS + q];
-        d += part[(size_t)(2 * c + 1) * IR_BLOCKS + q];
-      }
-      double r = d > 0 ? std::sqrt(a / d) : std::sqrt(a);
-      if (relres) relres[c] = r;
-      worst = std::max(worst, r);
-    }
-    if (worst <= tol || it >= max_iter) break;
-    CK(cudaMemcpyAsync(h->X, h->ir_y, sizeof(double) * N * nrhs, cudaMemcpyDeviceToDevice,
-                       h->stream));
-    rc = solve_fast(h, nrhs);
-    if (rc) return rc;
-    axpy_cols_kernel<<<1024, 256, 0, h->stream>>>(h->ir_x, h->X, N * nrhs);
-    CK(cudaGetLastError());
-    h->nlaunch += 1;
-  }
-  if (iters) *iters = it;
-  CK(cudaMemcpy2DAsync(d_x, sizeof(double) * ldx, h->ir_x, sizeof(double) * N,
-                       sizeof(double) * N, nrhs, cudaMemcpyDeviceToDevice, h->stream));
-  CK(cudaStreamSynchronize(h->stream));
-  return check_dev_err(h, "refine");
-}
-
-// Iterative refinement of a forest with a stopping test per system:
-// x0 = M^-1 b, then x += M^-1 (b - K x) on the systems whose
-// max_c ||b_c - K x_c|| / ||b_c|| (over the system's rows) is still above
-// tol.  relres: nsys x nrhs, system-major.
-int forest_refine_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double* d_x, int ldx,
-                         double tol, int max_iter, int* iters, double* relres) {
-  const int64_t N = h->n;
-  const int S = h->nsys;
-  int rc = build_solve_plans(h, nrhs);
-  if (rc) return rc;
-  if (nrhs > h->ir_cols) {
-    dfree(h, h->ir_b);
-    dfree(h, h->ir_x);
-    dfree(h, h->ir_y);
-    dfree(h, h->ir_part);
-    CK(dalloc(h, &h->ir_b, (size_t)(N * nrhs)));
-    CK(dalloc(h, &h->ir_x, (size_t)(N * nrhs)));
-    CK(dalloc(h, &h->ir_y, (size_t)(N * nrhs)));
-    CK(dalloc(h, &h->ir_part, (size_t)(2 * nrhs * IR_BLOCKS)));
-    h->ir_cols = nrhs;
-  }
-  double* d_out = nullptr;
-  unsigned char* d_done = nullptr;
-  int* d_off = nullptr;
-  CK(dalloc(h, &d_out, (size_t)2 * S * nrhs));
-  CK(dalloc(h, &d_done, (size_t)S));
-  CK(dalloc(h, &d_off, (size_t)S + 1));
-  CK(cudaMemcpyAsync(d_off, h->sys_off.data(), sizeof(int) * (S + 1), cudaMemcpyHostToDevice,
-                     h->stream));
-  CK(cudaMemsetAsync(d_done, 0, (size_t)S, h->stream));
-  CK(cudaMemcpy2DAsync(h->ir_b, sizeof(double) * N, d_b, sizeof(double) * ldb,
-                       sizeof(double) * N, nrhs, cudaMemcpyDeviceToDevice, h->stream));
-  CK(cudaMemcpyAsync(h->X, h->ir_b, sizeof(double) * N * nrhs, cudaMemcpyDeviceToDevice,
-                     h->stream));
-  rc = solve_fast(h, nrhs);
-  if (rc) return rc;
-  CK(cudaMemcpyAsync(h->ir_x, h->X, sizeof(double) * N * nrhs, cudaMemcpyDeviceToDevice,
-                     h->stream));
-  std::vector<double> out((size_t)2 * S * nrhs);
-  std::vector<unsigned char> done((size_t)S, 0);
-  int it = 0;
-  for (;; ++it) {
-    for (int c0 = 0; c0 < nrhs; c0 += 16) {
-      int nc = std::min(16, nrhs - c0);
-      rc = kmatvec_dev(h, nc, h->ir_x + c0 * N, (int)N, h->ir_y + c0 * N, (int)N);
-      if (rc) return rc;
-    }
-    forest_residual_kernel<<<S, 256, 0, h->stream>>>(h->ir_b, h->ir_y, N, nrhs, d_off, d_done,
-                                                     d_out);
-    CK(cudaGetLastError());
-    h->nlaunch += 1;
-    CK(d2h(h, out.data(), d_out, sizeof(double) * out.size()));
-    bool all = true;
-    for (int q = 0; q < S; ++q) {
-      double worst = 0.0;
-      for (int c = 0; c < nrhs; ++c) {
-        const double a = out[2 * ((size_t)q * nrhs + c)], d = out[2 * ((size_t)q * nrhs + c) + 1];
-        const double r = d > 0 ? std::sqrt(a / d) : std::sqrt(a);
-        if (!done[q] && relres) relres[(size_t)q * nrhs + c] = r;
-        worst = std::max(worst, r);
-      }
-      if (!done[q] && !(worst > tol)) done[q] = 1;
-      all &= done[q] != 0;
-    }
-    if (all || it >= max_iter) break;
-    // systems that converged in this pass still take this correction (their
-    // residual rows were written); from the next pass on they are frozen
-    CK(cudaMemcpyAsync(h->X, h->ir_y, sizeof(double) * N * nrhs, cudaMemcpyDeviceToDevice,
-                       h->stream));
-    rc = solve_fast(h, nrhs);
-    if (rc) return rc;
-    axpy_cols_kernel<<<1024, 256, 0, h->stream>>>(h->ir_x, h->X, N * nrhs);
-    CK(cudaGetLastError());
-    h->nlaunch += 1;
-    CK(cudaMemcpyAsync(d_done, done.data(), (size_t)S, cudaMemcpyHostToDevice, h->stream));
-  }
-  if (iters) *iters = it;
-  CK(cudaMemcpy2DAsync(d_x, sizeof(double) * ldx, h->ir_x, sizeof(double) * N,
-                       sizeof(double) * N, nrhs, cudaMemcpyDeviceToDevice, h->stream));
-  CK(cudaStreamSynchronize(h->stream));
-  dfree(h, d_out);
-  dfree(h, d_done);
-  dfree(h, d_off);
-  return check_dev_err(h, "forest refine");
-}
-
-// ------------------------------------------------------------- GMRES
-constexpr int GM_BLOCKS = 256;
-
-// part[(i * nrhs + c) * GM_BLOCKS + blk] = sum over this block's rows of
-// V_i[:, c] . W[:, c] for i < nv (V_i = V + i * n * nrhs).
-__global__ void gm_dots_kernel(const double* V, int nv, const double* W, int64_t n, int nrhs,
-                               double* part) {
-  __shared__ double red[8];
-  const int i = blockIdx.y;
-  const double* Vi = V + (int64_t)i * n * nrhs;
-  for (int c = 0; c < nrhs; ++c) {
-    double a = 0.0;
-    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n;
-         r += (int64_t)gridDim.x * blockDim.x)
-      a = fma(Vi[c * n + r], W[c * n + r], a);
-    a = warp_sum(a);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = a;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double t = 0.0;
-      for (int q = 0; q < (int)(blockDim.x >> 5); ++q) t += red[q];
-      part[((int64_t)i * nrhs + c) * gridDim.x + blockIdx.x] = t;
-    }
-    __syncthreads();
-  }
-}
-
-// out[k] = sum of the GM_BLOCKS partials of k (fixed order).
-__global__ void gm_sum_kernel(const double* part, int count, double* out) {
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
-    double t = 0.0;
-    for (int q = 0; q < GM_BLOCKS; ++q) t += part[(int64_t)k * GM_BLOCKS + q];
-    out[k] = t;
-  }
-}
-
-// W[:, c] -= sum_{i < nv} coef[i * nrhs + c] * V_i[:, c]
-__global__ void gm_sub_kernel(const double* V, int nv, const double* coef, double* W, int64_t n,
-                              int nrhs) {
-  const int64_t total = n * nrhs;
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
-       e += (int64_t)gridDim.x * blockDim.x) {
-    const int c = (int)(e / n);
-    double w = W[e];
-    for (int i = 0; i < nv; ++i) w = fma(-coef[i * nrhs + c], V[(int64_t)i * total + e], w);
-    W[e] = w;
-  }
-}
-
-// Y[:, c] = X[:, c] * scale[c] (scale 0 gives an exact zero column)
-__global__ void gm_scale_kernel(const double* X, const double* scale, double* Y, int64_t n,
-                                int nrhs) {
-  const int64_t total = n * nrhs;
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
-       e += (int64_t)gridDim.x * blockDim.x) {
-    const double sc = scale[e / n];
-    Y[e] = sc == 0.0 ? 0.0 : X[e] * sc;
-  }
-}
-
-// Host-side launch helpers bound to the handle's stream.
-int gm_dots(hodlr_t h, const double* V, int nv, const double* W, int nrhs, std::vector<double>& out) {
-  const int64_t N = h->n;
-  gm_dots_kernel<<<dim3(GM_BLOCKS, nv), 256, 0, h->stream>>>(V, nv, W, N, nrhs, h->gm_part);
-  gm_sum_kernel<<<(nv * nrhs + 255) / 256, 256, 0, h->stream>>>(h->gm_part, nv * nrhs, h->gm_h);
-  CK(cudaGetLastError());
-  h->nlaunch += 2;
-  out.resize((size_t)nv * nrhs);
-  CK(cudaMemcpyAsync(out.data(), h->gm_h, sizeof(double) * nv * nrhs, cudaMemcpyDeviceToHost,
-                     h->stream));
-  CK(cudaStreamSynchronize(h->stream));
-  return HODLR_OK;
-}
-
-int gm_sub(hodlr_t h, const double* V, int nv, const std::vector<double>& coef, double* W, int nrhs) {
-  const int64_t N = h->n;
-  CK(cudaMemcpyAsync(h->gm_h, coef.data(), sizeof(double) * nv * nrhs, cudaMemcpyHostToDevice,
-                     h->stream));
-  gm_sub_kernel<<<1024, 256, 0, h->stream>>>(V, nv, h->gm_h, W, N, nrhs);
-  CK(cudaGetLastError());
-  h->nlaunch += 1;
-  return HODLR_OK;
-}
-
-int gm_scale(hodlr_t h, const double* X, const std::vector<double>& sc, double* Y, int nrhs) {
-  const int64_t N = h->n;
-  CK(cudaMemcpyAsync(h->gm_h, sc.data(), sizeof(double) * nrhs, cudaMemcpyHostToDevice,
-                     h->stream));
-  gm_scale_kernel<<<1024, 256, 0, h->stream>>>(X, h->gm_h, Y, N, nrhs);
-  CK(cudaGetLastError());
-  h->nlaunch += 1;
-  return HODLR_OK;
-}
-
-// Restarted GMRES(m) on K x = b with the HODLR factor as a right
-// preconditioner (K M^-1 u = b, x = M^-1 u), all columns in lockstep so every
-// iteration costs one full-kernel product and one HODLR solve for all of
-// them.  Starts from the direct solve (the initial guess of iterative_Solve,
-// src/HODLR_Matrix.cpp:1169-1177) and stops when the true relative residual
-// max_c ||b_c - K x_c|| / ||b_c|| <= tol.  Classical Gram-Schmidt with one
-// re-orthogonalisation; Givens rotations as in IML's GMRES
-// (IML/include/gmres.h:83-153).
-int gmres_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double* d_x, int ldx,
-                 double tol, int max_iter, int m, int* iters, double* relres) {
-  const int64_t N = h->n;
-  int rc = build_solve_plans(h, nrhs);
-  if (rc) return rc;
-  if (nrhs > h->ir_cols) {
-    dfree(h, h->ir_b);
-    dfree(h, h->ir_x);
-    dfree(h, h->ir_y);
-    dfree(h, h->ir_part);
-    CK(dalloc(h, &h->ir_b, (size_t)(N * nrhs)));
-    CK(dalloc(h, &h->ir_x, (size_t)(N * nrhs)));
-    CK(dalloc(h, &h->ir_y, (size_t)(N * nrhs)));
-    CK(dalloc(h, &h->ir_part, (size_t)(2 * nrhs * IR_BLOCKS)));
-    h->ir_cols = nrhs;
-  }
-  if (m > h->gm_m || nrhs > h->gm_cols) {
-    dfree(h, h->gm_V);
-    dfree(h, h->gm_Z);
-    dfree(h, h->gm_h);
-    dfree(h, h->gm_part);
-    CK(dalloc(h, &h->gm_V, (size_t)((m + 1) * N * nrhs)));
-    CK(dalloc(h, &h->gm_Z, (size_t)(m * N * nrhs)));
-    CK(dalloc(h, &h->gm_h, (size_t)((m + 2) * nrhs)));
-    CK(dalloc(h, &h->gm_part, (size_t)((m + 2) * nrhs * GM_BLOCKS)));
-    h->gm_m = m;
-    h->gm_cols = nrhs;
-  }
-  const int64_t P = N * nrhs;
-  CK(cudaMemcpy2DAsync(h->ir_b, sizeof(double) * N, d_b, sizeof(double) * ldb,
-                       sizeof(double) * N, nrhs, cudaMemcpyDeviceToDevice, h->stream));
-  // x0 = M^-1 b
-  CK(cudaMemcpyAsync(h->X, h->ir_b, sizeof(double) * P, cudaMemcpyDeviceToDevice, h->stream));
-  rc = solve_fast(h, nrhs);
-  if (rc) return rc;
-  CK(cudaMemcpyAsync(h->ir_x, h->X, sizeof(double) * P, cudaMemcpyDeviceToDevice, h->stream));
-  std::vector<double> bnorm, tmp, hcol, coef;
-  rc = gm_dots(h, h->ir_b, 1, h->ir_b, nrhs, bnorm);
-  if (rc) return rc;
-  for (auto& v : bnorm) v = v > 0 ? std::sqrt(v) : 1.0;
-  int total_it = 0;
-  std::vector<double> worst_res(nrhs, HUGE_VAL);
-  for (int cycle = 0;; ++cycle) {
-    // r = b - K x  -> ir_y ; beta = ||r||
-    for (int c0 = 0; c0 < nrhs; c0 += 16) {
-      int nc = std::min(16, nrhs - c0);
-      rc = kmatvec_dev(h, nc, h->ir_x + c0 * N, (int)N, h->ir_y + c0 * N, (int)N);
-      if (rc) return rc;
-    }
-    ir_residual_kernel<<<IR_BLOCKS, 256, 0, h->stream>>>(h->ir_b, h->ir_y, N, nrhs, h->ir_part);
-    CK(cudaGetLastError());
-    h->nlaunch += 1;
-    rc = gm_dots(h, h->ir_y, 1, h->ir_y, nrhs, tmp);
-    if (rc) return rc;
-    std::vector<double> beta(nrhs);
-    double worst = 0.0;
-    for (int c = 0; c < nrhs; ++c) {
-      beta[c] = std::sqrt(std::max(tmp[c], 0.0));
-      worst_res[c] = beta[c] / bnorm[c];
-      worst = std::max(worst, worst_res[c]);
-    }
-    if (worst <= tol || total_it >= max_iter) break;
-    // V0 = r / beta
-    std::vector<double> sc(nrhs);
-    for (int c = 0; c < nrhs; ++c) sc[c] = beta[c] > 0 ? 1.0 / beta[c] : 0.0;
-    rc = gm_scale(h, h->ir_y, sc, h->gm_V, nrhs);
-    if (rc) return rc;
-    // per-column Hessenberg (column-major (m+1) x m), rotations, rhs g
-    std::vector<double> H((size_t)(m + 1) * m * nrhs, 0.0), cs((size_t)m * nrhs),
-        sn((size_t)m * nrhs), g((size_t)(m + 1) * nrhs, 0.0);
-    for (int c = 0; c < nrhs; ++c) g[c] = beta[c];
-    std::vector<int> done(nrhs, 0), used(nrhs, 0);
-    for (int c = 0; c < nrhs; ++c)
-      if (worst_res[c] <= tol) done[c] = 1;
-    int j = 0;
-    for (; j < m && total_it < max_iter; ++j, ++total_it) {
-      double* Vj = h->gm_V + (int64_t)j * P;
-      double* Zj = h->gm_Z + (int64_t)j * P;
-      // Z_j = M^-1 V_j ; W = K Z_j
-      CK(cudaMemcpyAsync(h->X, Vj, sizeof(double) * P, cudaMemcpyDeviceToDevice, h->stream));
-      rc = solve_fast(h, nrhs);
-      if (rc) return rc;
-      CK(cudaMemcpyAsync(Zj, h->X, sizeof(double) * P, cudaMemcpyDeviceToDevice, h->stream));
-      for (int c0 = 0; c0 < nrhs; c0 += 16) {
-        int nc = std::min(16, nrhs - c0);
-        rc = kmatvec_dev(h, nc, Zj + c0 * N, (int)N, h->ir_y + c0 * N, (int)N);
-        if (rc) return rc;
-      }
-      // classical Gram-Schmidt, twice
-      std::vector<double> hsum((size_t)(j + 1) * nrhs, 0.0);
-      for (int pass = 0; pass < 2; ++pass) {
-        rc = gm_dots(h, h->gm_V, j + 1, h->ir_y, nrhs, hcol);
-        if (rc) return rc;
-        for (int c = 0; c < nrhs; ++c)
-          if (done[c])
-            for (int i = 0; i <= j; ++i) hcol[(size_t)i * nrhs + c] = 0.0;
-        rc = gm_sub(h, h->gm_V, j + 1, hcol, h->ir_y, nrhs);
-        if (rc) return rc;
-        for (size_t q = 0; q < hsum.size(); ++q) hsum[q] += hcol[q];
-      }
-      rc = gm_dots(h, h->ir_y, 1, h->ir_y, nrhs, tmp);
-      if (rc) return rc;
-      std::vector<double> inv(nrhs, 0.0);
-      bool all_done = true;
-      for (int c = 0; c < nrhs; ++c) {
-        if (done[c]) continue;
-        double* Hc = &H[(size_t)c * (m + 1) * m];
-        for (int i = 0; i <= j; ++i) Hc[(size_t)j * (m + 1) + i] = hsum[(size_t)i * nrhs + c];
-        double hn = std::sqrt(std::max(tmp[c], 0.0));
-        Hc[(size_t)j * (m + 1) + j + 1] = hn;
-        inv[c] = hn > 0 ? 1.0 / hn : 0.0;
-        // apply previous rotations, then a new one
-        for (int i = 0; i < j; ++i) {
-          double a = Hc[(size_t)j * (m + 1) + i], b2 = Hc[(size_t)j * (m + 1) + i + 1];
-          double ci = cs[(size_t)c * m + i], si = sn[(size_t)c * m + i];
-          Hc[(size_t)j * (m + 1) + i] = ci * a + si * b2;
-          Hc[(size_t)j * (m + 1) + i + 1] = -si * a + ci * b2;
-        }
-        double a = Hc[(size_t)j * (m + 1) + j], b2 = Hc[(size_t)j * (m + 1) + j + 1];
-        double r = std::hypot(a, b2);
-        double ci = r > 0 ? a / r : 1.0, si = r > 0 ? b2 / r : 0.0;
-        cs[(size_t)c * m + j] = ci;
-        sn[(size_t)c * m + j] = si;
-        Hc[(size_t)j * (m + 1) + j] = r;
-        Hc[(size_t)j * (m + 1) + j + 1] = 0.0;
-        double gj = g[(size_t)j * nrhs + c];
-        g[(size_t)j * nrhs + c] = ci * gj;
-        g[(size_t)(j + 1) * nrhs + c] = -si * gj;
-        used[c] = j + 1;
-        // stop this column a little below tol; the true residual decides
-        if (std::fabs(g[(size_t)(j + 1) * nrhs + c]) <= 0.5 * tol * bnorm[c] || hn == 0.0)
-          done[c] = 1;
-        if (!done[c]) all_done = false;
-      }
-      rc = gm_scale(h, h->ir_y, inv, h->gm_V + (int64_t)(j + 1) * P, nrhs);
-      if (rc) return rc;
-      if (all_done) {
-        ++j;
-        ++total_it;
-        break;
-      }
-    }
-    // x += Z y, y from the triangular systems (per column)
-    std::vector<double> ycoef((size_t)m * nrhs, 0.0);
-    int nv = 0;
-    for (int c = 0; c < nrhs; ++c) {
-      const int k = used[c];
-      nv = std::max(nv, k);
-      const double* Hc = &H[(size_t)c * (m + 1) * m];
-      for (int i = k - 1; i >= 0; --i) {
-        double t = g[(size_t)i * nrhs + c];
-        for (int q = i + 1; q < k; ++q) t -= Hc[(size_t)q * (m + 1) + i] * ycoef[(size_t)q * nrhs + c];
-        ycoef[(size_t)i * nrhs + c] = Hc[(size_t)i * (m + 1) + i] != 0 ? t / Hc[(size_t)i * (m + 1) + i] : 0.0;
-      }
-    }
-    if (nv > 0) {
-      for (auto& v : ycoef) v = -v;  // gm_sub subtracts
-      rc = gm_sub(h, h->gm_Z, nv, ycoef, h->ir_x, nrhs);
-      if (rc) return rc;
-    }
-    (void)j;
-  }
-  if (iters) *iters = total_it;
-  if (relres)
-    for (int c = 0; c < nrhs; ++c) relres[c] = worst_res[c];
-  CK(cudaMemcpy2DAsync(d_x, sizeof(double) * ldx, h->ir_x, sizeof(double) * N,
-                       sizeof(double) * N, nrhs, cudaMemcpyDeviceToDevice, h->stream));
-  CK(cudaStreamSynchronize(h->stream));
-  return check_dev_err(h, "gmres");
-}
-
-int init_common(hodlr_t h) {
-  int dev = 0;
-  CK(cudaGetDevice(&dev));
-  CK(cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, dev));
-  int coop = 0;
-  CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
-  if (!coop) return fail(h, HODLR_ERR_UNSUPPORTED, "device lacks cooperative launch");
-  CK(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
-  h->stream = h->own_stream;
-  CK(cudaEventCreate(&h->ev0));
-  CK(cudaEventCreate(&h->ev1));
-  CK(dalloc(h, &h->d_err, 1));
-  CK(cudaMemsetAsync(h->d_err, 0, sizeof(unsigned), h->stream));
-  build_tree(h);
-  const int nl = (int)h->leaf_min.size();
-  if (h->smax > 160) return fail(h, HODLR_ERR_UNSUPPORTED, "leaf size above 160");
-  CK(dalloc(h, &h->d_leaf_min, (size_t)nl));
-  CK(dalloc(h, &h->d_leaf_size, (size_t)nl));
-  CK(h2d(h, h->d_leaf_min, h->leaf_min.data(), 4 * nl));
-  CK(h2d(h, h->d_leaf_size, h->leaf_size.data(), 4 * nl));
-  return HODLR_OK;
-}
-
-}  // namespace
+// C ABI of the B200 HODLR solver (include/hodlr_b200.h).  Entry points check
+// their arguments and forward to the host orchestration units (handle.h).
+#include "handle.h"
+
+using namespace hodlr_impl;
 
 // ---------------------------------------------------------------- C ABI
 extern "C" {
@@ -2383,42 +208,7 @@ int hodlr_set_index_tree_bounds(hodlr_t h, int nnodes, const int* split, const i
 
 int hodlr_logdet(hodlr_t h, double* log_abs_det, int* sign) {
   if (!h || !log_abs_det) return HODLR_ERR_ARG;
-  int rc = do_factorize(h);
-  if (rc) return rc;
-  const int nl = (int)h->leaf_min.size();
-  int nmax = nl;
-  for (auto& L : h->lv) nmax = std::max(nmax, (int)L.nmin.size());
-  double* d_out = nullptr;
-  CK(dalloc(h, &d_out, (size_t)3 * nmax));
-  std::vector<double> out((size_t)3 * nmax);
-  leaf_logdet_kernel<<<nl, 32, 0, h->stream>>>(h->d_lu, h->d_lu_off, h->d_leaf_min,
-                                               h->d_leaf_size, h->d_perm, d_out);
-  CK(cudaGetLastError());
-  CK(d2h(h, out.data(), d_out, sizeof(double) * 3 * nl));
-  double sum = 0.0;
-  long long flips = 0;
-  for (int q = 0; q < nl; ++q) {
-    sum += out[3 * q];
-    flips += (long long)out[3 * q + 1] + (long long)out[3 * q + 2];
-  }
-  // det K = prod_leaves det(leaf) * prod_nodes det(S_node) (Sylvester's
-  // identity at every node of the Woodbury recursion)
-  for (auto& L : h->lv) {
-    const int nn = (int)L.nmin.size();
-    if (!nn) continue;
-    schur_logdet_kernel<<<nn, 32, 0, h->stream>>>(L.d_nodes, L.S, L.piv, d_out);
-    CK(cudaGetLastError());
-    CK(d2h(h, out.data(), d_out, sizeof(double) * 3 * nn));
-    for (int q = 0; q < nn; ++q) {
-      sum += out[3 * q];
-      flips += (long long)out[3 * q + 1] + (long long)out[3 * q + 2];
-    }
-  }
-  h->nlaunch += 1 + (int)h->lv.size();
-  dfree(h, d_out);
-  *log_abs_det = sum;
-  if (sign) *sign = (flips & 1) ? -1 : 1;
-  return check_dev_err(h, "logdet");
+  return do_logdet(h, log_abs_det, sign);
 }
 
 int hodlr_get_num_systems(hodlr_t h, int* nsys) {
