@@ -7,7 +7,8 @@
 // (problem, tile row, tile column, K split); TN products with a long
 // reduction dimension (the top levels) are split along K into a workspace
 // and summed in a fixed order by gemm_splitk_reduce, so results do not
-// depend on scheduling.
+// depend on scheduling.  The products run on the FP64 tensor-core
+// instruction (mma.m8n8k4.f64).
 #include "common.cuh"
 #include "gemm.h"
 
@@ -15,20 +16,33 @@ namespace {
 
 constexpr int BM = 64, BN = 64, BK = 16, NT = 256;
 
+__device__ __forceinline__ void dmma_884(double (&d)[2], double a, double b) {
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+      : "+d"(d[0]), "+d"(d[1])
+      : "d"(a), "d"(b));
+}
+
 // mode: 0 store C = A^T B (or split partial), 1 C -= A B, 2 store C = A B
 //
-// Thread (tx, ty) of the 16 x 16 grid owns rows tx + 16 i and columns
-// ty + 16 j of the 64 x 64 tile, so a warp reads and writes 16 consecutive
-// rows of two columns (coalesced C traffic: the update of the ancestor
-// columns is most of the bytes).  The next k tile is loaded into registers
-// while the current one is consumed (two shared-memory buffers, one barrier
-// per tile).  Each output is still one FMA chain in k order.
+// The products run on the FP64 tensor-core instruction mma.m8n8k4.f64: warp
+// w (of 8) owns rows 32 (w % 2) .. +32 and columns 16 (w / 2) .. +16 of the
+// 64 x 64 tile as 4 x 2 MMA tiles of 8 x 8; each k tile of 16 is four MMA
+// steps of k = 4.  A and B tiles are staged in shared memory, the next one
+// loaded into registers while the current one is consumed (two buffers, one
+// barrier per k tile).  The accumulators then go through shared memory, so
+// that C is read and written by thread (tx, ty) at rows tx + 16 i and columns
+// ty + 16 j: a warp touches 16 consecutive rows of two columns (coalesced C
+// traffic: the update of the ancestor columns is most of the bytes).
 template <bool TRANS_A, int MODE>
 __global__ void __launch_bounds__(NT) gemm_kernel(const GemmProblem* __restrict__ probs,
                                                   const int4* __restrict__ tiles,
                                                   double* __restrict__ ws) {
-  __shared__ double As[2][BK][BM + 2];
-  __shared__ double Bs[2][BK][BN + 2];
+  constexpr int LDS = BM + 2;  // padded row of a staged k slice (BM == BN)
+  constexpr int LDC = BM + 1;  // padded row of the staged result tile
+  static_assert(BM == BN && 2 * 2 * BK * LDS >= BN * LDC, "result tile fits the operand buffers");
+  __shared__ double smem[2 * 2 * BK * LDS];
+  auto As = [&](int b, int k, int m) -> double& { return smem[(b * BK + k) * LDS + m]; };
+  auto Bs = [&](int b, int k, int n) -> double& { return smem[((2 + b) * BK + k) * LDS + n]; };
   const int4 t = tiles[blockIdx.x];
   const GemmProblem P = probs[t.x];
   const int m0 = t.y * BM, n0 = t.z * BN;
@@ -36,12 +50,15 @@ __global__ void __launch_bounds__(NT) gemm_kernel(const GemmProblem* __restrict_
   const int kchunk = P.kchunk > 0 ? P.kchunk : P.K;
   const int kb = ks * kchunk, ke = min(P.K, kb + kchunk);
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int wm = (warp & 1) * 32, wn = (warp >> 1) * 16;
+  const int fr = lane >> 2, fk = lane & 3;  // fragment row / k of this lane
   constexpr int LA = (BK * BM) / NT, LB = (BK * BN) / NT;
-  double acc[4][4];
+  double acc[4][2][2];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+    for (int j = 0; j < 2; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 
   double ra[LA], rb[LB];
   auto load = [&](int k0) {
@@ -75,14 +92,14 @@ __global__ void __launch_bounds__(NT) gemm_kernel(const GemmProblem* __restrict_
     for (int r = 0; r < LA; ++r) {
       const int e = threadIdx.x + r * NT;
       if (TRANS_A)
-        As[buf][e % BK][e / BK] = ra[r];
+        As(buf, e % BK, e / BK) = ra[r];
       else
-        As[buf][e / BM][e % BM] = ra[r];
+        As(buf, e / BM, e % BM) = ra[r];
     }
 #pragma unroll
     for (int r = 0; r < LB; ++r) {
       const int e = threadIdx.x + r * NT;
-      Bs[buf][e % BK][e / BK] = rb[r];
+      Bs(buf, e % BK, e / BK) = rb[r];
     }
   };
 
@@ -110,22 +127,31 @@ __global__ void __launch_bounds__(NT) gemm_kernel(const GemmProblem* __restrict_
     const bool more = k0 + BK < ke;
     if (more) load(k0 + BK);  // in flight while this tile is consumed
 #pragma unroll
-    for (int kk = 0; kk < BK; ++kk) {
-      double a[4], b[4];
+    for (int kk = 0; kk < BK; kk += 4) {
+      double a[4], b[2];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = As[buf][kk][tx + 16 * i];
+      for (int i = 0; i < 4; ++i) a[i] = As(buf, kk + fk, wm + 8 * i + fr);
 #pragma unroll
-      for (int j = 0; j < 4; ++j) b[j] = Bs[buf][kk][ty + 16 * j];
+      for (int j = 0; j < 2; ++j) b[j] = Bs(buf, kk + fk, wn + 8 * j + fr);
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+        for (int j = 0; j < 2; ++j) dmma_884(acc[i][j], a[i], b[j]);
     }
     if (more) store(buf ^ 1);  // the other buffer: last read before the previous barrier
     __syncthreads();
     buf ^= 1;
   }
-  // epilogue
+  // accumulators (lane: row fr, columns 2 fk, 2 fk + 1 of each 8 x 8 tile)
+  // to the staged result tile, then out in the coalesced mapping
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+      for (int e = 0; e < 2; ++e)
+        smem[(wn + 8 * j + 2 * fk + e) * LDC + wm + 8 * i + fr] = acc[i][j][e];
+  __syncthreads();
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
     const int gn = n0 + ty + 16 * j;
@@ -134,12 +160,13 @@ __global__ void __launch_bounds__(NT) gemm_kernel(const GemmProblem* __restrict_
     for (int i = 0; i < 4; ++i) {
       const int gm = m0 + tx + 16 * i;
       if (gm >= P.M) continue;
+      const double v = smem[(ty + 16 * j) * LDC + tx + 16 * i];
       if (MODE == 1) {
-        P.C[(int64_t)gn * P.ldc + gm] = cold[i][j] - acc[i][j];
+        P.C[(int64_t)gn * P.ldc + gm] = cold[i][j] - v;
       } else if (MODE == 0 && P.splits > 1) {
-        ws[P.ws_off + ((int64_t)ks * P.N + gn) * P.M + gm] = acc[i][j];
+        ws[P.ws_off + ((int64_t)ks * P.N + gn) * P.M + gm] = v;
       } else {
-        P.C[(int64_t)gn * P.ldc + gm] = acc[i][j];
+        P.C[(int64_t)gn * P.ldc + gm] = v;
       }
     }
   }
