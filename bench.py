@@ -317,6 +317,8 @@ def run_ours(args, rank, world, local_rank):
         g.set_precision("fp64")
         g.recLU_Compute()
 
+    sphere = None if args.no_sphere else run_sphere_pair(stream)
+
     # direct solve only (no refinement), for the phase breakdown
     g.solve_device(b_d.data_ptr(), x_d.data_ptr(), NRHS)
     t_direct_solve = g.get_recLU_SolveTime()
@@ -429,6 +431,7 @@ def run_ours(args, rank, world, local_rank):
                          "avg_launch_s": aca_s / max(aca_launch, 1.0),
                          "launches_per_step": aca_launch},
         "mixed": mixed,
+        "sphere_matern": sphere,
         "clocks": clocks,
         "gpu_launches": int(n_launch),
     }
@@ -446,6 +449,66 @@ def run_ours(args, rank, world, local_rank):
                        f"on the first {c['kmatvec_rows_timed']} rows, not 1e-10"),
             "measured": c,
         }
+    return out
+
+
+# The end-to-end target's shape (unit sphere, Matern-3/2 l = 0.1 + 1e-2 delta,
+# leaf 128, ACA tol 1e-10, one right-hand side) at the largest N whose FP64
+# factors fit one B200 (its top-level ranks grow like sqrt(N): 4117 here).
+SPHERE_N = 262144
+# The chosen mixed form on it: the preconditioner compressed at MIXED_TOL
+# (a factor in reduced precision needs no more) with MIXED_PREC tensor-core
+# Woodbury products; GMRES on the FP64 full-kernel residual to 1e-10.
+MIXED_TOL, MIXED_PREC = 1e-6, "tf32x3"
+
+
+def run_sphere_pair(stream, steps=2):
+    """FP64 (ACA tol 1e-10) against the mixed form on the sphere / Matern
+    shape, each timed over `steps` steps after one warm-up; a step is
+    compress + factor + GMRES until ||b - K x|| / ||b|| <= 1e-10."""
+    import torch
+    from dense_hodlr_b200 import HODLR_Matrix, KernelSpec
+    c = SCALE_CONFIGS["c5"]
+    pts = scale_points(c["cloud"], SPHERE_N)
+    b = np.random.default_rng(SEED + 1).standard_normal((SPHERE_N, c["nrhs"]))
+    b_d = torch.from_numpy(np.ascontiguousarray(b.T)).cuda()
+    x_d = torch.empty_like(b_d)
+    g = HODLR_Matrix(SPHERE_N, SPHERE_N, KernelSpec(c["kernel"], c["l"], c["shift"]), pts,
+                     c["leaf"])
+    out = {"workload": (f"N={SPHERE_N} uniform on the unit sphere, k-d ordered, Matern-3/2 "
+                        f"l=0.1 +1e-2*delta, leaf 128, 1 RHS N(0,1), to rel residual 1e-10"),
+           "steps": steps}
+    for name, tol, prec in (("fp64", c["tol"], "fp64"), ("mixed", MIXED_TOL, MIXED_PREC)):
+        g.set_LRTolerance(tol)
+        g.set_precision(prec)
+        rec = {"aca_tol": tol, "precision": prec}
+        for it in range(steps + 1):
+            g.reset()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            g.storeLRinTree()
+            g.recLU_Compute()
+            n_it, rel = g.iterative_solve_device(b_d.data_ptr(), x_d.data_ptr(), c["nrhs"],
+                                                 tol=RES_TOL, max_iter=MAX_IR, restart=40)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            if it == 0:
+                continue
+            rec.setdefault("ms", []).append(e0.elapsed_time(e1))
+            rec.update({"lr_s": g.get_LR_ComputationTime(),
+                        "factor_s": g.get_recLU_FactorizationTime(),
+                        "gmres_s": g.get_recLU_SolveTime(), "gmres_iterations": int(n_it),
+                        "rel_residual": float(rel.max()), "max_rank": int(g.ranks().max())})
+        rec["ms_per_step"] = float(np.mean(rec.pop("ms")))
+        rec["x"] = x_d.cpu().numpy().T.copy()
+        out[name] = rec
+    xf, xm = out["fp64"].pop("x"), out["mixed"].pop("x")
+    out["mixed"]["solution_rel_diff_vs_fp64"] = float(np.linalg.norm(xm - xf) /
+                                                      np.linalg.norm(xf))
+    out["mixed_speedup_vs_fp64"] = out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"]
+    del g
     return out
 
 
@@ -842,6 +905,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision leg")
+    ap.add_argument("--no-sphere", action="store_true",
+                    help="skip the sphere / Matern tol 1e-10 FP64-vs-mixed pair")
     args = ap.parse_args()
     if args.case:
         run_profile_case(args.case)

@@ -165,6 +165,11 @@ class HODLR_Matrix:
         _check(self._h, _L.lib().hodlr_set_capacity_hint(
             self._h, a.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), len(a)))
 
+    def reset(self):
+        """Drop the compression and factorization (reset_attributes,
+        src/HODLR_Matrix.cpp:1232-1246): the next solve recomputes both."""
+        _check(self._h, _L.lib().hodlr_reset(self._h))
+
     def set_aca_streaming(self, on):
         """Top-level ACA panels through the bulk-copy ring (1, default) or per-thread loads (0)."""
         _check(self._h, _L.lib().hodlr_set_aca_streaming(self._h, int(bool(on))))
