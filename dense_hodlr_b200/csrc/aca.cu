@@ -413,20 +413,37 @@ __device__ void residual_pass_ring(const AcaLaunch& L, const AcaBlock& B, double
 #pragma unroll
         for (int e = 0; e < E; ++e) s[e] = __dadd_rn(s[e], __dmul_rn(cf, v[u][e]));
       }
-      if (dots) {
+      if (dots && l0 < kd) {
+        // the tile's four column dots over the warp in one transposed
+        // reduction: after the exchanges at offsets 16 and 8, lane group
+        // q = lane / 8 holds partial sums of column q, then each group of 8
+        // lanes sums its own (6 shuffles instead of 4 x 5)
+        static_assert(TMA_BC == 4, "transposed reduction of four columns");
+        double d[TMA_BC];
 #pragma unroll
         for (int u = 0; u < TMA_BC; ++u) {
-          if (l0 + u >= kd) break;
-          double d = 0.0;
+          d[u] = 0.0;
 #pragma unroll
-          for (int e = 0; e < E; ++e) d = fma(v[u][e], vp[e], d);
-          d = warp_sum(d);
-          if (lane == 0) {
-            if (c == 0)
-              dotw[w * ldd + l0 + u] = d;
-            else
-              dotw[w * ldd + l0 + u] += d;
-          }
+          for (int e = 0; e < E; ++e) d[u] = fma(v[u][e], vp[e], d[u]);
+        }
+        const bool hi16 = (lane & 16) != 0, hi8 = (lane & 8) != 0;
+        // offset 16: lanes < 16 keep columns 0, 1; lanes >= 16 keep 2, 3
+        const double s0 = __shfl_xor_sync(0xffffffffu, hi16 ? d[0] : d[2], 16);
+        const double s1 = __shfl_xor_sync(0xffffffffu, hi16 ? d[1] : d[3], 16);
+        const double p0 = (hi16 ? d[2] : d[0]) + s0;
+        const double p1 = (hi16 ? d[3] : d[1]) + s1;
+        // offset 8: lanes with bit 3 clear keep the first of the pair
+        const double s2 = __shfl_xor_sync(0xffffffffu, hi8 ? p0 : p1, 8);
+        double t = (hi8 ? p1 : p0) + s2;
+        t += __shfl_xor_sync(0xffffffffu, t, 4);
+        t += __shfl_xor_sync(0xffffffffu, t, 2);
+        t += __shfl_xor_sync(0xffffffffu, t, 1);
+        const int u = (hi16 ? 2 : 0) + (hi8 ? 1 : 0);  // the column this lane group summed
+        if ((lane & 7) == 0 && l0 + u < kd) {
+          if (c == 0)
+            dotw[w * ldd + l0 + u] = t;
+          else
+            dotw[w * ldd + l0 + u] += t;
         }
       }
       __syncwarp();
