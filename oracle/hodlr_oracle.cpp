@@ -222,9 +222,46 @@ struct Oracle {
   bool compressed = false, factored = false;
   int status = 0;
 
+  // entries: 0 = the closed forms of kfun.h (the product's own formulas, bit
+  // for bit); 1 = this file's restatement of them as a user functor of the
+  // reference would write it, with libm's exp and sqrt (libm_entry)
+  int entry_mode = 0;
+  double lscale = 1.0;
+
   double entry(int i, int j) const {
     if (dense) return A[(size_t)j * n + i];
+    if (entry_mode == 1) return libm_entry(i, j);
     return hx_entry(kp, pts.data(), n, i, j);
+  }
+
+  // K(i, j) the way the reference's kernel functors compute it
+  // (test/test.cpp:13-18: a distance, then the formula with std::exp): the
+  // squared distance summed over dimensions, r / l and r^2 / l^2 by division,
+  // libm for exp and sqrt.  It shares no code with the product, whose
+  // entries differ from these in the last bits only.
+  double libm_entry(int i, int j) const {
+    if (i == j && kp.diag_replace) return kp.diag_value;
+    double r2 = 0.0;
+    for (int d = 0; d < dim; ++d) {
+      const double t = pts[(size_t)d * n + i] - pts[(size_t)d * n + j];
+      r2 = r2 + t * t;
+    }
+    const double l = lscale;
+    double v = 0.0;
+    switch (kp.type) {
+      case 0: v = std::exp(-r2 / (l * l)); break;
+      case 1: {
+        const double s = std::sqrt(3.0) * std::sqrt(r2) / l;
+        v = (1.0 + s) * std::exp(-s);
+        break;
+      }
+      case 2: v = 1.0 / std::sqrt(1.0 + r2 / (l * l)); break;
+      case 3: v = 1.0 + r2 / (l * l); break;
+      case 4: v = std::exp(-std::sqrt(r2) / l); break;
+      default: v = 0.0;
+    }
+    if (i == j) v = v + kp.shift;
+    return v;
   }
 };
 
@@ -908,8 +945,17 @@ void* orc_create_kernel(int n, int dim, const double* pts, int ktype, double lsc
   o->dense = false;
   o->pts.assign(pts, pts + (size_t)n * dim);
   o->kp = hx_make_kparams(ktype, dim, lscale, shift, diag_replace, diag_value);
+  o->lscale = lscale;
   build_tree(*o);
   return o;
+}
+
+// Entry formulas of a kernel oracle (Oracle::entry_mode); drops any
+// compression and factorization.
+void orc_set_entry_mode(void* h, int mode) {
+  Oracle* o = (Oracle*)h;
+  o->entry_mode = mode;
+  o->compressed = o->factored = false;
 }
 
 void* orc_create_dense(int n, const double* A, int lda, int leaf) {

@@ -37,6 +37,7 @@ def lib():
         L.orc_create_dense.restype = ctypes.c_void_p
         L.orc_create_dense.argtypes = [ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int]
         L.orc_destroy.argtypes = [ctypes.c_void_p]
+        L.orc_set_entry_mode.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.orc_set_user_tree.argtypes = [ctypes.c_void_p, ctypes.c_int, _ip, _ip, _ip]
         L.orc_set_user_tree.restype = ctypes.c_int
         L.orc_set_user_tree_bounds.argtypes = [ctypes.c_void_p, ctypes.c_int] + [_ip] * 7
@@ -96,12 +97,17 @@ class OracleHODLR:
 
     @classmethod
     def from_kernel(cls, pts, ktype, length_scale, shift=0.0, leaf=30,
-                    diag_replace=False, diag_value=0.0):
+                    diag_replace=False, diag_value=0.0, libm=False):
+        """libm=True: entries from the oracle's own formulas with libm's exp and
+        sqrt, as the reference's kernel functors compute them, instead of the
+        closed forms the product shares (last-bit differences)."""
         pts = np.ascontiguousarray(np.atleast_2d(pts), dtype=np.float64)  # (dim, n)
         dim, n = pts.shape
         h = lib().orc_create_kernel(n, dim, _ptr(pts), int(ktype), float(length_scale),
                                     float(shift), int(bool(diag_replace)),
                                     float(diag_value), int(leaf))
+        if libm:
+            lib().orc_set_entry_mode(h, 1)
         return cls(h, n, pts)
 
     @classmethod

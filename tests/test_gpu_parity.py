@@ -400,3 +400,30 @@ def test_log_determinant_matches_dense(kind, l, shift):
     assert abs(g.logAbsDeterminant() - ld) <= 1e-9 * abs(ld)
     s2, ld2 = g.slogdet()  # determinant() itself under/overflows at this size
     assert s2 == sgn and ld2 == g.logAbsDeterminant()
+
+
+def test_against_the_oracles_own_libm_entries(oracle_mod):
+    """Against an oracle that evaluates the entries with its own code and libm
+    (as the reference's kernel functors do), sharing no formula with the GPU.
+    The reference's own kernel functor (quadraticKernel, test/test.cpp:12-17,
+    r*r + 1 with a zero diagonal) is exact arithmetic: pivots, ranks and W/V
+    bit for bit.  The C1 Gaussian goes through exp, where last-bit entry
+    differences may move late pivots of a few blocks: there both solutions
+    are held to the dense FP64 LU at the same bar."""
+    rng = np.random.default_rng(11)
+    x = rng.uniform(-1.0, 1.0, 4000)[None, :]
+    g = HODLR_Matrix(4000, 4000, KernelSpec("quadratic", 1.0, 0.0, True, 0.0), x, 30)
+    g.set_LRTolerance(1e-8)
+    o = oracle_mod.OracleHODLR.from_kernel(x, 3, 1.0, leaf=30, diag_replace=True, libm=True)
+    o.set_lr(1e-8)
+    _compare_compression(g, o)
+    pts, rng2 = c1_points()
+    g = HODLR_Matrix(4096, 4096, KernelSpec("gaussian", 0.1, 1.0), pts, 64)
+    g.set_LRTolerance(1e-10)
+    o = oracle_mod.OracleHODLR.from_kernel(pts, 0, 0.1, shift=1.0, leaf=64, libm=True)
+    o.set_lr(1e-10)
+    b = rng2.standard_normal((4096, 1))
+    K = np.exp(-((pts[0][:, None] - pts[0][None, :]) ** 2) / 0.01) + np.eye(4096)
+    xd = np.linalg.solve(K, b)
+    for xs in (g.recLU_Solve(b), o.solve(b)):
+        assert np.linalg.norm(xs - xd) / np.linalg.norm(xd) < 1e-9

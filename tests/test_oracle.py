@@ -329,3 +329,40 @@ def test_golden_c1_pivots_and_ranks(oracle_mod):
     inner = o.inner_nodes()
     wv = [factor_hash(*o.lowrank(b, *block_shape(inner, b))) for b in range(o.num_blocks())]
     assert np.array_equal(np.array(wv, dtype=np.int64), g["wv_hash"])
+
+
+def test_entry_formula_independence(oracle_mod):
+    """The oracle's own libm entries (libm=True, written as the reference's
+    functors are, no code shared with the product) against the closed forms
+    the product and oracle share.  The reference's own kernel functor
+    (quadraticKernel, test/test.cpp:12-17: r*r + 1, diagonal 0) has exact
+    arithmetic, so both give the same bits and the same pivots, ranks and
+    factors.  Kernels through exp differ in the last bits (libm's exp is not
+    the closed form's), which is enough to move late ACA pivots: near
+    convergence a residual is about tol times the entries."""
+    rng = np.random.default_rng(3)
+    x = rng.uniform(-1.0, 1.0, 2000)[None, :]
+    a = oracle_mod.OracleHODLR.from_kernel(x, 3, 1.0, leaf=30, diag_replace=True)
+    b = oracle_mod.OracleHODLR.from_kernel(x, 3, 1.0, leaf=30, diag_replace=True, libm=True)
+    for o in (a, b):
+        o.set_lr(1e-8)
+        o.compress(4)
+    for i, j in rng.integers(0, 2000, (500, 2)):
+        assert a.entry(int(i), int(j)) == b.entry(int(i), int(j))
+    assert np.array_equal(a.ranks(), b.ranks())
+    inner = a.inner_nodes()
+    for k in range(a.num_blocks()):
+        pa, pb = a.pivots(k), b.pivots(k)
+        assert np.array_equal(pa[0], pb[0]) and np.array_equal(pa[1], pb[1])
+        lvl, mn, sp, mx = inner[k // 2]
+        m, n = (sp - mn + 1, mx - sp) if k % 2 == 0 else (mx - sp, sp - mn + 1)
+        Wa, Va = a.lowrank(k, m, n)
+        Wb, Vb = b.lowrank(k, m, n)
+        assert np.array_equal(Wa, Wb) and np.array_equal(Va, Vb)
+    # exp kernels: the same matrix to rounding
+    pts = np.sort(rng.uniform(-1.0, 1.0, 1000))[None, :]
+    g1 = oracle_mod.OracleHODLR.from_kernel(pts, 0, 0.1, shift=1.0, leaf=64)
+    g2 = oracle_mod.OracleHODLR.from_kernel(pts, 0, 0.1, shift=1.0, leaf=64, libm=True)
+    rel = max(abs(g1.entry(int(i), int(j)) - g2.entry(int(i), int(j))) /
+              abs(g2.entry(int(i), int(j))) for i, j in rng.integers(0, 1000, (2000, 2)))
+    assert rel < 1e-13
