@@ -317,7 +317,13 @@ def run_ours(args, rank, world, local_rank):
         g.set_precision("fp64")
         g.recLU_Compute()
 
-    sphere = None if args.no_sphere else run_sphere_pair(stream)
+    sphere = None
+    if not args.no_sphere:
+        try:
+            sphere = run_sphere_pair(stream)
+        except Exception as e:  # reported in the line; the headline workload stands alone
+            sphere = {"error": f"{type(e).__name__}: {e}"}
+        torch.cuda.synchronize()
 
     # direct solve only (no refinement), for the phase breakdown
     g.solve_device(b_d.data_ptr(), x_d.data_ptr(), NRHS)
