@@ -36,6 +36,14 @@
 
 namespace {
 
+// The block's W or V panel in the launch's element type.
+template <typename T>
+__device__ __forceinline__ T* panel_of(double* d, float* f);
+template <>
+__device__ __forceinline__ double* panel_of<double>(double* d, float*) { return d; }
+template <>
+__device__ __forceinline__ float* panel_of<float>(double*, float* f) { return f; }
+
 struct Shared {
   double red_v[32];
   int red_i[32];
@@ -182,8 +190,8 @@ __device__ void reduce_partials(Shared& sh, const double* part, int64_t stride, 
 // computed while the panel streams through for step k).  Returns the slice
 // argmax of |r| (first maximum), the first admissible candidate (unchosen,
 // |r| > minPiv) and the partial sum of squares of the stored column.
-template <int NT, int E, bool ROW>
-__device__ void residual_pass(const AcaLaunch& L, const AcaBlock& B, double* P, int lo, int hi,
+template <int NT, int E, bool ROW, typename T>
+__device__ void residual_pass(const AcaLaunch& L, const AcaBlock& B, T* P, int lo, int hi,
                               int k, const double* __restrict__ coef, bool dots,
                               double* __restrict__ dotw, int ldd, int fixed, const double* xfix,
                               double scale, const unsigned char* chosen, double& bv, int& bi,
@@ -192,7 +200,7 @@ __device__ void residual_pass(const AcaLaunch& L, const AcaBlock& B, double* P, 
   const int64_t ld = L.ld;
   const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
   const double minPiv = L.minPivot;
-  const double* __restrict__ Pr = P;  // columns < k are only read here
+  const T* __restrict__ Pr = P;  // columns < k are only read here
   const int kd = dots ? k - 1 : 0;
   bool first = true;
   for (int jb = lo; jb < hi; jb += E * NT, first = false) {
@@ -205,7 +213,7 @@ __device__ void residual_pass(const AcaLaunch& L, const AcaBlock& B, double* P, 
       ok[e] = jj[e] < hi;
       if (!ok[e]) jj[e] = lo;  // safe address; its products use vp = 0
       s[e] = 0.0;
-      vp[e] = (dots && ok[e]) ? Pr[jj[e] + (int64_t)(k - 1) * ld] : 0.0;
+      vp[e] = (dots && ok[e]) ? (double)Pr[jj[e] + (int64_t)(k - 1) * ld] : 0.0;
     }
     int l = 0;
     for (; l + U <= k; l += U) {
@@ -213,7 +221,7 @@ __device__ void residual_pass(const AcaLaunch& L, const AcaBlock& B, double* P, 
 #pragma unroll
       for (int u = 0; u < U; ++u)
 #pragma unroll
-        for (int e = 0; e < E; ++e) v[u][e] = Pr[jj[e] + (int64_t)(l + u) * ld];
+        for (int e = 0; e < E; ++e) v[u][e] = (double)Pr[jj[e] + (int64_t)(l + u) * ld];
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         const double c = coef[l + u];
@@ -242,7 +250,7 @@ __device__ void residual_pass(const AcaLaunch& L, const AcaBlock& B, double* P, 
       double d = 0.0;
 #pragma unroll
       for (int e = 0; e < E; ++e) {
-        const double v = Pr[jj[e] + (int64_t)l * ld];
+        const double v = (double)Pr[jj[e] + (int64_t)l * ld];
         s[e] = __dadd_rn(s[e], __dmul_rn(c, v));
         d = fma(v, vp[e], d);
       }
@@ -263,8 +271,11 @@ __device__ void residual_pass(const AcaLaunch& L, const AcaBlock& B, double* P, 
       double ent = ROW ? src_entry_xi(S, xfix, fixed, B.c0 + j)
                        : src_entry_xj(S, xfix, B.r0 + j, fixed);
       double r = __dsub_rn(ent, s[e]);
-      double stored = ROW ? r : __dmul_rn(scale, r);
-      P[j + (int64_t)k * ld] = stored;
+      // the panel keeps the value rounded to its type (no rounding for FP64),
+      // and the norms of the stopping test use what it keeps
+      const T kept = (T)(ROW ? r : __dmul_rn(scale, r));
+      const double stored = (double)kept;
+      P[j + (int64_t)k * ld] = kept;
       sq = fma(stored, stored, sq);
       double a = fabs(r);
       nonfinite |= !isfinite(r);
@@ -287,10 +298,11 @@ __device__ void residual_pass(const AcaLaunch& L, const AcaBlock& B, double* P, 
 constexpr int TMA_BC = 4;
 constexpr int TMA_S = 4;
 constexpr int TMA_NT = 256, TMA_E = 4, TMA_BR = TMA_NT * TMA_E;
-constexpr size_t TMA_RING_BYTES = sizeof(double) * TMA_S * TMA_BC * TMA_BR;  // 128 KB
+// ring bytes for panel elements of `es` bytes (128 KB for FP64, 64 KB for FP32)
+constexpr size_t tma_ring_bytes(size_t es) { return es * TMA_S * TMA_BC * TMA_BR; }
 
 struct Ring {
-  double* buf;      // TMA_S tiles of TMA_BC x TMA_BR doubles, column u at u * TMA_BR
+  void* buf;        // TMA_S tiles of TMA_BC x TMA_BR panel elements, column u at u * TMA_BR
   uint64_t* full;   // per tile: its copies landed (1 arrival + transaction bytes)
   uint64_t* empty;  // per tile: every warp is done with it (NT / 32 arrivals)
   uint32_t t;       // tiles this CTA has consumed (the same in every thread)
@@ -327,17 +339,18 @@ __device__ void mbar_wait_bounded(uint64_t* bar, uint32_t parity, unsigned* err)
 }
 
 // Thread 0: tile gt of the ring, `nc` columns from column l0 of P, `count`
-// rows from row0 (count even, row0 on an even global row).
-__device__ void ring_issue(Ring& R, uint32_t gt, const double* P, int64_t ld, int row0, int count,
+// rows from row0 (count and row0's global index multiples of 16 / sizeof(T)).
+template <typename T>
+__device__ void ring_issue(Ring& R, uint32_t gt, const T* P, int64_t ld, int row0, int count,
                            int l0, int nc, unsigned* err) {
   const int slot = (int)(gt % TMA_S);
   if (gt >= (uint32_t)TMA_S) mbar_wait_bounded(&R.empty[slot], ((gt / TMA_S) + 1) & 1, err);
-  const uint32_t bytes = (uint32_t)count * (uint32_t)sizeof(double);
+  const uint32_t bytes = (uint32_t)count * (uint32_t)sizeof(T);
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
                    smem_addr(&R.full[slot])),
                "r"(bytes * (uint32_t)nc)
                : "memory");
-  double* dst = R.buf + (size_t)slot * TMA_BC * TMA_BR;
+  T* dst = static_cast<T*>(R.buf) + (size_t)slot * TMA_BC * TMA_BR;
   for (int u = 0; u < nc; ++u)
     asm volatile(
         "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
@@ -352,8 +365,8 @@ __device__ void ring_issue(Ring& R, uint32_t gt, const double* P, int64_t ld, in
 // sums in l order with separately rounded products and sums, the argmax in
 // increasing index per thread; the fused dots add their chunk partials in a
 // GPU order, as there.
-template <int NT, int E, bool ROW>
-__device__ void residual_pass_ring(const AcaLaunch& L, const AcaBlock& B, double* P, int lo,
+template <int NT, int E, bool ROW, typename T>
+__device__ void residual_pass_ring(const AcaLaunch& L, const AcaBlock& B, T* P, int lo,
                                    int hi, int k, const double* __restrict__ coef, bool dots,
                                    double* __restrict__ dotw, int ldd, int fixed,
                                    const double* xfix, double scale, const unsigned char* chosen,
@@ -364,22 +377,23 @@ __device__ void residual_pass_ring(const AcaLaunch& L, const AcaBlock& B, double
   const int64_t ld = L.ld;
   const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
   const double minPiv = L.minPivot;
-  const int x0 = lo - ((gbase + lo) & 1);  // first chunk row: even global index
+  constexpr int A = 16 / (int)sizeof(T);  // elements per 16 bytes: copy alignment
+  const int x0 = lo - ((gbase + lo) & (A - 1));  // first chunk row: aligned global index
   const int nchunks = (hi - x0 + TMA_BR - 1) / TMA_BR;
   const int tpc = (k + TMA_BC - 1) / TMA_BC;  // tiles per chunk
-  const uint32_t T = (uint32_t)nchunks * (uint32_t)tpc;
+  const uint32_t ntiles = (uint32_t)nchunks * (uint32_t)tpc;
   const int kd = dots ? k - 1 : 0;
   auto issue = [&](uint32_t i) {
     const int c = (int)(i / tpc), l0 = (int)(i % tpc) * TMA_BC;
     const int row0 = x0 + c * TMA_BR;
-    const int count = (min(TMA_BR, hi - row0) + 1) & ~1;
+    const int count = (min(TMA_BR, hi - row0) + A - 1) & ~(A - 1);
     ring_issue(R, R.t + i, P, ld, row0, count, l0, min(TMA_BC, k - l0), L.err);
   };
-  if (tid == 0 && T > 0) {
+  if (tid == 0 && ntiles > 0) {
     // this CTA's earlier generic stores to the panel (after the caller's
     // __syncthreads) before the bulk copies read it
     asm volatile("fence.proxy.async.global;" ::: "memory");
-    for (uint32_t i = 0; i < T && i < (uint32_t)TMA_S; ++i) issue(i);
+    for (uint32_t i = 0; i < ntiles && i < (uint32_t)TMA_S; ++i) issue(i);
   }
   uint32_t i = 0;
   for (int c = 0; c < nchunks; ++c) {
@@ -392,20 +406,20 @@ __device__ void residual_pass_ring(const AcaLaunch& L, const AcaBlock& B, double
       jj[e] = jb + tid + e * NT;
       ok[e] = jj[e] >= lo && jj[e] < hi;
       s[e] = 0.0;
-      vp[e] = (dots && ok[e]) ? P[jj[e] + (int64_t)(k - 1) * ld] : 0.0;
+      vp[e] = (dots && ok[e]) ? (double)P[jj[e] + (int64_t)(k - 1) * ld] : 0.0;
     }
     for (int l0 = 0; l0 < k; l0 += TMA_BC, ++i) {
       const uint32_t gt = R.t + i;
       const int slot = (int)(gt % TMA_S);
       mbar_wait_bounded(&R.full[slot], (gt / TMA_S) & 1, L.err);
-      const double* tile = R.buf + (size_t)slot * TMA_BC * TMA_BR;
+      const T* tile = static_cast<const T*>(R.buf) + (size_t)slot * TMA_BC * TMA_BR;
       const int nc = min(TMA_BC, k - l0);
       double v[TMA_BC][E];
 #pragma unroll
       for (int u = 0; u < TMA_BC; ++u)
 #pragma unroll
         for (int e = 0; e < E; ++e)
-          v[u][e] = (u < nc && ok[e]) ? tile[u * TMA_BR + tid + e * NT] : 0.0;
+          v[u][e] = (u < nc && ok[e]) ? (double)tile[u * TMA_BR + tid + e * NT] : 0.0;
 #pragma unroll
       for (int u = 0; u < TMA_BC; ++u) {
         if (u >= nc) break;
@@ -450,7 +464,7 @@ __device__ void residual_pass_ring(const AcaLaunch& L, const AcaBlock& B, double
       if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(
                                       smem_addr(&R.empty[slot]))
                                   : "memory");
-      if (tid == 0 && i + TMA_S < T) issue(i + TMA_S);
+      if (tid == 0 && i + TMA_S < ntiles) issue(i + TMA_S);
     }
 #pragma unroll
     for (int e = 0; e < E; ++e) {
@@ -459,8 +473,11 @@ __device__ void residual_pass_ring(const AcaLaunch& L, const AcaBlock& B, double
       double ent = ROW ? src_entry_xi(S, xfix, fixed, B.c0 + j)
                        : src_entry_xj(S, xfix, B.r0 + j, fixed);
       double r = __dsub_rn(ent, s[e]);
-      double stored = ROW ? r : __dmul_rn(scale, r);
-      P[j + (int64_t)k * ld] = stored;
+      // the panel keeps the value rounded to its type (no rounding for FP64),
+      // and the norms of the stopping test use what it keeps
+      const T kept = (T)(ROW ? r : __dmul_rn(scale, r));
+      const double stored = (double)kept;
+      P[j + (int64_t)k * ld] = kept;
       sq = fma(stored, stored, sq);
       double a = fabs(r);
       nonfinite |= !isfinite(r);
@@ -471,29 +488,29 @@ __device__ void residual_pass_ring(const AcaLaunch& L, const AcaBlock& B, double
       if (cand == INT_MAX && a > minPiv && __ldcg(chosen + j) == 0) cand = j;
     }
   }
-  R.t += T;
+  R.t += ntiles;
 }
 
 // Partial dots of step k-1 over this CTA's slices when they could not be
 // fused into a residual pass (a zero residual row, or the capacity limit).
-template <int NT>
-__device__ void dots_only_pass(const AcaLaunch& L, const AcaBlock& B, int k, int i_lo, int i_hi,
-                               int j_lo, int j_hi, double* bank) {
+template <int NT, typename T>
+__device__ void dots_only_pass(const AcaLaunch& L, const T* BW, const T* BV, int k, int i_lo,
+                               int i_hi, int j_lo, int j_hi, int kcap, double* bank) {
   const int64_t ld = L.ld;
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const double* wk = B.W + (int64_t)(k - 1) * ld;
-  const double* vk = B.V + (int64_t)(k - 1) * ld;
+  const T* wk = BW + (int64_t)(k - 1) * ld;
+  const T* vk = BV + (int64_t)(k - 1) * ld;
   for (int l = w; l < k - 1; l += NT / 32) {
-    const double* wl = B.W + (int64_t)l * ld;
-    const double* vl = B.V + (int64_t)l * ld;
+    const T* wl = BW + (int64_t)l * ld;
+    const T* vl = BV + (int64_t)l * ld;
     double aw = 0.0, av = 0.0;
-    for (int i = i_lo + lane; i < i_hi; i += 32) aw = fma(wk[i], wl[i], aw);
-    for (int j = j_lo + lane; j < j_hi; j += 32) av = fma(vl[j], vk[j], av);
+    for (int i = i_lo + lane; i < i_hi; i += 32) aw = fma((double)wk[i], (double)wl[i], aw);
+    for (int j = j_lo + lane; j < j_hi; j += 32) av = fma((double)vl[j], (double)vk[j], av);
     aw = warp_sum(aw);
     av = warp_sum(av);
     if (lane == 0) {
       bank[l] = av;
-      bank[B.kcap + l] = aw;
+      bank[kcap + l] = aw;
     }
   }
 }
@@ -522,12 +539,15 @@ __device__ double resolve_eps(Shared& sh, const AcaLaunch& L, const AcaBlock& B,
 // RING: the residual passes stream their panel slices through the bulk-copy
 // ring (group levels of an even N); the dynamic shared memory then starts
 // with the ring's TMA_RING_BYTES.
-template <int NT, int E, bool RING>
+// T: the element type of the W/V panels (double; float for the mixed form's
+// compression, whose values are rounded to FP32 when stored and read back
+// into FP64 arithmetic).
+template <int NT, int E, bool RING, typename T>
 __global__ void __launch_bounds__(NT, (RING ? 1 : (NT == 256 ? 2 : 4))) aca_kernel(AcaLaunch L) {
   extern __shared__ __align__(128) double dyn_all[];
   __shared__ Shared sh;
   __shared__ __align__(8) uint64_t ring_full[TMA_S], ring_empty[TMA_S];
-  double* dyn = RING ? dyn_all + TMA_RING_BYTES / sizeof(double) : dyn_all;
+  double* dyn = RING ? dyn_all + tma_ring_bytes(sizeof(T)) / sizeof(double) : dyn_all;
   // dyn: row[kcap], then (unless L.dotg) per-warp dots[NT/32][kcap]
   constexpr int NW = NT / 32;
   const int b = L.cta_block ? (blockIdx.x < (unsigned)L.ncta ? L.cta_block[blockIdx.x] : L.nblocks)
@@ -535,6 +555,8 @@ __global__ void __launch_bounds__(NT, (RING ? 1 : (NT == 256 ? 2 : 4))) aca_kern
   const int tid = threadIdx.x;
   if (b >= L.nblocks) return;
   const AcaBlock B = L.blocks[b];
+  T* const BW = panel_of<T>(B.W, B.Wf);
+  T* const BV = panel_of<T>(B.V, B.Vf);
   const int G = L.cta_block ? B.G : L.G;
   const int g = L.cta_block ? (int)blockIdx.x - B.g0 : (int)(blockIdx.x % L.G);
   const int64_t grp0 = L.cta_block ? B.g0 : (int64_t)b * G;
@@ -594,7 +616,7 @@ __global__ void __launch_bounds__(NT, (RING ? 1 : (NT == 256 ? 2 : 4))) aca_kern
     if (k >= B.kcap) {
       if (pending) {
         const int bk0 = 8 + (k & 1) * (2 * B.kcap + 2);
-        dots_only_pass<NT>(L, B, k, i_lo, i_hi, j_lo, j_hi, part_me + bk0);
+        dots_only_pass<NT>(L, BW, BV, k, i_lo, i_hi, j_lo, j_hi, B.kcap, part_me + bk0);
         if (!group_sync(L, bar, G, gen, L.err)) { status = ACA_ERROR; break; }
         eps = resolve_eps<NT>(sh, L, B, part_grp, G, bk0, k, swp, svp, frob2);
         pending = 0;
@@ -613,7 +635,7 @@ __global__ void __launch_bounds__(NT, (RING ? 1 : (NT == 256 ? 2 : 4))) aca_kern
     const int bk = 8 + (k & 1) * (2 * B.kcap + 2);
     // ---------------- phase A: residual row on this CTA's column slice
     if (g == 0 && tid == 0) B.cR[cur] = 1;
-    for (int l = tid; l < k; l += NT) row[l] = __ldcg(B.W + cur + (int64_t)l * ld);
+    for (int l = tid; l < k; l += NT) row[l] = (double)__ldcg(BW + cur + (int64_t)l * ld);
     if (fuse && j_lo >= j_hi)  // an empty slice contributes zero dots
       for (int e = tid; e < NW * (k - 1); e += NT) dotw[(e / (k - 1)) * ldd + e % (k - 1)] = 0.0;
     __syncthreads();
@@ -627,10 +649,10 @@ __global__ void __launch_bounds__(NT, (RING ? 1 : (NT == 256 ? 2 : 4))) aca_kern
     double bv = -1.0, sv = 0.0;
     int bi = INT_MAX, cand = INT_MAX;
     if constexpr (RING)
-      residual_pass_ring<NT, E, true>(L, B, B.V, j_lo, j_hi, k, row, fuse, dotw, ldd, gi, xi, 1.0,
+      residual_pass_ring<NT, E, true>(L, B, BV, j_lo, j_hi, k, row, fuse, dotw, ldd, gi, xi, 1.0,
                                       B.cC, bv, bi, cand, sv, nonfinite, S, ring, B.c0);
     else
-      residual_pass<NT, E, true>(L, B, B.V, j_lo, j_hi, k, row, fuse, dotw, ldd, gi, xi, 1.0,
+      residual_pass<NT, E, true>(L, B, BV, j_lo, j_hi, k, row, fuse, dotw, ldd, gi, xi, 1.0,
                                  B.cC, bv, bi, cand, sv, nonfinite, S);
     __syncthreads();
     if (fuse)  // CTA partial dots of V, warps summed in order
@@ -659,7 +681,7 @@ __global__ void __launch_bounds__(NT, (RING ? 1 : (NT == 256 ? 2 : 4))) aca_kern
       // zero residual row (src/lowRank.cpp:187-195).  Whether the reference
       // even reached this step depends on epsilon_{k-1}: settle it first.
       if (pending) {
-        dots_only_pass<NT>(L, B, k, i_lo, i_hi, j_lo, j_hi, part_me + bk);
+        dots_only_pass<NT>(L, BW, BV, k, i_lo, i_hi, j_lo, j_hi, B.kcap, part_me + bk);
         if (!group_sync(L, bar, G, gen, L.err)) { status = ACA_ERROR; break; }
         eps = resolve_eps<NT>(sh, L, B, part_grp, G, bk, k, swp, svp, frob2);
         pending = 0;
@@ -688,8 +710,8 @@ __global__ void __launch_bounds__(NT, (RING ? 1 : (NT == 256 ? 2 : 4))) aca_kern
       cc = mcand;
     }
     if (g == 0 && tid == 0) B.cC[cc] = 1;
-    const double piv = __ddiv_rn(1.0, __ldcg(B.V + cc + (int64_t)k * ld));
-    for (int l = tid; l < k; l += NT) row[l] = __ldcg(B.V + cc + (int64_t)l * ld);
+    const double piv = __ddiv_rn(1.0, (double)__ldcg(BV + cc + (int64_t)k * ld));
+    for (int l = tid; l < k; l += NT) row[l] = (double)__ldcg(BV + cc + (int64_t)l * ld);
     if (fuse && i_lo >= i_hi)
       for (int e = tid; e < NW * (k - 1); e += NT) dotw[(e / (k - 1)) * ldd + e % (k - 1)] = 0.0;
     __syncthreads();
@@ -705,10 +727,10 @@ __global__ void __launch_bounds__(NT, (RING ? 1 : (NT == 256 ? 2 : 4))) aca_kern
     cand = INT_MAX;
     double sw = 0.0;
     if constexpr (RING)
-      residual_pass_ring<NT, E, false>(L, B, B.W, i_lo, i_hi, k, row, fuse, dotw, ldd, gj, xj,
+      residual_pass_ring<NT, E, false>(L, B, BW, i_lo, i_hi, k, row, fuse, dotw, ldd, gj, xj,
                                        piv, B.cR, bv, bi, cand, sw, nonfinite, S, ring, B.r0);
     else
-      residual_pass<NT, E, false>(L, B, B.W, i_lo, i_hi, k, row, fuse, dotw, ldd, gj, xj, piv,
+      residual_pass<NT, E, false>(L, B, BW, i_lo, i_hi, k, row, fuse, dotw, ldd, gj, xj, piv,
                                   B.cR, bv, bi, cand, sw, nonfinite, S);
     __syncthreads();
     if (fuse)
@@ -779,8 +801,8 @@ __global__ void __launch_bounds__(NT, (RING ? 1 : (NT == 256 ? 2 : 4))) aca_kern
   int rank = k;
   if (status == ACA_POST) {
     if (k == 0) {
-      for (int i = i_lo + tid; i < i_hi; i += NT) B.W[i] = 0.0;
-      for (int j = j_lo + tid; j < j_hi; j += NT) B.V[j] = 0.0;
+      for (int i = i_lo + tid; i < i_hi; i += NT) BW[i] = (T)0;
+      for (int j = j_lo + tid; j < j_hi; j += NT) BV[j] = (T)0;
       rank = 1;
       status = ACA_DONE;
     } else if (k >= ub - 1) {
@@ -797,9 +819,9 @@ __global__ void __launch_bounds__(NT, (RING ? 1 : (NT == 256 ? 2 : 4))) aca_kern
               if (d < S.kp.dim) xc[d] = __ldg(S.pts + d * S.ld + B.c0 + l);
           }
           for (int i = i_lo + tid; i < i_hi; i += NT)
-            B.W[i + (int64_t)l * ld] = src_entry_xj(S, xc, B.r0 + i, B.c0 + l);
+            BW[i + (int64_t)l * ld] = (T)src_entry_xj(S, xc, B.r0 + i, B.c0 + l);
           for (int j = j_lo + tid; j < j_hi; j += NT)
-            B.V[j + (int64_t)l * ld] = (j == l) ? 1.0 : 0.0;
+            BV[j + (int64_t)l * ld] = (T)((j == l) ? 1.0 : 0.0);
         }
         rank = n;
         status = ACA_DONE;
@@ -812,9 +834,9 @@ __global__ void __launch_bounds__(NT, (RING ? 1 : (NT == 256 ? 2 : 4))) aca_kern
               if (d < S.kp.dim) xr[d] = __ldg(S.pts + d * S.ld + B.r0 + l);
           }
           for (int j = j_lo + tid; j < j_hi; j += NT)
-            B.V[j + (int64_t)l * ld] = src_entry_xi(S, xr, B.r0 + l, B.c0 + j);
+            BV[j + (int64_t)l * ld] = (T)src_entry_xi(S, xr, B.r0 + l, B.c0 + j);
           for (int i = i_lo + tid; i < i_hi; i += NT)
-            B.W[i + (int64_t)l * ld] = (i == l) ? 1.0 : 0.0;
+            BW[i + (int64_t)l * ld] = (T)((i == l) ? 1.0 : 0.0);
         }
         rank = m;
         status = ACA_DONE;
@@ -846,8 +868,8 @@ __global__ void __launch_bounds__(NT, (RING ? 1 : (NT == 256 ? 2 : 4))) aca_kern
 
 }  // namespace
 
-static size_t aca_smem(int nt, int kcap_max, bool global_dots, bool ring) {
-  return (ring ? TMA_RING_BYTES : 0) +
+static size_t aca_smem(int nt, int kcap_max, bool global_dots, bool ring, bool f32) {
+  return (ring ? tma_ring_bytes(f32 ? sizeof(float) : sizeof(double)) : 0) +
          sizeof(double) * (size_t)(global_dots ? 1 : 1 + nt / 32) * (size_t)kcap_max;
 }
 
@@ -855,18 +877,23 @@ static size_t aca_smem(int nt, int kcap_max, bool global_dots, bool ring) {
 // than 100 KB of shared memory per CTA (without the ring: beyond that fewer
 // than two 256-thread CTAs fit on an SM), or with the ring once the CTA's
 // shared memory would pass 220 KB.
-bool aca_dots_global(int nt, int kcap_max, bool ring) {
-  return ring ? aca_smem(nt, kcap_max, false, true) > 220 * 1024
-              : aca_smem(nt, kcap_max, false, false) > 100 * 1024;
+bool aca_dots_global(int nt, int kcap_max, bool ring, bool f32) {
+  return ring ? aca_smem(nt, kcap_max, false, true, f32) > 220 * 1024
+              : aca_smem(nt, kcap_max, false, false, f32) > 100 * 1024;
 }
 
-size_t aca_smem_bytes(int nt, int kcap_max, bool ring) {
-  return aca_smem(nt, kcap_max, aca_dots_global(nt, kcap_max, ring), ring);
+size_t aca_smem_bytes(int nt, int kcap_max, bool ring, bool f32) {
+  return aca_smem(nt, kcap_max, aca_dots_global(nt, kcap_max, ring, f32), ring, f32);
 }
 
-static void* aca_fn(int nt, bool ring) {
-  if (ring) return (void*)aca_kernel<TMA_NT, TMA_E, true>;
-  return nt == 256 ? (void*)aca_kernel<256, 4, false> : (void*)aca_kernel<128, 2, false>;
+template <typename T>
+static void* aca_fn_t(int nt, bool ring) {
+  if (ring) return (void*)aca_kernel<TMA_NT, TMA_E, true, T>;
+  return nt == 256 ? (void*)aca_kernel<256, 4, false, T> : (void*)aca_kernel<128, 2, false, T>;
+}
+
+static void* aca_fn(int nt, bool ring, bool f32) {
+  return f32 ? aca_fn_t<float>(nt, ring) : aca_fn_t<double>(nt, ring);
 }
 
 // Dynamic shared memory above 48 KB, and the largest shared-memory carveout:
@@ -882,12 +909,12 @@ static int set_smem(void* fn, size_t smem) {
 }
 
 int aca_launch(const AcaLaunch& L, int nt, int kcap_max, bool cooperative, cudaStream_t s) {
-  const bool ring = L.ring != 0;
-  if (ring && (nt != TMA_NT || (L.ld & 1))) return (int)cudaErrorInvalidValue;
-  const size_t smem = aca_smem(nt, kcap_max, L.dotg != nullptr, ring);
+  const bool ring = L.ring != 0, f32 = L.f32 != 0;
+  if (ring && (nt != TMA_NT || (L.ld % (f32 ? 4 : 2)))) return (int)cudaErrorInvalidValue;
+  const size_t smem = aca_smem(nt, kcap_max, L.dotg != nullptr, ring, f32);
   dim3 grid(L.cta_block ? L.ncta : L.nblocks * L.G), block(nt);
   void* args[] = {(void*)&L};
-  void* fn = aca_fn(nt, ring);
+  void* fn = aca_fn(nt, ring, f32);
   if (int e = set_smem(fn, smem)) return e;
   cudaError_t e = cooperative ? cudaLaunchCooperativeKernel(fn, grid, block, args, smem, s)
                               : cudaLaunchKernel(fn, grid, block, args, smem, s);
@@ -895,9 +922,9 @@ int aca_launch(const AcaLaunch& L, int nt, int kcap_max, bool cooperative, cudaS
   return e == cudaSuccess ? 0 : (int)e;
 }
 
-int aca_max_coresident(int nt, int kcap_max, bool ring, int* per_sm) {
-  const size_t smem = aca_smem_bytes(nt, kcap_max, ring);
-  void* fn = aca_fn(nt, ring);
+int aca_max_coresident(int nt, int kcap_max, bool ring, bool f32, int* per_sm) {
+  const size_t smem = aca_smem_bytes(nt, kcap_max, ring, f32);
+  void* fn = aca_fn(nt, ring, f32);
   *per_sm = 0;
   if (int e = set_smem(fn, smem)) return e;
   int nb = 0;

@@ -44,9 +44,9 @@
 #include "rank_mlp.h"
 
 int aca_launch(const AcaLaunch& L, int nt, int kcap_max, bool cooperative, cudaStream_t s);
-int aca_max_coresident(int nt, int kcap_max, bool ring, int* per_sm);
-bool aca_dots_global(int nt, int kcap_max, bool ring);
-size_t aca_smem_bytes(int nt, int kcap_max, bool ring);
+int aca_max_coresident(int nt, int kcap_max, bool ring, bool f32, int* per_sm);
+bool aca_dots_global(int nt, int kcap_max, bool ring, bool f32);
+size_t aca_smem_bytes(int nt, int kcap_max, bool ring, bool f32);
 
 namespace hodlr_impl {
 
@@ -68,6 +68,11 @@ struct Level {
   int kcap = 0;
   double* W = nullptr;
   double* V = nullptr;
+  // FP32 panels of the mixed form's compression (f32): W and V are then null
+  // until the compression ends and converts them to FP64
+  float* Wf = nullptr;
+  float* Vf = nullptr;
+  bool f32 = false;
   unsigned char* cR = nullptr;
   unsigned char* cC = nullptr;
   int* prow = nullptr;
@@ -221,6 +226,7 @@ struct hodlr_handle_s {
   std::vector<int> cap_hint;  // initial W/V columns per level (0 = default)
   int gemm_prec = HODLR_GEMM_FP64;  // arithmetic of the Woodbury products
   bool aca_ring = true;  // group-level ACA panels through the bulk-copy ring
+  bool aca_f32 = false;  // compress into FP32 panels (hodlr_set_panel_precision)
   unsigned spin_limit = 0;       // polls of an ACA group barrier (0: HODLR_SPIN_LIMIT)
   bool bar_unreachable = false;  // ACA group barriers wait for one arrival too many
   std::vector<int> leaf_min, leaf_size;
@@ -331,6 +337,7 @@ std::vector<int4> block_geoms(hodlr_t h);
 int block_features_dev(hodlr_t h, const std::vector<int4>& geom, double l, float* d_F);
 int predict_ranks(hodlr_t h);
 int do_compress(hodlr_t h);
+int convert_level_to_fp64(hodlr_t h, Level& L);
 int upload_plan(hodlr_t h, std::vector<GemmProblem>& probs, bool split, DevPlan& out);
 int level_rank(const Level& L, int q);
 int run_tn(hodlr_t h, const DevPlan& P);

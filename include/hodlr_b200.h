@@ -327,6 +327,16 @@ int hodlr_set_factor_in_place(hodlr_t h, int mode);
  * setting applies from the next compression. */
 int hodlr_set_aca_streaming(hodlr_t h, int on);
 
+/* Element type of the W/V panels while ACA compresses (no counterpart in the
+ * reference; part of the mixed-precision form): bits = 64 (default, the
+ * reference's arithmetic, bit for bit) or 32.  With 32 every new ACA column
+ * is rounded to FP32 when stored and read back into FP64 arithmetic, so the
+ * compression streams half the bytes; pivots then differ from the FP64
+ * path's and the tolerance should be 1e-6 or looser (the stored columns
+ * carry FP32 rounding, 6e-8 relative).  The compressed panels are widened
+ * to FP64 for the factorization.  A change discards the compression. */
+int hodlr_set_panel_precision(hodlr_t h, int bits);
+
 /* Bounded device waits (no counterpart in the reference).  The CTAs of one
  * ACA block group meet at a barrier in global memory; a barrier that is not
  * complete after `polls` polls (0: the default, 2^26) gives up, the launch
