@@ -463,9 +463,10 @@ def run_ours(args, rank, world, local_rank):
 # factors fit one B200 (its top-level ranks grow like sqrt(N): 4117 here).
 SPHERE_N = 262144
 # The chosen mixed form on it: the preconditioner compressed at MIXED_TOL
-# (a factor in reduced precision needs no more) with MIXED_PREC tensor-core
-# Woodbury products; GMRES on the FP64 full-kernel residual to 1e-10.
-MIXED_TOL, MIXED_PREC = 1e-6, "tf32x3"
+# (a factor in reduced precision needs no more) into FP32 panels, with
+# MIXED_PREC tensor-core Woodbury products; GMRES on the FP64 full-kernel
+# residual to 1e-10.
+MIXED_TOL, MIXED_PREC, MIXED_PANEL_BITS = 1e-6, "tf32x3", 32
 
 
 def run_sphere_pair(stream, steps=2):
@@ -484,10 +485,12 @@ def run_sphere_pair(stream, steps=2):
     out = {"workload": (f"N={SPHERE_N} uniform on the unit sphere, k-d ordered, Matern-3/2 "
                         f"l=0.1 +1e-2*delta, leaf 128, 1 RHS N(0,1), to rel residual 1e-10"),
            "steps": steps}
-    for name, tol, prec in (("fp64", c["tol"], "fp64"), ("mixed", MIXED_TOL, MIXED_PREC)):
+    for name, tol, prec, bits in (("fp64", c["tol"], "fp64", 64),
+                                  ("mixed", MIXED_TOL, MIXED_PREC, MIXED_PANEL_BITS)):
         g.set_LRTolerance(tol)
         g.set_precision(prec)
-        rec = {"aca_tol": tol, "precision": prec}
+        g.set_panel_precision(bits)
+        rec = {"aca_tol": tol, "precision": prec, "aca_panel_bits": bits}
         for it in range(steps + 1):
             g.reset()
             torch.cuda.synchronize()
@@ -625,11 +628,12 @@ def run_profile_case(case):
 
 
 def run_tune(case):
-    """Sweep of the preconditioner's compression tolerance and Woodbury
-    precision on one configuration, case 'tune:<c3|c5|c2>:N[:tols[:precs]]'
-    (tols and precs comma-separated): for each ACA tolerance one compression,
-    then per precision the factorization and GMRES on the FP64 full-kernel
-    residual to 1e-10.  One JSON line per (tolerance, precision), flushed."""
+    """Sweep of the preconditioner's compression tolerance, panel precision and
+    Woodbury precision on one configuration,
+    case 'tune:<c3|c5|c2>:N[:tols[:precs[:panel bits]]]' (comma-separated
+    lists; panel bits 64 and/or 32): per (tolerance, panel bits) one
+    compression, then per precision the factorization and GMRES on the FP64
+    full-kernel residual to 1e-10.  One JSON line per combination, flushed."""
     import torch
     from dense_hodlr_b200 import HODLR_Matrix, KernelSpec
     parts = case.split(":")
@@ -637,6 +641,7 @@ def run_tune(case):
     n = int(parts[2])
     tols = [float(t) for t in parts[3].split(",")] if len(parts) > 3 else [1e-10, 1e-8, 1e-6, 1e-4]
     precs = parts[4].split(",") if len(parts) > 4 else ["fp64", "tf32x3", "tf32", "bf16"]
+    panels = [int(v) for v in parts[5].split(",")] if len(parts) > 5 else [64]
     if cfg == "c2":
         from dense_hodlr_b200.points import uniform_cube
         pts = uniform_cube(n, DIM, SEED)
@@ -649,14 +654,16 @@ def run_tune(case):
     b_d = torch.from_numpy(np.ascontiguousarray(b.T)).cuda()
     x_d = torch.empty_like(b_d)
     g = HODLR_Matrix(n, n, spec, pts, leaf)
-    for tol in tols:
+    for tol, bits in [(t, pb) for t in tols for pb in panels]:
         g.set_precision("fp64")
         g.set_LRTolerance(tol)
+        g.set_panel_precision(bits)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         g.storeLRinTree()
         t_lr = time.perf_counter() - t0
         kmax = int(g.ranks().max())
+        st = g.aca_stats()
         for prec in precs:
             g.set_precision(prec)
             torch.cuda.synchronize()
@@ -673,7 +680,9 @@ def run_tune(case):
             torch.cuda.synchronize()
             t_g = time.perf_counter() - t0
             print(json.dumps({"case": "tune", "cfg": cfg, "n": n, "aca_tol": tol,
-                              "precision": prec, "compress_s": t_lr, "kmax": kmax,
+                              "panel_bits": bits, "precision": prec, "compress_s": t_lr,
+                              "aca_gbs": st["bytes"] / max(st["seconds"], 1e-12) / 1e9,
+                              "kmax": kmax,
                               "factor_s": t_f, "gmres_s": t_g, "gmres_iterations": int(it),
                               "rel_residual": float(rel.max()),
                               "total_s": t_lr + t_f + t_g, "error": err}), flush=True)
