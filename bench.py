@@ -832,7 +832,8 @@ def batched_systems(nsys, seed=SEED):
 
 
 def run_batched(case):
-    """Uneven batch, case 'batched[:nsys[:max_points_per_forest[:precision]]]'.
+    """Uneven batch, case 'batched[:nsys[:max_points_per_forest[:precision[:in_place]]]]'
+    (in_place 1: K^-1 U over the U panels, which lets a forest hold more points).
     Systems are sorted by size and packed into forests (waves) of at most
     max_points points, each forest one handle whose level launches span its
     systems; per wave: compress, factor, direct solve and refinement until
@@ -844,6 +845,7 @@ def run_batched(case):
     nsys = int(parts[1]) if len(parts) > 1 else 512
     cap = int(parts[2]) if len(parts) > 2 else 1_200_000
     prec = parts[3] if len(parts) > 3 else "fp64"
+    in_place = int(parts[4]) if len(parts) > 4 else -1
     systems = batched_systems(nsys)
     order = sorted(range(nsys), key=lambda q: -systems[q][0].shape[1])
     waves, cur, npts = [], [], 0
@@ -861,11 +863,14 @@ def run_batched(case):
     res = {"case": "batched", "systems": nsys, "points": int(total_pts), "waves": len(waves),
            "max_points_per_forest": cap, "precision": prec}
 
+    peak_gb = []
+
     def run_waves(timed):
         worst, its, t_total = 0.0, [], 0.0
         for w in waves:
             F = HODLR_Matrix.forest([systems[q] for q in w], leaf=64)
             F.set_LRTolerance(1e-8)
+            F.set_factor_in_place(in_place)
             if prec != "fp64":
                 F.set_precision(prec)
             b = torch.from_numpy(rng.standard_normal(F.n)).cuda()
@@ -879,13 +884,16 @@ def run_batched(case):
             t_total += time.perf_counter() - t0
             worst = max(worst, float(rel.max()))
             its.append(it)
+            free, total = torch.cuda.mem_get_info()
+            peak_gb.append(round((total - free) / 1e9, 1))
             del F
         return t_total, worst, its
 
     run_waves(False)  # warm-up: device pool, modules
     t, worst, its = run_waves(True)
     res.update({"seconds": t, "systems_per_s": nsys / t, "max_rel_residual": worst,
-                "refine_corrections_per_wave": its})
+                "refine_corrections_per_wave": its, "device_used_gb_per_wave": peak_gb,
+                "in_place": in_place})
     # one handle per system, every 8th system, scaled by 8
     t1 = 0.0
     sample = list(range(0, nsys, 8))
