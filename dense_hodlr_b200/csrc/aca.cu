@@ -896,12 +896,16 @@ static void* aca_fn(int nt, bool ring, bool f32) {
   return f32 ? aca_fn_t<float>(nt, ring) : aca_fn_t<double>(nt, ring);
 }
 
-// Dynamic shared memory above 48 KB, and the largest shared-memory carveout:
-// the occupancy query that sizes a cooperative launch and the launch itself
-// then see the same per-SM capacity.
-static int set_smem(void* fn, size_t smem) {
-  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                       (int)cudaSharedmemCarveoutMaxShared);
+// Dynamic shared memory above 48 KB.  The ring kernels (160+ KB per CTA)
+// also ask for the largest shared-memory carveout, so that the occupancy
+// query sizing their cooperative launch and the launch see the same
+// capacity; the others keep the default split and its larger L1 for their
+// per-thread panel loads.
+static int set_smem(void* fn, size_t smem, bool ring) {
+  cudaError_t e = cudaSuccess;
+  if (ring)
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             (int)cudaSharedmemCarveoutMaxShared);
   if (e == cudaSuccess && smem > 48 * 1024)
     e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) cudaGetLastError();  // consume it: later launch checks stay clean
@@ -915,7 +919,7 @@ int aca_launch(const AcaLaunch& L, int nt, int kcap_max, bool cooperative, cudaS
   dim3 grid(L.cta_block ? L.ncta : L.nblocks * L.G), block(nt);
   void* args[] = {(void*)&L};
   void* fn = aca_fn(nt, ring, f32);
-  if (int e = set_smem(fn, smem)) return e;
+  if (int e = set_smem(fn, smem, ring)) return e;
   cudaError_t e = cooperative ? cudaLaunchCooperativeKernel(fn, grid, block, args, smem, s)
                               : cudaLaunchKernel(fn, grid, block, args, smem, s);
   if (e != cudaSuccess) cudaGetLastError();
@@ -926,7 +930,7 @@ int aca_max_coresident(int nt, int kcap_max, bool ring, bool f32, int* per_sm) {
   const size_t smem = aca_smem_bytes(nt, kcap_max, ring, f32);
   void* fn = aca_fn(nt, ring, f32);
   *per_sm = 0;
-  if (int e = set_smem(fn, smem)) return e;
+  if (int e = set_smem(fn, smem, ring)) return e;
   int nb = 0;
   cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, nt, smem);
   if (e != cudaSuccess) cudaGetLastError();

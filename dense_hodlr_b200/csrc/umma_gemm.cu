@@ -312,6 +312,8 @@ __global__ void umma_splitk_reduce(const GemmProblem* __restrict__ probs, const 
 
 }  // namespace
 
+constexpr int UMMA_MAX_KCHUNK = 4096;
+
 void umma_plan(std::vector<GemmProblem>& probs, std::vector<int4>& tiles, int64_t& ws_elems,
                bool allow_split, int target_ctas) {
   tiles.clear();
@@ -329,6 +331,11 @@ void umma_plan(std::vector<GemmProblem>& probs, std::vector<int4>& tiles, int64_
       int want = (int)((target_ctas + mn_tiles - 1) / std::max<int64_t>(mn_tiles, 1));
       splits = std::max(1, std::min(want, p.K / 1024));
     }
+    // FP32 accumulation in TMEM over at most UMMA_MAX_KCHUNK terms; longer
+    // reductions (V^T Y over the rows of a top node) are split and their
+    // partial tiles summed in FP64, so the accumulation error stays at the
+    // level of a few thousand FP32 additions whatever the node size
+    if (allow_split) splits = std::max(splits, (p.K + UMMA_MAX_KCHUNK - 1) / UMMA_MAX_KCHUNK);
     int kchunk = (p.K + splits - 1) / splits;
     kchunk = ((kchunk + 63) / 64) * 64;
     splits = (p.K + kchunk - 1) / kchunk;
