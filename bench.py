@@ -299,7 +299,7 @@ def run_ours(args, rank, world, local_rank):
         m0 = torch.cuda.Event(enable_timing=True)
         m1 = torch.cuda.Event(enable_timing=True)
         m_it, m_rel = [], []
-        m_steps = 2
+        m_steps = 5
         m0.record(stream)
         for _ in range(m_steps):
             it, rel = step()
@@ -317,13 +317,14 @@ def run_ours(args, rank, world, local_rank):
         g.set_precision("fp64")
         g.recLU_Compute()
 
-    sphere = None
-    if not args.no_sphere:
-        try:
-            sphere = run_sphere_pair(stream)
-        except Exception as e:  # reported in the line; the headline workload stands alone
-            sphere = {"error": f"{type(e).__name__}: {e}"}
-        torch.cuda.synchronize()
+    scale_pairs = {}
+    if not args.no_scale:
+        for key, cfg_name, n_cfg in SCALE_PAIRS:
+            try:
+                scale_pairs[key] = run_scale_pair(stream, cfg_name, n_cfg)
+            except Exception as e:  # reported in the line; the headline workload stands alone
+                scale_pairs[key] = {"error": f"{type(e).__name__}: {e}"}
+            torch.cuda.synchronize()
 
     # direct solve only (no refinement), for the phase breakdown
     g.solve_device(b_d.data_ptr(), x_d.data_ptr(), NRHS)
@@ -437,7 +438,7 @@ def run_ours(args, rank, world, local_rank):
                          "avg_launch_s": aca_s / max(aca_launch, 1.0),
                          "launches_per_step": aca_launch},
         "mixed": mixed,
-        "sphere_matern": sphere,
+        "scale_pairs": scale_pairs,
         "clocks": clocks,
         "gpu_launches": int(n_launch),
     }
@@ -458,65 +459,59 @@ def run_ours(args, rank, world, local_rank):
     return out
 
 
-# The end-to-end target's shape (unit sphere, Matern-3/2 l = 0.1 + 1e-2 delta,
-# leaf 128, ACA tol 1e-10, one right-hand side) at the largest N whose FP64
-# factors fit one B200 (its top-level ranks grow like sqrt(N): 4117 here).
-SPHERE_N = 262144
-# The chosen mixed form on it: the preconditioner compressed at MIXED_TOL
-# (a factor in reduced precision needs no more) into FP32 panels, with
-# MIXED_PREC tensor-core Woodbury products; GMRES on the FP64 full-kernel
-# residual to 1e-10.
-MIXED_TOL, MIXED_PREC, MIXED_PANEL_BITS = 1e-6, "tf32x3", 32
+# Extra keys of the bench line: the two configurations measured at their
+# full size or the largest that fits, FP64 against the mixed form, one timed
+# step each (compress + factor + GMRES until ||b - K x|| / ||b|| <= 1e-10).
+#  * the end-to-end target's shape (unit sphere, Matern-3/2 l = 0.1 + 1e-2
+#    delta, leaf 128, ACA tol 1e-10, 1 RHS) at N = 262144, the largest whose
+#    FP64 factors fit one B200 (its top rank, 4117 here, grows like sqrt(N));
+#  * the mixed-precision configuration (3D cube, Gaussian l = 0.3 + 0.1 delta,
+#    leaf 128, tol 1e-8, 16 RHS) at its full N = 2^20.
+# The mixed form keeps the configuration's tolerance (a looser preconditioner
+# stalled GMRES on the sphere shape at every tolerance from 1e-8 to 1e-5)
+# and runs the Woodbury products in 3xTF32 on tcgen05; its GMRES is capped at
+# MIXED_MAX_ITER iterations, beyond which it is reported as not converged.
+SCALE_PAIRS = (("sphere_matern", "c5", 262144), ("cube_gaussian", "c3", 1 << 20))
+MIXED_PREC, MIXED_MAX_ITER = "tf32x3", 30
 
 
-def run_sphere_pair(stream, steps=2):
-    """FP64 (ACA tol 1e-10) against the mixed form on the sphere / Matern
-    shape, each timed over `steps` steps after one warm-up; a step is
-    compress + factor + GMRES until ||b - K x|| / ||b|| <= 1e-10."""
+def run_scale_pair(stream, cfg_name, n):
     import torch
     from dense_hodlr_b200 import HODLR_Matrix, KernelSpec
-    c = SCALE_CONFIGS["c5"]
-    pts = scale_points(c["cloud"], SPHERE_N)
-    b = np.random.default_rng(SEED + 1).standard_normal((SPHERE_N, c["nrhs"]))
+    c = SCALE_CONFIGS[cfg_name]
+    pts = scale_points(c["cloud"], n)
+    b = np.random.default_rng(SEED + 1).standard_normal((n, c["nrhs"]))
     b_d = torch.from_numpy(np.ascontiguousarray(b.T)).cuda()
     x_d = torch.empty_like(b_d)
-    g = HODLR_Matrix(SPHERE_N, SPHERE_N, KernelSpec(c["kernel"], c["l"], c["shift"]), pts,
-                     c["leaf"])
-    out = {"workload": (f"N={SPHERE_N} uniform on the unit sphere, k-d ordered, Matern-3/2 "
-                        f"l=0.1 +1e-2*delta, leaf 128, 1 RHS N(0,1), to rel residual 1e-10"),
-           "steps": steps}
-    for name, tol, prec, bits in (("fp64", c["tol"], "fp64", 64),
-                                  ("mixed", MIXED_TOL, MIXED_PREC, MIXED_PANEL_BITS)):
-        g.set_LRTolerance(tol)
+    g = HODLR_Matrix(n, n, KernelSpec(c["kernel"], c["l"], c["shift"]), pts, c["leaf"])
+    g.set_LRTolerance(c["tol"])
+    out = {"n": n, "aca_tol": c["tol"], "nrhs": c["nrhs"], "steps": 1,
+           "note": "one step per leg, no warm-up of its own (the headline steps ran first)"}
+    for name, prec, max_iter in (("fp64", "fp64", MAX_IR), ("mixed", MIXED_PREC, MIXED_MAX_ITER)):
         g.set_precision(prec)
-        g.set_panel_precision(bits)
-        rec = {"aca_tol": tol, "precision": prec, "aca_panel_bits": bits}
-        for it in range(steps + 1):
-            g.reset()
-            torch.cuda.synchronize()
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            g.storeLRinTree()
-            g.recLU_Compute()
-            n_it, rel = g.iterative_solve_device(b_d.data_ptr(), x_d.data_ptr(), c["nrhs"],
-                                                 tol=RES_TOL, max_iter=MAX_IR, restart=40)
-            e1.record(stream)
-            torch.cuda.synchronize()
-            if it == 0:
-                continue
-            rec.setdefault("ms", []).append(e0.elapsed_time(e1))
-            rec.update({"lr_s": g.get_LR_ComputationTime(),
-                        "factor_s": g.get_recLU_FactorizationTime(),
-                        "gmres_s": g.get_recLU_SolveTime(), "gmres_iterations": int(n_it),
-                        "rel_residual": float(rel.max()), "max_rank": int(g.ranks().max())})
-        rec["ms_per_step"] = float(np.mean(rec.pop("ms")))
-        rec["x"] = x_d.cpu().numpy().T.copy()
-        out[name] = rec
+        g.reset()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        g.storeLRinTree()
+        g.recLU_Compute()
+        n_it, rel = g.iterative_solve_device(b_d.data_ptr(), x_d.data_ptr(), c["nrhs"],
+                                             tol=RES_TOL, max_iter=max_iter, restart=40)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        out[name] = {"precision": prec, "ms_per_step": e0.elapsed_time(e1),
+                     "lr_s": g.get_LR_ComputationTime(),
+                     "factor_s": g.get_recLU_FactorizationTime(),
+                     "gmres_s": g.get_recLU_SolveTime(), "gmres_iterations": int(n_it),
+                     "rel_residual": float(rel.max()), "converged": bool(rel.max() <= RES_TOL),
+                     "max_rank": int(g.ranks().max())}
+        out[name]["x"] = x_d.cpu().numpy().T.copy()
     xf, xm = out["fp64"].pop("x"), out["mixed"].pop("x")
     out["mixed"]["solution_rel_diff_vs_fp64"] = float(np.linalg.norm(xm - xf) /
                                                       np.linalg.norm(xf))
-    out["mixed_speedup_vs_fp64"] = out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"]
+    out["mixed_speedup_vs_fp64"] = (out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"]
+                                    if out["mixed"]["converged"] else None)
     del g
     return out
 
@@ -603,11 +598,18 @@ def run_profile_case(case):
         # launches after the aca_kernel ones) and one 8-RHS direct solve
         import torch
         from dense_hodlr_b200.points import uniform_cube
-        n = int(case.split(":")[1]) if ":" in case else N_PTS
-        pts = uniform_cube(n, DIM, SEED) if n != N_PTS else workload_inputs()[0]
+        parts = case.split(":")
+        n = int(parts[1]) if len(parts) > 1 else N_PTS
+        if len(parts) > 2:  # another configuration's shape, e.g. 'factor-profile:65536:c5'
+            c = SCALE_CONFIGS[parts[2]]
+            pts = scale_points(c["cloud"], n)
+            g = HODLR_Matrix(n, n, KernelSpec(c["kernel"], c["l"], c["shift"]), pts, c["leaf"])
+            g.set_LRTolerance(c["tol"])
+        else:
+            pts = uniform_cube(n, DIM, SEED) if n != N_PTS else workload_inputs()[0]
+            g = HODLR_Matrix(n, n, KernelSpec("matern32", LSCALE, SHIFT), pts, LEAF)
+            g.set_LRTolerance(TOL)
         b = np.random.default_rng(SEED + 1).standard_normal((n, NRHS))
-        g = HODLR_Matrix(n, n, KernelSpec("matern32", LSCALE, SHIFT), pts, LEAF)
-        g.set_LRTolerance(TOL)
         g.storeLRinTree()
         g.recLU_Compute()
         b_d = torch.from_numpy(np.ascontiguousarray(b.T)).cuda()
@@ -928,8 +930,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision leg")
-    ap.add_argument("--no-sphere", action="store_true",
-                    help="skip the sphere / Matern tol 1e-10 FP64-vs-mixed pair")
+    ap.add_argument("--no-scale", action="store_true",
+                    help="skip the FP64-vs-mixed pairs of the sphere and 2^20-point cube shapes")
     args = ap.parse_args()
     if args.case:
         run_profile_case(args.case)
