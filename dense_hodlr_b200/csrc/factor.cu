@@ -358,9 +358,10 @@ int do_factorize(hodlr_t h) {
     if (e) return cuda_fail(h, (cudaError_t)e, "schur_factor");
     h->nlaunch += schur_factor_launches(sds.data(), nn);
     if (L.coff > 0) {
-      e = schur_solve_launch(S, nn, -1, L.coff, L.max_sd, h->stream);
+      int nl_solve = 0;
+      e = schur_solve_factor_launch(S, nn, sds.data(), L.coff, h->stream, &nl_solve);
       if (e) return cuda_fail(h, (cudaError_t)e, "schur_solve");
-      h->nlaunch += 1;
+      h->nlaunch += nl_solve;
       // Y_a[rows_h] -= Y_l[rows_h, 0 : rank(U_h)] * y_h[:, level a's columns]
       // for every ancestor level a < l
       std::vector<GemmProblem> up;

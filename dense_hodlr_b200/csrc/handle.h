@@ -225,7 +225,10 @@ struct hodlr_handle_s {
   std::vector<hodlr_impl::Level> lv;
   std::vector<int> cap_hint;  // initial W/V columns per level (0 = default)
   int gemm_prec = HODLR_GEMM_FP64;  // arithmetic of the Woodbury products
-  bool aca_ring = true;  // group-level ACA panels through the bulk-copy ring
+  // group-level ACA panels through the bulk-copy ring (off by default: with
+  // one 256-thread CTA per SM it streamed slower than two CTAs of per-thread
+  // loads -- 3.05 vs 3.64 TB/s on the sphere shape, N = 262144)
+  bool aca_ring = false;
   bool aca_f32 = false;  // compress into FP32 panels (hodlr_set_panel_precision)
   unsigned spin_limit = 0;       // polls of an ACA group barrier (0: HODLR_SPIN_LIMIT)
   bool bar_unreachable = false;  // ACA group barriers wait for one arrival too many

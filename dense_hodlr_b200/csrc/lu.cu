@@ -200,13 +200,16 @@ __global__ void __launch_bounds__(LNT) leaf_solve_kernel(LeafSolveLaunch L) {
 // ---------------------------------------------------------- Schur form
 // S[node] (sd x sd, sd = kb + kt): identity blocks on the diagonal, the level
 // products of Z on the off-diagonal blocks.
+// CTA (node, y) fills every gridDim.y-th slice of the node's entries, so a
+// large S is written by many CTAs.
 __global__ void schur_form_kernel(SchurLaunch L) {
   const int node = blockIdx.x;
   const SchurNode N = L.nodes[node];
   const int sd = N.kb + N.kt;
   double* S = L.S + N.s_off;
   const double* Z = L.Z + N.z_off;  // sd x zcols, ld sd
-  for (int64_t e = threadIdx.x; e < (int64_t)sd * sd; e += blockDim.x) {
+  for (int64_t e = threadIdx.x + (int64_t)blockIdx.y * blockDim.x; e < (int64_t)sd * sd;
+       e += (int64_t)blockDim.x * gridDim.y) {
     int i = (int)(e % sd), j = (int)(e / sd);
     double v;
     if (i < N.kb && j < N.kb)
@@ -491,6 +494,119 @@ __global__ void __launch_bounds__(256) big_update_kernel(SchurLaunch L, BigNodes
   }
 }
 
+// ---------------------------------- blocked solve of large nodes' ancestor columns
+// y = S^-1 Z for the N.coff ancestor columns of a node with sd >= SCHUR_BIG_SD
+// (the factorization's schur solve, src/HODLR_Matrix.cpp:682): the LU's row
+// interchanges, then the unit-lower and the upper solves by 32-row diagonal
+// blocks, each a register-resident triangular solve (one thread per column)
+// followed by a 64 x 64-tiled update of the remaining rows over all SMs.  The
+// one-CTA-per-column-tile kernel would read the whole LU again for every 16
+// columns; here each block of the LU is read once per 64 columns.
+__global__ void __launch_bounds__(256) big_rhs_perm_kernel(SchurLaunch L, BigNodes B) {
+  const SchurNode N = L.nodes[B.idx[blockIdx.y]];
+  const int n = N.kb + N.kt;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= N.coff) return;
+  double* x = L.R + N.r_off + (int64_t)c * n;
+  const int* piv = L.piv + N.p_off;
+  for (int p = 0; p < n; ++p) {
+    const int q = __ldg(piv + p);
+    if (q != p) {
+      const double t = x[p];
+      x[p] = x[q];
+      x[q] = t;
+    }
+  }
+}
+
+template <bool LOWER>
+__global__ void __launch_bounds__(256) big_rhs_diag_kernel(SchurLaunch L, BigNodes B, int j0) {
+  __shared__ double t11[BNB][BNB + 1];
+  const SchurNode N = L.nodes[B.idx[blockIdx.y]];
+  const int n = N.kb + N.kt;
+  if (j0 >= n) return;
+  const int nb = min(BNB, n - j0);
+  const double* a = L.S + N.s_off;
+  for (int e = threadIdx.x; e < BNB * BNB; e += blockDim.x) {
+    const int i = e % BNB, p = e / BNB;
+    t11[i][p] = (i < nb && p < nb) ? a[(int64_t)(j0 + p) * n + j0 + i] : (i == p ? 1.0 : 0.0);
+  }
+  __syncthreads();
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= N.coff) return;
+  double* x = L.R + N.r_off + (int64_t)c * n + j0;
+  double u[BNB];
+#pragma unroll
+  for (int i = 0; i < BNB; ++i) u[i] = i < nb ? x[i] : 0.0;
+  if (LOWER) {  // unit lower, rows in order
+#pragma unroll
+    for (int i = 1; i < BNB; ++i)
+#pragma unroll
+      for (int p = 0; p < i; ++p) u[i] = fma(-t11[i][p], u[p], u[i]);
+  } else {  // upper, rows in reverse order
+#pragma unroll
+    for (int i = BNB - 1; i >= 0; --i) {
+      u[i] = u[i] / t11[i][i];
+#pragma unroll
+      for (int p = 0; p < i; ++p) u[p] = fma(-t11[p][i], u[i], u[p]);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < BNB; ++i)
+    if (i < nb) x[i] = u[i];
+}
+
+// Rows below the block (LOWER) or above it (!LOWER) of the node's ancestor
+// columns -= S[those rows, block columns] * the block's solved rows.
+template <bool LOWER>
+__global__ void __launch_bounds__(256) big_rhs_update_kernel(SchurLaunch L, BigNodes B, int j0) {
+  __shared__ double ls[BNB][BT + 1];  // S tile, [p][row]
+  __shared__ double us[BNB][BT + 1];  // solved block rows, [p][col]
+  const SchurNode N = L.nodes[B.idx[blockIdx.z]];
+  const int n = N.kb + N.kt;
+  if (j0 >= n) return;
+  const int nb = min(BNB, n - j0);
+  const int rlo = LOWER ? j0 + nb : 0, rhi = LOWER ? n : j0;
+  const int r0 = rlo + blockIdx.x * BT, c0 = blockIdx.y * BT;
+  if (r0 >= rhi || c0 >= N.coff) return;
+  const double* a = L.S + N.s_off;
+  double* x = L.R + N.r_off;
+  for (int e = threadIdx.x; e < BNB * BT; e += blockDim.x) {
+    const int i = e % BT, p = e / BT;
+    ls[p][i] = (p < nb && r0 + i < rhi) ? a[(int64_t)(j0 + p) * n + r0 + i] : 0.0;
+    us[p][i] = (p < nb && c0 + i < N.coff) ? x[(int64_t)(c0 + i) * n + j0 + p] : 0.0;
+  }
+  __syncthreads();
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  double acc[4][4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+#pragma unroll
+    for (int y = 0; y < 4; ++y) acc[q][y] = 0.0;
+#pragma unroll 8
+  for (int p = 0; p < BNB; ++p) {
+    double l[4], u[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) l[q] = ls[p][tx + 16 * q];
+#pragma unroll
+    for (int y = 0; y < 4; ++y) u[y] = us[p][ty + 16 * y];
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+      for (int y = 0; y < 4; ++y) acc[q][y] = fma(l[q], u[y], acc[q][y]);
+  }
+#pragma unroll
+  for (int y = 0; y < 4; ++y) {
+    const int c = c0 + ty + 16 * y;
+    if (c >= N.coff) continue;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int r = r0 + tx + 16 * q;
+      if (r < rhi) x[(int64_t)c * n + r] -= acc[q][y];
+    }
+  }
+}
+
 // x <- U^-1 L^-1 x for `ncol` columns in shared memory (x[c*ldx+i]) with the
 // packed LU of an n x n matrix in global memory (column-major, ld n): the
 // capacitance matrices, up to a few thousand rows, with few columns per CTA.
@@ -594,11 +710,12 @@ constexpr int STC = 16;
 // global memory (capacitance matrices too large for even one column).
 template <bool WARP_SUBST>
 __global__ void __launch_bounds__(256) schur_solve_kernel(SchurLaunch L, int ncols, int tc,
-                                                          bool in_smem) {
+                                                          bool in_smem, int skip_sd) {
   extern __shared__ double xs_smem[];
   const int node = blockIdx.y;
   const SchurNode N = L.nodes[node];
   const int n = N.kb + N.kt;
+  if (n >= skip_sd) return;  // left to the blocked solve
   const int cols = ncols < 0 ? N.coff : ncols;
   const int c0 = blockIdx.x * tc;
   if (c0 >= cols) return;
@@ -676,7 +793,10 @@ static int panel_width(int rows) {
 
 int schur_factor_launch(const SchurLaunch& L, int nnodes, const int* sd, cudaStream_t s) {
   if (nnodes == 0) return 0;
-  schur_form_kernel<<<nnodes, 256, 0, s>>>(L);
+  int form_y = 1;  // CTAs per node for forming S: about 64K entries each
+  for (int i = 0; i < nnodes; ++i)
+    form_y = std::max(form_y, (int)std::min<int64_t>(256, (int64_t)sd[i] * sd[i] / 65536 + 1));
+  schur_form_kernel<<<dim3(nnodes, form_y), 256, 0, s>>>(L);
   int small_max = 0, big_max = 0;
   std::vector<int> big;
   for (int i = 0; i < nnodes; ++i) {
@@ -739,6 +859,59 @@ int schur_factor_launches(const int* sd, int nnodes) {
   return n;
 }
 
+int schur_solve_factor_launch(const SchurLaunch& L, int nnodes, const int* sd, int coff,
+                              cudaStream_t s, int* launches) {
+  *launches = 0;
+  if (nnodes == 0 || coff <= 0) return 0;
+  std::vector<int> big;
+  int small_max = 0;
+  for (int i = 0; i < nnodes; ++i) {
+    if (sd[i] >= SCHUR_BIG_SD)
+      big.push_back(i);
+    else
+      small_max = std::max(small_max, sd[i]);
+  }
+  if (small_max > 0) {
+    const size_t col_bytes = sizeof(double) * (size_t)(small_max | 1);
+    const int tc = (int)std::max<size_t>(1, std::min<size_t>(STC, 200 * 1024 / col_bytes));
+    const size_t smem = col_bytes * tc;
+    if (smem > 48 * 1024)
+      cudaFuncSetAttribute(schur_solve_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem);
+    schur_solve_kernel<false><<<dim3((coff + tc - 1) / tc, nnodes), 256, smem, s>>>(
+        L, -1, tc, true, SCHUR_BIG_SD);
+    ++*launches;
+  }
+  const int ctiles = (coff + BT - 1) / BT, cblocks = (coff + 255) / 256;
+  for (size_t b0 = 0; b0 < big.size(); b0 += BIG_MAX) {
+    BigNodes B;
+    B.count = (int)std::min<size_t>(BIG_MAX, big.size() - b0);
+    int mx = 0;
+    for (int i = 0; i < B.count; ++i) {
+      B.idx[i] = big[b0 + i];
+      mx = std::max(mx, sd[big[b0 + i]]);
+    }
+    big_rhs_perm_kernel<<<dim3(cblocks, B.count), 256, 0, s>>>(L, B);
+    ++*launches;
+    for (int j0 = 0; j0 < mx; j0 += BNB) {
+      big_rhs_diag_kernel<true><<<dim3(cblocks, B.count), 256, 0, s>>>(L, B, j0);
+      const int rows = mx - j0 - BNB;
+      if (rows > 0)
+        big_rhs_update_kernel<true><<<dim3((rows + BT - 1) / BT, ctiles, B.count), 256, 0, s>>>(
+            L, B, j0);
+      *launches += 1 + (rows > 0);
+    }
+    for (int j0 = (mx - 1) / BNB * BNB; j0 >= 0; j0 -= BNB) {
+      big_rhs_diag_kernel<false><<<dim3(cblocks, B.count), 256, 0, s>>>(L, B, j0);
+      if (j0 > 0)
+        big_rhs_update_kernel<false><<<dim3((j0 + BT - 1) / BT, ctiles, B.count), 256, 0, s>>>(
+            L, B, j0);
+      *launches += 1 + (j0 > 0);
+    }
+  }
+  return (int)cudaGetLastError();
+}
+
 int schur_solve_launch(const SchurLaunch& L, int nnodes, int ncols, int max_cols, int max_sd,
                        cudaStream_t s) {
   if (nnodes == 0 || max_cols <= 0) return 0;
@@ -754,12 +927,12 @@ int schur_solve_launch(const SchurLaunch& L, int nnodes, int ncols, int max_cols
     if (smem > 48 * 1024)
       cudaFuncSetAttribute(schur_solve_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem);
-    schur_solve_kernel<true><<<grid, 256, smem, s>>>(L, ncols, tc, in_smem);
+    schur_solve_kernel<true><<<grid, 256, smem, s>>>(L, ncols, tc, in_smem, INT_MAX);
   } else {
     if (smem > 48 * 1024)
       cudaFuncSetAttribute(schur_solve_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem);
-    schur_solve_kernel<false><<<grid, 256, smem, s>>>(L, ncols, tc, in_smem);
+    schur_solve_kernel<false><<<grid, 256, smem, s>>>(L, ncols, tc, in_smem, INT_MAX);
   }
   return (int)cudaGetLastError();
 }

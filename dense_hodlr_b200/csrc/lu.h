@@ -58,3 +58,8 @@ int schur_factor_launch(const SchurLaunch& L, int nnodes, const int* sd, cudaStr
 int schur_factor_launches(const int* sd, int nnodes);
 int schur_solve_launch(const SchurLaunch& L, int nnodes, int ncols, int max_cols, int max_sd,
                        cudaStream_t s);
+// The factorization's solves y = S^-1 Z of the `coff` ancestor columns of every
+// node (R at r_off, ld sd); nodes with sd >= SCHUR_BIG_SD by the blocked
+// solve.  sd: host array of the nodes' sizes.  *launches: kernels launched.
+int schur_solve_factor_launch(const SchurLaunch& L, int nnodes, const int* sd, int coff,
+                              cudaStream_t s, int* launches);

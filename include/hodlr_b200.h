@@ -321,9 +321,9 @@ int hodlr_gemm_device(int precision, int mode, int m, int n, int k, const double
 int hodlr_set_factor_in_place(hodlr_t h, int mode);
 
 /* How the ACA of the few-block top levels reads its W/V panel slices (no
- * counterpart in the reference): on = 1 (default) streams them through a
- * shared-memory ring filled by bulk copies (used when N is even), 0 loads
- * them per thread.  Pivots, ranks and W/V are the same either way; the
+ * counterpart in the reference): on = 1 streams them through a shared-memory
+ * ring filled by bulk copies (used when N is even), 0 (default, measured
+ * faster) loads them per thread.  Pivots, ranks and W/V are the same either way; the
  * setting applies from the next compression. */
 int hodlr_set_aca_streaming(hodlr_t h, int on);
 

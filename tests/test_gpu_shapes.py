@@ -5,8 +5,8 @@ and for the minPivot skip-row path of ACA.
   ACA tol 1e-10): its ranks make the top capacitance matrices large enough
   for the multi-CTA blocked LU (sd >= SCHUR_BIG_SD = 768).
 * The cube / Gaussian shape (l = 0.3, shift 0.1, leaf 128, tol 1e-8) with 16
-  right-hand sides, through HODLR-preconditioned GMRES in every precision of
-  the Woodbury products.
+  right-hand sides, through HODLR-preconditioned GMRES with FP64, 3xTF32 and
+  TF32 Woodbury products.
 * minPivot >= 1 (src/lowRank.cpp:187-195 skip path, :197-203 and :217-227
   fallbacks): dense 10 * Gaussian + I with minPivot 2.5 (truncated to 2, as
   the reference passes it to an int).
@@ -83,7 +83,7 @@ def test_min_pivot_skip_rows_bit_exact(oracle_mod, n, leaf):
     assert np.linalg.norm(xs - xo) / np.linalg.norm(xo) <= SOLVE_TOL
 
 
-def test_cube_gaussian_16_rhs_gmres_every_precision(oracle_mod):
+def test_cube_gaussian_16_rhs_gmres_fp64_and_tf32_forms(oracle_mod):
     n, nrhs = 16384, 16
     pts = uniform_cube(n, 3, 5)
     g, o = _pair(oracle_mod, pts, "gaussian", 0.3, 1e-1, 128, 1e-8)
@@ -94,7 +94,9 @@ def test_cube_gaussian_16_rhs_gmres_every_precision(oracle_mod):
     xo = o.solve(b, nthreads=8)
     x64 = g.recLU_Solve(b)
     assert np.linalg.norm(x64 - xo) / np.linalg.norm(xo) <= SOLVE_TOL
-    for prec in ("fp64", "tf32x3", "tf32", "bf16"):
+    # BF16 is left out: a factor preconditions only while cond(K) * u < ~1, and
+    # here cond(K) ~ 2.5e4 against u = 3.9e-3 (it stalls near 1, as measured)
+    for prec in ("fp64", "tf32x3", "tf32"):
         g.set_precision(prec)
         g.recLU_Compute()
         it, rel, x = _device_gmres(g, b)
@@ -150,6 +152,7 @@ def test_fp32_panels_compress_to_tolerance_and_precondition(oracle_mod, n):
     g = HODLR_Matrix(n, n, KernelSpec("matern32", 0.2, 1e-2), pts, 128)
     g.set_LRTolerance(tol)
     g.set_panel_precision(32)
+    g.set_aca_streaming(1)  # taken where n % 4 == 0
     g.storeLRinTree()
     r32, r64 = g.ranks().astype(float), ref.ranks().astype(float)
     big = r64 >= 20
@@ -170,3 +173,26 @@ def test_fp32_panels_compress_to_tolerance_and_precondition(oracle_mod, n):
     it, rel, x = _device_gmres(g, bvec)
     assert rel.max() <= 1e-10
     assert np.all(g.residual(x, bvec) <= 1e-10)
+
+
+@pytest.mark.parametrize("n,dim", [(32768, 2), (20000, 3)])
+def test_ring_streaming_bit_identical_to_per_thread_loads(n, dim):
+    """The top-level ACA with its panel slices streamed through the bulk-copy
+    ring (hodlr_set_aca_streaming(1)) against per-thread loads: the same
+    pivots, ranks, iteration counts and W/V bits on every block."""
+    pts = uniform_cube(n, dim, 13)
+    out = []
+    for on in (0, 1):
+        g = HODLR_Matrix(n, n, KernelSpec("matern32", 0.2, 1e-2), pts, 128)
+        g.set_LRTolerance(1e-8)
+        g.set_aca_streaming(on)
+        g.storeLRinTree()
+        nb = g.num_blocks()
+        out.append((g.ranks(), [g.block_info(b)["iters"] for b in range(nb)],
+                    [g.pivots(b) for b in range(nb)], [g.lowrank(b) for b in range(8)]))
+    (r0, i0, p0, f0), (r1, i1, p1, f1) = out
+    assert np.array_equal(r0, r1) and i0 == i1
+    for a, b in zip(p0, p1):
+        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+    for (W0, V0), (W1, V1) in zip(f0, f1):
+        assert np.array_equal(W0, W1) and np.array_equal(V0, V1)
