@@ -297,8 +297,10 @@ __device__ void residual_pass(const AcaLaunch& L, const AcaBlock& B, T* P, int l
 // index so that every copy is 16-byte aligned (requires an even N).
 constexpr int TMA_BC = 4;
 constexpr int TMA_S = 4;
-constexpr int TMA_NT = 256, TMA_E = 4, TMA_BR = TMA_NT * TMA_E;
-// ring bytes for panel elements of `es` bytes (128 KB for FP64, 64 KB for FP32)
+// two elements per thread: 512-row chunks, so that the ring (64 KB for FP64,
+// 32 KB for FP32) and 128 registers per thread leave room for two CTAs per SM
+constexpr int TMA_NT = 256, TMA_E = 2, TMA_BR = TMA_NT * TMA_E;
+// ring bytes for panel elements of `es` bytes
 constexpr size_t tma_ring_bytes(size_t es) { return es * TMA_S * TMA_BC * TMA_BR; }
 
 struct Ring {
@@ -543,7 +545,7 @@ __device__ double resolve_eps(Shared& sh, const AcaLaunch& L, const AcaBlock& B,
 // compression, whose values are rounded to FP32 when stored and read back
 // into FP64 arithmetic).
 template <int NT, int E, bool RING, typename T>
-__global__ void __launch_bounds__(NT, (RING ? 1 : (NT == 256 ? 2 : 4))) aca_kernel(AcaLaunch L) {
+__global__ void __launch_bounds__(NT, (NT == 256 ? 2 : 4)) aca_kernel(AcaLaunch L) {
   extern __shared__ __align__(128) double dyn_all[];
   __shared__ Shared sh;
   __shared__ __align__(8) uint64_t ring_full[TMA_S], ring_empty[TMA_S];
@@ -873,13 +875,11 @@ static size_t aca_smem(int nt, int kcap_max, bool global_dots, bool ring, bool f
          sizeof(double) * (size_t)(global_dots ? 1 : 1 + nt / 32) * (size_t)kcap_max;
 }
 
-// The per-warp dot partials move to global memory once they would take more
-// than 100 KB of shared memory per CTA (without the ring: beyond that fewer
-// than two 256-thread CTAs fit on an SM), or with the ring once the CTA's
-// shared memory would pass 220 KB.
+// The per-warp dot partials move to global memory once the CTA's shared
+// memory would pass 100 KB (110 KB with the ring): beyond that fewer than two
+// 256-thread CTAs fit on an SM.
 bool aca_dots_global(int nt, int kcap_max, bool ring, bool f32) {
-  return ring ? aca_smem(nt, kcap_max, false, true, f32) > 220 * 1024
-              : aca_smem(nt, kcap_max, false, false, f32) > 100 * 1024;
+  return aca_smem(nt, kcap_max, false, ring, f32) > (ring ? 110 : 100) * 1024;
 }
 
 size_t aca_smem_bytes(int nt, int kcap_max, bool ring, bool f32) {
