@@ -408,7 +408,9 @@ int do_compress(hodlr_t h) {
       if (aca_max_coresident(256, L.kcap, false, h->aca_f32, &ps) ||
           aca_max_coresident(256, L.kcap, true, h->aca_f32, &ps_ring))
         return fail(h, HODLR_ERR_CUDA, "occupancy query failed");
-      const bool ring = h->aca_ring && (h->n % (h->aca_f32 ? 4 : 2) == 0) &&
+      // (FP64 panels only: with FP32 panels the ring's top-level ranks ran
+      // away from the per-thread path's, so FP32 compressions stream per thread)
+      const bool ring = h->aca_ring && !h->aca_f32 && (h->n % 2 == 0) &&
                         ps_ring * h->num_sms >= 2 * nb;
       if (ring) ps = ps_ring;
       // equal groups: CTAs sized by predicted work measured 2-8% slower on

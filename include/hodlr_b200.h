@@ -322,8 +322,8 @@ int hodlr_set_factor_in_place(hodlr_t h, int mode);
 
 /* How the ACA of the few-block top levels reads its W/V panel slices (no
  * counterpart in the reference): on = 1 streams them through a shared-memory
- * ring filled by bulk copies (used when N is even), 0 (default, measured
- * faster) loads them per thread.  Pivots, ranks and W/V are the same either way; the
+ * ring filled by bulk copies (used when N is even and the panels are
+ * FP64), 0 (default, measured faster) loads them per thread.  Pivots, ranks and W/V are the same either way; the
  * setting applies from the next compression. */
 int hodlr_set_aca_streaming(hodlr_t h, int on);
 

@@ -135,7 +135,7 @@ def test_factor_in_place_matches_separate_panels(oracle_mod):
     assert np.array_equal(W0, W2) and np.array_equal(V0, V2)
 
 
-@pytest.mark.parametrize("n", [16384, 9999])  # the ring path (n % 4 == 0) and the plain one
+@pytest.mark.parametrize("n", [16384, 9999])
 def test_fp32_panels_compress_to_tolerance_and_precondition(oracle_mod, n):
     """The mixed form's compression into FP32 panels (hodlr_set_panel_precision(32)),
     tol 1e-6: every top block's W V^T within 1e-5 of the block (Frobenius,
@@ -152,7 +152,7 @@ def test_fp32_panels_compress_to_tolerance_and_precondition(oracle_mod, n):
     g = HODLR_Matrix(n, n, KernelSpec("matern32", 0.2, 1e-2), pts, 128)
     g.set_LRTolerance(tol)
     g.set_panel_precision(32)
-    g.set_aca_streaming(1)  # taken where n % 4 == 0
+    g.set_aca_streaming(1)  # FP32 panels stream per thread even when the ring is asked for
     g.storeLRinTree()
     r32, r64 = g.ranks().astype(float), ref.ranks().astype(float)
     big = r64 >= 20
