@@ -495,7 +495,7 @@ __global__ void __launch_bounds__(256) big_update_kernel(SchurLaunch L, BigNodes
 }
 
 // ---------------------------------- blocked solve of large nodes' ancestor columns
-// y = S^-1 Z for the N.coff ancestor columns of a node with sd >= SCHUR_BIG_SD
+// y = S^-1 Z for the N.coff ancestor columns of a node with sd >= SCHUR_BIG_SOLVE_SD
 // (the factorization's schur solve, src/HODLR_Matrix.cpp:682): the LU's row
 // interchanges, then the unit-lower and the upper solves by 32-row diagonal
 // blocks, each a register-resident triangular solve (one thread per column)
@@ -866,7 +866,7 @@ int schur_solve_factor_launch(const SchurLaunch& L, int nnodes, const int* sd, i
   std::vector<int> big;
   int small_max = 0;
   for (int i = 0; i < nnodes; ++i) {
-    if (sd[i] >= SCHUR_BIG_SD)
+    if (sd[i] >= SCHUR_BIG_SOLVE_SD)
       big.push_back(i);
     else
       small_max = std::max(small_max, sd[i]);
@@ -879,7 +879,7 @@ int schur_solve_factor_launch(const SchurLaunch& L, int nnodes, const int* sd, i
       cudaFuncSetAttribute(schur_solve_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem);
     schur_solve_kernel<false><<<dim3((coff + tc - 1) / tc, nnodes), 256, smem, s>>>(
-        L, -1, tc, true, SCHUR_BIG_SD);
+        L, -1, tc, true, SCHUR_BIG_SOLVE_SD);
     ++*launches;
   }
   const int ctiles = (coff + BT - 1) / BT, cblocks = (coff + 255) / 256;

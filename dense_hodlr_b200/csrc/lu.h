@@ -52,6 +52,11 @@ int leaf_solve_launch(const LeafSolveLaunch& L, int nleaves, int smax, cudaStrea
 // blocked LU (panel, swap + triangular solve, tiled trailing update per 32
 // columns); smaller ones by one CTA each.
 constexpr int SCHUR_BIG_SD = 768;
+// The factorization's solves of the ancestor columns go blocked from this
+// size: below it one CTA per 16 columns reads the whole LU per tile (cheap
+// for small S, whose LU stays in L2), above it the blocked solve reads each
+// 32-row block of the LU once per 64 columns.
+constexpr int SCHUR_BIG_SOLVE_SD = 256;
 // sd: host array of the nodes' capacitance sizes (kb + kt), in node order.
 int schur_factor_launch(const SchurLaunch& L, int nnodes, const int* sd, cudaStream_t s);
 // Kernel launches schur_factor_launch makes for these sizes.
@@ -59,7 +64,7 @@ int schur_factor_launches(const int* sd, int nnodes);
 int schur_solve_launch(const SchurLaunch& L, int nnodes, int ncols, int max_cols, int max_sd,
                        cudaStream_t s);
 // The factorization's solves y = S^-1 Z of the `coff` ancestor columns of every
-// node (R at r_off, ld sd); nodes with sd >= SCHUR_BIG_SD by the blocked
-// solve.  sd: host array of the nodes' sizes.  *launches: kernels launched.
+// node (R at r_off, ld sd); nodes with sd >= SCHUR_BIG_SOLVE_SD by the
+// blocked solve.  sd: host array of the nodes' sizes.  *launches: kernels launched.
 int schur_solve_factor_launch(const SchurLaunch& L, int nnodes, const int* sd, int coff,
                               cudaStream_t s, int* launches);
