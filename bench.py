@@ -630,12 +630,11 @@ def run_profile_case(case):
 
 
 def run_tune(case):
-    """Sweep of the preconditioner's compression tolerance, panel precision and
-    Woodbury precision on one configuration,
-    case 'tune:<c3|c5|c2>:N[:tols[:precs[:panel bits]]]' (comma-separated
-    lists; panel bits 64 and/or 32): per (tolerance, panel bits) one
-    compression, then per precision the factorization and GMRES on the FP64
-    full-kernel residual to 1e-10.  One JSON line per combination, flushed."""
+    """Sweep of the preconditioner's compression tolerance and Woodbury
+    precision on one configuration, case 'tune:<c3|c5|c2>:N[:tols[:precs]]'
+    (comma-separated lists): per tolerance one compression, then per precision
+    the factorization and GMRES on the FP64 full-kernel residual to 1e-10.
+    One JSON line per combination, flushed."""
     import torch
     from dense_hodlr_b200 import HODLR_Matrix, KernelSpec
     parts = case.split(":")
@@ -643,7 +642,6 @@ def run_tune(case):
     n = int(parts[2])
     tols = [float(t) for t in parts[3].split(",")] if len(parts) > 3 else [1e-10, 1e-8, 1e-6, 1e-4]
     precs = parts[4].split(",") if len(parts) > 4 else ["fp64", "tf32x3", "tf32", "bf16"]
-    panels = [int(v) for v in parts[5].split(",")] if len(parts) > 5 else [64]
     if cfg == "c2":
         from dense_hodlr_b200.points import uniform_cube
         pts = uniform_cube(n, DIM, SEED)
@@ -656,10 +654,9 @@ def run_tune(case):
     b_d = torch.from_numpy(np.ascontiguousarray(b.T)).cuda()
     x_d = torch.empty_like(b_d)
     g = HODLR_Matrix(n, n, spec, pts, leaf)
-    for tol, bits in [(t, pb) for t in tols for pb in panels]:
+    for tol in tols:
         g.set_precision("fp64")
         g.set_LRTolerance(tol)
-        g.set_panel_precision(bits)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         g.storeLRinTree()
@@ -682,7 +679,7 @@ def run_tune(case):
             torch.cuda.synchronize()
             t_g = time.perf_counter() - t0
             print(json.dumps({"case": "tune", "cfg": cfg, "n": n, "aca_tol": tol,
-                              "panel_bits": bits, "precision": prec, "compress_s": t_lr,
+                              "precision": prec, "compress_s": t_lr,
                               "aca_gbs": st["bytes"] / max(st["seconds"], 1e-12) / 1e9,
                               "kmax": kmax,
                               "factor_s": t_f, "gmres_s": t_g, "gmres_iterations": int(it),

@@ -57,7 +57,6 @@ SIGNATURES = {
     "hodlr_set_capacity_hint": (_I, [_H, _PI, _I]),
     "hodlr_set_factor_in_place": (_I, [_H, _I]),
     "hodlr_set_aca_streaming": (_I, [_H, _I]),
-    "hodlr_set_panel_precision": (_I, [_H, _I]),
     "hodlr_set_wait_limit": (_I, [_H, ctypes.c_uint, _I]),
     "hodlr_get_factor_in_place": (_I, [_H, _PI]),
     "hodlr_trim_device_memory": (_I, []),

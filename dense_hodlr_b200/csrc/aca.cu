@@ -36,13 +36,9 @@
 
 namespace {
 
-// The block's W or V panel in the launch's element type.
+// The block's W or V panel in the launch's element type (FP64 panels).
 template <typename T>
-__device__ __forceinline__ T* panel_of(double* d, float* f);
-template <>
-__device__ __forceinline__ double* panel_of<double>(double* d, float*) { return d; }
-template <>
-__device__ __forceinline__ float* panel_of<float>(double*, float* f) { return f; }
+__device__ __forceinline__ T* panel_of(double* d) { return d; }
 
 struct Shared {
   double red_v[32];
@@ -541,9 +537,7 @@ __device__ double resolve_eps(Shared& sh, const AcaLaunch& L, const AcaBlock& B,
 // RING: the residual passes stream their panel slices through the bulk-copy
 // ring (group levels of an even N); the dynamic shared memory then starts
 // with the ring's TMA_RING_BYTES.
-// T: the element type of the W/V panels (double; float for the mixed form's
-// compression, whose values are rounded to FP32 when stored and read back
-// into FP64 arithmetic).
+// T: the element type of the W/V panels (double).
 template <int NT, int E, bool RING, typename T>
 __global__ void __launch_bounds__(NT, (NT == 256 ? 2 : 4)) aca_kernel(AcaLaunch L) {
   extern __shared__ __align__(128) double dyn_all[];
@@ -557,8 +551,8 @@ __global__ void __launch_bounds__(NT, (NT == 256 ? 2 : 4)) aca_kernel(AcaLaunch 
   const int tid = threadIdx.x;
   if (b >= L.nblocks) return;
   const AcaBlock B = L.blocks[b];
-  T* const BW = panel_of<T>(B.W, B.Wf);
-  T* const BV = panel_of<T>(B.V, B.Vf);
+  T* const BW = panel_of<T>(B.W);
+  T* const BV = panel_of<T>(B.V);
   const int G = L.cta_block ? B.G : L.G;
   const int g = L.cta_block ? (int)blockIdx.x - B.g0 : (int)(blockIdx.x % L.G);
   const int64_t grp0 = L.cta_block ? B.g0 : (int64_t)b * G;
@@ -893,7 +887,8 @@ static void* aca_fn_t(int nt, bool ring) {
 }
 
 static void* aca_fn(int nt, bool ring, bool f32) {
-  return f32 ? aca_fn_t<float>(nt, ring) : aca_fn_t<double>(nt, ring);
+  (void)f32;  // FP64 panels only
+  return aca_fn_t<double>(nt, ring);
 }
 
 // Dynamic shared memory above 48 KB.  The ring kernels (160+ KB per CTA)
@@ -913,8 +908,8 @@ static int set_smem(void* fn, size_t smem, bool ring) {
 }
 
 int aca_launch(const AcaLaunch& L, int nt, int kcap_max, bool cooperative, cudaStream_t s) {
-  const bool ring = L.ring != 0, f32 = L.f32 != 0;
-  if (ring && (nt != TMA_NT || (L.ld % (f32 ? 4 : 2)))) return (int)cudaErrorInvalidValue;
+  const bool ring = L.ring != 0, f32 = false;
+  if (ring && (nt != TMA_NT || (L.ld % 2))) return (int)cudaErrorInvalidValue;
   const size_t smem = aca_smem(nt, kcap_max, L.dotg != nullptr, ring, f32);
   dim3 grid(L.cta_block ? L.ncta : L.nblocks * L.G), block(nt);
   void* args[] = {(void*)&L};

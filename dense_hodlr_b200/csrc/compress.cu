@@ -4,60 +4,26 @@
 
 namespace hodlr_impl {
 
-// Grow level L to `cap` columns, keeping the first kcap ones (FP64 panels,
-// or FP32 ones for the mixed form's compression).
-template <typename T>
-static int grow_panels(hodlr_t h, T*& W, T*& V, int64_t N, int kcap, int cap) {
-  T *W2 = nullptr, *V2 = nullptr;
+// Grow level L to `cap` columns, keeping the first kcap ones.
+int grow_level(hodlr_t h, Level& L, int cap) {
+  const int64_t N = h->n;
+  double *W2 = nullptr, *V2 = nullptr;
   CK(dalloc(h, &W2, (size_t)(N * cap)));
   cudaError_t e = dalloc(h, &V2, (size_t)(N * cap));
   if (e != cudaSuccess) {
     dfree(h, W2);
     return cuda_fail(h, e, "grow_level");
   }
-  if (W && kcap > 0) {
-    CK(cudaMemcpyAsync(W2, W, sizeof(T) * N * kcap, cudaMemcpyDeviceToDevice, h->stream));
-    CK(cudaMemcpyAsync(V2, V, sizeof(T) * N * kcap, cudaMemcpyDeviceToDevice, h->stream));
+  if (L.W && L.kcap > 0) {
+    CK(cudaMemcpyAsync(W2, L.W, sizeof(double) * N * L.kcap, cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(V2, L.V, sizeof(double) * N * L.kcap, cudaMemcpyDeviceToDevice, h->stream));
   }
   CK(cudaStreamSynchronize(h->stream));
-  dfree(h, W);
-  dfree(h, V);
-  W = W2;
-  V = V2;
-  return HODLR_OK;
-}
-
-int grow_level(hodlr_t h, Level& L, int cap) {
-  const int rc = L.f32 ? grow_panels(h, L.Wf, L.Vf, h->n, L.kcap, cap)
-                       : grow_panels(h, L.W, L.V, h->n, L.kcap, cap);
-  if (rc) return rc;
+  dfree(h, L.W);
+  dfree(h, L.V);
+  L.W = W2;
+  L.V = V2;
   L.kcap = cap;
-  return HODLR_OK;
-}
-
-__global__ void widen_kernel(double* dst, const float* src, int64_t count) {
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < count;
-       e += (int64_t)gridDim.x * blockDim.x)
-    dst[e] = (double)src[e];
-}
-
-// The FP32 panels of a compressed level as FP64 panels of exactly kmax
-// columns (what the factorization reads); the FP32 ones are freed.
-int convert_level_to_fp64(hodlr_t h, Level& L) {
-  if (!L.f32) return HODLR_OK;
-  const int64_t N = h->n;
-  const int cols = std::max(1, std::min(L.kcap, L.kmax));
-  CK(dalloc(h, &L.W, (size_t)(N * cols)));
-  CK(dalloc(h, &L.V, (size_t)(N * cols)));
-  widen_kernel<<<1024, 256, 0, h->stream>>>(L.W, L.Wf, N * cols);
-  widen_kernel<<<1024, 256, 0, h->stream>>>(L.V, L.Vf, N * cols);
-  CK(cudaGetLastError());
-  h->nlaunch += 2;
-  CK(cudaStreamSynchronize(h->stream));
-  dfree(h, L.Wf);
-  dfree(h, L.Vf);
-  L.f32 = false;
-  L.kcap = cols;
   return HODLR_OK;
 }
 
@@ -66,10 +32,8 @@ void fill_block(hodlr_t h, Level& L, int q, AcaBlock& B) {
   block_geom(L, q, r0, c0, m, n);
   (void)h;
   B.st = L.d_st + q;
-  B.W = L.f32 ? nullptr : L.W + r0;
-  B.V = L.f32 ? nullptr : L.V + c0;
-  B.Wf = L.f32 ? L.Wf + r0 : nullptr;
-  B.Vf = L.f32 ? L.Vf + c0 : nullptr;
+  B.W = L.W + r0;
+  B.V = L.V + c0;
   B.cR = L.cR + r0;
   B.cC = L.cC + c0;
   B.prow = L.prow + r0;
@@ -157,12 +121,11 @@ int run_aca(hodlr_t h, std::vector<AcaBlock>& blocks, int G, int nt, int kcap_ma
   L.dotg = nullptr;
   L.dotg_stride = 0;
   L.ring = ring ? 1 : 0;
-  L.f32 = h->aca_f32 ? 1 : 0;
   L.spin_limit = h->spin_limit ? h->spin_limit : HODLR_SPIN_LIMIT;
   L.bar_extra = h->bar_unreachable ? 1u : 0u;
-  if (aca_smem_bytes(nt, kcap_max, ring, h->aca_f32) > 227 * 1024)
+  if (aca_smem_bytes(nt, kcap_max, ring, false) > 227 * 1024)
     return fail(h, HODLR_ERR_UNSUPPORTED, "block rank above the shared-memory limit of ACA");
-  if (aca_dots_global(nt, kcap_max, ring, h->aca_f32)) {
+  if (aca_dots_global(nt, kcap_max, ring, false)) {
     L.dotg_stride = (int64_t)(nt / 32) * kcap_max;
     const int64_t dneed = L.dotg_stride * ncta;
     if (dneed > h->dotg_cap) {
@@ -192,7 +155,6 @@ int run_aca(hodlr_t h, std::vector<AcaBlock>& blocks, int G, int nt, int kcap_ma
 // Allocate the per-level arrays of level L with `cap` low-rank columns.
 int init_level(hodlr_t h, Level& L, int cap) {
   const int64_t N = h->n;
-  L.f32 = h->aca_f32;
   int rc = grow_level(h, L, std::max(1, std::min(L.ub_max, cap)));
   if (rc) return rc;
   CK(dalloc(h, &L.cR, (size_t)N));
@@ -347,7 +309,7 @@ int do_compress(hodlr_t h) {
   };
   auto pred_or = [&](int l, int q) -> int64_t { return have_pred ? pred(l, q) + 1 : 1; };
   int per_sm = 0;
-  if (aca_max_coresident(256, 256, false, h->aca_f32, &per_sm))
+  if (aca_max_coresident(256, 256, false, false, &per_sm))
     return fail(h, HODLR_ERR_CUDA, "occupancy query failed");
   const int P0 = std::max(1, per_sm) * h->num_sms;
   std::vector<int> pooled_levels, group_levels;
@@ -405,12 +367,10 @@ int do_compress(hodlr_t h) {
       // least two of its one-per-SM CTAs to every block
       const int nb = L.nblocks();
       int ps = 0, ps_ring = 0;
-      if (aca_max_coresident(256, L.kcap, false, h->aca_f32, &ps) ||
-          aca_max_coresident(256, L.kcap, true, h->aca_f32, &ps_ring))
+      if (aca_max_coresident(256, L.kcap, false, false, &ps) ||
+          aca_max_coresident(256, L.kcap, true, false, &ps_ring))
         return fail(h, HODLR_ERR_CUDA, "occupancy query failed");
-      // (FP64 panels only: with FP32 panels the ring's top-level ranks ran
-      // away from the per-thread path's, so FP32 compressions stream per thread)
-      const bool ring = h->aca_ring && !h->aca_f32 && (h->n % 2 == 0) &&
+      const bool ring = h->aca_ring && (h->n % 2 == 0) &&
                         ps_ring * h->num_sms >= 2 * nb;
       if (ring) ps = ps_ring;
       // equal groups: CTAs sized by predicted work measured 2-8% slower on
@@ -439,7 +399,7 @@ int do_compress(hodlr_t h) {
   // ranks, level widths, column offsets, algorithmic bytes
   int64_t coff = 0;
   double bytes = 0;
-  const double es = h->aca_f32 ? 4.0 : 8.0;  // bytes of a panel element
+  const double es = 8.0;  // bytes of a panel element
   for (auto& L : h->lv) {
     L.kmax = 0;
     for (int q = 0; q < L.nblocks(); ++q) {
@@ -453,8 +413,6 @@ int do_compress(hodlr_t h) {
     }
     L.coff = (int)coff;
     coff += L.kmax;
-    int rc = convert_level_to_fp64(h, L);  // FP32 panels of the mixed form's compression
-    if (rc) return rc;
   }
   h->C = coff;
   h->aca_bytes = bytes;

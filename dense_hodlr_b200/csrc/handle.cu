@@ -87,9 +87,6 @@ void free_compress(hodlr_t h) {
   for (auto& L : h->lv) {
     dfree(h, L.W);
     dfree(h, L.V);
-    dfree(h, L.Wf);
-    dfree(h, L.Vf);
-    L.f32 = false;
     dfree(h, L.cR);
     dfree(h, L.cC);
     dfree(h, L.prow);

@@ -68,11 +68,6 @@ struct Level {
   int kcap = 0;
   double* W = nullptr;
   double* V = nullptr;
-  // FP32 panels of the mixed form's compression (f32): W and V are then null
-  // until the compression ends and converts them to FP64
-  float* Wf = nullptr;
-  float* Vf = nullptr;
-  bool f32 = false;
   unsigned char* cR = nullptr;
   unsigned char* cC = nullptr;
   int* prow = nullptr;
@@ -229,7 +224,6 @@ struct hodlr_handle_s {
   // one 256-thread CTA per SM it streamed slower than two CTAs of per-thread
   // loads -- 3.05 vs 3.64 TB/s on the sphere shape, N = 262144)
   bool aca_ring = false;
-  bool aca_f32 = false;  // compress into FP32 panels (hodlr_set_panel_precision)
   unsigned spin_limit = 0;       // polls of an ACA group barrier (0: HODLR_SPIN_LIMIT)
   bool bar_unreachable = false;  // ACA group barriers wait for one arrival too many
   std::vector<int> leaf_min, leaf_size;
@@ -340,7 +334,6 @@ std::vector<int4> block_geoms(hodlr_t h);
 int block_features_dev(hodlr_t h, const std::vector<int4>& geom, double l, float* d_F);
 int predict_ranks(hodlr_t h);
 int do_compress(hodlr_t h);
-int convert_level_to_fp64(hodlr_t h, Level& L);
 int upload_plan(hodlr_t h, std::vector<GemmProblem>& probs, bool split, DevPlan& out);
 int level_rank(const Level& L, int q);
 int run_tn(hodlr_t h, const DevPlan& P);

@@ -458,16 +458,6 @@ int hodlr_set_wait_limit(hodlr_t h, unsigned polls, int unreachable) {
   return HODLR_OK;
 }
 
-int hodlr_set_panel_precision(hodlr_t h, int bits) {
-  if (!h || (bits != 32 && bits != 64)) return HODLR_ERR_ARG;
-  if ((bits == 32) != h->aca_f32) {
-    CK(cudaStreamSynchronize(h->stream));
-    free_compress(h);
-    h->aca_f32 = bits == 32;
-  }
-  return HODLR_OK;
-}
-
 int hodlr_set_aca_streaming(hodlr_t h, int on) {
   if (!h || on < 0 || on > 1) return HODLR_ERR_ARG;
   h->aca_ring = on != 0;

@@ -36,10 +36,8 @@ struct AcaState;
 
 struct AcaBlock {
   AcaState* st;       // loop state of this block
-  double* W;          // FP64 panels, or (AcaLaunch::f32) null and
+  double* W;
   double* V;
-  float* Wf;          //   FP32 panels of the same layout
-  float* Vf;
   unsigned char* cR;  // chosen rows, local index
   unsigned char* cC;  // chosen columns, local index
   int* prow;          // pivot row of step t, local index
@@ -76,9 +74,7 @@ struct AcaLaunch {
   int ncta;              // CTAs of the launch when cta_block is set
   double* dotg;          // per-CTA per-warp dot partials in global memory (large ranks), or null
   int64_t dotg_stride;   // doubles per CTA in dotg (NT/32 * kcap_max)
-  int ring;              // 1: panel slices streamed by bulk copies (256 threads; ld a
-                         //    multiple of 2, or of 4 with FP32 panels)
-  int f32;               // 1: W/V panels in FP32 (AcaBlock::Wf/Vf)
+  int ring;              // 1: panel slices streamed by bulk copies (256 threads, even ld)
   unsigned spin_limit;   // polls of a group barrier before it gives up (DEV_ERR_TIMEOUT)
   unsigned bar_extra;    // arrivals a group barrier waits for beyond its G CTAs (0; 1 makes
                          // every barrier unreachable, to exercise the timeout path)

@@ -170,11 +170,6 @@ class HODLR_Matrix:
         src/HODLR_Matrix.cpp:1232-1246): the next solve recomputes both."""
         _check(self._h, _L.lib().hodlr_reset(self._h))
 
-    def set_panel_precision(self, bits):
-        """W/V panels of the compression in FP64 (64, default) or FP32 (32):
-        the mixed form's compression, for tolerances of 1e-6 or looser."""
-        _check(self._h, _L.lib().hodlr_set_panel_precision(self._h, int(bits)))
-
     def set_aca_streaming(self, on):
         """Top-level ACA panels through the bulk-copy ring (1, default) or per-thread loads (0)."""
         _check(self._h, _L.lib().hodlr_set_aca_streaming(self._h, int(bool(on))))

@@ -322,20 +322,10 @@ int hodlr_set_factor_in_place(hodlr_t h, int mode);
 
 /* How the ACA of the few-block top levels reads its W/V panel slices (no
  * counterpart in the reference): on = 1 streams them through a shared-memory
- * ring filled by bulk copies (used when N is even and the panels are
- * FP64), 0 (default, measured faster) loads them per thread.  Pivots, ranks and W/V are the same either way; the
+ * ring filled by bulk copies (used when N is even), 0 (default, measured
+ * faster) loads them per thread.  Pivots, ranks and W/V are the same either way; the
  * setting applies from the next compression. */
 int hodlr_set_aca_streaming(hodlr_t h, int on);
-
-/* Element type of the W/V panels while ACA compresses (no counterpart in the
- * reference; part of the mixed-precision form): bits = 64 (default, the
- * reference's arithmetic, bit for bit) or 32.  With 32 every new ACA column
- * is rounded to FP32 when stored and read back into FP64 arithmetic, so the
- * compression streams half the bytes; pivots then differ from the FP64
- * path's and the tolerance should be 1e-6 or looser (the stored columns
- * carry FP32 rounding, 6e-8 relative).  The compressed panels are widened
- * to FP64 for the factorization.  A change discards the compression. */
-int hodlr_set_panel_precision(hodlr_t h, int bits);
 
 /* Bounded device waits (no counterpart in the reference).  The CTAs of one
  * ACA block group meet at a barrier in global memory; a barrier that is not

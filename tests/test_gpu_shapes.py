@@ -135,46 +135,6 @@ def test_factor_in_place_matches_separate_panels(oracle_mod):
     assert np.array_equal(W0, W2) and np.array_equal(V0, V2)
 
 
-@pytest.mark.parametrize("n", [16384, 9999])
-def test_fp32_panels_compress_to_tolerance_and_precondition(oracle_mod, n):
-    """The mixed form's compression into FP32 panels (hodlr_set_panel_precision(32)),
-    tol 1e-6: every top block's W V^T within 1e-5 of the block (Frobenius,
-    relative, entries from the oracle), ranks within 10% of the FP64
-    compression's, and the factor (3xTF32 Woodbury products) as a GMRES
-    preconditioner to a 1e-10 residual with the FP64 kernel.  Block errors
-    are held to the FP64 compression's on the same block (ACA's stopping
-    test estimates, it does not bound)."""
-    pts = uniform_cube(n, 2, 29)
-    tol = 1e-6
-    ref = HODLR_Matrix(n, n, KernelSpec("matern32", 0.2, 1e-2), pts, 128)
-    ref.set_LRTolerance(tol)
-    ref.storeLRinTree()
-    g = HODLR_Matrix(n, n, KernelSpec("matern32", 0.2, 1e-2), pts, 128)
-    g.set_LRTolerance(tol)
-    g.set_panel_precision(32)
-    g.set_aca_streaming(1)  # FP32 panels stream per thread even when the ring is asked for
-    g.storeLRinTree()
-    r32, r64 = g.ranks().astype(float), ref.ranks().astype(float)
-    big = r64 >= 20
-    assert np.all(np.abs(r32[big] - r64[big]) <= 0.1 * r64[big] + 2)
-    o = oracle_mod.OracleHODLR.from_kernel(pts, 1, 0.2, shift=1e-2, leaf=128)
-    for b in range(6):
-        info = g.block_info(b)
-        m0, c0, m, nn = info["row0"], info["col0"], info["m"], info["n"]
-        rows = np.arange(m0, m0 + m)[:: max(1, m // 400)]
-        K = np.array([[o.entry(int(i), int(j)) for j in range(c0, c0 + nn)] for i in rows])
-        err = []
-        for h in (g, ref):
-            W, V = h.lowrank(b)
-            err.append(np.linalg.norm(W[rows - m0] @ V.T - K) / np.linalg.norm(K))
-        assert err[0] <= 3.0 * err[1] + 1e-6, (b, err)
-    g.set_precision("tf32x3")
-    bvec = np.random.default_rng(4).standard_normal((n, 2))
-    it, rel, x = _device_gmres(g, bvec)
-    assert rel.max() <= 1e-10
-    assert np.all(g.residual(x, bvec) <= 1e-10)
-
-
 @pytest.mark.parametrize("n,dim", [(32768, 2), (20000, 3)])
 def test_ring_streaming_bit_identical_to_per_thread_loads(n, dim):
     """The top-level ACA with its panel slices streamed through the bulk-copy
