@@ -386,7 +386,7 @@ __global__ void __launch_bounds__(SNT) schur_lu_kernel(SchurLaunch L, int pnb, i
 // A22 -= L21 U12 in 64 x 64 tiles over all SMs.  The pivot choices are the
 // column-wise first maxima, as in the one-CTA kernel.
 constexpr int BNB = 32;
-constexpr int BIG_MAX = 64;
+constexpr int BIG_MAX = 1024;  // nodes per launch (kernel parameter: 4 KB)
 struct BigNodes {
   int idx[BIG_MAX];
   int count;

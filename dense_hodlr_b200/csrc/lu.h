@@ -51,12 +51,12 @@ int leaf_solve_launch(const LeafSolveLaunch& L, int nleaves, int smax, cudaStrea
 // Capacitance matrices of at least this size are factored by the multi-CTA
 // blocked LU (panel, swap + triangular solve, tiled trailing update per 32
 // columns); smaller ones by one CTA each.
-constexpr int SCHUR_BIG_SD = 768;
+constexpr int SCHUR_BIG_SD = 384;
 // The factorization's solves of the ancestor columns go blocked from this
 // size: below it one CTA per 16 columns reads the whole LU per tile (cheap
 // for small S, whose LU stays in L2), above it the blocked solve reads each
 // 32-row block of the LU once per 64 columns.
-constexpr int SCHUR_BIG_SOLVE_SD = 256;
+constexpr int SCHUR_BIG_SOLVE_SD = 128;
 // sd: host array of the nodes' capacitance sizes (kb + kt), in node order.
 int schur_factor_launch(const SchurLaunch& L, int nnodes, const int* sd, cudaStream_t s);
 // Kernel launches schur_factor_launch makes for these sizes.

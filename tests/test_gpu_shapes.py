@@ -3,7 +3,7 @@ and for the minPivot skip-row path of ACA.
 
 * The sphere / Matern-3/2 shape (unit sphere, l = 0.1, shift 1e-2, leaf 128,
   ACA tol 1e-10): its ranks make the top capacitance matrices large enough
-  for the multi-CTA blocked LU (sd >= SCHUR_BIG_SD = 768).
+  for the multi-CTA blocked LU (sd >= SCHUR_BIG_SD = 384).
 * The cube / Gaussian shape (l = 0.3, shift 0.1, leaf 128, tol 1e-8) with 16
   right-hand sides, through HODLR-preconditioned GMRES with FP64, 3xTF32 and
   TF32 Woodbury products.
@@ -24,7 +24,7 @@ from .test_gpu_parity import SOLVE_TOL, _compare_compression, _pair
 
 pytestmark = pytest.mark.gpu
 
-BIG_SD = 768  # SCHUR_BIG_SD in csrc/lu.h
+BIG_SD = 384  # SCHUR_BIG_SD in csrc/lu.h
 
 
 def _device_gmres(g, b, tol=1e-10, max_iter=60):
