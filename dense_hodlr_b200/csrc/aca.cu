@@ -881,14 +881,16 @@ size_t aca_smem_bytes(int nt, int kcap_max, bool ring, bool f32) {
 }
 
 template <typename T>
-static void* aca_fn_t(int nt, bool ring) {
+static void* aca_fn_t(int nt, bool ring, bool narrow) {
   if (ring) return (void*)aca_kernel<TMA_NT, TMA_E, true, T>;
-  return nt == 256 ? (void*)aca_kernel<256, 4, false, T> : (void*)aca_kernel<128, 2, false, T>;
+  if (nt == 256)
+    return narrow ? (void*)aca_kernel<256, 2, false, T> : (void*)aca_kernel<256, 4, false, T>;
+  return (void*)aca_kernel<128, 2, false, T>;
 }
 
-static void* aca_fn(int nt, bool ring, bool f32) {
+static void* aca_fn(int nt, bool ring, bool f32, bool narrow = false) {
   (void)f32;  // FP64 panels only
-  return aca_fn_t<double>(nt, ring);
+  return aca_fn_t<double>(nt, ring, narrow);
 }
 
 // Dynamic shared memory above 48 KB.  The ring kernels (160+ KB per CTA)
@@ -913,7 +915,7 @@ int aca_launch(const AcaLaunch& L, int nt, int kcap_max, bool cooperative, cudaS
   const size_t smem = aca_smem(nt, kcap_max, L.dotg != nullptr, ring, f32);
   dim3 grid(L.cta_block ? L.ncta : L.nblocks * L.G), block(nt);
   void* args[] = {(void*)&L};
-  void* fn = aca_fn(nt, ring, f32);
+  void* fn = aca_fn(nt, ring, f32, L.narrow != 0);
   if (int e = set_smem(fn, smem, ring)) return e;
   cudaError_t e = cooperative ? cudaLaunchCooperativeKernel(fn, grid, block, args, smem, s)
                               : cudaLaunchKernel(fn, grid, block, args, smem, s);

@@ -121,6 +121,14 @@ int run_aca(hodlr_t h, std::vector<AcaBlock>& blocks, int G, int nt, int kcap_ma
   L.dotg = nullptr;
   L.dotg_stride = 0;
   L.ring = ring ? 1 : 0;
+  // slices of a group shorter than 768 rows: the 2-element instance (512-row
+  // chunks) leaves fewer lanes idle than the 4-element one (1024-row chunks)
+  L.narrow = 0;
+  if (!ring && nt == 256 && G > 1) {
+    int longest = 0;
+    for (auto& b : blocks) longest = std::max(longest, std::max(b.m, b.n));
+    L.narrow = (longest + G - 1) / G < 768 ? 1 : 0;
+  }
   L.spin_limit = h->spin_limit ? h->spin_limit : HODLR_SPIN_LIMIT;
   L.bar_extra = h->bar_unreachable ? 1u : 0u;
   if (aca_smem_bytes(nt, kcap_max, ring, false) > 227 * 1024)
