@@ -284,26 +284,27 @@ __device__ void residual_pass(const AcaLaunch& L, const AcaBlock& B, T* P, int l
   }
 }
 
-// ---------------------------------------------------------------- bulk-copy ring
-// The group levels stream their panel slices through shared memory: a ring
-// of TMA_S tiles, each TMA_BC panel columns x TMA_BR rows, filled by
-// cp.async.bulk copies (one per column) that complete on the tile's `full`
-// mbarrier; every warp releases a tile on its `empty` mbarrier and thread 0
-// then refills it with the tile TMA_S ahead.  Rows start on an even global
-// index so that every copy is 16-byte aligned (requires an even N).
-constexpr int TMA_BC = 4;
-constexpr int TMA_S = 4;
-// two elements per thread: 512-row chunks, so that the ring (64 KB for FP64,
-// 32 KB for FP32) and 128 registers per thread leave room for two CTAs per SM
-constexpr int TMA_NT = 256, TMA_E = 2, TMA_BR = TMA_NT * TMA_E;
-// ring bytes for panel elements of `es` bytes
-constexpr size_t tma_ring_bytes(size_t es) { return es * TMA_S * TMA_BC * TMA_BR; }
+// ---------------------------------------------------------------- bulk-copy rings
+// With streaming on, the group levels run 16 warps per CTA, and every warp
+// streams its own contiguous part of the CTA's slice through a private ring
+// of WR_S stages in shared memory, each WR_BC panel columns x WR_ROWS rows,
+// filled by cp.async.bulk copies (one per column) that complete on the
+// stage's mbarrier.  Lane 0 refills a stage as soon as its own warp is done
+// with it: no warp waits for another.  Rows start on an even global index so
+// that every copy is 16-byte aligned (requires an even N).
+constexpr int WR_NT = 512, WR_E = 4, WR_ROWS = 32 * WR_E;
+constexpr int WR_BC = 4, WR_SMAX = 3;
+constexpr int WR_NW = WR_NT / 32;
+// ring bytes of one CTA with `stages` stages (192 KB with 3)
+constexpr size_t wring_bytes(int stages) {
+  return sizeof(double) * (size_t)WR_NW * stages * WR_BC * WR_ROWS;
+}
 
-struct Ring {
-  void* buf;        // TMA_S tiles of TMA_BC x TMA_BR panel elements, column u at u * TMA_BR
-  uint64_t* full;   // per tile: its copies landed (1 arrival + transaction bytes)
-  uint64_t* empty;  // per tile: every warp is done with it (NT / 32 arrivals)
-  uint32_t t;       // tiles this CTA has consumed (the same in every thread)
+struct WRing {
+  double* buf;      // [warp][stage][column u][row], WR_ROWS rows per column
+  uint64_t* full;   // [warp][stage]: the stage's copies landed (1 arrival + bytes)
+  int stages;
+  uint32_t t;       // tiles this warp has consumed (the same in all its lanes)
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
@@ -336,90 +337,92 @@ __device__ void mbar_wait_bounded(uint64_t* bar, uint32_t parity, unsigned* err)
   }
 }
 
-// Thread 0: tile gt of the ring, `nc` columns from column l0 of P, `count`
-// rows from row0 (count and row0's global index multiples of 16 / sizeof(T)).
-template <typename T>
-__device__ void ring_issue(Ring& R, uint32_t gt, const T* P, int64_t ld, int row0, int count,
-                           int l0, int nc, unsigned* err) {
-  const int slot = (int)(gt % TMA_S);
-  if (gt >= (uint32_t)TMA_S) mbar_wait_bounded(&R.empty[slot], ((gt / TMA_S) + 1) & 1, err);
-  const uint32_t bytes = (uint32_t)count * (uint32_t)sizeof(T);
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
-                   smem_addr(&R.full[slot])),
+// Lane 0: this warp's tile number tw into its stage tw % stages -- `nc`
+// columns from l0 of P, `count` rows from row0 (count even, row0 on an even
+// global row).  The stage was last read by this warp before a __syncwarp;
+// the proxy fence orders those reads before the copies overwrite it.
+__device__ void wring_issue(WRing& R, int w, uint32_t tw, const double* P, int64_t ld, int row0,
+                            int count, int l0, int nc) {
+  const int slot = (int)(tw % (uint32_t)R.stages);
+  uint64_t* bar = R.full + w * WR_SMAX + slot;
+  const uint32_t bytes = (uint32_t)count * (uint32_t)sizeof(double);
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
                "r"(bytes * (uint32_t)nc)
                : "memory");
-  T* dst = static_cast<T*>(R.buf) + (size_t)slot * TMA_BC * TMA_BR;
+  double* dst = R.buf + ((size_t)(w * WR_SMAX + slot) * WR_BC) * WR_ROWS;
   for (int u = 0; u < nc; ++u)
     asm volatile(
         "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
-            "r"(smem_addr(dst + u * TMA_BR)),
-        "l"(P + row0 + (int64_t)(l0 + u) * ld), "r"(bytes), "r"(smem_addr(&R.full[slot]))
+            "r"(smem_addr(dst + u * WR_ROWS)),
+        "l"(P + row0 + (int64_t)(l0 + u) * ld), "r"(bytes), "r"(smem_addr(bar))
         : "memory");
 }
 
-// residual_pass with the panel slice streamed through the ring.  gbase: the
-// global row of P[0] (the block's first column for V, first row for W).
-// The same arithmetic as residual_pass, element for element: the residual
-// sums in l order with separately rounded products and sums, the argmax in
-// increasing index per thread; the fused dots add their chunk partials in a
-// GPU order, as there.
-template <int NT, int E, bool ROW, typename T>
-__device__ void residual_pass_ring(const AcaLaunch& L, const AcaBlock& B, T* P, int lo,
-                                   int hi, int k, const double* __restrict__ coef, bool dots,
-                                   double* __restrict__ dotw, int ldd, int fixed,
-                                   const double* xfix, double scale, const unsigned char* chosen,
-                                   double& bv, int& bi, int& cand, double& sq, bool& nonfinite,
-                                   const EntrySrc& S, Ring& R, int gbase) {
-  static_assert(NT * E == TMA_BR, "one chunk is one ring tile high");
-  if (lo >= hi) return;
+// residual_pass with every warp streaming its own rows through its ring.
+// gbase: the global row of P[0] (the block's first column for V, first row
+// for W).  The same arithmetic as residual_pass, element for element: the
+// residual sums in l order with separately rounded products and sums, the
+// argmax in increasing index per thread; the fused dots add their partials
+// in a GPU order, as there.
+template <int NT, int E, bool ROW>
+__device__ void residual_pass_wring(const AcaLaunch& L, const AcaBlock& B, double* P, int lo,
+                                    int hi, int k, const double* __restrict__ coef, bool dots,
+                                    double* __restrict__ dotw, int ldd, int fixed,
+                                    const double* xfix, double scale, const unsigned char* chosen,
+                                    double& bv, int& bi, int& cand, double& sq, bool& nonfinite,
+                                    const EntrySrc& S, WRing& R, int gbase) {
+  static_assert(NT == WR_NT && E == WR_E, "the warp ring's geometry");
+  constexpr int NW = NT / 32;
   const int64_t ld = L.ld;
   const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
   const double minPiv = L.minPivot;
-  constexpr int A = 16 / (int)sizeof(T);  // elements per 16 bytes: copy alignment
-  const int x0 = lo - ((gbase + lo) & (A - 1));  // first chunk row: aligned global index
-  const int nchunks = (hi - x0 + TMA_BR - 1) / TMA_BR;
-  const int tpc = (k + TMA_BC - 1) / TMA_BC;  // tiles per chunk
-  const uint32_t ntiles = (uint32_t)nchunks * (uint32_t)tpc;
   const int kd = dots ? k - 1 : 0;
-  auto issue = [&](uint32_t i) {
-    const int c = (int)(i / tpc), l0 = (int)(i % tpc) * TMA_BC;
-    const int row0 = x0 + c * TMA_BR;
-    const int count = (min(TMA_BR, hi - row0) + A - 1) & ~(A - 1);
-    ring_issue(R, R.t + i, P, ld, row0, count, l0, min(TMA_BC, k - l0), L.err);
-  };
-  if (tid == 0 && ntiles > 0) {
-    // this CTA's earlier generic stores to the panel (after the caller's
-    // __syncthreads) before the bulk copies read it
-    asm volatile("fence.proxy.async.global;" ::: "memory");
-    for (uint32_t i = 0; i < ntiles && i < (uint32_t)TMA_S; ++i) issue(i);
+  // this warp's rows: an even-sized share of the slice from an even global row
+  const int x0 = lo - ((gbase + lo) & 1);
+  int rw = (hi - x0 + NW - 1) / NW;
+  rw = (rw + 1) & ~1;
+  const int wlo = x0 + w * rw, whi = min(hi, wlo + rw);
+  if (lo >= hi || wlo >= whi) {  // no rows: zero partial dots from this warp
+    if (dots)
+      for (int l = lane; l < kd; l += 32) dotw[w * ldd + l] = 0.0;
+    return;
   }
-  uint32_t i = 0;
-  for (int c = 0; c < nchunks; ++c) {
-    const int jb = x0 + c * TMA_BR;
+  const int tpc = (k + WR_BC - 1) / WR_BC;  // tiles per chunk
+  if (lane == 0) {
+    // this warp's earlier generic stores to these rows, then the copies
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+  }
+  bool first = true;
+  for (int jb = wlo; jb < whi; jb += WR_ROWS, first = false) {
+    const int count = (min(WR_ROWS, whi - jb) + 1) & ~1;
+    if (lane == 0)
+      for (int q = 0; q < tpc && q < R.stages; ++q)
+        wring_issue(R, w, R.t + q, P, ld, jb, count, q * WR_BC, min(WR_BC, k - q * WR_BC));
     int jj[E];
     bool ok[E];
     double s[E], vp[E];
 #pragma unroll
     for (int e = 0; e < E; ++e) {
-      jj[e] = jb + tid + e * NT;
-      ok[e] = jj[e] >= lo && jj[e] < hi;
+      jj[e] = jb + lane + 32 * e;
+      ok[e] = jj[e] >= lo && jj[e] < whi;
       s[e] = 0.0;
-      vp[e] = (dots && ok[e]) ? (double)P[jj[e] + (int64_t)(k - 1) * ld] : 0.0;
+      vp[e] = (dots && ok[e]) ? P[jj[e] + (int64_t)(k - 1) * ld] : 0.0;
     }
-    for (int l0 = 0; l0 < k; l0 += TMA_BC, ++i) {
-      const uint32_t gt = R.t + i;
-      const int slot = (int)(gt % TMA_S);
-      mbar_wait_bounded(&R.full[slot], (gt / TMA_S) & 1, L.err);
-      const T* tile = static_cast<const T*>(R.buf) + (size_t)slot * TMA_BC * TMA_BR;
-      const int nc = min(TMA_BC, k - l0);
-      double v[TMA_BC][E];
+    for (int q = 0; q < tpc; ++q) {
+      const uint32_t tw = R.t + q;
+      const int slot = (int)(tw % (uint32_t)R.stages);
+      mbar_wait_bounded(R.full + w * WR_SMAX + slot, (tw / (uint32_t)R.stages) & 1, L.err);
+      const double* tile = R.buf + ((size_t)(w * WR_SMAX + slot) * WR_BC) * WR_ROWS;
+      const int l0 = q * WR_BC, nc = min(WR_BC, k - l0);
+      double v[WR_BC][E];
 #pragma unroll
-      for (int u = 0; u < TMA_BC; ++u)
+      for (int u = 0; u < WR_BC; ++u)
 #pragma unroll
         for (int e = 0; e < E; ++e)
-          v[u][e] = (u < nc && ok[e]) ? (double)tile[u * TMA_BR + tid + e * NT] : 0.0;
+          v[u][e] = (u < nc && ok[e]) ? tile[u * WR_ROWS + lane + 32 * e] : 0.0;
 #pragma unroll
-      for (int u = 0; u < TMA_BC; ++u) {
+      for (int u = 0; u < WR_BC; ++u) {
         if (u >= nc) break;
         const double cf = coef[l0 + u];
 #pragma unroll
@@ -430,21 +433,19 @@ __device__ void residual_pass_ring(const AcaLaunch& L, const AcaBlock& B, T* P, 
         // reduction: after the exchanges at offsets 16 and 8, lane group
         // q = lane / 8 holds partial sums of column q, then each group of 8
         // lanes sums its own (6 shuffles instead of 4 x 5)
-        static_assert(TMA_BC == 4, "transposed reduction of four columns");
-        double d[TMA_BC];
+        static_assert(WR_BC == 4, "transposed reduction of four columns");
+        double d[WR_BC];
 #pragma unroll
-        for (int u = 0; u < TMA_BC; ++u) {
+        for (int u = 0; u < WR_BC; ++u) {
           d[u] = 0.0;
 #pragma unroll
           for (int e = 0; e < E; ++e) d[u] = fma(v[u][e], vp[e], d[u]);
         }
         const bool hi16 = (lane & 16) != 0, hi8 = (lane & 8) != 0;
-        // offset 16: lanes < 16 keep columns 0, 1; lanes >= 16 keep 2, 3
         const double s0 = __shfl_xor_sync(0xffffffffu, hi16 ? d[0] : d[2], 16);
         const double s1 = __shfl_xor_sync(0xffffffffu, hi16 ? d[1] : d[3], 16);
         const double p0 = (hi16 ? d[2] : d[0]) + s0;
         const double p1 = (hi16 ? d[3] : d[1]) + s1;
-        // offset 8: lanes with bit 3 clear keep the first of the pair
         const double s2 = __shfl_xor_sync(0xffffffffu, hi8 ? p0 : p1, 8);
         double t = (hi8 ? p1 : p0) + s2;
         t += __shfl_xor_sync(0xffffffffu, t, 4);
@@ -452,18 +453,18 @@ __device__ void residual_pass_ring(const AcaLaunch& L, const AcaBlock& B, T* P, 
         t += __shfl_xor_sync(0xffffffffu, t, 1);
         const int u = (hi16 ? 2 : 0) + (hi8 ? 1 : 0);  // the column this lane group summed
         if ((lane & 7) == 0 && l0 + u < kd) {
-          if (c == 0)
+          if (first)
             dotw[w * ldd + l0 + u] = t;
           else
             dotw[w * ldd + l0 + u] += t;
         }
       }
       __syncwarp();
-      if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(
-                                      smem_addr(&R.empty[slot]))
-                                  : "memory");
-      if (tid == 0 && i + TMA_S < ntiles) issue(i + TMA_S);
+      if (lane == 0 && q + R.stages < tpc)
+        wring_issue(R, w, tw + R.stages, P, ld, jb, count, (q + R.stages) * WR_BC,
+                    min(WR_BC, k - (q + R.stages) * WR_BC));
     }
+    R.t += tpc;
 #pragma unroll
     for (int e = 0; e < E; ++e) {
       if (!ok[e]) continue;
@@ -471,11 +472,8 @@ __device__ void residual_pass_ring(const AcaLaunch& L, const AcaBlock& B, T* P, 
       double ent = ROW ? src_entry_xi(S, xfix, fixed, B.c0 + j)
                        : src_entry_xj(S, xfix, B.r0 + j, fixed);
       double r = __dsub_rn(ent, s[e]);
-      // the panel keeps the value rounded to its type (no rounding for FP64),
-      // and the norms of the stopping test use what it keeps
-      const T kept = (T)(ROW ? r : __dmul_rn(scale, r));
-      const double stored = (double)kept;
-      P[j + (int64_t)k * ld] = kept;
+      const double stored = ROW ? r : __dmul_rn(scale, r);
+      P[j + (int64_t)k * ld] = stored;
       sq = fma(stored, stored, sq);
       double a = fabs(r);
       nonfinite |= !isfinite(r);
@@ -486,7 +484,6 @@ __device__ void residual_pass_ring(const AcaLaunch& L, const AcaBlock& B, T* P, 
       if (cand == INT_MAX && a > minPiv && __ldcg(chosen + j) == 0) cand = j;
     }
   }
-  R.t += ntiles;
 }
 
 // Partial dots of step k-1 over this CTA's slices when they could not be
@@ -534,16 +531,16 @@ __device__ double resolve_eps(Shared& sh, const AcaLaunch& L, const AcaBlock& B,
   return sqrt(swp) * sqrt(svp) / sqrt(frob2);
 }
 
-// RING: the residual passes stream their panel slices through the bulk-copy
-// ring (group levels of an even N); the dynamic shared memory then starts
-// with the ring's TMA_RING_BYTES.
+// RING: the residual passes stream their panel slices through the warps'
+// bulk-copy rings (group levels of an even N, 512 threads); the dynamic
+// shared memory then starts with the rings' wring_bytes(L.ring_stages).
 // T: the element type of the W/V panels (double).
 template <int NT, int E, bool RING, typename T>
-__global__ void __launch_bounds__(NT, (NT == 256 ? 2 : 4)) aca_kernel(AcaLaunch L) {
+__global__ void __launch_bounds__(NT, (NT == 512 ? 1 : NT == 256 ? 2 : 4)) aca_kernel(AcaLaunch L) {
   extern __shared__ __align__(128) double dyn_all[];
   __shared__ Shared sh;
-  __shared__ __align__(8) uint64_t ring_full[TMA_S], ring_empty[TMA_S];
-  double* dyn = RING ? dyn_all + tma_ring_bytes(sizeof(T)) / sizeof(double) : dyn_all;
+  __shared__ __align__(8) uint64_t ring_full[RING ? WR_NW * WR_SMAX : 1];
+  double* dyn = RING ? dyn_all + wring_bytes(L.ring_stages) / sizeof(double) : dyn_all;
   // dyn: row[kcap], then (unless L.dotg) per-warp dots[NT/32][kcap]
   constexpr int NW = NT / 32;
   const int b = L.cta_block ? (blockIdx.x < (unsigned)L.ncta ? L.cta_block[blockIdx.x] : L.nblocks)
@@ -582,14 +579,11 @@ __global__ void __launch_bounds__(NT, (NT == 256 ? 2 : 4)) aca_kernel(AcaLaunch 
   double swp = st->swp, svp = st->svp;
   int near = st->near, pending = st->pending;
   bool nonfinite = false;
-  Ring ring{dyn_all, ring_full, ring_empty, 0};
+  WRing ring{dyn_all, ring_full, L.ring_stages, 0};
   if (RING) {
     if (tid == 0) {
-      for (int q = 0; q < TMA_S; ++q) {
+      for (int q = 0; q < WR_NW * WR_SMAX; ++q)
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&ring_full[q])));
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&ring_empty[q])),
-                     "r"(NT / 32));
-      }
       asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
@@ -645,8 +639,8 @@ __global__ void __launch_bounds__(NT, (NT == 256 ? 2 : 4)) aca_kernel(AcaLaunch 
     double bv = -1.0, sv = 0.0;
     int bi = INT_MAX, cand = INT_MAX;
     if constexpr (RING)
-      residual_pass_ring<NT, E, true>(L, B, BV, j_lo, j_hi, k, row, fuse, dotw, ldd, gi, xi, 1.0,
-                                      B.cC, bv, bi, cand, sv, nonfinite, S, ring, B.c0);
+      residual_pass_wring<NT, E, true>(L, B, BV, j_lo, j_hi, k, row, fuse, dotw, ldd, gi, xi,
+                                       1.0, B.cC, bv, bi, cand, sv, nonfinite, S, ring, B.c0);
     else
       residual_pass<NT, E, true>(L, B, BV, j_lo, j_hi, k, row, fuse, dotw, ldd, gi, xi, 1.0,
                                  B.cC, bv, bi, cand, sv, nonfinite, S);
@@ -723,8 +717,8 @@ __global__ void __launch_bounds__(NT, (NT == 256 ? 2 : 4)) aca_kernel(AcaLaunch 
     cand = INT_MAX;
     double sw = 0.0;
     if constexpr (RING)
-      residual_pass_ring<NT, E, false>(L, B, BW, i_lo, i_hi, k, row, fuse, dotw, ldd, gj, xj,
-                                       piv, B.cR, bv, bi, cand, sw, nonfinite, S, ring, B.r0);
+      residual_pass_wring<NT, E, false>(L, B, BW, i_lo, i_hi, k, row, fuse, dotw, ldd, gj, xj,
+                                        piv, B.cR, bv, bi, cand, sw, nonfinite, S, ring, B.r0);
     else
       residual_pass<NT, E, false>(L, B, BW, i_lo, i_hi, k, row, fuse, dotw, ldd, gj, xj, piv,
                                   B.cR, bv, bi, cand, sw, nonfinite, S);
@@ -864,16 +858,25 @@ __global__ void __launch_bounds__(NT, (NT == 256 ? 2 : 4)) aca_kernel(AcaLaunch 
 
 }  // namespace
 
+// Stages of the warp rings that fit beside kcap_max row coefficients (the
+// ring's dots are always in global memory): 3, 2, or 0 (no ring).
+int aca_ring_stages(int kcap_max) {
+  for (int st = WR_SMAX; st >= 2; --st)
+    if (wring_bytes(st) + sizeof(double) * (size_t)kcap_max <= 224 * 1024) return st;
+  return 0;
+}
+
 static size_t aca_smem(int nt, int kcap_max, bool global_dots, bool ring, bool f32) {
-  return (ring ? tma_ring_bytes(f32 ? sizeof(float) : sizeof(double)) : 0) +
+  (void)f32;
+  return (ring ? wring_bytes(aca_ring_stages(kcap_max)) : 0) +
          sizeof(double) * (size_t)(global_dots ? 1 : 1 + nt / 32) * (size_t)kcap_max;
 }
 
 // The per-warp dot partials move to global memory once the CTA's shared
-// memory would pass 100 KB (110 KB with the ring): beyond that fewer than two
-// 256-thread CTAs fit on an SM.
+// memory would pass 100 KB (beyond that fewer than two 256-thread CTAs fit on
+// an SM), and always with the warp rings (their stages fill shared memory).
 bool aca_dots_global(int nt, int kcap_max, bool ring, bool f32) {
-  return aca_smem(nt, kcap_max, false, ring, f32) > (ring ? 110 : 100) * 1024;
+  return ring || aca_smem(nt, kcap_max, false, false, f32) > 100 * 1024;
 }
 
 size_t aca_smem_bytes(int nt, int kcap_max, bool ring, bool f32) {
@@ -882,7 +885,7 @@ size_t aca_smem_bytes(int nt, int kcap_max, bool ring, bool f32) {
 
 template <typename T>
 static void* aca_fn_t(int nt, bool ring, bool narrow) {
-  if (ring) return (void*)aca_kernel<TMA_NT, TMA_E, true, T>;
+  if (ring) return (void*)aca_kernel<WR_NT, WR_E, true, T>;
   if (nt == 256)
     return narrow ? (void*)aca_kernel<256, 2, false, T> : (void*)aca_kernel<256, 4, false, T>;
   return (void*)aca_kernel<128, 2, false, T>;
@@ -911,7 +914,9 @@ static int set_smem(void* fn, size_t smem, bool ring) {
 
 int aca_launch(const AcaLaunch& L, int nt, int kcap_max, bool cooperative, cudaStream_t s) {
   const bool ring = L.ring != 0, f32 = false;
-  if (ring && (nt != TMA_NT || (L.ld % 2))) return (int)cudaErrorInvalidValue;
+  if (ring && (nt != WR_NT || (L.ld % 2) || L.ring_stages != aca_ring_stages(kcap_max) ||
+               L.ring_stages < 2))
+    return (int)cudaErrorInvalidValue;
   const size_t smem = aca_smem(nt, kcap_max, L.dotg != nullptr, ring, f32);
   dim3 grid(L.cta_block ? L.ncta : L.nblocks * L.G), block(nt);
   void* args[] = {(void*)&L};

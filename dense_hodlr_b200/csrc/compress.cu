@@ -121,6 +121,7 @@ int run_aca(hodlr_t h, std::vector<AcaBlock>& blocks, int G, int nt, int kcap_ma
   L.dotg = nullptr;
   L.dotg_stride = 0;
   L.ring = ring ? 1 : 0;
+  L.ring_stages = ring ? aca_ring_stages(kcap_max) : 0;
   // slices of a group shorter than 768 rows: the 2-element instance (512-row
   // chunks) leaves fewer lanes idle than the 4-element one (1024-row chunks)
   L.narrow = 0;
@@ -375,10 +376,11 @@ int do_compress(hodlr_t h) {
       // least two of its one-per-SM CTAs to every block
       const int nb = L.nblocks();
       int ps = 0, ps_ring = 0;
+      const bool ring_fits = aca_ring_stages(L.kcap) >= 2;
       if (aca_max_coresident(256, L.kcap, false, false, &ps) ||
-          aca_max_coresident(256, L.kcap, true, false, &ps_ring))
+          (ring_fits && aca_max_coresident(512, L.kcap, true, false, &ps_ring)))
         return fail(h, HODLR_ERR_CUDA, "occupancy query failed");
-      const bool ring = h->aca_ring && (h->n % 2 == 0) &&
+      const bool ring = h->aca_ring && ring_fits && (h->n % 2 == 0) &&
                         ps_ring * h->num_sms >= 2 * nb;
       if (ring) ps = ps_ring;
       // equal groups: CTAs sized by predicted work measured 2-8% slower on
@@ -389,7 +391,7 @@ int do_compress(hodlr_t h) {
       for (;;) {  // a cooperative launch the driver refuses is retried with half the groups
         L.G = G;
         for (int q = 0; q < nb; ++q) fill_block(h, L, q, bl[q]);
-        rc = run_aca(h, bl, G, G > 1 || ring ? 256 : 128, L.kcap, ring);
+        rc = run_aca(h, bl, G, ring ? 512 : G > 1 ? 256 : 128, L.kcap, ring);
         if (rc != HODLR_ERR_RETRY_SMALLER) break;
         if (G == 1) return fail(h, HODLR_ERR_CUDA, "aca_launch: cooperative launch refused");
         G = std::max(1, G / 2);

@@ -47,6 +47,7 @@ int aca_launch(const AcaLaunch& L, int nt, int kcap_max, bool cooperative, cudaS
 int aca_max_coresident(int nt, int kcap_max, bool ring, bool f32, int* per_sm);
 bool aca_dots_global(int nt, int kcap_max, bool ring, bool f32);
 size_t aca_smem_bytes(int nt, int kcap_max, bool ring, bool f32);
+int aca_ring_stages(int kcap_max);
 
 namespace hodlr_impl {
 

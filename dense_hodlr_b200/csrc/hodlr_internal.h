@@ -74,7 +74,9 @@ struct AcaLaunch {
   int ncta;              // CTAs of the launch when cta_block is set
   double* dotg;          // per-CTA per-warp dot partials in global memory (large ranks), or null
   int64_t dotg_stride;   // doubles per CTA in dotg (NT/32 * kcap_max)
-  int ring;              // 1: panel slices streamed by bulk copies (256 threads, even ld)
+  int ring;              // 1: panel slices streamed by per-warp bulk-copy rings (512
+                         //    threads, even ld)
+  int ring_stages;       // stages of each warp's ring (aca_ring_stages(kcap_max))
   int narrow;            // 1 (256 threads, no ring): 2 elements per thread, 512-row chunks
   unsigned spin_limit;   // polls of a group barrier before it gives up (DEV_ERR_TIMEOUT)
   unsigned bar_extra;    // arrivals a group barrier waits for beyond its G CTAs (0; 1 makes
