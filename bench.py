@@ -243,12 +243,12 @@ def run_ours(args, rank, world, local_rank):
     b_d = torch.from_numpy(np.ascontiguousarray(b.T)).to(dev)  # column-major N x NRHS
     x_d = torch.empty_like(b_d)
 
-    def step():
+    def step(max_iter=MAX_IR):
         assert lib.hodlr_reset(g._h) == 0
         g.storeLRinTree()
         g.recLU_Compute()
         return g.iterative_solve_device(b_d.data_ptr(), x_d.data_ptr(), NRHS, tol=RES_TOL,
-                                        max_iter=MAX_IR, restart=32)
+                                        max_iter=max_iter, restart=32)
 
     def launches():
         c = ctypes.c_longlong()
@@ -287,6 +287,22 @@ def run_ours(args, rank, world, local_rank):
     ms_max = slowest_rank(ms, world, dev)
     clocks = clk.summary()
 
+    # end to end through the C ABI with host buffers: create (points H2D),
+    # compress, factor, solve + refine (b H2D, x D2H), destroy
+    x_host = np.zeros_like(b, order="F")
+    e2e_times = []
+    for it in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        g2 = HODLR_Matrix(N_PTS, N_PTS, spec, pts, LEAF)
+        g2.set_LRTolerance(TOL)
+        x_host = g2.iterative_Solve(b, MAX_IR, RES_TOL)
+        del g2
+        torch.cuda.synchronize()
+        if it >= args.warmup:
+            e2e_times.append(time.perf_counter() - t0)
+    e2e_s = slowest_rank(float(np.mean(e2e_times)), world, dev)
+
     # mixed precision (3xTF32 tensor-core Woodbury products, FP64 leaf and
     # capacitance LUs and residual) to the same accuracy.  TF32 and BF16
     # factors stop being preconditioners at this shift (cond(K) * u > 1).
@@ -294,7 +310,7 @@ def run_ours(args, rank, world, local_rank):
     if not args.no_mixed:
         g.set_precision("tf32x3")
         for _ in range(1):
-            step()
+            step(MIXED_C2_MAX_ITER)
         torch.cuda.synchronize()
         m0 = torch.cuda.Event(enable_timing=True)
         m1 = torch.cuda.Event(enable_timing=True)
@@ -302,7 +318,7 @@ def run_ours(args, rank, world, local_rank):
         m_steps = 5
         m0.record(stream)
         for _ in range(m_steps):
-            it, rel = step()
+            it, rel = step(MIXED_C2_MAX_ITER)
             m_it.append(it)
             m_rel.append(float(rel.max()))
         m1.record(stream)
@@ -310,6 +326,7 @@ def run_ours(args, rank, world, local_rank):
         m_ms = m0.elapsed_time(m1) / m_steps
         mixed = {"precision": "tf32x3", "ms_per_step": m_ms, "steps": m_steps,
                  "gmres_iterations": int(max(m_it)), "rel_residual": max(m_rel),
+                 "converged": bool(max(m_rel) <= RES_TOL),
                  "factor_s": g.get_recLU_FactorizationTime(),
                  "speedup_vs_fp64": ms_max / m_ms,
                  "note": ("TF32 and BF16 Woodbury products diverge on this system "
@@ -341,22 +358,6 @@ def run_ours(args, rank, world, local_rank):
     k1.record(stream)
     torch.cuda.synchronize()
     t_kmatvec = k0.elapsed_time(k1) / 1000.0
-
-    # end to end through the C ABI with host buffers: create (points H2D),
-    # compress, factor, solve + refine (b H2D, x D2H), destroy
-    x_host = np.zeros_like(b, order="F")
-    e2e_times = []
-    for it in range(args.warmup + args.steps):
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        g2 = HODLR_Matrix(N_PTS, N_PTS, spec, pts, LEAF)
-        g2.set_LRTolerance(TOL)
-        x_host = g2.iterative_Solve(b, MAX_IR, RES_TOL)
-        del g2
-        torch.cuda.synchronize()
-        if it >= args.warmup:
-            e2e_times.append(time.perf_counter() - t0)
-    e2e_s = slowest_rank(float(np.mean(e2e_times)), world, dev)
 
     # accuracy (outside the timed region): full-kernel FP64 residual
     relres = g.residual(x_host, b)
@@ -473,6 +474,7 @@ def run_ours(args, rank, world, local_rank):
 # MIXED_MAX_ITER iterations, beyond which it is reported as not converged.
 SCALE_PAIRS = (("sphere_matern", "c5", 262144), ("cube_gaussian", "c3", 1 << 20))
 MIXED_PREC, MIXED_MAX_ITER = "tf32x3", 8
+MIXED_C2_MAX_ITER = 30  # 3xTF32 on the headline workload converges in a few iterations
 
 
 def run_scale_pair(stream, cfg_name, n):

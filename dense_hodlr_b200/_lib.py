@@ -15,11 +15,15 @@ ERR_STATE = 6
 ERR_NONFINITE = 7
 ERR_TIMEOUT = 8
 ERR_IO = 9
+ERR_CHECK = 10
+FORM_RECLU = 0
+FORM_RECSM = 1
 
 _STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "device memory exhausted",
            4: "unsupported on the GPU path", 5: "exact-zero pivot", 6: "call out of order",
            7: "non-finite value", 8: "device wait timed out",
-           9: "file could not be read or written"}
+           9: "file could not be read or written",
+           10: "check failed: an extent or index outside its buffer"}
 
 
 def status_string(s):
@@ -58,6 +62,9 @@ SIGNATURES = {
     "hodlr_set_factor_in_place": (_I, [_H, _I]),
     "hodlr_set_aca_streaming": (_I, [_H, _I]),
     "hodlr_set_wait_limit": (_I, [_H, ctypes.c_uint, _I]),
+    "hodlr_set_checked": (_I, [_H, _I]),
+    "hodlr_set_solver_form": (_I, [_H, _I]),
+    "hodlr_get_solver_form": (_I, [_H, ctypes.POINTER(ctypes.c_int)]),
     "hodlr_get_factor_in_place": (_I, [_H, _PI]),
     "hodlr_trim_device_memory": (_I, []),
     "hodlr_create_forest": (_I, [ctypes.POINTER(_H), _I, _PI, _I, _PD, ctypes.POINTER(KernelDesc),

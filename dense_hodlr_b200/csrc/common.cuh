@@ -28,6 +28,12 @@ enum {
   DEV_ERR_TIMEOUT = 1,      // a bounded spin wait gave up
   DEV_ERR_NONFINITE = 2,    // a NaN/Inf entry or residual was produced
   DEV_ERR_SINGULAR = 4,     // an exact-zero LU pivot
+  DEV_ERR_INDEX = 8,        // a pivot / permutation index outside its range (access skipped)
+  // where DEV_ERR_INDEX was raised
+  DEV_ERR_AT_LEAF_PERM = 16,     // leaf solve: row permutation
+  DEV_ERR_AT_SOLVE_PIV = 32,     // capacitance solve (one CTA per column tile): interchanges
+  DEV_ERR_AT_BLOCKED_PIV = 64,   // blocked ancestor-column solve: interchanges
+  DEV_ERR_AT_LU_SWAP = 128,      // multi-CTA LU: interchanges outside the panel
 };
 
 // The entry source for blocks of the system that holds point i: in a forest

@@ -5,7 +5,9 @@
 
 namespace hodlr_impl {
 
-int upload_plan(hodlr_t h, std::vector<GemmProblem>& probs, bool split, DevPlan& out) {
+// split: TN problems (C = A^T B), which may be split along K; else NN.
+int upload_plan(hodlr_t h, std::vector<GemmProblem>& probs, bool split, DevPlan& out,
+                const char* what) {
   std::vector<int4> tiles;
   int64_t ws = 0;
   if (h->gemm_prec == HODLR_GEMM_FP64)
@@ -26,7 +28,9 @@ int upload_plan(hodlr_t h, std::vector<GemmProblem>& probs, bool split, DevPlan&
     CK(dalloc(h, &out.tiles, (size_t)out.ntiles));
     CK(h2d(h, out.tiles, tiles.data(), sizeof(int4) * out.ntiles));
   }
-  return ensure_ws(h, ws);
+  int rc = ensure_ws(h, ws);
+  if (rc) return rc;
+  return check_gemm(h, probs, split, what);
 }
 
 int level_rank(const Level& L, int q) { return L.st[q].rank; }
@@ -152,6 +156,26 @@ int do_factorize(hodlr_t h) {
     int e = leaf_lu_launch(L, nl, h->smax, h->stream);
     if (e) return cuda_fail(h, (cudaError_t)e, "leaf_lu_launch");
     h->nlaunch += 1;
+    rc = check_phase(h, "factor: leaf LU");
+    if (rc) return rc;
+    if (h->checked) {  // every leaf's row permutation is a permutation of its rows
+      std::vector<int> perm(N);
+      CK(d2h(h, perm.data(), h->d_perm, sizeof(int) * N));
+      for (int p = 0; p < nl; ++p) {
+        const int r0 = h->leaf_min[p], s = h->leaf_size[p];
+        std::vector<char> seen(s, 0);
+        for (int i = 0; i < s; ++i) {
+          const int v = perm[r0 + i];
+          if (v < 0 || v >= s || seen[v]) {
+            char msg[160];
+            snprintf(msg, sizeof msg, "factor: leaf %d (rows %d..%d) permutation entry %d = %d", p,
+                     r0, r0 + s - 1, i, v);
+            return fail(h, HODLR_ERR_CHECK, msg);
+          }
+          seen[v] = 1;
+        }
+      }
+    }
   }
   // Y_l = the U panel of every level, zero padded to kmax columns: its own
   // allocation, or W_l itself (in place) when that cannot be had
@@ -221,8 +245,11 @@ int do_factorize(hodlr_t h) {
     S.X = Xinv;
     S.ldx = N;
     S.ncols = sm;
+    S.err = h->d_err;
     int e = leaf_solve_launch(S, nl, sm, h->stream);
     if (e) return cuda_fail(h, (cudaError_t)e, "leaf_solve_launch");
+    rc = check_phase(h, "factor: leaf inverses");
+    if (rc) return rc;
     // per level, in passes of CH columns through an N x CH buffer
     GemmProblem* d_probs = nullptr;
     int4* d_tiles = nullptr;
@@ -256,8 +283,12 @@ int do_factorize(hodlr_t h) {
         }
         CK(h2d(h, d_probs, probs.data(), sizeof(GemmProblem) * probs.size()));
         CK(h2d(h, d_tiles, tiles.data(), sizeof(int4) * tiles.size()));
+        rc = check_gemm(h, probs, false, "factor: leaf inverse product");
+        if (rc) return rc;
         e = gemm_nn_launch(d_probs, d_tiles, (int)tiles.size(), h->stream);
         if (e) return cuda_fail(h, (cudaError_t)e, "leaf inverse product");
+        rc = check_phase(h, "factor: leaf inverse product");
+        if (rc) return rc;
         CK(cudaMemcpyAsync(L.Yl + (int64_t)c0 * N, Y2, sizeof(double) * N * nc,
                            cudaMemcpyDeviceToDevice, h->stream));
         h->nlaunch += 1;
@@ -281,7 +312,7 @@ int do_factorize(hodlr_t h) {
       sn.kt = level_rank(L, 2 * p);
       sn.kb = level_rank(L, 2 * p + 1);
       sn.coff = L.coff;
-      sn.pad = 0;
+      sn.order = h->sm_form ? 1 : 0;
       const int sd = sn.kb + sn.kt;
       L.max_sd = std::max(L.max_sd, sd);
       sn.s_off = s_tot;
@@ -322,7 +353,7 @@ int do_factorize(hodlr_t h) {
           t.B = A.Yl + mn;
           t.N = ncols_t;
           t.ldb = (int)N;
-          t.C = h->Z + sn.z_off + (int64_t)A.coff * sd;
+          t.C = h->Z + sn.z_off + (int64_t)A.coff * sd + (h->sm_form ? sn.kt : 0);
           t.ldc = sd;
           tn.push_back(t);
         }
@@ -335,16 +366,22 @@ int do_factorize(hodlr_t h) {
           b.B = A.Yl + sp + 1;
           b.N = ncols_b;
           b.ldb = (int)N;
-          b.C = h->Z + sn.z_off + (int64_t)A.coff * sd + sn.kb;
+          b.C = h->Z + sn.z_off + (int64_t)A.coff * sd + (h->sm_form ? 0 : sn.kb);
           b.ldc = sd;
           tn.push_back(b);
         }
       }
     }
-    int rc2 = upload_plan(h, tn, true, L.tn);
+    int rc2 = upload_plan(h, tn, true, L.tn, "factor: V^T Y products");
     if (rc2) return rc2;
     int e = run_tn(h, L.tn);
     if (e) return cuda_fail(h, (cudaError_t)e, "gemm_tn");
+    rc2 = check_phase(h, "factor: V^T Y products");
+    if (rc2) return rc2;
+    rc2 = check_extent(h, L.S, sizeof(double) * s_tot, "capacitance matrices", "factor");
+    if (!rc2) rc2 = check_extent(h, L.piv, sizeof(int) * p_tot, "capacitance pivots", "factor");
+    if (!rc2) rc2 = check_extent(h, h->Z, sizeof(double) * z_tot, "Schur right-hand sides", "factor");
+    if (rc2) return rc2;
     SchurLaunch S;
     S.nodes = L.d_nodes;
     S.S = L.S;
@@ -357,11 +394,33 @@ int do_factorize(hodlr_t h) {
     e = schur_factor_launch(S, nn, sds.data(), h->stream);
     if (e) return cuda_fail(h, (cudaError_t)e, "schur_factor");
     h->nlaunch += schur_factor_launches(sds.data(), nn);
+    rc2 = check_phase(h, "factor: capacitance LU");
+    if (rc2) return rc2;
+    if (h->checked) {  // LAPACK-style interchanges: piv[p] in [p, sd)
+      std::vector<int> piv(p_tot);
+      CK(d2h(h, piv.data(), L.piv, sizeof(int) * p_tot));
+      for (int p = 0; p < nn; ++p) {
+        const SchurNode& sn = L.nodes[p];
+        const int sd = sn.kb + sn.kt;
+        for (int i = 0; i < sd; ++i) {
+          const int q = piv[sn.p_off + i];
+          if (q < i || q >= sd) {
+            char msg[192];
+            snprintf(msg, sizeof msg,
+                     "factor: level %d node %d (sd %d, %s LU) pivot %d = %d", l, p, sd,
+                     sd >= SCHUR_BIG_SD ? "multi-CTA" : "one-CTA", i, q);
+            return fail(h, HODLR_ERR_CHECK, msg);
+          }
+        }
+      }
+    }
     if (L.coff > 0) {
       int nl_solve = 0;
       e = schur_solve_factor_launch(S, nn, sds.data(), L.coff, h->stream, &nl_solve);
       if (e) return cuda_fail(h, (cudaError_t)e, "schur_solve");
       h->nlaunch += nl_solve;
+      rc2 = check_phase(h, "factor: ancestor-column solve");
+      if (rc2) return rc2;
       // Y_a[rows_h] -= Y_l[rows_h, 0 : rank(U_h)] * y_h[:, level a's columns]
       // for every ancestor level a < l
       std::vector<GemmProblem> up;
@@ -380,7 +439,7 @@ int do_factorize(hodlr_t h) {
             t.lda = (int)N;
             t.M = sp - mn + 1;
             t.K = sn.kt;
-            t.B = h->Z + sn.z_off + sn.kb + (int64_t)A.coff * sd;
+            t.B = h->Z + sn.z_off + (h->sm_form ? 0 : sn.kb) + (int64_t)A.coff * sd;
             t.ldb = sd;
             t.N = A.kmax;
             up.push_back(t);
@@ -393,17 +452,19 @@ int do_factorize(hodlr_t h) {
             b.lda = (int)N;
             b.M = mx - sp;
             b.K = sn.kb;
-            b.B = h->Z + sn.z_off + (int64_t)A.coff * sd;
+            b.B = h->Z + sn.z_off + (h->sm_form ? sn.kt : 0) + (int64_t)A.coff * sd;
             b.ldb = sd;
             b.N = A.kmax;
             up.push_back(b);
           }
         }
       }
-      rc2 = upload_plan(h, up, false, L.nn);
+      rc2 = upload_plan(h, up, false, L.nn, "factor: Y updates");
       if (rc2) return rc2;
       e = run_nn(h, L.nn);
       if (e) return cuda_fail(h, (cudaError_t)e, "gemm_nn_sub");
+      rc2 = check_phase(h, "factor: Y updates");
+      if (rc2) return rc2;
     }
   }
   CK(cudaEventRecord(h->ev1, h->stream));

@@ -132,7 +132,48 @@ int check_dev_err(hodlr_t h, const char* where) {
   if (e & DEV_ERR_TIMEOUT) return fail(h, HODLR_ERR_TIMEOUT, std::string(where) + ": device wait timed out");
   if (e & DEV_ERR_NONFINITE) return fail(h, HODLR_ERR_NONFINITE, std::string(where) + ": non-finite value");
   if (e & DEV_ERR_SINGULAR) return fail(h, HODLR_ERR_SINGULAR, std::string(where) + ": exact-zero pivot");
+  if (e & DEV_ERR_INDEX) {
+    std::string at;
+    if (e & DEV_ERR_AT_LEAF_PERM) at += " [leaf permutation]";
+    if (e & DEV_ERR_AT_SOLVE_PIV) at += " [capacitance solve pivots]";
+    if (e & DEV_ERR_AT_BLOCKED_PIV) at += " [blocked solve pivots]";
+    if (e & DEV_ERR_AT_LU_SWAP) at += " [multi-CTA LU interchanges]";
+    return fail(h, HODLR_ERR_CHECK, std::string(where) + ": pivot or permutation index out of range" + at);
+  }
   return fail(h, HODLR_ERR_CUDA, where);
+}
+
+int check_phase(hodlr_t h, const char* where) {
+  if (!h->checked) return HODLR_OK;
+  cudaError_t e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return cuda_fail(h, e, where);
+  return check_dev_err(h, where);
+}
+
+int check_extent(hodlr_t h, const void* p, size_t bytes, const char* what, const char* where) {
+  if (!h->checked || bytes == 0 || h->pool.holds(p, bytes)) return HODLR_OK;
+  char msg[256];
+  snprintf(msg, sizeof msg, "%s: %s [%p, +%zu bytes) is outside the handle's allocations", where,
+           what, p, bytes);
+  return fail(h, HODLR_ERR_CHECK, msg);
+}
+
+int check_gemm(hodlr_t h, const std::vector<GemmProblem>& probs, bool tn, const char* where) {
+  if (!h->checked) return HODLR_OK;
+  const size_t e = sizeof(double);
+  for (const auto& p : probs) {
+    if (p.M <= 0 || p.N <= 0 || p.K <= 0) continue;
+    // A: K x M (tn) or M x K, B: K x N, C: M x N, all column-major
+    const size_t a = tn ? (size_t)(p.M - 1) * p.lda + p.K : (size_t)(p.K - 1) * p.lda + p.M;
+    int rc = check_extent(h, p.A, a * e, "GEMM operand A", where);
+    if (!rc) rc = check_extent(h, p.B, ((size_t)(p.N - 1) * p.ldb + p.K) * e, "GEMM operand B", where);
+    if (!rc) rc = check_extent(h, p.C, ((size_t)(p.N - 1) * p.ldc + p.M) * e, "GEMM result C", where);
+    if (!rc && p.splits > 1)
+      rc = check_extent(h, h->ws + p.ws_off, (size_t)p.splits * p.M * p.N * e, "split-K slice",
+                        where);
+    if (rc) return rc;
+  }
+  return HODLR_OK;
 }
 
 EntrySrc make_src(hodlr_t h) {
@@ -154,6 +195,8 @@ int init_common(hodlr_t h) {
   int coop = 0;
   CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
   if (!coop) return fail(h, HODLR_ERR_UNSUPPORTED, "device lacks cooperative launch");
+  const char* chk = getenv("HODLR_CHECKED");
+  h->checked = chk && *chk && strcmp(chk, "0") != 0;
   CK(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
   h->stream = h->own_stream;
   CK(cudaEventCreate(&h->ev0));

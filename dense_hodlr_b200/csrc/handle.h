@@ -29,6 +29,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -159,6 +160,15 @@ struct DevPool {
     if (e == cudaSuccess) size[*p] = bytes;
     return e;
   }
+  // the live allocation that holds [p, p + bytes), if any (checked mode)
+  bool holds(const void* p, size_t bytes) const {
+    const char* c = (const char*)p;
+    for (auto& a : size) {
+      const char* b = (const char*)a.first;
+      if (c >= b && c + bytes <= b + a.second) return true;
+    }
+    return false;
+  }
   void free(void* p) {
     auto it = size.find(p);
     if (it == size.end()) return;
@@ -225,6 +235,12 @@ struct hodlr_handle_s {
   // one 256-thread CTA per SM it streamed slower than two CTAs of per-thread
   // loads -- 3.05 vs 3.64 TB/s on the sphere shape, N = 262144)
   bool aca_ring = false;
+  // factorization form (hodlr_set_solver_form): false recLU's Schur systems
+  // [bottom; top], true recSM's perturbI systems [top; bottom]
+  bool sm_form = false;
+  // checked mode (hodlr_set_checked): operand extents verified on the host
+  // before launches, no solve graph, a sync + error check after each group
+  bool checked = false;
   unsigned spin_limit = 0;       // polls of an ACA group barrier (0: HODLR_SPIN_LIMIT)
   bool bar_unreachable = false;  // ACA group barriers wait for one arrival too many
   std::vector<int> leaf_min, leaf_size;
@@ -322,6 +338,13 @@ cudaError_t d2h(hodlr_t h, void* dst, const void* src, size_t bytes);
 cudaError_t copy2d(hodlr_t h, void* dst, size_t dpitch, const void* src, size_t spitch,
                    size_t width, size_t rows, cudaMemcpyKind kind);
 int check_dev_err(hodlr_t h, const char* where);
+// Checked mode: synchronise and check the error word after a launch group.
+int check_phase(hodlr_t h, const char* where);
+// Checked mode: [p, p + bytes) lies inside a live allocation of the handle.
+int check_extent(hodlr_t h, const void* p, size_t bytes, const char* what, const char* where);
+// Checked mode: every operand of a grouped GEMM (tn: C = A^T B, else C (-)= A B)
+// and its split-K slice of the workspace.
+int check_gemm(hodlr_t h, const std::vector<GemmProblem>& probs, bool tn, const char* where);
 EntrySrc make_src(hodlr_t h);
 int grow_level(hodlr_t h, Level& L, int cap);
 void fill_block(hodlr_t h, Level& L, int q, AcaBlock& B);
@@ -335,7 +358,8 @@ std::vector<int4> block_geoms(hodlr_t h);
 int block_features_dev(hodlr_t h, const std::vector<int4>& geom, double l, float* d_F);
 int predict_ranks(hodlr_t h);
 int do_compress(hodlr_t h);
-int upload_plan(hodlr_t h, std::vector<GemmProblem>& probs, bool split, DevPlan& out);
+int upload_plan(hodlr_t h, std::vector<GemmProblem>& probs, bool split, DevPlan& out,
+                const char* what = "grouped GEMM");
 int level_rank(const Level& L, int q);
 int run_tn(hodlr_t h, const DevPlan& P);
 int run_nn(hodlr_t h, const DevPlan& P);

@@ -458,6 +458,30 @@ int hodlr_set_wait_limit(hodlr_t h, unsigned polls, int unreachable) {
   return HODLR_OK;
 }
 
+int hodlr_set_solver_form(hodlr_t h, int form) {
+  if (!h || (form != HODLR_FORM_RECLU && form != HODLR_FORM_RECSM)) return HODLR_ERR_ARG;
+  const bool sm = form == HODLR_FORM_RECSM;
+  if (sm != h->sm_form) {
+    CK(cudaStreamSynchronize(h->stream));
+    free_factor(h);  // the compression is kept, unless a factorization overwrote W
+    h->sm_form = sm;
+  }
+  return HODLR_OK;
+}
+
+int hodlr_get_solver_form(hodlr_t h, int* form) {
+  if (!h || !form) return HODLR_ERR_ARG;
+  *form = h->sm_form ? HODLR_FORM_RECSM : HODLR_FORM_RECLU;
+  return HODLR_OK;
+}
+
+int hodlr_set_checked(hodlr_t h, int on) {
+  if (!h || on < 0 || on > 1) return HODLR_ERR_ARG;
+  CK(cudaStreamSynchronize(h->stream));
+  h->checked = on != 0;
+  return HODLR_OK;
+}
+
 int hodlr_set_aca_streaming(hodlr_t h, int on) {
   if (!h || on < 0 || on > 1) return HODLR_ERR_ARG;
   h->aca_ring = on != 0;

@@ -187,7 +187,13 @@ __global__ void __launch_bounds__(LNT) leaf_solve_kernel(LeafSolveLaunch L) {
   const int* perm = L.perm + r0;
   for (int e = tid; e < s * ncol; e += LNT) {
     int i = e % s, c = e / s;
-    x[c * ldx + i] = L.X[(int64_t)(c0 + c) * L.ldx + r0 + perm[i]];
+    const int pi = perm[i];
+    if (pi < 0 || pi >= s) {  // never written by a valid leaf LU: skip and report
+      if (L.err) atomicOr(L.err, DEV_ERR_INDEX | DEV_ERR_AT_LEAF_PERM);
+      x[c * ldx + i] = 0.0;
+      continue;
+    }
+    x[c * ldx + i] = L.X[(int64_t)(c0 + c) * L.ldx + r0 + pi];
   }
   __syncthreads();
   lu_solve_tile(SmemLU{lu, lda}, s, x, ldx, ncol);
@@ -199,7 +205,10 @@ __global__ void __launch_bounds__(LNT) leaf_solve_kernel(LeafSolveLaunch L) {
 
 // ---------------------------------------------------------- Schur form
 // S[node] (sd x sd, sd = kb + kt): identity blocks on the diagonal, the level
-// products of Z on the off-diagonal blocks.
+// products of Z on the off-diagonal blocks.  With n1 the size of the first
+// unknown block (kb in recLU order, kt in recSM order), Z's rows follow the
+// same order and its own-level columns start at coff: the upper-right block
+// is Z[:n1, coff + (j - n1)], the lower-left Z[n1:, coff + j].
 // CTA (node, y) fills every gridDim.y-th slice of the node's entries, so a
 // large S is written by many CTAs.
 __global__ void schur_form_kernel(SchurLaunch L) {
@@ -208,17 +217,16 @@ __global__ void schur_form_kernel(SchurLaunch L) {
   const int sd = N.kb + N.kt;
   double* S = L.S + N.s_off;
   const double* Z = L.Z + N.z_off;  // sd x zcols, ld sd
+  const int n1 = N.order ? N.kt : N.kb;
   for (int64_t e = threadIdx.x + (int64_t)blockIdx.y * blockDim.x; e < (int64_t)sd * sd;
        e += (int64_t)blockDim.x * gridDim.y) {
     int i = (int)(e % sd), j = (int)(e / sd);
     double v;
-    if (i < N.kb && j < N.kb)
+    if ((i < n1) == (j < n1))
       v = (i == j) ? 1.0 : 0.0;
-    else if (i >= N.kb && j >= N.kb)
-      v = (i == j) ? 1.0 : 0.0;
-    else if (i < N.kb)  // top-right: V_b^T K_t^-1 U_t = Z rows [0,kb), cols coff + (j - kb)
-      v = Z[(int64_t)(N.coff + j - N.kb) * sd + i];
-    else  // bottom-left: V_t^T K_b^-1 U_b = Z rows [kb, sd), cols coff + j
+    else if (i < n1)  // recLU: V_b^T K_t^-1 U_t; recSM: V_t^T K_b^-1 U_b
+      v = Z[(int64_t)(N.coff + j - n1) * sd + i];
+    else  // recLU: V_t^T K_b^-1 U_b; recSM: V_b^T K_t^-1 U_t
       v = Z[(int64_t)(N.coff + j) * sd + i];
     S[(int64_t)j * sd + i] = v;
   }
@@ -427,6 +435,10 @@ __global__ void __launch_bounds__(256) big_swap_trsm_kernel(SchurLaunch L, BigNo
   double* ac = a + (int64_t)col * n;
   for (int c = 0; c < nb; ++c) {
     const int q = sp[c];
+    if (q < j0 + c || q >= n) {  // not an LU interchange: skip and report
+      atomicOr(L.err, DEV_ERR_INDEX | DEV_ERR_AT_LU_SWAP);
+      continue;
+    }
     if (q != j0 + c) {
       const double t = ac[j0 + c];
       ac[j0 + c] = ac[q];
@@ -511,6 +523,10 @@ __global__ void __launch_bounds__(256) big_rhs_perm_kernel(SchurLaunch L, BigNod
   const int* piv = L.piv + N.p_off;
   for (int p = 0; p < n; ++p) {
     const int q = __ldg(piv + p);
+    if (q < p || q >= n) {  // not an LU interchange: skip and report
+      atomicOr(L.err, DEV_ERR_INDEX | DEV_ERR_AT_BLOCKED_PIV);
+      continue;
+    }
     if (q != p) {
       const double t = x[p];
       x[p] = x[q];
@@ -736,6 +752,10 @@ __global__ void __launch_bounds__(256) schur_solve_kernel(SchurLaunch L, int nco
     double* xc = xs + c * ldx;
     for (int p = 0; p < n; ++p) {
       int q = piv[p];
+      if (q < p || q >= n) {  // not an LU interchange: skip and report
+        atomicOr(L.err, DEV_ERR_INDEX | DEV_ERR_AT_SOLVE_PIV);
+        continue;
+      }
       if (q != p) {
         double t = xc[p];
         xc[p] = xc[q];

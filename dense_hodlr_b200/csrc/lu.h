@@ -25,12 +25,16 @@ struct LeafSolveLaunch {
   double* X;     // N x ncols panel, column-major
   int64_t ldx;
   int ncols;
+  unsigned* err;  // DEV_ERR_INDEX: a permutation entry outside its leaf
 };
 
 struct SchurNode {
   int kb, kt;       // ranks of the bottom / top off-diagonal blocks
   int coff;         // number of ancestor columns (Schur right-hand sides)
-  int pad;
+  // unknown order of the capacitance system: 0 [bottom rank; top rank], the
+  // Schur matrix of recLU (src/HODLR_Matrix.cpp:663-670); 1 [top; bottom],
+  // the perturbI matrix I + VT U of recSM (src/perturbI.cpp:28-38)
+  int order;
   int64_t s_off;    // S (sd x sd) offset
   int64_t z_off;    // Z (sd x zcols) offset
   int64_t r_off;    // right-hand sides (sd x cols) offset for the solve

@@ -47,7 +47,7 @@ int build_solve_plans(hodlr_t h, int nrhs) {
       a.B = h->X + mn;
       a.N = nrhs;
       a.ldb = (int)N;
-      a.C = h->zs + sn[p].r_off;
+      a.C = h->zs + sn[p].r_off + (h->sm_form ? sn[p].kt : 0);
       a.ldc = sd;
       tn.push_back(a);
       GemmProblem b{};
@@ -58,7 +58,7 @@ int build_solve_plans(hodlr_t h, int nrhs) {
       b.B = h->X + sp + 1;
       b.N = nrhs;
       b.ldb = (int)N;
-      b.C = h->zs + sn[p].r_off + sn[p].kb;
+      b.C = h->zs + sn[p].r_off + (h->sm_form ? 0 : sn[p].kb);
       b.ldc = sd;
       tn.push_back(b);
       GemmProblem c{};
@@ -68,7 +68,7 @@ int build_solve_plans(hodlr_t h, int nrhs) {
       c.lda = (int)N;
       c.M = sp - mn + 1;
       c.K = sn[p].kt;
-      c.B = h->zs + sn[p].r_off + sn[p].kb;
+      c.B = h->zs + sn[p].r_off + (h->sm_form ? 0 : sn[p].kb);
       c.ldb = sd;
       c.N = nrhs;
       up.push_back(c);
@@ -79,14 +79,14 @@ int build_solve_plans(hodlr_t h, int nrhs) {
       d.lda = (int)N;
       d.M = mx - sp;
       d.K = sn[p].kb;
-      d.B = h->zs + sn[p].r_off;
+      d.B = h->zs + sn[p].r_off + (h->sm_form ? sn[p].kt : 0);
       d.ldb = sd;
       d.N = nrhs;
       up.push_back(d);
     }
-    int rc = upload_plan(h, tn, true, L.stn);
+    int rc = upload_plan(h, tn, true, L.stn, "solve: V^T X products");
     if (rc) return rc;
-    rc = upload_plan(h, up, false, L.snn);
+    rc = upload_plan(h, up, false, L.snn, "solve: X updates");
     if (rc) return rc;
     L.solve_nrhs = nrhs;
   }
@@ -105,14 +105,26 @@ int solve_in_place(hodlr_t h, int nrhs) {
   S.X = h->X;
   S.ldx = N;
   S.ncols = nrhs;
+  S.err = h->d_err;
   int e = leaf_solve_launch(S, (int)h->leaf_min.size(), h->smax, h->stream);
   if (e) return cuda_fail(h, (cudaError_t)e, "leaf_solve");
   h->nlaunch += 1;
+  int rc = check_phase(h, "solve: leaves");
+  if (rc) return rc;
   for (int l = (int)h->lv.size() - 1; l >= 0; --l) {
     Level& L = h->lv[l];
     const int nn = (int)L.nmin.size();
     e = run_tn(h, L.stn);
     if (e) return cuda_fail(h, (cudaError_t)e, "solve gemm_tn");
+    rc = check_phase(h, "solve: V^T X products");
+    if (!rc && h->checked)
+      for (const auto& sn : L.nodes) {
+        const int64_t sd = sn.kb + sn.kt;
+        rc = check_extent(h, L.S + sn.s_off, sizeof(double) * sd * sd, "capacitance LU", "solve");
+        if (!rc) rc = check_extent(h, L.piv + sn.p_off, sizeof(int) * sd, "pivots", "solve");
+        if (rc) break;
+      }
+    if (rc) return rc;
     SchurLaunch SL;
     SL.nodes = L.d_snodes;
     SL.S = L.S;
@@ -123,8 +135,12 @@ int solve_in_place(hodlr_t h, int nrhs) {
     e = schur_solve_launch(SL, nn, nrhs, nrhs, L.max_sd, h->stream);
     if (e) return cuda_fail(h, (cudaError_t)e, "solve schur");
     h->nlaunch += 1;
+    rc = check_phase(h, "solve: capacitance");
+    if (rc) return rc;
     e = run_nn(h, L.snn);
     if (e) return cuda_fail(h, (cudaError_t)e, "solve gemm_nn");
+    rc = check_phase(h, "solve: X updates");
+    if (rc) return rc;
   }
   return HODLR_OK;
 }
@@ -133,7 +149,7 @@ int solve_in_place(hodlr_t h, int nrhs) {
 // the right-hand-side count, stream, buffers, precision and factorization
 // are the same (one launch instead of ~4 per level).
 int solve_fast(hodlr_t h, int nrhs) {
-  if (h->sg_off) return solve_in_place(h, nrhs);
+  if (h->sg_off || h->checked) return solve_in_place(h, nrhs);
   const void* key[4] = {h->X, h->zs, h->ws, (const void*)(intptr_t)(h->gemm_prec + 1)};
   bool same = h->sg_exec && h->sg_nrhs == nrhs && h->sg_stream == h->stream &&
               h->sg_gen == h->factor_gen;
@@ -312,7 +328,7 @@ int kmatvec_dev(hodlr_t h, int nrhs, const double* d_x, int ldx, double* d_y, in
   int e = sym ? kmatvec_sym_launch(L, sym, h->stream) : kmatvec_launch(L, sp, h->stream);
   if (e) return cuda_fail(h, (cudaError_t)e, "kmatvec");
   h->nlaunch += 1 + (sym || sp > 1);
-  return HODLR_OK;
+  return check_phase(h, "full-kernel product");
 }
 
 
@@ -552,7 +568,7 @@ int gm_sub(hodlr_t h, const double* V, int nv, const std::vector<double>& coef, 
   gm_sub_kernel<<<1024, 256, 0, h->stream>>>(V, nv, h->gm_h, W, N, nrhs);
   CK(cudaGetLastError());
   h->nlaunch += 1;
-  return HODLR_OK;
+  return check_phase(h, "gmres: basis combination");
 }
 
 int gm_scale(hodlr_t h, const double* X, const std::vector<double>& sc, double* Y, int nrhs) {
@@ -562,7 +578,7 @@ int gm_scale(hodlr_t h, const double* X, const std::vector<double>& sc, double* 
   gm_scale_kernel<<<1024, 256, 0, h->stream>>>(X, h->gm_h, Y, N, nrhs);
   CK(cudaGetLastError());
   h->nlaunch += 1;
-  return HODLR_OK;
+  return check_phase(h, "gmres: column scaling");
 }
 
 // Restarted GMRES(m) on K x = b with the HODLR factor as a right

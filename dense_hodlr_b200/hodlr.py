@@ -170,8 +170,16 @@ class HODLR_Matrix:
         src/HODLR_Matrix.cpp:1232-1246): the next solve recomputes both."""
         _check(self._h, _L.lib().hodlr_reset(self._h))
 
+    def set_checked(self, on=True):
+        """Checked mode (hodlr_set_checked): operand extents verified before every
+        launch group, the solve without its CUDA graph, and a synchronisation
+        after every group, so that a device error names the group that raised
+        it.  Same results, slower; HODLR_CHECKED=1 in the environment turns it
+        on for every new handle."""
+        _check(self._h, _L.lib().hodlr_set_checked(self._h, int(bool(on))))
+
     def set_aca_streaming(self, on):
-        """Top-level ACA panels through the bulk-copy ring (1, default) or per-thread loads (0)."""
+        """Top-level ACA panels through the bulk-copy ring (1) or per-thread loads (0, default)."""
         _check(self._h, _L.lib().hodlr_set_aca_streaming(self._h, int(bool(on))))
 
     def set_factor_in_place(self, mode):
@@ -188,10 +196,37 @@ class HODLR_Matrix:
     def storeLRinTree(self):
         _check(self._h, _L.lib().hodlr_compress(self._h))
 
+    def set_solver_form(self, form):
+        """'recLU' (default) or 'recSM' (hodlr_set_solver_form): the
+        factorization every solve, refinement and log-determinant uses.
+        Changing it drops the factorization; the compression is kept."""
+        f = {"recLU": _L.FORM_RECLU, "recSM": _L.FORM_RECSM}.get(form)
+        if f is None:
+            raise HODLRError(_L.ERR_ARG, "solver form is 'recLU' or 'recSM'")
+        _check(self._h, _L.lib().hodlr_set_solver_form(self._h, f))
+
+    def get_solver_form(self):
+        f = ctypes.c_int()
+        _check(self._h, _L.lib().hodlr_get_solver_form(self._h, ctypes.byref(f)))
+        return "recSM" if f.value == _L.FORM_RECSM else "recLU"
+
     def recLU_Compute(self):
+        """Compression and the recLU factorization (src/HODLR_Matrix.cpp:794-803)."""
+        self.set_solver_form("recLU")
         _check(self._h, _L.lib().hodlr_factorize(self._h))
 
     def recLU_Solve(self, input_RHS):
+        """recLU_Solve (src/HODLR_Matrix.cpp:757-792)."""
+        self.set_solver_form("recLU")
+        return self._direct_solve(input_RHS, "recLU")
+
+    def recSM_Solve(self, input_RHS):
+        """recSM_Solve (src/HODLR_Matrix.cpp:805-841): the recursive
+        Sherman-Morrison factorization (perturbI nodes) and its solve."""
+        self.set_solver_form("recSM")
+        return self._direct_solve(input_RHS, "recSM")
+
+    def _direct_solve(self, input_RHS, name):
         b = _as_f64_fortran(input_RHS)
         if b.shape[0] != self.n:
             raise HODLRError(_L.ERR_ARG, "right-hand side has the wrong number of rows")
@@ -202,7 +237,7 @@ class HODLR_Matrix:
         if self.printResultInfo:
             rel = self.residual(x, b)
             print("**************************************************")
-            print("Solver Type                      = recLU")
+            print(f"Solver Type                      = {name}")
             print(f"Low-Rank Computation Time        = {self.get_LR_ComputationTime()} seconds")
             print(f"Factorization Time               = {self.get_recLU_FactorizationTime()} seconds")
             print(f"Solve Time                       = {self.get_recLU_SolveTime()} seconds")
@@ -308,6 +343,18 @@ class HODLR_Matrix:
         return self._times()[2]
 
     def get_recLU_TotalTime(self):
+        return self._times()[3]
+
+    # the recSM timings (members without getters in the reference,
+    # include/HODLR_Matrix.hpp:297-299): the last factorization and solve,
+    # whichever form ran
+    def get_recSM_FactorizationTime(self):
+        return self._times()[1]
+
+    def get_recSM_SolveTime(self):
+        return self._times()[2]
+
+    def get_recSM_TotalTime(self):
         return self._times()[3]
 
     def get_MatrixSize(self):

@@ -11,7 +11,8 @@
 //    (hodlr_kernel_desc + coordinates), a dense matrix, or (compiled with
 //    nvcc) a functor with a __device__ operator()(int i, int j), evaluated on
 //    the GPU into a stored n x n matrix;
-//  * only the "partialPiv_ACA" low-rank method and the recLU solver exist.
+//  * only the "partialPiv_ACA" low-rank method exists; recLU_Solve and
+//    recSM_Solve share one factorization at a time (switching refactors).
 // Without Eigen the matrices are hodlr_b200::Matrix (column-major); with
 // Eigen on the include path the Eigen::MatrixXd overloads are added.
 #ifndef HODLR_B200_HODLR_MATRIX_HPP
@@ -111,28 +112,34 @@ class user_IndexTree {
   }
   void printTree() const { printTree(rootNode, 0); }
 
-  // pre-order arrays for hodlr_set_index_tree
-  void flatten(std::vector<int>& split, std::vector<int>& left, std::vector<int>& right) const {
+  // pre-order arrays for hodlr_set_index_tree_bounds: split and children, and
+  // the four rank bounds of every node (bounds[0..3] = top min, bottom min,
+  // top max, bottom max; -1: none)
+  void flatten(std::vector<int>& split, std::vector<int>& left, std::vector<int>& right,
+               std::vector<int> (&bounds)[4]) const {
     split.clear();
     left.clear();
     right.clear();
-    if (rootNode) add(rootNode, split, left, right);
+    for (auto& b : bounds) b.clear();
+    if (rootNode) add(rootNode, split, left, right, bounds);
   }
 
  private:
   static int add(const node* nd, std::vector<int>& split, std::vector<int>& left,
-                 std::vector<int>& right) {
-    if (nd->topOffDiag_minRank != -1 || nd->bottOffDiag_minRank != -1 ||
-        nd->topOffDiag_maxRank != -1 || nd->bottOffDiag_maxRank != -1 ||
-        !(nd->LR_Method.empty() || nd->LR_Method == "partialPiv_ACA"))
+                 std::vector<int>& right, std::vector<int> (&bounds)[4]) {
+    if (!(nd->LR_Method.empty() || nd->LR_Method == "partialPiv_ACA"))
       throw hodlr_b200::Error(HODLR_ERR_UNSUPPORTED,
-                              "user tree rank bounds / low-rank methods are not on the GPU path");
+                              "only partial-pivot ACA is on the GPU path");
     const int id = (int)split.size();
     split.push_back(nd->splitIndex);
     left.push_back(-1);
     right.push_back(-1);
-    if (nd->left) left[id] = add(nd->left, split, left, right);
-    if (nd->right) right[id] = add(nd->right, split, left, right);
+    bounds[0].push_back(nd->topOffDiag_minRank);
+    bounds[1].push_back(nd->bottOffDiag_minRank);
+    bounds[2].push_back(nd->topOffDiag_maxRank);
+    bounds[3].push_back(nd->bottOffDiag_maxRank);
+    if (nd->left) left[id] = add(nd->left, split, left, right, bounds);
+    if (nd->right) right[id] = add(nd->right, split, left, right, bounds);
     return id;
   }
   static void freeTree(node* nd) {
@@ -278,9 +285,13 @@ class HODLR_Matrix {
 
   // ------------------------------------------------------------- solvers
   void storeLRinTree() { hodlr_b200::check(h_, hodlr_compress(h_), "storeLRinTree"); }
-  void recLU_Compute() { hodlr_b200::check(h_, hodlr_factorize(h_), "recLU_Compute"); }
+  void recLU_Compute() {
+    form(HODLR_FORM_RECLU);
+    hodlr_b200::check(h_, hodlr_factorize(h_), "recLU_Compute");
+  }
 
   hodlr_b200::Matrix recLU_Solve(const hodlr_b200::Matrix& input_RHS) {
+    form(HODLR_FORM_RECLU);
     hodlr_b200::Matrix x(input_RHS.rows(), input_RHS.cols());
     solve_raw(input_RHS.rows(), input_RHS.cols(), input_RHS.data(), x.data());
     if (printResultInfo) print_result(input_RHS.cols(), input_RHS.data(), x.data());
@@ -307,8 +318,28 @@ class HODLR_Matrix {
     return x;
   }
 
+  // recSM_Solve (reference :215, src/HODLR_Matrix.cpp:805-841): the recursive
+  // Sherman-Morrison (perturbI) factorization and its solve
+  hodlr_b200::Matrix recSM_Solve(const hodlr_b200::Matrix& input_RHS) {
+    form(HODLR_FORM_RECSM);
+    hodlr_b200::Matrix x(input_RHS.rows(), input_RHS.cols());
+    solve_raw(input_RHS.rows(), input_RHS.cols(), input_RHS.data(), x.data());
+    if (printResultInfo) print_result(input_RHS.cols(), input_RHS.data(), x.data());
+    return x;
+  }
+
 #ifdef HODLR_B200_HAVE_EIGEN
+  Eigen::MatrixXd recSM_Solve(const Eigen::MatrixXd& input_RHS) {
+    form(HODLR_FORM_RECSM);
+    Eigen::MatrixXd b = input_RHS;
+    Eigen::MatrixXd x(b.rows(), b.cols());
+    solve_raw((int)b.rows(), (int)b.cols(), b.data(), x.data());
+    if (printResultInfo) print_result((int)b.cols(), b.data(), x.data());
+    return x;
+  }
+
   Eigen::MatrixXd recLU_Solve(const Eigen::MatrixXd& input_RHS) {
+    form(HODLR_FORM_RECLU);
     Eigen::MatrixXd b = input_RHS;  // contiguous, column-major
     Eigen::MatrixXd x(b.rows(), b.cols());
     solve_raw((int)b.rows(), (int)b.cols(), b.data(), x.data());
@@ -348,13 +379,16 @@ class HODLR_Matrix {
   int last_iterations_ = 0;
 
   void set_tree(const user_IndexTree& t) {
-    std::vector<int> split, left, right;
-    t.flatten(split, left, right);
+    std::vector<int> split, left, right, b[4];
+    t.flatten(split, left, right, b);
     hodlr_b200::check(h_,
-                      hodlr_set_index_tree(h_, (int)split.size(), split.data(), left.data(),
-                                           right.data()),
+                      hodlr_set_index_tree_bounds(h_, (int)split.size(), split.data(),
+                                                  left.data(), right.data(), b[0].data(),
+                                                  b[1].data(), b[2].data(), b[3].data()),
                       "user_IndexTree");
   }
+
+  void form(int f) { hodlr_b200::check(h_, hodlr_set_solver_form(h_, f), "solver form"); }
 
   void solve_raw(int rows, int nrhs, const double* b, double* x) {
     if (rows != n_) throw hodlr_b200::Error(HODLR_ERR_ARG, "right-hand side has the wrong number of rows");

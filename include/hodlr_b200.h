@@ -31,6 +31,7 @@ typedef struct hodlr_handle_s* hodlr_t;
 #define HODLR_ERR_NONFINITE 7   /* a NaN/Inf matrix entry or residual */
 #define HODLR_ERR_TIMEOUT 8     /* a bounded device wait gave up */
 #define HODLR_ERR_IO 9          /* a file could not be opened, read or written */
+#define HODLR_ERR_CHECK 10      /* checked mode: an extent or index outside its buffer */
 
 /* kernel families: K_ij = f(r_ij) (+ shift on the diagonal) */
 #define HODLR_KERNEL_GAUSSIAN 0          /* exp(-r^2/l^2) */
@@ -216,6 +217,22 @@ int hodlr_get_num_systems(hodlr_t h, int* nsys);
  * signed value omits the row permutations, this one does not). */
 int hodlr_logdet(hodlr_t h, double* log_abs_det, int* sign);
 
+/* Factorization form.  HODLR_FORM_RECLU (default): recLU_Factorize /
+ * recLU_Solve (src/HODLR_Matrix.cpp:612-755), each node's Schur system with
+ * the bottom block's rank first.  HODLR_FORM_RECSM: recSM_Factorize /
+ * recSM_Solve (src/HODLR_Matrix.cpp:520-610,805-841), each node a perturbed
+ * identity I + U V^T (src/perturbI.cpp:15-59) whose K^-1 U panels come from
+ * the descendants' inverses applied level by level and whose capacitance
+ * system I + V^T U has the top block's rank first.  Both run the same
+ * level-batched kernels; the form decides the capacitance systems (and so
+ * their pivots and the rounding of the solution, not its value).  Changing
+ * the form drops the factorization (the compression is kept); every solve,
+ * refinement and log-determinant entry point then uses the new form. */
+#define HODLR_FORM_RECLU 0
+#define HODLR_FORM_RECSM 1
+int hodlr_set_solver_form(hodlr_t h, int form);
+int hodlr_get_solver_form(hodlr_t h, int* form);
+
 /* User index tree, replacing the constructors that take a user_IndexTree
  * (include/HODLR_Matrix.hpp:85,184; built by userTree_To_HODLRTree,
  * src/HODLR_Tree.cpp:207-327).  Nodes in pre-order, node 0 the root covering
@@ -335,6 +352,19 @@ int hodlr_set_aca_streaming(hodlr_t h, int on);
  * its group has -- a wait nothing completes -- so that this path can be
  * tested; set it back to 0 for normal work. */
 int hodlr_set_wait_limit(hodlr_t h, unsigned polls, int unreachable);
+
+/* Checked mode (no counterpart in the reference; a debugging aid).  on = 1:
+ * before every grouped GEMM, capacitance and leaf launch the host verifies
+ * that each operand's extent lies inside a live allocation of the handle,
+ * the direct solve runs without its CUDA graph, and the stream is
+ * synchronised after every launch group so that a device error names the
+ * group that raised it.  A violation returns HODLR_ERR_CHECK without
+ * launching.  The environment variable HODLR_CHECKED=1 turns it on for
+ * every handle at creation.  Results are the same as unchecked; only
+ * slower.  (Pivot and permutation indices are range-checked on the device
+ * in every mode: an index outside its range skips the access and the call
+ * returns HODLR_ERR_CHECK.) */
+int hodlr_set_checked(hodlr_t h, int on);
 int hodlr_get_factor_in_place(hodlr_t h, int* levels);
 
 /* Number of kernels this handle has launched since it was created. */

@@ -10,6 +10,8 @@
 //                                                 chooseNextRowCol)
 //   factorize   src/HODLR_Matrix.cpp:505-518,612-692 (recLU_Factorize)
 //   solve       src/HODLR_Matrix.cpp:694-755     (recLU_Solve)
+//   recSM       src/HODLR_Matrix.cpp:520-610,805-841, src/perturbI.cpp:15-83
+//               (recSM_Factorize, recSM_Solve, perturbI, calcDeterminant)
 //   entries     src/kernel.cpp:19-39             (kernelMatrix block / () / *)
 // Eigen's PartialPivLU, GEMM and norms (third party, not in the reference
 // tree) are restated from their mathematical definitions: row partial
@@ -219,6 +221,13 @@ struct Oracle {
   std::vector<LU> schurLU;        // per inner node
   std::vector<Mat> topSolnLR, bottSolnLR;
   std::vector<int> leaf_pos;     // node id -> leaf position
+  // recSM: per inner node the U panels after the descendants' inverses
+  // (topOffDiagU_SM / bottOffDiagU_SM) and the LU of its perturbI matrix
+  // I + VT U, order [top rank; bottom rank]
+  std::vector<Mat> smTop, smBott;
+  std::vector<LU> eqLU;
+  std::vector<LU> smLeafLU;
+  bool sm_factored = false;
   bool compressed = false, factored = false;
   int status = 0;
 
@@ -805,6 +814,7 @@ void compress(Oracle& o, int nthreads) {
     o.leafMat[p] = M;
   });
   o.compressed = true;
+  o.sm_factored = false;
 }
 
 // recLU_Factorize(rhs, node) (src/HODLR_Matrix.cpp:612-692).  The two
@@ -931,6 +941,141 @@ Mat rec_solve(const Oracle& o, const Mat& rhs, int id, int spawn = 1) {
   return res;
 }
 
+// ---------------------------------------------------------------- recSM
+// perturbI::solve (src/perturbI.cpp:50-55) of inner node p on the rows of
+// its own range: x - U eq^-1 (VT x), U = [smTop 0; 0 smBott],
+// VT = [0 V_top^T; V_bott^T 0] (src/perturbI.cpp:15-40).
+Mat perturb_solve(const Oracle& o, int p, const Mat& x) {
+  const Node& nd = o.nodes[o.inner[p]];
+  const Block& T = o.blocks[2 * p];
+  const Block& Bt = o.blocks[2 * p + 1];
+  const int st = nd.split - nd.min + 1, sb = nd.max - nd.split, c = x.c;
+  const int kt = T.rank, kb = Bt.rank;
+  Mat xt(st, c), xb(sb, c);
+  for (int j = 0; j < c; ++j) {
+    for (int i = 0; i < st; ++i) xt(i, j) = x(i, j);
+    for (int i = 0; i < sb; ++i) xb(i, j) = x(st + i, j);
+  }
+  Mat vt = matTmul(T.V, xb), vb = matTmul(Bt.V, xt);  // V_top^T x_bott, V_bott^T x_top
+  Mat r(kt + kb, c);
+  for (int j = 0; j < c; ++j) {
+    for (int i = 0; i < kt; ++i) r(i, j) = vt(i, j);
+    for (int i = 0; i < kb; ++i) r(kt + i, j) = vb(i, j);
+  }
+  Mat y = o.eqLU[p].solve(r);
+  Mat yt(kt, c), yb(kb, c);
+  for (int j = 0; j < c; ++j) {
+    for (int i = 0; i < kt; ++i) yt(i, j) = y(i, j);
+    for (int i = 0; i < kb; ++i) yb(i, j) = y(kt + i, j);
+  }
+  Mat ut = matmul(o.smTop[p], yt), ub = matmul(o.smBott[p], yb);
+  Mat out(st + sb, c);
+  for (int j = 0; j < c; ++j) {
+    for (int i = 0; i < st; ++i) out(i, j) = xt(i, j) - ut(i, j);
+    for (int i = 0; i < sb; ++i) out(st + i, j) = xb(i, j) - ub(i, j);
+  }
+  return out;
+}
+
+// The perturbI matrix of inner node p, I + VT U, and its LU
+// (src/perturbI.cpp:28-48): [I, V_top^T smBott; V_bott^T smTop, I].
+void perturb_factor(Oracle& o, int p) {
+  const Block& T = o.blocks[2 * p];
+  const Block& Bt = o.blocks[2 * p + 1];
+  const int kt = T.rank, kb = Bt.rank, sd = kt + kb;
+  Mat E(sd, sd);
+  for (int i = 0; i < sd; ++i) E(i, i) = 1.0;
+  Mat tr = matTmul(T.V, o.smBott[p]);   // kt x kb
+  Mat bl = matTmul(Bt.V, o.smTop[p]);   // kb x kt
+  for (int j = 0; j < kb; ++j)
+    for (int i = 0; i < kt; ++i) E(i, kt + j) = tr(i, j);
+  for (int j = 0; j < kt; ++j)
+    for (int i = 0; i < kb; ++i) E(kt + i, j) = bl(i, j);
+  o.eqLU[p].factor(E);
+}
+
+// Rows [r0, r0 + rows) of an inner node's U_SM panel (cols all) <- child^-1
+// of them, child = node id c (a leaf LU or the child's perturbI).
+void apply_child_inverse(Oracle& o, int c, Mat& panel, int r0) {
+  const Node& cn = o.nodes[c];
+  const int rows = cn.max - cn.min + 1;
+  Mat x(rows, panel.c);
+  for (int j = 0; j < panel.c; ++j)
+    for (int i = 0; i < rows; ++i) x(i, j) = panel(r0 + i, j);
+  Mat y = cn.leaf ? o.smLeafLU[o.leaf_pos[c]].solve(x) : perturb_solve(o, o.inner_pos[c], x);
+  for (int j = 0; j < panel.c; ++j)
+    for (int i = 0; i < rows; ++i) panel(r0 + i, j) = y(i, j);
+}
+
+// recSM_Factorize (src/HODLR_Matrix.cpp:520-592): U_SM starts as U; for each
+// level d from the deepest up to 1, the nodes at level d are factored (leaf
+// LU, or the perturbI of their current U_SM) and every inner node above them
+// has the rows of each such descendant replaced by that descendant's inverse
+// applied to them; finally the root's perturbI.
+void recsm_factor(Oracle& o) {
+  const int ni = (int)o.inner.size();
+  o.smTop.assign(ni, Mat());
+  o.smBott.assign(ni, Mat());
+  o.eqLU.assign(ni, LU());
+  o.smLeafLU.assign(o.leaves.size(), LU());
+  for (int p = 0; p < ni; ++p) {
+    o.smTop[p] = o.blocks[2 * p].W;
+    o.smBott[p] = o.blocks[2 * p + 1].W;
+  }
+  if (ni == 0) {  // the root is a leaf
+    for (size_t q = 0; q < o.leaves.size(); ++q) o.smLeafLU[q].factor(o.leafMat[q]);
+    o.sm_factored = true;
+    return;
+  }
+  for (int d = o.numLevels - 1; d > 0; --d) {
+    for (size_t id = 0; id < o.nodes.size(); ++id) {  // the nodes of level d
+      const Node& nd = o.nodes[id];
+      if (nd.level != d) continue;
+      if (nd.leaf)
+        o.smLeafLU[o.leaf_pos[id]].factor(o.leafMat[o.leaf_pos[id]]);
+      else
+        perturb_factor(o, o.inner_pos[id]);
+    }
+    for (int p = 0; p < ni; ++p) {  // every inner node above level d
+      const Node& an = o.nodes[o.inner[p]];
+      if (an.level >= d) continue;
+      for (size_t id = 0; id < o.nodes.size(); ++id) {
+        const Node& cn = o.nodes[id];
+        if (cn.level != d || cn.min < an.min || cn.max > an.max) continue;
+        if (cn.max <= an.split)
+          apply_child_inverse(o, (int)id, o.smTop[p], cn.min - an.min);
+        else
+          apply_child_inverse(o, (int)id, o.smBott[p], cn.min - an.split - 1);
+      }
+    }
+  }
+  perturb_factor(o, 0);
+  o.sm_factored = true;
+}
+
+// recSM_Solve(node, rhs) (src/HODLR_Matrix.cpp:594-610): the children in
+// place, then the node's perturbI on its rows.
+void recsm_solve(const Oracle& o, Mat& X, int id) {
+  const Node& nd = o.nodes[id];
+  const int rows = nd.max - nd.min + 1;
+  Mat x(rows, X.c);
+  if (nd.leaf) {
+    for (int j = 0; j < X.c; ++j)
+      for (int i = 0; i < rows; ++i) x(i, j) = X(nd.min + i, j);
+    Mat y = o.smLeafLU[o.leaf_pos[id]].solve(x);
+    for (int j = 0; j < X.c; ++j)
+      for (int i = 0; i < rows; ++i) X(nd.min + i, j) = y(i, j);
+    return;
+  }
+  recsm_solve(o, X, nd.left);
+  recsm_solve(o, X, nd.right);
+  for (int j = 0; j < X.c; ++j)
+    for (int i = 0; i < rows; ++i) x(i, j) = X(nd.min + i, j);
+  Mat y = perturb_solve(o, o.inner_pos[id], x);
+  for (int j = 0; j < X.c; ++j)
+    for (int i = 0; i < rows; ++i) X(nd.min + i, j) = y(i, j);
+}
+
 }  // namespace
 
 // ------------------------------------------------------------ C interface
@@ -955,7 +1100,7 @@ void* orc_create_kernel(int n, int dim, const double* pts, int ktype, double lsc
 void orc_set_entry_mode(void* h, int mode) {
   Oracle* o = (Oracle*)h;
   o->entry_mode = mode;
-  o->compressed = o->factored = false;
+  o->compressed = o->factored = o->sm_factored = false;
 }
 
 void* orc_create_dense(int n, const double* A, int lda, int leaf) {
@@ -992,7 +1137,7 @@ int orc_set_user_tree_bounds(void* h, int nn, const int* split, const int* left,
     return 1;
   }
   finish_tree(o, lv, lo);
-  o.compressed = o.factored = false;
+  o.compressed = o.factored = o.sm_factored = false;
   return 0;
 }
 
@@ -1004,7 +1149,7 @@ void orc_set_lr(void* h, double tol, double minPivot) {
   Oracle* o = (Oracle*)h;
   o->tol = tol;
   o->minPivot = (int)minPivot;  // the reference passes a double into an int parameter
-  o->compressed = o->factored = false;
+  o->compressed = o->factored = o->sm_factored = false;
 }
 
 int orc_compress(void* h, int nthreads) {
@@ -1045,6 +1190,46 @@ int orc_solve_mt(void* h, int nrhs, const double* b, double* x, int nthreads) {
 
 int orc_solve(void* h, int nrhs, const double* b, double* x) {
   return orc_solve_mt(h, nrhs, b, x, 1);
+}
+
+// recSM_Solve (src/HODLR_Matrix.cpp:805-841): compress if needed, the recSM
+// factorization (kept), then the solve.  Returns the exact-zero pivots met.
+int orc_recsm_solve(void* h, int nrhs, const double* b, double* x) {
+  Oracle* o = (Oracle*)h;
+  if (!o->compressed) compress(*o, 1);
+  if (!o->sm_factored) recsm_factor(*o);
+  Mat X(o->n, nrhs);
+  std::memcpy(X.a.data(), b, sizeof(double) * (size_t)o->n * nrhs);
+  recsm_solve(*o, X, 0);  // node 0: the root
+  std::memcpy(x, X.a.data(), sizeof(double) * (size_t)o->n * nrhs);
+  int nz = 0;
+  for (auto& l : o->smLeafLU) nz += l.nzero;
+  for (auto& l : o->eqLU) nz += l.nzero;
+  return nz;
+}
+
+// calcDeterminant (src/HODLR_Matrix.cpp:1660-1697, src/perturbI.cpp:61-83):
+// the sum of log|u_ii| over the leaf LUs and the perturbI LUs of the recSM
+// factorization, and the product of their diagonals' signs with the
+// interchanges' parity (the reference's determinant_ omits that parity).
+double orc_recsm_logdet(void* h, int* sign) {
+  Oracle* o = (Oracle*)h;
+  if (!o->compressed) compress(*o, 1);
+  if (!o->sm_factored) recsm_factor(*o);
+  double ld = 0.0;
+  int sg = 1;
+  auto add = [&](const LU& f) {
+    for (int i = 0; i < f.lu.r; ++i) {
+      const double d = f.lu(i, i);
+      ld += std::log(std::fabs(d));
+      if (d < 0) sg = -sg;
+      if (f.piv[i] != i) sg = -sg;
+    }
+  };
+  for (auto& f : o->smLeafLU) add(f);
+  for (auto& f : o->eqLU) add(f);
+  if (sign) *sign = sg;
+  return ld;
 }
 
 int orc_num_levels(void* h) { return ((Oracle*)h)->numLevels; }

@@ -48,6 +48,9 @@ def lib():
         L.orc_factorize_mt.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.orc_solve.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp]
         L.orc_solve_mt.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp, ctypes.c_int]
+        L.orc_recsm_solve.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp]
+        L.orc_recsm_logdet.argtypes = [ctypes.c_void_p, _ip]
+        L.orc_recsm_logdet.restype = ctypes.c_double
         for f in ("orc_num_levels", "orc_num_inner", "orc_num_leaves"):
             getattr(L, f).argtypes = [ctypes.c_void_p]
         L.orc_inner_info.argtypes = [ctypes.c_void_p, ctypes.c_int, _ip, _ip, _ip, _ip]
@@ -152,6 +155,23 @@ class OracleHODLR:
         x = np.zeros_like(b, order="F")
         lib().orc_solve_mt(self.h, b.shape[1], _ptr(b), _ptr(x), int(nthreads))
         return x
+
+    def recsm_solve(self, b):
+        """recSM_Solve (src/HODLR_Matrix.cpp:805-841): the recursive
+        Sherman-Morrison factorization (kept) and its solve."""
+        b = np.asfortranarray(b, dtype=np.float64)
+        if b.ndim == 1:
+            b = b.reshape(-1, 1, order="F")
+        x = np.zeros_like(b, order="F")
+        lib().orc_recsm_solve(self.h, b.shape[1], _ptr(b), _ptr(x))
+        return x
+
+    def recsm_slogdet(self):
+        """(sign, log|det|) from the recSM factorization's leaf and perturbI
+        LUs (calcDeterminant, src/HODLR_Matrix.cpp:1660-1697)."""
+        sg = ctypes.c_int()
+        ld = lib().orc_recsm_logdet(self.h, ctypes.byref(sg))
+        return sg.value, ld
 
     # tree / block introspection
     def num_levels(self):

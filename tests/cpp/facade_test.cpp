@@ -92,16 +92,25 @@ int main() {
     double du = Ku.logAbsDeterminant(), dd = Kd.logAbsDeterminant();
     std::printf("user tree: solution diff %g, log|det| %.12g vs %.12g\n", e, du, dd);
     fails += !(e < 1e-9) + !(std::fabs(du - dd) < 1e-8 * std::fabs(dd));
+    // rank bounds of a user node reach the GPU ACA: the root's top block
+    // stops at rank 5 (src/lowRank.cpp:244-247)
     user_IndexTree bounded;
     bounded.rootNode = new user_IndexTree::node();
     bounded.rootNode->splitIndex = 999;
     bounded.rootNode->topOffDiag_maxRank = 5;
-    try {
-      HODLR_Matrix Kb(n, n, k, X.data(), 1, 64, bounded);
-      fails += 1;
-    } catch (const hodlr_b200::Error& err) {
-      fails += (err.status() != HODLR_ERR_UNSUPPORTED);
-    }
+    HODLR_Matrix Kb(n, n, k, X.data(), 1, 64, bounded);
+    Kb.set_LRTolerance(1e-12);
+    Kb.storeLRinTree();
+    int rk[2] = {0, 0};
+    hodlr_b200::check(Kb.handle(), hodlr_get_ranks(Kb.handle(), rk), "ranks");
+    std::printf("bounded user tree: root ranks %d %d\n", rk[0], rk[1]);
+    fails += !(rk[0] == 5 && rk[1] > 5);
+    // recSM_Solve (reference :215): the perturbI factorization solves the
+    // same system
+    Matrix xs = Kd.recSM_Solve(b), xl = Kd.recLU_Solve(b);
+    double es = rel_err(xs, xl);
+    std::printf("recSM vs recLU: %g\n", es);
+    fails += !(es < 1e-10);
   }
   try {
     HODLR_Matrix bad(10, 10, [](int, int, void*) { return 0.0; }, nullptr, 30);
