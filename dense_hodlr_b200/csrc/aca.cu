@@ -906,8 +906,7 @@ static int set_smem(void* fn, size_t smem, bool ring) {
   if (ring)
     e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
                              (int)cudaSharedmemCarveoutMaxShared);
-  if (e == cudaSuccess && smem > 48 * 1024)
-    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess) e = smem_opt_in(fn, smem);
   if (e != cudaSuccess) cudaGetLastError();  // consume it: later launch checks stay clean
   return (int)e;
 }

@@ -10,6 +10,13 @@
 
 #define HODLR_INLINE __device__ __forceinline__
 
+// Dynamic shared memory of a launch: opted in at its exact size before every
+// launch.  The 48 KB a kernel gets without the opt-in counts its static
+// shared memory too, so a dynamic size just under 48 KB can still need it.
+inline cudaError_t smem_opt_in(const void* fn, size_t dyn_bytes) {
+  return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_bytes);
+}
+
 // Status codes of the C ABI (mirrored in include/hodlr_b200.h).
 enum {
   HS_OK = 0,

@@ -776,12 +776,18 @@ __global__ void __launch_bounds__(256) schur_solve_kernel(SchurLaunch L, int nco
   }
 }
 
+// Launch helpers return the first CUDA error at once.
+#define LCK(call)                             \
+  do {                                        \
+    cudaError_t e__ = (call);                 \
+    if (e__ != cudaSuccess) return (int)e__;  \
+  } while (0)
+
 }  // namespace
 
 int leaf_lu_launch(const LeafLULaunch& L, int nleaves, int smax, cudaStream_t s) {
   size_t smem = sizeof(double) * (size_t)smax * (smax | 1);
-  if (smem > 48 * 1024)
-    cudaFuncSetAttribute(leaf_lu_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  LCK(smem_opt_in((const void*)leaf_lu_kernel, smem));
   leaf_lu_kernel<<<nleaves, LNT, smem, s>>>(L);
   return (int)cudaGetLastError();
 }
@@ -791,14 +797,12 @@ int leaf_solve_launch(const LeafSolveLaunch& L, int nleaves, int smax, cudaStrea
   if (L.ncols <= 16) {
     constexpr int TC = 16;
     size_t smem = sizeof(double) * (size_t)(smax | 1) * (smax + TC);
-    cudaFuncSetAttribute(leaf_solve_kernel<TC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)smem);
+    LCK(smem_opt_in((const void*)leaf_solve_kernel<TC>, smem));
     leaf_solve_kernel<TC><<<dim3((L.ncols + TC - 1) / TC, nleaves), LNT, smem, s>>>(L);
   } else {
     constexpr int TC = 64;
     size_t smem = sizeof(double) * (size_t)(smax | 1) * (smax + TC);
-    cudaFuncSetAttribute(leaf_solve_kernel<TC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)smem);
+    LCK(smem_opt_in((const void*)leaf_solve_kernel<TC>, smem));
     leaf_solve_kernel<TC><<<dim3((L.ncols + TC - 1) / TC, nleaves), LNT, smem, s>>>(L);
   }
   return (int)cudaGetLastError();
@@ -817,6 +821,7 @@ int schur_factor_launch(const SchurLaunch& L, int nnodes, const int* sd, cudaStr
   for (int i = 0; i < nnodes; ++i)
     form_y = std::max(form_y, (int)std::min<int64_t>(256, (int64_t)sd[i] * sd[i] / 65536 + 1));
   schur_form_kernel<<<dim3(nnodes, form_y), 256, 0, s>>>(L);
+  LCK(cudaGetLastError());
   int small_max = 0, big_max = 0;
   std::vector<int> big;
   for (int i = 0; i < nnodes; ++i) {
@@ -830,10 +835,9 @@ int schur_factor_launch(const SchurLaunch& L, int nnodes, const int* sd, cudaStr
   if (small_max > 0) {
     const int pnb = panel_width(small_max);
     size_t smem = (size_t)small_max * pnb * sizeof(double);
-    if (smem > 48 * 1024)
-      cudaFuncSetAttribute(schur_lu_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)smem);
+    LCK(smem_opt_in((const void*)schur_lu_kernel, smem));
     schur_lu_kernel<<<nnodes, SNT, smem, s>>>(L, pnb, SCHUR_BIG_SD);
+    LCK(cudaGetLastError());
   }
   for (size_t b0 = 0; b0 < big.size(); b0 += BIG_MAX) {
     BigNodes B;
@@ -845,16 +849,17 @@ int schur_factor_launch(const SchurLaunch& L, int nnodes, const int* sd, cudaStr
     }
     const int pnb = std::min(BNB, panel_width(mx));
     const size_t smem = (size_t)mx * pnb * sizeof(double);
-    if (smem > 48 * 1024)
-      cudaFuncSetAttribute(big_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)smem);
+    LCK(smem_opt_in((const void*)big_panel_kernel, smem));
     for (int j0 = 0; j0 < mx; j0 += BNB) {
       big_panel_kernel<<<B.count, SNT, smem, s>>>(L, B, j0, pnb);
+      LCK(cudaGetLastError());
       big_swap_trsm_kernel<<<dim3((mx + 255) / 256, B.count), 256, 0, s>>>(L, B, j0);
+      LCK(cudaGetLastError());
       const int rest = mx - j0 - BNB;
       if (rest > 0) {
         const int t = (rest + BT - 1) / BT;
         big_update_kernel<<<dim3(t, t, B.count), 256, 0, s>>>(L, B, j0);
+        LCK(cudaGetLastError());
       }
     }
   }
@@ -895,11 +900,10 @@ int schur_solve_factor_launch(const SchurLaunch& L, int nnodes, const int* sd, i
     const size_t col_bytes = sizeof(double) * (size_t)(small_max | 1);
     const int tc = (int)std::max<size_t>(1, std::min<size_t>(STC, 200 * 1024 / col_bytes));
     const size_t smem = col_bytes * tc;
-    if (smem > 48 * 1024)
-      cudaFuncSetAttribute(schur_solve_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)smem);
+    LCK(smem_opt_in((const void*)schur_solve_kernel<false>, smem));
     schur_solve_kernel<false><<<dim3((coff + tc - 1) / tc, nnodes), 256, smem, s>>>(
         L, -1, tc, true, SCHUR_BIG_SOLVE_SD);
+    LCK(cudaGetLastError());
     ++*launches;
   }
   const int ctiles = (coff + BT - 1) / BT, cblocks = (coff + 255) / 256;
@@ -912,20 +916,27 @@ int schur_solve_factor_launch(const SchurLaunch& L, int nnodes, const int* sd, i
       mx = std::max(mx, sd[big[b0 + i]]);
     }
     big_rhs_perm_kernel<<<dim3(cblocks, B.count), 256, 0, s>>>(L, B);
+    LCK(cudaGetLastError());
     ++*launches;
     for (int j0 = 0; j0 < mx; j0 += BNB) {
       big_rhs_diag_kernel<true><<<dim3(cblocks, B.count), 256, 0, s>>>(L, B, j0);
+      LCK(cudaGetLastError());
       const int rows = mx - j0 - BNB;
-      if (rows > 0)
+      if (rows > 0) {
         big_rhs_update_kernel<true><<<dim3((rows + BT - 1) / BT, ctiles, B.count), 256, 0, s>>>(
             L, B, j0);
+        LCK(cudaGetLastError());
+      }
       *launches += 1 + (rows > 0);
     }
     for (int j0 = (mx - 1) / BNB * BNB; j0 >= 0; j0 -= BNB) {
       big_rhs_diag_kernel<false><<<dim3(cblocks, B.count), 256, 0, s>>>(L, B, j0);
-      if (j0 > 0)
+      LCK(cudaGetLastError());
+      if (j0 > 0) {
         big_rhs_update_kernel<false><<<dim3((j0 + BT - 1) / BT, ctiles, B.count), 256, 0, s>>>(
             L, B, j0);
+        LCK(cudaGetLastError());
+      }
       *launches += 1 + (j0 > 0);
     }
   }
@@ -944,14 +955,10 @@ int schur_solve_launch(const SchurLaunch& L, int nnodes, int ncols, int max_cols
   const size_t smem = in_smem ? col_bytes * tc : 0;
   const dim3 grid((max_cols + tc - 1) / tc, nnodes);
   if (ncols >= 0) {
-    if (smem > 48 * 1024)
-      cudaFuncSetAttribute(schur_solve_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)smem);
+    LCK(smem_opt_in((const void*)schur_solve_kernel<true>, smem));
     schur_solve_kernel<true><<<grid, 256, smem, s>>>(L, ncols, tc, in_smem, INT_MAX);
   } else {
-    if (smem > 48 * 1024)
-      cudaFuncSetAttribute(schur_solve_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)smem);
+    LCK(smem_opt_in((const void*)schur_solve_kernel<false>, smem));
     schur_solve_kernel<false><<<grid, 256, smem, s>>>(L, ncols, tc, in_smem, INT_MAX);
   }
   return (int)cudaGetLastError();
