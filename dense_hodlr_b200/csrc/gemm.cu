@@ -22,7 +22,7 @@ __device__ __forceinline__ void dmma_884(double (&d)[2], double a, double b) {
       : "d"(a), "d"(b));
 }
 
-// mode: 0 store C = A^T B (or split partial), 1 C -= A B, 2 store C = A B
+// mode: 0 store C = A^T B (or split partial), 1 C -= A B, 2 store C = A B, 3 C += A B
 //
 // The products run on the FP64 tensor-core instruction mma.m8n8k4.f64: warp
 // w (of 8) owns rows 32 (w % 2) .. +32 and columns 16 (w / 2) .. +16 of the
@@ -106,7 +106,7 @@ __global__ void __launch_bounds__(NT) gemm_kernel(const GemmProblem* __restrict_
   // NN-subtract: the C tile is read before the k loop (it does not change
   // there), so its load overlaps the products instead of stalling the epilogue
   double cold[4][4];
-  if (MODE == 1) {
+  if (MODE == 1 || MODE == 3) {
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       const int gn = n0 + ty + 16 * j;
@@ -163,6 +163,8 @@ __global__ void __launch_bounds__(NT) gemm_kernel(const GemmProblem* __restrict_
       const double v = smem[(ty + 16 * j) * LDC + tx + 16 * i];
       if (MODE == 1) {
         P.C[(int64_t)gn * P.ldc + gm] = cold[i][j] - v;
+      } else if (MODE == 3) {
+        P.C[(int64_t)gn * P.ldc + gm] = cold[i][j] + v;
       } else if (MODE == 0 && P.splits > 1) {
         ws[P.ws_off + ((int64_t)ks * P.N + gn) * P.M + gm] = v;
       } else {
@@ -206,6 +208,13 @@ int gemm_nn_sub_launch(const GemmProblem* d_probs, const int4* d_tiles, int ntil
                        cudaStream_t s) {
   if (ntiles == 0) return 0;
   gemm_kernel<false, 1><<<ntiles, NT, 0, s>>>(d_probs, d_tiles, nullptr);
+  return (int)cudaGetLastError();
+}
+
+int gemm_nn_add_launch(const GemmProblem* d_probs, const int4* d_tiles, int ntiles,
+                       cudaStream_t s) {
+  if (ntiles == 0) return 0;
+  gemm_kernel<false, 3><<<ntiles, NT, 0, s>>>(d_probs, d_tiles, nullptr);
   return (int)cudaGetLastError();
 }
 

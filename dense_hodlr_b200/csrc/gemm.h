@@ -30,6 +30,9 @@ int gemm_nn_sub_launch(const GemmProblem* d_probs, const int4* d_tiles, int ntil
                        cudaStream_t s);
 // C (M x N) = A B, A M x K, B K x N (no split along K)
 int gemm_nn_launch(const GemmProblem* d_probs, const int4* d_tiles, int ntiles, cudaStream_t s);
+// C (M x N) += A B
+int gemm_nn_add_launch(const GemmProblem* d_probs, const int4* d_tiles, int ntiles,
+                       cudaStream_t s);
 
 // tcgen05 forms of the same products (operands converted to prec in shared
 // memory, FP32 accumulation in tensor memory, FP64 results).

@@ -41,6 +41,11 @@ __global__ void __launch_bounds__(LNT) leaf_lu_kernel(LeafLULaunch L) {
   }
   for (int i = tid; i < s; i += LNT) perm[i] = i;
   __syncthreads();
+  if (L.a_copy)
+    for (int e = tid; e < s * s; e += LNT) {
+      int i = e % s, j = e / s;
+      L.a_copy[r0 + i + (int64_t)j * L.lda_copy] = a[j * lda + i];
+    }
   bool singular = false, nonfinite = false;
   for (int p = 0; p < s; ++p) {
     // pivot search in column p, rows p..s-1, first maximum

@@ -14,6 +14,10 @@ struct LeafLULaunch {
   int* perm;              // length N: row permutation of each leaf, local indices
   EntrySrc src;
   unsigned* err;
+  // optional: the assembled leaf blocks before factoring, leaf (r0, s) at
+  // a_copy[r0 + i + j * lda_copy] (i, j < s)
+  double* a_copy;
+  int64_t lda_copy;
 };
 
 struct LeafSolveLaunch {

@@ -116,17 +116,13 @@ def test_user_tree_rank_bounds_match_oracle(oracle_mod, n, leaf):
     b = np.random.default_rng(5).standard_normal((n, 2))
     x = g.recLU_Solve(b)
     xo = o.solve(b, nthreads=8)
-    rel = np.linalg.norm(x - xo) / np.linalg.norm(xo)
-    if n <= 1000:
-        assert rel <= SOLVE_TOL
-    else:
-        # Ranks capped at 5 and 3 leave a HODLR matrix far from K and badly
-        # conditioned (|x| ~ 160 |b|): two FP64 factorizations in different
-        # summation orders agree to ~1e-9 here (the blocked solve of the
-        # 128+-row capacitance systems orders its sums differently from the
-        # oracle's substitution).  The solutions are held to 1e-8, and the
-        # GPU's to the oracle's own accuracy on the HODLR operator itself.
-        assert rel <= 1e-8
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= SOLVE_TOL
+    if n > 1000:
+        # Ranks capped at 5 and 3 leave a badly conditioned HODLR matrix
+        # (|x| ~ 160 |b|), where a factorization that is not backward stable
+        # shows: the residual on the compressed operator itself must be the
+        # oracle's (an unrefined product with explicit leaf inverses left it
+        # 28x larger, with the solution still within 1e-9)
         rg, ro = _hodlr_residual(g, pts, 0.2, 1e-2, x, b), _hodlr_residual(g, pts, 0.2, 1e-2, xo, b)
         assert rg <= 1.5 * ro + 1e-14, (rg, ro)
 
