@@ -301,7 +301,9 @@ constexpr size_t wring_bytes(int stages) {
 }
 
 struct WRing {
-  double* buf;      // [warp][stage][column u][row], WR_ROWS rows per column
+  // [warp][stage][column u][row], WR_ROWS rows per column: a warp's stages
+  // are `stages` apart (wring_bytes(stages) in all), not WR_SMAX
+  double* buf;
   uint64_t* full;   // [warp][stage]: the stage's copies landed (1 arrival + bytes)
   int stages;
   uint32_t t;       // tiles this warp has consumed (the same in all its lanes)
@@ -350,7 +352,7 @@ __device__ void wring_issue(WRing& R, int w, uint32_t tw, const double* P, int64
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
                "r"(bytes * (uint32_t)nc)
                : "memory");
-  double* dst = R.buf + ((size_t)(w * WR_SMAX + slot) * WR_BC) * WR_ROWS;
+  double* dst = R.buf + ((size_t)(w * R.stages + slot) * WR_BC) * WR_ROWS;
   for (int u = 0; u < nc; ++u)
     asm volatile(
         "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
@@ -413,7 +415,7 @@ __device__ void residual_pass_wring(const AcaLaunch& L, const AcaBlock& B, doubl
       const uint32_t tw = R.t + q;
       const int slot = (int)(tw % (uint32_t)R.stages);
       mbar_wait_bounded(R.full + w * WR_SMAX + slot, (tw / (uint32_t)R.stages) & 1, L.err);
-      const double* tile = R.buf + ((size_t)(w * WR_SMAX + slot) * WR_BC) * WR_ROWS;
+      const double* tile = R.buf + ((size_t)(w * R.stages + slot) * WR_BC) * WR_ROWS;
       const int l0 = q * WR_BC, nc = min(WR_BC, k - l0);
       double v[WR_BC][E];
 #pragma unroll

@@ -272,6 +272,7 @@ struct hodlr_handle_s {
   int ir_cols = 0;
   double* gm_V = nullptr;  // GMRES bases: (m+1) and m panels of N x nrhs
   double* gm_Z = nullptr;
+  double* gm_W = nullptr;  // the products K Z_j (m panels): the residual's update
   double* gm_h = nullptr;  // small device buffers of coefficients / partials
   double* gm_part = nullptr;
   int gm_m = 0, gm_cols = 0;

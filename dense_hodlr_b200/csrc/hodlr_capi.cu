@@ -263,6 +263,7 @@ void hodlr_destroy(hodlr_t h) {
   dfree(h, h->ir_part);
   dfree(h, h->gm_V);
   dfree(h, h->gm_Z);
+  dfree(h, h->gm_W);
   dfree(h, h->gm_h);
   dfree(h, h->gm_part);
   dfree(h, h->part);

@@ -585,10 +585,16 @@ int gm_scale(hodlr_t h, const double* X, const std::vector<double>& sc, double* 
 // preconditioner (K M^-1 u = b, x = M^-1 u), all columns in lockstep so every
 // iteration costs one full-kernel product and one HODLR solve for all of
 // them.  Starts from the direct solve (the initial guess of iterative_Solve,
-// src/HODLR_Matrix.cpp:1169-1177) and stops when the true relative residual
+// src/HODLR_Matrix.cpp:1169-1177) and stops when the relative residual
 // max_c ||b_c - K x_c|| / ||b_c|| <= tol.  Classical Gram-Schmidt with one
 // re-orthogonalisation; Givens rotations as in IML's GMRES
 // (IML/include/gmres.h:83-153).
+//
+// The residual b - K x is formed with a full-kernel product once, for the
+// initial guess.  Each cycle's update x += Z y is matched by r -= W y with
+// W_j = K Z_j, the products the iterations already computed (kept before
+// their orthogonalisation), so r stays b - K x up to the rounding of that
+// combination -- no further full-kernel product per cycle.
 int gmres_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double* d_x, int ldx,
                  double tol, int max_iter, int m, int* iters, double* relres) {
   const int64_t N = h->n;
@@ -608,10 +614,12 @@ int gmres_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double* d_x, i
   if (m > h->gm_m || nrhs > h->gm_cols) {
     dfree(h, h->gm_V);
     dfree(h, h->gm_Z);
+    dfree(h, h->gm_W);
     dfree(h, h->gm_h);
     dfree(h, h->gm_part);
     CK(dalloc(h, &h->gm_V, (size_t)((m + 1) * N * nrhs)));
     CK(dalloc(h, &h->gm_Z, (size_t)(m * N * nrhs)));
+    CK(dalloc(h, &h->gm_W, (size_t)(m * N * nrhs)));
     CK(dalloc(h, &h->gm_h, (size_t)((m + 2) * nrhs)));
     CK(dalloc(h, &h->gm_part, (size_t)((m + 2) * nrhs * GM_BLOCKS)));
     h->gm_m = m;
@@ -631,16 +639,17 @@ int gmres_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double* d_x, i
   for (auto& v : bnorm) v = v > 0 ? std::sqrt(v) : 1.0;
   int total_it = 0;
   std::vector<double> worst_res(nrhs, HUGE_VAL);
+  // r = b - K x0 -> ir_y (the one full-kernel product for the residual)
+  for (int c0 = 0; c0 < nrhs; c0 += 16) {
+    int nc = std::min(16, nrhs - c0);
+    rc = kmatvec_dev(h, nc, h->ir_x + c0 * N, (int)N, h->ir_y + c0 * N, (int)N);
+    if (rc) return rc;
+  }
+  ir_residual_kernel<<<IR_BLOCKS, 256, 0, h->stream>>>(h->ir_b, h->ir_y, N, nrhs, h->ir_part);
+  CK(cudaGetLastError());
+  h->nlaunch += 1;
   for (int cycle = 0;; ++cycle) {
-    // r = b - K x  -> ir_y ; beta = ||r||
-    for (int c0 = 0; c0 < nrhs; c0 += 16) {
-      int nc = std::min(16, nrhs - c0);
-      rc = kmatvec_dev(h, nc, h->ir_x + c0 * N, (int)N, h->ir_y + c0 * N, (int)N);
-      if (rc) return rc;
-    }
-    ir_residual_kernel<<<IR_BLOCKS, 256, 0, h->stream>>>(h->ir_b, h->ir_y, N, nrhs, h->ir_part);
-    CK(cudaGetLastError());
-    h->nlaunch += 1;
+    // ir_y = r = b - K x ; beta = ||r||
     rc = gm_dots(h, h->ir_y, 1, h->ir_y, nrhs, tmp);
     if (rc) return rc;
     std::vector<double> beta(nrhs);
@@ -677,6 +686,8 @@ int gmres_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double* d_x, i
         rc = kmatvec_dev(h, nc, Zj + c0 * N, (int)N, h->ir_y + c0 * N, (int)N);
         if (rc) return rc;
       }
+      CK(cudaMemcpyAsync(h->gm_W + (int64_t)j * P, h->ir_y, sizeof(double) * P,
+                         cudaMemcpyDeviceToDevice, h->stream));
       // classical Gram-Schmidt, twice
       std::vector<double> hsum((size_t)(j + 1) * nrhs, 0.0);
       for (int pass = 0; pass < 2; ++pass) {
@@ -744,7 +755,12 @@ int gmres_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double* d_x, i
         ycoef[(size_t)i * nrhs + c] = Hc[(size_t)i * (m + 1) + i] != 0 ? t / Hc[(size_t)i * (m + 1) + i] : 0.0;
       }
     }
+    // r <- beta V_0 - W y (= r - K Z y), then x <- x + Z y
+    rc = gm_scale(h, h->gm_V, beta, h->ir_y, nrhs);
+    if (rc) return rc;
     if (nv > 0) {
+      rc = gm_sub(h, h->gm_W, nv, ycoef, h->ir_y, nrhs);
+      if (rc) return rc;
       for (auto& v : ycoef) v = -v;  // gm_sub subtracts
       rc = gm_sub(h, h->gm_Z, nv, ycoef, h->ir_x, nrhs);
       if (rc) return rc;
