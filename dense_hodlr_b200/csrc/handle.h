@@ -231,10 +231,10 @@ struct hodlr_handle_s {
   std::vector<hodlr_impl::Level> lv;
   std::vector<int> cap_hint;  // initial W/V columns per level (0 = default)
   int gemm_prec = HODLR_GEMM_FP64;  // arithmetic of the Woodbury products
-  // group-level ACA panels through the bulk-copy ring (off by default: with
-  // one 256-thread CTA per SM it streamed slower than two CTAs of per-thread
-  // loads -- 3.05 vs 3.64 TB/s on the sphere shape, N = 262144)
-  bool aca_ring = false;
+  // group-level ACA panels through the warps' bulk-copy rings (measured
+  // 4.61 vs 3.65 TB/s of per-thread loads on the sphere shape at N = 262144,
+  // 2.85 vs 2.37 on the 2D cloud; the same bits either way)
+  bool aca_ring = true;
   // factorization form (hodlr_set_solver_form): false recLU's Schur systems
   // [bottom; top], true recSM's perturbI systems [top; bottom]
   bool sm_form = false;

@@ -179,7 +179,7 @@ class HODLR_Matrix:
         _check(self._h, _L.lib().hodlr_set_checked(self._h, int(bool(on))))
 
     def set_aca_streaming(self, on):
-        """Top-level ACA panels through the bulk-copy ring (1) or per-thread loads (0, default)."""
+        """Top-level ACA panels through the bulk-copy rings (1, default) or per-thread loads (0)."""
         _check(self._h, _L.lib().hodlr_set_aca_streaming(self._h, int(bool(on))))
 
     def set_factor_in_place(self, mode):

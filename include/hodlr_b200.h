@@ -131,11 +131,14 @@ int hodlr_solve_refined(hodlr_t h, int nrhs, const double* b, int ldb, double* x
  * src/HODLR_Matrix.cpp:1138-1213): GMRES(restart) preconditioned by the HODLR
  * factor, starting from the recLU solution.  The reference runs IML GMRES
  * with left preconditioning on dense input only; here the preconditioner is
- * applied on the right so that the stopping test is the true relative
- * residual max_c ||b_c - K x_c|| / ||b_c|| <= tol, the full-kernel product
- * is FP64 with entries generated on the fly, and all right-hand sides
- * iterate together.  *iters = GMRES iterations (full-kernel products after
- * the first residual).  Device pointers; the second form takes host buffers. */
+ * applied on the right so that the stopping test is the relative residual
+ * max_c ||b_c - K x_c|| / ||b_c|| <= tol of the iterate itself: the residual
+ * of the initial guess comes from one full-kernel product, and each cycle's
+ * update x += Z y is matched by r -= (K Z) y with the products the iterations
+ * computed (no further product for the test).  The full-kernel product is
+ * FP64 with entries generated on the fly, and all right-hand sides iterate
+ * together.  *iters = GMRES iterations (full-kernel products after the
+ * first residual).  Device pointers; the second form takes host buffers. */
 int hodlr_iterative_solve_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double* d_x,
                                  int ldx, double tol, int max_iter, int restart, int* iters,
                                  double* relres);
@@ -338,10 +341,10 @@ int hodlr_gemm_device(int precision, int mode, int m, int n, int k, const double
 int hodlr_set_factor_in_place(hodlr_t h, int mode);
 
 /* How the ACA of the few-block top levels reads its W/V panel slices (no
- * counterpart in the reference): on = 1 streams them through a shared-memory
- * ring filled by bulk copies (used when N is even), 0 (default, measured
- * faster) loads them per thread.  Pivots, ranks and W/V are the same either way; the
- * setting applies from the next compression. */
+ * counterpart in the reference): on = 1 (default) streams them through
+ * per-warp shared-memory rings filled by bulk copies (used when N is even;
+ * measured 1.2-1.3x faster), 0 loads them per thread.  Pivots, ranks and W/V
+ * are the same either way; the setting applies from the next compression. */
 int hodlr_set_aca_streaming(hodlr_t h, int on);
 
 /* Bounded device waits (no counterpart in the reference).  The CTAs of one
