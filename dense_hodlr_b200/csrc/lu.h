@@ -61,10 +61,12 @@ int leaf_solve_launch(const LeafSolveLaunch& L, int nleaves, int smax, cudaStrea
 // columns); smaller ones by one CTA each.
 constexpr int SCHUR_BIG_SD = 384;
 // The factorization's solves of the ancestor columns go blocked from this
-// size: below it one CTA per 16 columns reads the whole LU per tile (cheap
-// for small S, whose LU stays in L2), above it the blocked solve reads each
-// 32-row block of the LU once per 64 columns.
-constexpr int SCHUR_BIG_SOLVE_SD = 128;
+// size (one 32-row diagonal block): the blocked solve reads each 32-row block
+// of the LU once per 64 columns and keeps every SM busy, where one CTA per 16
+// columns runs a latency-bound substitution per tile (measured on the 2D
+// Matern workload at N = 262144: factorization 0.146 s with the blocked solve
+// from 128 rows, 0.141 from 64, 0.128 from 32).
+constexpr int SCHUR_BIG_SOLVE_SD = 32;
 // sd: host array of the nodes' capacitance sizes (kb + kt), in node order.
 int schur_factor_launch(const SchurLaunch& L, int nnodes, const int* sd, cudaStream_t s);
 // Kernel launches schur_factor_launch makes for these sizes.
