@@ -371,7 +371,9 @@ int solve_in_place(hodlr_t h, int nrhs);
 int solve_fast(hodlr_t h, int nrhs);
 int do_solve_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double* d_x, int ldx,
                     bool host_io);
-int kmatvec_dev(hodlr_t h, int nrhs, const double* d_x, int ldx, double* d_y, int ldy);
+// skip (forest only, device): per-system flags of systems whose rows are left out
+int kmatvec_dev(hodlr_t h, int nrhs, const double* d_x, int ldx, double* d_y, int ldy,
+                const unsigned char* skip = nullptr);
 int refine_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double* d_x, int ldx,
                   double tol, int max_iter, int* iters, double* relres);
 int forest_refine_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double* d_x, int ldx,

@@ -647,6 +647,7 @@ __global__ void __launch_bounds__(KT) kmatvec_forest_kernel(KmatvecLaunch L,
   __shared__ double vs[NR][KT];
   __shared__ double tab[HX_TANG_TABLE_SIZE];
   const int4 it = items[blockIdx.x];
+  if (L.skip && L.skip[it.w]) return;  // a converged system of a refinement
   const hx_kparams kp = L.src.kps[it.w];
   for (int i = threadIdx.x; i < HX_TANG_TABLE_SIZE; i += blockDim.x) tab[i] = c_tang[i];
   int row[RPT];

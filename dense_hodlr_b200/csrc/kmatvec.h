@@ -14,6 +14,9 @@ struct KmatvecLaunch {
   int64_t ldy;
   double* ws;  // nsplit x nrhs x n partials (nsplit > 1)
   int n, nrhs;
+  // forest form only: per-system flags; a flagged system's rows are skipped
+  // (Y keeps what it held).  Null: every system.
+  const unsigned char* skip = nullptr;
 };
 
 int kmatvec_splits(int n, int num_sms);

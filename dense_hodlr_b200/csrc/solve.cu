@@ -294,9 +294,11 @@ __global__ void axpy_cols_kernel(double* X, const double* D, int64_t total) {
     X[e] += D[e];
 }
 
-int kmatvec_dev(hodlr_t h, int nrhs, const double* d_x, int ldx, double* d_y, int ldy) {
+int kmatvec_dev(hodlr_t h, int nrhs, const double* d_x, int ldx, double* d_y, int ldy,
+                const unsigned char* skip) {
   if (h->nsys) {  // forest: block-diagonal product
     KmatvecLaunch L;
+    L.skip = skip;
     L.src = make_src(h);
     L.X = d_x;
     L.ldx = ldx;
@@ -443,9 +445,11 @@ int forest_refine_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double
   std::vector<unsigned char> done((size_t)S, 0);
   int it = 0;
   for (;; ++it) {
+    // systems frozen by an earlier pass are left out of the product (their
+    // rows of Y are not read for a correction: the residual kernel zeroes them)
     for (int c0 = 0; c0 < nrhs; c0 += 16) {
       int nc = std::min(16, nrhs - c0);
-      rc = kmatvec_dev(h, nc, h->ir_x + c0 * N, (int)N, h->ir_y + c0 * N, (int)N);
+      rc = kmatvec_dev(h, nc, h->ir_x + c0 * N, (int)N, h->ir_y + c0 * N, (int)N, d_done);
       if (rc) return rc;
     }
     forest_residual_kernel<<<S, 256, 0, h->stream>>>(h->ir_b, h->ir_y, N, nrhs, d_off, d_done,
