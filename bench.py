@@ -833,8 +833,14 @@ def batched_systems(nsys, seed=SEED):
 
 
 def run_batched(case):
-    """Uneven batch, case 'batched[:nsys[:max_points_per_forest[:precision[:in_place]]]]'
-    (in_place 1: K^-1 U over the U panels, which lets a forest hold more points).
+    """Uneven batch, case
+    'batched[:nsys[:max_points_per_forest[:precision[:in_place[:solver]]]]]' (in_place 1:
+    K^-1 U over the U panels, which lets a forest hold more points; solver 'refine' or
+    'gmres': per-system refinement or per-system HODLR-preconditioned GMRES).  The
+    default forest size, 450000 points, was the fastest of 0.3M, 0.45M, 0.6M, 0.8M and
+    1.2M on this batch (6.9, 6.8, 7.6, 8.5, 9.1 s with refinement): a forest's
+    panels span its points at each level's largest capacity, so smaller forests of
+    similar-sized systems move fewer bytes.
     Systems are sorted by size and packed into forests (waves) of at most
     max_points points, each forest one handle whose level launches span its
     systems; per wave: compress, factor, direct solve and refinement until
@@ -844,9 +850,10 @@ def run_batched(case):
     from dense_hodlr_b200 import HODLR_Matrix, _lib
     parts = case.split(":")
     nsys = int(parts[1]) if len(parts) > 1 else 512
-    cap = int(parts[2]) if len(parts) > 2 else 1_200_000
-    prec = parts[3] if len(parts) > 3 else "fp64"
-    in_place = int(parts[4]) if len(parts) > 4 else -1
+    cap = int(parts[2]) if len(parts) > 2 and parts[2] else 450_000
+    prec = parts[3] if len(parts) > 3 and parts[3] else "fp64"
+    in_place = int(parts[4]) if len(parts) > 4 and parts[4] else -1
+    solver = parts[5] if len(parts) > 5 and parts[5] else "refine"
     systems = batched_systems(nsys)
     order = sorted(range(nsys), key=lambda q: -systems[q][0].shape[1])
     waves, cur, npts = [], [], 0
@@ -862,7 +869,7 @@ def run_batched(case):
     rng = np.random.default_rng(SEED + 3)
     total_pts = sum(p.shape[1] for p, _ in systems)
     res = {"case": "batched", "systems": nsys, "points": int(total_pts), "waves": len(waves),
-           "max_points_per_forest": cap, "precision": prec}
+           "max_points_per_forest": cap, "precision": prec, "solver": solver}
 
     peak_gb = []
 
@@ -880,7 +887,12 @@ def run_batched(case):
             t0 = time.perf_counter()
             F.storeLRinTree()
             F.recLU_Compute()
-            it, rel = F.forest_refine_device(b.data_ptr(), x.data_ptr(), 1, tol=1e-10, max_iter=100)
+            if solver == "gmres":
+                it, rel = F.iterative_solve_device(b.data_ptr(), x.data_ptr(), 1, tol=1e-10,
+                                                   max_iter=100, restart=32)
+            else:
+                it, rel = F.forest_refine_device(b.data_ptr(), x.data_ptr(), 1, tol=1e-10,
+                                                 max_iter=100)
             torch.cuda.synchronize()
             t_total += time.perf_counter() - t0
             worst = max(worst, float(rel.max()))
@@ -893,7 +905,7 @@ def run_batched(case):
     run_waves(False)  # warm-up: device pool, modules
     t, worst, its = run_waves(True)
     res.update({"seconds": t, "systems_per_s": nsys / t, "max_rel_residual": worst,
-                "refine_corrections_per_wave": its, "device_used_gb_per_wave": peak_gb,
+                "iterations_per_wave": its, "device_used_gb_per_wave": peak_gb,
                 "in_place": in_place})
     # one handle per system, every 8th system, scaled by 8
     t1 = 0.0
@@ -911,7 +923,11 @@ def run_batched(case):
             g.set_precision(prec)
         g.storeLRinTree()
         g.recLU_Compute()
-        g.solve_refined_device(b.data_ptr(), x.data_ptr(), 1, tol=1e-10, max_iter=100)
+        if solver == "gmres":
+            g.iterative_solve_device(b.data_ptr(), x.data_ptr(), 1, tol=1e-10, max_iter=100,
+                                     restart=32)
+        else:
+            g.solve_refined_device(b.data_ptr(), x.data_ptr(), 1, tol=1e-10, max_iter=100)
         torch.cuda.synchronize()
         t1 += time.perf_counter() - t0
         del g

@@ -209,6 +209,7 @@ struct hodlr_handle_s {
   std::vector<hx_kparams> sys_kp;
   hx_kparams* d_kps = nullptr;
   int* d_psys = nullptr;
+  int* d_sysoff = nullptr;  // nsys + 1 row offsets on the device (GMRES segments)
   int4* d_fitems = nullptr;  // full-kernel product work items, by kernel family
   int ftype_off[HX_FOREST_TYPES + 1] = {0};
   double* d_fnorm = nullptr;  // per-system residual and right-hand-side norms

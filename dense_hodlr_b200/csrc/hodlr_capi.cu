@@ -273,6 +273,7 @@ void hodlr_destroy(hodlr_t h) {
   dfree(h, h->dotg);
   dfree(h, h->d_kps);
   dfree(h, h->d_psys);
+  dfree(h, h->d_sysoff);
   dfree(h, h->d_fitems);
   dfree(h, h->d_fnorm);
   dfree(h, h->d_model);

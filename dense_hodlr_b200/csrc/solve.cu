@@ -527,39 +527,83 @@ __global__ void gm_sum_kernel(const double* part, int count, double* out) {
   }
 }
 
-// W[:, c] -= sum_{i < nv} coef[i * nrhs + c] * V_i[:, c]
+// Segments: in a forest every system is its own GMRES problem, so inner
+// products and coefficients are per (system, column) -- "virtual column"
+// v = s * nrhs + c of Vc = S * nrhs, S = 1 outside a forest.  Coefficient
+// arrays are indexed [i][v]; psys (null when S == 1) maps a row to its system.
+
+// part[(i * S + s) * nrhs + c] = V_i[rows of s, c] . W[rows of s, c]: one CTA
+// per (system, i), rows in order of a fixed tree (forests only).
+__global__ void gm_seg_dots_kernel(const double* V, int nv, const double* W, int64_t n, int nrhs,
+                                   const int* off, int S, double* out) {
+  __shared__ double red[8];
+  const int sys = blockIdx.x, i = blockIdx.y;
+  const double* Vi = V + (int64_t)i * n * nrhs;
+  const int r0 = off[sys], r1 = off[sys + 1];
+  for (int c = 0; c < nrhs; ++c) {
+    double a = 0.0;
+    for (int r = r0 + threadIdx.x; r < r1; r += blockDim.x)
+      a = fma(Vi[c * n + r], W[c * n + r], a);
+    a = warp_sum(a);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = a;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int q = 0; q < (int)(blockDim.x >> 5); ++q) t += red[q];
+      out[((int64_t)i * S + sys) * nrhs + c] = t;
+    }
+    __syncthreads();
+  }
+}
+
+// W[:, c] -= sum_{i < nv} coef[(i * S + s) * nrhs + c] * V_i[:, c], s the row's system
 __global__ void gm_sub_kernel(const double* V, int nv, const double* coef, double* W, int64_t n,
-                              int nrhs) {
+                              int nrhs, const int* psys, int S) {
   const int64_t total = n * nrhs;
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
        e += (int64_t)gridDim.x * blockDim.x) {
     const int c = (int)(e / n);
+    const int sys = psys ? psys[e - (int64_t)c * n] : 0;
     double w = W[e];
-    for (int i = 0; i < nv; ++i) w = fma(-coef[i * nrhs + c], V[(int64_t)i * total + e], w);
+    for (int i = 0; i < nv; ++i)
+      w = fma(-coef[((int64_t)i * S + sys) * nrhs + c], V[(int64_t)i * total + e], w);
     W[e] = w;
   }
 }
 
-// Y[:, c] = X[:, c] * scale[c] (scale 0 gives an exact zero column)
+// Y[:, c] = X[:, c] * scale[s * nrhs + c] (scale 0 gives an exact zero)
 __global__ void gm_scale_kernel(const double* X, const double* scale, double* Y, int64_t n,
-                                int nrhs) {
+                                int nrhs, const int* psys) {
   const int64_t total = n * nrhs;
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
        e += (int64_t)gridDim.x * blockDim.x) {
-    const double sc = scale[e / n];
+    const int c = (int)(e / n);
+    const int sys = psys ? psys[e - (int64_t)c * n] : 0;
+    const double sc = scale[(int64_t)sys * nrhs + c];
     Y[e] = sc == 0.0 ? 0.0 : X[e] * sc;
   }
 }
 
-// Host-side launch helpers bound to the handle's stream.
+static int gm_segments(hodlr_t h) { return h->nsys ? h->nsys : 1; }
+
+// Host-side launch helpers bound to the handle's stream.  out / coef / sc
+// hold nv * S * nrhs (dots, combinations) or S * nrhs (scaling) values.
 int gm_dots(hodlr_t h, const double* V, int nv, const double* W, int nrhs, std::vector<double>& out) {
   const int64_t N = h->n;
-  gm_dots_kernel<<<dim3(GM_BLOCKS, nv), 256, 0, h->stream>>>(V, nv, W, N, nrhs, h->gm_part);
-  gm_sum_kernel<<<(nv * nrhs + 255) / 256, 256, 0, h->stream>>>(h->gm_part, nv * nrhs, h->gm_h);
+  const int S = gm_segments(h);
+  if (S == 1) {
+    gm_dots_kernel<<<dim3(GM_BLOCKS, nv), 256, 0, h->stream>>>(V, nv, W, N, nrhs, h->gm_part);
+    gm_sum_kernel<<<(nv * nrhs + 255) / 256, 256, 0, h->stream>>>(h->gm_part, nv * nrhs, h->gm_h);
+    h->nlaunch += 2;
+  } else {
+    gm_seg_dots_kernel<<<dim3(S, nv), 256, 0, h->stream>>>(V, nv, W, N, nrhs, h->d_sysoff, S,
+                                                            h->gm_h);
+    h->nlaunch += 1;
+  }
   CK(cudaGetLastError());
-  h->nlaunch += 2;
-  out.resize((size_t)nv * nrhs);
-  CK(cudaMemcpyAsync(out.data(), h->gm_h, sizeof(double) * nv * nrhs, cudaMemcpyDeviceToHost,
+  const size_t cnt = (size_t)nv * S * nrhs;
+  out.resize(cnt);
+  CK(cudaMemcpyAsync(out.data(), h->gm_h, sizeof(double) * cnt, cudaMemcpyDeviceToHost,
                      h->stream));
   CK(cudaStreamSynchronize(h->stream));
   return HODLR_OK;
@@ -567,9 +611,11 @@ int gm_dots(hodlr_t h, const double* V, int nv, const double* W, int nrhs, std::
 
 int gm_sub(hodlr_t h, const double* V, int nv, const std::vector<double>& coef, double* W, int nrhs) {
   const int64_t N = h->n;
-  CK(cudaMemcpyAsync(h->gm_h, coef.data(), sizeof(double) * nv * nrhs, cudaMemcpyHostToDevice,
-                     h->stream));
-  gm_sub_kernel<<<1024, 256, 0, h->stream>>>(V, nv, h->gm_h, W, N, nrhs);
+  const int S = gm_segments(h);
+  CK(cudaMemcpyAsync(h->gm_h, coef.data(), sizeof(double) * nv * S * nrhs,
+                     cudaMemcpyHostToDevice, h->stream));
+  gm_sub_kernel<<<1024, 256, 0, h->stream>>>(V, nv, h->gm_h, W, N, nrhs,
+                                             S > 1 ? h->d_psys : nullptr, S);
   CK(cudaGetLastError());
   h->nlaunch += 1;
   return check_phase(h, "gmres: basis combination");
@@ -577,9 +623,11 @@ int gm_sub(hodlr_t h, const double* V, int nv, const std::vector<double>& coef, 
 
 int gm_scale(hodlr_t h, const double* X, const std::vector<double>& sc, double* Y, int nrhs) {
   const int64_t N = h->n;
-  CK(cudaMemcpyAsync(h->gm_h, sc.data(), sizeof(double) * nrhs, cudaMemcpyHostToDevice,
+  const int S = gm_segments(h);
+  CK(cudaMemcpyAsync(h->gm_h, sc.data(), sizeof(double) * S * nrhs, cudaMemcpyHostToDevice,
                      h->stream));
-  gm_scale_kernel<<<1024, 256, 0, h->stream>>>(X, h->gm_h, Y, N, nrhs);
+  gm_scale_kernel<<<1024, 256, 0, h->stream>>>(X, h->gm_h, Y, N, nrhs,
+                                               S > 1 ? h->d_psys : nullptr);
   CK(cudaGetLastError());
   h->nlaunch += 1;
   return check_phase(h, "gmres: column scaling");
@@ -592,7 +640,10 @@ int gm_scale(hodlr_t h, const double* X, const std::vector<double>& sc, double* 
 // src/HODLR_Matrix.cpp:1169-1177) and stops when the relative residual
 // max_c ||b_c - K x_c|| / ||b_c|| <= tol.  Classical Gram-Schmidt with one
 // re-orthogonalisation; Givens rotations as in IML's GMRES
-// (IML/include/gmres.h:83-153).
+// (IML/include/gmres.h:83-153).  On a forest every (system, column) pair is
+// its own GMRES problem -- its own inner products, Hessenberg matrix and
+// stopping test on the system's rows -- and the systems whose columns have
+// all converged are left out of the block-diagonal product.
 //
 // The residual b - K x is formed with a full-kernel product once, for the
 // initial guess.  Each cycle's update x += Z y is matched by r -= W y with
@@ -602,6 +653,8 @@ int gm_scale(hodlr_t h, const double* X, const std::vector<double>& sc, double* 
 int gmres_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double* d_x, int ldx,
                  double tol, int max_iter, int m, int* iters, double* relres) {
   const int64_t N = h->n;
+  const int S = gm_segments(h);
+  const int VC = S * nrhs;  // virtual columns
   int rc = build_solve_plans(h, nrhs);
   if (rc) return rc;
   if (nrhs > h->ir_cols) {
@@ -624,10 +677,19 @@ int gmres_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double* d_x, i
     CK(dalloc(h, &h->gm_V, (size_t)((m + 1) * N * nrhs)));
     CK(dalloc(h, &h->gm_Z, (size_t)(m * N * nrhs)));
     CK(dalloc(h, &h->gm_W, (size_t)(m * N * nrhs)));
-    CK(dalloc(h, &h->gm_h, (size_t)((m + 2) * nrhs)));
+    CK(dalloc(h, &h->gm_h, (size_t)((m + 2) * (int64_t)S * nrhs)));
     CK(dalloc(h, &h->gm_part, (size_t)((m + 2) * nrhs * GM_BLOCKS)));
     h->gm_m = m;
     h->gm_cols = nrhs;
+  }
+  unsigned char* d_skip = nullptr;
+  if (S > 1) {
+    if (!h->d_sysoff) {
+      CK(dalloc(h, &h->d_sysoff, (size_t)S + 1));
+      CK(h2d(h, h->d_sysoff, h->sys_off.data(), sizeof(int) * (S + 1)));
+    }
+    CK(dalloc(h, &d_skip, (size_t)S));
+    CK(cudaMemsetAsync(d_skip, 0, (size_t)S, h->stream));
   }
   const int64_t P = N * nrhs;
   CK(cudaMemcpy2DAsync(h->ir_b, sizeof(double) * N, d_b, sizeof(double) * ldb,
@@ -642,7 +704,7 @@ int gmres_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double* d_x, i
   if (rc) return rc;
   for (auto& v : bnorm) v = v > 0 ? std::sqrt(v) : 1.0;
   int total_it = 0;
-  std::vector<double> worst_res(nrhs, HUGE_VAL);
+  std::vector<double> worst_res(VC, HUGE_VAL);
   // r = b - K x0 -> ir_y (the one full-kernel product for the residual)
   for (int c0 = 0; c0 < nrhs; c0 += 16) {
     int nc = std::min(16, nrhs - c0);
@@ -652,34 +714,43 @@ int gmres_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double* d_x, i
   ir_residual_kernel<<<IR_BLOCKS, 256, 0, h->stream>>>(h->ir_b, h->ir_y, N, nrhs, h->ir_part);
   CK(cudaGetLastError());
   h->nlaunch += 1;
+  std::vector<unsigned char> skip(S, 0);
   for (int cycle = 0;; ++cycle) {
-    // ir_y = r = b - K x ; beta = ||r||
+    // ir_y = r = b - K x ; beta = ||r|| per virtual column
     rc = gm_dots(h, h->ir_y, 1, h->ir_y, nrhs, tmp);
     if (rc) return rc;
-    std::vector<double> beta(nrhs);
+    std::vector<double> beta(VC);
     double worst = 0.0;
-    for (int c = 0; c < nrhs; ++c) {
-      beta[c] = std::sqrt(std::max(tmp[c], 0.0));
-      worst_res[c] = beta[c] / bnorm[c];
-      worst = std::max(worst, worst_res[c]);
+    for (int v = 0; v < VC; ++v) {
+      beta[v] = std::sqrt(std::max(tmp[v], 0.0));
+      worst_res[v] = beta[v] / bnorm[v];
+      worst = std::max(worst, worst_res[v]);
     }
     if (worst <= tol || total_it >= max_iter) break;
     // V0 = r / beta
-    std::vector<double> sc(nrhs);
-    for (int c = 0; c < nrhs; ++c) sc[c] = beta[c] > 0 ? 1.0 / beta[c] : 0.0;
+    std::vector<double> sc(VC);
+    for (int v = 0; v < VC; ++v) sc[v] = beta[v] > 0 ? 1.0 / beta[v] : 0.0;
     rc = gm_scale(h, h->ir_y, sc, h->gm_V, nrhs);
     if (rc) return rc;
-    // per-column Hessenberg (column-major (m+1) x m), rotations, rhs g
-    std::vector<double> H((size_t)(m + 1) * m * nrhs, 0.0), cs((size_t)m * nrhs),
-        sn((size_t)m * nrhs), g((size_t)(m + 1) * nrhs, 0.0);
-    for (int c = 0; c < nrhs; ++c) g[c] = beta[c];
-    std::vector<int> done(nrhs, 0), used(nrhs, 0);
-    for (int c = 0; c < nrhs; ++c)
-      if (worst_res[c] <= tol) done[c] = 1;
+    // per virtual column Hessenberg (column-major (m+1) x m), rotations, rhs g
+    std::vector<double> H((size_t)(m + 1) * m * VC, 0.0), cs((size_t)m * VC),
+        sn((size_t)m * VC), g((size_t)(m + 1) * VC, 0.0);
+    for (int v = 0; v < VC; ++v) g[v] = beta[v];
+    std::vector<int> done(VC, 0), used(VC, 0);
+    for (int v = 0; v < VC; ++v)
+      if (worst_res[v] <= tol) done[v] = 1;
     int j = 0;
     for (; j < m && total_it < max_iter; ++j, ++total_it) {
       double* Vj = h->gm_V + (int64_t)j * P;
       double* Zj = h->gm_Z + (int64_t)j * P;
+      if (S > 1) {  // systems with every column converged leave the product
+        for (int q = 0; q < S; ++q) {
+          bool all = true;
+          for (int c = 0; c < nrhs; ++c) all &= done[(size_t)q * nrhs + c] != 0;
+          skip[q] = all;
+        }
+        CK(cudaMemcpyAsync(d_skip, skip.data(), (size_t)S, cudaMemcpyHostToDevice, h->stream));
+      }
       // Z_j = M^-1 V_j ; W = K Z_j
       CK(cudaMemcpyAsync(h->X, Vj, sizeof(double) * P, cudaMemcpyDeviceToDevice, h->stream));
       rc = solve_fast(h, nrhs);
@@ -687,56 +758,56 @@ int gmres_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double* d_x, i
       CK(cudaMemcpyAsync(Zj, h->X, sizeof(double) * P, cudaMemcpyDeviceToDevice, h->stream));
       for (int c0 = 0; c0 < nrhs; c0 += 16) {
         int nc = std::min(16, nrhs - c0);
-        rc = kmatvec_dev(h, nc, Zj + c0 * N, (int)N, h->ir_y + c0 * N, (int)N);
+        rc = kmatvec_dev(h, nc, Zj + c0 * N, (int)N, h->ir_y + c0 * N, (int)N, d_skip);
         if (rc) return rc;
       }
       CK(cudaMemcpyAsync(h->gm_W + (int64_t)j * P, h->ir_y, sizeof(double) * P,
                          cudaMemcpyDeviceToDevice, h->stream));
       // classical Gram-Schmidt, twice
-      std::vector<double> hsum((size_t)(j + 1) * nrhs, 0.0);
+      std::vector<double> hsum((size_t)(j + 1) * VC, 0.0);
       for (int pass = 0; pass < 2; ++pass) {
         rc = gm_dots(h, h->gm_V, j + 1, h->ir_y, nrhs, hcol);
         if (rc) return rc;
-        for (int c = 0; c < nrhs; ++c)
-          if (done[c])
-            for (int i = 0; i <= j; ++i) hcol[(size_t)i * nrhs + c] = 0.0;
+        for (int v = 0; v < VC; ++v)
+          if (done[v])
+            for (int i = 0; i <= j; ++i) hcol[(size_t)i * VC + v] = 0.0;
         rc = gm_sub(h, h->gm_V, j + 1, hcol, h->ir_y, nrhs);
         if (rc) return rc;
         for (size_t q = 0; q < hsum.size(); ++q) hsum[q] += hcol[q];
       }
       rc = gm_dots(h, h->ir_y, 1, h->ir_y, nrhs, tmp);
       if (rc) return rc;
-      std::vector<double> inv(nrhs, 0.0);
+      std::vector<double> inv(VC, 0.0);
       bool all_done = true;
-      for (int c = 0; c < nrhs; ++c) {
-        if (done[c]) continue;
-        double* Hc = &H[(size_t)c * (m + 1) * m];
-        for (int i = 0; i <= j; ++i) Hc[(size_t)j * (m + 1) + i] = hsum[(size_t)i * nrhs + c];
-        double hn = std::sqrt(std::max(tmp[c], 0.0));
+      for (int v = 0; v < VC; ++v) {
+        if (done[v]) continue;
+        double* Hc = &H[(size_t)v * (m + 1) * m];
+        for (int i = 0; i <= j; ++i) Hc[(size_t)j * (m + 1) + i] = hsum[(size_t)i * VC + v];
+        double hn = std::sqrt(std::max(tmp[v], 0.0));
         Hc[(size_t)j * (m + 1) + j + 1] = hn;
-        inv[c] = hn > 0 ? 1.0 / hn : 0.0;
+        inv[v] = hn > 0 ? 1.0 / hn : 0.0;
         // apply previous rotations, then a new one
         for (int i = 0; i < j; ++i) {
           double a = Hc[(size_t)j * (m + 1) + i], b2 = Hc[(size_t)j * (m + 1) + i + 1];
-          double ci = cs[(size_t)c * m + i], si = sn[(size_t)c * m + i];
+          double ci = cs[(size_t)v * m + i], si = sn[(size_t)v * m + i];
           Hc[(size_t)j * (m + 1) + i] = ci * a + si * b2;
           Hc[(size_t)j * (m + 1) + i + 1] = -si * a + ci * b2;
         }
         double a = Hc[(size_t)j * (m + 1) + j], b2 = Hc[(size_t)j * (m + 1) + j + 1];
         double r = std::hypot(a, b2);
         double ci = r > 0 ? a / r : 1.0, si = r > 0 ? b2 / r : 0.0;
-        cs[(size_t)c * m + j] = ci;
-        sn[(size_t)c * m + j] = si;
+        cs[(size_t)v * m + j] = ci;
+        sn[(size_t)v * m + j] = si;
         Hc[(size_t)j * (m + 1) + j] = r;
         Hc[(size_t)j * (m + 1) + j + 1] = 0.0;
-        double gj = g[(size_t)j * nrhs + c];
-        g[(size_t)j * nrhs + c] = ci * gj;
-        g[(size_t)(j + 1) * nrhs + c] = -si * gj;
-        used[c] = j + 1;
-        // stop this column a little below tol; the true residual decides
-        if (std::fabs(g[(size_t)(j + 1) * nrhs + c]) <= 0.5 * tol * bnorm[c] || hn == 0.0)
-          done[c] = 1;
-        if (!done[c]) all_done = false;
+        double gj = g[(size_t)j * VC + v];
+        g[(size_t)j * VC + v] = ci * gj;
+        g[(size_t)(j + 1) * VC + v] = -si * gj;
+        used[v] = j + 1;
+        // stop this column a little below tol; the residual update decides
+        if (std::fabs(g[(size_t)(j + 1) * VC + v]) <= 0.5 * tol * bnorm[v] || hn == 0.0)
+          done[v] = 1;
+        if (!done[v]) all_done = false;
       }
       rc = gm_scale(h, h->ir_y, inv, h->gm_V + (int64_t)(j + 1) * P, nrhs);
       if (rc) return rc;
@@ -746,17 +817,17 @@ int gmres_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double* d_x, i
         break;
       }
     }
-    // x += Z y, y from the triangular systems (per column)
-    std::vector<double> ycoef((size_t)m * nrhs, 0.0);
+    // x += Z y, y from the triangular systems (per virtual column)
+    std::vector<double> ycoef((size_t)m * VC, 0.0);
     int nv = 0;
-    for (int c = 0; c < nrhs; ++c) {
-      const int k = used[c];
+    for (int v = 0; v < VC; ++v) {
+      const int k = used[v];
       nv = std::max(nv, k);
-      const double* Hc = &H[(size_t)c * (m + 1) * m];
+      const double* Hc = &H[(size_t)v * (m + 1) * m];
       for (int i = k - 1; i >= 0; --i) {
-        double t = g[(size_t)i * nrhs + c];
-        for (int q = i + 1; q < k; ++q) t -= Hc[(size_t)q * (m + 1) + i] * ycoef[(size_t)q * nrhs + c];
-        ycoef[(size_t)i * nrhs + c] = Hc[(size_t)i * (m + 1) + i] != 0 ? t / Hc[(size_t)i * (m + 1) + i] : 0.0;
+        double t = g[(size_t)i * VC + v];
+        for (int q = i + 1; q < k; ++q) t -= Hc[(size_t)q * (m + 1) + i] * ycoef[(size_t)q * VC + v];
+        ycoef[(size_t)i * VC + v] = Hc[(size_t)i * (m + 1) + i] != 0 ? t / Hc[(size_t)i * (m + 1) + i] : 0.0;
       }
     }
     // r <- beta V_0 - W y (= r - K Z y), then x <- x + Z y
@@ -772,11 +843,16 @@ int gmres_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double* d_x, i
     (void)j;
   }
   if (iters) *iters = total_it;
-  if (relres)
-    for (int c = 0; c < nrhs; ++c) relres[c] = worst_res[c];
+  if (relres)  // per column, the worst system
+    for (int c = 0; c < nrhs; ++c) {
+      double w = 0.0;
+      for (int q = 0; q < S; ++q) w = std::max(w, worst_res[(size_t)q * nrhs + c]);
+      relres[c] = w;
+    }
   CK(cudaMemcpy2DAsync(d_x, sizeof(double) * ldx, h->ir_x, sizeof(double) * N,
                        sizeof(double) * N, nrhs, cudaMemcpyDeviceToDevice, h->stream));
   CK(cudaStreamSynchronize(h->stream));
+  dfree(h, d_skip);
   return check_dev_err(h, "gmres");
 }
 
