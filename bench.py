@@ -335,7 +335,7 @@ def run_ours(args, rank, world, local_rank):
         g.recLU_Compute()
 
     scale_pairs = {}
-    if not args.no_scale:
+    if not args.no_scale and world == 1:  # extra keys of the one-GPU line
         for key, cfg_name, n_cfg in SCALE_PAIRS:
             try:
                 scale_pairs[key] = run_scale_pair(stream, cfg_name, n_cfg)
