@@ -561,8 +561,8 @@ def run_profile_case(case):
 
     aca-profile: N=131072 2D uniform k-d ordered, Matern-3/2 l=0.2 + 1e-2
     delta, tol 1e-8, capacity hints large enough that every level is one
-    launch; the first aca_kernel launch is the top level (2 blocks of 65536^2,
-    148 CTAs each), whose W/V panels (~0.9 GB) exceed L2.
+    launch; the pooled deep levels launch first and the top level (2 blocks of
+    65536^2, 74 CTAs each) last, its W/V panels (~0.9 GB) far above L2.
     """
     from dense_hodlr_b200 import HODLR_Matrix, KernelSpec
     from dense_hodlr_b200.points import uniform_cube
