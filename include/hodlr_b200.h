@@ -261,7 +261,11 @@ int hodlr_set_index_tree_bounds(hodlr_t h, int nnodes, const int* split, const i
 /* Factor (if needed), direct solve, then iterative refinement with the FP64
  * residual until every system q has max_c ||b_c - K x_c|| / ||b_c|| <= tol
  * over its own rows (or max_iter corrections).  relres: nsys x nrhs,
- * system-major; a converged system's x is left unchanged afterwards. */
+ * system-major; a converged system's x is left unchanged afterwards, and its
+ * rows leave the full-kernel product.  hodlr_iterative_solve(_device) on a
+ * forest runs GMRES per system instead: every (system, column) pair has its
+ * own inner products, Hessenberg matrix and stopping test on the system's
+ * rows; relres[c] is then the worst system's residual of column c. */
 int hodlr_forest_refine_device(hodlr_t h, int nrhs, const double* d_b, int ldb, double* d_x,
                                int ldx, double tol, int max_iter, int* iters, double* relres);
 
