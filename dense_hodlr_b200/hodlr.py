@@ -140,7 +140,10 @@ class HODLR_Matrix:
 
     def __del__(self):
         if getattr(self, "_h", None):
-            _L.lib().hodlr_destroy(self._h)
+            try:
+                _L.lib().hodlr_destroy(self._h)
+            except TypeError:  # interpreter shutdown: the module globals are gone
+                pass
             self._h = None
 
     # ------------------------------------------------------------ setters
