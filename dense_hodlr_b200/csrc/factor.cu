@@ -22,11 +22,11 @@ int upload_plan(hodlr_t h, std::vector<GemmProblem>& probs, bool split, DevPlan&
   for (auto& p : probs) out.any_split |= p.splits > 1;
   if (out.nprob) {
     CK(dalloc(h, &out.probs, (size_t)out.nprob));
-    CK(h2d(h, out.probs, probs.data(), sizeof(GemmProblem) * out.nprob));
+    CK(h2d_async(h, out.probs, probs.data(), sizeof(GemmProblem) * out.nprob));
   }
   if (out.ntiles) {
     CK(dalloc(h, &out.tiles, (size_t)out.ntiles));
-    CK(h2d(h, out.tiles, tiles.data(), sizeof(int4) * out.ntiles));
+    CK(h2d_async(h, out.tiles, tiles.data(), sizeof(int4) * out.ntiles));
   }
   int rc = ensure_ws(h, ws);
   if (rc) return rc;
@@ -142,8 +142,7 @@ int do_factorize(hodlr_t h) {
   CK(dalloc(h, &h->d_lu, (size_t)tot));
   CK(dalloc(h, &h->d_lu_off, (size_t)nl));
   CK(dalloc(h, &h->d_perm, (size_t)N));
-  CK(cudaMemcpyAsync(h->d_lu_off, lu_off.data(), sizeof(int64_t) * nl, cudaMemcpyHostToDevice,
-                     h->stream));
+  CK(h2d_async(h, h->d_lu_off, lu_off.data(), sizeof(int64_t) * nl));
   // the assembled leaf blocks (N x smax, leaf (r0, s) at rows r0.., columns
   // 0..s-1): the residual of the refinement step of K^-1 U below
   double* Aleaf = nullptr;
@@ -215,17 +214,16 @@ int do_factorize(hodlr_t h) {
       CK(dalloc(h, &d_r0, nb));
       CK(dalloc(h, &d_m, nb));
       CK(dalloc(h, &d_rk, nb));
-      CK(cudaMemcpyAsync(d_r0, r0s.data(), 4 * nb, cudaMemcpyHostToDevice, h->stream));
-      CK(cudaMemcpyAsync(d_m, ms.data(), 4 * nb, cudaMemcpyHostToDevice, h->stream));
-      CK(cudaMemcpyAsync(d_rk, rk.data(), 4 * nb, cudaMemcpyHostToDevice, h->stream));
+      CK(h2d_async(h, d_r0, r0s.data(), 4 * nb));
+      CK(h2d_async(h, d_m, ms.data(), 4 * nb));
+      CK(h2d_async(h, d_rk, rk.data(), 4 * nb));
       int maxm = 0;
       for (int m : ms) maxm = std::max(maxm, m);
       dim3 grid(std::min(64, (maxm + 255) / 256), nb, std::min(L.kmax, 64));
       y_init_kernel<<<grid, 256, 0, h->stream>>>(L.Yl, L.W, N, L.kmax, d_r0, d_m, d_rk, nb);
       CK(cudaGetLastError());
       h->nlaunch += 1;
-      CK(cudaStreamSynchronize(h->stream));
-      dfree(h, d_r0);
+      dfree(h, d_r0);  // reused only after the stream has drained (DevPool)
       dfree(h, d_m);
       dfree(h, d_rk);
     }
@@ -301,9 +299,8 @@ int do_factorize(hodlr_t h) {
           tiles_cap = tiles.size();
         }
         for (int q = 0; q < 3; ++q)
-          CK(cudaMemcpyAsync(d_probs + (size_t)q * nl, probs[q].data(), sizeof(GemmProblem) * nl,
-                             cudaMemcpyHostToDevice, h->stream));
-        CK(h2d(h, d_tiles, tiles.data(), sizeof(int4) * tiles.size()));
+          CK(h2d_async(h, d_probs + (size_t)q * nl, probs[q].data(), sizeof(GemmProblem) * nl));
+        CK(h2d_async(h, d_tiles, tiles.data(), sizeof(int4) * tiles.size()));
         for (int q = 0; q < 3; ++q) {
           rc = check_gemm(h, probs[q], false, "factor: leaf inverse product");
           if (rc) return rc;
@@ -352,8 +349,7 @@ int do_factorize(hodlr_t h) {
     CK(dalloc(h, &L.S, (size_t)s_tot));
     CK(dalloc(h, &L.piv, (size_t)p_tot));
     CK(dalloc(h, &L.d_nodes, (size_t)nn));
-    CK(cudaMemcpyAsync(L.d_nodes, L.nodes.data(), sizeof(SchurNode) * nn,
-                       cudaMemcpyHostToDevice, h->stream));
+    CK(h2d_async(h, L.d_nodes, L.nodes.data(), sizeof(SchurNode) * nn));
     if (z_tot > h->z_cap) {
       dfree(h, h->Z);
       CK(dalloc(h, &h->Z, (size_t)z_tot));

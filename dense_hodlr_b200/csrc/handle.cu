@@ -110,18 +110,54 @@ int ensure_ws(hodlr_t h, int64_t elems) {
 // non-blocking stream, so a synchronous cudaMemcpy (legacy default stream) is
 // not ordered with its kernels; every copy goes through these instead and
 // returns after the stream has drained.
+// Each of them drains the stream, after which the pinned staging memory of
+// h2d_async is free again.
+static cudaError_t drained(hodlr_t h, cudaError_t e) {
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e == cudaSuccess) h->pin_used = 0;
+  return e;
+}
 cudaError_t h2d(hodlr_t h, void* dst, const void* src, size_t bytes) {
-  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, h->stream);
-  return e != cudaSuccess ? e : cudaStreamSynchronize(h->stream);
+  return drained(h, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, h->stream));
 }
 cudaError_t d2h(hodlr_t h, void* dst, const void* src, size_t bytes) {
-  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, h->stream);
-  return e != cudaSuccess ? e : cudaStreamSynchronize(h->stream);
+  return drained(h, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, h->stream));
+}
+
+// A pageable cudaMemcpyAsync to the device synchronises the stream before it
+// starts, so the host would wait for every queued kernel before planning the
+// next launches.  These uploads go through pinned staging memory instead:
+// the host copies the bytes there and queues the copy.  The staging area is
+// reused once the stream has drained (any of the calls above), or here when
+// it is full.
+cudaError_t h2d_async(hodlr_t h, void* dst, const void* src, size_t bytes) {
+  if (bytes == 0) return cudaSuccess;
+  const size_t need = (bytes + 255) & ~(size_t)255;
+  if (h->pin_used + need > h->pin_cap) {
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return e;
+    h->pin_used = 0;
+    if (need > h->pin_cap) {
+      if (h->pin) cudaFreeHost(h->pin);
+      h->pin = nullptr;
+      h->pin_cap = 0;
+      const size_t cap = std::max(need, (size_t)8 << 20);
+      e = cudaMallocHost((void**)&h->pin, cap);
+      if (e != cudaSuccess) {
+        h->pin = nullptr;
+        return e;
+      }
+      h->pin_cap = cap;
+    }
+  }
+  char* p = h->pin + h->pin_used;
+  memcpy(p, src, bytes);
+  h->pin_used += need;
+  return cudaMemcpyAsync(dst, p, bytes, cudaMemcpyHostToDevice, h->stream);
 }
 cudaError_t copy2d(hodlr_t h, void* dst, size_t dpitch, const void* src, size_t spitch,
                    size_t width, size_t rows, cudaMemcpyKind kind) {
-  cudaError_t e = cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, rows, kind, h->stream);
-  return e != cudaSuccess ? e : cudaStreamSynchronize(h->stream);
+  return drained(h, cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, rows, kind, h->stream));
 }
 
 int check_dev_err(hodlr_t h, const char* where) {

@@ -260,6 +260,9 @@ struct hodlr_handle_s {
   // allocated, 0 never, 1 always (hodlr_set_factor_in_place)
   int in_place = -1;
   bool w_consumed = false;  // some level's W holds K^-1 U: recompress before refactoring
+  // pinned host staging of uploads that do not wait for the stream (h2d_async)
+  char* pin = nullptr;
+  size_t pin_cap = 0, pin_used = 0;
   double* ws = nullptr;  // GEMM split-K / kmatvec workspace
   int64_t ws_cap = 0;
   double* Z = nullptr;  // per-level Schur right-hand sides (factor)
@@ -336,6 +339,9 @@ bool user_subtree(hodlr_t h, int level, int mn, int mx, int u, std::vector<char>
 void build_tree(hodlr_t h);
 int ensure_ws(hodlr_t h, int64_t elems);
 cudaError_t h2d(hodlr_t h, void* dst, const void* src, size_t bytes);
+// Upload without waiting: src is copied into the handle's pinned staging
+// memory at once (src may be reused on return) and the copy is queued.
+cudaError_t h2d_async(hodlr_t h, void* dst, const void* src, size_t bytes);
 cudaError_t d2h(hodlr_t h, void* dst, const void* src, size_t bytes);
 cudaError_t copy2d(hodlr_t h, void* dst, size_t dpitch, const void* src, size_t spitch,
                    size_t width, size_t rows, cudaMemcpyKind kind);

@@ -281,6 +281,7 @@ void hodlr_destroy(hodlr_t h) {
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->pin) cudaFreeHost(h->pin);
   h->pool.release_all(h->stream);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
   delete h;

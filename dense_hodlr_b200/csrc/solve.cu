@@ -34,7 +34,7 @@ int build_solve_plans(hodlr_t h, int nrhs) {
     }
     dfree(h, L.d_snodes);
     CK(dalloc(h, &L.d_snodes, (size_t)nn));
-    CK(h2d(h, L.d_snodes, sn.data(), sizeof(SchurNode) * nn));
+    CK(h2d_async(h, L.d_snodes, sn.data(), sizeof(SchurNode) * nn));
     std::vector<GemmProblem> tn, up;
     for (int p = 0; p < nn; ++p) {
       const int sd = sn[p].kb + sn[p].kt;
