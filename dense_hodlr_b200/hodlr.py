@@ -268,9 +268,11 @@ class HODLR_Matrix:
                         init_LRTolerance=None, input_LR_Method="partialPiv_ACA",
                         directSolve_Method="recLU", restart=32):
         """iterative_Solve (include/HODLR_Matrix.hpp:219): HODLR-preconditioned
-        GMRES from the recLU solution, to a true relative residual of
-        stop_tolerance.  Returns the solution like the reference; the iteration
-        count and residuals are kept in self.last_iterations / last_relres."""
+        GMRES from the recLU solution, to a relative residual ||b - K x|| / ||b||
+        of stop_tolerance with the full FP64 kernel (formed once by a product,
+        then updated from the products of the iterations).  Returns the
+        solution like the reference; the iteration count and residuals are
+        kept in self.last_iterations / last_relres."""
         if init_LRTolerance is not None:
             self.set_LRTolerance(init_LRTolerance)
         self.set_LRMethod(input_LR_Method)
