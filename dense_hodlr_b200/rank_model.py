@@ -78,6 +78,7 @@ def generate(kind, pairs, seed=0, max_seconds=900.0, log=None):
         l = float(np.exp(rng.uniform(np.log(0.05), np.log(0.5))))
         tol = float(rng.choice([1e-6, 1e-8, 1e-10]))
         run += 1
+        tr = time.time()
         try:
             F, T = block_dataset(cloud(name, n, seed * 1000 + run), kind, l, tol, leaf)
         except HODLRError as e:  # e.g. a rank beyond ACA's shared-memory limit
@@ -87,6 +88,9 @@ def generate(kind, pairs, seed=0, max_seconds=900.0, log=None):
         Fs.append(F)
         Ts.append(T)
         total += len(T)
+        if log:
+            log(f"run {run} {name} n={n} leaf={leaf} l={l:.3f} tol={tol:g}: "
+                f"{len(T)} blocks in {time.time() - tr:.2f} s, total {total}")
     return np.concatenate(Fs), np.concatenate(Ts)
 
 
