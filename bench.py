@@ -691,10 +691,11 @@ def run_tune(case):
 
 def run_aca_ab(case):
     """ACA with the top levels' panels streamed through the bulk-copy ring
-    against per-thread loads, case 'aca-ab[:N[:cfg]]' (default: the FP64
-    workload's cloud at N = 262144; cfg 'c5' for the sphere / Matern tol 1e-10
-    shape): one compression each way (after a warm-up), the ACA time and
-    algorithmic GB/s of each, and whether ranks and pivots agree."""
+    (mode 1: one copy per column; mode 2: one 2D tensor copy per tile)
+    against per-thread loads (mode 0), case 'aca-ab[:N[:cfg]]' (default: the
+    FP64 workload's cloud at N = 262144; cfg 'c5' for the sphere / Matern tol
+    1e-10 shape): one compression each way (after a warm-up), the ACA time
+    and algorithmic GB/s of each, and whether ranks and pivots agree."""
     from dense_hodlr_b200 import HODLR_Matrix, KernelSpec
     parts = case.split(":")
     n = int(parts[1]) if len(parts) > 1 and parts[1] else N_PTS
@@ -709,7 +710,7 @@ def run_aca_ab(case):
         spec, leaf, tol = KernelSpec("matern32", LSCALE, SHIFT), LEAF, TOL
     out = {"case": "aca-ab", "n": n, "cfg": cfg}
     res = {}
-    for on in (1, 0, 1):
+    for on in (1, 2, 0, 1, 2):
         g = HODLR_Matrix(n, n, spec, pts, leaf)
         g.set_LRTolerance(tol)
         g.set_aca_streaming(on)
@@ -721,11 +722,10 @@ def run_aca_ab(case):
                               "lr_s": g.get_LR_ComputationTime(),
                               "max_rank": int(g.ranks().max())}
         del g
-    r1, p1 = res[1]
     r0, p0 = res[0]
-    out["ranks_equal"] = bool(np.array_equal(r1, r0))
+    out["ranks_equal"] = all(bool(np.array_equal(res[m][0], r0)) for m in (1, 2))
     out["pivots_equal"] = all(np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
-                              for a, b in zip(p1, p0))
+                              for m in (1, 2) for a, b in zip(res[m][1], p0))
     return out
 
 

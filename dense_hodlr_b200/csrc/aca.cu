@@ -361,6 +361,53 @@ __device__ void wring_issue(WRing& R, int w, uint32_t tw, const double* P, int64
         : "memory");
 }
 
+// Lane 0: the same tile as wring_issue, as one 2D tensor copy of the whole
+// box (WR_ROWS rows from arena row x, WR_BC columns from column y).  Rows or
+// columns past the slice land in the stage unread (the consumer masks them);
+// past the arena they are zero-filled, and the transaction always counts the
+// full box.  x is even by construction (16-byte aligned start) and every
+// stage starts on a 128-byte boundary (the ring heads dynamic shared memory,
+// stages are 4 KB); a copy breaking either rule would be invalid, so it is
+// refused: the stage completes without data and the launch reports
+// DEV_ERR_INDEX.
+__device__ void wring_issue_tile(WRing& R, int w, uint32_t tw, const CUtensorMap* map, int x,
+                                 int y, unsigned* err) {
+  const int slot = (int)(tw % (uint32_t)R.stages);
+  uint64_t* bar = R.full + w * WR_SMAX + slot;
+  double* dst = R.buf + ((size_t)(w * R.stages + slot) * WR_BC) * WR_ROWS;
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  if ((x & 1) || (smem_addr(dst) & 127u)) {
+    atomicOr(err, DEV_ERR_INDEX);
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+    return;
+  }
+  constexpr uint32_t bytes = (uint32_t)(sizeof(double) * WR_ROWS * WR_BC);
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+               "r"(bytes)
+               : "memory");
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_addr(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_addr(bar))
+      : "memory");
+}
+
+// Lane 0, before the CTA exits: every copy this warp issued has landed.
+// In normal flow each issued tile was waited for; a wait that gave up (an
+// error raised elsewhere in the launch) can leave copies in flight, and the
+// CTA's shared memory must not be released under them.  A stage's tiles
+// complete in issue order, so waiting for the last tile of each stage (the
+// last `stages` tiles) suffices; each wait is bounded.
+__device__ void wring_drain(const WRing& R, int w) {
+  const uint32_t t0 = R.t > (uint32_t)R.stages ? R.t - (uint32_t)R.stages : 0u;
+  for (uint32_t tw = t0; tw < R.t; ++tw) {
+    uint64_t* bar = R.full + w * WR_SMAX + (int)(tw % (uint32_t)R.stages);
+    const uint32_t parity = (tw / (uint32_t)R.stages) & 1u;
+    for (uint32_t polls = 0; polls < (1u << 20) && !mbar_try(bar, parity); ++polls)
+      __nanosleep(64);
+  }
+}
+
 // residual_pass with every warp streaming its own rows through its ring.
 // gbase: the global row of P[0] (the block's first column for V, first row
 // for W).  The same arithmetic as residual_pass, element for element: the
@@ -395,12 +442,19 @@ __device__ void residual_pass_wring(const AcaLaunch& L, const AcaBlock& B, doubl
     // this warp's earlier generic stores to these rows, then the copies
     asm volatile("fence.proxy.async.global;" ::: "memory");
   }
+  const CUtensorMap* map = ROW ? &L.map_v : &L.map_w;  // the arena P lies in (ring_tile)
   bool first = true;
   for (int jb = wlo; jb < whi; jb += WR_ROWS, first = false) {
     const int count = (min(WR_ROWS, whi - jb) + 1) & ~1;
+    // lane 0: tile q of this chunk into the warp's stage for tile number tw
+    auto issue = [&](uint32_t tw, int q) {
+      if (L.ring_tile)
+        wring_issue_tile(R, w, tw, map, gbase + jb, q * WR_BC, L.err);
+      else
+        wring_issue(R, w, tw, P, ld, jb, count, q * WR_BC, min(WR_BC, k - q * WR_BC));
+    };
     if (lane == 0)
-      for (int q = 0; q < tpc && q < R.stages; ++q)
-        wring_issue(R, w, R.t + q, P, ld, jb, count, q * WR_BC, min(WR_BC, k - q * WR_BC));
+      for (int q = 0; q < tpc && q < R.stages; ++q) issue(R.t + q, q);
     int jj[E];
     bool ok[E];
     double s[E], vp[E];
@@ -462,9 +516,7 @@ __device__ void residual_pass_wring(const AcaLaunch& L, const AcaBlock& B, doubl
         }
       }
       __syncwarp();
-      if (lane == 0 && q + R.stages < tpc)
-        wring_issue(R, w, tw + R.stages, P, ld, jb, count, (q + R.stages) * WR_BC,
-                    min(WR_BC, k - (q + R.stages) * WR_BC));
+      if (lane == 0 && q + R.stages < tpc) issue(tw + R.stages, q + R.stages);
     }
     R.t += tpc;
 #pragma unroll
@@ -538,7 +590,7 @@ __device__ double resolve_eps(Shared& sh, const AcaLaunch& L, const AcaBlock& B,
 // shared memory then starts with the rings' wring_bytes(L.ring_stages).
 // T: the element type of the W/V panels (double).
 template <int NT, int E, bool RING, typename T>
-__global__ void __launch_bounds__(NT, (NT == 512 ? 1 : NT == 256 ? 2 : 4)) aca_kernel(AcaLaunch L) {
+__global__ void __launch_bounds__(NT, (NT == 512 ? 1 : NT == 256 ? 2 : 4)) aca_kernel(const __grid_constant__ AcaLaunch L) {
   extern __shared__ __align__(128) double dyn_all[];
   __shared__ Shared sh;
   __shared__ __align__(8) uint64_t ring_full[RING ? WR_NW * WR_SMAX : 1];
@@ -856,6 +908,8 @@ __global__ void __launch_bounds__(NT, (NT == 512 ? 1 : NT == 256 ? 2 : 4)) aca_k
     st->svp = svp;
     st->pending = pending;
   }
+  if constexpr (RING)
+    if ((tid & 31) == 0) wring_drain(ring, tid >> 5);
 }
 
 }  // namespace
@@ -866,6 +920,53 @@ int aca_ring_stages(int kcap_max) {
   for (int st = WR_SMAX; st >= 2; --st)
     if (wring_bytes(st) + sizeof(double) * (size_t)kcap_max <= 224 * 1024) return st;
   return 0;
+}
+
+namespace {
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library); null when the driver does not provide it.
+EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault,
+                                         &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      p = nullptr;
+    }
+    return reinterpret_cast<EncodeTiledFn>(p);
+  }();
+  return fn;
+}
+
+// A 2D map over an n x kcap column-major arena (leading dimension n) whose
+// box is one ring tile: WR_ROWS rows by WR_BC columns.  The copy's start row
+// must give a 16-byte aligned address; the kernel keeps it even.
+bool panel_map(CUtensorMap* m, const double* base, int64_t n, int kcap) {
+  EncodeTiledFn f = encode_tiled();
+  if (!f || !base || ((uintptr_t)base & 15) || (n & 1) || n <= 0 || kcap <= 0) return false;
+  const cuuint64_t dim[2] = {(cuuint64_t)n, (cuuint64_t)kcap};
+  const cuuint64_t stride[1] = {(cuuint64_t)n * sizeof(double)};
+  const cuuint32_t box[2] = {(cuuint32_t)WR_ROWS, (cuuint32_t)WR_BC};
+  const cuuint32_t elem[2] = {1, 1};
+  return f(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double*>(base), dim, stride, box,
+           elem, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+}  // namespace
+
+// The launch's W and V maps for one tensor copy per ring tile; false (and
+// the per-column copies) when either cannot be encoded.
+bool aca_ring_tile_maps(AcaLaunch& L, const double* W, const double* V, int64_t n, int kcap) {
+  return panel_map(&L.map_w, W, n, kcap) && panel_map(&L.map_v, V, n, kcap);
 }
 
 static size_t aca_smem(int nt, int kcap_max, bool global_dots, bool ring, bool f32) {

@@ -61,7 +61,7 @@ bool level_done(const Level& L) {
 // One ACA launch over `blocks`: groups of G CTAs each, or, with `groups`,
 // groups[i] CTAs for block i (a CTA table maps CTAs to blocks).
 int run_aca(hodlr_t h, std::vector<AcaBlock>& blocks, int G, int nt, int kcap_max,
-            bool ring, const std::vector<int>* groups) {
+            bool ring, const std::vector<int>* groups, const Level* arena) {
   const int nb = (int)blocks.size();
   if (nb == 0) return HODLR_OK;
   int ncta = nb * G;
@@ -122,6 +122,12 @@ int run_aca(hodlr_t h, std::vector<AcaBlock>& blocks, int G, int nt, int kcap_ma
   L.dotg_stride = 0;
   L.ring = ring ? 1 : 0;
   L.ring_stages = ring ? aca_ring_stages(kcap_max) : 0;
+  // one tensor copy per ring tile needs every block's panels in the level's
+  // arenas (fill_block: W + r0, V + c0); a map that cannot be encoded keeps
+  // the per-column copies
+  L.ring_tile = 0;
+  if (ring && h->aca_ring_tile && arena && arena->kcap == kcap_max)
+    L.ring_tile = aca_ring_tile_maps(L, arena->W, arena->V, h->n, arena->kcap) ? 1 : 0;
   // slices of a group shorter than 768 rows: the 2-element instance (512-row
   // chunks) leaves fewer lanes idle than the 4-element one (1024-row chunks)
   L.narrow = 0;
@@ -391,7 +397,7 @@ int do_compress(hodlr_t h) {
       for (;;) {  // a cooperative launch the driver refuses is retried with half the groups
         L.G = G;
         for (int q = 0; q < nb; ++q) fill_block(h, L, q, bl[q]);
-        rc = run_aca(h, bl, G, ring ? 512 : G > 1 ? 256 : 128, L.kcap, ring);
+        rc = run_aca(h, bl, G, ring ? 512 : G > 1 ? 256 : 128, L.kcap, ring, nullptr, &L);
         if (rc != HODLR_ERR_RETRY_SMALLER) break;
         if (G == 1) return fail(h, HODLR_ERR_CUDA, "aca_launch: cooperative launch refused");
         G = std::max(1, G / 2);

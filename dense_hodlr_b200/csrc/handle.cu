@@ -233,6 +233,13 @@ int init_common(hodlr_t h) {
   if (!coop) return fail(h, HODLR_ERR_UNSUPPORTED, "device lacks cooperative launch");
   const char* chk = getenv("HODLR_CHECKED");
   h->checked = chk && *chk && strcmp(chk, "0") != 0;
+  // HODLR_ACA_STREAMING=0|1|2: the ACA panel streaming mode of new handles
+  // (hodlr_set_aca_streaming); unset or anything else keeps the default
+  const char* acs = getenv("HODLR_ACA_STREAMING");
+  if (acs && acs[0] >= '0' && acs[0] <= '2' && acs[1] == 0) {
+    h->aca_ring = acs[0] != '0';
+    h->aca_ring_tile = acs[0] == '2';
+  }
   CK(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
   h->stream = h->own_stream;
   CK(cudaEventCreate(&h->ev0));

@@ -49,6 +49,7 @@ int aca_max_coresident(int nt, int kcap_max, bool ring, bool f32, int* per_sm);
 bool aca_dots_global(int nt, int kcap_max, bool ring, bool f32);
 size_t aca_smem_bytes(int nt, int kcap_max, bool ring, bool f32);
 int aca_ring_stages(int kcap_max);
+bool aca_ring_tile_maps(AcaLaunch& L, const double* W, const double* V, int64_t n, int kcap);
 
 namespace hodlr_impl {
 
@@ -232,10 +233,12 @@ struct hodlr_handle_s {
   std::vector<hodlr_impl::Level> lv;
   std::vector<int> cap_hint;  // initial W/V columns per level (0 = default)
   int gemm_prec = HODLR_GEMM_FP64;  // arithmetic of the Woodbury products
-  // group-level ACA panels through the warps' bulk-copy rings (measured
-  // 4.61 vs 3.65 TB/s of per-thread loads on the sphere shape at N = 262144,
-  // 2.85 vs 2.37 on the 2D cloud; the same bits either way)
+  // group-level ACA panels through the warps' rings (per-thread loads: 3.59
+  // TB/s on the sphere shape at N = 262144, 2.38 on the 2D cloud) ...
   bool aca_ring = true;
+  // ... each ring tile one 2D tensor copy (4.87 and 3.30 TB/s) rather than
+  // one bulk copy per column (4.28 and 2.85 TB/s); the same bits every way
+  bool aca_ring_tile = true;
   // factorization form (hodlr_set_solver_form): false recLU's Schur systems
   // [bottom; top], true recSM's perturbI systems [top; bottom]
   bool sm_form = false;
@@ -358,7 +361,8 @@ int grow_level(hodlr_t h, Level& L, int cap);
 void fill_block(hodlr_t h, Level& L, int q, AcaBlock& B);
 bool level_done(const Level& L);
 int run_aca(hodlr_t h, std::vector<AcaBlock>& blocks, int G, int nt, int kcap_max,
-            bool ring = false, const std::vector<int>* groups = nullptr);
+            bool ring = false, const std::vector<int>* groups = nullptr,
+            const Level* arena = nullptr);
 int init_level(hodlr_t h, Level& L, int cap);
 int sync_level(hodlr_t h, Level& L, bool* done);
 int level_kmax(const Level& L);

@@ -486,8 +486,9 @@ int hodlr_set_checked(hodlr_t h, int on) {
 }
 
 int hodlr_set_aca_streaming(hodlr_t h, int on) {
-  if (!h || on < 0 || on > 1) return HODLR_ERR_ARG;
+  if (!h || on < 0 || on > 2) return HODLR_ERR_ARG;
   h->aca_ring = on != 0;
+  h->aca_ring_tile = on == 2;
   return HODLR_OK;
 }
 

@@ -1,6 +1,7 @@
 // Internal structures shared by the kernels and the host orchestration.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -81,4 +82,10 @@ struct AcaLaunch {
   unsigned spin_limit;   // polls of a group barrier before it gives up (DEV_ERR_TIMEOUT)
   unsigned bar_extra;    // arrivals a group barrier waits for beyond its G CTAs (0; 1 makes
                          // every barrier unreachable, to exercise the timeout path)
+  int ring_tile;         // 1 (with ring): each ring tile is one 2D tensor copy through
+                         // map_w / map_v instead of one bulk copy per column
+  // 2D maps over the level's W and V arenas (rows: N, columns: the level's
+  // kcap, row stride ld), box WR_ROWS rows x WR_BC columns; set when ring_tile
+  alignas(64) CUtensorMap map_w;
+  alignas(64) CUtensorMap map_v;
 };

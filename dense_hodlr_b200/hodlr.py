@@ -182,8 +182,10 @@ class HODLR_Matrix:
         _check(self._h, _L.lib().hodlr_set_checked(self._h, int(bool(on))))
 
     def set_aca_streaming(self, on):
-        """Top-level ACA panels through the bulk-copy rings (1, default) or per-thread loads (0)."""
-        _check(self._h, _L.lib().hodlr_set_aca_streaming(self._h, int(bool(on))))
+        """Top-level ACA panels through the warps' rings, one 2D tensor copy per
+        ring tile (2, default) or one bulk copy per panel column (1), or loaded
+        per thread (0).  Same results in every mode."""
+        _check(self._h, _L.lib().hodlr_set_aca_streaming(self._h, int(on)))
 
     def set_factor_in_place(self, mode):
         """K^-1 U over the U panels: 1 always, 0 never, -1 (default) only when

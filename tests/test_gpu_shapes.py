@@ -138,11 +138,12 @@ def test_factor_in_place_matches_separate_panels(oracle_mod):
 @pytest.mark.parametrize("n,dim", [(32768, 2), (20000, 3)])
 def test_ring_streaming_bit_identical_to_per_thread_loads(n, dim):
     """The top-level ACA with its panel slices streamed through the bulk-copy
-    ring (hodlr_set_aca_streaming(1)) against per-thread loads: the same
-    pivots, ranks, iteration counts and W/V bits on every block."""
+    ring, one copy per column (hodlr_set_aca_streaming(1)) or one 2D tensor
+    copy per tile (2), against per-thread loads: the same pivots, ranks,
+    iteration counts and W/V bits on every block."""
     pts = uniform_cube(n, dim, 13)
     out = []
-    for on in (0, 1):
+    for on in (0, 1, 2):
         g = HODLR_Matrix(n, n, KernelSpec("matern32", 0.2, 1e-2), pts, 128)
         g.set_LRTolerance(1e-8)
         g.set_aca_streaming(on)
@@ -150,12 +151,13 @@ def test_ring_streaming_bit_identical_to_per_thread_loads(n, dim):
         nb = g.num_blocks()
         out.append((g.ranks(), [g.block_info(b)["iters"] for b in range(nb)],
                     [g.pivots(b) for b in range(nb)], [g.lowrank(b) for b in range(8)]))
-    (r0, i0, p0, f0), (r1, i1, p1, f1) = out
-    assert np.array_equal(r0, r1) and i0 == i1
-    for a, b in zip(p0, p1):
-        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
-    for (W0, V0), (W1, V1) in zip(f0, f1):
-        assert np.array_equal(W0, W1) and np.array_equal(V0, V1)
+    r0, i0, p0, f0 = out[0]
+    for r1, i1, p1, f1 in out[1:]:
+        assert np.array_equal(r0, r1) and i0 == i1
+        for a, b in zip(p0, p1):
+            assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+        for (W0, V0), (W1, V1) in zip(f0, f1):
+            assert np.array_equal(W0, W1) and np.array_equal(V0, V1)
 
 
 def test_checked_mode_gives_the_same_solution():

@@ -22,7 +22,7 @@ pytestmark = pytest.mark.gpu
 HODLR_ERR_TIMEOUT = 8
 
 
-@pytest.mark.parametrize("streaming", [1, 0])
+@pytest.mark.parametrize("streaming", [2, 1, 0])
 def test_aca_group_barrier_times_out_and_the_handle_recovers(streaming):
     n = 32768  # the top levels run with groups of CTAs per block
     pts = uniform_cube(n, 2, 77)
